@@ -1,0 +1,410 @@
+"""Test infrastructure, not product code.
+
+ctypes front ends for the two CPU checkers of the CUDA backend:
+
+* ``Oracle`` - the plain-C restatement in ``rsd_oracle.c`` (``_build/librsd_oracle.so``);
+* ``Reference`` - the Residuum reference templates compiled unmodified through
+  ``ref_harness.cpp`` (``_ref/libresiduum_ref.so``), present wherever ``build()`` could see the
+  reference checkout.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU legs import this package.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "librsd_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libresiduum_ref.so")
+
+_P = C.c_void_p
+_D = C.c_double
+_I32 = C.c_int32
+_I64 = C.c_int64
+
+
+def build(ref_root="/root/reference"):
+    """Compile the restatement and, when the reference checkout exists, the reference harness."""
+    env = dict(os.environ)
+    targets = ["all"] if os.path.isdir(ref_root) else [os.path.join(HERE, "_build", "librsd_oracle.so")]
+    subprocess.run(["make", "-s", "-C", HERE, "REF=" + ref_root] + targets, check=True, env=env)
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_P)
+
+
+def _f64(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Report(C.Structure):
+    _fields_ = [("converged", _I32), ("iterations", _I64), ("initialResidual", _D),
+                ("finalResidual", _D), ("finalResidualRel", _D)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# ---------------------------------------------------------------------------------------------
+# restatement
+# ---------------------------------------------------------------------------------------------
+class _Mesh(C.Structure):
+    _fields_ = [("nsd", _I32), ("order", _I32), ("nnodes", _I64), ("nelem", _I64), ("npe", _I32),
+                ("nfaces", _I32), ("xyz", C.POINTER(_D)), ("ien", C.POINTER(_I64)), ("rng", C.POINTER(_I32))]
+
+
+class _Model(C.Structure):
+    _fields_ = [("nq", _I32), ("k_expr", C.c_char_p), ("dk_expr", C.c_char_p), ("k_const", _D),
+                ("k_elem", _P), ("rho", _D), ("cp", _D), ("src_expr", C.c_char_p), ("bc_expr", C.c_char_p * 6)]
+
+
+_olib = None
+
+
+def oracle_lib():
+    global _olib
+    if _olib is None:
+        if not os.path.exists(ORACLE_SO):
+            raise RuntimeError("oracle library missing: run oracle.build() (make -C oracle)")
+        L = C.CDLL(ORACLE_SO)
+        L.ro_mesh_block.argtypes = [_I32, _P, _P, _P, _I32, C.POINTER(_Mesh)]
+        L.ro_mesh_free.argtypes = [C.POINTER(_Mesh)]
+        L.ro_problem_create.argtypes = [C.POINTER(_Mesh), C.POINTER(_Model)]
+        L.ro_problem_create.restype = _P
+        L.ro_problem_destroy.argtypes = [_P]
+        L.ro_last_error.restype = C.c_char_p
+        L.ro_num_free.argtypes = [_P]; L.ro_num_free.restype = _I64
+        L.ro_nnz.argtypes = [_P]; L.ro_nnz.restype = _I64
+        L.ro_dofmap.argtypes = [_P, _P, _P, _P]
+        L.ro_pattern.argtypes = [_P, _P, _P]
+        L.ro_set_time.argtypes = [_P, _D]
+        L.ro_bc_node_values.argtypes = [_P, _P]
+        L.ro_assemble_matrix.argtypes = [_P, _D, _D, _D, _D, _P, _P, _P]
+        L.ro_assemble_vector.argtypes = [_P, _I32, _D, _P, _P, _P, _P]
+        L.ro_lift.argtypes = [_P, _D, _D, _P]
+        L.ro_diagonal.argtypes = [_P, _D, _D, _P, _P]
+        L.ro_adjoint_gradient.argtypes = [_P, _P, _P, _P]
+        L.ro_spmv.argtypes = [_I64, _P, _P, _P, _P, _P]
+        L.ro_csr_solve.argtypes = [_I32, _I32, _I64, _P, _P, _P, _P, _P, _D, _I64, _I64, C.POINTER(Report)]
+        L.ro_steady.argtypes = [_P, _I32, _I32, _D, _I64, _I64, _P, C.POINTER(Report)]
+        L.ro_backward_euler.argtypes = [_P, _D, _I64, _I32, _I32, _D, _I64, _I64, _P, _P, _P]
+        L.ro_newton.argtypes = [_P, _D, _D, _I64, _I32, _I32, _D, _I64, _I64, _P, C.POINTER(Report)]
+        L.ro_expr_eval.argtypes = [C.c_char_p, _D, _D, _D, _D, _D, C.POINTER(_D)]
+        _olib = L
+    return _olib
+
+
+def expr_eval(src, t=0.0, x=0.0, y=0.0, z=0.0, T=0.0):
+    out = _D()
+    if oracle_lib().ro_expr_eval(src.encode(), t, x, y, z, T, C.byref(out)):
+        raise ValueError(oracle_lib().ro_last_error().decode())
+    return out.value
+
+
+class BlockMesh:
+    """BlockMesh2D/3D through the restatement; arrays copied out as numpy."""
+
+    def __init__(self, nsd, nel, lo, hi, order):
+        L = oracle_lib()
+        self._m = _Mesh()
+        nel = np.asarray(list(nel) + [1] * (3 - len(nel)), dtype=np.int32)
+        lo = np.asarray(list(lo) + [0.0] * (3 - len(lo)), dtype=np.float64)
+        hi = np.asarray(list(hi) + [0.0] * (3 - len(hi)), dtype=np.float64)
+        if L.ro_mesh_block(nsd, _ptr(nel), _ptr(lo), _ptr(hi), order, C.byref(self._m)):
+            raise ValueError(L.ro_last_error().decode())
+        m = self._m
+        self.nsd, self.order, self.npe, self.nfaces = m.nsd, m.order, m.npe, m.nfaces
+        self.nnodes, self.nelem = m.nnodes, m.nelem
+        self.xyz = np.ctypeslib.as_array(m.xyz, shape=(m.nnodes * m.nsd,)).copy()
+        self.ien = np.ctypeslib.as_array(m.ien, shape=(m.nelem * m.npe,)).copy()
+        self.rng = np.ctypeslib.as_array(m.rng, shape=(m.nelem * m.nfaces,)).copy()
+
+    def __del__(self):
+        try:
+            oracle_lib().ro_mesh_free(C.byref(self._m))
+        except Exception:
+            pass
+
+
+class Oracle:
+    """The restatement for one mesh + model: dof map, pattern, element loops, solvers, stages."""
+
+    def __init__(self, mesh, nq, k_const=1.0, k_expr=None, dk_expr=None, k_elem=None, rho=1.0, cp=1.0,
+                 src_expr=None, bc=None):
+        L = oracle_lib()
+        self.mesh = mesh
+        self._kelem = None if k_elem is None else _f64(k_elem)
+        md = _Model()
+        md.nq = nq
+        md.k_expr = k_expr.encode() if k_expr else None
+        md.dk_expr = dk_expr.encode() if dk_expr else None
+        md.k_const = k_const
+        md.k_elem = _ptr(self._kelem)
+        md.rho, md.cp = rho, cp
+        md.src_expr = src_expr.encode() if src_expr else None
+        for tag, ex in (bc or {}).items():
+            md.bc_expr[tag] = ex.encode()
+        self._model = md
+        self.h = L.ro_problem_create(C.byref(mesh._m), C.byref(md))
+        if not self.h:
+            raise ValueError(L.ro_last_error().decode())
+        self.n = L.ro_num_free(self.h)
+        self.nnz = L.ro_nnz(self.h)
+
+    def __del__(self):
+        try:
+            oracle_lib().ro_problem_destroy(self.h)
+        except Exception:
+            pass
+
+    def dofmap(self):
+        t2a = np.zeros(self.mesh.nnodes, np.int32)
+        a2t = np.zeros(max(self.n, 1), np.int32)
+        ctag = np.zeros(self.mesh.nnodes, np.int32)
+        oracle_lib().ro_dofmap(self.h, _ptr(t2a), _ptr(a2t), _ptr(ctag))
+        return t2a, a2t[: self.n], ctag
+
+    def pattern(self):
+        rp = np.zeros(self.n + 1, np.int64)
+        col = np.zeros(max(self.nnz, 1), np.int64)
+        oracle_lib().ro_pattern(self.h, _ptr(rp), _ptr(col))
+        return rp, col[: self.nnz]
+
+    def set_time(self, t):
+        oracle_lib().ro_set_time(self.h, t)
+
+    def bc_node_values(self):
+        g = np.zeros(self.mesh.nnodes)
+        oracle_lib().ro_bc_node_values(self.h, _ptr(g))
+        return g
+
+    def assemble_matrix(self, c_diff=1.0, c_mass=0.0, c_tdiff=0.0, c_tmass=0.0, U=None, Udot=None):
+        val = np.zeros(self.nnz)
+        oracle_lib().ro_assemble_matrix(self.h, c_diff, c_mass, c_tdiff, c_tmass, _ptr(_f64(U)), _ptr(_f64(Udot)), _ptr(val))
+        return val
+
+    def assemble_vector(self, which, coef=0.0, U=None, Udot=None, operand=None):
+        out = np.zeros(self.n)
+        U, Udot, operand = _f64(U), _f64(Udot), _f64(operand)
+        oracle_lib().ro_assemble_vector(self.h, which, coef, _ptr(U), _ptr(Udot), _ptr(operand), _ptr(out))
+        return out
+
+    def lift(self, F, c_diff=1.0, c_mass=0.0):
+        F = np.array(F, dtype=np.float64)
+        oracle_lib().ro_lift(self.h, c_diff, c_mass, _ptr(F))
+        return F
+
+    def diagonal(self, c_diff=1.0, c_mass=0.0, U=None):
+        d = np.zeros(self.n)
+        oracle_lib().ro_diagonal(self.h, c_diff, c_mass, _ptr(_f64(U)), _ptr(d))
+        return d
+
+    def adjoint_gradient(self, T, lam):
+        g = np.zeros(self.mesh.nelem)
+        oracle_lib().ro_adjoint_gradient(self.h, _ptr(_f64(T)), _ptr(_f64(lam)), _ptr(g))
+        return g
+
+    def steady(self, solver=0, precond=1, tol=1e-10, maxit=1000, krylov=30, U=None):
+        U = np.zeros(self.n) if U is None else np.array(U, dtype=np.float64)
+        rep = Report()
+        oracle_lib().ro_steady(self.h, solver, precond, tol, maxit, krylov, _ptr(U), C.byref(rep))
+        return U, rep.as_dict()
+
+    def backward_euler(self, dt, nsteps, U0, solver=0, precond=1, tol=1e-8, maxit=1000, krylov=30):
+        U = np.array(U0, dtype=np.float64)
+        res = np.zeros(nsteps)
+        its = np.zeros(nsteps, np.int64)
+        rc = oracle_lib().ro_backward_euler(self.h, dt, nsteps, solver, precond, tol, maxit, krylov, _ptr(U), _ptr(res), _ptr(its))
+        return U, res, its, rc
+
+    def newton(self, abs_tol=1e-10, rel_tol=1e-10, maxit=50, solver=1, precond=1, tol=1e-12, lin_maxit=1000,
+               krylov=30, U=None):
+        U = np.zeros(self.n) if U is None else np.array(U, dtype=np.float64)
+        rep = Report()
+        oracle_lib().ro_newton(self.h, abs_tol, rel_tol, maxit, solver, precond, tol, lin_maxit, krylov, _ptr(U), C.byref(rep))
+        return U, rep.as_dict()
+
+
+def spmv(rowPtr, col, val, x):
+    rowPtr = np.ascontiguousarray(rowPtr, np.int64)
+    col = np.ascontiguousarray(col, np.int64)
+    y = np.zeros(len(rowPtr) - 1)
+    oracle_lib().ro_spmv(len(rowPtr) - 1, _ptr(rowPtr), _ptr(col), _ptr(_f64(val)), _ptr(_f64(x)), _ptr(y))
+    return y
+
+
+def csr_solve(rowPtr, col, val, b, x0=None, solver=0, precond=1, tol=1e-10, maxit=1000, krylov=30):
+    rowPtr = np.ascontiguousarray(rowPtr, np.int64)
+    col = np.ascontiguousarray(col, np.int64)
+    n = len(rowPtr) - 1
+    x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
+    rep = Report()
+    oracle_lib().ro_csr_solve(solver, precond, n, _ptr(rowPtr), _ptr(col), _ptr(_f64(val)), _ptr(_f64(b)), _ptr(x),
+                              tol, maxit, krylov, C.byref(rep))
+    return x, rep.as_dict()
+
+
+# ---------------------------------------------------------------------------------------------
+# reference harness
+# ---------------------------------------------------------------------------------------------
+class _RefDesc(C.Structure):
+    _fields_ = [("nsd", _I32), ("order", _I32), ("nq", _I32), ("nx", _I32), ("ny", _I32), ("nz", _I32),
+                ("lo", _D * 3), ("hi", _D * 3), ("ess_mask", _I32), ("bc_kind", _I32), ("bc_val", _D * 6),
+                ("src_kind", _I32), ("src_c", _D), ("k_a", _D), ("k_b", _D), ("rho", _D), ("cp", _D),
+                ("k_elem", _P)]
+
+
+_rlib = None
+
+
+def reference_available():
+    return os.path.exists(REF_SO)
+
+
+def ref_lib():
+    global _rlib
+    if _rlib is None:
+        # The harness instantiates std::num_put facets itself; loaded RTLD_LOCAL its facet ids
+        # would differ from libstdc++'s and the reference's ostringstream formatting
+        # (solver/linear/LinearSolverFactory.hpp:44-46) would index the wrong facet.  Putting
+        # libstdc++ in the global scope first makes every facet id resolve to one definition.
+        C.CDLL("libstdc++.so.6", mode=C.RTLD_GLOBAL)
+        L = C.CDLL(REF_SO)
+        L.ref_create.argtypes = [C.POINTER(_RefDesc)]; L.ref_create.restype = _P
+        L.ref_destroy.argtypes = [_P]
+        L.ref_last_error.restype = C.c_char_p
+        for f in ("ref_num_nodes", "ref_num_elems", "ref_num_free", "ref_nnz"):
+            getattr(L, f).argtypes = [_P]; getattr(L, f).restype = _I64
+        L.ref_dofmap.argtypes = [_P, _P, _P]
+        L.ref_mesh.argtypes = [_P, _P, _P, _P]
+        L.ref_pattern.argtypes = [_P, _P, _P]
+        L.ref_assemble_matrix.argtypes = [_P, C.c_int, _D, _P, _P, _P]
+        L.ref_assemble_vector.argtypes = [_P, C.c_int, _D, _P, _P, _P, _P]
+        L.ref_lift.argtypes = [_P, C.c_int, _D, _P]
+        L.ref_diagonal.argtypes = [_P, C.c_int, _D, _P, _P]
+        L.ref_steady.argtypes = [_P, C.c_int, C.c_int, _D, _I64, _I64, _P, C.POINTER(Report)]
+        L.ref_newton.argtypes = [_P, _D, _D, _I64, C.c_int, C.c_int, _D, _I64, _I64, _P, C.POINTER(Report)]
+        L.ref_backward_euler.argtypes = [_P, _D, _I64, C.c_int, C.c_int, _D, _I64, _I64, _P, _P]
+        L.ref_adjoint_gradient.argtypes = [_P, _P, _P, _P]
+        L.ref_csr_solve.argtypes = [C.c_int, C.c_int, _I64, _P, _P, _P, _P, _P, _D, _I64, _I64, C.POINTER(Report)]
+        L.ref_spmv.argtypes = [_I64, _P, _P, _P, _P, _P]
+        _rlib = L
+    return _rlib
+
+
+class Reference:
+    """The reference's own templates for one block mesh (closed-form models, see ref_harness.cpp).
+
+    bc_kind 0: constant per essential tag (bc_val); 1: g = x; 2: g = (1-x)(1-y).
+    src_kind 0: f = src_c; 1: f = src_c * x*y(*z).  k(T) = k_a + k_b*T.
+    """
+
+    FORMSETS = {"K": 0, "K+cM": 1, "K+KT": 2, "J_BE": 3, "M": 4}
+
+    def __init__(self, nsd, order, nq, nel, lo, hi, ess_tags, bc_kind=0, bc_val=None, src_kind=0, src_c=0.0,
+                 k_a=1.0, k_b=0.0, rho=1.0, cp=1.0, k_elem=None):
+        L = ref_lib()
+        d = _RefDesc()
+        d.nsd, d.order, d.nq = nsd, order, nq
+        nel = list(nel) + [1] * (3 - len(nel))
+        d.nx, d.ny, d.nz = nel
+        for i in range(nsd):
+            d.lo[i], d.hi[i] = lo[i], hi[i]
+        d.ess_mask = sum(1 << t for t in ess_tags)
+        d.bc_kind = bc_kind
+        for t, v in (bc_val or {}).items():
+            d.bc_val[t] = v
+        d.src_kind, d.src_c = src_kind, src_c
+        d.k_a, d.k_b, d.rho, d.cp = k_a, k_b, rho, cp
+        self._kelem = None if k_elem is None else _f64(k_elem)
+        d.k_elem = _ptr(self._kelem)
+        self.h = L.ref_create(C.byref(d))
+        if not self.h:
+            raise ValueError(L.ref_last_error().decode())
+        self.nnodes = L.ref_num_nodes(self.h)
+        self.nelem = L.ref_num_elems(self.h)
+        self.n = L.ref_num_free(self.h)
+        self._nnz = None
+
+    def __del__(self):
+        try:
+            ref_lib().ref_destroy(self.h)
+        except Exception:
+            pass
+
+    @property
+    def nnz(self):
+        if self._nnz is None:
+            self._nnz = ref_lib().ref_nnz(self.h)
+        return self._nnz
+
+    def dofmap(self):
+        t2a = np.zeros(self.nnodes, np.int32)
+        a2t = np.zeros(max(self.n, 1), np.int32)
+        ref_lib().ref_dofmap(self.h, _ptr(t2a), _ptr(a2t))
+        return t2a, a2t[: self.n]
+
+    def pattern(self):
+        rp = np.zeros(self.n + 1, np.int64)
+        col = np.zeros(max(self.nnz, 1), np.int64)
+        ref_lib().ref_pattern(self.h, _ptr(rp), _ptr(col))
+        return rp, col[: self.nnz]
+
+    def assemble_matrix(self, formset="K", c=0.0, U=None, Udot=None):
+        val = np.zeros(self.nnz)
+        ref_lib().ref_assemble_matrix(self.h, self.FORMSETS[formset], c, _ptr(_f64(U)), _ptr(_f64(Udot)), _ptr(val))
+        return val
+
+    def assemble_vector(self, which, coef=0.0, U=None, Udot=None, operand=None):
+        out = np.zeros(self.n)
+        U, Udot, operand = _f64(U), _f64(Udot), _f64(operand)
+        ref_lib().ref_assemble_vector(self.h, which, coef, _ptr(U), _ptr(Udot), _ptr(operand), _ptr(out))
+        return out
+
+    def lift(self, F, formset="K", c=0.0):
+        F = np.array(F, dtype=np.float64)
+        ref_lib().ref_lift(self.h, self.FORMSETS[formset], c, _ptr(F))
+        return F
+
+    def diagonal(self, formset="K", c=0.0, U=None):
+        d = np.zeros(self.n)
+        ref_lib().ref_diagonal(self.h, self.FORMSETS[formset], c, _ptr(_f64(U)), _ptr(d))
+        return d
+
+    def steady(self, solver=0, precond=1, tol=1e-10, maxit=1000, krylov=30, U=None):
+        U = np.zeros(self.n) if U is None else np.array(U, dtype=np.float64)
+        rep = Report()
+        ref_lib().ref_steady(self.h, solver, precond, tol, maxit, krylov, _ptr(U), C.byref(rep))
+        return U, rep.as_dict()
+
+    def newton(self, abs_tol=1e-10, rel_tol=1e-10, maxit=50, solver=1, precond=1, tol=1e-12, lin_maxit=1000,
+               krylov=30, U=None):
+        U = np.zeros(self.n) if U is None else np.array(U, dtype=np.float64)
+        rep = Report()
+        ref_lib().ref_newton(self.h, abs_tol, rel_tol, maxit, solver, precond, tol, lin_maxit, krylov, _ptr(U), C.byref(rep))
+        return U, rep.as_dict()
+
+    def backward_euler(self, dt, nsteps, U0, solver=0, precond=1, tol=1e-8, maxit=1000, krylov=30):
+        U = np.array(U0, dtype=np.float64)
+        res = np.zeros(nsteps)
+        rc = ref_lib().ref_backward_euler(self.h, dt, nsteps, solver, precond, tol, maxit, krylov, _ptr(U), _ptr(res))
+        return U, res, rc
+
+    def adjoint_gradient(self, T, lam):
+        g = np.zeros(self.nelem)
+        ref_lib().ref_adjoint_gradient(self.h, _ptr(_f64(T)), _ptr(_f64(lam)), _ptr(g))
+        return g
+
+
+def ref_csr_solve(rowPtr, col, val, b, x0=None, solver=0, precond=1, tol=1e-10, maxit=1000, krylov=30):
+    rowPtr = np.ascontiguousarray(rowPtr, np.int64)
+    col = np.ascontiguousarray(col, np.int64)
+    n = len(rowPtr) - 1
+    x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
+    rep = Report()
+    ref_lib().ref_csr_solve(solver, precond, n, _ptr(rowPtr), _ptr(col), _ptr(_f64(val)), _ptr(_f64(b)), _ptr(x),
+                            tol, maxit, krylov, C.byref(rep))
+    return x, rep.as_dict()
