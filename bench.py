@@ -1,0 +1,403 @@
+"""Benchmark: one Backward-Euler step of 3D transient heat on a 128^3 Q1-hex mesh, solved to a
+1e-8 relative residual checked in FP64 -- mixed FP32/FP64 CG+Jacobi (the headline) beside plain
+FP64 CG+Jacobi on the same steps, plus the dominant kernel's roofline and the reference CPU path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--size S] [--impl ours|reference]
+
+A step is everything BackwardEulerRunner::step does in the reference: Udot, K + M/dt assembly,
+load, (1/dt) M U_prev, Dirichlet lift, the CG solve warm-started from U, the stage residual norm
+and the advance.  Inputs are synthetic (the configuration's seeded sine-mode initial condition).
+With N > 1 every rank runs an independent replica (the solve has no exchange step to shard).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def load_package():
+    import importlib.util
+    name = "residuum_solver_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    pkg = os.path.join(ROOT, "residuum-solver_b200")
+    spec = importlib.util.spec_from_file_location(name, os.path.join(pkg, "__init__.py"), submodule_search_locations=[pkg])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+# ---------------------------------------------------------------------------------------------
+# synthetic input: std::mt19937_64 (its output sequence is fixed by the C++ standard), uniform
+# double u = (x >> 11) * 2^-53, integer in [a, b] = a + floor(u (b - a + 1))
+# ---------------------------------------------------------------------------------------------
+class MT19937_64:
+    def __init__(self, seed):
+        self.mt = [0] * 312
+        self.mt[0] = seed & 0xFFFFFFFFFFFFFFFF
+        for i in range(1, 312):
+            self.mt[i] = (6364136223846793005 * (self.mt[i - 1] ^ (self.mt[i - 1] >> 62)) + i) & 0xFFFFFFFFFFFFFFFF
+        self.idx = 312
+
+    def next(self):
+        if self.idx >= 312:
+            mt = self.mt
+            for i in range(312):
+                x = (mt[i] & 0xFFFFFFFF80000000) | (mt[(i + 1) % 312] & 0x7FFFFFFF)
+                xa = x >> 1
+                if x & 1:
+                    xa ^= 0xB5026F5AA96619E9
+                mt[i] = mt[(i + 156) % 312] ^ xa
+            self.idx = 0
+        y = self.mt[self.idx]
+        self.idx += 1
+        y ^= (y >> 29) & 0x5555555555555555
+        y ^= (y << 17) & 0x71D67FFFEDA60000
+        y ^= (y << 37) & 0xFFF7EEE000000000
+        y ^= y >> 43
+        return y & 0xFFFFFFFFFFFFFFFF
+
+    def uniform(self):
+        return (self.next() >> 11) * (1.0 / 9007199254740992.0)
+
+    def integer(self, a, b):
+        return a + int(self.uniform() * (b - a + 1))
+
+
+def sine_modes(seed=2, modes=8):
+    """T0(x) = sum_m 0.1 sin(a_m . x + b_m), a_m = pi * i_m with i_m ~ U{1..8}^3, b_m ~ U[0, 2pi);
+    per mode the three integers are drawn before the phase."""
+    g = MT19937_64(seed)
+    A, B = [], []
+    for _ in range(modes):
+        A.append([np.pi * g.integer(1, 8) for _ in range(3)])
+        B.append(2.0 * np.pi * g.uniform())
+    return np.array(A), np.array(B)
+
+
+def initial_condition(xyz, a2t, seed=2):
+    A, B = sine_modes(seed)
+    X = xyz.reshape(-1, 3)[a2t]
+    return (0.1 * np.sin(X @ A.T + B[None, :])).sum(axis=1)
+
+
+# ---------------------------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1])); mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel):
+    """DRAM traffic per launch for a kernel from the committed ncu summary, or None."""
+    p = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        if kernel in d:
+            return d[kernel]
+    return None
+
+
+# ---------------------------------------------------------------------------------------------
+# reference CPU path (oracle/_ref: the reference templates compiled unmodified), bounded sample
+# ---------------------------------------------------------------------------------------------
+def reference_sample(sample_size, nsteps, warmup):
+    import oracle
+    if not oracle.reference_available():
+        return None
+    r = oracle.Reference(3, 1, 2, [sample_size] * 3, [0, 0, 0], [1, 1, 1], list(range(6)), bc_kind=0, rho=1.0, cp=1.0)
+    from importlib import import_module
+    xyz = import_module("residuum_solver_b200.blockmesh").block_mesh(3, [sample_size] * 3, [0, 0, 0], [1, 1, 1], 1)[0]
+    t2a, a2t = r.dofmap()
+    U0 = initial_condition(xyz, a2t)
+    _, _, rc, st = r.backward_euler(1e-3, warmup + nsteps, U0, tol=1e-8, maxit=100000, stats=True)
+    st = st[warmup:]
+    return {"n": r.n, "nnz": r.nnz, "elements": r.nelem, "step_s": st[:, 0], "solve_s": st[:, 1], "iters": st[:, 2], "rc": rc}
+
+
+def extrapolate(ref, n_elem, nnz, iters):
+    """Scale a reference sample to the full workload: element loops by the element count, the CG
+    solve by nnz x iterations (the reference runs the same CG as the device FP64 path, so the
+    device's FP64 iteration count is the reference's at full size)."""
+    step = float(np.median(ref["step_s"]))
+    solve = float(np.median(ref["solve_s"]))
+    it = float(np.median(ref["iters"]))
+    loops = (step - solve) * (n_elem / ref["elements"])
+    cg = solve * (nnz / ref["nnz"]) * (iters / max(it, 1.0))
+    return 1e3 * (loops + cg), step * 1e3
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    try:
+        import oracle
+        if not oracle.reference_available():
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libresiduum_ref.so not built (reference tree absent at build time)"}))
+            return
+        ref = reference_sample(args.cpu_sample, args.steps, args.warmup)
+    except Exception as e:  # noqa: BLE001
+        print(json.dumps({"impl": "reference", "unavailable": f"reference sample failed: {e}"}))
+        return
+    # without the device run at hand, scale CG by nnz and by the sample's own iteration growth
+    # (iterations ~ h^-1 for BE-preconditioned CG at fixed dt: a documented estimate)
+    S = args.size
+    n_elem, nnz = S ** 3, (3 * S - 5) ** 3
+    iters = float(np.median(ref["iters"])) * (S / args.cpu_sample)
+    ms, sample_ms = extrapolate(ref, n_elem, nnz, iters)
+    line = {"impl": "reference", "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD.format(S=S), "parallelism": "replicas"},
+            "cpu_baseline": {"value": ms, "unit": "ms", "cores": 1, "kind": "reference",
+                             "sample": f"{args.steps} Backward-Euler steps of the {args.cpu_sample}^3 problem through the reference templates (oracle/_ref), median {sample_ms:.0f} ms per step, scaled to {S}^3: element loops by elements, CG by nnz x iterations"},
+            "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+METRIC = "time to a 1e-8 FP64-checked relative residual per Backward-Euler step, mixed FP32/FP64 CG+Jacobi (FP64 CG alongside)"
+WORKLOAD = ("3D transient heat, unit cube, {S}^3 Q1 hexes, k = rho*cp = 1, Backward Euler dt = 1e-3, "
+            "T0 = 8 seeded sine modes (amplitude 0.1, seed 2), Dirichlet T = 0 on all faces")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--size", type=int, default=128)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-sample", type=int, default=48)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--reliable-delta", type=float, default=0.0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    rsd = load_package()
+    from importlib import import_module
+    bm = import_module("residuum_solver_b200.blockmesh")
+    ctx = rsd.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=local)
+
+    S = args.size
+    xyz, ien, rng = bm.block_mesh(3, [S, S, S], [0, 0, 0], [1, 1, 1], 1)
+    mesh = rsd.Mesh(ctx, 3, 1, xyz, ien, rng)
+    heat = rsd.Heat(ctx, mesh, 2, k_const=1.0, rho=1.0, cp=1.0, dirichlet={t: "0" for t in range(6)})
+    n, nnz = heat.n, heat.nnz
+    t2a, a2t = heat.dofmap()
+    U0 = initial_condition(xyz, a2t)
+    U, Up = ctx.array(n), ctx.array(n)
+    dt = 1e-3
+    cfgs = {
+        "mixed": rsd.SolverConfig.make(type=rsd.CG, precond=rsd.JACOBI, precision=rsd.MIXED, tol=1e-8, max_iters=100000,
+                                       reliable_delta=args.reliable_delta),
+        "fp64": rsd.SolverConfig.make(type=rsd.CG, precond=rsd.JACOBI, precision=rsd.FP64, tol=1e-8, max_iters=100000),
+    }
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+            torch.cuda.synchronize()
+
+    def run(cfg, steps, warmup, profile=False, clocks=None):
+        U.upload(U0); Up.upload(U0)
+        heat.set_time(0.0)
+        for _ in range(warmup):
+            heat.be_step(dt, U, Up, cfg)
+        reps = []
+        if profile:
+            ctx.profile(True)
+        barrier()
+        if clocks:
+            clocks.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            reps.append(heat.be_step(dt, U, Up, cfg))
+        e1.record(stream)
+        e1.synchronize()
+        clk = clocks.stop() if clocks else None
+        barrier()
+        ms = e0.elapsed_time(e1) / steps
+        prof = {}
+        if profile:
+            for fam in ("spmv_dot_f32", "spmv_dot_f64", "cg_update", "cg_pupdate", "reliable_update", "assemble_matrix", "assemble_vector"):
+                prof[fam] = ctx.profile_get(fam)
+            ctx.profile(False)
+        return ms, reps, prof, clk
+
+    clocks = ClockSampler(local)
+    ms_mx, reps_mx, prof_mx, clk = run(cfgs["mixed"], args.steps, args.warmup, profile=True, clocks=clocks)
+    ms_64, reps_64, prof_64, _ = run(cfgs["fp64"], args.steps, args.warmup, profile=True)
+
+    # end to end through the public API with host buffers: H2D of the step's state from pinned
+    # host memory, the step, D2H of the new state, every step
+    hU = torch.from_numpy(U0.copy()).pin_memory()
+    hUp = torch.from_numpy(U0.copy()).pin_memory()
+    U.upload(U0); Up.upload(U0)
+    heat.set_time(0.0)
+    for _ in range(args.warmup):
+        heat.be_step(dt, U, Up, cfgs["mixed"])
+    lib, C = rsd.lib(), __import__("ctypes")
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        rsd.check(lib.rsd_memcpy(ctx.h, U.ptr, C.c_void_p(hU.data_ptr()), 8 * n, rsd.RSD_H2D))
+        rsd.check(lib.rsd_memcpy(ctx.h, Up.ptr, C.c_void_p(hUp.data_ptr()), 8 * n, rsd.RSD_H2D))
+        heat.be_step(dt, U, Up, cfgs["mixed"])
+        rsd.check(lib.rsd_memcpy(ctx.h, C.c_void_p(hU.data_ptr()), U.ptr, 8 * n, rsd.RSD_D2H))
+        hUp.copy_(hU)
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    ms_e2e = e0.elapsed_time(e1) / args.steps
+
+    def reduce_max(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    ms_mx, ms_64, ms_e2e = reduce_max(ms_mx), reduce_max(ms_64), reduce_max(ms_e2e)
+
+    # dominant kernel of the mixed step: the FP32 SpMV (+ p.Ap) of every CG iteration
+    launches, tot = prof_mx["spmv_dot_f32"]
+    avg_ms = tot / max(launches, 1)
+    bytes_spmv32 = nnz * (4 + 4) + 4 * (n + 1) + 2 * n * 4
+    peak, peak_kind = measured_peak_hbm()
+    achieved = bytes_spmv32 / (avg_ms * 1e-3) / 1e9 if launches else None
+    l64, t64 = prof_64["spmv_dot_f64"]
+    bytes_spmv64 = nnz * (8 + 4) + 4 * (n + 1) + 2 * n * 8
+    achieved64 = bytes_spmv64 / ((t64 / max(l64, 1)) * 1e-3) / 1e9 if l64 else None
+    traffic = ncu_traffic("k_mx_spmv_dot")
+
+    it_mx = [r["iterations"] for r in reps_mx]
+    it_64 = [r["iterations"] for r in reps_64]
+    solve_mx = sum(prof_mx[f][1] for f in ("spmv_dot_f32", "cg_update", "cg_pupdate", "reliable_update")) / args.steps
+    solve_64 = sum(prof_64[f][1] for f in ("spmv_dot_f64", "cg_update", "cg_pupdate")) / args.steps
+    # launches per step: 7 element/vector kernels + rate + 3 memsets-free init kernels + 4 (mixed) per iteration
+    # issued (including the no-op tail of the last polling chunk) -> counted from the profiler plus fixed ones
+    issued_mx = sum(prof_mx[f][0] for f in ("spmv_dot_f32", "cg_update", "cg_pupdate", "reliable_update", "assemble_matrix", "assemble_vector"))
+    gpu_launches = int(issued_mx + args.steps * (1 + 2 + 2))   # + rate, invdiag/init, residual combine/dot
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            ref = reference_sample(args.cpu_sample, 2, 1)
+            if ref is not None:
+                est, sample_ms = extrapolate(ref, S ** 3, nnz, float(np.median(it_64)))
+                cpu = {"value": est, "unit": "ms", "cores": 1, "kind": "reference",
+                       "sample": (f"2 Backward-Euler steps (after 1 warm-up) of the {args.cpu_sample}^3 problem through the "
+                                  f"reference templates (oracle/_ref), median {sample_ms:.0f} ms per step; scaled to {S}^3 "
+                                  f"by elements for the element loops and by nnz x the device FP64 iteration count for CG")}
+        except Exception as e:  # noqa: BLE001
+            cpu = {"value": None, "unit": "ms", "cores": 1, "kind": "reference", "sample": f"failed: {e}"}
+
+    line = {
+        "metric": METRIC, "value": ms_mx, "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_mx, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD.format(S=S), "n_free": n, "nnz": nnz, "elements": S ** 3, "parallelism": "replicas",
+                   "l2": "inputs larger than L2 (CSR FP64 values + columns %.2f GB)" % (nnz * 12 / 1e9)},
+        "fp64_ms_per_step": ms_64,
+        "speedup_mixed_vs_fp64_step": ms_64 / ms_mx,
+        "solve_ms_per_step": {"mixed": solve_mx, "fp64": solve_64},
+        "speedup_mixed_vs_fp64_solve": solve_64 / solve_mx if solve_mx else None,
+        "iterations": {"mixed": it_mx, "fp64": it_64},
+        "reliable_updates": [r["refinements"] for r in reps_mx],
+        "true_residual_rel": {"mixed": max(r["trueResidualRel"] for r in reps_mx), "fp64": max(r["trueResidualRel"] for r in reps_64)},
+        "roofline": {"kernel": "k_mx_spmv_dot (FP32 CSR SpMV + p.Ap)", "bound": "hbm", "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak if achieved else None,
+                     "frac_nominal_8tbs": achieved / 8000.0 if achieved else None, "algorithmic_bytes": bytes_spmv32,
+                     "avg_launch_us": avg_ms * 1e3, "launches": launches, "traffic": traffic,
+                     "fp64_spmv": {"achieved": achieved64, "frac": achieved64 / peak if achieved64 else None,
+                                   "algorithmic_bytes": bytes_spmv64, "avg_launch_us": 1e3 * t64 / max(l64, 1)}},
+        "kernel_ms_per_step": {k: v[1] / args.steps for k, v in prof_mx.items()},
+        "cpu_baseline": cpu,
+        "e2e": {"value": ms_e2e, "unit": "ms", "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 8 * n},
+        "gpu_launches": gpu_launches,
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    del heat, mesh
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,199 @@
+/* rsd.h - C ABI of the B200 (sm_100a) backend for the Residuum heat-equation hot path.
+ *
+ * Plain pointers, sizes and status codes; no exceptions, no C++ or torch types cross this line.
+ * Each entry point names the reference interface it stands in for (paths relative to the
+ * Residuum reference tree).  Device pointers are CUDA global-memory pointers on the context's
+ * device; "host" arguments are ordinary CPU memory.
+ *
+ * Conventions
+ *   - every function returns RSD_OK (0) or a negative RSD_E* code; rsd_last_error_string()
+ *     describes the last failure on the calling thread;
+ *   - one rsd_ctx owns one CUDA stream; calls on a context are ordered on that stream and
+ *     return after their results are complete unless documented otherwise;
+ *   - solver non-convergence is not an error: it is report.converged == 0, as the reference's
+ *     solvers return false with a filled SolverReport (linalg/solver/iterative/cg/Solver.tpp:110-117).
+ */
+#ifndef RSD_H
+#define RSD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RSD_OK 0
+#define RSD_EINVAL (-1)       /* bad argument, size or unsupported discretization */
+#define RSD_ENOMEM (-2)       /* device allocation failed */
+#define RSD_ECUDA (-3)        /* CUDA runtime error */
+#define RSD_EBREAKDOWN (-5)   /* Krylov breakdown with a non-finite scalar */
+#define RSD_ENAN (-6)         /* non-finite value detected */
+#define RSD_EPARSE (-7)       /* expression string could not be compiled */
+#define RSD_ETIMEOUT (-8)     /* a bounded device wait gave up */
+
+typedef struct rsd_ctx rsd_ctx;
+typedef struct rsd_csr rsd_csr;
+typedef struct rsd_mesh rsd_mesh;
+typedef struct rsd_heat rsd_heat;
+
+/* CopyKind (include/linalg/types/backend/cuda/CopyKind.hpp:9-14) */
+enum { RSD_H2H = 0, RSD_H2D = 1, RSD_D2H = 2, RSD_D2D = 3 };
+
+/* LinearSolverConfig::Type / PreconditionerConfig::Type (include/solver/config/LinearSolverConfig.hpp) */
+enum { RSD_CG = 0, RSD_GMRES = 1 };
+enum { RSD_IDENTITY = 0, RSD_JACOBI = 1 };
+enum { RSD_FP64 = 0, RSD_MIXED = 1 };
+enum { RSD_TOL_RELATIVE = 0, RSD_TOL_ABSOLUTE = 1 };
+
+/* SolverReport (include/linalg/solver/base/SolverReport.hpp:12-28) plus device-path extras */
+typedef struct rsd_report {
+	int32_t converged;
+	int32_t status;              /* RSD_OK or the RSD_E* that stopped the solve */
+	int64_t iterations;
+	double initialResidual;      /* ||b - A x0|| */
+	double finalResidual;        /* ||r_k|| of the recurrence (reference semantics) */
+	double finalResidualRel;     /* finalResidual / (initialResidual + 1e-50) */
+	double trueResidualRel;      /* mixed precision: ||b - A64 x|| / ||r0||, recomputed in FP64 */
+	int64_t refinements;         /* mixed precision: FP64 residual replacements */
+} rsd_report;
+
+/* cg::Config / gmres::Config (linalg/solver/iterative/{cg,gmres}/Config.hpp) plus precision */
+typedef struct rsd_solver_cfg {
+	int32_t type;                /* RSD_CG or RSD_GMRES */
+	int32_t precond;             /* RSD_IDENTITY or RSD_JACOBI */
+	int32_t precision;           /* RSD_FP64 or RSD_MIXED (FP32 inner, FP64 residual) */
+	int32_t tol_type;            /* RSD_TOL_RELATIVE or RSD_TOL_ABSOLUTE */
+	double tol;
+	int64_t max_iters;
+	int64_t krylov_dim;          /* GMRES restart length m */
+	double reliable_delta;       /* mixed CG: FP64 residual replacement when |r| falls by this factor (0: 0.1) */
+} rsd_solver_cfg;
+
+/* ---- lifetime (linalg/types/backend/CUDA.hpp:23-73 has no context; these give it one) ---- */
+int rsd_ctx_create(int device, rsd_ctx** out);
+int rsd_ctx_destroy(rsd_ctx* ctx);
+int rsd_ctx_sync(rsd_ctx* ctx);
+void* rsd_ctx_stream(rsd_ctx* ctx);
+const char* rsd_last_error_string(void);
+int rsd_version(int32_t* major, int32_t* minor);
+/* Tracing (the reference has only its benchmark Timer, include/benchmark/core/Timer.hpp:10-24):
+ * when enabled, every launch of the kernel families "spmv_dot_f64", "spmv_dot_f32", "cg_update",
+ * "cg_pupdate", "reliable_update", "assemble_matrix", "assemble_vector", "spmv" is bracketed by
+ * CUDA events on the context stream; rsd_ctx_profile_get returns launches and summed device time.
+ * Enabling (or disabling) resets the totals. */
+int rsd_ctx_profile(rsd_ctx* ctx, int32_t enable);
+int rsd_ctx_profile_get(rsd_ctx* ctx, const char* family, int64_t* launches, double* total_ms);
+
+/* ---- memory: CUDA::alloc / copy / zero / set (linalg/types/backend/CUDA.hpp:30-71) ---- */
+int rsd_alloc(rsd_ctx* ctx, size_t bytes, void** dptr);
+int rsd_free(rsd_ctx* ctx, void* dptr);
+int rsd_memcpy(rsd_ctx* ctx, void* dst, const void* src, size_t bytes, int32_t kind);
+int rsd_memset_zero(rsd_ctx* ctx, void* dptr, size_t bytes);
+int rsd_fill_f64(rsd_ctx* ctx, double* x, int64_t n, double value);
+int rsd_fill_f32(rsd_ctx* ctx, float* x, int64_t n, float value);
+
+/* ---- BLAS-1: operations::dot/axpy/axpby/scal/copy/multiply/norm
+ *      (linalg/operations/VectorOps.hpp:10-36, backend/cpu/VectorOps.tpp:7-86).
+ *      Reductions are deterministic (fixed two-stage order) and return to host memory. ---- */
+int rsd_dot(rsd_ctx* ctx, int64_t n, const double* x, const double* y, double* out);
+int rsd_nrm2(rsd_ctx* ctx, int64_t n, const double* x, double* out);
+int rsd_axpy(rsd_ctx* ctx, int64_t n, double alpha, const double* x, double* y);
+int rsd_axpby(rsd_ctx* ctx, int64_t n, double alpha, double beta, const double* x, double* y);
+int rsd_scal(rsd_ctx* ctx, int64_t n, double alpha, double* x);
+int rsd_copy(rsd_ctx* ctx, int64_t n, const double* x, double* y);
+int rsd_mul(rsd_ctx* ctx, int64_t n, const double* x, const double* y, double* z);
+
+/* ---- CSR matrix: CSRMatrix<Real, CUDA> (linalg/types/CSRMatrix.hpp:14-88).  Host input uses
+ *      the reference's 64-bit Index; the device copy holds 32-bit rowPtr/colIdx (nnz < 2^31). ---- */
+int rsd_csr_create(rsd_ctx* ctx, int64_t nrows, int64_t nnz, const int64_t* row_ptr, const int64_t* col_idx,
+                   const double* values, rsd_csr** out);
+int rsd_csr_destroy(rsd_csr* A);
+int rsd_csr_info(const rsd_csr* A, int64_t* nrows, int64_t* nnz);
+int rsd_csr_values(rsd_csr* A, double** dvalues);
+int rsd_csr_set_values(rsd_ctx* ctx, rsd_csr* A, const double* host_values);
+int rsd_csr_get_values(rsd_ctx* ctx, const rsd_csr* A, double* host_values);
+int rsd_csr_get_pattern(rsd_ctx* ctx, const rsd_csr* A, int64_t* host_row_ptr, int64_t* host_col_idx);
+/* operations::matvec (linalg/operations/backend/cpu/MatrixOps.tpp:5-23), device vectors */
+int rsd_spmv(rsd_ctx* ctx, const rsd_csr* A, const double* x, double* y);
+/* FP32 copy of the values (refreshed from FP64) and its SpMV, for the mixed-precision path */
+int rsd_csr_sync_f32(rsd_ctx* ctx, rsd_csr* A);
+int rsd_spmv_f32(rsd_ctx* ctx, const rsd_csr* A, const float* x, float* y);
+/* CSROperator::diagonal (linalg/operator/CSROperator.hpp:40-45), operations::lump (MatrixOps.tpp:25-43) */
+int rsd_csr_diagonal(rsd_ctx* ctx, const rsd_csr* A, double* d);
+int rsd_csr_lump(rsd_ctx* ctx, const rsd_csr* A, double* d);
+/* Jacobi::update (linalg/solver/preconditioner/Jacobi.hpp:23-36): invD = |d|>1e-300 ? 1/d : 1 */
+int rsd_jacobi_setup(rsd_ctx* ctx, const rsd_csr* A, double* inv_diag);
+/* SpMV launch shape: lanes per row (2..32, power of two) and threads per block; 0 picks defaults */
+int rsd_csr_set_launch(rsd_csr* A, int32_t lanes_per_row, int32_t block_threads);
+int rsd_csr_autotune(rsd_ctx* ctx, rsd_csr* A, int32_t* lanes_per_row, int32_t* block_threads, double* best_us);
+
+/* ---- Krylov solves: CGRunner / GMRESRunner::solve (linalg/solver/iterative/cg/Solver.tpp:13-119,
+ *      gmres/Solver.tpp:3-170) through LinearSolverRunner::solve(b, x, report)
+ *      (linalg/solver/base/LinearSolverRunner.hpp:16); b and x are device vectors. ---- */
+int rsd_solve(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const double* b, double* x, rsd_report* report);
+
+/* ---- mesh: mesh::Data (include/mesh/Data.hpp:13-35), host arrays in that layout ---- */
+int rsd_mesh_create(rsd_ctx* ctx, int32_t nsd, int32_t order, int64_t num_nodes, int64_t num_elements,
+                    const double* xyz, const int64_t* ien, const int32_t* rng, rsd_mesh** out);
+int rsd_mesh_destroy(rsd_mesh* m);
+
+/* ---- heat problem: HeatProblem<CUDA, HeatEquation<NSD,NSD,Family>>
+ *      (application/heateq/problem/HeatProblem.hpp:34-206).  Expression strings use the
+ *      reference's exprtk syntax subset (numbers, t x y z T, pi, + - * / ^, unary -, sin cos tan
+ *      exp log sqrt abs). ---- */
+typedef struct rsd_heat_desc {
+	int32_t nq;                      /* Gauss points per direction */
+	double k_const;                  /* conductivity when k_expr is NULL */
+	const char* k_expr;              /* k(T), or NULL */
+	const char* dk_expr;             /* dk/dT(T), or NULL (0) */
+	const double* k_elem;            /* host, one multiplier per element, or NULL */
+	double rho, cp;                  /* density, specific heat */
+	const char* src_expr;            /* volumetric source f(t,x,y,z), or NULL (0) */
+	const char* dirichlet_expr[6];   /* Dirichlet value per boundary tag; NULL = tag not essential */
+} rsd_heat_desc;
+
+/* constructor + TopologicalDOF::buildConstraints + Assembler::createMatrix
+ * (HeatProblem.tpp:4-176, topology/TopologicalDOF.tpp:34-111, fem/assembly/backend/cpu/Assembler.tpp:8-76) */
+int rsd_heat_create(rsd_ctx* ctx, const rsd_mesh* m, const rsd_heat_desc* desc, rsd_heat** out);
+int rsd_heat_destroy(rsd_heat* h);
+int rsd_heat_info(const rsd_heat* h, int64_t* num_free, int64_t* nnz);
+int rsd_heat_dofmap(rsd_ctx* ctx, const rsd_heat* h, int32_t* host_topo_to_alg, int32_t* host_alg_to_topo);
+int rsd_heat_matrix(rsd_heat* h, rsd_csr** A);       /* the problem's K/J storage (owned by h) */
+int rsd_heat_set_time(rsd_ctx* ctx, rsd_heat* h, double t);   /* re-evaluates Dirichlet node values */
+int rsd_heat_set_k_elem(rsd_ctx* ctx, rsd_heat* h, const double* k_elem_device);
+
+/* Assembler::assembleMatrix (fem/assembly/backend/cpu/Assembler.tpp:86-140): zero A, then
+ * scatter c_diff*Diffusion + c_mass*Mass + c_tdiff*TangentDiffusion + c_tmass*TangentMass.
+ * U (free DOFs; Dirichlet values injected, GatherMode::Full) and Udot (GatherMode::Free) are
+ * device vectors or NULL (zero).  A must have h's pattern (rsd_heat_matrix or a copy). */
+int rsd_assemble_matrix(rsd_ctx* ctx, rsd_heat* h, double c_diff, double c_mass, double c_tdiff, double c_tmass,
+                        const double* U, const double* Udot, rsd_csr* A);
+/* Assembler::assembleVector (Assembler.tpp:199-255) with the stages' form/operand pairings:
+ * which 0: load (SourceForm); 1: Diffusion on U (Full); 2: rho*cp*Mass on U (Full);
+ * 3: rho*cp*Mass on Udot (Free); 4: Diffusion + coef*Mass on operand (Free; FEMOperator::apply) */
+int rsd_assemble_vector(rsd_ctx* ctx, rsd_heat* h, int32_t which, double coef, const double* U, const double* Udot,
+                        const double* operand, double* out);
+/* BoundaryApplicator::applyEssentialBCs (fem/boundary/backend/cpu/BoundaryApplicator.tpp:7-64) */
+int rsd_apply_dirichlet_lift(rsd_ctx* ctx, rsd_heat* h, double c_diff, double c_mass, double* F);
+/* Assembler::assembleDiagonal (Assembler.tpp:142-197) */
+int rsd_assemble_diagonal(rsd_ctx* ctx, rsd_heat* h, double c_diff, double c_mass, const double* U, double* d);
+
+/* ---- stages ---- */
+/* SteadyStage linear assemble + solve (solver/stage/SteadyStage.hpp:60-84); U device in/out */
+int rsd_heat_steady(rsd_ctx* ctx, rsd_heat* h, const rsd_solver_cfg* cfg, double* U, rsd_report* report);
+/* BackwardEulerRunner::step over BackwardEulerStage, linear mode
+ * (solver/timestepper/BackwardEuler.hpp:32-70, solver/stage/BackwardEulerStage.hpp:71-124):
+ * advances h's time by dt from Uprev to U (both device; U holds the warm start on entry), then
+ * copies U into Uprev; residual_norm receives the stage's residualNorm() (may be NULL). */
+int rsd_heat_be_step(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver_cfg* cfg, double* U, double* Uprev,
+                     rsd_report* report, double* residual_norm);
+/* NewtonRunner::solve over SteadyStage nonlinear mode (solver/nonlinear/Newton.hpp:32-83,
+ * solver/stage/SteadyStage.hpp:89-116): R = F - K(T)T, J = K + K_T, J dU = R, U += dU */
+int rsd_heat_newton(rsd_ctx* ctx, rsd_heat* h, double abs_tol, double rel_tol, int64_t max_iters,
+                    const rsd_solver_cfg* linear, double* U, rsd_report* report);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -287,7 +287,7 @@ def ref_lib():
         L.ref_diagonal.argtypes = [_P, C.c_int, _D, _P, _P]
         L.ref_steady.argtypes = [_P, C.c_int, C.c_int, _D, _I64, _I64, _P, C.POINTER(Report)]
         L.ref_newton.argtypes = [_P, _D, _D, _I64, C.c_int, C.c_int, _D, _I64, _I64, _P, C.POINTER(Report)]
-        L.ref_backward_euler.argtypes = [_P, _D, _I64, C.c_int, C.c_int, _D, _I64, _I64, _P, _P]
+        L.ref_backward_euler.argtypes = [_P, _D, _I64, C.c_int, C.c_int, _D, _I64, _I64, _P, _P, _P]
         L.ref_adjoint_gradient.argtypes = [_P, _P, _P, _P]
         L.ref_csr_solve.argtypes = [C.c_int, C.c_int, _I64, _P, _P, _P, _P, _P, _D, _I64, _I64, C.POINTER(Report)]
         L.ref_spmv.argtypes = [_I64, _P, _P, _P, _P, _P]
@@ -387,10 +387,15 @@ class Reference:
         ref_lib().ref_newton(self.h, abs_tol, rel_tol, maxit, solver, precond, tol, lin_maxit, krylov, _ptr(U), C.byref(rep))
         return U, rep.as_dict()
 
-    def backward_euler(self, dt, nsteps, U0, solver=0, precond=1, tol=1e-8, maxit=1000, krylov=30):
+    def backward_euler(self, dt, nsteps, U0, solver=0, precond=1, tol=1e-8, maxit=1000, krylov=30, stats=False):
+        """BackwardEulerRunner over BackwardEulerStage; with stats=True also returns per-step
+        (step seconds, solve seconds, CG iterations) measured around the reference calls."""
         U = np.array(U0, dtype=np.float64)
         res = np.zeros(nsteps)
-        rc = ref_lib().ref_backward_euler(self.h, dt, nsteps, solver, precond, tol, maxit, krylov, _ptr(U), _ptr(res))
+        st = np.zeros(3 * nsteps)
+        rc = ref_lib().ref_backward_euler(self.h, dt, nsteps, solver, precond, tol, maxit, krylov, _ptr(U), _ptr(res), _ptr(st))
+        if stats:
+            return U, res, rc, st.reshape(nsteps, 3)
         return U, res, rc
 
     def adjoint_gradient(self, T, lam):

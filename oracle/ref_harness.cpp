@@ -20,6 +20,7 @@
 //     application/heateq/problem/HeatProblem.tpp:217-289 without YAML, IO, loggers or monitors,
 //     so that the reference's own SteadyStage / BackwardEulerStage / NewtonRunner drive it.
 //   * ref_adjoint_gradient: an FP64 element loop over the reference QP evaluator + DiffusionForm.
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -218,7 +219,7 @@ struct Base {
 	virtual void diagonal(int formset, double massCoef, const double* U, double* d) = 0;
 	virtual int steady(int solverType, int precond, double tol, int64_t maxit, int64_t krylov, double* U, ref_report* rep) = 0;
 	virtual int newton(double absTol, double relTol, int64_t maxit, int solverType, int precond, double tol, int64_t linMaxit, int64_t krylov, double* U, ref_report* rep) = 0;
-	virtual int backwardEuler(double dt, int64_t nsteps, int solverType, int precond, double tol, int64_t maxit, int64_t krylov, double* U, double* residualPerStep) = 0;
+	virtual int backwardEuler(double dt, int64_t nsteps, int solverType, int precond, double tol, int64_t maxit, int64_t krylov, double* U, double* residualPerStep, double* stepStats) = 0;
 	virtual void adjointGradient(const double* T, const double* lam, double* grad) = 0;
 };
 
@@ -351,19 +352,24 @@ struct RefHeatProblem final : Base {
 	struct ReportingRunner final : linalg::solver::LinearSolverRunner<VecT> {
 		std::unique_ptr<linalg::solver::LinearSolverRunner<VecT>> inner;
 		linalg::solver::SolverReport<VecT>* sink;
+		double* seconds;
 		bool solve(const VecT& b, VecT& x, linalg::solver::SolverReport<VecT>& report) override {
+			const auto t0 = std::chrono::steady_clock::now();
 			bool ok = inner->solve(b, x, report);
+			*seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 			*sink = report;
 			return ok;
 		}
 	};
 	linalg::solver::SolverReport<VecT> lastReport_;
+	double lastSolveSeconds_ = 0.0;
 	template<typename FormsT, typename ModelT>
 	std::unique_ptr<linalg::solver::LinearSolverRunner<VecT>> makeLinearRunner(const Real*, const FormsT&, const ModelT&, StateVectorT&, MatT& K) {
 		using Op = linalg::op::CSROperator<MatT>;
 		auto r = std::make_unique<ReportingRunner>();
 		r->inner = solver::linear::makeLinearSolverRunner<Op, VecT>(Op(K), topo_->numFreeDOFs(), *inst_.linear, logCfg_.linear, equationLabel(), dofNames(), topo_->numFreeDOFs(), fem::dof::DOFOrdering::Interleaved);
 		r->sink = &lastReport_;
+		r->seconds = &lastSolveSeconds_;
 		return r;
 	}
 	Index numFreeDOFs() const { return topo_->numFreeDOFs(); }
@@ -507,7 +513,8 @@ struct RefHeatProblem final : Base {
 	}
 
 	// BackwardEulerStage + BackwardEulerRunner (solver/timestepper/BackwardEuler.hpp:32-70), linear mode
-	int backwardEuler(double dt, int64_t nsteps, int solverType, int precond, double tol, int64_t maxit, int64_t krylov, double* U, double* residualPerStep) override {
+	// stepStats (optional, 3 per step): wall seconds of runner.step(), of its linear solve, CG iterations
+	int backwardEuler(double dt, int64_t nsteps, int solverType, int precond, double tol, int64_t maxit, int64_t krylov, double* U, double* residualPerStep, double* stepStats) override {
 		setLinear(solverType, precond, tol, maxit, krylov);
 		tsCfg_.type = solver::config::TimeStepperConfig::Type::BackwardEuler;
 		tsCfg_.t0 = 0.0; tsCfg_.tf = dt * (double)nsteps;
@@ -520,7 +527,14 @@ struct RefHeatProblem final : Base {
 		solver::timestepper::BackwardEulerRunner<solver::stage::BackwardEulerStage<RefHeatProblem>> runner(stage, tsCfg_, std::make_unique<solver::timestepper::ConstantStepSizePolicy>(dt), utils::logging::timestepper::Logger(utils::logging::NullLogger{}));
 		int rc = 0;
 		for (int64_t s = 0; s < nsteps && !runner.finished(); ++s) {
+			const auto t0 = std::chrono::steady_clock::now();
 			if (!runner.step()) { rc = 1; break; }
+			const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+			if (stepStats) {
+				stepStats[3 * s] = secs;
+				stepStats[3 * s + 1] = lastSolveSeconds_;
+				stepStats[3 * s + 2] = (double)lastReport_.iterations;
+			}
 			if (residualPerStep) residualPerStep[s] = stage.residualNorm();
 		}
 		for (Index i = 0; i < numFree(); ++i) U[i] = U_->data()[i];
@@ -596,8 +610,8 @@ int ref_steady(void* h, int solverType, int precond, double tol, int64_t maxit, 
 int ref_newton(void* h, double absTol, double relTol, int64_t maxit, int solverType, int precond, double tol, int64_t linMaxit, int64_t krylov, double* U, ref_report* rep) {
 	try { return static_cast<Base*>(h)->newton(absTol, relTol, maxit, solverType, precond, tol, linMaxit, krylov, U, rep); } catch (const std::exception& e) { g_err = e.what(); return -1; }
 }
-int ref_backward_euler(void* h, double dt, int64_t nsteps, int solverType, int precond, double tol, int64_t maxit, int64_t krylov, double* U, double* resPerStep) {
-	try { return static_cast<Base*>(h)->backwardEuler(dt, nsteps, solverType, precond, tol, maxit, krylov, U, resPerStep); } catch (const std::exception& e) { g_err = e.what(); return -1; }
+int ref_backward_euler(void* h, double dt, int64_t nsteps, int solverType, int precond, double tol, int64_t maxit, int64_t krylov, double* U, double* resPerStep, double* stepStats) {
+	try { return static_cast<Base*>(h)->backwardEuler(dt, nsteps, solverType, precond, tol, maxit, krylov, U, resPerStep, stepStats); } catch (const std::exception& e) { g_err = e.what(); return -1; }
 }
 void ref_adjoint_gradient(void* h, const double* T, const double* lam, double* grad) { static_cast<Base*>(h)->adjointGradient(T, lam, grad); }
 

@@ -1,0 +1,403 @@
+"""ctypes front end of librsd_cuda.so, the sm_100a C-ABI backend for the Residuum heat-equation
+hot path (declared in include/rsd.h).
+
+This is the binding a Python caller (tests, bench.py, a PyTorch autograd wrapper) uses; C++ callers
+use the header layer in residuum_cuda/.  There is no CPU fallback: every call goes to the CUDA
+library, and importing raises if the library is missing.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librsd_cuda.so")
+
+_P, _D, _I32, _I64, _SZ = C.c_void_p, C.c_double, C.c_int32, C.c_int64, C.c_size_t
+
+RSD_H2H, RSD_H2D, RSD_D2H, RSD_D2D = 0, 1, 2, 3
+CG, GMRES = 0, 1
+IDENTITY, JACOBI = 0, 1
+FP64, MIXED = 0, 1
+RELATIVE, ABSOLUTE = 0, 1
+
+ERRORS = {-1: "RSD_EINVAL", -2: "RSD_ENOMEM", -3: "RSD_ECUDA", -5: "RSD_EBREAKDOWN", -6: "RSD_ENAN",
+          -7: "RSD_EPARSE", -8: "RSD_ETIMEOUT"}
+
+
+class RsdError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Report(C.Structure):
+    """rsd_report: SolverReport plus the FP64-checked residual of mixed precision."""
+    _fields_ = [("converged", _I32), ("status", _I32), ("iterations", _I64), ("initialResidual", _D),
+                ("finalResidual", _D), ("finalResidualRel", _D), ("trueResidualRel", _D), ("refinements", _I64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class SolverConfig(C.Structure):
+    _fields_ = [("type", _I32), ("precond", _I32), ("precision", _I32), ("tol_type", _I32), ("tol", _D),
+                ("max_iters", _I64), ("krylov_dim", _I64), ("reliable_delta", _D)]
+
+    @classmethod
+    def make(cls, type=CG, precond=JACOBI, precision=FP64, tol=1e-10, max_iters=1000, krylov_dim=30,
+             tol_type=RELATIVE, reliable_delta=0.0):
+        return cls(type, precond, precision, tol_type, tol, max_iters, krylov_dim, reliable_delta)
+
+
+class HeatDesc(C.Structure):
+    _fields_ = [("nq", _I32), ("k_const", _D), ("k_expr", C.c_char_p), ("dk_expr", C.c_char_p), ("k_elem", _P),
+                ("rho", _D), ("cp", _D), ("src_expr", C.c_char_p), ("dirichlet_expr", C.c_char_p * 6)]
+
+
+_lib = None
+
+# (name, argtypes) for every entry point of include/rsd.h
+SIGNATURES = {
+    "rsd_ctx_create": [C.c_int, C.POINTER(_P)],
+    "rsd_ctx_destroy": [_P],
+    "rsd_ctx_sync": [_P],
+    "rsd_ctx_stream": [_P],
+    "rsd_last_error_string": [],
+    "rsd_version": [C.POINTER(_I32), C.POINTER(_I32)],
+    "rsd_ctx_profile": [_P, _I32],
+    "rsd_ctx_profile_get": [_P, C.c_char_p, C.POINTER(_I64), C.POINTER(_D)],
+    "rsd_alloc": [_P, _SZ, C.POINTER(_P)],
+    "rsd_free": [_P, _P],
+    "rsd_memcpy": [_P, _P, _P, _SZ, _I32],
+    "rsd_memset_zero": [_P, _P, _SZ],
+    "rsd_fill_f64": [_P, _P, _I64, _D],
+    "rsd_fill_f32": [_P, _P, _I64, C.c_float],
+    "rsd_dot": [_P, _I64, _P, _P, C.POINTER(_D)],
+    "rsd_nrm2": [_P, _I64, _P, C.POINTER(_D)],
+    "rsd_axpy": [_P, _I64, _D, _P, _P],
+    "rsd_axpby": [_P, _I64, _D, _D, _P, _P],
+    "rsd_scal": [_P, _I64, _D, _P],
+    "rsd_copy": [_P, _I64, _P, _P],
+    "rsd_mul": [_P, _I64, _P, _P, _P],
+    "rsd_csr_create": [_P, _I64, _I64, _P, _P, _P, C.POINTER(_P)],
+    "rsd_csr_destroy": [_P],
+    "rsd_csr_info": [_P, C.POINTER(_I64), C.POINTER(_I64)],
+    "rsd_csr_values": [_P, C.POINTER(_P)],
+    "rsd_csr_set_values": [_P, _P, _P],
+    "rsd_csr_get_values": [_P, _P, _P],
+    "rsd_csr_get_pattern": [_P, _P, _P, _P],
+    "rsd_spmv": [_P, _P, _P, _P],
+    "rsd_csr_sync_f32": [_P, _P],
+    "rsd_spmv_f32": [_P, _P, _P, _P],
+    "rsd_csr_diagonal": [_P, _P, _P],
+    "rsd_csr_lump": [_P, _P, _P],
+    "rsd_jacobi_setup": [_P, _P, _P],
+    "rsd_csr_set_launch": [_P, _I32, _I32],
+    "rsd_csr_autotune": [_P, _P, C.POINTER(_I32), C.POINTER(_I32), C.POINTER(_D)],
+    "rsd_solve": [_P, _P, C.POINTER(SolverConfig), _P, _P, C.POINTER(Report)],
+    "rsd_mesh_create": [_P, _I32, _I32, _I64, _I64, _P, _P, _P, C.POINTER(_P)],
+    "rsd_mesh_destroy": [_P],
+    "rsd_heat_create": [_P, _P, C.POINTER(HeatDesc), C.POINTER(_P)],
+    "rsd_heat_destroy": [_P],
+    "rsd_heat_info": [_P, C.POINTER(_I64), C.POINTER(_I64)],
+    "rsd_heat_dofmap": [_P, _P, _P, _P],
+    "rsd_heat_matrix": [_P, C.POINTER(_P)],
+    "rsd_heat_set_time": [_P, _P, _D],
+    "rsd_heat_set_k_elem": [_P, _P, _P],
+    "rsd_assemble_matrix": [_P, _P, _D, _D, _D, _D, _P, _P, _P],
+    "rsd_assemble_vector": [_P, _P, _I32, _D, _P, _P, _P, _P],
+    "rsd_apply_dirichlet_lift": [_P, _P, _D, _D, _P],
+    "rsd_assemble_diagonal": [_P, _P, _D, _D, _P, _P],
+    "rsd_heat_steady": [_P, _P, C.POINTER(SolverConfig), _P, C.POINTER(Report)],
+    "rsd_heat_be_step": [_P, _P, _D, C.POINTER(SolverConfig), _P, _P, C.POINTER(Report), C.POINTER(_D)],
+    "rsd_heat_newton": [_P, _P, _D, _D, _I64, C.POINTER(SolverConfig), _P, C.POINTER(Report)],
+}
+
+
+def lib():
+    """Load the in-tree library (built by build.py); there is deliberately no fallback."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with residuum-solver_b200/build.py")
+        L = C.CDLL(LIB_PATH)
+        for name, args in SIGNATURES.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_int
+        L.rsd_last_error_string.restype = C.c_char_p
+        L.rsd_ctx_stream.restype = _P
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    if rc != 0:
+        raise RsdError(rc, lib().rsd_last_error_string().decode())
+
+
+_DT = {np.float64: 8, np.float32: 4, np.int32: 4, np.int64: 8}
+
+
+class Context:
+    """One device + one CUDA stream (rsd_ctx)."""
+
+    def __init__(self, device=0):
+        self.h = _P()
+        check(lib().rsd_ctx_create(device, C.byref(self.h)))
+
+    def close(self):
+        if self.h:
+            lib().rsd_ctx_destroy(self.h)
+            self.h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync(self):
+        check(lib().rsd_ctx_sync(self.h))
+
+    def stream(self):
+        return lib().rsd_ctx_stream(self.h)
+
+    def profile(self, enable=True):
+        """Time every launch of the library's kernel families with CUDA events (resets totals)."""
+        check(lib().rsd_ctx_profile(self.h, 1 if enable else 0))
+
+    def profile_get(self, family):
+        n, ms = _I64(), _D()
+        check(lib().rsd_ctx_profile_get(self.h, family.encode(), C.byref(n), C.byref(ms)))
+        return n.value, ms.value
+
+    def array(self, n, dtype=np.float64):
+        return DeviceArray(self, n, dtype)
+
+    def to_device(self, a, dtype=None):
+        a = np.ascontiguousarray(a, dtype=dtype or a.dtype)
+        d = DeviceArray(self, a.size, a.dtype.type)
+        d.upload(a)
+        return d
+
+
+class DeviceArray:
+    """A device allocation from rsd_alloc with numpy upload/download."""
+
+    def __init__(self, ctx, n, dtype=np.float64):
+        self.ctx, self.n, self.dtype = ctx, int(n), np.dtype(dtype).type
+        self.nbytes = self.n * _DT[self.dtype]
+        self.ptr = _P()
+        check(lib().rsd_alloc(ctx.h, max(self.nbytes, 1), C.byref(self.ptr)))
+
+    def __del__(self):
+        try:
+            if self.ptr:
+                lib().rsd_free(self.ctx.h, self.ptr)
+        except Exception:
+            pass
+
+    def upload(self, a):
+        a = np.ascontiguousarray(a, dtype=self.dtype)
+        assert a.size == self.n
+        check(lib().rsd_memcpy(self.ctx.h, self.ptr, a.ctypes.data_as(_P), self.nbytes, RSD_H2D))
+        return self
+
+    def download(self):
+        out = np.empty(self.n, dtype=self.dtype)
+        check(lib().rsd_memcpy(self.ctx.h, out.ctypes.data_as(_P), self.ptr, self.nbytes, RSD_D2H))
+        return out
+
+    def zero(self):
+        check(lib().rsd_memset_zero(self.ctx.h, self.ptr, self.nbytes))
+        return self
+
+    def fill(self, v):
+        if self.dtype == np.float64:
+            check(lib().rsd_fill_f64(self.ctx.h, self.ptr, self.n, v))
+        else:
+            check(lib().rsd_fill_f32(self.ctx.h, self.ptr, self.n, v))
+        return self
+
+
+def _ptr(a):
+    return None if a is None else (a.ptr if isinstance(a, DeviceArray) else a)
+
+
+class CSR:
+    """rsd_csr: CSRMatrix<Real, CUDA>; 32-bit indices on the device."""
+
+    def __init__(self, ctx, handle, owned=True):
+        self.ctx, self.h, self.owned = ctx, handle, owned
+        n, nnz = _I64(), _I64()
+        check(lib().rsd_csr_info(self.h, C.byref(n), C.byref(nnz)))
+        self.n, self.nnz = n.value, nnz.value
+
+    @classmethod
+    def from_host(cls, ctx, row_ptr, col, val=None):
+        rp = np.ascontiguousarray(row_ptr, np.int64)
+        cl = np.ascontiguousarray(col, np.int64)
+        v = None if val is None else np.ascontiguousarray(val, np.float64)
+        h = _P()
+        check(lib().rsd_csr_create(ctx.h, len(rp) - 1, len(cl), rp.ctypes.data_as(_P), cl.ctypes.data_as(_P),
+                                   None if v is None else v.ctypes.data_as(_P), C.byref(h)))
+        return cls(ctx, h)
+
+    def __del__(self):
+        try:
+            if self.owned and self.h:
+                lib().rsd_csr_destroy(self.h)
+        except Exception:
+            pass
+
+    def values(self):
+        out = np.empty(self.nnz)
+        check(lib().rsd_csr_get_values(self.ctx.h, self.h, out.ctypes.data_as(_P)))
+        return out
+
+    def set_values(self, v):
+        v = np.ascontiguousarray(v, np.float64)
+        check(lib().rsd_csr_set_values(self.ctx.h, self.h, v.ctypes.data_as(_P)))
+
+    def pattern(self):
+        rp = np.empty(self.n + 1, np.int64)
+        col = np.empty(self.nnz, np.int64)
+        check(lib().rsd_csr_get_pattern(self.ctx.h, self.h, rp.ctypes.data_as(_P), col.ctypes.data_as(_P)))
+        return rp, col
+
+    def spmv(self, x, y):
+        check(lib().rsd_spmv(self.ctx.h, self.h, _ptr(x), _ptr(y)))
+
+    def spmv_f32(self, x, y):
+        check(lib().rsd_spmv_f32(self.ctx.h, self.h, _ptr(x), _ptr(y)))
+
+    def sync_f32(self):
+        check(lib().rsd_csr_sync_f32(self.ctx.h, self.h))
+
+    def diagonal(self, d):
+        check(lib().rsd_csr_diagonal(self.ctx.h, self.h, _ptr(d)))
+
+    def lump(self, d):
+        check(lib().rsd_csr_lump(self.ctx.h, self.h, _ptr(d)))
+
+    def jacobi(self, inv_d):
+        check(lib().rsd_jacobi_setup(self.ctx.h, self.h, _ptr(inv_d)))
+
+    def set_launch(self, lanes=0, block=0):
+        check(lib().rsd_csr_set_launch(self.h, lanes, block))
+
+    def autotune(self):
+        lanes, block, us = _I32(), _I32(), _D()
+        check(lib().rsd_csr_autotune(self.ctx.h, self.h, C.byref(lanes), C.byref(block), C.byref(us)))
+        return lanes.value, block.value, us.value
+
+
+def solve(ctx, A, b, x, cfg=None, **kw):
+    cfg = cfg or SolverConfig.make(**kw)
+    rep = Report()
+    check(lib().rsd_solve(ctx.h, A.h, C.byref(cfg), _ptr(b), _ptr(x), C.byref(rep)))
+    return rep.as_dict()
+
+
+class Mesh:
+    """rsd_mesh from mesh::Data-layout host arrays (xyz node-major, ien element-major, rng per face)."""
+
+    def __init__(self, ctx, nsd, order, xyz, ien, rng):
+        self.ctx = ctx
+        xyz = np.ascontiguousarray(xyz, np.float64)
+        ien = np.ascontiguousarray(ien, np.int64)
+        rng = np.ascontiguousarray(rng, np.int32)
+        npe = (order + 1) ** nsd
+        self.nsd, self.order, self.npe = nsd, order, npe
+        self.nnodes, self.nelem = xyz.size // nsd, ien.size // npe
+        self.h = _P()
+        check(lib().rsd_mesh_create(ctx.h, nsd, order, self.nnodes, self.nelem, xyz.ctypes.data_as(_P),
+                                    ien.ctypes.data_as(_P), rng.ctypes.data_as(_P), C.byref(self.h)))
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().rsd_mesh_destroy(self.h)
+        except Exception:
+            pass
+
+
+class Heat:
+    """rsd_heat: the heat problem (dof map, pattern, element loops, stages) on the device."""
+
+    def __init__(self, ctx, mesh, nq, k_const=1.0, k_expr=None, dk_expr=None, k_elem=None, rho=1.0, cp=1.0,
+                 src_expr=None, dirichlet=None):
+        self.ctx, self.mesh = ctx, mesh
+        d = HeatDesc()
+        d.nq, d.k_const, d.rho, d.cp = nq, k_const, rho, cp
+        d.k_expr = k_expr.encode() if k_expr else None
+        d.dk_expr = dk_expr.encode() if dk_expr else None
+        d.src_expr = src_expr.encode() if src_expr else None
+        ke = None if k_elem is None else np.ascontiguousarray(k_elem, np.float64)
+        d.k_elem = None if ke is None else ke.ctypes.data_as(_P)
+        for tag, ex in (dirichlet or {}).items():
+            d.dirichlet_expr[tag] = ex.encode()
+        self.h = _P()
+        check(lib().rsd_heat_create(ctx.h, mesh.h, C.byref(d), C.byref(self.h)))
+        n, nnz = _I64(), _I64()
+        check(lib().rsd_heat_info(self.h, C.byref(n), C.byref(nnz)))
+        self.n, self.nnz = n.value, nnz.value
+        a = _P()
+        check(lib().rsd_heat_matrix(self.h, C.byref(a)))
+        self.K = CSR(ctx, a, owned=False)
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().rsd_heat_destroy(self.h)
+        except Exception:
+            pass
+
+    def dofmap(self):
+        t2a = np.empty(self.mesh.nnodes, np.int32)
+        a2t = np.empty(max(self.n, 1), np.int32)
+        check(lib().rsd_heat_dofmap(self.ctx.h, self.h, t2a.ctypes.data_as(_P), a2t.ctypes.data_as(_P)))
+        return t2a, a2t[: self.n]
+
+    def set_time(self, t):
+        check(lib().rsd_heat_set_time(self.ctx.h, self.h, t))
+
+    def set_k_elem(self, k_dev):
+        check(lib().rsd_heat_set_k_elem(self.ctx.h, self.h, _ptr(k_dev)))
+
+    def assemble_matrix(self, c_diff=1.0, c_mass=0.0, c_tdiff=0.0, c_tmass=0.0, U=None, Udot=None, A=None):
+        A = A or self.K
+        check(lib().rsd_assemble_matrix(self.ctx.h, self.h, c_diff, c_mass, c_tdiff, c_tmass, _ptr(U), _ptr(Udot), A.h))
+        return A
+
+    def assemble_vector(self, which, out, coef=0.0, U=None, Udot=None, operand=None):
+        check(lib().rsd_assemble_vector(self.ctx.h, self.h, which, coef, _ptr(U), _ptr(Udot), _ptr(operand), _ptr(out)))
+        return out
+
+    def lift(self, F, c_diff=1.0, c_mass=0.0):
+        check(lib().rsd_apply_dirichlet_lift(self.ctx.h, self.h, c_diff, c_mass, _ptr(F)))
+
+    def diagonal(self, d, c_diff=1.0, c_mass=0.0, U=None):
+        check(lib().rsd_assemble_diagonal(self.ctx.h, self.h, c_diff, c_mass, _ptr(U), _ptr(d)))
+
+    def steady(self, U, cfg=None, **kw):
+        cfg = cfg or SolverConfig.make(**kw)
+        rep = Report()
+        check(lib().rsd_heat_steady(self.ctx.h, self.h, C.byref(cfg), _ptr(U), C.byref(rep)))
+        return rep.as_dict()
+
+    def be_step(self, dt, U, Uprev, cfg=None, **kw):
+        cfg = cfg or SolverConfig.make(**kw)
+        rep, res = Report(), _D()
+        check(lib().rsd_heat_be_step(self.ctx.h, self.h, dt, C.byref(cfg), _ptr(U), _ptr(Uprev), C.byref(rep), C.byref(res)))
+        d = rep.as_dict()
+        d["residualNorm"] = res.value
+        return d
+
+    def newton(self, U, abs_tol=1e-10, rel_tol=1e-10, max_iters=50, cfg=None, **kw):
+        cfg = cfg or SolverConfig.make(type=GMRES, **kw)
+        rep = Report()
+        check(lib().rsd_heat_newton(self.ctx.h, self.h, abs_tol, rel_tol, max_iters, C.byref(cfg), _ptr(U), C.byref(rep)))
+        return rep.as_dict()

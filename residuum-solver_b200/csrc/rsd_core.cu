@@ -1,0 +1,567 @@
+// Context, memory, errors, expression compiler, mesh upload, DOF map and CSR pattern.
+#include <algorithm>
+#include <cctype>
+#include <cmath>
+#include <cstring>
+#include <thread>
+
+#include "rsd_internal.cuh"
+
+namespace rsd {
+
+static thread_local std::string g_last_error;
+
+int set_error(int code, const std::string& msg) {
+	g_last_error = msg;
+	return code;
+}
+
+int cuda_error(cudaError_t e, const char* what) {
+	const int code = (e == cudaErrorMemoryAllocation) ? RSD_ENOMEM : RSD_ECUDA;
+	return set_error(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------------------------------------
+// expression compiler: recursive descent over the exprtk subset the reference's configurations use
+// (src/utils/expression/ScalarExpression.cpp:3-30, equation/heateq/evaluator/TemperatureExpression.hpp:31-58)
+// ---------------------------------------------------------------------------------------------
+namespace {
+struct Parser {
+	const char* s;
+	size_t pos = 0;
+	bool err = false;
+	DevExpr* e;
+	int nconst = 0;
+	void emit(ExprOp op, int arg = 0, double c = 0.0) {
+		if (e->n >= kExprMax) { err = true; return; }
+		e->op[e->n] = op;
+		if (op == E_CONST) { e->c[nconst] = c; e->arg[e->n] = (int8_t)nconst++; }
+		else e->arg[e->n] = (int8_t)arg;
+		e->n++;
+	}
+	void ws() { while (s[pos] && std::isspace((unsigned char)s[pos])) pos++; }
+	void primary() {
+		ws();
+		const char c = s[pos];
+		if (c == '(') { pos++; expr(); ws(); if (s[pos] != ')') { err = true; return; } pos++; return; }
+		if (std::isdigit((unsigned char)c) || c == '.') {
+			char* end = nullptr;
+			const double v = std::strtod(s + pos, &end);
+			if (end == s + pos) { err = true; return; }
+			pos = (size_t)(end - s);
+			emit(E_CONST, 0, v);
+			return;
+		}
+		if (std::isalpha((unsigned char)c) || c == '_') {
+			std::string name;
+			while (std::isalnum((unsigned char)s[pos]) || s[pos] == '_') name += s[pos++];
+			static const char* vars[] = {"t", "x", "y", "z", "T"};
+			for (int v = 0; v < 5; ++v) if (name == vars[v]) { emit(E_VAR, v); return; }
+			if (name == "pi") { emit(E_CONST, 0, 3.14159265358979323846); return; }
+			static const char* fns[] = {"sin", "cos", "tan", "exp", "log", "sqrt", "abs"};
+			static const ExprOp fop[] = {E_SIN, E_COS, E_TAN, E_EXP, E_LOG, E_SQRT, E_ABS};
+			for (int f = 0; f < 7; ++f)
+				if (name == fns[f]) {
+					ws();
+					if (s[pos] != '(') { err = true; return; }
+					pos++; expr(); ws();
+					if (s[pos] != ')') { err = true; return; }
+					pos++;
+					emit(fop[f]);
+					return;
+				}
+		}
+		err = true;
+	}
+	void power() { primary(); ws(); if (s[pos] == '^') { pos++; unary(); emit(E_POW); } }
+	void unary() {
+		ws();
+		if (s[pos] == '-') { pos++; unary(); emit(E_NEG); return; }
+		if (s[pos] == '+') { pos++; unary(); return; }
+		power();
+	}
+	void term() {
+		unary();
+		for (;;) { ws(); const char c = s[pos]; if (c != '*' && c != '/') return; pos++; unary(); emit(c == '*' ? E_MUL : E_DIV); }
+	}
+	void expr() {
+		term();
+		for (;;) { ws(); const char c = s[pos]; if (c != '+' && c != '-') return; pos++; term(); emit(c == '+' ? E_ADD : E_SUB); }
+	}
+};
+}  // namespace
+
+int compile_expr(const char* src, DevExpr* out) {
+	*out = DevExpr();
+	if (!src) return RSD_OK;
+	Parser p{src, 0, false, out};
+	p.expr();
+	p.ws();
+	if (p.err || src[p.pos] != 0 || out->n == 0) {
+		*out = DevExpr();
+		return set_error(RSD_EPARSE, std::string("cannot compile expression '") + src + "'");
+	}
+	return RSD_OK;
+}
+
+double eval_expr_host(const DevExpr& e, double t, double x, double y, double z, double T) {
+	double st[kExprMax];
+	int sp = 0;
+	const double v[5] = {t, x, y, z, T};
+	for (int i = 0; i < e.n; ++i) {
+		switch (e.op[i]) {
+			case E_CONST: st[sp++] = e.c[e.arg[i]]; break;
+			case E_VAR: st[sp++] = v[e.arg[i]]; break;
+			case E_ADD: sp--; st[sp - 1] = st[sp - 1] + st[sp]; break;
+			case E_SUB: sp--; st[sp - 1] = st[sp - 1] - st[sp]; break;
+			case E_MUL: sp--; st[sp - 1] = st[sp - 1] * st[sp]; break;
+			case E_DIV: sp--; st[sp - 1] = st[sp - 1] / st[sp]; break;
+			case E_POW: sp--; st[sp - 1] = std::pow(st[sp - 1], st[sp]); break;
+			case E_NEG: st[sp - 1] = -st[sp - 1]; break;
+			case E_SIN: st[sp - 1] = std::sin(st[sp - 1]); break;
+			case E_COS: st[sp - 1] = std::cos(st[sp - 1]); break;
+			case E_TAN: st[sp - 1] = std::tan(st[sp - 1]); break;
+			case E_EXP: st[sp - 1] = std::exp(st[sp - 1]); break;
+			case E_LOG: st[sp - 1] = std::log(st[sp - 1]); break;
+			case E_SQRT: st[sp - 1] = std::sqrt(st[sp - 1]); break;
+			default: st[sp - 1] = std::fabs(st[sp - 1]); break;
+		}
+	}
+	return e.n ? st[0] : 0.0;
+}
+
+// ---------------------------------------------------------------------------------------------
+// host parallel-for over [0, n)
+// ---------------------------------------------------------------------------------------------
+template <typename Fn>
+static void parallel_for(int64_t n, Fn&& fn) {
+	unsigned nt = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+	if (n < 65536) nt = 1;
+	std::vector<std::thread> th;
+	const int64_t chunk = (n + nt - 1) / nt;
+	for (unsigned t = 0; t < nt; ++t) {
+		const int64_t b = t * chunk, e = std::min<int64_t>(n, b + chunk);
+		if (b >= e) break;
+		th.emplace_back([=, &fn] { fn(b, e); });
+	}
+	for (auto& t : th) t.join();
+}
+
+// ---------------------------------------------------------------------------------------------
+// TopologicalDOF::buildConstraints, Interleaved ordering (topology/TopologicalDOF.tpp:34-111):
+// nodes on faces whose tag is essential are constrained; the constraint tag is the last face
+// (in element, face order) that marked the node; free nodes are numbered in ascending order.
+// Face-node lists are LagrangeQuad/Hex::getFaceNodes (fem/basis/LagrangeQuad.tpp:136-155,
+// fem/basis/LagrangeHex.tpp:263-304).
+// ---------------------------------------------------------------------------------------------
+static int face_nodes(int nsd, int p, int f, int* out) {
+	const int q = p + 1;
+	int k = 0;
+	if (nsd == 2) {
+		for (int i = 0; i < q; ++i) out[k++] = f == 0 ? i * q : f == 1 ? i * q + p : f == 2 ? i : i + q * p;
+		return k;
+	}
+	for (int j = 0; j < q; ++j)
+		for (int i = 0; i < q; ++i) {
+			int v;
+			switch (f) {
+				case 0: v = i * q + j * q * q; break;
+				case 1: v = i * q + j * q * q + p; break;
+				case 2: v = i + j * q * q; break;
+				case 3: v = i + j * q * q + q * p; break;
+				case 4: v = i + j * q; break;
+				default: v = i + j * q + q * q * p; break;
+			}
+			out[k++] = v;
+		}
+	return k;
+}
+
+int build_dofmap(rsd_heat* h) {
+	const rsd_mesh* m = h->m;
+	h->h_t2a.assign(m->nnodes, 0);
+	h->h_ctag.assign(m->nnodes, -1);
+	int fn[64];
+	for (int64_t e = 0; e < m->nelem; ++e)
+		for (int f = 0; f < m->nfaces; ++f) {
+			const int32_t tag = m->h_rng[e * m->nfaces + f];
+			if (tag < 0 || tag > 5 || !h->essential[tag]) continue;
+			const int npf = face_nodes(m->nsd, m->order, f, fn);
+			for (int i = 0; i < npf; ++i) {
+				const int32_t node = m->h_ien[e * m->npe + fn[i]];
+				h->h_t2a[node] = -1;
+				h->h_ctag[node] = tag;
+			}
+		}
+	h->h_a2t.clear();
+	h->h_a2t.reserve(m->nnodes);
+	int64_t alg = 0;
+	for (int64_t i = 0; i < m->nnodes; ++i) {
+		if (h->h_t2a[i] == -1) continue;
+		h->h_t2a[i] = (int32_t)alg++;
+		h->h_a2t.push_back((int32_t)i);
+	}
+	h->n = alg;
+	return RSD_OK;
+}
+
+// diagonal position per row (CSROperator::diagonal's getDataIndex, linalg/types/CSRMatrix.hpp:49-73)
+static void diag_index(int64_t n, const int32_t* rp, const int32_t* col, int32_t* d) {
+	parallel_for(n, [&](int64_t b, int64_t e) {
+		for (int64_t i = b; i < e; ++i) {
+			const int32_t* first = col + rp[i];
+			const int32_t* last = col + rp[i + 1];
+			const int32_t* it = std::lower_bound(first, last, (int32_t)i);
+			d[i] = (it != last && *it == i) ? (int32_t)(it - col) : -1;
+		}
+	});
+}
+
+static int upload_csr(rsd_ctx* ctx, int64_t n, const std::vector<int32_t>& rp, const std::vector<int32_t>& col,
+                      const double* hval, rsd_csr** out) {
+	const int64_t nnz = rp[n];
+	rsd_csr* A = new rsd_csr();
+	A->n = n;
+	A->nnz = nnz;
+	std::vector<int32_t> d(n);
+	diag_index(n, rp.data(), col.data(), d.data());
+	auto fail = [&](cudaError_t e, const char* w) { cudaFree(A->rowPtr); cudaFree(A->col); cudaFree(A->val); cudaFree(A->diag); delete A; return cuda_error(e, w); };
+	cudaError_t e;
+	if ((e = cudaMalloc(&A->rowPtr, sizeof(int32_t) * (n + 1))) != cudaSuccess) return fail(e, "cudaMalloc rowPtr");
+	if ((e = cudaMalloc(&A->col, sizeof(int32_t) * std::max<int64_t>(nnz, 1))) != cudaSuccess) return fail(e, "cudaMalloc col");
+	if ((e = cudaMalloc(&A->val, sizeof(double) * std::max<int64_t>(nnz, 1))) != cudaSuccess) return fail(e, "cudaMalloc val");
+	if ((e = cudaMalloc(&A->diag, sizeof(int32_t) * std::max<int64_t>(n, 1))) != cudaSuccess) return fail(e, "cudaMalloc diag");
+	if ((e = cudaMemcpyAsync(A->rowPtr, rp.data(), sizeof(int32_t) * (n + 1), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload rowPtr");
+	if (nnz && (e = cudaMemcpyAsync(A->col, col.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload col");
+	if (n && (e = cudaMemcpyAsync(A->diag, d.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload diag");
+	if (hval && nnz) e = cudaMemcpyAsync(A->val, hval, sizeof(double) * nnz, cudaMemcpyHostToDevice, ctx->stream);
+	else e = cudaMemsetAsync(A->val, 0, sizeof(double) * std::max<int64_t>(nnz, 1), ctx->stream);
+	if (e != cudaSuccess) return fail(e, "upload values");
+	if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return fail(e, "csr upload sync");
+	*out = A;
+	return RSD_OK;
+}
+
+// Assembler<CPU>::createMatrix (fem/assembly/backend/cpu/Assembler.tpp:8-76): row i holds the
+// sorted, unique free columns of every element touching free DOF i.  Built per row from a
+// node->element incidence list, in parallel on the host (one-time setup).
+int build_pattern(rsd_ctx* ctx, const rsd_heat* h, rsd_csr** out) {
+	const rsd_mesh* m = h->m;
+	const int64_t n = h->n, nn = m->nnodes, ne = m->nelem;
+	const int npe = m->npe;
+	std::vector<int64_t> ioff(nn + 1, 0);
+	for (int64_t i = 0; i < ne * npe; ++i) ioff[m->h_ien[i] + 1]++;
+	for (int64_t i = 0; i < nn; ++i) ioff[i + 1] += ioff[i];
+	std::vector<int32_t> inc(ne * npe);
+	{
+		std::vector<int64_t> cur(ioff.begin(), ioff.end() - 1);
+		for (int64_t e = 0; e < ne; ++e)
+			for (int a = 0; a < npe; ++a) inc[cur[m->h_ien[e * npe + a]]++] = (int32_t)e;
+	}
+	std::vector<int32_t> rp(n + 1, 0);
+	auto row_cols = [&](int64_t r, std::vector<int32_t>& buf) {
+		buf.clear();
+		const int32_t node = h->h_a2t[r];
+		for (int64_t k = ioff[node]; k < ioff[node + 1]; ++k) {
+			const int32_t* en = &m->h_ien[(int64_t)inc[k] * npe];
+			for (int b = 0; b < npe; ++b) { const int32_t c = h->h_t2a[en[b]]; if (c >= 0) buf.push_back(c); }
+		}
+		std::sort(buf.begin(), buf.end());
+		buf.erase(std::unique(buf.begin(), buf.end()), buf.end());
+	};
+	parallel_for(n, [&](int64_t b, int64_t e) {
+		std::vector<int32_t> buf;
+		for (int64_t r = b; r < e; ++r) { row_cols(r, buf); rp[r + 1] = (int32_t)buf.size(); }
+	});
+	int64_t total = 0;
+	for (int64_t r = 0; r < n; ++r) {
+		total += rp[r + 1];
+		if (total > INT32_MAX) return set_error(RSD_EINVAL, "pattern has 2^31 or more non-zeros");
+		rp[r + 1] = (int32_t)total;
+	}
+	std::vector<int32_t> col(total);
+	parallel_for(n, [&](int64_t b, int64_t e) {
+		std::vector<int32_t> buf;
+		for (int64_t r = b; r < e; ++r) { row_cols(r, buf); std::copy(buf.begin(), buf.end(), col.begin() + rp[r]); }
+	});
+	return upload_csr(ctx, n, rp, col, nullptr, out);
+}
+
+// ---------------------------------------------------------------------------------------------
+// per-kernel-family event timing
+// ---------------------------------------------------------------------------------------------
+static const char* kFamilyNames[PF_COUNT] = {"spmv_dot_f64", "spmv_dot_f32", "cg_update", "cg_pupdate", "reliable_update",
+                                             "assemble_matrix", "assemble_vector", "spmv"};
+
+int prof_begin(rsd_ctx* ctx, int family) {
+	Profiler& p = ctx->prof;
+	if (!p.on) return -1;
+	if (p.used + 2 > p.pool.size()) {
+		if (p.used + 2 > 1 << 16) prof_flush(ctx);
+		while (p.used + 2 > p.pool.size()) {
+			cudaEvent_t e;
+			if (cudaEventCreate(&e) != cudaSuccess) return -1;
+			p.pool.push_back(e);
+		}
+	}
+	const int pair = (int)(p.used / 2);
+	cudaEventRecord(p.pool[p.used], ctx->stream);
+	p.used += 2;
+	if ((int)p.fam.size() <= pair) p.fam.resize(pair + 1);
+	p.fam[pair] = family;
+	return pair;
+}
+
+void prof_end(rsd_ctx* ctx, int pair) {
+	if (pair < 0) return;
+	cudaEventRecord(ctx->prof.pool[2 * pair + 1], ctx->stream);
+}
+
+int prof_flush(rsd_ctx* ctx) {
+	Profiler& p = ctx->prof;
+	if (!p.used) return RSD_OK;
+	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+	for (size_t k = 0; k < p.used / 2; ++k) {
+		float ms = 0.f;
+		if (p.fam[k] < 0) continue;
+		if (cudaEventElapsedTime(&ms, p.pool[2 * k], p.pool[2 * k + 1]) == cudaSuccess) {
+			p.launches[p.fam[k]] += 1;
+			p.total_ms[p.fam[k]] += ms;
+		}
+	}
+	p.used = 0;
+	return RSD_OK;
+}
+
+}  // namespace rsd
+
+using namespace rsd;
+
+// =============================================================================================
+// C ABI
+// =============================================================================================
+extern "C" {
+
+int rsd_ctx_profile(rsd_ctx* c, int32_t enable) {
+	if (!c) return set_error(RSD_EINVAL, "null context");
+	RSD_CHECK(prof_flush(c));
+	c->prof.on = enable != 0;
+	for (int f = 0; f < PF_COUNT; ++f) { c->prof.launches[f] = 0; c->prof.total_ms[f] = 0.0; }
+	return RSD_OK;
+}
+
+int rsd_ctx_profile_get(rsd_ctx* c, const char* family, int64_t* launches, double* total_ms) {
+	if (!c || !family) return set_error(RSD_EINVAL, "null argument");
+	RSD_CHECK(prof_flush(c));
+	for (int f = 0; f < PF_COUNT; ++f)
+		if (!std::strcmp(family, kFamilyNames[f])) {
+			if (launches) *launches = c->prof.launches[f];
+			if (total_ms) *total_ms = c->prof.total_ms[f];
+			return RSD_OK;
+		}
+	return set_error(RSD_EINVAL, std::string("unknown kernel family ") + family);
+}
+
+const char* rsd_last_error_string(void) { return g_last_error.c_str(); }
+
+int rsd_version(int32_t* major, int32_t* minor) {
+	if (major) *major = 0;
+	if (minor) *minor = 1;
+	return RSD_OK;
+}
+
+int rsd_ctx_create(int device, rsd_ctx** out) {
+	if (!out) return set_error(RSD_EINVAL, "null output");
+	int count = 0;
+	RSD_CUDA(cudaGetDeviceCount(&count));
+	if (device < 0 || device >= count) return set_error(RSD_EINVAL, "no such CUDA device");
+	RSD_CUDA(cudaSetDevice(device));
+	rsd_ctx* c = new rsd_ctx();
+	c->device = device;
+	cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+	cudaError_t e;
+	if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) { delete c; return cuda_error(e, "cudaStreamCreate"); }
+	if ((e = cudaMalloc(&c->s.partials, sizeof(double) * kMaxPartials * 4)) != cudaSuccess ||
+	    (e = cudaMalloc(&c->s.scal, sizeof(DevScalars) * 4)) != cudaSuccess ||
+	    (e = cudaMallocHost(&c->s.hscal, sizeof(DevScalars) * 4)) != cudaSuccess ||
+	    (e = cudaMallocHost(&c->s.hbuf, sizeof(double) * 64)) != cudaSuccess) {
+		rsd_ctx_destroy(c);
+		return cuda_error(e, "context scratch");
+	}
+	cudaMemsetAsync(c->s.scal, 0, sizeof(DevScalars) * 4, c->stream);
+	cudaStreamSynchronize(c->stream);
+	*out = c;
+	return RSD_OK;
+}
+
+int rsd_ctx_destroy(rsd_ctx* c) {
+	if (!c) return RSD_OK;
+	cudaSetDevice(c->device);
+	if (c->stream) cudaStreamSynchronize(c->stream);
+	for (cudaEvent_t e : c->prof.pool) cudaEventDestroy(e);
+	cudaFree(c->s.partials);
+	cudaFree(c->s.scal);
+	cudaFreeHost(c->s.hscal);
+	cudaFreeHost(c->s.hbuf);
+	if (c->stream) cudaStreamDestroy(c->stream);
+	delete c;
+	return RSD_OK;
+}
+
+int rsd_ctx_sync(rsd_ctx* c) {
+	if (!c) return set_error(RSD_EINVAL, "null context");
+	RSD_CUDA(cudaStreamSynchronize(c->stream));
+	return RSD_OK;
+}
+
+void* rsd_ctx_stream(rsd_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int rsd_alloc(rsd_ctx* c, size_t bytes, void** dptr) {
+	if (!c || !dptr) return set_error(RSD_EINVAL, "null argument");
+	RSD_CUDA(cudaSetDevice(c->device));
+	*dptr = nullptr;
+	RSD_CUDA(cudaMalloc(dptr, bytes ? bytes : 1));
+	return RSD_OK;
+}
+
+int rsd_free(rsd_ctx* c, void* dptr) {
+	if (!c) return set_error(RSD_EINVAL, "null context");
+	if (dptr) {
+		RSD_CUDA(cudaStreamSynchronize(c->stream));
+		RSD_CUDA(cudaFree(dptr));
+	}
+	return RSD_OK;
+}
+
+int rsd_memcpy(rsd_ctx* c, void* dst, const void* src, size_t bytes, int32_t kind) {
+	if (!c) return set_error(RSD_EINVAL, "null context");
+	if (bytes == 0) return RSD_OK;
+	if (kind == RSD_H2H) { std::memmove(dst, src, bytes); return RSD_OK; }
+	cudaMemcpyKind k = kind == RSD_H2D ? cudaMemcpyHostToDevice : kind == RSD_D2H ? cudaMemcpyDeviceToHost
+	                 : kind == RSD_D2D ? cudaMemcpyDeviceToDevice : cudaMemcpyDefault;
+	RSD_CUDA(cudaMemcpyAsync(dst, src, bytes, k, c->stream));
+	RSD_CUDA(cudaStreamSynchronize(c->stream));
+	return RSD_OK;
+}
+
+int rsd_memset_zero(rsd_ctx* c, void* dptr, size_t bytes) {
+	if (!c) return set_error(RSD_EINVAL, "null context");
+	RSD_CUDA(cudaMemsetAsync(dptr, 0, bytes, c->stream));
+	RSD_CUDA(cudaStreamSynchronize(c->stream));
+	return RSD_OK;
+}
+
+int rsd_csr_create(rsd_ctx* c, int64_t nrows, int64_t nnz, const int64_t* row_ptr, const int64_t* col_idx,
+                   const double* values, rsd_csr** out) {
+	if (!c || !out || nrows < 0 || nnz < 0 || !row_ptr || (nnz && !col_idx)) return set_error(RSD_EINVAL, "bad CSR arguments");
+	if (nnz > INT32_MAX || nrows > INT32_MAX) return set_error(RSD_EINVAL, "CSR too large for 32-bit indices");
+	if (row_ptr[0] != 0 || row_ptr[nrows] != nnz) return set_error(RSD_EINVAL, "rowPtr does not span nnz");
+	std::vector<int32_t> rp(nrows + 1), col(nnz);
+	for (int64_t i = 0; i <= nrows; ++i) {
+		if (i && row_ptr[i] < row_ptr[i - 1]) return set_error(RSD_EINVAL, "rowPtr not monotone");
+		rp[i] = (int32_t)row_ptr[i];
+	}
+	for (int64_t p = 0; p < nnz; ++p) {
+		if (col_idx[p] < 0 || col_idx[p] >= nrows) return set_error(RSD_EINVAL, "column index out of range");
+		col[p] = (int32_t)col_idx[p];
+	}
+	RSD_CUDA(cudaSetDevice(c->device));
+	return upload_csr(c, nrows, rp, col, values, out);
+}
+
+int rsd_csr_destroy(rsd_csr* A) {
+	if (!A) return RSD_OK;
+	cudaDeviceSynchronize();
+	if (A->owns_pattern) { cudaFree(A->rowPtr); cudaFree(A->col); cudaFree(A->diag); }
+	cudaFree(A->val);
+	cudaFree(A->val32);
+	delete A;
+	return RSD_OK;
+}
+
+int rsd_csr_info(const rsd_csr* A, int64_t* nrows, int64_t* nnz) {
+	if (!A) return set_error(RSD_EINVAL, "null matrix");
+	if (nrows) *nrows = A->n;
+	if (nnz) *nnz = A->nnz;
+	return RSD_OK;
+}
+
+int rsd_csr_values(rsd_csr* A, double** dvalues) {
+	if (!A || !dvalues) return set_error(RSD_EINVAL, "null argument");
+	*dvalues = A->val;
+	A->version++;   // the caller may write through the pointer
+	return RSD_OK;
+}
+
+int rsd_csr_set_values(rsd_ctx* c, rsd_csr* A, const double* hv) {
+	if (!c || !A || !hv) return set_error(RSD_EINVAL, "null argument");
+	A->version++;
+	return rsd_memcpy(c, A->val, hv, sizeof(double) * A->nnz, RSD_H2D);
+}
+
+int rsd_csr_get_values(rsd_ctx* c, const rsd_csr* A, double* hv) {
+	if (!c || !A || !hv) return set_error(RSD_EINVAL, "null argument");
+	return rsd_memcpy(c, hv, A->val, sizeof(double) * A->nnz, RSD_D2H);
+}
+
+int rsd_csr_get_pattern(rsd_ctx* c, const rsd_csr* A, int64_t* hrp, int64_t* hcol) {
+	if (!c || !A) return set_error(RSD_EINVAL, "null argument");
+	std::vector<int32_t> rp(A->n + 1), col(A->nnz);
+	RSD_CHECK(rsd_memcpy(c, rp.data(), A->rowPtr, sizeof(int32_t) * (A->n + 1), RSD_D2H));
+	if (A->nnz) RSD_CHECK(rsd_memcpy(c, col.data(), A->col, sizeof(int32_t) * A->nnz, RSD_D2H));
+	if (hrp) for (int64_t i = 0; i <= A->n; ++i) hrp[i] = rp[i];
+	if (hcol) for (int64_t p = 0; p < A->nnz; ++p) hcol[p] = col[p];
+	return RSD_OK;
+}
+
+int rsd_csr_set_launch(rsd_csr* A, int32_t lanes, int32_t block) {
+	if (!A) return set_error(RSD_EINVAL, "null matrix");
+	if (lanes && (lanes < 1 || lanes > 32 || (lanes & (lanes - 1)))) return set_error(RSD_EINVAL, "lanes per row must be a power of two in 1..32");
+	if (block && (block < 32 || block > 1024 || block % 32)) return set_error(RSD_EINVAL, "block must be a multiple of 32 in 32..1024");
+	A->lanes = lanes;
+	A->block = block;
+	return RSD_OK;
+}
+
+int rsd_mesh_create(rsd_ctx* c, int32_t nsd, int32_t order, int64_t num_nodes, int64_t num_elements,
+                    const double* xyz, const int64_t* ien, const int32_t* rng, rsd_mesh** out) {
+	if (!c || !out || !xyz || !ien || !rng) return set_error(RSD_EINVAL, "null argument");
+	if (nsd != 2 && nsd != 3) return set_error(RSD_EINVAL, "spatial dimension must be 2 or 3");
+	if (order < 1 || order > 3) return set_error(RSD_EINVAL, "basis order must be 1..3 (kMaxBasisOrder)");
+	int npe = (order + 1) * (order + 1) * (nsd == 3 ? order + 1 : 1);
+	if (npe > 32) return set_error(RSD_EINVAL, "elements with more than 32 nodes (Q3 hex) are not supported");
+	if (num_nodes <= 0 || num_nodes > INT32_MAX || num_elements <= 0 || num_elements * npe > INT32_MAX)
+		return set_error(RSD_EINVAL, "mesh too large for 32-bit connectivity");
+	rsd_mesh* m = new rsd_mesh();
+	m->nsd = nsd; m->order = order; m->npe = npe; m->nfaces = nsd == 3 ? 6 : 4;
+	m->nnodes = num_nodes; m->nelem = num_elements;
+	m->h_xyz.assign(xyz, xyz + num_nodes * nsd);
+	m->h_ien.resize(num_elements * npe);
+	for (int64_t i = 0; i < num_elements * npe; ++i) {
+		if (ien[i] < 0 || ien[i] >= num_nodes) { delete m; return set_error(RSD_EINVAL, "connectivity references a missing node"); }
+		m->h_ien[i] = (int32_t)ien[i];
+	}
+	m->h_rng.assign(rng, rng + num_elements * m->nfaces);
+	cudaError_t e;
+	if ((e = cudaMalloc(&m->xyz, sizeof(double) * m->h_xyz.size())) != cudaSuccess ||
+	    (e = cudaMalloc(&m->ien, sizeof(int32_t) * m->h_ien.size())) != cudaSuccess ||
+	    (e = cudaMemcpyAsync(m->xyz, m->h_xyz.data(), sizeof(double) * m->h_xyz.size(), cudaMemcpyHostToDevice, c->stream)) != cudaSuccess ||
+	    (e = cudaMemcpyAsync(m->ien, m->h_ien.data(), sizeof(int32_t) * m->h_ien.size(), cudaMemcpyHostToDevice, c->stream)) != cudaSuccess ||
+	    (e = cudaStreamSynchronize(c->stream)) != cudaSuccess) {
+		cudaFree(m->xyz); cudaFree(m->ien); delete m;
+		return cuda_error(e, "mesh upload");
+	}
+	*out = m;
+	return RSD_OK;
+}
+
+int rsd_mesh_destroy(rsd_mesh* m) {
+	if (!m) return RSD_OK;
+	cudaDeviceSynchronize();
+	cudaFree(m->xyz);
+	cudaFree(m->ien);
+	delete m;
+	return RSD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,260 @@
+// HeatProblem-equivalent object on the device and the stage-level drivers built on it:
+// steady linear solve, one Backward-Euler step and the Newton loop.
+#include <cmath>
+#include <cstring>
+
+#include "rsd_kernels.cuh"
+
+namespace rsd {
+
+int build_tables(rsd_heat* h);
+int assemble_lift(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, double* F);
+
+static bool uses_time(const DevExpr& e) {
+	for (int i = 0; i < e.n; ++i) if (e.op[i] == E_VAR && e.arg[i] == 0) return true;
+	return false;
+}
+
+// Dirichlet value per constrained node at the current time: the constraint tag's expression at
+// the node's coordinates, as gatherElementVector evaluates it (fem/assembly/backend/cpu/ElementMap.tpp:55-65)
+int upload_bc_values(rsd_ctx* ctx, rsd_heat* h) {
+	const rsd_mesh* m = h->m;
+	std::vector<double> g(m->nnodes, 0.0);
+	for (int64_t i = 0; i < m->nnodes; ++i) {
+		if (h->h_t2a[i] >= 0) continue;
+		const double* x = &m->h_xyz[i * m->nsd];
+		g[i] = eval_expr_host(h->bcExpr[h->h_ctag[i]], h->time, x[0], x[1], m->nsd == 3 ? x[2] : 0.0, 0.0);
+	}
+	RSD_CUDA(cudaMemcpyAsync(h->g, g.data(), sizeof(double) * m->nnodes, cudaMemcpyHostToDevice, ctx->stream));
+	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+	return RSD_OK;
+}
+
+static bool bc_time_dependent(const rsd_heat* h) {
+	for (int t = 0; t < 6; ++t) if (h->essential[t] && uses_time(h->bcExpr[t])) return true;
+	return false;
+}
+
+static int set_time(rsd_ctx* ctx, rsd_heat* h, double t) {
+	const bool changed = t != h->time;
+	h->time = t;
+	if (changed && bc_time_dependent(h)) return upload_bc_values(ctx, h);
+	return RSD_OK;
+}
+
+__global__ void k_be_rate(int64_t n, double inv_dt, const double* __restrict__ U, const double* __restrict__ Up, double* __restrict__ Ud) {
+	// copy(U, Udot); axpby(-1/dt, 1/dt, Uprev, Udot)  (BackwardEulerStage.hpp:73-74)
+	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+		Ud[i] = inv_dt * U[i] + (-inv_dt) * Up[i];
+}
+__global__ void k_residual_combine(int64_t n, const double* __restrict__ F, double* __restrict__ R) {
+	// axpby(1, -1, F, R): R = -R + F
+	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+		R[i] = -1.0 * R[i] + 1.0 * F[i];
+}
+
+static void free_heat(rsd_heat* h) {
+	cudaFree(h->t2a); cudaFree(h->g); cudaFree(h->kElem); cudaFree(h->tables);
+	cudaFree(h->F); cudaFree(h->R); cudaFree(h->Udot); cudaFree(h->ms); cudaFree(h->dU);
+	if (h->K) rsd_csr_destroy(h->K);
+	delete h;
+}
+
+}  // namespace rsd
+
+using namespace rsd;
+
+extern "C" {
+
+int rsd_heat_create(rsd_ctx* ctx, const rsd_mesh* m, const rsd_heat_desc* d, rsd_heat** out) {
+	if (!ctx || !m || !d || !out) return set_error(RSD_EINVAL, "null argument");
+	if (d->nq < 1 || d->nq > 5) return set_error(RSD_EINVAL, "quadrature points per direction must be 1..5 (kMaxQuadraturePoints1D)");
+	RSD_CUDA(cudaSetDevice(ctx->device));
+	rsd_heat* h = new rsd_heat();
+	h->m = m;
+	h->nq1 = d->nq;
+	h->k_const = d->k_const;
+	h->rho = d->rho;
+	h->cp = d->cp;
+	int rc;
+	if ((rc = compile_expr(d->k_expr, &h->kExpr)) || (rc = compile_expr(d->dk_expr, &h->dkExpr)) || (rc = compile_expr(d->src_expr, &h->srcExpr))) { delete h; return rc; }
+	for (int t = 0; t < 6; ++t) {
+		if (!d->dirichlet_expr[t]) continue;
+		if ((rc = compile_expr(d->dirichlet_expr[t], &h->bcExpr[t]))) { delete h; return rc; }
+		h->essential[t] = true;
+	}
+	build_dofmap(h);
+	cudaError_t e;
+	const int64_t nn = m->nnodes, n = std::max<int64_t>(h->n, 1);
+	if ((e = cudaMalloc(&h->t2a, sizeof(int32_t) * nn)) != cudaSuccess || (e = cudaMalloc(&h->g, sizeof(double) * nn)) != cudaSuccess ||
+	    (e = cudaMalloc(&h->F, sizeof(double) * n)) != cudaSuccess || (e = cudaMalloc(&h->R, sizeof(double) * n)) != cudaSuccess ||
+	    (e = cudaMalloc(&h->Udot, sizeof(double) * n)) != cudaSuccess || (e = cudaMalloc(&h->ms, sizeof(double) * n)) != cudaSuccess ||
+	    (e = cudaMalloc(&h->dU, sizeof(double) * n)) != cudaSuccess) {
+		free_heat(h);
+		return cuda_error(e, "heat problem allocation");
+	}
+	if ((e = cudaMemcpyAsync(h->t2a, h->h_t2a.data(), sizeof(int32_t) * nn, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) { free_heat(h); return cuda_error(e, "dof map upload"); }
+	if (d->k_elem) {
+		if ((e = cudaMalloc(&h->kElem, sizeof(double) * m->nelem)) != cudaSuccess ||
+		    (e = cudaMemcpyAsync(h->kElem, d->k_elem, sizeof(double) * m->nelem, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) {
+			free_heat(h);
+			return cuda_error(e, "element conductivity upload");
+		}
+	}
+	if ((rc = build_tables(h)) || (rc = upload_bc_values(ctx, h)) || (rc = build_pattern(ctx, h, &h->K))) { free_heat(h); return rc; }
+	*out = h;
+	return RSD_OK;
+}
+
+int rsd_heat_destroy(rsd_heat* h) {
+	if (!h) return RSD_OK;
+	cudaDeviceSynchronize();
+	free_heat(h);
+	return RSD_OK;
+}
+
+int rsd_heat_info(const rsd_heat* h, int64_t* num_free, int64_t* nnz) {
+	if (!h) return set_error(RSD_EINVAL, "null problem");
+	if (num_free) *num_free = h->n;
+	if (nnz) *nnz = h->K->nnz;
+	return RSD_OK;
+}
+
+int rsd_heat_dofmap(rsd_ctx* ctx, const rsd_heat* h, int32_t* t2a, int32_t* a2t) {
+	(void)ctx;
+	if (!h) return set_error(RSD_EINVAL, "null problem");
+	if (t2a) std::memcpy(t2a, h->h_t2a.data(), sizeof(int32_t) * h->h_t2a.size());
+	if (a2t) std::memcpy(a2t, h->h_a2t.data(), sizeof(int32_t) * h->h_a2t.size());
+	return RSD_OK;
+}
+
+int rsd_heat_matrix(rsd_heat* h, rsd_csr** A) {
+	if (!h || !A) return set_error(RSD_EINVAL, "null argument");
+	*A = h->K;
+	return RSD_OK;
+}
+
+int rsd_heat_set_time(rsd_ctx* ctx, rsd_heat* h, double t) {
+	if (!ctx || !h) return set_error(RSD_EINVAL, "null argument");
+	h->time = t;
+	return upload_bc_values(ctx, h);
+}
+
+int rsd_heat_set_k_elem(rsd_ctx* ctx, rsd_heat* h, const double* k) {
+	if (!ctx || !h) return set_error(RSD_EINVAL, "null argument");
+	if (!k) { cudaFree(h->kElem); h->kElem = nullptr; return RSD_OK; }
+	if (!h->kElem) RSD_CUDA(cudaMalloc(&h->kElem, sizeof(double) * h->m->nelem));
+	RSD_CUDA(cudaMemcpyAsync(h->kElem, k, sizeof(double) * h->m->nelem, cudaMemcpyDeviceToDevice, ctx->stream));
+	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+	return RSD_OK;
+}
+
+int rsd_assemble_matrix(rsd_ctx* ctx, rsd_heat* h, double cd, double cm, double ct, double ctm, const double* U,
+                        const double* Udot, rsd_csr* A) {
+	if (!ctx || !h || !A) return set_error(RSD_EINVAL, "null argument");
+	RSD_CHECK(assemble_matrix(ctx, h, cd, cm, ct, ctm, U, Udot, A));
+	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+	return RSD_OK;
+}
+
+int rsd_assemble_vector(rsd_ctx* ctx, rsd_heat* h, int32_t which, double coef, const double* U, const double* Udot,
+                        const double* operand, double* out) {
+	if (!ctx || !h || !out || which < 0 || which > 4) return set_error(RSD_EINVAL, "bad argument");
+	RSD_CHECK(assemble_vector(ctx, h, which, coef, U, Udot, operand, out, 1.0, false));
+	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+	return RSD_OK;
+}
+
+int rsd_apply_dirichlet_lift(rsd_ctx* ctx, rsd_heat* h, double cd, double cm, double* F) {
+	if (!ctx || !h || !F) return set_error(RSD_EINVAL, "null argument");
+	RSD_CHECK(assemble_lift(ctx, h, cd, cm, F));
+	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+	return RSD_OK;
+}
+
+int rsd_assemble_diagonal(rsd_ctx* ctx, rsd_heat* h, double cd, double cm, const double* U, double* d) {
+	if (!ctx || !h || !d) return set_error(RSD_EINVAL, "null argument");
+	RSD_CHECK(assemble_diagonal(ctx, h, cd, cm, U, d));
+	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+	return RSD_OK;
+}
+
+// SteadyStage linear: assemble K, load, lift; solve K U = F (solver/stage/SteadyStage.hpp:60-84)
+int rsd_heat_steady(rsd_ctx* ctx, rsd_heat* h, const rsd_solver_cfg* cfg, double* U, rsd_report* rep) {
+	if (!ctx || !h || !cfg || !U) return set_error(RSD_EINVAL, "null argument");
+	RSD_CHECK(assemble_matrix(ctx, h, 1.0, 0.0, 0.0, 0.0, U, nullptr, h->K));
+	RSD_CHECK(assemble_vector(ctx, h, 0, 0.0, U, nullptr, nullptr, h->F, 1.0, false));
+	RSD_CHECK(assemble_lift(ctx, h, 1.0, 0.0, h->F));
+	return solve(ctx, h->K, cfg, h->F, U, rep);
+}
+
+// one BackwardEulerRunner::step, linear mode (solver/timestepper/BackwardEuler.hpp:32-70 over
+// solver/stage/BackwardEulerStage.hpp:71-124)
+int rsd_heat_be_step(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver_cfg* cfg, double* U, double* Uprev,
+                     rsd_report* rep, double* residual_norm) {
+	if (!ctx || !h || !cfg || !U || !Uprev || !(dt > 0)) return set_error(RSD_EINVAL, "bad argument");
+	const int64_t n = h->n;
+	const double t = h->time + dt, inv = 1.0 / dt;
+	const int gv = vec_grid(ctx, n);
+	h->dt = dt;
+	RSD_CHECK(set_time(ctx, h, t));
+	k_be_rate<<<gv, 256, 0, ctx->stream>>>(n, inv, U, Uprev, h->Udot);
+	RSD_CHECK(assemble_matrix(ctx, h, 1.0, inv, 0.0, 0.0, U, h->Udot, h->K));                 // K + M/dt
+	RSD_CHECK(assemble_vector(ctx, h, 0, 0.0, U, h->Udot, nullptr, h->F, 1.0, false));      // load
+	RSD_CHECK(set_time(ctx, h, t - dt));
+	RSD_CHECK(assemble_vector(ctx, h, 2, 0.0, Uprev, nullptr, nullptr, h->F, inv, true));   // F += (1/dt) M Uprev
+	RSD_CHECK(set_time(ctx, h, t));
+	RSD_CHECK(assemble_lift(ctx, h, 1.0, inv, h->F));                                      // F -= (K + M/dt) G
+	RSD_CHECK(solve(ctx, h->K, cfg, h->F, U, rep));
+	if (residual_norm) {
+		// BackwardEulerStage::residualNorm (:113-124) with the Udot of this step's assemble()
+		RSD_CHECK(assemble_vector(ctx, h, 1, 0.0, U, h->Udot, nullptr, h->R, 1.0, false));
+		RSD_CHECK(assemble_vector(ctx, h, 3, 0.0, U, h->Udot, nullptr, h->R, 1.0, true));
+		k_residual_combine<<<gv, 256, 0, ctx->stream>>>(n, h->F, h->R);
+		RSD_CUDA(cudaGetLastError());
+		double rr = 0.0;
+		RSD_CHECK(dot_device(ctx, n, h->R, h->R, &rr));
+		*residual_norm = std::sqrt(rr);
+	}
+	RSD_CUDA(cudaMemcpyAsync(Uprev, U, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));   // advance()
+	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+	return RSD_OK;
+}
+
+// NewtonRunner::solve over SteadyStage nonlinear mode (solver/nonlinear/Newton.hpp:32-83)
+int rsd_heat_newton(rsd_ctx* ctx, rsd_heat* h, double abs_tol, double rel_tol, int64_t max_iters,
+                    const rsd_solver_cfg* lin, double* U, rsd_report* rep) {
+	if (!ctx || !h || !lin || !U) return set_error(RSD_EINVAL, "bad argument");
+	const int64_t n = h->n;
+	const int gv = vec_grid(ctx, n);
+	rsd_report R{};
+	double res0 = 0.0;
+	for (int64_t it = 0; it < max_iters; ++it) {
+		RSD_CHECK(assemble_vector(ctx, h, 0, 0.0, U, nullptr, nullptr, h->F, 1.0, false));   // assembleLoad
+		RSD_CHECK(assemble_vector(ctx, h, 1, 0.0, U, nullptr, nullptr, h->R, 1.0, false));   // K(T) T, Full gather
+		k_residual_combine<<<gv, 256, 0, ctx->stream>>>(n, h->F, h->R);                       // R = F - K(T) T
+		RSD_CUDA(cudaGetLastError());
+		double rr = 0.0;
+		RSD_CHECK(dot_device(ctx, n, h->R, h->R, &rr));
+		const double res = std::sqrt(rr);
+		if (it == 0) res0 = res;
+		const double rel = res0 > 0.0 ? res / res0 : 0.0;
+		R.iterations = it;
+		R.initialResidual = res0; R.finalResidual = res; R.finalResidualRel = rel; R.trueResidualRel = rel;
+		if (!std::isfinite(res)) { R.status = RSD_ENAN; break; }
+		if (res < abs_tol || rel < rel_tol) { R.converged = 1; break; }
+		RSD_CHECK(assemble_matrix(ctx, h, 1.0, 0.0, 1.0, 0.0, U, nullptr, h->K));             // J = K + K_T
+		RSD_CUDA(cudaMemsetAsync(h->dU, 0, sizeof(double) * n, ctx->stream));
+		rsd_report lr;
+		RSD_CHECK(solve(ctx, h->K, lin, h->R, h->dU, &lr));
+		R.refinements += lr.iterations;                                                      // total inner iterations
+		if (!lr.converged) { R.status = lr.status; break; }
+		RSD_CHECK(rsd_axpy(ctx, n, 1.0, h->dU, U));                                           // U += dU
+		if (it == max_iters - 1) R.iterations = max_iters;
+	}
+	if (rep) *rep = R;
+	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+	return RSD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,178 @@
+// Internal declarations shared by the sm_100a translation units of librsd_cuda.so.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/rsd.h"
+
+namespace rsd {
+
+// ---------------------------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------------------------
+int set_error(int code, const std::string& msg);
+int cuda_error(cudaError_t e, const char* what);
+
+#define RSD_CUDA(call)                                                   \
+	do {                                                                 \
+		cudaError_t e_ = (call);                                         \
+		if (e_ != cudaSuccess) return ::rsd::cuda_error(e_, #call);      \
+	} while (0)
+
+#define RSD_CHECK(expr)                      \
+	do {                                     \
+		int rc_ = (expr);                    \
+		if (rc_ != RSD_OK) return rc_;       \
+	} while (0)
+
+// ---------------------------------------------------------------------------------------------
+// launch geometry: B200 has 148 SMs; grids are sized as multiples of the SM count
+// ---------------------------------------------------------------------------------------------
+constexpr int kReduceThreads = 256;
+constexpr int kMaxPartials = 148 * 8;   // one partial per block of a reduction grid
+
+// device scalars of one reduction / Krylov iteration (kept on the device, read by the next kernel)
+struct DevScalars {
+	double rz, pAp, alpha, beta, rr, res0, res, rzNew;
+	double rel, spare0, spare1, spare2;
+	int32_t done, converged, status, pad;
+	int64_t iter;
+	uint32_t ticket;      // last-block-done counter (reset by the last block)
+	uint32_t ticket2;
+};
+
+struct rsd_scratch {
+	double* partials = nullptr;    // kMaxPartials * 4 doubles
+	DevScalars* scal = nullptr;    // device scalars
+	DevScalars* hscal = nullptr;   // pinned host mirror
+	double* hbuf = nullptr;        // pinned host staging (64 doubles)
+};
+
+}  // namespace rsd
+
+namespace rsd {
+// per-kernel-family launch timing with CUDA events on the context stream (off by default)
+enum ProfFamily { PF_SPMV_DOT_F64, PF_SPMV_DOT_F32, PF_CG_UPDATE, PF_CG_PUPDATE, PF_RELIABLE, PF_ASM_MATRIX,
+                  PF_ASM_VECTOR, PF_SPMV, PF_COUNT };
+struct Profiler {
+	bool on = false;
+	std::vector<cudaEvent_t> pool;
+	std::vector<int> fam;          // family of each recorded pair
+	size_t used = 0;               // events in use (pairs * 2)
+	int64_t launches[PF_COUNT] = {};
+	double total_ms[PF_COUNT] = {};
+};
+}  // namespace rsd
+
+struct rsd_ctx {
+	int device = 0;
+	int num_sms = 148;
+	cudaStream_t stream = nullptr;
+	rsd::rsd_scratch s;
+	rsd::Profiler prof;
+};
+
+namespace rsd {
+// bracket one launch: prof_begin returns the pair index or -1 when profiling is off
+int prof_begin(rsd_ctx* ctx, int family);
+void prof_end(rsd_ctx* ctx, int pair);
+int prof_flush(rsd_ctx* ctx);   // fold recorded pairs into the totals (synchronizes the stream)
+}  // namespace rsd
+
+struct rsd_csr {
+	int64_t n = 0, nnz = 0;
+	int32_t* rowPtr = nullptr;     // n+1
+	int32_t* col = nullptr;        // nnz
+	double* val = nullptr;         // nnz
+	float* val32 = nullptr;        // nnz, lazily created for the mixed-precision path
+	int32_t* diag = nullptr;       // n: position of the diagonal entry or -1
+	int lanes = 0;                 // SpMV lanes per row (0: default from nnz/row)
+	int block = 0;                 // SpMV threads per block (0: default)
+	bool owns_pattern = true;
+	uint64_t version = 1;          // bumped whenever the FP64 values may have changed
+	uint64_t version32 = 0;        // FP64 version the FP32 copy was made from
+};
+
+namespace rsd {
+
+// ---------------------------------------------------------------------------------------------
+// expressions: host compiler + device stack machine (bytecode shared by every kernel)
+// ---------------------------------------------------------------------------------------------
+constexpr int kExprMax = 48;
+enum ExprOp : int8_t { E_CONST, E_VAR, E_ADD, E_SUB, E_MUL, E_DIV, E_POW, E_NEG, E_SIN, E_COS, E_TAN, E_EXP, E_LOG, E_SQRT, E_ABS };
+struct DevExpr {
+	int32_t n = 0;          // 0: expression absent
+	int8_t op[kExprMax];
+	int8_t arg[kExprMax];   // variable index (t x y z T) for E_VAR, constant slot for E_CONST
+	double c[kExprMax];
+};
+int compile_expr(const char* src, DevExpr* out);
+double eval_expr_host(const DevExpr& e, double t, double x, double y, double z, double T);
+
+// ---------------------------------------------------------------------------------------------
+// reductions and vector kernels (rsd_blas.cu)
+// ---------------------------------------------------------------------------------------------
+int reduce_grid(rsd_ctx* ctx, int64_t n);
+int dot_device(rsd_ctx* ctx, int64_t n, const double* x, const double* y, double* host_out);
+int spmv_f64(rsd_ctx* ctx, const rsd_csr* A, const double* x, double* y);
+int spmv_f32(rsd_ctx* ctx, const rsd_csr* A, const float* x, float* y);
+int build_diag_index(rsd_ctx* ctx, rsd_csr* A);
+int default_lanes(const rsd_csr* A);
+
+// ---------------------------------------------------------------------------------------------
+// Krylov (rsd_krylov.cu)
+// ---------------------------------------------------------------------------------------------
+int solve(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const double* b, double* x, rsd_report* rep);
+
+}  // namespace rsd
+
+// ---------------------------------------------------------------------------------------------
+// mesh and heat problem (rsd_core.cu / rsd_assemble.cu / rsd_heat.cu)
+// ---------------------------------------------------------------------------------------------
+struct rsd_mesh {
+	int32_t nsd = 0, order = 0, npe = 0, nfaces = 0;
+	int64_t nnodes = 0, nelem = 0;
+	std::vector<double> h_xyz;
+	std::vector<int32_t> h_ien;     // element-major, 32-bit
+	std::vector<int32_t> h_rng;
+	double* xyz = nullptr;          // device, node-major (x,y[,z])
+	int32_t* ien = nullptr;         // device, element-major
+};
+
+struct rsd_heat {
+	const rsd_mesh* m = nullptr;
+	int32_t nq1 = 2;                // Gauss points per direction
+	double k_const = 1.0, rho = 1.0, cp = 1.0;
+	rsd::DevExpr kExpr, dkExpr, srcExpr;
+	rsd::DevExpr bcExpr[6];
+	bool essential[6] = {false, false, false, false, false, false};
+	std::vector<int32_t> h_t2a, h_a2t, h_ctag;
+	int64_t n = 0;
+	int32_t* t2a = nullptr;         // device, per node (-1: constrained)
+	double* g = nullptr;            // device, Dirichlet value per node at the current time
+	double* kElem = nullptr;        // device, per element (or null)
+	double* tables = nullptr;       // device: N, dNdxi, w per quadrature point
+	int nq = 0;                     // total quadrature points
+	double time = 0.0;
+	rsd_csr* K = nullptr;           // matrix with the problem's pattern
+	// stage scratch
+	double *F = nullptr, *R = nullptr, *Udot = nullptr, *ms = nullptr, *dU = nullptr;
+	double dt = 0.0;
+};
+
+namespace rsd {
+int build_dofmap(rsd_heat* h);
+int build_pattern(rsd_ctx* ctx, const rsd_heat* h, rsd_csr** out);
+int upload_bc_values(rsd_ctx* ctx, rsd_heat* h);
+int assemble_matrix(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, double cTDiff, double cTMass,
+                    const double* U, const double* Udot, rsd_csr* A);
+int assemble_vector(rsd_ctx* ctx, rsd_heat* h, int which, double coef, const double* U, const double* Udot,
+                    const double* operand, double* out, double outScale, bool accumulate);
+int assemble_diagonal(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, const double* U, double* d);
+int assemble_lift(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, double* F);
+int build_tables(rsd_heat* h);
+}  // namespace rsd

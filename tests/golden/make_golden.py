@@ -1,0 +1,88 @@
+"""Generate the golden fixtures in this folder from the reference's own templates.
+
+    python tests/golden/make_golden.py
+
+Every array comes from oracle/_ref/libresiduum_ref.so, i.e. the unmodified Residuum templates
+(Assembler<CPU>, BoundaryApplicator<CPU>, TopologicalDOF, cg/gmres::Solver, SteadyStage,
+BackwardEulerStage, NewtonRunner) compiled from the reference tree by oracle/Makefile.  The
+fixtures are small so that the GPU tests can pin the CUDA path to the reference on a machine
+without the reference tree.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+import oracle  # noqa: E402
+
+
+def save(name, **arrays):
+    path = os.path.join(HERE, name)
+    np.savez_compressed(path, **arrays)
+    print(path, {k: np.asarray(v).shape for k, v in arrays.items()})
+
+
+def element_case(name, nsd, order, nq, nel, lo, hi, ess, bc_kind, src_kind, src_c, k_a=1.0, k_b=0.0, k_elem=None,
+                 bc_val=None, seed=0):
+    r = oracle.Reference(nsd, order, nq, nel, lo, hi, ess, bc_kind=bc_kind, bc_val=bc_val, src_kind=src_kind,
+                         src_c=src_c, k_a=k_a, k_b=k_b, k_elem=k_elem)
+    t2a, a2t = r.dofmap()
+    rp, col = r.pattern()
+    rng = np.random.default_rng(seed)
+    U = 0.1 * rng.standard_normal(r.n)
+    Ud = rng.standard_normal(r.n)
+    ones = np.ones(r.n)
+    F = r.assemble_vector(0)
+    arrays = dict(t2a=t2a, a2t=a2t, row_ptr=rp, col=col, U=U, Udot=Ud,
+                  K=r.assemble_matrix("K", U=U), K_cM=r.assemble_matrix("K+cM", 7.5, U=U),
+                  K_KT=r.assemble_matrix("K+KT", U=U), F=F,
+                  lift=r.lift(F, "K") - F, lift_cM=r.lift(F, "K+cM", 7.5) - F,
+                  O_ones=r.assemble_vector(4, 0.0, operand=ones), O_cM=r.assemble_vector(4, 2.5, operand=Ud),
+                  R_diff=r.assemble_vector(1, U=U), M_U=r.assemble_vector(2, U=U), M_Udot=r.assemble_vector(3, Udot=Ud),
+                  diag=r.diagonal("K+cM", 7.5, U=U))
+    if k_elem is not None:
+        arrays["k_elem"] = np.asarray(k_elem)
+    save(name, **arrays)
+    return r
+
+
+def main():
+    # reference fem-tier fixtures: 4x4 Q1 on [0,4]^2, g = x on LEFT/RIGHT/TOP, f = x*y
+    # (tests/integration/fem/heateq/cpu/HeatEquationMinimal2D.cpp) and 4^3 Q1 on [0,4]^3, g = x on the
+    # four lateral faces, f = x*y*z (HeatEquationMinimal3D.cpp)
+    element_case("q1_quad_4x4.npz", 2, 1, 2, [4, 4], [0, 0], [4, 4], [0, 1, 3], 1, 1, 1.0)
+    element_case("q1_hex_4x4x4.npz", 3, 1, 2, [4, 4, 4], [0, 0, 0], [4, 4, 4], [0, 1, 2, 3], 1, 1, 1.0)
+    # Q2 hex with k(T) = 1 + 0.5 T, Dirichlet 0 / 1 on x = 0 / 1 (the 48^3 Q2 nonlinear configuration's physics)
+    element_case("q2_hex_3x3x2.npz", 3, 2, 3, [3, 3, 2], [0, 0, 0], [1, 1, 1], [0, 1], 0, 0, 10.0, k_a=1.0, k_b=0.5,
+                 bc_val={0: 0.0, 1: 1.0})
+    # Q2 quad with per-element conductivity and g = (1-x)(1-y)
+    ke = np.exp(np.random.default_rng(7).standard_normal(15))
+    element_case("q2_quad_kelem.npz", 2, 2, 3, [5, 3], [0, 0], [1, 1], [0, 1, 2, 3], 2, 0, 1.0, k_elem=ke)
+
+    # steady 2D Q1 16x16, T = (1-x)(1-y) on all sides, CG + Jacobi to 1e-10 (the 64x64 configuration's physics)
+    r = oracle.Reference(2, 1, 2, [16, 16], [0, 0], [1, 1], [0, 1, 2, 3], bc_kind=2)
+    U, rep = r.steady(0, 1, 1e-10, 1000)
+    save("steady_q1_quad_16.npz", U=U, iterations=rep["iterations"], finalResidual=rep["finalResidual"],
+         initialResidual=rep["initialResidual"])
+    U, rep = r.steady(1, 1, 1e-10, 1000, 7)
+    save("steady_gmres7_q1_quad_16.npz", U=U, iterations=rep["iterations"], finalResidual=rep["finalResidual"])
+
+    # Backward Euler, 3D Q1 6x5x4, Dirichlet 0, dt = 1e-2, 5 steps, CG + Jacobi 1e-8
+    r = oracle.Reference(3, 1, 2, [6, 5, 4], [0, 0, 0], [1, 1, 1], list(range(6)), bc_kind=0)
+    U0 = np.sin(np.arange(r.n) * 0.37)
+    U, res, rc = r.backward_euler(1e-2, 5, U0, tol=1e-8)
+    save("be_q1_hex_6x5x4.npz", U0=U0, U=U, residual=res)
+
+    # Newton + GMRES(30) + Jacobi, Q2 hex 3^3, k = 1 + 0.5 T, f = 10, T = 0 / 1 on x = 0 / 1
+    r = oracle.Reference(3, 2, 3, [3, 3, 3], [0, 0, 0], [1, 1, 1], [0, 1], bc_kind=0, bc_val={0: 0.0, 1: 1.0},
+                         src_kind=0, src_c=10.0, k_a=1.0, k_b=0.5)
+    U, rep = r.newton(1e-10, 1e-10, 50, 1, 1, 1e-12, 1000, 30)
+    save("newton_q2_hex_3.npz", U=U, iterations=rep["iterations"], finalResidual=rep["finalResidual"])
+
+
+if __name__ == "__main__":
+    if not oracle.reference_available():
+        sys.exit("oracle/_ref/libresiduum_ref.so is missing: run make -C oracle (needs the reference tree)")
+    main()

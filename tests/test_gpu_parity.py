@@ -1,0 +1,273 @@
+"""GPU parity: the CUDA path through the C ABI against the golden fixtures (the reference
+templates' own output) and the C restatement, on the same seeded inputs.
+
+Tolerances: integer work (DOF map, CSR pattern) is bit-exact; FP64 values and solutions agree to
+<= 1e-12 relative (max-abs error over max-abs value); FP32 work states its own bound in each test.
+"""
+from importlib import import_module
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+REL = 1e-12
+
+
+def relerr(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def bm():
+    return import_module("residuum_solver_b200.blockmesh")
+
+
+def make_heat(rsd, ctx, nsd, order, nq, nel, lo, hi, **kw):
+    xyz, ien, rng = bm().block_mesh(nsd, nel, lo, hi, order)
+    mesh = rsd.Mesh(ctx, nsd, order, xyz, ien, rng)
+    return rsd.Heat(ctx, mesh, nq, **kw)
+
+
+CASES = [
+    ("q1_quad_4x4.npz", 2, 1, 2, [4, 4], [0, 0], [4, 4], dict(src_expr="x*y", dirichlet={0: "x", 1: "x", 3: "x"})),
+    ("q1_hex_4x4x4.npz", 3, 1, 2, [4, 4, 4], [0, 0, 0], [4, 4, 4], dict(src_expr="x*y*z", dirichlet={t: "x" for t in range(4)})),
+    ("q2_hex_3x3x2.npz", 3, 2, 3, [3, 3, 2], [0, 0, 0], [1, 1, 1],
+     dict(src_expr="10", k_expr="1 + 0.5*T", dk_expr="0.5", dirichlet={0: "0", 1: "1"})),
+    ("q2_quad_kelem.npz", 2, 2, 3, [5, 3], [0, 0], [1, 1], dict(src_expr="1", dirichlet={t: "(1-x)*(1-y)" for t in range(4)})),
+]
+
+
+@pytest.mark.parametrize("name,nsd,order,nq,nel,lo,hi,kw", CASES)
+def test_element_loops_match_reference(rsd, ctx, name, nsd, order, nq, nel, lo, hi, kw):
+    g = golden(name)
+    if "k_elem" in g:
+        kw = dict(kw, k_elem=g["k_elem"])
+    h = make_heat(rsd, ctx, nsd, order, nq, nel, lo, hi, **kw)
+    t2a, a2t = h.dofmap()
+    assert (t2a == g["t2a"]).all() and (a2t == g["a2t"]).all()            # bit-exact DOF map
+    rp, col = h.K.pattern()
+    assert (rp == g["row_ptr"]).all() and (col == g["col"]).all()         # bit-exact pattern
+    n = h.n
+    U, Ud = ctx.to_device(g["U"]), ctx.to_device(g["Udot"])
+    h.assemble_matrix(U=U)
+    assert relerr(h.K.values(), g["K"]) <= REL
+    h.assemble_matrix(1.0, 7.5, U=U)
+    assert relerr(h.K.values(), g["K_cM"]) <= REL
+    h.assemble_matrix(1.0, 0.0, 1.0, 0.0, U=U)
+    assert relerr(h.K.values(), g["K_KT"]) <= REL
+    out = ctx.array(n)
+    h.assemble_vector(0, out)
+    F = out.download()
+    assert relerr(F, g["F"]) <= REL
+    Fd = ctx.to_device(g["F"])
+    h.lift(Fd)
+    assert relerr(Fd.download() - g["F"], g["lift"]) <= REL
+    Fd = ctx.to_device(g["F"])
+    h.lift(Fd, 1.0, 7.5)
+    assert relerr(Fd.download() - g["F"], g["lift_cM"]) <= REL
+    ones = ctx.to_device(np.ones(n))
+    h.assemble_vector(4, out, coef=0.0, operand=ones)
+    assert relerr(out.download(), g["O_ones"]) <= REL
+    h.assemble_vector(4, out, coef=2.5, operand=Ud)
+    assert relerr(out.download(), g["O_cM"]) <= REL
+    h.assemble_vector(1, out, U=U)
+    assert relerr(out.download(), g["R_diff"]) <= REL
+    h.assemble_vector(2, out, U=U)
+    assert relerr(out.download(), g["M_U"]) <= REL
+    h.assemble_vector(3, out, Udot=Ud)
+    assert relerr(out.download(), g["M_Udot"]) <= REL
+    h.diagonal(out, 1.0, 7.5, U=U)
+    assert relerr(out.download(), g["diag"]) <= REL
+
+
+def test_steady_cg_and_gmres_match_reference(rsd, ctx):
+    h = make_heat(rsd, ctx, 2, 1, 2, [16, 16], [0, 0], [1, 1], dirichlet={t: "(1-x)*(1-y)" for t in range(4)})
+    g = golden("steady_q1_quad_16.npz")
+    U = ctx.array(h.n).zero()
+    rep = h.steady(U, type=rsd.CG, precond=rsd.JACOBI, tol=1e-10, max_iters=1000)
+    assert rep["converged"] and rep["iterations"] == g["iterations"]
+    assert relerr(U.download(), g["U"]) <= REL
+    g = golden("steady_gmres7_q1_quad_16.npz")
+    U.zero()
+    rep = h.steady(U, type=rsd.GMRES, precond=rsd.JACOBI, tol=1e-10, max_iters=1000, krylov_dim=7)
+    assert rep["converged"] and rep["iterations"] == g["iterations"]
+    assert relerr(U.download(), g["U"]) <= REL
+
+
+def test_backward_euler_matches_reference(rsd, ctx):
+    g = golden("be_q1_hex_6x5x4.npz")
+    h = make_heat(rsd, ctx, 3, 1, 2, [6, 5, 4], [0, 0, 0], [1, 1, 1], rho=1.0, cp=1.0, dirichlet={t: "0" for t in range(6)})
+    U, Up = ctx.to_device(g["U0"]), ctx.to_device(g["U0"])
+    res = []
+    for _ in range(5):
+        rep = h.be_step(1e-2, U, Up, type=rsd.CG, precond=rsd.JACOBI, tol=1e-8, max_iters=1000)
+        assert rep["converged"]
+        res.append(rep["residualNorm"])
+    assert relerr(U.download(), g["U"]) <= REL
+    assert relerr(res, g["residual"]) <= 1e-9   # norms of residuals ~1e-8 of their parts: cancellation
+
+
+def test_newton_gmres_matches_reference(rsd, ctx):
+    g = golden("newton_q2_hex_3.npz")
+    h = make_heat(rsd, ctx, 3, 2, 3, [3, 3, 3], [0, 0, 0], [1, 1, 1], src_expr="10", k_expr="1 + 0.5*T", dk_expr="0.5",
+                  dirichlet={0: "0", 1: "1"})
+    U = ctx.array(h.n).zero()
+    cfg = rsd.SolverConfig.make(type=rsd.GMRES, precond=rsd.JACOBI, tol=1e-12, max_iters=1000, krylov_dim=30)
+    rep = h.newton(U, 1e-10, 1e-10, 50, cfg=cfg)
+    assert rep["converged"] and rep["iterations"] == g["iterations"]
+    assert relerr(U.download(), g["U"]) <= 1e-11
+
+
+def random_csr(n, per_row, seed):
+    rng = np.random.default_rng(seed)
+    rows = []
+    for i in range(n):
+        c = np.unique(np.concatenate([[i], rng.integers(0, n, per_row)]))
+        rows.append(c)
+    rp = np.zeros(n + 1, np.int64)
+    rp[1:] = np.cumsum([len(r) for r in rows])
+    col = np.concatenate(rows).astype(np.int64)
+    val = rng.standard_normal(len(col))
+    return rp, col, val
+
+
+@pytest.mark.parametrize("n,per_row", [(1, 1), (7, 3), (1000, 9), (20000, 27), (5000, 120)])
+def test_spmv_matches_reference(rsd, ctx, n, per_row):
+    rp, col, val = random_csr(n, per_row, n)
+    A = rsd.CSR.from_host(ctx, rp, col, val)
+    x = np.random.default_rng(1).standard_normal(n)
+    y_ref = oracle.spmv(rp, col, val, x)
+    xd, yd = ctx.to_device(x), ctx.array(n)
+    for lanes in (0, 2, 4, 8, 16, 32):
+        A.set_launch(lanes, 0)
+        A.spmv(xd, yd)
+        assert relerr(yd.download(), y_ref) <= 1e-13
+    # FP32 values and vector: error bounded by the row's absolute sum times a few FP32 ulps
+    A.set_launch(0, 0)
+    A.sync_f32()
+    x32, y32 = ctx.to_device(x.astype(np.float32)), ctx.array(n, np.float32)
+    A.spmv_f32(x32, y32)
+    bound = 4 * np.finfo(np.float32).eps * oracle.spmv(rp, col, np.abs(val), np.abs(x)) * (rp[1:] - rp[:-1]).max()
+    assert (np.abs(y32.download() - y_ref) <= bound + 1e-30).all()
+
+
+def test_blas1_matches_numpy(rsd, ctx):
+    rng = np.random.default_rng(3)
+    n = 100003
+    x, y = rng.standard_normal(n), rng.standard_normal(n)
+    xd, yd = ctx.to_device(x), ctx.to_device(y)
+    import ctypes as C
+    out = C.c_double()
+    rsd.check(rsd.lib().rsd_dot(ctx.h, n, xd.ptr, yd.ptr, C.byref(out)))
+    assert abs(out.value - x @ y) <= 1e-12 * np.abs(x * y).sum()
+    rsd.check(rsd.lib().rsd_axpby(ctx.h, n, 2.0, -0.5, xd.ptr, yd.ptr))
+    assert relerr(yd.download(), -0.5 * y + 2.0 * x) <= 1e-15
+    rsd.check(rsd.lib().rsd_mul(ctx.h, n, xd.ptr, xd.ptr, yd.ptr))
+    assert relerr(yd.download(), x * x) == 0.0
+    rsd.check(rsd.lib().rsd_nrm2(ctx.h, n, xd.ptr, C.byref(out)))
+    assert abs(out.value - np.linalg.norm(x)) <= 1e-12 * np.linalg.norm(x)
+    rsd.check(rsd.lib().rsd_dot(ctx.h, 0, xd.ptr, yd.ptr, C.byref(out)))
+    assert out.value == 0.0
+
+
+def test_krylov_known_answers(rsd, ctx):
+    # cg/Solver.cpp:12-68 and gmres/Solver.cpp:12-172 of the reference's unit tests
+    A = rsd.CSR.from_host(ctx, [0, 2, 4], [0, 1, 0, 1], [4.0, 1.0, 1.0, 3.0])
+    b, x = ctx.to_device(np.array([1.0, 2.0])), ctx.array(2).zero()
+    rep = rsd.solve(ctx, A, b, x, type=rsd.CG, tol=1e-12)
+    assert rep["converged"] and np.allclose(x.download(), [1 / 11, 7 / 11], atol=1e-10)
+    B = rsd.CSR.from_host(ctx, [0, 2, 4], [0, 1, 0, 1], [2.0, 1.0, 3.0, 4.0])
+    b2, x2 = ctx.to_device(np.array([1.0, 3.0])), ctx.array(2).zero()
+    rep = rsd.solve(ctx, B, b2, x2, type=rsd.GMRES, krylov_dim=1, tol=1e-10, max_iters=200)
+    assert rep["converged"] and np.allclose(x2.download(), [0.2, 0.6], atol=1e-8)
+
+
+def test_mixed_precision_reaches_fp64_checked_tolerance(rsd, ctx):
+    h = make_heat(rsd, ctx, 3, 1, 2, [24, 24, 24], [0, 0, 0], [1, 1, 1], src_expr="1", dirichlet={t: "0" for t in range(6)})
+    n = h.n
+    h.assemble_matrix(1.0, 1000.0)
+    F = ctx.array(n)
+    h.assemble_vector(0, F)
+    x64, xmx = ctx.array(n).zero(), ctx.array(n).zero()
+    r64 = rsd.solve(ctx, h.K, F, x64, type=rsd.CG, tol=1e-8)
+    rmx = rsd.solve(ctx, h.K, F, xmx, type=rsd.CG, precision=rsd.MIXED, tol=1e-8)
+    assert r64["converged"] and rmx["converged"] and rmx["refinements"] >= 1
+    assert rmx["trueResidualRel"] < 1e-8          # checked in FP64 with the FP64 matrix
+    assert r64["trueResidualRel"] < 1.01e-8
+    # stated error against the FP64 solve: both within tol * cond of the exact solution
+    assert relerr(xmx.download(), x64.download()) < 1e-6
+
+
+def test_edge_cases(rsd, ctx):
+    # empty matrix
+    E = rsd.CSR.from_host(ctx, [0], [], [])
+    assert E.n == 0
+    rep = rsd.solve(ctx, E, None, None, type=rsd.CG)
+    assert rep["converged"]
+    # maxIters = 1: no iteration runs (cg/Solver.tpp:66), not converged
+    A = rsd.CSR.from_host(ctx, [0, 2, 4], [0, 1, 0, 1], [4.0, 1.0, 1.0, 3.0])
+    b, x = ctx.to_device(np.array([1.0, 2.0])), ctx.array(2).zero()
+    rep = rsd.solve(ctx, A, b, x, type=rsd.CG, tol=1e-12, max_iters=1)
+    assert not rep["converged"] and rep["iterations"] == 1
+    # Jacobi with a (near) zero diagonal uses 1 (Jacobi.hpp:33)
+    Z = rsd.CSR.from_host(ctx, [0, 1, 2], [0, 1], [1e-320, 2.0])
+    d = ctx.array(2)
+    Z.jacobi(d)
+    assert (d.download() == [1.0, 0.5]).all()
+    # NaN in the right-hand side comes back as a status, not a hang
+    bn, xn = ctx.to_device(np.array([np.nan, 1.0])), ctx.array(2).zero()
+    rep = rsd.solve(ctx, A, bn, xn, type=rsd.CG, tol=1e-12, max_iters=50)
+    assert not rep["converged"] and rep["status"] in (-5, -6)
+    # invalid arguments are errors
+    with pytest.raises(rsd.RsdError):
+        rsd.CSR.from_host(ctx, [0, 2], [0, 5], [1.0, 1.0])
+    xyz, ien, rng = bm().block_mesh(2, [2, 2], [0, 0], [1, 1], 1)
+    mesh = rsd.Mesh(ctx, 2, 1, xyz, ien, rng)
+    with pytest.raises(rsd.RsdError) as e:
+        rsd.Heat(ctx, mesh, 2, src_expr="not an expression (")
+    assert e.value.code == -7
+    with pytest.raises(rsd.RsdError):
+        rsd.Heat(ctx, mesh, 7)
+    with pytest.raises(rsd.RsdError):
+        xyz3, ien3, rng3 = bm().block_mesh(3, [1, 1, 1], [0, 0, 0], [1, 1, 1], 3)
+        rsd.Mesh(ctx, 3, 3, xyz3, ien3, rng3)       # Q3 hex: 64 nodes per element, unsupported
+
+
+def test_larger_case_against_restatement(rsd, ctx):
+    # 20^3 Q1 hex: pattern bit-exact and values within 1e-12 of the restatement
+    m = oracle.BlockMesh(3, [20, 20, 20], [0, 0, 0], [1, 1, 1], 1)
+    o = oracle.Oracle(m, 2, src_expr="1", bc={t: "0" for t in range(6)})
+    h = make_heat(rsd, ctx, 3, 1, 2, [20, 20, 20], [0, 0, 0], [1, 1, 1], src_expr="1", dirichlet={t: "0" for t in range(6)})
+    rp, col = h.K.pattern()
+    orp, ocol = o.pattern()
+    assert (rp == orp).all() and (col == ocol).all()
+    h.assemble_matrix(1.0, 1000.0)
+    assert relerr(h.K.values(), o.assemble_matrix(1.0, 1000.0)) <= REL
+    F = ctx.array(h.n)
+    h.assemble_vector(0, F)
+    assert relerr(F.download(), o.assemble_vector(0)) <= REL
+
+
+def test_size_independent_properties_at_scale(rsd, ctx):
+    # 96^3 Q1 hex (857k rows): K + M/dt is symmetric with positive diagonal, SpMV is linear,
+    # K.1 vanishes on rows away from the Dirichlet boundary
+    h = make_heat(rsd, ctx, 3, 1, 2, [96, 96, 96], [0, 0, 0], [1, 1, 1], dirichlet={t: "0" for t in range(6)})
+    n = h.n
+    h.assemble_matrix(1.0, 0.0)
+    rng = np.random.default_rng(5)
+    x, y = rng.standard_normal(n), rng.standard_normal(n)
+    xd, yd, zd = ctx.to_device(x), ctx.to_device(y), ctx.to_device(x + 2 * y)
+    ax, ay, az = ctx.array(n), ctx.array(n), ctx.array(n)
+    h.K.spmv(xd, ax); h.K.spmv(yd, ay); h.K.spmv(zd, az)
+    assert relerr(az.download(), ax.download() + 2 * ay.download()) < 1e-12
+    ones, k1 = ctx.to_device(np.ones(n)), ctx.array(n)
+    h.K.spmv(ones, k1)
+    t2a, a2t = h.dofmap()
+    ijk = np.stack(np.unravel_index(a2t, (97, 97, 97)), 1)
+    interior = ((ijk >= 2) & (ijk <= 94)).all(1)
+    assert np.abs(k1.download()[interior]).max() < 1e-12
+    # symmetry via x.Ay == y.Ax
+    assert abs(x @ ay.download() - y @ ax.download()) < 1e-10 * abs(x @ ax.download())
