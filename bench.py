@@ -224,6 +224,8 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=48)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--reliable-delta", type=float, default=0.0)
+    ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
+                    help="run one solver path only (no e2e, no CPU leg): for profiler captures")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -298,6 +300,16 @@ def main():
         return ms, reps, prof, clk
 
     clocks = ClockSampler(local)
+    if args.only:
+        ms, reps, prof, _ = run(cfgs[args.only], args.steps, args.warmup, profile=False)
+        if rank == 0:
+            print(json.dumps({"only": args.only, "ms_per_step": ms, "iterations": [r["iterations"] for r in reps],
+                              "true_residual_rel": [r["trueResidualRel"] for r in reps]}))
+        del heat, mesh
+        ctx.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     ms_mx, reps_mx, prof_mx, clk = run(cfgs["mixed"], args.steps, args.warmup, profile=True, clocks=clocks)
     ms_64, reps_64, prof_64, _ = run(cfgs["fp64"], args.steps, args.warmup, profile=True)
 

@@ -23,11 +23,16 @@ namespace rsd {
 struct AsmParams {
 	int64_t nelem;
 	int32_t nq;
-	int32_t which;              // vector kernels: 0 load, 1 diffusion(U), 2 mass(U), 3 mass(Udot), 4 operator(V), 5 lift, 6 adjoint
+	// vector kernels: 0 load, 1 diffusion(U), 2 mass(U), 3 mass(Udot), 4 operator(V), 5 lift, 6 adjoint,
+	// 7 Backward-Euler right-hand side load + coef*mass(U), 8 stage residual diffusion(U) + mass(Udot),
+	// 9 Newton residual load - diffusion(U)
+	int32_t which;
+	const int32_t* __restrict__ elist;  // element subset (lift: elements touching a constrained node) or null
 	const double* __restrict__ xyz;
 	const int32_t* __restrict__ ien;
 	const int32_t* __restrict__ t2a;
 	const double* __restrict__ g;       // Dirichlet value per node
+	const double* __restrict__ gPrev;   // Dirichlet value per node at the previous time (which 7), or null
 	const double* __restrict__ kElem;
 	const double* __restrict__ tables;  // [nq][G][4] (N, dxi, deta, dzeta) then w[nq]
 	double kConst, rho, cp, time;
@@ -105,11 +110,11 @@ __device__ __forceinline__ void phys_grad(const double (&inv)[9], const double (
 
 // element data for the lane: node, row, coordinates; returns false when the lane has no node
 template <int NSD, int P>
-__device__ __forceinline__ bool load_node(const AsmParams& prm, int64_t e, int a, int32_t& node, int32_t& row, double (&xa)[3]) {
+__device__ __forceinline__ bool load_node(const AsmParams& prm, bool valid, int64_t e, int a, int32_t& node, int32_t& row, double (&xa)[3]) {
 	using E = Elem<NSD, P>;
 	xa[0] = xa[1] = xa[2] = 0.0;
 	node = 0; row = -1;
-	if (e >= prm.nelem || a >= E::NPE) return false;
+	if (!valid || a >= E::NPE) return false;
 	node = prm.ien[e * E::NPE + a];
 	row = prm.t2a[node];
 #pragma unroll
@@ -145,7 +150,7 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_matrix(const AsmParams prm)
 		const int64_t e = eb + slot;
 		int32_t node, row;
 		double xa[3];
-		const bool has = load_node<NSD, P>(prm, e, a, node, row, xa);
+		const bool has = load_node<NSD, P>(prm, e < prm.nelem, e, a, node, row, xa);
 		double Ua = 0.0;
 		if (has && needState) Ua = row >= 0 ? (prm.U ? prm.U[row] : 0.0) : prm.g[node];
 		const double ke = (prm.kElem && e < prm.nelem) ? prm.kElem[e] : 1.0;
@@ -238,27 +243,33 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_vector(const AsmParams prm)
 	const int64_t warpId = (int64_t)blockIdx.x * warpsPerBlock + (threadIdx.x >> 5);
 	const int64_t warpStride = (int64_t)gridDim.x * warpsPerBlock;
 	const int which = prm.which;
-	const bool needT = (prm.kExpr.n != 0) && (which == 1 || which == 4);
+	const bool kT = prm.kExpr.n != 0;
+	const bool hasLoad = which == 0 || which == 7 || which == 9;
+	const bool opState = kT && which == 4;   // the operator takes k(T) from the state U, not the operand
 	for (int64_t eb = warpId * EPW; eb < prm.nelem; eb += warpStride * EPW) {
-		const int64_t e = eb + slot;
+		const int64_t idx = eb + slot;
+		const bool inRange = idx < prm.nelem;
+		const int64_t e = inRange ? (prm.elist ? (int64_t)prm.elist[idx] : idx) : 0;
 		int32_t node, row;
 		double xa[3];
-		const bool has = load_node<NSD, P>(prm, e, a, node, row, xa);
-		// gathered operand (V) and state (Ua for k(T))
-		double Va = 0.0, Ua = 0.0;
+		const bool has = load_node<NSD, P>(prm, inRange, e, a, node, row, xa);
+		// gathered operand V, second operand W (Udot) and state U (for k(T))
+		double Va = 0.0, Wa = 0.0, Ua = 0.0;
 		if (has) {
 			const double fullU = row >= 0 ? (prm.U ? prm.U[row] : 0.0) : prm.g[node];
 			switch (which) {
-				case 1: case 2: Va = fullU; break;                                         // GatherMode::Full
-				case 3: Va = (row >= 0 && prm.Udot) ? prm.Udot[row] : 0.0; break;          // Free
-				case 4: Va = (row >= 0 && prm.V) ? prm.V[row] : 0.0; break;                // Free
-				case 5: Va = row >= 0 ? 0.0 : prm.g[node]; break;                          // Constrained
-				case 6: Va = (row >= 0 && prm.V) ? prm.V[row] : 0.0; Ua = fullU; break;    // lambda (Free), T (Full)
+				case 1: case 2: case 8: case 9: Va = fullU; break;                          // GatherMode::Full
+				case 3: Va = (row >= 0 && prm.Udot) ? prm.Udot[row] : 0.0; break;           // Free
+				case 4: Va = (row >= 0 && prm.V) ? prm.V[row] : 0.0; break;                 // Free
+				case 5: Va = row >= 0 ? 0.0 : prm.g[node]; break;                           // Constrained
+				case 6: Va = (row >= 0 && prm.V) ? prm.V[row] : 0.0; Ua = fullU; break;     // lambda (Free), T (Full)
+				case 7: Va = row >= 0 ? (prm.U ? prm.U[row] : 0.0) : (prm.gPrev ? prm.gPrev[node] : prm.g[node]); break;
 				default: break;
 			}
-			if (needT) Ua = fullU;
+			if (which == 8) Wa = (row >= 0 && prm.Udot) ? prm.Udot[row] : 0.0;
+			if (opState) Ua = fullU;
 		}
-		const double ke = (prm.kElem && e < prm.nelem) ? prm.kElem[e] : 1.0;
+		const double ke = (prm.kElem && inRange) ? prm.kElem[e] : 1.0;
 		double Fa = 0.0, ge = 0.0;
 		for (int q = 0; q < prm.nq; ++q) {
 			const double* tq = tab + (q * G) * 4;
@@ -273,13 +284,13 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_vector(const AsmParams prm)
 			double dx[3];
 			phys_grad<NSD>(inv, dxi, dx);
 			const double wm = measure * wq[q];
-			if (which == 0) {
+			if (hasLoad) {
 				double xq[3] = {0.0, 0.0, 0.0};
 #pragma unroll
 				for (int i = 0; i < NSD; ++i) xq[i] = group_sum<G>(Na * xa[i]);
 				const double f = prm.srcExpr.n ? eval_expr(prm.srcExpr, prm.time, xq[0], xq[1], NSD == 3 ? xq[2] : 0.0, 0.0) : 0.0;
 				Fa += (f * Na) * wm;
-				continue;
+				if (which == 0) continue;
 			}
 			const double Vq = group_sum<G>(Na * Va);
 			double gv[3] = {0.0, 0.0, 0.0};
@@ -296,9 +307,12 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_vector(const AsmParams prm)
 				continue;
 			}
 			double k = prm.kConst;
-			if (needT) k = eval_expr(prm.kExpr, 0.0, 0.0, 0.0, 0.0, group_sum<G>(Na * Ua));
-			// the lift interpolates no state: a temperature-dependent k is taken at T = 0
-			else if (which == 5 && prm.kExpr.n) k = eval_expr(prm.kExpr, 0.0, 0.0, 0.0, 0.0, 0.0);
+			if (kT) {
+				// diffusion of U takes T from U itself; the operator from the state; the lift
+				// interpolates no state, so k is taken at T = 0 there
+				const double T = (which == 1 || which == 8 || which == 9) ? Vq : opState ? group_sum<G>(Na * Ua) : 0.0;
+				k = eval_expr(prm.kExpr, 0.0, 0.0, 0.0, 0.0, T);
+			}
 			double dd = 0.0;
 #pragma unroll
 			for (int i = 0; i < NSD; ++i) dd += dx[i] * gv[i];
@@ -308,11 +322,18 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_vector(const AsmParams prm)
 				case 2: case 3: Fa += mass * wm; break;
 				case 4: Fa += (ke * k * dd + prm.coef * mass) * wm; break;
 				case 5: Fa += (prm.cDiff * ke * k * dd + prm.cMass * mass) * wm; break;
+				case 7: Fa += prm.coef * mass * wm; break;
+				case 8: {
+					const double Wq = group_sum<G>(Na * Wa);
+					Fa += (ke * k * dd + prm.rho * prm.cp * Na * Wq) * wm;
+					break;
+				}
+				case 9: Fa -= ke * k * dd * wm; break;
 				default: break;
 			}
 		}
 		if (which == 6) {
-			if (a == 0 && e < prm.nelem) prm.out[e] = ge;
+			if (a == 0 && inRange) prm.out[e] = ge;
 		} else if (has && row >= 0) {
 			atomicAdd(prm.out + row, prm.outScale * Fa);
 		}
@@ -337,7 +358,7 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_diag(const AsmParams prm) {
 		const int64_t e = eb + slot;
 		int32_t node, row;
 		double xa[3];
-		const bool has = load_node<NSD, P>(prm, e, a, node, row, xa);
+		const bool has = load_node<NSD, P>(prm, e < prm.nelem, e, a, node, row, xa);
 		double Ua = 0.0;
 		if (has && needT) Ua = row >= 0 ? (prm.U ? prm.U[row] : 0.0) : prm.g[node];
 		const double ke = (prm.kElem && e < prm.nelem) ? prm.kElem[e] : 1.0;
@@ -472,7 +493,7 @@ static int launch_one(void (*kern)(const AsmParams), dim3 gr, size_t smem, rsd_c
 		const int nsd = h->m->nsd, ord = h->m->order, G = group_width(h->m->npe);             \
 		const size_t smem = sizeof(double) * (h->nq * G * 4 + h->nq);                         \
 		const int epb = (kAsmThreads / 32) * (32 / G);                                        \
-		int64_t blocks = (h->m->nelem + epb - 1) / epb;                                       \
+		int64_t blocks = (p.nelem + epb - 1) / epb;                                           \
 		blocks = std::min<int64_t>(blocks, (int64_t)ctx->num_sms * 16);                       \
 		dim3 gr((unsigned)std::max<int64_t>(blocks, 1));                                      \
 		if (nsd == 2 && ord == 1) return launch_one(KERNEL<2, 1>, gr, smem, ctx, p);          \
@@ -506,6 +527,7 @@ int assemble_vector(rsd_ctx* ctx, rsd_heat* h, int which, double coef, const dou
                     const double* operand, double* out, double outScale, bool accumulate) {
 	AsmParams p = params_for(h);
 	p.which = which; p.coef = coef; p.U = U; p.Udot = Udot; p.V = operand; p.out = out; p.outScale = outScale;
+	if (which == 7 && h->gPrevValid) p.gPrev = h->gPrev;
 	if (!accumulate) {
 		const int64_t len = which == 6 ? h->m->nelem : h->n;
 		RSD_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * std::max<int64_t>(len, 1), ctx->stream));
@@ -516,10 +538,16 @@ int assemble_vector(rsd_ctx* ctx, rsd_heat* h, int which, double coef, const dou
 	return rc;
 }
 
+// the lift visits only elements with a constrained node: every other element adds exact zeros
 int assemble_lift(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, double* F) {
+	if (h->nbElems == 0) return RSD_OK;
 	AsmParams p = params_for(h);
 	p.which = 5; p.cDiff = cDiff; p.cMass = cMass; p.out = F; p.outScale = -1.0;
-	return launch_k_asm_vector(ctx, h, p);
+	p.elist = h->bElems; p.nelem = h->nbElems;
+	const int pr = prof_begin(ctx, PF_ASM_VECTOR);
+	const int rc = launch_k_asm_vector(ctx, h, p);
+	prof_end(ctx, pr);
+	return rc;
 }
 
 int assemble_diagonal(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, const double* U, double* d) {

@@ -15,20 +15,22 @@ static bool uses_time(const DevExpr& e) {
 	return false;
 }
 
-// Dirichlet value per constrained node at the current time: the constraint tag's expression at
-// the node's coordinates, as gatherElementVector evaluates it (fem/assembly/backend/cpu/ElementMap.tpp:55-65)
-int upload_bc_values(rsd_ctx* ctx, rsd_heat* h) {
+// Dirichlet value per constrained node at time t: the constraint tag's expression at the node's
+// coordinates, as gatherElementVector evaluates it (fem/assembly/backend/cpu/ElementMap.tpp:55-65)
+static int bc_values_to(rsd_ctx* ctx, const rsd_heat* h, double t, double* dst) {
 	const rsd_mesh* m = h->m;
 	std::vector<double> g(m->nnodes, 0.0);
 	for (int64_t i = 0; i < m->nnodes; ++i) {
 		if (h->h_t2a[i] >= 0) continue;
 		const double* x = &m->h_xyz[i * m->nsd];
-		g[i] = eval_expr_host(h->bcExpr[h->h_ctag[i]], h->time, x[0], x[1], m->nsd == 3 ? x[2] : 0.0, 0.0);
+		g[i] = eval_expr_host(h->bcExpr[h->h_ctag[i]], t, x[0], x[1], m->nsd == 3 ? x[2] : 0.0, 0.0);
 	}
-	RSD_CUDA(cudaMemcpyAsync(h->g, g.data(), sizeof(double) * m->nnodes, cudaMemcpyHostToDevice, ctx->stream));
+	RSD_CUDA(cudaMemcpyAsync(dst, g.data(), sizeof(double) * m->nnodes, cudaMemcpyHostToDevice, ctx->stream));
 	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
 	return RSD_OK;
 }
+
+int upload_bc_values(rsd_ctx* ctx, rsd_heat* h) { return bc_values_to(ctx, h, h->time, h->g); }
 
 static bool bc_time_dependent(const rsd_heat* h) {
 	for (int t = 0; t < 6; ++t) if (h->essential[t] && uses_time(h->bcExpr[t])) return true;
@@ -47,14 +49,20 @@ __global__ void k_be_rate(int64_t n, double inv_dt, const double* __restrict__ U
 	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
 		Ud[i] = inv_dt * U[i] + (-inv_dt) * Up[i];
 }
-__global__ void k_residual_combine(int64_t n, const double* __restrict__ F, double* __restrict__ R) {
-	// axpby(1, -1, F, R): R = -R + F
-	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-		R[i] = -1.0 * R[i] + 1.0 * F[i];
+// |F - R| with the deterministic grid reduction: axpby(1, -1, F, R) then norm(R)
+// (BackwardEulerStage.hpp:120-122), without storing F - R
+__global__ void k_diff_norm(int64_t n, const double* __restrict__ F, const double* __restrict__ R, double* partials,
+                            unsigned* ticket, double* out) {
+	double v[1] = {0.0};
+	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+		const double d = -1.0 * R[i] + 1.0 * F[i];
+		v[0] += d * d;
+	}
+	if (grid_sum<1>(v, partials, ticket)) *out = sqrt(v[0]);
 }
 
 static void free_heat(rsd_heat* h) {
-	cudaFree(h->t2a); cudaFree(h->g); cudaFree(h->kElem); cudaFree(h->tables);
+	cudaFree(h->t2a); cudaFree(h->g); cudaFree(h->kElem); cudaFree(h->tables); cudaFree(h->bElems); cudaFree(h->gPrev);
 	cudaFree(h->F); cudaFree(h->R); cudaFree(h->Udot); cudaFree(h->ms); cudaFree(h->dU);
 	if (h->K) rsd_csr_destroy(h->K);
 	delete h;
@@ -100,6 +108,21 @@ int rsd_heat_create(rsd_ctx* ctx, const rsd_mesh* m, const rsd_heat_desc* d, rsd
 			free_heat(h);
 			return cuda_error(e, "element conductivity upload");
 		}
+	}
+	{
+		// elements touching a constrained node: the only ones the Dirichlet lift can change
+		std::vector<int32_t> be;
+		for (int64_t el = 0; el < m->nelem; ++el)
+			for (int a = 0; a < m->npe; ++a)
+				if (h->h_t2a[m->h_ien[el * m->npe + a]] < 0) { be.push_back((int32_t)el); break; }
+		h->nbElems = (int64_t)be.size();
+		if (h->nbElems &&
+		    ((e = cudaMalloc(&h->bElems, sizeof(int32_t) * be.size())) != cudaSuccess ||
+		     (e = cudaMemcpyAsync(h->bElems, be.data(), sizeof(int32_t) * be.size(), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)) {
+			free_heat(h);
+			return cuda_error(e, "boundary element list");
+		}
+		if ((e = cudaMalloc(&h->gPrev, sizeof(double) * nn)) != cudaSuccess) { free_heat(h); return cuda_error(e, "allocation"); }
 	}
 	if ((rc = build_tables(h)) || (rc = upload_bc_values(ctx, h)) || (rc = build_pattern(ctx, h, &h->K))) { free_heat(h); return rc; }
 	*out = h;
@@ -198,26 +221,26 @@ int rsd_heat_be_step(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver_cfg*
 	const int gv = vec_grid(ctx, n);
 	h->dt = dt;
 	RSD_CHECK(set_time(ctx, h, t));
+	// Dirichlet values at t - dt for the mass right-hand side (gathered Full at currentTime_ - dt_)
+	h->gPrevValid = bc_time_dependent(h);
+	if (h->gPrevValid) RSD_CHECK(bc_values_to(ctx, h, t - dt, h->gPrev));
 	k_be_rate<<<gv, 256, 0, ctx->stream>>>(n, inv, U, Uprev, h->Udot);
 	RSD_CHECK(assemble_matrix(ctx, h, 1.0, inv, 0.0, 0.0, U, h->Udot, h->K));                 // K + M/dt
-	RSD_CHECK(assemble_vector(ctx, h, 0, 0.0, U, h->Udot, nullptr, h->F, 1.0, false));      // load
-	RSD_CHECK(set_time(ctx, h, t - dt));
-	RSD_CHECK(assemble_vector(ctx, h, 2, 0.0, Uprev, nullptr, nullptr, h->F, inv, true));   // F += (1/dt) M Uprev
-	RSD_CHECK(set_time(ctx, h, t));
+	RSD_CHECK(assemble_vector(ctx, h, 7, inv, Uprev, nullptr, nullptr, h->F, 1.0, false));  // load + (1/dt) M Uprev
 	RSD_CHECK(assemble_lift(ctx, h, 1.0, inv, h->F));                                      // F -= (K + M/dt) G
 	RSD_CHECK(solve(ctx, h->K, cfg, h->F, U, rep));
 	if (residual_norm) {
-		// BackwardEulerStage::residualNorm (:113-124) with the Udot of this step's assemble()
-		RSD_CHECK(assemble_vector(ctx, h, 1, 0.0, U, h->Udot, nullptr, h->R, 1.0, false));
-		RSD_CHECK(assemble_vector(ctx, h, 3, 0.0, U, h->Udot, nullptr, h->R, 1.0, true));
-		k_residual_combine<<<gv, 256, 0, ctx->stream>>>(n, h->F, h->R);
+		// BackwardEulerStage::residualNorm (:113-124) with the Udot of this step's assemble():
+		// K U (Full) + M Udot in one element pass, then |F - R|
+		RSD_CHECK(assemble_vector(ctx, h, 8, 0.0, U, h->Udot, nullptr, h->R, 1.0, false));
+		double* dres = &ctx->s.scal[3].spare1;
+		k_diff_norm<<<red_grid(ctx, n), kReduceThreads, 0, ctx->stream>>>(n, h->F, h->R, ctx->s.partials, &ctx->s.scal[3].ticket, dres);
 		RSD_CUDA(cudaGetLastError());
-		double rr = 0.0;
-		RSD_CHECK(dot_device(ctx, n, h->R, h->R, &rr));
-		*residual_norm = std::sqrt(rr);
+		RSD_CUDA(cudaMemcpyAsync(ctx->s.hbuf + 8, dres, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
 	}
 	RSD_CUDA(cudaMemcpyAsync(Uprev, U, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));   // advance()
 	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+	if (residual_norm) *residual_norm = ctx->s.hbuf[8];
 	return RSD_OK;
 }
 
@@ -226,14 +249,11 @@ int rsd_heat_newton(rsd_ctx* ctx, rsd_heat* h, double abs_tol, double rel_tol, i
                     const rsd_solver_cfg* lin, double* U, rsd_report* rep) {
 	if (!ctx || !h || !lin || !U) return set_error(RSD_EINVAL, "bad argument");
 	const int64_t n = h->n;
-	const int gv = vec_grid(ctx, n);
 	rsd_report R{};
 	double res0 = 0.0;
 	for (int64_t it = 0; it < max_iters; ++it) {
-		RSD_CHECK(assemble_vector(ctx, h, 0, 0.0, U, nullptr, nullptr, h->F, 1.0, false));   // assembleLoad
-		RSD_CHECK(assemble_vector(ctx, h, 1, 0.0, U, nullptr, nullptr, h->R, 1.0, false));   // K(T) T, Full gather
-		k_residual_combine<<<gv, 256, 0, ctx->stream>>>(n, h->F, h->R);                       // R = F - K(T) T
-		RSD_CUDA(cudaGetLastError());
+		// assembleLoad and assembleResidual (K(T) T, Full gather) in one element pass: R = F - K(T) T
+		RSD_CHECK(assemble_vector(ctx, h, 9, 0.0, U, nullptr, nullptr, h->R, 1.0, false));
 		double rr = 0.0;
 		RSD_CHECK(dot_device(ctx, n, h->R, h->R, &rr));
 		const double res = std::sqrt(rr);

@@ -159,6 +159,10 @@ struct rsd_heat {
 	int nq = 0;                     // total quadrature points
 	double time = 0.0;
 	rsd_csr* K = nullptr;           // matrix with the problem's pattern
+	int32_t* bElems = nullptr;      // device: elements with at least one constrained node (lift)
+	int64_t nbElems = 0;
+	double* gPrev = nullptr;        // device: Dirichlet values at the previous time (time-dependent BCs)
+	bool gPrevValid = false;
 	// stage scratch
 	double *F = nullptr, *R = nullptr, *Udot = nullptr, *ms = nullptr, *dU = nullptr;
 	double dt = 0.0;
