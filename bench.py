@@ -311,7 +311,7 @@ def main():
             dist.destroy_process_group()
         return
     ms_mx, reps_mx, prof_mx, clk = run(cfgs["mixed"], args.steps, args.warmup, profile=True, clocks=clocks)
-    ms_64, reps_64, prof_64, _ = run(cfgs["fp64"], args.steps, args.warmup, profile=True)
+    ms_64, reps_64, prof_64, clk64 = run(cfgs["fp64"], args.steps, args.warmup, profile=True, clocks=ClockSampler(local))
 
     # end to end through the public API with host buffers: H2D of the step's state from pinned
     # host memory, the step, D2H of the new state, every step
@@ -398,6 +398,8 @@ def main():
                      "fp64_spmv": {"achieved": achieved64, "frac": achieved64 / peak if achieved64 else None,
                                    "algorithmic_bytes": bytes_spmv64, "avg_launch_us": 1e3 * t64 / max(l64, 1)}},
         "kernel_ms_per_step": {k: v[1] / args.steps for k, v in prof_mx.items()},
+        "kernel_ms_per_step_fp64": {k: v[1] / args.steps for k, v in prof_64.items()},
+        "clocks_fp64": clk64,
         "cpu_baseline": cpu,
         "e2e": {"value": ms_e2e, "unit": "ms", "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 8 * n},
         "gpu_launches": gpu_launches,

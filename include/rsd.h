@@ -110,9 +110,10 @@ int rsd_csr_create(rsd_ctx* ctx, int64_t nrows, int64_t nnz, const int64_t* row_
                    const double* values, rsd_csr** out);
 int rsd_csr_destroy(rsd_csr* A);
 int rsd_csr_info(const rsd_csr* A, int64_t* nrows, int64_t* nnz);
-int rsd_csr_values(rsd_csr* A, double** dvalues);
+/* device pointer to the CSR-order values (writes through it are allowed until the next call on A) */
+int rsd_csr_values(rsd_ctx* ctx, rsd_csr* A, double** dvalues);
 int rsd_csr_set_values(rsd_ctx* ctx, rsd_csr* A, const double* host_values);
-int rsd_csr_get_values(rsd_ctx* ctx, const rsd_csr* A, double* host_values);
+int rsd_csr_get_values(rsd_ctx* ctx, rsd_csr* A, double* host_values);
 int rsd_csr_get_pattern(rsd_ctx* ctx, const rsd_csr* A, int64_t* host_row_ptr, int64_t* host_col_idx);
 /* operations::matvec (linalg/operations/backend/cpu/MatrixOps.tpp:5-23), device vectors */
 int rsd_spmv(rsd_ctx* ctx, const rsd_csr* A, const double* x, double* y);
@@ -124,7 +125,10 @@ int rsd_csr_diagonal(rsd_ctx* ctx, const rsd_csr* A, double* d);
 int rsd_csr_lump(rsd_ctx* ctx, const rsd_csr* A, double* d);
 /* Jacobi::update (linalg/solver/preconditioner/Jacobi.hpp:23-36): invD = |d|>1e-300 ? 1/d : 1 */
 int rsd_jacobi_setup(rsd_ctx* ctx, const rsd_csr* A, double* inv_diag);
-/* SpMV launch shape: lanes per row (2..32, power of two) and threads per block; 0 picks defaults */
+/* Execution layout and launch shape of SpMV and the Krylov kernels: lanes_per_row 0 selects the
+ * SELL-32 layout (one thread per row, slices of 32 rows stored column-major; the default),
+ * 1..32 (power of two) CSR with that many lanes per row; block_threads 64..512 (power of two),
+ * 0 for the default.  The autotuner times every choice and keeps the fastest. */
 int rsd_csr_set_launch(rsd_csr* A, int32_t lanes_per_row, int32_t block_threads);
 int rsd_csr_autotune(rsd_ctx* ctx, rsd_csr* A, int32_t* lanes_per_row, int32_t* block_threads, double* best_us);
 

@@ -83,7 +83,7 @@ SIGNATURES = {
     "rsd_csr_create": [_P, _I64, _I64, _P, _P, _P, C.POINTER(_P)],
     "rsd_csr_destroy": [_P],
     "rsd_csr_info": [_P, C.POINTER(_I64), C.POINTER(_I64)],
-    "rsd_csr_values": [_P, C.POINTER(_P)],
+    "rsd_csr_values": [_P, _P, C.POINTER(_P)],
     "rsd_csr_set_values": [_P, _P, _P],
     "rsd_csr_get_values": [_P, _P, _P],
     "rsd_csr_get_pattern": [_P, _P, _P, _P],

@@ -3,14 +3,18 @@
 // Dirichlet lifting), diagonal and the adjoint's element gradient.
 //
 // Layout: a group of G lanes (G = next power of two >= nodes per element, at most 32) owns one
-// element; lane a owns local node a.  Quadrature tables (N, dN/dxi per point and node, weights)
-// live in shared memory.  Per quadrature point the Jacobian and any interpolated field are summed
-// over the group with xor shuffles (every lane gets the total), and row a of the element matrix is
-// formed against the tables, which all lanes of a warp read at the same address (broadcast):
-//     (dN_a/dx . dN_b/dx) = sum_al G_a[al] dN_b/dxi_al,   G_a = invJ^T dN_a/dx,
-// so no per-point exchange of physical gradients between lanes is needed.  Each lane then adds its
-// row into the CSR values with FP64 atomics (colour-free scatter) after a binary search of the
-// column in its row (the rows are sorted; Assembler.tpp:8-76).
+// element, several elements per warp.  Each element goes through three phases:
+//   1. lane a stages node a (coordinates and the gathered fields) in shared memory;
+//   2. lane q evaluates quadrature point q (q = lane, lane + G, ...): Jacobian, inverse layout,
+//      measure, interpolated state and fields, the conductivity model and the source, written
+//      once as a per-point record (no point is evaluated twice and no shuffle is needed);
+//   3. lane a forms its row of the element matrix (or its vector entry) from the records, which
+//      the lanes of a group read at one address (broadcast), and from the shape-function tables:
+//          dN_a/dx . dN_b/dx = sum_al G_a[al] dN_b/dxi_al,   G_a = invJ^T dN_a/dx,
+//      where dN_b/dxi at a point is the same table entry for every lane of the warp.
+// Matrix rows are added with FP64 atomics (colour-free scatter) straight into the SELL-32 execution
+// layout of the values, at positions from a precomputed element -> slot map, or, without the map,
+// after a binary search of the column in the sorted CSR row (fem/assembly/backend/cpu/Assembler.tpp:8-76).
 //
 // Geometry follows JacobianTransform (fem/geometry/JacobianTransform.tpp): measure = sqrt(det(J^T J)),
 // 2D gradient transform with the true inverse, 3D with the cofactor/det layout (:160-185).
@@ -19,6 +23,11 @@
 #include "rsd_kernels.cuh"
 
 namespace rsd {
+
+// SELL-32 slot of CSR position q of row `row`
+__device__ __forceinline__ int32_t sell_slot(const int32_t* sStart, const int32_t* rp, int32_t row, int32_t q) {
+	return sStart[row >> 5] + 32 * (q - rp[row]) + (row & 31);
+}
 
 struct AsmParams {
 	int64_t nelem;
@@ -37,10 +46,13 @@ struct AsmParams {
 	const double* __restrict__ tables;  // [nq][G][4] (N, dxi, deta, dzeta) then w[nq]
 	double kConst, rho, cp, time;
 	DevExpr kExpr, dkExpr, srcExpr;
-	// matrix
+	// matrix: CSR pattern for the column search, SELL-32 slice starts and values for the scatter
 	const int32_t* __restrict__ rp;
 	const int32_t* __restrict__ col;
+	const int32_t* __restrict__ sStart;
 	double* __restrict__ val;
+	const int32_t* __restrict__ slots;  // element -> SELL slot map [e][a][b] (row stride slotStride), or null
+	int32_t slotStride;
 	double cDiff, cMass, cTDiff, cTMass;
 	// vectors
 	const double* __restrict__ U;
@@ -59,29 +71,89 @@ struct Elem {
 };
 
 constexpr int kAsmThreads = 128;
+constexpr int kAsmWarps = kAsmThreads / 32;
 
-// geometry at one quadrature point: J summed over the group, then inverse layout and measure
-template <int NSD, int G>
-__device__ __forceinline__ void qp_geometry(const double (&xa)[3], const double (&dxi)[3], double (&inv)[9], double& measure) {
+// per-point record: inverse layout (9), w*measure, k, dk, grad T (3), V, grad V (3), W, f, spare
+constexpr int R_INV = 0, R_WM = 9, R_K = 10, R_DK = 11, R_GT = 12, R_V = 15, R_GV = 16, R_W = 19, R_F = 20, REC = 22;
+// per-node staging: x (3), U, V, W
+constexpr int N_X = 0, N_U = 3, N_V = 4, N_W = 5, NREC = 6;
+
+__host__ __device__ inline int table_stride(int G) { return G * 4 + 1; }                      // odd: no bank conflicts across q
+__host__ __device__ inline int node_area(int npe) { return npe * NREC + 1; }
+__host__ __device__ inline int point_area(int nq) { return nq * REC + 1; }
+
+size_t asm_smem_bytes(int npe, int nq) {
+	const int G = npe <= 4 ? 4 : npe <= 8 ? 8 : npe <= 16 ? 16 : 32;
+	const int EPW = 32 / G;
+	return sizeof(double) * ((size_t)nq * table_stride(G) + nq + (size_t)kAsmWarps * EPW * (node_area(npe) + point_area(nq)));
+}
+
+// what phase 2 must evaluate
+struct Needs {
+	bool state;    // T, grad T (k(T), tangents)
+	bool field;    // V, grad V
+	bool field2;   // W (second operand, mass only)
+	bool load;     // x_q and f(t, x_q)
+};
+
+template <int NSD, int P>
+__device__ __forceinline__ void stage_tables(const AsmParams& prm, double* sm) {
+	using E = Elem<NSD, P>;
+	const int TS = table_stride(E::G);
+	for (int i = threadIdx.x; i < prm.nq * E::G * 4; i += blockDim.x) {
+		const int q = i / (E::G * 4), r = i % (E::G * 4);
+		sm[q * TS + r] = prm.tables[i];
+	}
+	for (int i = threadIdx.x; i < prm.nq; i += blockDim.x) sm[prm.nq * TS + i] = prm.tables[prm.nq * E::G * 4 + i];
+	__syncthreads();
+}
+
+// phase 2: one quadrature point, all inputs from the staged node data
+template <int NSD, int P>
+__device__ __forceinline__ void eval_point(const AsmParams& prm, const Needs& nd, const double* tq, double w,
+                                           const double* nodes, double ke, double* rec) {
+	using E = Elem<NSD, P>;
+	constexpr int NPE = E::NPE;
 	double J[9];
 #pragma unroll
-	for (int i = 0; i < NSD; ++i)
+	for (int i = 0; i < NSD * NSD; ++i) J[i] = 0.0;
+	double Tq = 0.0, Vq = 0.0, Wq = 0.0, xq[3] = {0.0, 0.0, 0.0}, dT[3] = {0.0, 0.0, 0.0}, dV[3] = {0.0, 0.0, 0.0};
+#pragma unroll 4
+	for (int b = 0; b < NPE; ++b) {
+		const double* t = tq + b * 4;
+		const double* nb = nodes + b * NREC;
 #pragma unroll
-		for (int al = 0; al < NSD; ++al) J[i * NSD + al] = group_sum<G>(dxi[al] * xa[i]);
+		for (int i = 0; i < NSD; ++i)
+#pragma unroll
+			for (int al = 0; al < NSD; ++al) J[i * NSD + al] += t[1 + al] * nb[N_X + i];
+		if (nd.state) {
+			Tq += t[0] * nb[N_U];
+#pragma unroll
+			for (int al = 0; al < NSD; ++al) dT[al] += t[1 + al] * nb[N_U];
+		}
+		if (nd.field) {
+			Vq += t[0] * nb[N_V];
+#pragma unroll
+			for (int al = 0; al < NSD; ++al) dV[al] += t[1 + al] * nb[N_V];
+		}
+		if (nd.field2) Wq += t[0] * nb[N_W];
+		if (nd.load)
+#pragma unroll
+			for (int i = 0; i < NSD; ++i) xq[i] += t[0] * nb[N_X + i];
+	}
+	double inv[9], detg;
 	if (NSD == 2) {
 		const double g0 = J[0] * J[0] + J[2] * J[2], g1 = J[0] * J[1] + J[2] * J[3], g3 = J[1] * J[1] + J[3] * J[3];
-		const double detg = g0 * g3 - g1 * g1;
-		const double detJ = J[0] * J[3] - J[1] * J[2];
-		const double di = 1.0 / detJ;
+		detg = g0 * g3 - g1 * g1;
+		const double di = 1.0 / (J[0] * J[3] - J[1] * J[2]);
 		inv[0] = di * J[3]; inv[1] = -di * J[1]; inv[2] = -di * J[2]; inv[3] = di * J[0];
-		measure = sqrt(detg);
 	} else {
 		double gm[9];
 #pragma unroll
 		for (int b = 0; b < 3; ++b)
 #pragma unroll
 			for (int a = 0; a < 3; ++a) gm[b * 3 + a] = J[a] * J[b] + J[3 + a] * J[3 + b] + J[6 + a] * J[6 + b];
-		const double detg = gm[0] * (gm[4] * gm[8] - gm[5] * gm[7]) - gm[1] * (gm[3] * gm[8] - gm[5] * gm[6]) + gm[2] * (gm[3] * gm[7] - gm[4] * gm[6]);
+		detg = gm[0] * (gm[4] * gm[8] - gm[5] * gm[7]) - gm[1] * (gm[3] * gm[8] - gm[5] * gm[6]) + gm[2] * (gm[3] * gm[7] - gm[4] * gm[6]);
 		const double detJ = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) + J[2] * (J[3] * J[7] - J[4] * J[6]);
 		const double di = 1.0 / detJ;
 		inv[0] = di * (J[4] * J[8] - J[5] * J[7]);
@@ -93,119 +165,153 @@ __device__ __forceinline__ void qp_geometry(const double (&xa)[3], const double 
 		inv[6] = di * (J[1] * J[5] - J[2] * J[4]);
 		inv[7] = -di * (J[0] * J[5] - J[2] * J[3]);
 		inv[8] = di * (J[0] * J[4] - J[1] * J[3]);
-		measure = sqrt(detg);
 	}
+#pragma unroll
+	for (int i = 0; i < NSD * NSD; ++i) rec[R_INV + i] = inv[i];
+	rec[R_WM] = sqrt(detg) * w;
+	// physical gradients of the interpolated fields: grad_i = sum_al inv[i][al] d/dxi_al
+	if (nd.state) {
+#pragma unroll
+		for (int i = 0; i < NSD; ++i) {
+			double s = 0.0;
+#pragma unroll
+			for (int al = 0; al < NSD; ++al) s += inv[i * NSD + al] * dT[al];
+			rec[R_GT + i] = s;
+		}
+	}
+	if (nd.field) {
+		rec[R_V] = Vq;
+#pragma unroll
+		for (int i = 0; i < NSD; ++i) {
+			double s = 0.0;
+#pragma unroll
+			for (int al = 0; al < NSD; ++al) s += inv[i * NSD + al] * dV[al];
+			rec[R_GV + i] = s;
+		}
+	}
+	if (nd.field2) rec[R_W] = Wq;
+	// models: k(T) and dk/dT (ConductivityModel.hpp:60-96), the per-element factor applies to diffusion
+	const double k = prm.kExpr.n ? eval_expr(prm.kExpr, 0.0, 0.0, 0.0, 0.0, nd.state ? Tq : 0.0) : prm.kConst;
+	rec[R_K] = ke * k;
+	rec[R_DK] = prm.dkExpr.n ? eval_expr(prm.dkExpr, 0.0, 0.0, 0.0, 0.0, nd.state ? Tq : 0.0) : 0.0;
+	if (nd.load) rec[R_F] = prm.srcExpr.n ? eval_expr(prm.srcExpr, prm.time, xq[0], xq[1], NSD == 3 ? xq[2] : 0.0, 0.0) : 0.0;
 }
 
+// lane a's physical gradient at a point: dx_i = sum_al inv[i][al] dN_a/dxi_al
 template <int NSD>
-__device__ __forceinline__ void phys_grad(const double (&inv)[9], const double (&dxi)[3], double (&dx)[3]) {
+__device__ __forceinline__ void node_grad(const double* rec, const double* ta, double (&dx)[3]) {
 #pragma unroll
 	for (int i = 0; i < NSD; ++i) {
 		double s = 0.0;
 #pragma unroll
-		for (int al = 0; al < NSD; ++al) s += inv[i * NSD + al] * dxi[al];
+		for (int al = 0; al < NSD; ++al) s += rec[R_INV + i * NSD + al] * ta[1 + al];
 		dx[i] = s;
 	}
 }
 
-// element data for the lane: node, row, coordinates; returns false when the lane has no node
-template <int NSD, int P>
-__device__ __forceinline__ bool load_node(const AsmParams& prm, bool valid, int64_t e, int a, int32_t& node, int32_t& row, double (&xa)[3]) {
-	using E = Elem<NSD, P>;
-	xa[0] = xa[1] = xa[2] = 0.0;
-	node = 0; row = -1;
-	if (!valid || a >= E::NPE) return false;
-	node = prm.ien[e * E::NPE + a];
-	row = prm.t2a[node];
-#pragma unroll
-	for (int i = 0; i < NSD; ++i) xa[i] = prm.xyz[(int64_t)node * NSD + i];
-	return true;
-}
+// the warp-uniform element loop shared by every kernel: EPW elements per warp per trip
+#define RSD_ELEMENT_LOOP_BEGIN                                                                   \
+	using E = Elem<NSD, P>;                                                                      \
+	constexpr int NPE = E::NPE, G = E::G, EPW = E::EPW;                                           \
+	extern __shared__ double sm[];                                                               \
+	stage_tables<NSD, P>(prm, sm);                                                               \
+	const int TS = table_stride(G);                                                              \
+	const double* tab = sm;                                                                      \
+	const double* wq = sm + prm.nq * TS;                                                         \
+	const int lane = threadIdx.x & 31, a = lane % G, slot = lane / G, warp = threadIdx.x >> 5;   \
+	double* wbase = sm + prm.nq * TS + prm.nq + (size_t)warp * EPW * (node_area(NPE) + point_area(prm.nq)); \
+	double* nodes = wbase + slot * (node_area(NPE) + point_area(prm.nq));                        \
+	double* recs = nodes + node_area(NPE);                                                       \
+	const int64_t warpId = (int64_t)blockIdx.x * kAsmWarps + warp;                               \
+	const int64_t warpStride = (int64_t)gridDim.x * kAsmWarps;                                   \
+	for (int64_t eb = warpId * EPW; eb < prm.nelem; eb += warpStride * EPW) {                    \
+		const int64_t idx = eb + slot;                                                           \
+		const bool inRange = idx < prm.nelem;                                                    \
+		const int64_t e = inRange ? (prm.elist ? (int64_t)prm.elist[idx] : idx) : 0;             \
+		const bool has = inRange && a < NPE;                                                     \
+		int32_t node = 0, row = -1;                                                              \
+		if (has) {                                                                               \
+			node = prm.ien[e * NPE + a];                                                         \
+			row = prm.t2a[node];                                                                 \
+		}                                                                                        \
+		const double ke = (prm.kElem && inRange) ? prm.kElem[e] : 1.0;
 
-template <int NSD, int P>
-__device__ __forceinline__ void load_tables(const AsmParams& prm, double* sm) {
-	using E = Elem<NSD, P>;
-	const int total = prm.nq * E::G * 4 + prm.nq;
-	for (int i = threadIdx.x; i < total; i += blockDim.x) sm[i] = prm.tables[i];
-	__syncthreads();
-}
+#define RSD_STAGE_NODE(Uv, Vv, Wv)                                                               \
+		if (has) {                                                                               \
+			double* nb = nodes + a * NREC;                                                       \
+			_Pragma("unroll") for (int i = 0; i < NSD; ++i) nb[N_X + i] = prm.xyz[(int64_t)node * NSD + i]; \
+			nb[N_U] = (Uv); nb[N_V] = (Vv); nb[N_W] = (Wv);                                      \
+		}                                                                                        \
+		__syncwarp();                                                                            \
+		if (inRange)                                                                             \
+			for (int q = a; q < prm.nq; q += G)                                                  \
+				eval_point<NSD, P>(prm, nd, tab + q * TS, wq[q], nodes, ke, recs + q * REC);     \
+		__syncwarp();
+
+#define RSD_ELEMENT_LOOP_END                                                                     \
+		__syncwarp();                                                                            \
+	}
 
 // ---------------------------------------------------------------------------------------------
-// Assembler::assembleMatrix (fem/assembly/backend/cpu/Assembler.tpp:86-140)
+// Assembler::assembleMatrix (fem/assembly/backend/cpu/Assembler.tpp:86-140):
+// c_diff*Diffusion + c_mass*Mass + c_tdiff*TangentDiffusion (+ TangentMass, zero for constant cp)
 // ---------------------------------------------------------------------------------------------
 template <int NSD, int P>
 __global__ void __launch_bounds__(kAsmThreads) k_asm_matrix(const AsmParams prm) {
-	using E = Elem<NSD, P>;
-	constexpr int NPE = E::NPE, G = E::G, EPW = E::EPW;
-	extern __shared__ double sm[];
-	load_tables<NSD, P>(prm, sm);
-	const double* tab = sm;
-	const double* wq = sm + prm.nq * G * 4;
-	const int lane = threadIdx.x & 31, a = lane % G, slot = lane / G;
-	const int warpsPerBlock = blockDim.x >> 5;
-	const int64_t warpId = (int64_t)blockIdx.x * warpsPerBlock + (threadIdx.x >> 5);
-	const int64_t warpStride = (int64_t)gridDim.x * warpsPerBlock;
-	const bool needState = prm.kExpr.n || prm.dkExpr.n || prm.cTDiff != 0.0 || prm.cTMass != 0.0;
-	for (int64_t eb = warpId * EPW; eb < prm.nelem; eb += warpStride * EPW) {
-		const int64_t e = eb + slot;
-		int32_t node, row;
-		double xa[3];
-		const bool has = load_node<NSD, P>(prm, e < prm.nelem, e, a, node, row, xa);
-		double Ua = 0.0;
-		if (has && needState) Ua = row >= 0 ? (prm.U ? prm.U[row] : 0.0) : prm.g[node];
-		const double ke = (prm.kElem && e < prm.nelem) ? prm.kElem[e] : 1.0;
-		double Ke[NPE];
+	Needs nd{};
+	nd.state = prm.kExpr.n || prm.dkExpr.n || prm.cTDiff != 0.0;
+	RSD_ELEMENT_LOOP_BEGIN
+	const double Ua = (has && nd.state) ? (row >= 0 ? (prm.U ? prm.U[row] : 0.0) : prm.g[node]) : 0.0;
+	RSD_STAGE_NODE(Ua, 0.0, 0.0)
+	double Ke[NPE];
 #pragma unroll
-		for (int b = 0; b < NPE; ++b) Ke[b] = 0.0;
+	for (int b = 0; b < NPE; ++b) Ke[b] = 0.0;
+	if (has) {
 		for (int q = 0; q < prm.nq; ++q) {
-			const double* tq = tab + (q * G) * 4;
-			double Na = 0.0, dxi[3] = {0.0, 0.0, 0.0};
-			if (a < NPE) {
-				Na = tq[a * 4];
-#pragma unroll
-				for (int al = 0; al < NSD; ++al) dxi[al] = tq[a * 4 + 1 + al];
-			}
-			double inv[9], measure;
-			qp_geometry<NSD, G>(xa, dxi, inv, measure);
+			const double* rec = recs + q * REC;
+			const double* tq = tab + q * TS;
+			const double* ta = tq + a * 4;
 			double dx[3];
-			phys_grad<NSD>(inv, dxi, dx);
-			double k = prm.kConst, dk = 0.0, gradT[3] = {0.0, 0.0, 0.0};
-			if (needState) {
-				const double T = group_sum<G>(Na * Ua);
-#pragma unroll
-				for (int i = 0; i < NSD; ++i) gradT[i] = group_sum<G>(dx[i] * Ua);
-				if (prm.kExpr.n) k = eval_expr(prm.kExpr, 0.0, 0.0, 0.0, 0.0, T);
-				if (prm.dkExpr.n) dk = eval_expr(prm.dkExpr, 0.0, 0.0, 0.0, 0.0, T);
-			}
-			const double wm = measure * wq[q];
-			// G_a = invJ^T dx  ->  dN_a/dx . dN_b/dx = G_a . dN_b/dxi
+			node_grad<NSD>(rec, ta, dx);
 			double Ga[3];
 #pragma unroll
 			for (int al = 0; al < NSD; ++al) {
 				double s = 0.0;
 #pragma unroll
-				for (int i = 0; i < NSD; ++i) s += inv[i * NSD + al] * dx[i];
+				for (int i = 0; i < NSD; ++i) s += rec[R_INV + i * NSD + al] * dx[i];
 				Ga[al] = s;
 			}
-			const double cd = prm.cDiff * ke * k * wm;
-			const double cm = prm.cMass * prm.rho * prm.cp * Na * wm;
-			double ct = 0.0;
+			const double wm = rec[R_WM];
+			const double cd = prm.cDiff * rec[R_K] * wm;
+			double cm = prm.cMass * prm.rho * prm.cp * ta[0] * wm;
 			if (prm.cTDiff != 0.0) {
 				double s = 0.0;
 #pragma unroll
-				for (int i = 0; i < NSD; ++i) s += dx[i] * dk * gradT[i];
-				ct = prm.cTDiff * s * wm;
+				for (int i = 0; i < NSD; ++i) s += dx[i] * rec[R_DK] * rec[R_GT + i];
+				cm += prm.cTDiff * s * wm;
 			}
 #pragma unroll
 			for (int b = 0; b < NPE; ++b) {
-				const double* tb = tq + b * 4;   // same address across the warp: broadcast
+				const double* tb = tq + b * 4;   // one address for the whole warp: broadcast
 				double gd = 0.0;
 #pragma unroll
 				for (int al = 0; al < NSD; ++al) gd += Ga[al] * tb[1 + al];
-				Ke[b] += cd * gd + (cm + ct) * tb[0];
+				Ke[b] += cd * gd + cm * tb[0];
 			}
 		}
-		// scatter row a (free rows only) into the CSR values
+	}
+	// scatter row a (free rows only) into the SELL-32 values
+	if (prm.slots) {
+		// precomputed positions: one contiguous run of NPE slots per lane, -1 for constrained pairs
+		const int32_t* sl = prm.slots + ((int64_t)e * NPE + a) * prm.slotStride;
+#pragma unroll
+		for (int b = 0; b < NPE; ++b) {
+			if (has && row >= 0) {
+				const int32_t s = __ldcs(sl + b);
+				if (s >= 0) atomicAdd(prm.val + s, Ke[b]);
+			}
+		}
+	} else {
 		const int base = lane - a;
 #pragma unroll
 		for (int b = 0; b < NPE; ++b) {
@@ -215,175 +321,148 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_matrix(const AsmParams prm)
 				int lo = prm.rp[row], hi = end;
 				while (lo < hi) {
 					const int mid = (lo + hi) >> 1;
-					const int32_t cm2 = prm.col[mid];
-					if (cm2 < cb) lo = mid + 1; else hi = mid;
+					if (prm.col[mid] < cb) lo = mid + 1; else hi = mid;
 				}
-				if (lo < end && prm.col[lo] == cb) atomicAdd(prm.val + lo, Ke[b]);
+				if (lo < end && prm.col[lo] == cb) atomicAdd(prm.val + sell_slot(prm.sStart, prm.rp, row, lo), Ke[b]);
 			}
 		}
+	}
+	RSD_ELEMENT_LOOP_END
+}
+
+// element -> SELL-32 slot map, built once per pattern: slot[e][a][b] = slot of column t2a[node_b]
+// in row t2a[node_a], -1 when either DOF is constrained
+template <int NSD, int P>
+__global__ void k_build_slots(int64_t nelem, const int32_t* __restrict__ ien, const int32_t* __restrict__ t2a,
+                              const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
+                              const int32_t* __restrict__ sStart, int32_t* __restrict__ slots, int32_t stride) {
+	using E = Elem<NSD, P>;
+	constexpr int NPE = E::NPE;
+	const int64_t total = nelem * NPE;
+	for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+		const int64_t e = t / NPE;
+		const int a = (int)(t % NPE);
+		const int32_t row = t2a[ien[e * NPE + a]];
+		int32_t* out = slots + t * stride;
+		for (int b = 0; b < NPE; ++b) {
+			const int32_t cb = t2a[ien[e * NPE + b]];
+			int32_t s = -1;
+			if (row >= 0 && cb >= 0) {
+				const int end = rp[row + 1];
+				int lo = rp[row], hi = end;
+				while (lo < hi) {
+					const int mid = (lo + hi) >> 1;
+					if (col[mid] < cb) lo = mid + 1; else hi = mid;
+				}
+				if (lo < end && col[lo] == cb) s = sell_slot(sStart, rp, row, lo);
+			}
+			out[b] = s;
+		}
+		for (int b = NPE; b < stride; ++b) out[b] = -1;
 	}
 }
 
 // ---------------------------------------------------------------------------------------------
 // Assembler::assembleVector (Assembler.tpp:199-255), BoundaryApplicator::applyEssentialBCs
-// (fem/boundary/backend/cpu/BoundaryApplicator.tpp:7-64) and the adjoint element gradient.
-// The vector forms use sum_b (dN_a/dx . dN_b/dx) V_b = dN_a/dx . grad V with grad V summed over
-// the group, and sum_b N_a N_b V_b = N_a V(x_q).
+// (fem/boundary/backend/cpu/BoundaryApplicator.tpp:7-64) and the adjoint element gradient:
+// sum_b (dN_a/dx . dN_b/dx) V_b = dN_a/dx . grad V and sum_b N_a N_b V_b = N_a V(x_q), with V and
+// grad V evaluated once per point in phase 2.
 // ---------------------------------------------------------------------------------------------
 template <int NSD, int P>
 __global__ void __launch_bounds__(kAsmThreads) k_asm_vector(const AsmParams prm) {
-	using E = Elem<NSD, P>;
-	constexpr int NPE = E::NPE, G = E::G, EPW = E::EPW;
-	extern __shared__ double sm[];
-	load_tables<NSD, P>(prm, sm);
-	const double* tab = sm;
-	const double* wq = sm + prm.nq * G * 4;
-	const int lane = threadIdx.x & 31, a = lane % G, slot = lane / G;
-	const int warpsPerBlock = blockDim.x >> 5;
-	const int64_t warpId = (int64_t)blockIdx.x * warpsPerBlock + (threadIdx.x >> 5);
-	const int64_t warpStride = (int64_t)gridDim.x * warpsPerBlock;
 	const int which = prm.which;
-	const bool kT = prm.kExpr.n != 0;
-	const bool hasLoad = which == 0 || which == 7 || which == 9;
-	const bool opState = kT && which == 4;   // the operator takes k(T) from the state U, not the operand
-	for (int64_t eb = warpId * EPW; eb < prm.nelem; eb += warpStride * EPW) {
-		const int64_t idx = eb + slot;
-		const bool inRange = idx < prm.nelem;
-		const int64_t e = inRange ? (prm.elist ? (int64_t)prm.elist[idx] : idx) : 0;
-		int32_t node, row;
-		double xa[3];
-		const bool has = load_node<NSD, P>(prm, inRange, e, a, node, row, xa);
-		// gathered operand V, second operand W (Udot) and state U (for k(T))
-		double Va = 0.0, Wa = 0.0, Ua = 0.0;
-		if (has) {
-			const double fullU = row >= 0 ? (prm.U ? prm.U[row] : 0.0) : prm.g[node];
-			switch (which) {
-				case 1: case 2: case 8: case 9: Va = fullU; break;                          // GatherMode::Full
-				case 3: Va = (row >= 0 && prm.Udot) ? prm.Udot[row] : 0.0; break;           // Free
-				case 4: Va = (row >= 0 && prm.V) ? prm.V[row] : 0.0; break;                 // Free
-				case 5: Va = row >= 0 ? 0.0 : prm.g[node]; break;                           // Constrained
-				case 6: Va = (row >= 0 && prm.V) ? prm.V[row] : 0.0; Ua = fullU; break;     // lambda (Free), T (Full)
-				case 7: Va = row >= 0 ? (prm.U ? prm.U[row] : 0.0) : (prm.gPrev ? prm.gPrev[node] : prm.g[node]); break;
-				default: break;
-			}
-			if (which == 8) Wa = (row >= 0 && prm.Udot) ? prm.Udot[row] : 0.0;
-			if (opState) Ua = fullU;
+	Needs nd{};
+	nd.load = which == 0 || which == 7 || which == 9;
+	nd.field = which != 0;
+	nd.field2 = which == 8;
+	// k(T): diffusion of U takes T from U itself (staged as V, mirrored into U), the operator from the state
+	nd.state = (prm.kExpr.n != 0 && (which == 1 || which == 4 || which == 8 || which == 9)) || which == 6;
+	RSD_ELEMENT_LOOP_BEGIN
+	double Va = 0.0, Wa = 0.0, Ua = 0.0;
+	if (has) {
+		const double fullU = row >= 0 ? (prm.U ? prm.U[row] : 0.0) : prm.g[node];
+		switch (which) {
+			case 1: case 2: case 8: case 9: Va = fullU; break;                          // GatherMode::Full
+			case 3: Va = (row >= 0 && prm.Udot) ? prm.Udot[row] : 0.0; break;           // Free
+			case 4: Va = (row >= 0 && prm.V) ? prm.V[row] : 0.0; break;                 // Free
+			case 5: Va = row >= 0 ? 0.0 : prm.g[node]; break;                           // Constrained
+			case 6: Va = (row >= 0 && prm.V) ? prm.V[row] : 0.0; break;                 // lambda (Free)
+			case 7: Va = row >= 0 ? (prm.U ? prm.U[row] : 0.0) : (prm.gPrev ? prm.gPrev[node] : prm.g[node]); break;
+			default: break;
 		}
-		const double ke = (prm.kElem && inRange) ? prm.kElem[e] : 1.0;
-		double Fa = 0.0, ge = 0.0;
+		if (which == 8) Wa = (row >= 0 && prm.Udot) ? prm.Udot[row] : 0.0;
+		Ua = (which == 4 || which == 6) ? fullU : Va;
+	}
+	RSD_STAGE_NODE(Ua, Va, Wa)
+	double Fa = 0.0, ge = 0.0;
+	if (has) {
 		for (int q = 0; q < prm.nq; ++q) {
-			const double* tq = tab + (q * G) * 4;
-			double Na = 0.0, dxi[3] = {0.0, 0.0, 0.0};
-			if (a < NPE) {
-				Na = tq[a * 4];
-#pragma unroll
-				for (int al = 0; al < NSD; ++al) dxi[al] = tq[a * 4 + 1 + al];
-			}
-			double inv[9], measure;
-			qp_geometry<NSD, G>(xa, dxi, inv, measure);
-			double dx[3];
-			phys_grad<NSD>(inv, dxi, dx);
-			const double wm = measure * wq[q];
-			if (hasLoad) {
-				double xq[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-				for (int i = 0; i < NSD; ++i) xq[i] = group_sum<G>(Na * xa[i]);
-				const double f = prm.srcExpr.n ? eval_expr(prm.srcExpr, prm.time, xq[0], xq[1], NSD == 3 ? xq[2] : 0.0, 0.0) : 0.0;
-				Fa += (f * Na) * wm;
-				if (which == 0) continue;
-			}
-			const double Vq = group_sum<G>(Na * Va);
-			double gv[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-			for (int i = 0; i < NSD; ++i) gv[i] = group_sum<G>(dx[i] * Va);
+			const double* rec = recs + q * REC;
+			const double* ta = tab + q * TS + a * 4;
+			const double wm = rec[R_WM];
+			const double Na = ta[0];
 			if (which == 6) {
-				double gt[3];
+				// adjoint: grad lambda . grad T with unit conductivity, summed once per point
+				if (a == 0) {
+					double s = 0.0;
 #pragma unroll
-				for (int i = 0; i < NSD; ++i) gt[i] = group_sum<G>(dx[i] * Ua);
-				double s = 0.0;
-#pragma unroll
-				for (int i = 0; i < NSD; ++i) s += gv[i] * gt[i];
-				ge += s * wm;
+					for (int i = 0; i < NSD; ++i) s += rec[R_GV + i] * rec[R_GT + i];
+					ge += s * wm;
+				}
 				continue;
 			}
-			double k = prm.kConst;
-			if (kT) {
-				// diffusion of U takes T from U itself; the operator from the state; the lift
-				// interpolates no state, so k is taken at T = 0 there
-				const double T = (which == 1 || which == 8 || which == 9) ? Vq : opState ? group_sum<G>(Na * Ua) : 0.0;
-				k = eval_expr(prm.kExpr, 0.0, 0.0, 0.0, 0.0, T);
-			}
+			if (nd.load) Fa += (rec[R_F] * Na) * wm;
+			if (which == 0) continue;
+			double dx[3];
+			node_grad<NSD>(rec, ta, dx);
 			double dd = 0.0;
 #pragma unroll
-			for (int i = 0; i < NSD; ++i) dd += dx[i] * gv[i];
-			const double mass = prm.rho * prm.cp * Na * Vq;
+			for (int i = 0; i < NSD; ++i) dd += dx[i] * rec[R_GV + i];
+			const double kd = rec[R_K] * dd;               // per-element factor included
+			const double mass = prm.rho * prm.cp * Na * rec[R_V];
 			switch (which) {
-				case 1: Fa += ke * k * dd * wm; break;
+				case 1: Fa += kd * wm; break;
 				case 2: case 3: Fa += mass * wm; break;
-				case 4: Fa += (ke * k * dd + prm.coef * mass) * wm; break;
-				case 5: Fa += (prm.cDiff * ke * k * dd + prm.cMass * mass) * wm; break;
+				case 4: Fa += (kd + prm.coef * mass) * wm; break;
+				case 5: Fa += (prm.cDiff * kd + prm.cMass * mass) * wm; break;
 				case 7: Fa += prm.coef * mass * wm; break;
-				case 8: {
-					const double Wq = group_sum<G>(Na * Wa);
-					Fa += (ke * k * dd + prm.rho * prm.cp * Na * Wq) * wm;
-					break;
-				}
-				case 9: Fa -= ke * k * dd * wm; break;
+				case 8: Fa += (kd + prm.rho * prm.cp * Na * rec[R_W]) * wm; break;
+				case 9: Fa -= kd * wm; break;
 				default: break;
 			}
 		}
-		if (which == 6) {
-			if (a == 0 && inRange) prm.out[e] = ge;
-		} else if (has && row >= 0) {
-			atomicAdd(prm.out + row, prm.outScale * Fa);
-		}
 	}
+	if (which == 6) {
+		if (a == 0 && inRange) prm.out[e] = ge;
+	} else if (has && row >= 0) {
+		atomicAdd(prm.out + row, prm.outScale * Fa);
+	}
+	RSD_ELEMENT_LOOP_END
 }
 
 // Assembler::assembleDiagonal (Assembler.tpp:142-197) for c_diff*Diffusion + c_mass*Mass
 template <int NSD, int P>
 __global__ void __launch_bounds__(kAsmThreads) k_asm_diag(const AsmParams prm) {
-	using E = Elem<NSD, P>;
-	constexpr int NPE = E::NPE, G = E::G, EPW = E::EPW;
-	extern __shared__ double sm[];
-	load_tables<NSD, P>(prm, sm);
-	const double* tab = sm;
-	const double* wq = sm + prm.nq * G * 4;
-	const int lane = threadIdx.x & 31, a = lane % G, slot = lane / G;
-	const int warpsPerBlock = blockDim.x >> 5;
-	const int64_t warpId = (int64_t)blockIdx.x * warpsPerBlock + (threadIdx.x >> 5);
-	const int64_t warpStride = (int64_t)gridDim.x * warpsPerBlock;
-	const bool needT = prm.kExpr.n != 0;
-	for (int64_t eb = warpId * EPW; eb < prm.nelem; eb += warpStride * EPW) {
-		const int64_t e = eb + slot;
-		int32_t node, row;
-		double xa[3];
-		const bool has = load_node<NSD, P>(prm, e < prm.nelem, e, a, node, row, xa);
-		double Ua = 0.0;
-		if (has && needT) Ua = row >= 0 ? (prm.U ? prm.U[row] : 0.0) : prm.g[node];
-		const double ke = (prm.kElem && e < prm.nelem) ? prm.kElem[e] : 1.0;
-		double Da = 0.0;
+	Needs nd{};
+	nd.state = prm.kExpr.n != 0;
+	RSD_ELEMENT_LOOP_BEGIN
+	const double Ua = (has && nd.state) ? (row >= 0 ? (prm.U ? prm.U[row] : 0.0) : prm.g[node]) : 0.0;
+	RSD_STAGE_NODE(Ua, 0.0, 0.0)
+	double Da = 0.0;
+	if (has) {
 		for (int q = 0; q < prm.nq; ++q) {
-			const double* tq = tab + (q * G) * 4;
-			double Na = 0.0, dxi[3] = {0.0, 0.0, 0.0};
-			if (a < NPE) {
-				Na = tq[a * 4];
-#pragma unroll
-				for (int al = 0; al < NSD; ++al) dxi[al] = tq[a * 4 + 1 + al];
-			}
-			double inv[9], measure;
-			qp_geometry<NSD, G>(xa, dxi, inv, measure);
+			const double* rec = recs + q * REC;
+			const double* ta = tab + q * TS + a * 4;
 			double dx[3];
-			phys_grad<NSD>(inv, dxi, dx);
-			double k = prm.kConst;
-			if (needT) k = eval_expr(prm.kExpr, 0.0, 0.0, 0.0, 0.0, group_sum<G>(Na * Ua));
+			node_grad<NSD>(rec, ta, dx);
 			double dd = 0.0;
 #pragma unroll
 			for (int i = 0; i < NSD; ++i) dd += dx[i] * dx[i];
-			Da += (prm.cDiff * ke * k * dd + prm.cMass * prm.rho * prm.cp * Na * Na) * measure * wq[q];
+			Da += (prm.cDiff * rec[R_K] * dd + prm.cMass * prm.rho * prm.cp * ta[0] * ta[0]) * rec[R_WM];
 		}
-		if (has && row >= 0) atomicAdd(prm.out + row, Da);
 	}
+	if (has && row >= 0) atomicAdd(prm.out + row, Da);
+	RSD_ELEMENT_LOOP_END
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -429,6 +508,7 @@ int build_tables(rsd_heat* h) {
 	double gx[5], gw[5];
 	gauss_legendre(q1, gx, gw);
 	const int nq = nsd == 3 ? q1 * q1 * q1 : q1 * q1;
+	if (asm_smem_bytes(h->m->npe, nq) > 227 * 1024) return set_error(RSD_EINVAL, "too many quadrature points for this element");
 	std::vector<double> t(nq * G * 4 + nq, 0.0);
 	int q = 0;
 	for (int k = 0; k < (nsd == 3 ? q1 : 1); ++k)
@@ -491,8 +571,8 @@ static int launch_one(void (*kern)(const AsmParams), dim3 gr, size_t smem, rsd_c
 #define RSD_ASM_DISPATCH(KERNEL)                                                              \
 	static int launch_##KERNEL(rsd_ctx* ctx, const rsd_heat* h, const AsmParams& p) {         \
 		const int nsd = h->m->nsd, ord = h->m->order, G = group_width(h->m->npe);             \
-		const size_t smem = sizeof(double) * (h->nq * G * 4 + h->nq);                         \
-		const int epb = (kAsmThreads / 32) * (32 / G);                                        \
+		const size_t smem = asm_smem_bytes(h->m->npe, h->nq);                                 \
+		const int epb = kAsmWarps * (32 / G);                                                 \
 		int64_t blocks = (p.nelem + epb - 1) / epb;                                           \
 		blocks = std::min<int64_t>(blocks, (int64_t)ctx->num_sms * 16);                       \
 		dim3 gr((unsigned)std::max<int64_t>(blocks, 1));                                      \
@@ -508,14 +588,49 @@ RSD_ASM_DISPATCH(k_asm_matrix)
 RSD_ASM_DISPATCH(k_asm_vector)
 RSD_ASM_DISPATCH(k_asm_diag)
 
+// Build the element -> CSR slot map for h's pattern (once).  Skipped, leaving the binary-search
+// scatter, when RSD_SLOT_MAP=0 or when the map would take more than a quarter of free memory.
+static int ensure_slots(rsd_ctx* ctx, rsd_heat* h) {
+	if (h->slots || h->slotsTried) return RSD_OK;
+	h->slotsTried = true;
+	const char* env = getenv("RSD_SLOT_MAP");
+	if (env && env[0] == '0') return RSD_OK;
+	const int npe = h->m->npe;
+	const int stride = (npe + 3) & ~3;
+	const size_t bytes = sizeof(int32_t) * (size_t)h->m->nelem * npe * stride;
+	size_t freeB = 0, totalB = 0;
+	RSD_CUDA(cudaMemGetInfo(&freeB, &totalB));
+	if (bytes > freeB / 4) return RSD_OK;
+	if (cudaMalloc(&h->slots, bytes) != cudaSuccess) { cudaGetLastError(); h->slots = nullptr; return RSD_OK; }
+	h->slotStride = stride;
+	const int64_t total = h->m->nelem * npe;
+	const int blocks = (int)std::min<int64_t>((total + 255) / 256, (int64_t)ctx->num_sms * 8);
+	const int nsd = h->m->nsd, ord = h->m->order;
+	const rsd_csr* K = h->K;
+#define RSD_SLOTS(D, Q) k_build_slots<D, Q><<<std::max(blocks, 1), 256, 0, ctx->stream>>>(h->m->nelem, h->m->ien, h->t2a, K->rowPtr, K->col, K->sStart, h->slots, stride)
+	if (nsd == 2 && ord == 1) RSD_SLOTS(2, 1);
+	else if (nsd == 2 && ord == 2) RSD_SLOTS(2, 2);
+	else if (nsd == 2 && ord == 3) RSD_SLOTS(2, 3);
+	else if (nsd == 3 && ord == 1) RSD_SLOTS(3, 1);
+	else RSD_SLOTS(3, 2);
+#undef RSD_SLOTS
+	RSD_CUDA(cudaGetLastError());
+	return RSD_OK;
+}
+
 int assemble_matrix(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, double cTDiff, double cTMass,
                     const double* U, const double* Udot, rsd_csr* A) {
 	if (A->n != h->n || A->nnz != h->K->nnz) return set_error(RSD_EINVAL, "matrix does not have the problem's pattern");
+	RSD_CHECK(ensure_slots(ctx, h));
 	AsmParams p = params_for(h);
-	p.rp = A->rowPtr; p.col = A->col; p.val = A->val;
+	p.rp = A->rowPtr; p.col = A->col; p.sStart = A->sStart; p.val = A->sVal;
+	// the slot map indexes h's pattern; another matrix of equal size may differ, so it searches
+	if (A == h->K || A->rowPtr == h->K->rowPtr) { p.slots = h->slots; p.slotStride = h->slotStride; }
 	p.cDiff = cDiff; p.cMass = cMass; p.cTDiff = cTDiff; p.cTMass = cTMass;
 	p.U = U; p.Udot = Udot;
-	RSD_CUDA(cudaMemsetAsync(A->val, 0, sizeof(double) * std::max<int64_t>(A->nnz, 1), ctx->stream));
+	RSD_CUDA(cudaMemsetAsync(A->sVal, 0, sizeof(double) * std::max<int64_t>(A->ssize, 1), ctx->stream));
+	A->sellValid = true;
+	A->csrValid = false;
 	A->version++;
 	const int pr = prof_begin(ctx, PF_ASM_MATRIX);
 	const int rc = launch_k_asm_matrix(ctx, h, p);

@@ -1,6 +1,8 @@
-// BLAS-1, deterministic reductions, CSR SpMV (FP64 / FP32), diagonal, lump and Jacobi setup.
+// BLAS-1, deterministic reductions, SpMV (SELL-32 and CSR-vector, FP64 / FP32), layout syncs,
+// diagonal, lump, Jacobi setup and the SpMV launch autotuner.
 #include <algorithm>
 #include <cmath>
+#include <vector>
 
 #include "rsd_kernels.cuh"
 
@@ -44,21 +46,72 @@ int dot_device(rsd_ctx* ctx, int64_t n, const double* x, const double* y, double
 }
 
 // ---------------------------------------------------------------------------------------------
-// SpMV: operations::matvec (linalg/operations/backend/cpu/MatrixOps.tpp:5-23) as vector-CSR:
-// a group of L lanes per row, streaming 4-byte columns and 8/4-byte values, x through L2.
+// layout syncs between CSR (API order) and SELL-32 (execution order)
+// ---------------------------------------------------------------------------------------------
+__global__ void k_sell_from_csr(int64_t ssize, const int32_t* __restrict__ src, const double* __restrict__ val, double* __restrict__ sval) {
+	for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < ssize; s += (int64_t)gridDim.x * blockDim.x) {
+		const int32_t q = src[s];
+		sval[s] = q >= 0 ? val[q] : 0.0;
+	}
+}
+__global__ void k_csr_from_sell(int64_t ssize, const int32_t* __restrict__ src, const double* __restrict__ sval, double* __restrict__ val) {
+	for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < ssize; s += (int64_t)gridDim.x * blockDim.x) {
+		const int32_t q = src[s];
+		if (q >= 0) val[q] = sval[s];
+	}
+}
+__global__ void k_to_f32(int64_t n, const double* __restrict__ a, float* __restrict__ b) {
+	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) b[i] = (float)a[i];
+}
+
+int sell_sync(rsd_ctx* ctx, rsd_csr* A) {
+	if (A->sellValid) return RSD_OK;
+	if (A->ssize) {
+		k_sell_from_csr<<<vec_grid(ctx, A->ssize), 256, 0, ctx->stream>>>(A->ssize, A->sSrc, A->val, A->sVal);
+		RSD_CUDA(cudaGetLastError());
+	}
+	A->sellValid = true;
+	return RSD_OK;
+}
+
+int csr_sync(rsd_ctx* ctx, rsd_csr* A) {
+	if (A->csrValid) return RSD_OK;
+	if (A->ssize) {
+		k_csr_from_sell<<<vec_grid(ctx, A->ssize), 256, 0, ctx->stream>>>(A->ssize, A->sSrc, A->sVal, A->val);
+		RSD_CUDA(cudaGetLastError());
+	}
+	A->csrValid = true;
+	return RSD_OK;
+}
+
+int exec_sync(rsd_ctx* ctx, rsd_csr* A) { return A->format == 0 ? sell_sync(ctx, A) : csr_sync(ctx, A); }
+
+int f32_sync(rsd_ctx* ctx, rsd_csr* A) {
+	RSD_CHECK(exec_sync(ctx, A));
+	if (!A->val32) RSD_CUDA(cudaMalloc(&A->val32, sizeof(float) * std::max<int64_t>(std::max(A->ssize, A->nnz), 1)));
+	if (A->version32 == A->version && A->fmt32 == A->format) return RSD_OK;
+	const int64_t len = A->format == 0 ? A->ssize : A->nnz;
+	if (len) {
+		k_to_f32<<<vec_grid(ctx, len), 256, 0, ctx->stream>>>(len, exec_val(A), A->val32);
+		RSD_CUDA(cudaGetLastError());
+	}
+	A->version32 = A->version;
+	A->fmt32 = A->format;
+	return RSD_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// SpMV: operations::matvec (linalg/operations/backend/cpu/MatrixOps.tpp:5-23), SELL-32 (L == 0,
+// a warp per slice) or CSR-vector (L lanes per row)
 // ---------------------------------------------------------------------------------------------
 template <int L, typename T>
-__global__ void __launch_bounds__(256) k_spmv(int64_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
-                                              const T* __restrict__ val, const T* __restrict__ x, T* __restrict__ y) {
-	const int lane = threadIdx.x & (L - 1);
-	const int64_t g0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / L;
-	const int64_t gs = ((int64_t)gridDim.x * blockDim.x) / L;
-	// warp-uniform trip count: the whole warp iterates while any of its groups has a row
-	const int64_t warp0 = g0 - ((threadIdx.x & 31) / L);
-	for (int64_t base = warp0; base < n; base += gs) {
-		const int64_t row = base + ((threadIdx.x & 31) / L);
-		const T s = csr_row<L, T, T>(rp, col, val, x, row, n, lane);
-		if (lane == 0 && row < n) y[row] = s;
+__global__ void __launch_bounds__(512) k_spmv(int64_t n, MatView<T> A, const T* __restrict__ x, T* __restrict__ y) {
+	const L2Pol pol = make_l2pol();
+	RowLoop<L> rl;
+	for (int64_t base = rl.base; base < n; base += rl.step) {
+		const int64_t row = base + rl.sub;
+		const T s = row_dot<L, T, T>(A, x, row, n, rl.lane, pol);
+		if (rl.lane == 0 && row < n) sth(y + row, s, pol.first);
 	}
 }
 
@@ -66,62 +119,56 @@ int default_lanes(const rsd_csr* A) {
 	if (A->lanes) return A->lanes;
 	const double avg = A->n ? (double)A->nnz / (double)A->n : 1.0;
 	if (avg <= 6) return 2;
-	if (avg <= 14) return 4;
 	if (avg <= 40) return 4;
 	if (avg <= 96) return 8;
 	return 16;
 }
 
-template <typename T>
-static int spmv_t(rsd_ctx* ctx, const rsd_csr* A, const T* val, const T* x, T* y) {
-	if (A->n == 0) return RSD_OK;
-	const int L = default_lanes(A);
-	const int block = A->block ? A->block : 256;
-	int64_t blocks = (A->n * L + block - 1) / block;
+static int grid_for(const rsd_ctx* ctx, int64_t n, int L, int block) {
+	int64_t blocks = (n * std::max(L, 1) + block - 1) / block;
 	blocks = std::min<int64_t>(blocks, (int64_t)ctx->num_sms * (2048 / block));
-	dim3 g((unsigned)std::max<int64_t>(blocks, 1));
-	switch (L) {
-		case 1: k_spmv<1, T><<<g, block, 0, ctx->stream>>>(A->n, A->rowPtr, A->col, val, x, y); break;
-		case 2: k_spmv<2, T><<<g, block, 0, ctx->stream>>>(A->n, A->rowPtr, A->col, val, x, y); break;
-		case 4: k_spmv<4, T><<<g, block, 0, ctx->stream>>>(A->n, A->rowPtr, A->col, val, x, y); break;
-		case 8: k_spmv<8, T><<<g, block, 0, ctx->stream>>>(A->n, A->rowPtr, A->col, val, x, y); break;
-		case 16: k_spmv<16, T><<<g, block, 0, ctx->stream>>>(A->n, A->rowPtr, A->col, val, x, y); break;
-		default: k_spmv<32, T><<<g, block, 0, ctx->stream>>>(A->n, A->rowPtr, A->col, val, x, y); break;
-	}
+	return (int)std::max<int64_t>(blocks, 1);
+}
+
+int spmv_f64(rsd_ctx* ctx, const rsd_csr* Ac, const double* x, double* y) {
+	rsd_csr* A = const_cast<rsd_csr*>(Ac);
+	if (A->n == 0) return RSD_OK;
+	RSD_CHECK(exec_sync(ctx, A));
+	const int block = A->block ? A->block : 256;
+	const int L = exec_lanes(A);
+	const MatView<double> V = view64(A);
+	RSD_DISPATCH_L(L, (k_spmv<LL, double><<<grid_for(ctx, A->n, LL, block), block, 0, ctx->stream>>>(A->n, V, x, y)));
 	RSD_CUDA(cudaGetLastError());
 	return RSD_OK;
 }
 
-int spmv_f64(rsd_ctx* ctx, const rsd_csr* A, const double* x, double* y) { return spmv_t<double>(ctx, A, A->val, x, y); }
-int spmv_f32(rsd_ctx* ctx, const rsd_csr* A, const float* x, float* y) { return spmv_t<float>(ctx, A, A->val32, x, y); }
-
-__global__ void k_to_f32(int64_t n, const double* __restrict__ a, float* __restrict__ b) {
-	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) b[i] = (float)a[i];
+int spmv_f32(rsd_ctx* ctx, const rsd_csr* Ac, const float* x, float* y) {
+	rsd_csr* A = const_cast<rsd_csr*>(Ac);
+	if (A->n == 0) return RSD_OK;
+	RSD_CHECK(f32_sync(ctx, A));
+	const int block = A->block ? A->block : 256;
+	const int L = exec_lanes(A);
+	const MatView<float> V = view32(A);
+	RSD_DISPATCH_L(L, (k_spmv<LL, float><<<grid_for(ctx, A->n, LL, block), block, 0, ctx->stream>>>(A->n, V, x, y)));
+	RSD_CUDA(cudaGetLastError());
+	return RSD_OK;
 }
 
-// CSROperator::diagonal (linalg/operator/CSROperator.hpp:40-45) via the precomputed diagonal slot;
-// a missing diagonal is an error in the reference (std::out_of_range) and 0 here, flagged by the caller
+// CSROperator::diagonal (linalg/operator/CSROperator.hpp:40-45) through the precomputed diagonal
+// slot; Jacobi::update's inverse (linalg/solver/preconditioner/Jacobi.hpp:31-34) when invert is set
 __global__ void k_diag(int64_t n, const int32_t* __restrict__ dpos, const double* __restrict__ val, double* __restrict__ d, int invert) {
 	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
 		const int32_t p = dpos[i];
 		const double v = p >= 0 ? val[p] : 0.0;
-		// Jacobi::update (linalg/solver/preconditioner/Jacobi.hpp:31-34)
 		d[i] = invert ? ((fabs(v) > 1e-300) ? 1.0 / v : 1.0) : v;
 	}
 }
 
-// operations::lump (MatrixOps.tpp:25-43): row sums, one group of 4 lanes per row
-__global__ void k_lump(int64_t n, const int32_t* __restrict__ rp, const double* __restrict__ val, double* __restrict__ d) {
-	const int lane = threadIdx.x & 3;
-	const int64_t g0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / 4, gs = ((int64_t)gridDim.x * blockDim.x) / 4;
-	const int64_t warp0 = g0 - ((threadIdx.x & 31) / 4);
-	for (int64_t base = warp0; base < n; base += gs) {
-		const int64_t row = base + ((threadIdx.x & 31) / 4);
-		double s = 0.0;
-		if (row < n) for (int p = rp[row] + lane; p < rp[row + 1]; p += 4) s += val[p];
-		s = group_sum<4>(s);
-		if (lane == 0 && row < n) d[row] = s;
-	}
+// operations::lump (MatrixOps.tpp:25-43): row sums over the SELL-32 layout (padding adds zeros)
+__global__ void k_lump(int64_t n, MatView<double> A, double* __restrict__ d) {
+	const L2Pol pol = make_l2pol();
+	for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n; row += (int64_t)gridDim.x * blockDim.x)
+		d[row] = row_sum<0, double, double>(A, row, n, 0, pol, [](int) { return 1.0; });
 }
 
 }  // namespace rsd
@@ -195,20 +242,17 @@ int rsd_mul(rsd_ctx* c, int64_t n, const double* x, const double* y, double* z) 
 
 int rsd_spmv(rsd_ctx* c, const rsd_csr* A, const double* x, double* y) {
 	if (!c || !A || (A->n && (!x || !y))) return set_error(RSD_EINVAL, "null argument");
+	const int pr = prof_begin(c, PF_SPMV);
 	RSD_CHECK(spmv_f64(c, A, x, y));
+	prof_end(c, pr);
 	RSD_CUDA(cudaStreamSynchronize(c->stream));
 	return RSD_OK;
 }
 
 int rsd_csr_sync_f32(rsd_ctx* c, rsd_csr* A) {
 	if (!c || !A) return set_error(RSD_EINVAL, "null argument");
-	if (!A->val32) RSD_CUDA(cudaMalloc(&A->val32, sizeof(float) * std::max<int64_t>(A->nnz, 1)));
-	if (A->nnz) {
-		k_to_f32<<<vec_grid(c, A->nnz), 256, 0, c->stream>>>(A->nnz, A->val, A->val32);
-		RSD_CUDA(cudaGetLastError());
-	}
+	RSD_CHECK(f32_sync(c, A));
 	RSD_CUDA(cudaStreamSynchronize(c->stream));
-	A->version32 = A->version;
 	return RSD_OK;
 }
 
@@ -220,45 +264,63 @@ int rsd_spmv_f32(rsd_ctx* c, const rsd_csr* A, const float* x, float* y) {
 	return RSD_OK;
 }
 
-int rsd_csr_diagonal(rsd_ctx* c, const rsd_csr* A, double* d) {
+int rsd_csr_diagonal(rsd_ctx* c, const rsd_csr* Ac, double* d) {
+	rsd_csr* A = const_cast<rsd_csr*>(Ac);
 	if (!c || !A || (A->n && !d)) return set_error(RSD_EINVAL, "null argument");
 	if (!A->n) return RSD_OK;
-	k_diag<<<vec_grid(c, A->n), 256, 0, c->stream>>>(A->n, A->diag, A->val, d, 0);
+	RSD_CHECK(exec_sync(c, A));
+	k_diag<<<vec_grid(c, A->n), 256, 0, c->stream>>>(A->n, exec_diag(A), exec_val(A), d, 0);
 	RSD_CUDA(cudaGetLastError());
 	RSD_CUDA(cudaStreamSynchronize(c->stream));
 	return RSD_OK;
 }
 
-int rsd_jacobi_setup(rsd_ctx* c, const rsd_csr* A, double* invD) {
+int rsd_jacobi_setup(rsd_ctx* c, const rsd_csr* Ac, double* invD) {
+	rsd_csr* A = const_cast<rsd_csr*>(Ac);
 	if (!c || !A || (A->n && !invD)) return set_error(RSD_EINVAL, "null argument");
 	if (!A->n) return RSD_OK;
-	k_diag<<<vec_grid(c, A->n), 256, 0, c->stream>>>(A->n, A->diag, A->val, invD, 1);
+	RSD_CHECK(exec_sync(c, A));
+	k_diag<<<vec_grid(c, A->n), 256, 0, c->stream>>>(A->n, exec_diag(A), exec_val(A), invD, 1);
 	RSD_CUDA(cudaGetLastError());
 	RSD_CUDA(cudaStreamSynchronize(c->stream));
 	return RSD_OK;
 }
 
-// SpMV launch autotuner: times every lanes-per-row x block combination on this matrix with CUDA
-// events (median of 5 launches after 2 warm-ups) and keeps the fastest in A's launch settings.
+int rsd_csr_lump(rsd_ctx* c, const rsd_csr* Ac, double* d) {
+	rsd_csr* A = const_cast<rsd_csr*>(Ac);
+	if (!c || !A || (A->n && !d)) return set_error(RSD_EINVAL, "null argument");
+	if (!A->n) return RSD_OK;
+	RSD_CHECK(sell_sync(c, A));
+	k_lump<<<vec_grid(c, A->n), 256, 0, c->stream>>>(A->n, MatView<double>{A->sStart, A->sCol, A->sVal}, d);
+	RSD_CUDA(cudaGetLastError());
+	RSD_CUDA(cudaStreamSynchronize(c->stream));
+	return RSD_OK;
+}
+
+// SpMV launch autotuner: times SELL-32 and CSR-vector with 2..32 lanes per row, each at 128, 256
+// and 512 threads per block, with CUDA events (median of 5 launches after 2 warm-ups), and keeps
+// the fastest in A's launch settings.
 int rsd_csr_autotune(rsd_ctx* c, rsd_csr* A, int32_t* lanes_out, int32_t* block_out, double* best_us) {
 	if (!c || !A) return set_error(RSD_EINVAL, "null argument");
-	if (A->n == 0) { if (lanes_out) *lanes_out = 2; if (block_out) *block_out = 256; if (best_us) *best_us = 0; return RSD_OK; }
+	if (A->n == 0) { if (lanes_out) *lanes_out = 0; if (block_out) *block_out = 256; if (best_us) *best_us = 0; return RSD_OK; }
 	double *x = nullptr, *y = nullptr;
 	RSD_CUDA(cudaMalloc(&x, sizeof(double) * A->n));
 	RSD_CUDA(cudaMalloc(&y, sizeof(double) * A->n));
 	k_fill<double><<<vec_grid(c, A->n), 256, 0, c->stream>>>(x, A->n, 1.0);
+	RSD_CHECK(sell_sync(c, A));
+	RSD_CHECK(csr_sync(c, A));
 	cudaEvent_t e0, e1;
 	cudaEventCreate(&e0);
 	cudaEventCreate(&e1);
-	const int lanes[] = {2, 4, 8, 16, 32};
+	const int lanes[] = {0, 2, 4, 8, 16, 32};   // 0: SELL-32
 	const int blocks[] = {128, 256, 512};
-	int bestL = default_lanes(A), bestB = 256;
+	int bestL = 0, bestB = 256;
 	double best = 1e30;
-	const int savedL = A->lanes, savedB = A->block;
+	const int savedF = A->format, savedL = A->lanes, savedB = A->block;
 	int rc = RSD_OK;
 	for (int L : lanes)
 		for (int B : blocks) {
-			A->lanes = L; A->block = B;
+			A->format = L ? 1 : 0; A->lanes = L; A->block = B;
 			std::vector<float> ts;
 			for (int rep = 0; rep < 7 && rc == RSD_OK; ++rep) {
 				cudaEventRecord(e0, c->stream);
@@ -278,21 +340,13 @@ int rsd_csr_autotune(rsd_ctx* c, rsd_csr* A, int32_t* lanes_out, int32_t* block_
 	cudaEventDestroy(e1);
 	cudaFree(x);
 	cudaFree(y);
-	if (rc != RSD_OK) { A->lanes = savedL; A->block = savedB; return rc; }
+	if (rc != RSD_OK) { A->format = savedF; A->lanes = savedL; A->block = savedB; return rc; }
+	A->format = bestL ? 1 : 0;
 	A->lanes = bestL;
 	A->block = bestB;
 	if (lanes_out) *lanes_out = bestL;
 	if (block_out) *block_out = bestB;
 	if (best_us) *best_us = best;
-	return RSD_OK;
-}
-
-int rsd_csr_lump(rsd_ctx* c, const rsd_csr* A, double* d) {
-	if (!c || !A || (A->n && !d)) return set_error(RSD_EINVAL, "null argument");
-	if (!A->n) return RSD_OK;
-	k_lump<<<vec_grid(c, A->n * 4), 256, 0, c->stream>>>(A->n, A->rowPtr, A->val, d);
-	RSD_CUDA(cudaGetLastError());
-	RSD_CUDA(cudaStreamSynchronize(c->stream));
 	return RSD_OK;
 }
 

@@ -217,6 +217,11 @@ static void diag_index(int64_t n, const int32_t* rp, const int32_t* col, int32_t
 	});
 }
 
+static void free_csr_arrays(rsd_csr* A) {
+	cudaFree(A->rowPtr); cudaFree(A->col); cudaFree(A->val); cudaFree(A->diag);
+	cudaFree(A->sStart); cudaFree(A->sCol); cudaFree(A->sVal); cudaFree(A->val32); cudaFree(A->sSrc); cudaFree(A->sDiag);
+}
+
 static int upload_csr(rsd_ctx* ctx, int64_t n, const std::vector<int32_t>& rp, const std::vector<int32_t>& col,
                       const double* hval, rsd_csr** out) {
 	const int64_t nnz = rp[n];
@@ -225,19 +230,59 @@ static int upload_csr(rsd_ctx* ctx, int64_t n, const std::vector<int32_t>& rp, c
 	A->nnz = nnz;
 	std::vector<int32_t> d(n);
 	diag_index(n, rp.data(), col.data(), d.data());
-	auto fail = [&](cudaError_t e, const char* w) { cudaFree(A->rowPtr); cudaFree(A->col); cudaFree(A->val); cudaFree(A->diag); delete A; return cuda_error(e, w); };
+	// SELL-32 layout: slice s holds rows 32s..32s+31, padded to its longest row
+	const int64_t ns = (n + 31) / 32;
+	std::vector<int64_t> start(ns + 1, 0);
+	for (int64_t s = 0; s < ns; ++s) {
+		int32_t len = 0;
+		for (int64_t i = 32 * s; i < std::min<int64_t>(n, 32 * s + 32); ++i) len = std::max(len, rp[i + 1] - rp[i]);
+		start[s + 1] = start[s] + 32 * (int64_t)len;
+	}
+	const int64_t ssize = start[ns];
+	if (ssize > INT32_MAX) { delete A; return set_error(RSD_EINVAL, "padded SELL layout has 2^31 or more slots"); }
+	std::vector<int32_t> sStart(ns + 1), sCol(std::max<int64_t>(ssize, 1)), sSrc(std::max<int64_t>(ssize, 1), -1), sDiag(std::max<int64_t>(n, 1), -1);
+	for (int64_t s = 0; s <= ns; ++s) sStart[s] = (int32_t)start[s];
+	parallel_for(ns, [&](int64_t b, int64_t e) {
+		for (int64_t s = b; s < e; ++s) {
+			const int64_t len = (start[s + 1] - start[s]) / 32;
+			for (int64_t l = 0; l < 32; ++l) {
+				const int64_t i = 32 * s + l;
+				for (int64_t j = 0; j < len; ++j) {
+					const int64_t slot = start[s] + 32 * j + l;
+					if (i < n && rp[i] + j < rp[i + 1]) { sCol[slot] = col[rp[i] + j]; sSrc[slot] = (int32_t)(rp[i] + j); }
+					else sCol[slot] = (int32_t)(i < n ? i : 0);   // padding: value 0, a valid column
+				}
+				if (i < n && d[i] >= 0) sDiag[i] = (int32_t)(start[s] + 32 * (d[i] - rp[i]) + l);
+			}
+		}
+	});
+	A->nslices = ns;
+	A->ssize = ssize;
+	auto fail = [&](cudaError_t e, const char* w) { free_csr_arrays(A); delete A; return cuda_error(e, w); };
+	const size_t S = (size_t)std::max<int64_t>(ssize, 1);
 	cudaError_t e;
 	if ((e = cudaMalloc(&A->rowPtr, sizeof(int32_t) * (n + 1))) != cudaSuccess) return fail(e, "cudaMalloc rowPtr");
 	if ((e = cudaMalloc(&A->col, sizeof(int32_t) * std::max<int64_t>(nnz, 1))) != cudaSuccess) return fail(e, "cudaMalloc col");
 	if ((e = cudaMalloc(&A->val, sizeof(double) * std::max<int64_t>(nnz, 1))) != cudaSuccess) return fail(e, "cudaMalloc val");
 	if ((e = cudaMalloc(&A->diag, sizeof(int32_t) * std::max<int64_t>(n, 1))) != cudaSuccess) return fail(e, "cudaMalloc diag");
+	if ((e = cudaMalloc(&A->sStart, sizeof(int32_t) * (ns + 1))) != cudaSuccess) return fail(e, "cudaMalloc sStart");
+	if ((e = cudaMalloc(&A->sCol, sizeof(int32_t) * S)) != cudaSuccess) return fail(e, "cudaMalloc sCol");
+	if ((e = cudaMalloc(&A->sVal, sizeof(double) * S)) != cudaSuccess) return fail(e, "cudaMalloc sVal");
+	if ((e = cudaMalloc(&A->sSrc, sizeof(int32_t) * S)) != cudaSuccess) return fail(e, "cudaMalloc sSrc");
+	if ((e = cudaMalloc(&A->sDiag, sizeof(int32_t) * std::max<int64_t>(n, 1))) != cudaSuccess) return fail(e, "cudaMalloc sDiag");
 	if ((e = cudaMemcpyAsync(A->rowPtr, rp.data(), sizeof(int32_t) * (n + 1), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload rowPtr");
 	if (nnz && (e = cudaMemcpyAsync(A->col, col.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload col");
 	if (n && (e = cudaMemcpyAsync(A->diag, d.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload diag");
+	if ((e = cudaMemcpyAsync(A->sStart, sStart.data(), sizeof(int32_t) * (ns + 1), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload sStart");
+	if ((e = cudaMemcpyAsync(A->sCol, sCol.data(), sizeof(int32_t) * S, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload sCol");
+	if ((e = cudaMemcpyAsync(A->sSrc, sSrc.data(), sizeof(int32_t) * S, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload sSrc");
+	if ((e = cudaMemcpyAsync(A->sDiag, sDiag.data(), sizeof(int32_t) * std::max<int64_t>(n, 1), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload sDiag");
 	if (hval && nnz) e = cudaMemcpyAsync(A->val, hval, sizeof(double) * nnz, cudaMemcpyHostToDevice, ctx->stream);
 	else e = cudaMemsetAsync(A->val, 0, sizeof(double) * std::max<int64_t>(nnz, 1), ctx->stream);
 	if (e != cudaSuccess) return fail(e, "upload values");
 	if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return fail(e, "csr upload sync");
+	A->csrValid = true;
+	A->sellValid = false;
 	*out = A;
 	return RSD_OK;
 }
@@ -472,9 +517,7 @@ int rsd_csr_create(rsd_ctx* c, int64_t nrows, int64_t nnz, const int64_t* row_pt
 int rsd_csr_destroy(rsd_csr* A) {
 	if (!A) return RSD_OK;
 	cudaDeviceSynchronize();
-	if (A->owns_pattern) { cudaFree(A->rowPtr); cudaFree(A->col); cudaFree(A->diag); }
-	cudaFree(A->val);
-	cudaFree(A->val32);
+	free_csr_arrays(A);
 	delete A;
 	return RSD_OK;
 }
@@ -486,21 +529,28 @@ int rsd_csr_info(const rsd_csr* A, int64_t* nrows, int64_t* nnz) {
 	return RSD_OK;
 }
 
-int rsd_csr_values(rsd_csr* A, double** dvalues) {
-	if (!A || !dvalues) return set_error(RSD_EINVAL, "null argument");
+int rsd_csr_values(rsd_ctx* c, rsd_csr* A, double** dvalues) {
+	if (!c || !A || !dvalues) return set_error(RSD_EINVAL, "null argument");
+	RSD_CHECK(csr_sync(c, A));
 	*dvalues = A->val;
-	A->version++;   // the caller may write through the pointer
+	// the caller may write through the pointer: the CSR layout becomes the current one
+	A->sellValid = false;
+	A->version++;
 	return RSD_OK;
 }
 
 int rsd_csr_set_values(rsd_ctx* c, rsd_csr* A, const double* hv) {
 	if (!c || !A || !hv) return set_error(RSD_EINVAL, "null argument");
+	RSD_CHECK(rsd_memcpy(c, A->val, hv, sizeof(double) * A->nnz, RSD_H2D));
+	A->csrValid = true;
+	A->sellValid = false;
 	A->version++;
-	return rsd_memcpy(c, A->val, hv, sizeof(double) * A->nnz, RSD_H2D);
+	return RSD_OK;
 }
 
-int rsd_csr_get_values(rsd_ctx* c, const rsd_csr* A, double* hv) {
+int rsd_csr_get_values(rsd_ctx* c, rsd_csr* A, double* hv) {
 	if (!c || !A || !hv) return set_error(RSD_EINVAL, "null argument");
+	RSD_CHECK(csr_sync(c, A));
 	return rsd_memcpy(c, hv, A->val, sizeof(double) * A->nnz, RSD_D2H);
 }
 
@@ -517,7 +567,8 @@ int rsd_csr_get_pattern(rsd_ctx* c, const rsd_csr* A, int64_t* hrp, int64_t* hco
 int rsd_csr_set_launch(rsd_csr* A, int32_t lanes, int32_t block) {
 	if (!A) return set_error(RSD_EINVAL, "null matrix");
 	if (lanes && (lanes < 1 || lanes > 32 || (lanes & (lanes - 1)))) return set_error(RSD_EINVAL, "lanes per row must be a power of two in 1..32");
-	if (block && (block < 32 || block > 1024 || block % 32)) return set_error(RSD_EINVAL, "block must be a multiple of 32 in 32..1024");
+	if (block && (block < 64 || block > 512 || (block & (block - 1)))) return set_error(RSD_EINVAL, "block must be a power of two in 64..512");
+	A->format = lanes ? 1 : 0;
 	A->lanes = lanes;
 	A->block = block;
 	return RSD_OK;

@@ -83,19 +83,42 @@ void prof_end(rsd_ctx* ctx, int pair);
 int prof_flush(rsd_ctx* ctx);   // fold recorded pairs into the totals (synchronizes the stream)
 }  // namespace rsd
 
+// A CSR matrix (the API's storage, CSRMatrix's layout with 32-bit indices) plus its SELL-32
+// execution layout: rows in slices of 32, each slice stored column-major and padded to its
+// longest row, so that a warp's loads of values and columns are contiguous and consecutive rows'
+// gathers of x are neighbours.  Entry j of row i lives at sStart[i/32] + 32 j + i%32; padding has
+// value 0 and the row's own column.  Values may be current in either layout (csrValid/sellValid).
 struct rsd_csr {
 	int64_t n = 0, nnz = 0;
 	int32_t* rowPtr = nullptr;     // n+1
 	int32_t* col = nullptr;        // nnz
 	double* val = nullptr;         // nnz
-	float* val32 = nullptr;        // nnz, lazily created for the mixed-precision path
 	int32_t* diag = nullptr;       // n: position of the diagonal entry or -1
-	int lanes = 0;                 // SpMV lanes per row (0: default from nnz/row)
+	// SELL-32
+	int64_t nslices = 0, ssize = 0;
+	int32_t* sStart = nullptr;     // nslices+1
+	int32_t* sCol = nullptr;       // ssize
+	double* sVal = nullptr;        // ssize
+	int32_t* sSrc = nullptr;       // ssize: CSR position of the slot, -1 for padding
+	int32_t* sDiag = nullptr;      // n: slot of the diagonal entry or -1
+	bool csrValid = true, sellValid = false;
+	int format = 0;                // SpMV layout: 0 SELL-32, 1 CSR vector with `lanes` lanes per row
+	int lanes = 0;                 // CSR SpMV lanes per row (0: default from nnz/row)
 	int block = 0;                 // SpMV threads per block (0: default)
 	bool owns_pattern = true;
 	uint64_t version = 1;          // bumped whenever the FP64 values may have changed
+	// FP32 copy of the values for the mixed-precision path, in the layout `fmt32` (lazily created)
+	float* val32 = nullptr;        // max(ssize, nnz)
+	int fmt32 = -1;
 	uint64_t version32 = 0;        // FP64 version the FP32 copy was made from
 };
+
+namespace rsd {
+int sell_sync(rsd_ctx* ctx, rsd_csr* A);     // SELL values current (from CSR if needed)
+int csr_sync(rsd_ctx* ctx, rsd_csr* A);      // CSR values current (from SELL if needed)
+int f32_sync(rsd_ctx* ctx, rsd_csr* A);      // FP32 copy current, in the execution layout
+int exec_sync(rsd_ctx* ctx, rsd_csr* A);     // FP64 values current in the execution layout
+}  // namespace rsd
 
 namespace rsd {
 
@@ -163,6 +186,9 @@ struct rsd_heat {
 	int64_t nbElems = 0;
 	double* gPrev = nullptr;        // device: Dirichlet values at the previous time (time-dependent BCs)
 	bool gPrevValid = false;
+	int32_t* slots = nullptr;       // device: element -> CSR position map for K's pattern
+	int32_t slotStride = 0;
+	bool slotsTried = false;
 	// stage scratch
 	double *F = nullptr, *R = nullptr, *Udot = nullptr, *ms = nullptr, *dU = nullptr;
 	double dt = 0.0;

@@ -1,5 +1,6 @@
 // Device building blocks shared by the kernels: warp/block reductions, the deterministic
-// last-block-done grid reduction, streaming loads, the CSR row product and the expression VM.
+// last-block-done grid reduction, L2-hinted loads, the CSR / SELL-32 row products and the
+// expression VM.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -16,6 +17,54 @@ template <typename T>
 __device__ __forceinline__ T ld_stream(const T* p) { return __ldcs(p); }
 template <typename T>
 __device__ __forceinline__ T ld_ro(const T* p) { return __ldg(p); }
+
+// ---- explicit L2 eviction priorities -------------------------------------------------------
+// The Krylov loops stream the matrix (hundreds of MB) and several vectors per iteration through
+// L2, while the SpMV gathers one vector (p) at column indices.  If other vector traffic evicts p,
+// the gathers turn into latency-bound DRAM misses (measured: 147 us -> 265 us for the FP64 128^3
+// SpMV after three vector writes).  So: matrix streams and single-use vector traffic are loaded and
+// stored evict-first, the gathered vector evict-last.
+struct L2Pol {
+	uint64_t first, last;
+};
+__device__ __forceinline__ L2Pol make_l2pol() {
+	L2Pol p;
+	asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p.first));
+	asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p.last));
+	return p;
+}
+__device__ __forceinline__ double ldh(const double* a, uint64_t pol) {
+	double v;
+	asm volatile("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+	return v;
+}
+__device__ __forceinline__ float ldh(const float* a, uint64_t pol) {
+	float v;
+	asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+	return v;
+}
+__device__ __forceinline__ int32_t ldh(const int32_t* a, uint64_t pol) {
+	int32_t v;
+	asm volatile("ld.global.nc.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
+	return v;
+}
+// coherent (non-.nc) load, for data written earlier in the same kernel's lifetime by other blocks
+__device__ __forceinline__ double ldh_rw(const double* a, uint64_t pol) {
+	double v;
+	asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+	return v;
+}
+__device__ __forceinline__ float ldh_rw(const float* a, uint64_t pol) {
+	float v;
+	asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+	return v;
+}
+__device__ __forceinline__ void sth(double* a, double v, uint64_t pol) {
+	asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(a), "d"(v), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void sth(float* a, float v, uint64_t pol) {
+	asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(a), "f"(v), "l"(pol) : "memory");
+}
 
 template <int W, typename T>
 __device__ __forceinline__ T group_sum(T v) {
@@ -72,19 +121,57 @@ __device__ __forceinline__ bool grid_sum(double (&v)[NCH], double* partials, uns
 	return threadIdx.x == 0;
 }
 
-// one CSR row times x by a group of L lanes; every lane of the group returns the full sum
-template <int L, typename T, typename AccT>
-__device__ __forceinline__ AccT csr_row(const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
-                                       const T* __restrict__ val, const T* __restrict__ x, int64_t row, int64_t n,
-                                       int lane) {
+// The matrix as a kernel sees it: CSR (ptr = row pointer) or SELL-32 (ptr = slice starts), with
+// the values in the precision of the kernel.
+template <typename T>
+struct MatView {
+	const int32_t* __restrict__ ptr;
+	const int32_t* __restrict__ col;
+	const T* __restrict__ val;
+};
+
+// sum over one row of val * xf(column).  L == 0: SELL-32, one thread per row (entries 32 slots
+// apart, so a warp's value/column loads are contiguous); L > 0: CSR with a group of L lanes per row,
+// every lane of the group receiving the total.  Values and columns stream evict-first; xf reads the
+// gathered vector with evict-last.
+template <int L, typename T, typename AccT, typename XF>
+__device__ __forceinline__ AccT row_sum(const MatView<T>& A, int64_t row, int64_t n, int lane, const L2Pol& pol, XF xf) {
 	AccT s = AccT(0);
 	if (row < n) {
-		const int b = rp[row], e = rp[row + 1];
+		int q, e, st;
+		if constexpr (L == 0) {
+			const int64_t sl = row >> 5;
+			q = A.ptr[sl] + (int)(row & 31); e = A.ptr[sl + 1]; st = 32;
+		} else {
+			q = A.ptr[row] + lane; e = A.ptr[row + 1]; st = L;
+		}
 #pragma unroll 4
-		for (int p = b + lane; p < e; p += L) s += (AccT)ld_stream(val + p) * (AccT)ld_ro(x + ld_stream(col + p));
+		for (; q < e; q += st) s += (AccT)ldh(A.val + q, pol.first) * xf(ldh(A.col + q, pol.first));
 	}
-	return group_sum<L>(s);
+	if constexpr (L > 1) s = group_sum<L>(s);
+	return s;
 }
+
+template <int L, typename T, typename AccT>
+__device__ __forceinline__ AccT row_dot(const MatView<T>& A, const T* __restrict__ x, int64_t row, int64_t n, int lane, const L2Pol& pol) {
+	return row_sum<L, T, AccT>(A, row, n, lane, pol, [&](int c) { return (AccT)ldh(x + c, pol.last); });
+}
+
+// Row-loop geometry shared by the row kernels: a group of G = max(L,1) threads per row, rows
+// handed out warp by warp so that a warp's rows are consecutive (a whole SELL slice when L == 0).
+template <int L>
+struct RowLoop {
+	static constexpr int G = L ? L : 1;
+	int lane;
+	int64_t base, step, sub;
+	__device__ __forceinline__ RowLoop() {
+		lane = threadIdx.x & (G - 1);
+		sub = (threadIdx.x & 31) / G;
+		const int64_t g0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / G;
+		base = g0 - sub;
+		step = ((int64_t)gridDim.x * blockDim.x) / G;
+	}
+};
 
 // expression stack machine (bytecode from compile_expr)
 __device__ __forceinline__ double eval_expr(const DevExpr& e, double t, double x, double y, double z, double T) {
@@ -114,6 +201,29 @@ __device__ __forceinline__ double eval_expr(const DevExpr& e, double t, double x
 	}
 	return e.n ? st[0] : 0.0;
 }
+
+// lanes per row of the execution layout: 0 for SELL-32, else the CSR group size
+inline int exec_lanes(const rsd_csr* A) { return A->format == 0 ? 0 : default_lanes(A); }
+inline MatView<double> view64(const rsd_csr* A) {
+	return A->format == 0 ? MatView<double>{A->sStart, A->sCol, A->sVal} : MatView<double>{A->rowPtr, A->col, A->val};
+}
+inline MatView<float> view32(const rsd_csr* A) {
+	return MatView<float>{A->format == 0 ? A->sStart : A->rowPtr, A->format == 0 ? A->sCol : A->col, A->val32};
+}
+// diagonal position and values of the execution layout
+inline const int32_t* exec_diag(const rsd_csr* A) { return A->format == 0 ? A->sDiag : A->diag; }
+inline const double* exec_val(const rsd_csr* A) { return A->format == 0 ? A->sVal : A->val; }
+
+#define RSD_DISPATCH_L(L, CALL)                          \
+	switch (L) {                                         \
+		case 0: { constexpr int LL = 0; CALL; } break;   \
+		case 1: { constexpr int LL = 1; CALL; } break;   \
+		case 2: { constexpr int LL = 2; CALL; } break;   \
+		case 4: { constexpr int LL = 4; CALL; } break;   \
+		case 8: { constexpr int LL = 8; CALL; } break;   \
+		case 16: { constexpr int LL = 16; CALL; } break; \
+		default: { constexpr int LL = 32; CALL; } break; \
+	}
 
 inline int vec_grid(const rsd_ctx* ctx, int64_t n, int threads = 256) {
 	int64_t b = (n + threads - 1) / threads;

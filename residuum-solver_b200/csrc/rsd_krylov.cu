@@ -29,23 +29,21 @@ __device__ __forceinline__ bool is_done(const CgScal* S) { return *((volatile co
 // ---- FP64 PCG: linalg/solver/iterative/cg/Solver.tpp:13-119 ----------------------------------
 // r = b - A x; z = M r; p = z; rz = r.z; res0 = |r|   (Solver.tpp:31-63)
 template <int L>
-__global__ void __launch_bounds__(256) k_cg_init(int64_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
-                                                 const double* __restrict__ val, const double* __restrict__ b,
+__global__ void __launch_bounds__(256) k_cg_init(int64_t n, MatView<double> A, const double* __restrict__ b,
                                                  const double* __restrict__ x, double* __restrict__ r, double* __restrict__ p,
                                                  const double* __restrict__ invD, CgScal* S, double* partials, double tol,
                                                  int relMode, int64_t maxIters) {
-	const int lane = threadIdx.x & (L - 1);
-	const int64_t g0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / L, gs = ((int64_t)gridDim.x * blockDim.x) / L;
-	const int64_t warp0 = g0 - ((threadIdx.x & 31) / L);
+	const L2Pol pol = make_l2pol();
+	const RowLoop<L> rl;
 	double v[2] = {0.0, 0.0};
-	for (int64_t base = warp0; base < n; base += gs) {
-		const int64_t row = base + ((threadIdx.x & 31) / L);
-		const double ax = csr_row<L, double, double>(rp, col, val, x, row, n, lane);
-		if (lane == 0 && row < n) {
-			const double ri = b[row] + (-1.0) * ax;
-			const double zi = invD ? ri * invD[row] : ri;
-			r[row] = ri;
-			p[row] = zi;
+	for (int64_t base = rl.base; base < n; base += rl.step) {
+		const int64_t row = base + rl.sub;
+		const double ax = row_dot<L, double, double>(A, x, row, n, rl.lane, pol);
+		if (rl.lane == 0 && row < n) {
+			const double ri = ldh(b + row, pol.first) + (-1.0) * ax;
+			const double zi = invD ? ri * ldh(invD + row, pol.first) : ri;
+			sth(r + row, ri, pol.first);
+			sth(p + row, zi, pol.last);
 			v[0] += ri * ri;
 			v[1] += ri * zi;
 		}
@@ -63,18 +61,16 @@ __global__ void __launch_bounds__(256) k_cg_init(int64_t n, const int32_t* __res
 
 // Ap = A p; alpha = rz / p.Ap   (Solver.tpp:69-73)
 template <int L>
-__global__ void __launch_bounds__(256) k_cg_spmv_dot(int64_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
-                                                     const double* __restrict__ val, const double* __restrict__ p,
+__global__ void __launch_bounds__(256) k_cg_spmv_dot(int64_t n, MatView<double> A, const double* __restrict__ p,
                                                      double* __restrict__ Ap, CgScal* S, double* partials) {
 	if (is_done(S)) return;
-	const int lane = threadIdx.x & (L - 1);
-	const int64_t g0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / L, gs = ((int64_t)gridDim.x * blockDim.x) / L;
-	const int64_t warp0 = g0 - ((threadIdx.x & 31) / L);
+	const L2Pol pol = make_l2pol();
+	const RowLoop<L> rl;
 	double v[1] = {0.0};
-	for (int64_t base = warp0; base < n; base += gs) {
-		const int64_t row = base + ((threadIdx.x & 31) / L);
-		const double s = csr_row<L, double, double>(rp, col, val, p, row, n, lane);
-		if (lane == 0 && row < n) { Ap[row] = s; v[0] += p[row] * s; }
+	for (int64_t base = rl.base; base < n; base += rl.step) {
+		const int64_t row = base + rl.sub;
+		const double s = row_dot<L, double, double>(A, p, row, n, rl.lane, pol);
+		if (rl.lane == 0 && row < n) { sth(Ap + row, s, pol.first); v[0] += ldh(p + row, pol.last) * s; }
 	}
 	if (grid_sum<1>(v, partials, &S->ticket)) {
 		S->pAp = v[0];
@@ -90,12 +86,13 @@ __global__ void __launch_bounds__(256) k_cg_update(int64_t n, double* __restrict
                                                    int relMode, int64_t maxIters) {
 	if (is_done(S)) return;
 	const double alpha = S->alpha;
+	const L2Pol pol = make_l2pol();
 	double v[2] = {0.0, 0.0};
 	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-		x[i] += alpha * p[i];
-		const double ri = r[i] + (-alpha) * Ap[i];
-		r[i] = ri;
-		const double zi = invD ? ri * invD[i] : ri;
+		sth(x + i, ldh_rw(x + i, pol.first) + alpha * ldh(p + i, pol.first), pol.first);
+		const double ri = ldh_rw(r + i, pol.first) + (-alpha) * ldh(Ap + i, pol.first);
+		sth(r + i, ri, pol.first);
+		const double zi = invD ? ri * ldh(invD + i, pol.first) : ri;
 		v[0] += ri * ri;
 		v[1] += ri * zi;
 	}
@@ -117,9 +114,11 @@ __global__ void __launch_bounds__(256) k_cg_pupdate(int64_t n, double* __restric
                                                     const double* __restrict__ invD, const CgScal* S) {
 	if (is_done(S)) return;
 	const double beta = S->beta;
+	const L2Pol pol = make_l2pol();
 	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-		const double zi = invD ? r[i] * invD[i] : r[i];
-		p[i] = p[i] * beta + 1.0 * zi;
+		const double ri = ldh(r + i, pol.first);
+		const double zi = invD ? ri * ldh(invD + i, pol.first) : ri;
+		sth(p + i, ldh_rw(p + i, pol.first) * beta + 1.0 * zi, pol.last);   // the next SpMV gathers p
 	}
 }
 
@@ -128,35 +127,23 @@ __global__ void __launch_bounds__(256) k_cg_pupdate(int64_t n, double* __restric
 // residual drops by `delta` since the last replacement, or claims convergence, the true residual
 // r = b - A64 (x + y) is recomputed in FP64 and replaces the recurrence residual; the FP32
 // correction y is folded into x.  Convergence is declared on the FP64 residual only.
-// r0 = b - A64 x in FP64; when val32 is given the same pass writes the FP32 copy of the values
+// r0 = b - A64 x in FP64
 template <int L>
-__global__ void __launch_bounds__(256) k_mx_init(int64_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
-                                                 const double* __restrict__ val, float* __restrict__ val32,
-                                                 const double* __restrict__ b,
+__global__ void __launch_bounds__(256) k_mx_init(int64_t n, MatView<double> A, const double* __restrict__ b,
                                                  const double* __restrict__ x, float* __restrict__ r, float* __restrict__ p,
                                                  float* __restrict__ y, const float* __restrict__ invD, CgScal* S,
                                                  double* partials, double tol, int relMode, int64_t maxIters) {
-	const int lane = threadIdx.x & (L - 1);
-	const int64_t g0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / L, gs = ((int64_t)gridDim.x * blockDim.x) / L;
-	const int64_t warp0 = g0 - ((threadIdx.x & 31) / L);
+	const L2Pol pol = make_l2pol();
+	const RowLoop<L> rl;
 	double v[2] = {0.0, 0.0};
-	for (int64_t base = warp0; base < n; base += gs) {
-		const int64_t row = base + ((threadIdx.x & 31) / L);
-		double ax = 0.0;
-		if (row < n) {
-			const int bb = rp[row], e = rp[row + 1];
-			for (int q = bb + lane; q < e; q += L) {
-				const double a = ld_stream(val + q);
-				if (val32) val32[q] = (float)a;
-				ax += a * ld_ro(x + ld_stream(col + q));
-			}
-		}
-		ax = group_sum<L>(ax);
-		if (lane == 0 && row < n) {
-			const double r64 = b[row] - ax;
+	for (int64_t base = rl.base; base < n; base += rl.step) {
+		const int64_t row = base + rl.sub;
+		const double ax = row_dot<L, double, double>(A, x, row, n, rl.lane, pol);
+		if (rl.lane == 0 && row < n) {
+			const double r64 = ldh(b + row, pol.first) - ax;
 			const float ri = (float)r64;
-			const float zi = invD ? ri * invD[row] : ri;
-			r[row] = ri; p[row] = zi; y[row] = 0.0f;
+			const float zi = invD ? ri * ldh(invD + row, pol.first) : ri;
+			sth(r + row, ri, pol.first); sth(p + row, zi, pol.last); sth(y + row, 0.0f, pol.first);
 			v[0] += r64 * r64;
 			v[1] += (double)ri * (double)zi;
 		}
@@ -173,19 +160,17 @@ __global__ void __launch_bounds__(256) k_mx_init(int64_t n, const int32_t* __res
 }
 
 template <int L>
-__global__ void __launch_bounds__(256) k_mx_spmv_dot(int64_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
-                                                     const float* __restrict__ val, const float* __restrict__ p,
+__global__ void __launch_bounds__(256) k_mx_spmv_dot(int64_t n, MatView<float> A, const float* __restrict__ p,
                                                      float* __restrict__ Ap, CgScal* S, double* partials) {
 	if (is_done(S)) return;
 	if (blockIdx.x == 0 && threadIdx.x == 0) { S->reliable = 0; S->apply_xy = 0; }
-	const int lane = threadIdx.x & (L - 1);
-	const int64_t g0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / L, gs = ((int64_t)gridDim.x * blockDim.x) / L;
-	const int64_t warp0 = g0 - ((threadIdx.x & 31) / L);
+	const L2Pol pol = make_l2pol();
+	const RowLoop<L> rl;
 	double v[1] = {0.0};
-	for (int64_t base = warp0; base < n; base += gs) {
-		const int64_t row = base + ((threadIdx.x & 31) / L);
-		const float s = csr_row<L, float, float>(rp, col, val, p, row, n, lane);
-		if (lane == 0 && row < n) { Ap[row] = s; v[0] += (double)p[row] * (double)s; }
+	for (int64_t base = rl.base; base < n; base += rl.step) {
+		const int64_t row = base + rl.sub;
+		const float s = row_dot<L, float, float>(A, p, row, n, rl.lane, pol);
+		if (rl.lane == 0 && row < n) { sth(Ap + row, s, pol.first); v[0] += (double)ldh(p + row, pol.last) * (double)s; }
 	}
 	if (grid_sum<1>(v, partials, &S->ticket)) {
 		S->pAp = v[0];
@@ -200,12 +185,13 @@ __global__ void __launch_bounds__(256) k_mx_update(int64_t n, float* __restrict_
                                                    int relMode, int64_t maxIters, double delta) {
 	if (is_done(S)) return;
 	const float alpha = (float)S->alpha;
+	const L2Pol pol = make_l2pol();
 	double v[2] = {0.0, 0.0};
 	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-		y[i] += alpha * p[i];
-		const float ri = r[i] - alpha * Ap[i];
-		r[i] = ri;
-		const float zi = invD ? ri * invD[i] : ri;
+		sth(y + i, ldh_rw(y + i, pol.first) + alpha * ldh(p + i, pol.first), pol.first);
+		const float ri = ldh_rw(r + i, pol.first) - alpha * ldh(Ap + i, pol.first);
+		sth(r + i, ri, pol.first);
+		const float zi = invD ? ri * ldh(invD + i, pol.first) : ri;
 		v[0] += (double)ri * (double)ri;
 		v[1] += (double)ri * (double)zi;
 	}
@@ -225,32 +211,23 @@ __global__ void __launch_bounds__(256) k_mx_update(int64_t n, float* __restrict_
 
 // reliable update: r64 = b - A64 (x + y), r = (float) r64, rz with the new r
 template <int L>
-__global__ void __launch_bounds__(256) k_mx_reliable(int64_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
-                                                     const double* __restrict__ val, const double* __restrict__ b,
+__global__ void __launch_bounds__(256) k_mx_reliable(int64_t n, MatView<double> A, const double* __restrict__ b,
                                                      const double* __restrict__ x, const float* __restrict__ y,
                                                      float* __restrict__ r, const float* __restrict__ invD, CgScal* S,
                                                      double* partials, double tol, int relMode, int64_t maxIters) {
 	if (is_done(S) || !*((volatile const int32_t*)&S->reliable)) return;
-	const int lane = threadIdx.x & (L - 1);
-	const int64_t g0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / L, gs = ((int64_t)gridDim.x * blockDim.x) / L;
-	const int64_t warp0 = g0 - ((threadIdx.x & 31) / L);
+	const L2Pol pol = make_l2pol();
+	const RowLoop<L> rl;
 	double v[2] = {0.0, 0.0};
-	for (int64_t base = warp0; base < n; base += gs) {
-		const int64_t row = base + ((threadIdx.x & 31) / L);
-		double s = 0.0;
-		if (row < n) {
-			const int bb = rp[row], e = rp[row + 1];
-			for (int q = bb + lane; q < e; q += L) {
-				const int c = ld_stream(col + q);
-				s += ld_stream(val + q) * (ld_ro(x + c) + (double)ld_ro(y + c));
-			}
-		}
-		s = group_sum<L>(s);
-		if (lane == 0 && row < n) {
-			const double r64 = b[row] - s;
+	for (int64_t base = rl.base; base < n; base += rl.step) {
+		const int64_t row = base + rl.sub;
+		const double s = row_sum<L, double, double>(A, row, n, rl.lane, pol,
+		                                            [&](int c) { return ldh(x + c, pol.last) + (double)ldh(y + c, pol.last); });
+		if (rl.lane == 0 && row < n) {
+			const double r64 = ldh(b + row, pol.first) - s;
 			const float ri = (float)r64;
-			const float zi = invD ? ri * invD[row] : ri;
-			r[row] = ri;
+			const float zi = invD ? ri * ldh(invD + row, pol.first) : ri;
+			sth(r + row, ri, pol.first);
 			v[0] += r64 * r64;
 			v[1] += (double)ri * (double)zi;
 		}
@@ -277,11 +254,16 @@ __global__ void __launch_bounds__(256) k_mx_pupdate(int64_t n, double* __restric
 	const int done = is_done(S);
 	if (!apply && done) return;
 	const float beta = (float)S->beta;
+	const L2Pol pol = make_l2pol();
 	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-		if (apply) { x[i] = x[i] + (double)y[i]; y[i] = 0.0f; }
+		if (apply) {
+			sth(x + i, ldh_rw(x + i, pol.first) + (double)ldh_rw(y + i, pol.first), pol.first);
+			sth(y + i, 0.0f, pol.first);
+		}
 		if (!done) {
-			const float zi = invD ? r[i] * invD[i] : r[i];
-			p[i] = p[i] * beta + zi;
+			const float ri = ldh(r + i, pol.first);
+			const float zi = invD ? ri * ldh(invD + i, pol.first) : ri;
+			sth(p + i, ldh_rw(p + i, pol.first) * beta + zi, pol.last);   // the next SpMV gathers p
 		}
 	}
 }
@@ -303,17 +285,15 @@ __global__ void k_invdiag64(int64_t n, const int32_t* __restrict__ dpos, const d
 
 // ||b - A x|| in FP64 (device scalar)
 template <int L>
-__global__ void __launch_bounds__(256) k_true_res(int64_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
-                                                  const double* __restrict__ val, const double* __restrict__ b,
+__global__ void __launch_bounds__(256) k_true_res(int64_t n, MatView<double> A, const double* __restrict__ b,
                                                   const double* __restrict__ x, double* partials, unsigned* ticket, double* out) {
-	const int lane = threadIdx.x & (L - 1);
-	const int64_t g0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / L, gs = ((int64_t)gridDim.x * blockDim.x) / L;
-	const int64_t warp0 = g0 - ((threadIdx.x & 31) / L);
+	const L2Pol pol = make_l2pol();
+	const RowLoop<L> rl;
 	double v[1] = {0.0};
-	for (int64_t base = warp0; base < n; base += gs) {
-		const int64_t row = base + ((threadIdx.x & 31) / L);
-		const double ax = csr_row<L, double, double>(rp, col, val, x, row, n, lane);
-		if (lane == 0 && row < n) { const double ri = b[row] - ax; v[0] += ri * ri; }
+	for (int64_t base = rl.base; base < n; base += rl.step) {
+		const int64_t row = base + rl.sub;
+		const double ax = row_dot<L, double, double>(A, x, row, n, rl.lane, pol);
+		if (rl.lane == 0 && row < n) { const double ri = ldh(b + row, pol.first) - ax; v[0] += ri * ri; }
 	}
 	if (grid_sum<1>(v, partials, ticket)) *out = sqrt(v[0]);
 }
@@ -339,7 +319,7 @@ static int get_ws(rsd_ctx* ctx, size_t bytes, void** out) {
 }
 
 static int row_blocks(const rsd_ctx* ctx, int64_t n, int L, int block = 256) {
-	int64_t b = (n * L + block - 1) / block;
+	int64_t b = (n * std::max(L, 1) + block - 1) / block;
 	b = std::min<int64_t>(b, std::min<int64_t>(kMaxPartials, (int64_t)ctx->num_sms * (2048 / block)));
 	return (int)std::max<int64_t>(b, 1);
 }
@@ -348,16 +328,6 @@ static int vec_blocks(const rsd_ctx* ctx, int64_t n) {
 	b = std::min<int64_t>(b, std::min<int64_t>(kMaxPartials, (int64_t)ctx->num_sms * 8));
 	return (int)std::max<int64_t>(b, 1);
 }
-
-#define RSD_DISPATCH_L(L, CALL)                      \
-	switch (L) {                                     \
-		case 1: { constexpr int LL = 1; CALL; } break;  \
-		case 2: { constexpr int LL = 2; CALL; } break;  \
-		case 4: { constexpr int LL = 4; CALL; } break;  \
-		case 8: { constexpr int LL = 8; CALL; } break;  \
-		case 16: { constexpr int LL = 16; CALL; } break; \
-		default: { constexpr int LL = 32; CALL; } break; \
-	}
 
 static int finish_report(rsd_ctx* ctx, CgScal* S, rsd_report* rep) {
 	CgScal h;
@@ -415,7 +385,9 @@ struct Poller {
 
 static int cg_fp64(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const double* b, double* x, rsd_report* rep) {
 	const int64_t n = A->n;
-	const int L = default_lanes(A);
+	RSD_CHECK(exec_sync(ctx, A));
+	const int L = exec_lanes(A);
+	const MatView<double> V = view64(A);
 	void* wsv;
 	RSD_CHECK(get_ws(ctx, sizeof(double) * (4 * n + 64), &wsv));
 	double* r = (double*)wsv;
@@ -427,8 +399,8 @@ static int cg_fp64(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const do
 	const int rel = cfg->tol_type == RSD_TOL_RELATIVE;
 	const int gr = row_blocks(ctx, n, L), gv = vec_blocks(ctx, n);
 	// Jacobi::update on every solve (cg/Solver.tpp:22)
-	if (invD) k_invdiag64<<<gv, 256, 0, ctx->stream>>>(n, A->diag, A->val, invD);
-	RSD_DISPATCH_L(L, (k_cg_init<LL><<<gr, 256, 0, ctx->stream>>>(n, A->rowPtr, A->col, A->val, b, x, r, p, invD, S, ctx->s.partials, cfg->tol, rel, cfg->max_iters)));
+	if (invD) k_invdiag64<<<gv, 256, 0, ctx->stream>>>(n, exec_diag(A), exec_val(A), invD);
+	RSD_DISPATCH_L(L, (k_cg_init<LL><<<gr, 256, 0, ctx->stream>>>(n, V, b, x, r, p, invD, S, ctx->s.partials, cfg->tol, rel, cfg->max_iters)));
 	RSD_CUDA(cudaGetLastError());
 	Poller poll{ctx, S, (int32_t*)ctx->s.hbuf};
 	RSD_CHECK(poll.init());
@@ -438,7 +410,7 @@ static int cg_fp64(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const do
 	for (int64_t it = 0; it < cfg->max_iters + 2 * chunk && !fin; it += chunk) {
 		for (int c = 0; c < chunk; ++c) {
 			int pr = prof_begin(ctx, PF_SPMV_DOT_F64);
-			RSD_DISPATCH_L(L, (k_cg_spmv_dot<LL><<<gr, 256, 0, ctx->stream>>>(n, A->rowPtr, A->col, A->val, p, Ap, S, ctx->s.partials)));
+			RSD_DISPATCH_L(L, (k_cg_spmv_dot<LL><<<gr, 256, 0, ctx->stream>>>(n, V, p, Ap, S, ctx->s.partials)));
 			prof_end(ctx, pr);
 			int pu = prof_begin(ctx, PF_CG_UPDATE);
 			k_cg_update<<<gv, 256, 0, ctx->stream>>>(n, x, r, p, Ap, invD, S, ctx->s.partials, cfg->tol, rel, cfg->max_iters);
@@ -455,7 +427,7 @@ static int cg_fp64(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const do
 	discard_idle(ctx, pairs, 3, rep ? rep->iterations : 0);
 	// FP64 check of the final iterate: ||b - A x|| / ||r0||
 	double* tr = &scal_slot(ctx, 1)->res;
-	RSD_DISPATCH_L(L, (k_true_res<LL><<<gr, 256, 0, ctx->stream>>>(n, A->rowPtr, A->col, A->val, b, x, ctx->s.partials, &scal_slot(ctx, 1)->ticket, tr)));
+	RSD_DISPATCH_L(L, (k_true_res<LL><<<gr, 256, 0, ctx->stream>>>(n, V, b, x, ctx->s.partials, &scal_slot(ctx, 1)->ticket, tr)));
 	RSD_CUDA(cudaGetLastError());
 	double h = 0.0;
 	RSD_CUDA(cudaMemcpyAsync(&h, tr, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -466,10 +438,10 @@ static int cg_fp64(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const do
 
 static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const double* b, double* x, rsd_report* rep) {
 	const int64_t n = A->n;
-	const int L = default_lanes(A);
-	float* refresh32 = nullptr;   // FP32 copy stale: rebuild it inside the initial-residual pass
-	if (!A->val32) RSD_CUDA(cudaMalloc(&A->val32, sizeof(float) * std::max<int64_t>(A->nnz, 1)));
-	if (A->version32 != A->version) { refresh32 = A->val32; A->version32 = A->version; }
+	RSD_CHECK(f32_sync(ctx, A));
+	const int L = exec_lanes(A);
+	const MatView<double> V = view64(A);
+	const MatView<float> V32 = view32(A);
 	void* wsv;
 	RSD_CHECK(get_ws(ctx, sizeof(float) * (5 * n + 64), &wsv));
 	float* r = (float*)wsv;
@@ -482,8 +454,8 @@ static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const d
 	const int rel = cfg->tol_type == RSD_TOL_RELATIVE;
 	const double delta = cfg->reliable_delta > 0 ? cfg->reliable_delta : 0.1;
 	const int gr = row_blocks(ctx, n, L), gv = vec_blocks(ctx, n);
-	if (invD) k_invdiag32<<<gv, 256, 0, ctx->stream>>>(n, A->diag, A->val, invD);
-	RSD_DISPATCH_L(L, (k_mx_init<LL><<<gr, 256, 0, ctx->stream>>>(n, A->rowPtr, A->col, A->val, refresh32, b, x, r, p, y, invD, S, ctx->s.partials, cfg->tol, rel, cfg->max_iters)));
+	if (invD) k_invdiag32<<<gv, 256, 0, ctx->stream>>>(n, exec_diag(A), exec_val(A), invD);
+	RSD_DISPATCH_L(L, (k_mx_init<LL><<<gr, 256, 0, ctx->stream>>>(n, V, b, x, r, p, y, invD, S, ctx->s.partials, cfg->tol, rel, cfg->max_iters)));
 	RSD_CUDA(cudaGetLastError());
 	Poller poll{ctx, S, (int32_t*)ctx->s.hbuf};
 	RSD_CHECK(poll.init());
@@ -493,13 +465,13 @@ static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const d
 	for (int64_t it = 0; it < cfg->max_iters + 2 * chunk && !fin; it += chunk) {
 		for (int c = 0; c < chunk; ++c) {
 			int pr = prof_begin(ctx, PF_SPMV_DOT_F32);
-			RSD_DISPATCH_L(L, (k_mx_spmv_dot<LL><<<gr, 256, 0, ctx->stream>>>(n, A->rowPtr, A->col, A->val32, p, Ap, S, ctx->s.partials)));
+			RSD_DISPATCH_L(L, (k_mx_spmv_dot<LL><<<gr, 256, 0, ctx->stream>>>(n, V32, p, Ap, S, ctx->s.partials)));
 			prof_end(ctx, pr);
 			int pu = prof_begin(ctx, PF_CG_UPDATE);
 			k_mx_update<<<gv, 256, 0, ctx->stream>>>(n, y, r, p, Ap, invD, S, ctx->s.partials, cfg->tol, rel, cfg->max_iters, delta);
 			prof_end(ctx, pu);
 			int pq = prof_begin(ctx, PF_RELIABLE);
-			RSD_DISPATCH_L(L, (k_mx_reliable<LL><<<gr, 256, 0, ctx->stream>>>(n, A->rowPtr, A->col, A->val, b, x, y, r, invD, S, ctx->s.partials, cfg->tol, rel, cfg->max_iters)));
+			RSD_DISPATCH_L(L, (k_mx_reliable<LL><<<gr, 256, 0, ctx->stream>>>(n, V, b, x, y, r, invD, S, ctx->s.partials, cfg->tol, rel, cfg->max_iters)));
 			prof_end(ctx, pq);
 			int pp = prof_begin(ctx, PF_CG_PUPDATE);
 			k_mx_pupdate<<<gv, 256, 0, ctx->stream>>>(n, x, y, p, r, invD, S);
@@ -572,7 +544,8 @@ static int gmres_fp64(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const
 	const double breakdownTol = 1e-14, eps = 1e-50;
 	std::vector<double> H((m + 1) * m, 0.0), cs(m), sn(m), g(m + 1), yv(m), col(m + 2);
 	auto Hat = [&](int64_t i, int64_t j) -> double& { return H[j * (m + 1) + i]; };
-	if (invD) k_invdiag64<<<gv, 256, 0, ctx->stream>>>(n, A->diag, A->val, invD);
+	RSD_CHECK(exec_sync(ctx, A));
+	if (invD) k_invdiag64<<<gv, 256, 0, ctx->stream>>>(n, exec_diag(A), exec_val(A), invD);
 	auto residual = [&](double* beta) -> int {
 		RSD_CHECK(spmv_f64(ctx, A, x, w));
 		k_resid<<<gv, 256, 0, ctx->stream>>>(n, b, w, Q);

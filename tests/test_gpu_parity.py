@@ -146,12 +146,53 @@ def test_spmv_matches_reference(rsd, ctx, n, per_row):
         A.spmv(xd, yd)
         assert relerr(yd.download(), y_ref) <= 1e-13
     # FP32 values and vector: error bounded by the row's absolute sum times a few FP32 ulps
-    A.set_launch(0, 0)
-    A.sync_f32()
-    x32, y32 = ctx.to_device(x.astype(np.float32)), ctx.array(n, np.float32)
-    A.spmv_f32(x32, y32)
     bound = 4 * np.finfo(np.float32).eps * oracle.spmv(rp, col, np.abs(val), np.abs(x)) * (rp[1:] - rp[:-1]).max()
-    assert (np.abs(y32.download() - y_ref) <= bound + 1e-30).all()
+    x32, y32 = ctx.to_device(x.astype(np.float32)), ctx.array(n, np.float32)
+    for lanes in (0, 4):
+        A.set_launch(lanes, 0)
+        A.sync_f32()
+        A.spmv_f32(x32, y32)
+        assert (np.abs(y32.download() - y_ref) <= bound + 1e-30).all()
+
+
+def test_layouts_stay_in_step(rsd, ctx):
+    # Values live in CSR (API order) and SELL-32 (execution order); every write through one layout
+    # must be seen through the other, in FP64 and in the FP32 copy.
+    h = make_heat(rsd, ctx, 3, 1, 2, [9, 7, 5], [0, 0, 0], [1, 1, 1], dirichlet={0: "0", 1: "0"})
+    m = oracle.BlockMesh(3, [9, 7, 5], [0, 0, 0], [1, 1, 1], 1)
+    o = oracle.Oracle(m, 2, bc={0: "0", 1: "0"})
+    rp, col = h.K.pattern()
+    n = h.n
+    h.assemble_matrix(1.0, 3.0)                      # scatter lands in SELL
+    v = o.assemble_matrix(1.0, 3.0)
+    x = np.random.default_rng(4).standard_normal(n)
+    xd, yd = ctx.to_device(x), ctx.array(n)
+    for lanes in (0, 4):
+        h.K.set_launch(lanes, 0)
+        h.K.spmv(xd, yd)
+        assert relerr(yd.download(), oracle.spmv(rp, col, v, x)) <= REL
+    assert relerr(h.K.values(), v) <= REL          # SELL -> CSR
+    h.K.set_values(2.0 * v)                          # CSR -> SELL
+    d = ctx.array(n)
+    for lanes in (0, 8):
+        h.K.set_launch(lanes, 0)
+        h.K.spmv(xd, yd)
+        assert relerr(yd.download(), oracle.spmv(rp, col, 2.0 * v, x)) <= REL
+        h.K.diagonal(d)
+        dia = np.array([v[rp[i]:rp[i + 1]][col[rp[i]:rp[i + 1]] == i][0] for i in range(n)])
+        assert relerr(d.download(), 2.0 * dia) == 0.0
+        h.K.lump(d)
+        assert relerr(d.download(), 2.0 * np.add.reduceat(v, rp[:-1])) <= REL
+        # the FP32 copy follows the FP64 values and the layout
+        h.K.sync_f32()
+        x32, y32 = ctx.to_device(x.astype(np.float32)), ctx.array(n, np.float32)
+        h.K.spmv_f32(x32, y32)
+        assert relerr(y32.download(), oracle.spmv(rp, col, 2.0 * v, x)) <= 1e-5
+    h.K.set_launch(0, 0)
+    lanes, block, us = h.K.autotune()
+    assert lanes in (0, 2, 4, 8, 16, 32) and block in (128, 256, 512) and us > 0
+    h.K.spmv(xd, yd)
+    assert relerr(yd.download(), oracle.spmv(rp, col, 2.0 * v, x)) <= REL
 
 
 def test_blas1_matches_numpy(rsd, ctx):
