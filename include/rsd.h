@@ -136,6 +136,17 @@ int rsd_csr_autotune(rsd_ctx* ctx, rsd_csr* A, int32_t* lanes_per_row, int32_t* 
  *      gmres/Solver.tpp:3-170) through LinearSolverRunner::solve(b, x, report)
  *      (linalg/solver/base/LinearSolverRunner.hpp:16); b and x are device vectors. ---- */
 int rsd_solve(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const double* b, double* x, rsd_report* report);
+/* FP64 CG (cfg->type RSD_CG, cfg->precision RSD_FP64; identity or Jacobi) that allocates nothing:
+ * no counterpart in the reference.  Same kernels, grids and reductions as rsd_solve's FP64 CG, so
+ * the same iterates and report, but its scratch (residual, search direction, A p, inverse diagonal,
+ * reduction partials and device scalars) is one file-scope device array of 8 MiB + 19 KiB, which
+ * limits A to at most 262,144 rows; larger matrices are rejected with RSD_EINVAL and a message.
+ * The scalars and reduction tickets that must start at zero are cleared on the stream by each call.
+ * The array is shared by every call on a device: calls that overlap on one device (two host threads,
+ * or two streams in flight) race on it and must be serialized by the caller.  The first call on a
+ * device looks up the array's device address (setup), so make it before any stream capture. */
+int rsd_cg_solve_static(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const double* b, double* x,
+                        rsd_report* report);
 
 /* ---- mesh: mesh::Data (include/mesh/Data.hpp:13-35), host arrays in that layout ---- */
 int rsd_mesh_create(rsd_ctx* ctx, int32_t nsd, int32_t order, int64_t num_nodes, int64_t num_elements,

@@ -96,6 +96,7 @@ SIGNATURES = {
     "rsd_csr_set_launch": [_P, _I32, _I32],
     "rsd_csr_autotune": [_P, _P, C.POINTER(_I32), C.POINTER(_I32), C.POINTER(_D)],
     "rsd_solve": [_P, _P, C.POINTER(SolverConfig), _P, _P, C.POINTER(Report)],
+    "rsd_cg_solve_static": [_P, _P, C.POINTER(SolverConfig), _P, _P, C.POINTER(Report)],
     "rsd_mesh_create": [_P, _I32, _I32, _I64, _I64, _P, _P, _P, C.POINTER(_P)],
     "rsd_mesh_destroy": [_P],
     "rsd_heat_create": [_P, _P, C.POINTER(HeatDesc), C.POINTER(_P)],
@@ -298,6 +299,14 @@ def solve(ctx, A, b, x, cfg=None, **kw):
     cfg = cfg or SolverConfig.make(**kw)
     rep = Report()
     check(lib().rsd_solve(ctx.h, A.h, C.byref(cfg), _ptr(b), _ptr(x), C.byref(rep)))
+    return rep.as_dict()
+
+
+def solve_static(ctx, A, b, x, cfg=None, **kw):
+    """FP64 CG through rsd_cg_solve_static: no allocation, at most 262,144 rows."""
+    cfg = cfg or SolverConfig.make(**kw)
+    rep = Report()
+    check(lib().rsd_cg_solve_static(ctx.h, A.h, C.byref(cfg), _ptr(b), _ptr(x), C.byref(rep)))
     return rep.as_dict()
 
 

@@ -7,6 +7,8 @@
 // per chunk of iterations; kernels of an already-finished solve return immediately.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <mutex>
 #include <vector>
 
 #include "rsd_kernels.cuh"
@@ -630,6 +632,86 @@ static int gmres_fp64(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const
 	return RSD_OK;
 }
 
+// ---- FP64 PCG over a static device scratch ---------------------------------------------------
+// The same kernels, grids and reductions as cg_fp64 (so the same iterates, bit for bit), with every
+// scratch buffer carved from one file-scope device array instead of the context's workspace: the
+// call allocates nothing.  The array is sized for kStaticMaxRows rows; one array per device, shared
+// by every call on that device.
+constexpr int64_t kStaticMaxRows = int64_t(1) << 18;                 // 262,144 rows
+constexpr size_t kStaticHeadBytes = 2 * sizeof(DevScalars) + sizeof(double) * 2 * kMaxPartials;
+constexpr size_t kStaticHeadAligned = (kStaticHeadBytes + 255) & ~size_t(255);
+constexpr size_t kStaticScratchBytes = kStaticHeadAligned + sizeof(double) * 4 * kStaticMaxRows;   // 8 MiB + 19 KiB
+static_assert(sizeof(DevScalars) % 8 == 0, "the partials after the two scalar slots stay 8-byte aligned");
+
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_cg_static_scratch[kStaticScratchBytes];
+
+namespace {
+
+constexpr int kStaticMaxDevices = 64;
+static std::mutex g_static_mu;
+static void* g_static_ptr[kStaticMaxDevices];
+
+// device address of this device's scratch, looked up once per device
+static int static_scratch(rsd_ctx* ctx, unsigned char** out) {
+	if (ctx->device < 0 || ctx->device >= kStaticMaxDevices) return set_error(RSD_EINVAL, "device index out of range for the static scratch table");
+	std::lock_guard<std::mutex> lk(g_static_mu);
+	if (!g_static_ptr[ctx->device]) {
+		void* p = nullptr;
+		const cudaError_t e = cudaGetSymbolAddress(&p, g_cg_static_scratch);
+		if (e != cudaSuccess) return cuda_error(e, "cudaGetSymbolAddress(static CG scratch)");
+		g_static_ptr[ctx->device] = p;
+	}
+	*out = (unsigned char*)g_static_ptr[ctx->device];
+	return RSD_OK;
+}
+
+static int cg_fp64_static(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const double* b, double* x, rsd_report* rep) {
+	const int64_t n = A->n;
+	unsigned char* base = nullptr;
+	RSD_CHECK(static_scratch(ctx, &base));
+	CgScal* S = reinterpret_cast<CgScal*>(base);
+	CgScal* S1 = reinterpret_cast<CgScal*>(base + sizeof(DevScalars));
+	double* partials = reinterpret_cast<double*>(base + 2 * sizeof(DevScalars));
+	double* r = reinterpret_cast<double*>(base + kStaticHeadAligned);
+	double* p = r + n;
+	double* Ap = p + n;
+	double* invD = cfg->precond == RSD_JACOBI ? Ap + n : nullptr;
+	// the reduction tickets and the done/converged flags must start at zero on every call
+	RSD_CUDA(cudaMemsetAsync(base, 0, 2 * sizeof(DevScalars), ctx->stream));
+	RSD_CHECK(exec_sync(ctx, A));
+	const int L = exec_lanes(A);
+	const MatView<double> V = view64(A);
+	const int rel = cfg->tol_type == RSD_TOL_RELATIVE;
+	const int gr = row_blocks(ctx, n, L), gv = vec_blocks(ctx, n);
+	if (invD) k_invdiag64<<<gv, 256, 0, ctx->stream>>>(n, exec_diag(A), exec_val(A), invD);
+	RSD_DISPATCH_L(L, (k_cg_init<LL><<<gr, 256, 0, ctx->stream>>>(n, V, b, x, r, p, invD, S, partials, cfg->tol, rel, cfg->max_iters)));
+	RSD_CUDA(cudaGetLastError());
+	const int chunk = 8;
+	for (int64_t it = 0; it < cfg->max_iters + 2 * chunk; it += chunk) {
+		for (int c = 0; c < chunk; ++c) {
+			RSD_DISPATCH_L(L, (k_cg_spmv_dot<LL><<<gr, 256, 0, ctx->stream>>>(n, V, p, Ap, S, partials)));
+			k_cg_update<<<gv, 256, 0, ctx->stream>>>(n, x, r, p, Ap, invD, S, partials, cfg->tol, rel, cfg->max_iters);
+			k_cg_pupdate<<<gv, 256, 0, ctx->stream>>>(n, p, r, invD, S);
+		}
+		RSD_CUDA(cudaGetLastError());
+		int32_t done = 0;   // pageable host word: the copy returns once the flag has been read
+		RSD_CUDA(cudaMemcpyAsync(&done, &S->done, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+		RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+		if (done) break;
+	}
+	RSD_CHECK(finish_report(ctx, S, rep));
+	double* tr = &S1->res;
+	RSD_DISPATCH_L(L, (k_true_res<LL><<<gr, 256, 0, ctx->stream>>>(n, V, b, x, partials, &S1->ticket, tr)));
+	RSD_CUDA(cudaGetLastError());
+	double h = 0.0;
+	RSD_CUDA(cudaMemcpyAsync(&h, tr, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+	if (rep) rep->trueResidualRel = h / (rep->initialResidual + 1e-50);
+	return RSD_OK;
+}
+
 }  // namespace
 
 int solve(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const double* b, double* x, rsd_report* rep) {
@@ -650,4 +732,23 @@ int solve(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const double* b, 
 
 extern "C" int rsd_solve(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const double* b, double* x, rsd_report* rep) {
 	return rsd::solve(ctx, A, cfg, b, x, rep);
+}
+
+extern "C" int rsd_cg_solve_static(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const double* b, double* x,
+                                   rsd_report* rep) {
+	using namespace rsd;
+	if (!ctx || !A || !cfg || (A->n && (!b || !x))) return set_error(RSD_EINVAL, "null argument");
+	if (cfg->type != RSD_CG || cfg->precision != RSD_FP64)
+		return set_error(RSD_EINVAL, "rsd_cg_solve_static runs FP64 CG only (type RSD_CG, precision RSD_FP64)");
+	if (cfg->max_iters < 0 || !(cfg->tol >= 0)) return set_error(RSD_EINVAL, "bad solver configuration");
+	if (A->n > kStaticMaxRows) {
+		char msg[160];
+		snprintf(msg, sizeof msg, "rsd_cg_solve_static: %lld rows exceed the static scratch limit of %lld rows",
+		         (long long)A->n, (long long)kStaticMaxRows);
+		return set_error(RSD_EINVAL, msg);
+	}
+	if (rep) *rep = rsd_report{};
+	if (A->n == 0) { if (rep) rep->converged = 1; return RSD_OK; }
+	RSD_CUDA(cudaSetDevice(ctx->device));
+	return cg_fp64_static(ctx, A, cfg, b, x, rep);
 }
