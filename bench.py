@@ -310,8 +310,36 @@ def main():
         if dist is not None:
             dist.destroy_process_group()
         return
-    ms_mx, reps_mx, prof_mx, clk = run(cfgs["mixed"], args.steps, args.warmup, profile=True, clocks=clocks)
-    ms_64, reps_64, prof_64, clk64 = run(cfgs["fp64"], args.steps, args.warmup, profile=True, clocks=ClockSampler(local))
+    # timed: the solves run as cached CUDA graphs; then the same steps once more with per-kernel
+    # event timing (plain launches) for the breakdown and the roofline
+    ms_mx, reps_mx, _, clk = run(cfgs["mixed"], args.steps, args.warmup, clocks=clocks)
+    ms_64, reps_64, _, clk64 = run(cfgs["fp64"], args.steps, args.warmup, clocks=ClockSampler(local))
+    _, _, prof_mx, _ = run(cfgs["mixed"], args.steps, args.warmup, profile=True)
+    _, _, prof_64, _ = run(cfgs["fp64"], args.steps, args.warmup, profile=True)
+
+    # time to the FP64-checked 1e-8 residual of the first step's system alone: K + M/dt, b = M U0 / dt,
+    # warm start x0 = U0; median of 5 solves per precision, each from the same x0
+    heat.assemble_matrix(1.0, 1.0 / dt)
+    b = ctx.array(n)
+    U.upload(U0)
+    heat.assemble_vector(2, b, U=U)
+    rsd.check(rsd.lib().rsd_scal(ctx.h, n, 1.0 / dt, b.ptr))
+    x = ctx.array(n)
+    solve_t, solve_it, solve_tr = {}, {}, {}
+    for key in ("mixed", "fp64"):
+        ts = []
+        for rep_i in range(7):
+            rsd.check(rsd.lib().rsd_copy(ctx.h, n, U.ptr, x.ptr))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            r = rsd.solve(ctx, heat.K, b, x, cfgs[key])
+            e1.record(stream)
+            e1.synchronize()
+            if rep_i >= 2:
+                ts.append(e0.elapsed_time(e1))
+        solve_t[key] = float(np.median(ts))
+        solve_it[key] = r["iterations"]
+        solve_tr[key] = r["trueResidualRel"]
 
     # end to end through the public API with host buffers: H2D of the step's state from pinned
     # host memory, the step, D2H of the new state, every step
@@ -344,6 +372,7 @@ def main():
         return float(t.item())
 
     ms_mx, ms_64, ms_e2e = reduce_max(ms_mx), reduce_max(ms_64), reduce_max(ms_e2e)
+    solve_t = {k: reduce_max(v) for k, v in solve_t.items()}
 
     # dominant kernel of the mixed step: the FP32 SpMV (+ p.Ap) of every CG iteration
     launches, tot = prof_mx["spmv_dot_f32"]
@@ -360,10 +389,10 @@ def main():
     it_64 = [r["iterations"] for r in reps_64]
     solve_mx = sum(prof_mx[f][1] for f in ("spmv_dot_f32", "cg_update", "cg_pupdate", "reliable_update")) / args.steps
     solve_64 = sum(prof_64[f][1] for f in ("spmv_dot_f64", "cg_update", "cg_pupdate")) / args.steps
-    # launches per step: 7 element/vector kernels + rate + 3 memsets-free init kernels + 4 (mixed) per iteration
-    # issued (including the no-op tail of the last polling chunk) -> counted from the profiler plus fixed ones
-    issued_mx = sum(prof_mx[f][0] for f in ("spmv_dot_f32", "cg_update", "cg_pupdate", "reliable_update", "assemble_matrix", "assemble_vector"))
-    gpu_launches = int(issued_mx + args.steps * (1 + 2 + 2))   # + rate, invdiag/init, residual combine/dot
+    # kernels run in the timed mixed steps: per step 9 outside the solve (Udot, K + M/dt, right-hand side,
+    # lift, FP32 value copy, inverse diagonal, initial residual, stage residual, its norm), per CG
+    # iteration 3 (SpMV + p.Ap, update, p update) and one per FP64 residual replacement
+    gpu_launches = int(sum(9 + 3 * r["iterations"] + r["refinements"] for r in reps_mx))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -386,8 +415,11 @@ def main():
                    "l2": "inputs larger than L2 (CSR FP64 values + columns %.2f GB)" % (nnz * 12 / 1e9)},
         "fp64_ms_per_step": ms_64,
         "speedup_mixed_vs_fp64_step": ms_64 / ms_mx,
-        "solve_ms_per_step": {"mixed": solve_mx, "fp64": solve_64},
-        "speedup_mixed_vs_fp64_solve": solve_64 / solve_mx if solve_mx else None,
+        "time_to_1e8_solve_ms": {"mixed": solve_t["mixed"], "fp64": solve_t["fp64"],
+                                 "speedup_mixed_vs_fp64": solve_t["fp64"] / solve_t["mixed"],
+                                 "iterations": solve_it, "true_residual_rel": solve_tr,
+                                 "how": "first step's system, x0 = U0 on the device, CUDA events around rsd_solve (graph, warm), median of 5"},
+        "solve_kernel_ms_per_step": {"mixed": solve_mx, "fp64": solve_64},
         "iterations": {"mixed": it_mx, "fp64": it_64},
         "reliable_updates": [r["refinements"] for r in reps_mx],
         "true_residual_rel": {"mixed": max(r["trueResidualRel"] for r in reps_mx), "fp64": max(r["trueResidualRel"] for r in reps_64)},

@@ -124,11 +124,8 @@ int default_lanes(const rsd_csr* A) {
 	return 16;
 }
 
-static int grid_for(const rsd_ctx* ctx, int64_t n, int L, int block) {
-	int64_t blocks = (n * std::max(L, 1) + block - 1) / block;
-	blocks = std::min<int64_t>(blocks, (int64_t)ctx->num_sms * (2048 / block));
-	return (int)std::max<int64_t>(blocks, 1);
-}
+// one full wave of the kernel's resident blocks (grid-stride loop over the rows)
+#define SPMV_GRID(kern, L, block) wave_blocks(ctx, kern, block, A->n * std::max(L, 1), INT64_MAX)
 
 int spmv_f64(rsd_ctx* ctx, const rsd_csr* Ac, const double* x, double* y) {
 	rsd_csr* A = const_cast<rsd_csr*>(Ac);
@@ -137,7 +134,7 @@ int spmv_f64(rsd_ctx* ctx, const rsd_csr* Ac, const double* x, double* y) {
 	const int block = A->block ? A->block : 256;
 	const int L = exec_lanes(A);
 	const MatView<double> V = view64(A);
-	RSD_DISPATCH_L(L, (k_spmv<LL, double><<<grid_for(ctx, A->n, LL, block), block, 0, ctx->stream>>>(A->n, V, x, y)));
+	RSD_DISPATCH_L(L, (k_spmv<LL, double><<<SPMV_GRID((k_spmv<LL, double>), LL, block), block, 0, ctx->stream>>>(A->n, V, x, y)));
 	RSD_CUDA(cudaGetLastError());
 	return RSD_OK;
 }
@@ -149,7 +146,7 @@ int spmv_f32(rsd_ctx* ctx, const rsd_csr* Ac, const float* x, float* y) {
 	const int block = A->block ? A->block : 256;
 	const int L = exec_lanes(A);
 	const MatView<float> V = view32(A);
-	RSD_DISPATCH_L(L, (k_spmv<LL, float><<<grid_for(ctx, A->n, LL, block), block, 0, ctx->stream>>>(A->n, V, x, y)));
+	RSD_DISPATCH_L(L, (k_spmv<LL, float><<<SPMV_GRID((k_spmv<LL, float>), LL, block), block, 0, ctx->stream>>>(A->n, V, x, y)));
 	RSD_CUDA(cudaGetLastError());
 	return RSD_OK;
 }

@@ -1,5 +1,7 @@
 // Context, memory, errors, expression compiler, mesh upload, DOF map and CSR pattern.
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <cctype>
 #include <cmath>
 #include <cstring>
@@ -217,9 +219,24 @@ static void diag_index(int64_t n, const int32_t* rp, const int32_t* col, int32_t
 	});
 }
 
+int resident_blocks(const void* kernel, int block) {
+	static std::mutex mu;
+	static std::map<std::pair<const void*, int>, int> cache;
+	std::lock_guard<std::mutex> lk(mu);
+	auto it = cache.find({kernel, block});
+	if (it != cache.end()) return it->second;
+	int occ = 0;
+	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, block, 0) != cudaSuccess || occ < 1) {
+		cudaGetLastError();
+		occ = 1;
+	}
+	cache[{kernel, block}] = occ;
+	return occ;
+}
+
 static void free_csr_arrays(rsd_csr* A) {
 	cudaFree(A->rowPtr); cudaFree(A->col); cudaFree(A->val); cudaFree(A->diag);
-	cudaFree(A->sStart); cudaFree(A->sCol); cudaFree(A->sVal); cudaFree(A->val32); cudaFree(A->sSrc); cudaFree(A->sDiag);
+	cudaFree(A->sStart); cudaFree(A->sCol); cudaFree(A->sVal); cudaFree(A->val32); cudaFree(A->sSrc); cudaFree(A->sDiag); cudaFree(A->sCol16); cudaFree(A->sBase);
 }
 
 static int upload_csr(rsd_ctx* ctx, int64_t n, const std::vector<int32_t>& rp, const std::vector<int32_t>& col,
@@ -241,21 +258,42 @@ static int upload_csr(rsd_ctx* ctx, int64_t n, const std::vector<int32_t>& rp, c
 	const int64_t ssize = start[ns];
 	if (ssize > INT32_MAX) { delete A; return set_error(RSD_EINVAL, "padded SELL layout has 2^31 or more slots"); }
 	std::vector<int32_t> sStart(ns + 1), sCol(std::max<int64_t>(ssize, 1)), sSrc(std::max<int64_t>(ssize, 1), -1), sDiag(std::max<int64_t>(n, 1), -1);
+	std::vector<int32_t> sMin(std::max<int64_t>(ns, 1)), sMax(std::max<int64_t>(ns, 1));
 	for (int64_t s = 0; s <= ns; ++s) sStart[s] = (int32_t)start[s];
 	parallel_for(ns, [&](int64_t b, int64_t e) {
 		for (int64_t s = b; s < e; ++s) {
 			const int64_t len = (start[s + 1] - start[s]) / 32;
+			const int64_t r0 = 32 * s;
+			// padding repeats a column the row already holds (value 0), so that it reads nothing new
+			const int32_t pad0 = rp[r0] < rp[r0 + 1] ? col[rp[r0]] : (int32_t)r0;
+			int32_t lo = INT32_MAX, hi = INT32_MIN;
 			for (int64_t l = 0; l < 32; ++l) {
-				const int64_t i = 32 * s + l;
+				const int64_t i = r0 + l;
+				const int32_t pad = i < n ? (rp[i] < rp[i + 1] ? col[rp[i + 1] - 1] : (int32_t)i) : pad0;
 				for (int64_t j = 0; j < len; ++j) {
 					const int64_t slot = start[s] + 32 * j + l;
 					if (i < n && rp[i] + j < rp[i + 1]) { sCol[slot] = col[rp[i] + j]; sSrc[slot] = (int32_t)(rp[i] + j); }
-					else sCol[slot] = (int32_t)(i < n ? i : 0);   // padding: value 0, a valid column
+					else sCol[slot] = pad;
+					lo = std::min(lo, sCol[slot]);
+					hi = std::max(hi, sCol[slot]);
 				}
 				if (i < n && d[i] >= 0) sDiag[i] = (int32_t)(start[s] + 32 * (d[i] - rp[i]) + l);
 			}
+			sMin[s] = len ? lo : 0;
+			sMax[s] = len ? hi : 0;
 		}
 	});
+	// 16-bit columns: every slice's columns within 65,535 of the slice's smallest one
+	bool narrow = ssize > 0;
+	for (int64_t s = 0; s < ns && narrow; ++s) narrow = (int64_t)sMax[s] - sMin[s] <= 65535;
+	std::vector<uint16_t> sCol16;
+	if (narrow) {
+		sCol16.resize(ssize);
+		parallel_for(ns, [&](int64_t b, int64_t e) {
+			for (int64_t s = b; s < e; ++s)
+				for (int64_t q = start[s]; q < start[s + 1]; ++q) sCol16[q] = (uint16_t)(sCol[q] - sMin[s]);
+		});
+	}
 	A->nslices = ns;
 	A->ssize = ssize;
 	auto fail = [&](cudaError_t e, const char* w) { free_csr_arrays(A); delete A; return cuda_error(e, w); };
@@ -277,6 +315,12 @@ static int upload_csr(rsd_ctx* ctx, int64_t n, const std::vector<int32_t>& rp, c
 	if ((e = cudaMemcpyAsync(A->sCol, sCol.data(), sizeof(int32_t) * S, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload sCol");
 	if ((e = cudaMemcpyAsync(A->sSrc, sSrc.data(), sizeof(int32_t) * S, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload sSrc");
 	if ((e = cudaMemcpyAsync(A->sDiag, sDiag.data(), sizeof(int32_t) * std::max<int64_t>(n, 1), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload sDiag");
+	if (narrow) {
+		if ((e = cudaMalloc(&A->sCol16, sizeof(uint16_t) * ssize)) != cudaSuccess) return fail(e, "cudaMalloc sCol16");
+		if ((e = cudaMalloc(&A->sBase, sizeof(int32_t) * ns)) != cudaSuccess) return fail(e, "cudaMalloc sBase");
+		if ((e = cudaMemcpyAsync(A->sCol16, sCol16.data(), sizeof(uint16_t) * ssize, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload sCol16");
+		if ((e = cudaMemcpyAsync(A->sBase, sMin.data(), sizeof(int32_t) * ns, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload sBase");
+	}
 	if (hval && nnz) e = cudaMemcpyAsync(A->val, hval, sizeof(double) * nnz, cudaMemcpyHostToDevice, ctx->stream);
 	else e = cudaMemsetAsync(A->val, 0, sizeof(double) * std::max<int64_t>(nnz, 1), ctx->stream);
 	if (e != cudaSuccess) return fail(e, "upload values");
@@ -444,6 +488,7 @@ int rsd_ctx_destroy(rsd_ctx* c) {
 	cudaSetDevice(c->device);
 	if (c->stream) cudaStreamSynchronize(c->stream);
 	for (cudaEvent_t e : c->prof.pool) cudaEventDestroy(e);
+	free_graph_cache(c);
 	cudaFree(c->s.partials);
 	cudaFree(c->s.scal);
 	cudaFreeHost(c->s.hscal);

@@ -74,6 +74,7 @@ struct rsd_ctx {
 	cudaStream_t stream = nullptr;
 	rsd::rsd_scratch s;
 	rsd::Profiler prof;
+	void* graphs = nullptr;        // cached CG solve graphs (rsd_krylov.cu)
 };
 
 namespace rsd {
@@ -101,8 +102,12 @@ struct rsd_csr {
 	double* sVal = nullptr;        // ssize
 	int32_t* sSrc = nullptr;       // ssize: CSR position of the slot, -1 for padding
 	int32_t* sDiag = nullptr;      // n: slot of the diagonal entry or -1
+	// narrow columns: sBase[s] + sCol16[slot] == sCol[slot], present when every slice's columns
+	// lie within 65,535 of its smallest (then the SELL kernels read 2 instead of 4 bytes per slot)
+	uint16_t* sCol16 = nullptr;    // ssize
+	int32_t* sBase = nullptr;      // nslices
 	bool csrValid = true, sellValid = false;
-	int format = 0;                // SpMV layout: 0 SELL-32, 1 CSR vector with `lanes` lanes per row
+	int format = 0;                // SpMV layout: 0 SELL-32 (narrow columns when present), 1 CSR vector with `lanes` lanes per row
 	int lanes = 0;                 // CSR SpMV lanes per row (0: default from nnz/row)
 	int block = 0;                 // SpMV threads per block (0: default)
 	bool owns_pattern = true;
@@ -117,6 +122,7 @@ namespace rsd {
 int sell_sync(rsd_ctx* ctx, rsd_csr* A);     // SELL values current (from CSR if needed)
 int csr_sync(rsd_ctx* ctx, rsd_csr* A);      // CSR values current (from SELL if needed)
 int f32_sync(rsd_ctx* ctx, rsd_csr* A);      // FP32 copy current, in the execution layout
+void free_graph_cache(rsd_ctx* ctx);         // release the context's cached solve graphs
 int exec_sync(rsd_ctx* ctx, rsd_csr* A);     // FP64 values current in the execution layout
 }  // namespace rsd
 

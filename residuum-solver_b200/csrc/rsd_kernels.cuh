@@ -43,6 +43,11 @@ __device__ __forceinline__ float ldh(const float* a, uint64_t pol) {
 	asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
 	return v;
 }
+__device__ __forceinline__ uint16_t ldh(const uint16_t* a, uint64_t pol) {
+	unsigned short v;
+	asm volatile("ld.global.nc.L2::cache_hint.u16 %0, [%1], %2;" : "=h"(v) : "l"(a), "l"(pol));
+	return v;
+}
 __device__ __forceinline__ int32_t ldh(const int32_t* a, uint64_t pol) {
 	int32_t v;
 	asm volatile("ld.global.nc.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
@@ -128,25 +133,52 @@ struct MatView {
 	const int32_t* __restrict__ ptr;
 	const int32_t* __restrict__ col;
 	const T* __restrict__ val;
+	const uint16_t* __restrict__ col16 = nullptr;   // SELL-32 narrow columns (L == -1)
+	const int32_t* __restrict__ base = nullptr;
 };
 
 // sum over one row of val * xf(column).  L == 0: SELL-32, one thread per row (entries 32 slots
-// apart, so a warp's value/column loads are contiguous); L > 0: CSR with a group of L lanes per row,
-// every lane of the group receiving the total.  Values and columns stream evict-first; xf reads the
-// gathered vector with evict-last.
+// apart, so a warp's value/column loads are contiguous); L == -1: SELL-32 with 16-bit column
+// offsets from the slice base; L > 0: CSR with a group of L lanes per row, every lane of the group
+// receiving the total.  Values and columns stream evict-first; xf reads the gathered vector with
+// evict-last.
 template <int L, typename T, typename AccT, typename XF>
 __device__ __forceinline__ AccT row_sum(const MatView<T>& A, int64_t row, int64_t n, int lane, const L2Pol& pol, XF xf) {
 	AccT s = AccT(0);
 	if (row < n) {
-		int q, e, st;
-		if constexpr (L == 0) {
+		if constexpr (L <= 0) {
+			// the slice's length is the same for the whole warp; loads are issued four slots at a
+			// time (values, columns, then the gathers) and summed in row order
 			const int64_t sl = row >> 5;
-			q = A.ptr[sl] + (int)(row & 31); e = A.ptr[sl + 1]; st = 32;
+			const int s0 = A.ptr[sl];
+			const int len = (A.ptr[sl + 1] - s0) >> 5;
+			const int q0 = s0 + (int)(row & 31);
+			const T* __restrict__ vp = A.val + q0;
+			int cb = 0;
+			const int32_t* __restrict__ cp32 = nullptr;
+			const uint16_t* __restrict__ cp16 = nullptr;
+			if constexpr (L < 0) { cb = A.base[sl]; cp16 = A.col16 + q0; } else { cp32 = A.col + q0; }
+			auto colat = [&](int j) -> int {
+				if constexpr (L < 0) return cb + (int)ldh(cp16 + 32 * j, pol.first);
+				else return ldh(cp32 + 32 * j, pol.first);
+			};
+			int j = 0;
+			for (; j + 4 <= len; j += 4) {
+				const T v0 = ldh(vp + 32 * j, pol.first), v1 = ldh(vp + 32 * (j + 1), pol.first);
+				const T v2 = ldh(vp + 32 * (j + 2), pol.first), v3 = ldh(vp + 32 * (j + 3), pol.first);
+				const int c0 = colat(j), c1 = colat(j + 1), c2 = colat(j + 2), c3 = colat(j + 3);
+				const AccT x0 = xf(c0), x1 = xf(c1), x2 = xf(c2), x3 = xf(c3);
+				s += (AccT)v0 * x0;
+				s += (AccT)v1 * x1;
+				s += (AccT)v2 * x2;
+				s += (AccT)v3 * x3;
+			}
+			for (; j < len; ++j) s += (AccT)ldh(vp + 32 * j, pol.first) * xf(colat(j));
 		} else {
-			q = A.ptr[row] + lane; e = A.ptr[row + 1]; st = L;
-		}
+			const int e = A.ptr[row + 1];
 #pragma unroll 4
-		for (; q < e; q += st) s += (AccT)ldh(A.val + q, pol.first) * xf(ldh(A.col + q, pol.first));
+			for (int q = A.ptr[row] + lane; q < e; q += L) s += (AccT)ldh(A.val + q, pol.first) * xf(ldh(A.col + q, pol.first));
+		}
 	}
 	if constexpr (L > 1) s = group_sum<L>(s);
 	return s;
@@ -161,7 +193,7 @@ __device__ __forceinline__ AccT row_dot(const MatView<T>& A, const T* __restrict
 // handed out warp by warp so that a warp's rows are consecutive (a whole SELL slice when L == 0).
 template <int L>
 struct RowLoop {
-	static constexpr int G = L ? L : 1;
+	static constexpr int G = L > 0 ? L : 1;
 	int lane;
 	int64_t base, step, sub;
 	__device__ __forceinline__ RowLoop() {
@@ -202,13 +234,16 @@ __device__ __forceinline__ double eval_expr(const DevExpr& e, double t, double x
 	return e.n ? st[0] : 0.0;
 }
 
-// lanes per row of the execution layout: 0 for SELL-32, else the CSR group size
-inline int exec_lanes(const rsd_csr* A) { return A->format == 0 ? 0 : default_lanes(A); }
+// lanes per row of the execution layout: -1 for SELL-32 with narrow columns, 0 for SELL-32, else
+// the CSR group size
+inline int exec_lanes(const rsd_csr* A) { return A->format == 0 ? (A->sCol16 ? -1 : 0) : default_lanes(A); }
 inline MatView<double> view64(const rsd_csr* A) {
-	return A->format == 0 ? MatView<double>{A->sStart, A->sCol, A->sVal} : MatView<double>{A->rowPtr, A->col, A->val};
+	return A->format == 0 ? MatView<double>{A->sStart, A->sCol, A->sVal, A->sCol16, A->sBase}
+	                      : MatView<double>{A->rowPtr, A->col, A->val};
 }
 inline MatView<float> view32(const rsd_csr* A) {
-	return MatView<float>{A->format == 0 ? A->sStart : A->rowPtr, A->format == 0 ? A->sCol : A->col, A->val32};
+	return A->format == 0 ? MatView<float>{A->sStart, A->sCol, A->val32, A->sCol16, A->sBase}
+	                      : MatView<float>{A->rowPtr, A->col, A->val32};
 }
 // diagonal position and values of the execution layout
 inline const int32_t* exec_diag(const rsd_csr* A) { return A->format == 0 ? A->sDiag : A->diag; }
@@ -216,6 +251,7 @@ inline const double* exec_val(const rsd_csr* A) { return A->format == 0 ? A->sVa
 
 #define RSD_DISPATCH_L(L, CALL)                          \
 	switch (L) {                                         \
+		case -1: { constexpr int LL = -1; CALL; } break; \
 		case 0: { constexpr int LL = 0; CALL; } break;   \
 		case 1: { constexpr int LL = 1; CALL; } break;   \
 		case 2: { constexpr int LL = 2; CALL; } break;   \
@@ -224,6 +260,18 @@ inline const double* exec_val(const rsd_csr* A) { return A->format == 0 ? A->sVa
 		case 16: { constexpr int LL = 16; CALL; } break; \
 		default: { constexpr int LL = 32; CALL; } break; \
 	}
+
+// resident blocks per SM of `kernel` at `block` threads (cached per kernel and block size)
+int resident_blocks(const void* kernel, int block);
+
+// grid of a grid-stride kernel: the blocks `threads` need, at most one full wave of resident blocks
+// (so no block starts after the first ones finish) and at most `cap` (the reduction partials)
+template <typename K>
+inline int wave_blocks(const rsd_ctx* ctx, K* kernel, int block, int64_t threads, int64_t cap = kMaxPartials) {
+	const int64_t need = (threads + block - 1) / block;
+	const int64_t wave = (int64_t)ctx->num_sms * resident_blocks((const void*)kernel, block);
+	return (int)std::max<int64_t>(1, std::min(std::min(need, wave), cap));
+}
 
 inline int vec_grid(const rsd_ctx* ctx, int64_t n, int threads = 256) {
 	int64_t b = (n + threads - 1) / threads;

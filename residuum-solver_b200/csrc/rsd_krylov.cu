@@ -8,6 +8,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <iterator>
 #include <mutex>
 #include <vector>
 
@@ -28,6 +31,27 @@ static CgScal* scal_slot(rsd_ctx* ctx, int k) { return reinterpret_cast<CgScal*>
 
 __device__ __forceinline__ bool is_done(const CgScal* S) { return *((volatile const int32_t*)&S->done) != 0; }
 
+// Graph mode: the whole solve is one CUDA graph whose iterations run under a conditional WHILE node
+// (and, for mixed precision, the FP64 residual replacement under a nested IF node).  The kernels
+// steer both from the device: the p-update sets the WHILE condition from the done flag, the update
+// sets the IF condition from the replacement flag.  `limit` bounds the body executions of one launch
+// (max_iters plus slack) so that the loop ends even if no kernel ever declared the solve done.
+struct GraphCtl {
+	unsigned long long hw, hr;   // cudaGraphConditionalHandle of the WHILE and IF nodes
+	int32_t on, limit;
+};
+
+__device__ __forceinline__ void graph_continue(CgScal* S, const GraphCtl& gc) {
+	const int32_t bodies = S->pad + 1;   // body executions in this launch (pad starts at zero)
+	S->pad = bodies;
+	bool go = !is_done(S);
+	if (go && bodies >= gc.limit) {
+		S->done = 1; S->converged = 0; S->status = RSD_ETIMEOUT;
+		go = false;
+	}
+	cudaGraphSetConditional(gc.hw, go ? 1u : 0u);
+}
+
 // ---- FP64 PCG: linalg/solver/iterative/cg/Solver.tpp:13-119 ----------------------------------
 // r = b - A x; z = M r; p = z; rz = r.z; res0 = |r|   (Solver.tpp:31-63)
 template <int L>
@@ -43,8 +67,8 @@ __global__ void __launch_bounds__(256) k_cg_init(int64_t n, MatView<double> A, c
 		const double ax = row_dot<L, double, double>(A, x, row, n, rl.lane, pol);
 		if (rl.lane == 0 && row < n) {
 			const double ri = ldh(b + row, pol.first) + (-1.0) * ax;
-			const double zi = invD ? ri * ldh(invD + row, pol.first) : ri;
-			sth(r + row, ri, pol.first);
+			const double zi = invD ? ri * ldh(invD + row, pol.last) : ri;
+			sth(r + row, ri, pol.last);
 			sth(p + row, zi, pol.last);
 			v[0] += ri * ri;
 			v[1] += ri * zi;
@@ -72,7 +96,7 @@ __global__ void __launch_bounds__(256) k_cg_spmv_dot(int64_t n, MatView<double> 
 	for (int64_t base = rl.base; base < n; base += rl.step) {
 		const int64_t row = base + rl.sub;
 		const double s = row_dot<L, double, double>(A, p, row, n, rl.lane, pol);
-		if (rl.lane == 0 && row < n) { sth(Ap + row, s, pol.first); v[0] += ldh(p + row, pol.last) * s; }
+		if (rl.lane == 0 && row < n) { sth(Ap + row, s, pol.last); v[0] += ldh(p + row, pol.last) * s; }
 	}
 	if (grid_sum<1>(v, partials, &S->ticket)) {
 		S->pAp = v[0];
@@ -91,10 +115,10 @@ __global__ void __launch_bounds__(256) k_cg_update(int64_t n, double* __restrict
 	const L2Pol pol = make_l2pol();
 	double v[2] = {0.0, 0.0};
 	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-		sth(x + i, ldh_rw(x + i, pol.first) + alpha * ldh(p + i, pol.first), pol.first);
-		const double ri = ldh_rw(r + i, pol.first) + (-alpha) * ldh(Ap + i, pol.first);
-		sth(r + i, ri, pol.first);
-		const double zi = invD ? ri * ldh(invD + i, pol.first) : ri;
+		sth(x + i, ldh_rw(x + i, pol.last) + alpha * ldh(p + i, pol.last), pol.last);
+		const double ri = ldh_rw(r + i, pol.last) + (-alpha) * ldh(Ap + i, pol.last);
+		sth(r + i, ri, pol.last);
+		const double zi = invD ? ri * ldh(invD + i, pol.last) : ri;
 		v[0] += ri * ri;
 		v[1] += ri * zi;
 	}
@@ -113,14 +137,15 @@ __global__ void __launch_bounds__(256) k_cg_update(int64_t n, double* __restrict
 
 // p = beta p + z   (Solver.tpp:103-104: scal then axpy)
 __global__ void __launch_bounds__(256) k_cg_pupdate(int64_t n, double* __restrict__ p, const double* __restrict__ r,
-                                                    const double* __restrict__ invD, const CgScal* S) {
+                                                    const double* __restrict__ invD, CgScal* S, GraphCtl gc) {
+	if (gc.on && blockIdx.x == 0 && threadIdx.x == 0) graph_continue(S, gc);
 	if (is_done(S)) return;
 	const double beta = S->beta;
 	const L2Pol pol = make_l2pol();
 	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-		const double ri = ldh(r + i, pol.first);
-		const double zi = invD ? ri * ldh(invD + i, pol.first) : ri;
-		sth(p + i, ldh_rw(p + i, pol.first) * beta + 1.0 * zi, pol.last);   // the next SpMV gathers p
+		const double ri = ldh(r + i, pol.last);
+		const double zi = invD ? ri * ldh(invD + i, pol.last) : ri;
+		sth(p + i, ldh_rw(p + i, pol.last) * beta + 1.0 * zi, pol.last);   // the next SpMV gathers p
 	}
 }
 
@@ -144,8 +169,8 @@ __global__ void __launch_bounds__(256) k_mx_init(int64_t n, MatView<double> A, c
 		if (rl.lane == 0 && row < n) {
 			const double r64 = ldh(b + row, pol.first) - ax;
 			const float ri = (float)r64;
-			const float zi = invD ? ri * ldh(invD + row, pol.first) : ri;
-			sth(r + row, ri, pol.first); sth(p + row, zi, pol.last); sth(y + row, 0.0f, pol.first);
+			const float zi = invD ? ri * ldh(invD + row, pol.last) : ri;
+			sth(r + row, ri, pol.last); sth(p + row, zi, pol.last); sth(y + row, 0.0f, pol.last);
 			v[0] += r64 * r64;
 			v[1] += (double)ri * (double)zi;
 		}
@@ -172,7 +197,7 @@ __global__ void __launch_bounds__(256) k_mx_spmv_dot(int64_t n, MatView<float> A
 	for (int64_t base = rl.base; base < n; base += rl.step) {
 		const int64_t row = base + rl.sub;
 		const float s = row_dot<L, float, float>(A, p, row, n, rl.lane, pol);
-		if (rl.lane == 0 && row < n) { sth(Ap + row, s, pol.first); v[0] += (double)ldh(p + row, pol.last) * (double)s; }
+		if (rl.lane == 0 && row < n) { sth(Ap + row, s, pol.last); v[0] += (double)ldh(p + row, pol.last) * (double)s; }
 	}
 	if (grid_sum<1>(v, partials, &S->ticket)) {
 		S->pAp = v[0];
@@ -184,16 +209,16 @@ __global__ void __launch_bounds__(256) k_mx_spmv_dot(int64_t n, MatView<float> A
 __global__ void __launch_bounds__(256) k_mx_update(int64_t n, float* __restrict__ y, float* __restrict__ r,
                                                    const float* __restrict__ p, const float* __restrict__ Ap,
                                                    const float* __restrict__ invD, CgScal* S, double* partials, double tol,
-                                                   int relMode, int64_t maxIters, double delta) {
+                                                   int relMode, int64_t maxIters, double delta, GraphCtl gc) {
 	if (is_done(S)) return;
 	const float alpha = (float)S->alpha;
 	const L2Pol pol = make_l2pol();
 	double v[2] = {0.0, 0.0};
 	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-		sth(y + i, ldh_rw(y + i, pol.first) + alpha * ldh(p + i, pol.first), pol.first);
-		const float ri = ldh_rw(r + i, pol.first) - alpha * ldh(Ap + i, pol.first);
-		sth(r + i, ri, pol.first);
-		const float zi = invD ? ri * ldh(invD + i, pol.first) : ri;
+		sth(y + i, ldh_rw(y + i, pol.last) + alpha * ldh(p + i, pol.last), pol.last);
+		const float ri = ldh_rw(r + i, pol.last) - alpha * ldh(Ap + i, pol.last);
+		sth(r + i, ri, pol.last);
+		const float zi = invD ? ri * ldh(invD + i, pol.last) : ri;
 		v[0] += (double)ri * (double)ri;
 		v[1] += (double)ri * (double)zi;
 	}
@@ -208,6 +233,7 @@ __global__ void __launch_bounds__(256) k_mx_update(int64_t n, float* __restrict_
 		} else {
 			S->beta = v[1] / S->rz; S->rz = v[1];
 		}
+		if (gc.on) cudaGraphSetConditional(gc.hr, S->reliable ? 1u : 0u);
 	}
 }
 
@@ -228,8 +254,8 @@ __global__ void __launch_bounds__(256) k_mx_reliable(int64_t n, MatView<double> 
 		if (rl.lane == 0 && row < n) {
 			const double r64 = ldh(b + row, pol.first) - s;
 			const float ri = (float)r64;
-			const float zi = invD ? ri * ldh(invD + row, pol.first) : ri;
-			sth(r + row, ri, pol.first);
+			const float zi = invD ? ri * ldh(invD + row, pol.last) : ri;
+			sth(r + row, ri, pol.last);
 			v[0] += r64 * r64;
 			v[1] += (double)ri * (double)zi;
 		}
@@ -251,7 +277,8 @@ __global__ void __launch_bounds__(256) k_mx_reliable(int64_t n, MatView<double> 
 // fold y into x after a replacement; p = beta p + z
 __global__ void __launch_bounds__(256) k_mx_pupdate(int64_t n, double* __restrict__ x, float* __restrict__ y,
                                                     float* __restrict__ p, const float* __restrict__ r,
-                                                    const float* __restrict__ invD, const CgScal* S) {
+                                                    const float* __restrict__ invD, CgScal* S, GraphCtl gc) {
+	if (gc.on && blockIdx.x == 0 && threadIdx.x == 0) graph_continue(S, gc);
 	const int apply = *((volatile const int32_t*)&S->apply_xy);
 	const int done = is_done(S);
 	if (!apply && done) return;
@@ -259,13 +286,13 @@ __global__ void __launch_bounds__(256) k_mx_pupdate(int64_t n, double* __restric
 	const L2Pol pol = make_l2pol();
 	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
 		if (apply) {
-			sth(x + i, ldh_rw(x + i, pol.first) + (double)ldh_rw(y + i, pol.first), pol.first);
-			sth(y + i, 0.0f, pol.first);
+			sth(x + i, ldh_rw(x + i, pol.last) + (double)ldh_rw(y + i, pol.last), pol.last);
+			sth(y + i, 0.0f, pol.last);
 		}
 		if (!done) {
-			const float ri = ldh(r + i, pol.first);
-			const float zi = invD ? ri * ldh(invD + i, pol.first) : ri;
-			sth(p + i, ldh_rw(p + i, pol.first) * beta + zi, pol.last);   // the next SpMV gathers p
+			const float ri = ldh(r + i, pol.last);
+			const float zi = invD ? ri * ldh(invD + i, pol.last) : ri;
+			sth(p + i, ldh_rw(p + i, pol.last) * beta + zi, pol.last);   // the next SpMV gathers p
 		}
 	}
 }
@@ -320,16 +347,14 @@ static int get_ws(rsd_ctx* ctx, size_t bytes, void** out) {
 	return RSD_OK;
 }
 
-static int row_blocks(const rsd_ctx* ctx, int64_t n, int L, int block = 256) {
-	int64_t b = (n * std::max(L, 1) + block - 1) / block;
-	b = std::min<int64_t>(b, std::min<int64_t>(kMaxPartials, (int64_t)ctx->num_sms * (2048 / block)));
-	return (int)std::max<int64_t>(b, 1);
-}
-static int vec_blocks(const rsd_ctx* ctx, int64_t n) {
-	int64_t b = (n + 255) / 256;
-	b = std::min<int64_t>(b, std::min<int64_t>(kMaxPartials, (int64_t)ctx->num_sms * 8));
-	return (int)std::max<int64_t>(b, 1);
-}
+// grids of the row kernels (n rows, max(L,1) threads each) and vector kernels (n entries): one
+// full wave of each kernel's resident blocks; used inside functions that define ctx, n and L
+#define RG(kern) wave_blocks(ctx, kern, 256, n * std::max(L, 1))
+#define VG(kern) wave_blocks(ctx, kern, 256, n)
+
+// workspace vectors start 256-byte aligned: every warp's 32 consecutive entries then fall in whole
+// 32-byte sectors
+static int64_t pad_len(int64_t n) { return (n + 63) & ~int64_t(63); }
 
 static int finish_report(rsd_ctx* ctx, CgScal* S, rsd_report* rep) {
 	CgScal h;
@@ -385,55 +410,216 @@ struct Poller {
 	}
 };
 
+// ---- graph mode plumbing ---------------------------------------------------------------------
+// A solve's graph is cached on the context per precision and rebuilt only when anything it
+// captured changes (pointers, sizes, launch shapes, tolerances).
+struct CgKey {
+	const void* p[14];
+	int64_t i[8];
+	double d[2];
+	bool operator==(const CgKey& o) const { return std::memcmp(this, &o, sizeof(CgKey)) == 0; }
+};
+struct CgGraph {
+	CgKey key{};
+	bool valid = false;
+	cudaGraph_t graph = nullptr;
+	cudaGraphExec_t exec = nullptr;
+	void release() {
+		if (exec) cudaGraphExecDestroy(exec);
+		if (graph) cudaGraphDestroy(graph);
+		exec = nullptr; graph = nullptr; valid = false;
+	}
+};
+struct GraphCache {
+	CgGraph cg[2];   // 0: FP64, 1: mixed
+};
+
+static bool graph_mode(const rsd_ctx* ctx) {
+	if (ctx->prof.on) return false;              // per-kernel timing needs the plain launches
+	const char* e = getenv("RSD_CG_GRAPH");
+	return !(e && e[0] == '0');
+}
+
+static GraphCache* graph_cache(rsd_ctx* ctx) {
+	if (!ctx->graphs) ctx->graphs = new GraphCache();
+	return static_cast<GraphCache*>(ctx->graphs);
+}
+
+// leaf nodes of the work captured so far on the stream
+static int capture_leaves(cudaStream_t s, const cudaGraphNode_t** deps, size_t* nd) {
+	cudaStreamCaptureStatus st;
+	RSD_CUDA(cudaStreamGetCaptureInfo(s, &st, nullptr, nullptr, deps, nd));
+	if (st != cudaStreamCaptureStatusActive) return set_error(RSD_ECUDA, "stream capture is not active");
+	return RSD_OK;
+}
+
+// add a conditional node of `type` to `g` behind `deps`; returns the node and its body graph
+static int add_conditional(cudaGraph_t g, const cudaGraphNode_t* deps, size_t nd, cudaGraphConditionalHandle h,
+                           cudaGraphConditionalNodeType type, cudaGraphNode_t* node, cudaGraph_t* body) {
+	cudaGraphNodeParams np{};
+	np.type = cudaGraphNodeTypeConditional;
+	np.conditional.handle = h;
+	np.conditional.type = type;
+	np.conditional.size = 1;
+	RSD_CUDA(cudaGraphAddNode(node, g, deps, nd, &np));
+	*body = np.conditional.phGraph_out[0];
+	return RSD_OK;
+}
+
+// Build prologue -> WHILE(body_a -> [IF(reliable)] -> body_b) -> epilogue into one executable graph.
+// Each stage function launches its kernels on ctx->stream, which is being captured.
+template <typename Pro, typename BodyA, typename Rel, typename BodyB, typename Epi>
+static int build_cg_graph(rsd_ctx* ctx, bool with_if, int32_t limit, Pro prologue, BodyA body_a, Rel reliable,
+                          BodyB body_b, Epi epilogue, CgGraph* G) {
+	cudaStream_t s = ctx->stream;
+	G->release();
+	RSD_CUDA(cudaGraphCreate(&G->graph, 0));
+	cudaGraphConditionalHandle hw = 0, hr = 0;
+	RSD_CUDA(cudaGraphConditionalHandleCreate(&hw, G->graph, 1, cudaGraphCondAssignDefault));
+	auto fail = [&](int rc) {
+		cudaGraph_t junk = nullptr;
+		cudaStreamCaptureStatus st;
+		if (cudaStreamIsCapturing(s, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone) cudaStreamEndCapture(s, &junk);
+		cudaGetLastError();
+		G->release();
+		return rc;
+	};
+	int rc;
+	// prologue, then the WHILE node behind it
+	RSD_CUDA(cudaStreamBeginCaptureToGraph(s, G->graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+	if ((rc = prologue()) != RSD_OK) return fail(rc);
+	const cudaGraphNode_t* deps = nullptr;
+	size_t nd = 0;
+	if ((rc = capture_leaves(s, &deps, &nd)) != RSD_OK) return fail(rc);
+	cudaGraphNode_t wnode;
+	cudaGraph_t body;
+	if ((rc = add_conditional(G->graph, deps, nd, hw, cudaGraphCondTypeWhile, &wnode, &body)) != RSD_OK) return fail(rc);
+	cudaGraph_t out = nullptr;
+	if (cudaStreamEndCapture(s, &out) != cudaSuccess) return fail(cuda_error(cudaGetLastError(), "end capture (prologue)"));
+	// the loop body
+	cudaGraph_t ifBody = nullptr;
+	if (with_if && cudaGraphConditionalHandleCreate(&hr, body, 0, cudaGraphCondAssignDefault) != cudaSuccess)
+		return fail(cuda_error(cudaGetLastError(), "conditional handle (IF)"));
+	const GraphCtl gc{hw, hr, 1, limit};
+	if (cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+		return fail(cuda_error(cudaGetLastError(), "begin capture (body)"));
+	if ((rc = body_a(gc)) != RSD_OK) return fail(rc);
+	if (with_if) {
+		if ((rc = capture_leaves(s, &deps, &nd)) != RSD_OK) return fail(rc);
+		cudaGraphNode_t inode;
+		if ((rc = add_conditional(body, deps, nd, hr, cudaGraphCondTypeIf, &inode, &ifBody)) != RSD_OK) return fail(rc);
+		if (cudaStreamUpdateCaptureDependencies(s, &inode, 1, cudaStreamSetCaptureDependencies) != cudaSuccess)
+			return fail(cuda_error(cudaGetLastError(), "capture dependencies (IF)"));
+	}
+	if ((rc = body_b(gc)) != RSD_OK) return fail(rc);
+	if (cudaStreamEndCapture(s, &out) != cudaSuccess) return fail(cuda_error(cudaGetLastError(), "end capture (body)"));
+	if (with_if) {
+		if (cudaStreamBeginCaptureToGraph(s, ifBody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+			return fail(cuda_error(cudaGetLastError(), "begin capture (IF body)"));
+		if ((rc = reliable()) != RSD_OK) return fail(rc);
+		if (cudaStreamEndCapture(s, &out) != cudaSuccess) return fail(cuda_error(cudaGetLastError(), "end capture (IF body)"));
+	}
+	// epilogue behind the WHILE node
+	if (cudaStreamBeginCaptureToGraph(s, G->graph, &wnode, nullptr, 1, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+		return fail(cuda_error(cudaGetLastError(), "begin capture (epilogue)"));
+	if ((rc = epilogue()) != RSD_OK) return fail(rc);
+	if (cudaStreamEndCapture(s, &out) != cudaSuccess) return fail(cuda_error(cudaGetLastError(), "end capture (epilogue)"));
+	if (cudaGraphInstantiate(&G->exec, G->graph, 0) != cudaSuccess) return fail(cuda_error(cudaGetLastError(), "graph instantiate"));
+	G->valid = true;
+	return RSD_OK;
+}
+
+static int32_t body_limit(int64_t max_iters) { return (int32_t)std::min<int64_t>(max_iters + 4, INT32_MAX - 1); }
+
 static int cg_fp64(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const double* b, double* x, rsd_report* rep) {
 	const int64_t n = A->n;
 	RSD_CHECK(exec_sync(ctx, A));
 	const int L = exec_lanes(A);
 	const MatView<double> V = view64(A);
 	void* wsv;
-	RSD_CHECK(get_ws(ctx, sizeof(double) * (4 * n + 64), &wsv));
+	const int64_t ns = pad_len(n);
+	RSD_CHECK(get_ws(ctx, sizeof(double) * 4 * ns, &wsv));
 	double* r = (double*)wsv;
-	double* p = r + n;
-	double* Ap = p + n;
-	double* invD = cfg->precond == RSD_JACOBI ? Ap + n : nullptr;
+	double* p = r + ns;
+	double* Ap = p + ns;
+	double* invD = cfg->precond == RSD_JACOBI ? Ap + ns : nullptr;
 	CgScal* S = scal_slot(ctx, 0);
-	RSD_CUDA(cudaMemsetAsync(S, 0, sizeof(CgScal), ctx->stream));
+	CgScal* S1 = scal_slot(ctx, 1);
+	double* partials = ctx->s.partials;
 	const int rel = cfg->tol_type == RSD_TOL_RELATIVE;
-	const int gr = row_blocks(ctx, n, L), gv = vec_blocks(ctx, n);
-	// Jacobi::update on every solve (cg/Solver.tpp:22)
-	if (invD) k_invdiag64<<<gv, 256, 0, ctx->stream>>>(n, exec_diag(A), exec_val(A), invD);
-	RSD_DISPATCH_L(L, (k_cg_init<LL><<<gr, 256, 0, ctx->stream>>>(n, V, b, x, r, p, invD, S, ctx->s.partials, cfg->tol, rel, cfg->max_iters)));
-	RSD_CUDA(cudaGetLastError());
-	Poller poll{ctx, S, (int32_t*)ctx->s.hbuf};
-	RSD_CHECK(poll.init());
-	const int chunk = 8;
-	bool fin = false;
-	std::vector<int> pairs;
-	for (int64_t it = 0; it < cfg->max_iters + 2 * chunk && !fin; it += chunk) {
-		for (int c = 0; c < chunk; ++c) {
-			int pr = prof_begin(ctx, PF_SPMV_DOT_F64);
-			RSD_DISPATCH_L(L, (k_cg_spmv_dot<LL><<<gr, 256, 0, ctx->stream>>>(n, V, p, Ap, S, ctx->s.partials)));
-			prof_end(ctx, pr);
-			int pu = prof_begin(ctx, PF_CG_UPDATE);
-			k_cg_update<<<gv, 256, 0, ctx->stream>>>(n, x, r, p, Ap, invD, S, ctx->s.partials, cfg->tol, rel, cfg->max_iters);
-			prof_end(ctx, pu);
-			int pp = prof_begin(ctx, PF_CG_PUPDATE);
-			k_cg_pupdate<<<gv, 256, 0, ctx->stream>>>(n, p, r, invD, S);
-			prof_end(ctx, pp);
-			if (pr >= 0) { pairs.push_back(pr); pairs.push_back(pu); pairs.push_back(pp); }
-		}
+	const double tol = cfg->tol;
+	const int64_t maxIt = cfg->max_iters;
+	cudaStream_t st = ctx->stream;
+	auto prologue = [&]() -> int {
+		RSD_CUDA(cudaMemsetAsync(S, 0, sizeof(CgScal), st));
+		// Jacobi::update on every solve (cg/Solver.tpp:22)
+		if (invD) k_invdiag64<<<VG(k_invdiag64), 256, 0, st>>>(n, exec_diag(A), exec_val(A), invD);
+		RSD_DISPATCH_L(L, (k_cg_init<LL><<<RG(k_cg_init<LL>), 256, 0, st>>>(n, V, b, x, r, p, invD, S, partials, tol, rel, maxIt)));
 		RSD_CUDA(cudaGetLastError());
-		RSD_CHECK(poll.post(&fin));
+		return RSD_OK;
+	};
+	auto body_a = [&](GraphCtl) -> int {
+		RSD_DISPATCH_L(L, (k_cg_spmv_dot<LL><<<RG(k_cg_spmv_dot<LL>), 256, 0, st>>>(n, V, p, Ap, S, partials)));
+		k_cg_update<<<VG(k_cg_update), 256, 0, st>>>(n, x, r, p, Ap, invD, S, partials, tol, rel, maxIt);
+		RSD_CUDA(cudaGetLastError());
+		return RSD_OK;
+	};
+	auto body_b = [&](GraphCtl gc) -> int {
+		k_cg_pupdate<<<VG(k_cg_pupdate), 256, 0, st>>>(n, p, r, invD, S, gc);
+		RSD_CUDA(cudaGetLastError());
+		return RSD_OK;
+	};
+	// FP64 check of the final iterate: ||b - A x|| into S1->res
+	auto epilogue = [&]() -> int {
+		RSD_DISPATCH_L(L, (k_true_res<LL><<<RG(k_true_res<LL>), 256, 0, st>>>(n, V, b, x, partials, &S1->ticket, &S1->res)));
+		RSD_CUDA(cudaGetLastError());
+		return RSD_OK;
+	};
+	if (graph_mode(ctx)) {
+		CgGraph& G = graph_cache(ctx)->cg[0];
+		CgKey key{};
+		const void* ptrs[] = {A, V.ptr, V.col, V.val, exec_diag(A), b, x, r, invD, S, partials};
+		std::copy(std::begin(ptrs), std::end(ptrs), key.p);
+		const int64_t ints[] = {n, L, maxIt, rel};
+		std::copy(std::begin(ints), std::end(ints), key.i);
+		key.d[0] = tol;
+		if (!G.valid || !(G.key == key)) {
+			RSD_CHECK(build_cg_graph(ctx, false, body_limit(maxIt), prologue, body_a, [] { return RSD_OK; }, body_b, epilogue, &G));
+			G.key = key;
+		}
+		RSD_CUDA(cudaGraphLaunch(G.exec, st));
+		RSD_CHECK(finish_report(ctx, S, rep));
+	} else {
+		RSD_CHECK(prologue());
+		Poller poll{ctx, S, (int32_t*)ctx->s.hbuf};
+		RSD_CHECK(poll.init());
+		const int chunk = 8;
+		bool fin = false;
+		std::vector<int> pairs;
+		const GraphCtl off{0, 0, 0, 0};
+		for (int64_t it = 0; it < maxIt + 2 * chunk && !fin; it += chunk) {
+			for (int c = 0; c < chunk; ++c) {
+				int pr = prof_begin(ctx, PF_SPMV_DOT_F64);
+				RSD_DISPATCH_L(L, (k_cg_spmv_dot<LL><<<RG(k_cg_spmv_dot<LL>), 256, 0, st>>>(n, V, p, Ap, S, partials)));
+				prof_end(ctx, pr);
+				int pu = prof_begin(ctx, PF_CG_UPDATE);
+				k_cg_update<<<VG(k_cg_update), 256, 0, st>>>(n, x, r, p, Ap, invD, S, partials, tol, rel, maxIt);
+				prof_end(ctx, pu);
+				int pp = prof_begin(ctx, PF_CG_PUPDATE);
+				k_cg_pupdate<<<VG(k_cg_pupdate), 256, 0, st>>>(n, p, r, invD, S, off);
+				prof_end(ctx, pp);
+				if (pr >= 0) { pairs.push_back(pr); pairs.push_back(pu); pairs.push_back(pp); }
+			}
+			RSD_CUDA(cudaGetLastError());
+			RSD_CHECK(poll.post(&fin));
+		}
+		RSD_CHECK(finish_report(ctx, S, rep));
+		discard_idle(ctx, pairs, 3, rep ? rep->iterations : 0);
+		RSD_CHECK(epilogue());
 	}
-	RSD_CHECK(finish_report(ctx, S, rep));
-	discard_idle(ctx, pairs, 3, rep ? rep->iterations : 0);
-	// FP64 check of the final iterate: ||b - A x|| / ||r0||
-	double* tr = &scal_slot(ctx, 1)->res;
-	RSD_DISPATCH_L(L, (k_true_res<LL><<<gr, 256, 0, ctx->stream>>>(n, V, b, x, ctx->s.partials, &scal_slot(ctx, 1)->ticket, tr)));
-	RSD_CUDA(cudaGetLastError());
 	double h = 0.0;
-	RSD_CUDA(cudaMemcpyAsync(&h, tr, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+	RSD_CUDA(cudaMemcpyAsync(&h, &S1->res, sizeof(double), cudaMemcpyDeviceToHost, st));
+	RSD_CUDA(cudaStreamSynchronize(st));
 	if (rep) rep->trueResidualRel = h / (rep->initialResidual + 1e-50);
 	return RSD_OK;
 }
@@ -445,49 +631,103 @@ static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const d
 	const MatView<double> V = view64(A);
 	const MatView<float> V32 = view32(A);
 	void* wsv;
-	RSD_CHECK(get_ws(ctx, sizeof(float) * (5 * n + 64), &wsv));
+	const int64_t ns = pad_len(n);
+	RSD_CHECK(get_ws(ctx, sizeof(float) * 5 * ns, &wsv));
 	float* r = (float*)wsv;
-	float* p = r + n;
-	float* Ap = p + n;
-	float* y = Ap + n;
-	float* invD = cfg->precond == RSD_JACOBI ? y + n : nullptr;
+	float* p = r + ns;
+	float* Ap = p + ns;
+	float* y = Ap + ns;
+	float* invD = cfg->precond == RSD_JACOBI ? y + ns : nullptr;
 	CgScal* S = scal_slot(ctx, 0);
-	RSD_CUDA(cudaMemsetAsync(S, 0, sizeof(CgScal), ctx->stream));
+	double* partials = ctx->s.partials;
 	const int rel = cfg->tol_type == RSD_TOL_RELATIVE;
 	const double delta = cfg->reliable_delta > 0 ? cfg->reliable_delta : 0.1;
-	const int gr = row_blocks(ctx, n, L), gv = vec_blocks(ctx, n);
-	if (invD) k_invdiag32<<<gv, 256, 0, ctx->stream>>>(n, exec_diag(A), exec_val(A), invD);
-	RSD_DISPATCH_L(L, (k_mx_init<LL><<<gr, 256, 0, ctx->stream>>>(n, V, b, x, r, p, y, invD, S, ctx->s.partials, cfg->tol, rel, cfg->max_iters)));
-	RSD_CUDA(cudaGetLastError());
-	Poller poll{ctx, S, (int32_t*)ctx->s.hbuf};
-	RSD_CHECK(poll.init());
-	const int chunk = 8;
-	bool fin = false;
-	std::vector<int> pairs;
-	for (int64_t it = 0; it < cfg->max_iters + 2 * chunk && !fin; it += chunk) {
-		for (int c = 0; c < chunk; ++c) {
-			int pr = prof_begin(ctx, PF_SPMV_DOT_F32);
-			RSD_DISPATCH_L(L, (k_mx_spmv_dot<LL><<<gr, 256, 0, ctx->stream>>>(n, V32, p, Ap, S, ctx->s.partials)));
-			prof_end(ctx, pr);
-			int pu = prof_begin(ctx, PF_CG_UPDATE);
-			k_mx_update<<<gv, 256, 0, ctx->stream>>>(n, y, r, p, Ap, invD, S, ctx->s.partials, cfg->tol, rel, cfg->max_iters, delta);
-			prof_end(ctx, pu);
-			int pq = prof_begin(ctx, PF_RELIABLE);
-			RSD_DISPATCH_L(L, (k_mx_reliable<LL><<<gr, 256, 0, ctx->stream>>>(n, V, b, x, y, r, invD, S, ctx->s.partials, cfg->tol, rel, cfg->max_iters)));
-			prof_end(ctx, pq);
-			int pp = prof_begin(ctx, PF_CG_PUPDATE);
-			k_mx_pupdate<<<gv, 256, 0, ctx->stream>>>(n, x, y, p, r, invD, S);
-			prof_end(ctx, pp);
-			if (pr >= 0) { pairs.push_back(pr); pairs.push_back(pu); pairs.push_back(pq); pairs.push_back(pp); }
-		}
+	const double tol = cfg->tol;
+	const int64_t maxIt = cfg->max_iters;
+	cudaStream_t st = ctx->stream;
+	auto prologue = [&]() -> int {
+		RSD_CUDA(cudaMemsetAsync(S, 0, sizeof(CgScal), st));
+		if (invD) k_invdiag32<<<VG(k_invdiag32), 256, 0, st>>>(n, exec_diag(A), exec_val(A), invD);
+		RSD_DISPATCH_L(L, (k_mx_init<LL><<<RG(k_mx_init<LL>), 256, 0, st>>>(n, V, b, x, r, p, y, invD, S, partials, tol, rel, maxIt)));
 		RSD_CUDA(cudaGetLastError());
-		RSD_CHECK(poll.post(&fin));
+		return RSD_OK;
+	};
+	auto body_a = [&](GraphCtl gc) -> int {
+		RSD_DISPATCH_L(L, (k_mx_spmv_dot<LL><<<RG(k_mx_spmv_dot<LL>), 256, 0, st>>>(n, V32, p, Ap, S, partials)));
+		k_mx_update<<<VG(k_mx_update), 256, 0, st>>>(n, y, r, p, Ap, invD, S, partials, tol, rel, maxIt, delta, gc);
+		RSD_CUDA(cudaGetLastError());
+		return RSD_OK;
+	};
+	auto reliable = [&]() -> int {
+		RSD_DISPATCH_L(L, (k_mx_reliable<LL><<<RG(k_mx_reliable<LL>), 256, 0, st>>>(n, V, b, x, y, r, invD, S, partials, tol, rel, maxIt)));
+		RSD_CUDA(cudaGetLastError());
+		return RSD_OK;
+	};
+	auto body_b = [&](GraphCtl gc) -> int {
+		k_mx_pupdate<<<VG(k_mx_pupdate), 256, 0, st>>>(n, x, y, p, r, invD, S, gc);
+		RSD_CUDA(cudaGetLastError());
+		return RSD_OK;
+	};
+	if (graph_mode(ctx)) {
+		CgGraph& G = graph_cache(ctx)->cg[1];
+		CgKey key{};
+		const void* ptrs[] = {A, V.ptr, V.col, V.val, V32.val, exec_diag(A), b, x, r, invD, S, partials};
+		std::copy(std::begin(ptrs), std::end(ptrs), key.p);
+		const int64_t ints[] = {n, L, maxIt, rel};
+		std::copy(std::begin(ints), std::end(ints), key.i);
+		key.d[0] = tol;
+		key.d[1] = delta;
+		if (!G.valid || !(G.key == key)) {
+			RSD_CHECK(build_cg_graph(ctx, true, body_limit(maxIt), prologue, body_a, reliable, body_b, [] { return RSD_OK; }, &G));
+			G.key = key;
+		}
+		RSD_CUDA(cudaGraphLaunch(G.exec, st));
+		RSD_CHECK(finish_report(ctx, S, rep));
+	} else {
+		RSD_CHECK(prologue());
+		Poller poll{ctx, S, (int32_t*)ctx->s.hbuf};
+		RSD_CHECK(poll.init());
+		const int chunk = 8;
+		bool fin = false;
+		std::vector<int> pairs;
+		const GraphCtl off{0, 0, 0, 0};
+		for (int64_t it = 0; it < maxIt + 2 * chunk && !fin; it += chunk) {
+			for (int c = 0; c < chunk; ++c) {
+				int pr = prof_begin(ctx, PF_SPMV_DOT_F32);
+				RSD_DISPATCH_L(L, (k_mx_spmv_dot<LL><<<RG(k_mx_spmv_dot<LL>), 256, 0, st>>>(n, V32, p, Ap, S, partials)));
+				prof_end(ctx, pr);
+				int pu = prof_begin(ctx, PF_CG_UPDATE);
+				k_mx_update<<<VG(k_mx_update), 256, 0, st>>>(n, y, r, p, Ap, invD, S, partials, tol, rel, maxIt, delta, off);
+				prof_end(ctx, pu);
+				int pq = prof_begin(ctx, PF_RELIABLE);
+				RSD_CHECK(reliable());
+				prof_end(ctx, pq);
+				int pp = prof_begin(ctx, PF_CG_PUPDATE);
+				k_mx_pupdate<<<VG(k_mx_pupdate), 256, 0, st>>>(n, x, y, p, r, invD, S, off);
+				prof_end(ctx, pp);
+				if (pr >= 0) { pairs.push_back(pr); pairs.push_back(pu); pairs.push_back(pq); pairs.push_back(pp); }
+			}
+			RSD_CUDA(cudaGetLastError());
+			RSD_CHECK(poll.post(&fin));
+		}
+		RSD_CHECK(finish_report(ctx, S, rep));
+		discard_idle(ctx, pairs, 4, rep ? rep->iterations : 0);
 	}
-	RSD_CHECK(finish_report(ctx, S, rep));
-	discard_idle(ctx, pairs, 4, rep ? rep->iterations : 0);
 	if (rep) { rep->finalResidual = rep->trueResidualRel * rep->initialResidual; rep->finalResidualRel = rep->trueResidualRel; }
 	return RSD_OK;
 }
+
+}  // namespace
+
+void free_graph_cache(rsd_ctx* ctx) {
+	if (!ctx->graphs) return;
+	GraphCache* c = static_cast<GraphCache*>(ctx->graphs);
+	for (CgGraph& g : c->cg) g.release();
+	delete c;
+	ctx->graphs = nullptr;
+}
+
+namespace {
 
 // ---- GMRES(m): linalg/solver/iterative/gmres/Solver.tpp:3-170 ---------------------------------
 // Device: SpMV, preconditioner, the MGS dot/axpy pairs (each h_ij stays on the device), norms and
@@ -540,7 +780,7 @@ static int gmres_fp64(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const
 	double* invD = cfg->precond == RSD_JACOBI ? z + n : nullptr;
 	double* dH = z + 2 * n;          // device column buffer: h_0..h_{j+1}, plus y
 	double* dY = dH + (m + 2);
-	const int gv = vec_blocks(ctx, n), grd = red_grid(ctx, n);
+	const int gv = vec_grid(ctx, n), grd = red_grid(ctx, n);
 	unsigned* ticket = &scal_slot(ctx, 2)->ticket;
 	const bool relMode = cfg->tol_type == RSD_TOL_RELATIVE;
 	const double breakdownTol = 1e-14, eps = 1e-50;
@@ -637,7 +877,7 @@ static int gmres_fp64(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const
 // scratch buffer carved from one file-scope device array instead of the context's workspace: the
 // call allocates nothing.  The array is sized for kStaticMaxRows rows; one array per device, shared
 // by every call on that device.
-constexpr int64_t kStaticMaxRows = int64_t(1) << 18;                 // 262,144 rows
+constexpr int64_t kStaticMaxRows = int64_t(1) << 18;                 // 262,144 rows (a multiple of 64)
 constexpr size_t kStaticHeadBytes = 2 * sizeof(DevScalars) + sizeof(double) * 2 * kMaxPartials;
 constexpr size_t kStaticHeadAligned = (kStaticHeadBytes + 255) & ~size_t(255);
 constexpr size_t kStaticScratchBytes = kStaticHeadAligned + sizeof(double) * 4 * kStaticMaxRows;   // 8 MiB + 19 KiB
@@ -674,26 +914,26 @@ static int cg_fp64_static(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, c
 	CgScal* S = reinterpret_cast<CgScal*>(base);
 	CgScal* S1 = reinterpret_cast<CgScal*>(base + sizeof(DevScalars));
 	double* partials = reinterpret_cast<double*>(base + 2 * sizeof(DevScalars));
+	const int64_t ns = pad_len(n);   // kStaticMaxRows is a multiple of the padding
 	double* r = reinterpret_cast<double*>(base + kStaticHeadAligned);
-	double* p = r + n;
-	double* Ap = p + n;
-	double* invD = cfg->precond == RSD_JACOBI ? Ap + n : nullptr;
+	double* p = r + ns;
+	double* Ap = p + ns;
+	double* invD = cfg->precond == RSD_JACOBI ? Ap + ns : nullptr;
 	// the reduction tickets and the done/converged flags must start at zero on every call
 	RSD_CUDA(cudaMemsetAsync(base, 0, 2 * sizeof(DevScalars), ctx->stream));
 	RSD_CHECK(exec_sync(ctx, A));
 	const int L = exec_lanes(A);
 	const MatView<double> V = view64(A);
 	const int rel = cfg->tol_type == RSD_TOL_RELATIVE;
-	const int gr = row_blocks(ctx, n, L), gv = vec_blocks(ctx, n);
-	if (invD) k_invdiag64<<<gv, 256, 0, ctx->stream>>>(n, exec_diag(A), exec_val(A), invD);
-	RSD_DISPATCH_L(L, (k_cg_init<LL><<<gr, 256, 0, ctx->stream>>>(n, V, b, x, r, p, invD, S, partials, cfg->tol, rel, cfg->max_iters)));
+	if (invD) k_invdiag64<<<VG(k_invdiag64), 256, 0, ctx->stream>>>(n, exec_diag(A), exec_val(A), invD);
+	RSD_DISPATCH_L(L, (k_cg_init<LL><<<RG(k_cg_init<LL>), 256, 0, ctx->stream>>>(n, V, b, x, r, p, invD, S, partials, cfg->tol, rel, cfg->max_iters)));
 	RSD_CUDA(cudaGetLastError());
 	const int chunk = 8;
 	for (int64_t it = 0; it < cfg->max_iters + 2 * chunk; it += chunk) {
 		for (int c = 0; c < chunk; ++c) {
-			RSD_DISPATCH_L(L, (k_cg_spmv_dot<LL><<<gr, 256, 0, ctx->stream>>>(n, V, p, Ap, S, partials)));
-			k_cg_update<<<gv, 256, 0, ctx->stream>>>(n, x, r, p, Ap, invD, S, partials, cfg->tol, rel, cfg->max_iters);
-			k_cg_pupdate<<<gv, 256, 0, ctx->stream>>>(n, p, r, invD, S);
+			RSD_DISPATCH_L(L, (k_cg_spmv_dot<LL><<<RG(k_cg_spmv_dot<LL>), 256, 0, ctx->stream>>>(n, V, p, Ap, S, partials)));
+			k_cg_update<<<VG(k_cg_update), 256, 0, ctx->stream>>>(n, x, r, p, Ap, invD, S, partials, cfg->tol, rel, cfg->max_iters);
+			k_cg_pupdate<<<VG(k_cg_pupdate), 256, 0, ctx->stream>>>(n, p, r, invD, S, GraphCtl{0, 0, 0, 0});
 		}
 		RSD_CUDA(cudaGetLastError());
 		int32_t done = 0;   // pageable host word: the copy returns once the flag has been read
@@ -703,7 +943,7 @@ static int cg_fp64_static(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, c
 	}
 	RSD_CHECK(finish_report(ctx, S, rep));
 	double* tr = &S1->res;
-	RSD_DISPATCH_L(L, (k_true_res<LL><<<gr, 256, 0, ctx->stream>>>(n, V, b, x, partials, &S1->ticket, tr)));
+	RSD_DISPATCH_L(L, (k_true_res<LL><<<RG(k_true_res<LL>), 256, 0, ctx->stream>>>(n, V, b, x, partials, &S1->ticket, tr)));
 	RSD_CUDA(cudaGetLastError());
 	double h = 0.0;
 	RSD_CUDA(cudaMemcpyAsync(&h, tr, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));

@@ -134,7 +134,7 @@ def random_csr(n, per_row, seed):
     return rp, col, val
 
 
-@pytest.mark.parametrize("n,per_row", [(1, 1), (7, 3), (1000, 9), (20000, 27), (5000, 120)])
+@pytest.mark.parametrize("n,per_row", [(1, 1), (7, 3), (1000, 9), (20000, 27), (5000, 120), (100000, 5)])
 def test_spmv_matches_reference(rsd, ctx, n, per_row):
     rp, col, val = random_csr(n, per_row, n)
     A = rsd.CSR.from_host(ctx, rp, col, val)
@@ -240,6 +240,38 @@ def test_mixed_precision_reaches_fp64_checked_tolerance(rsd, ctx):
     assert r64["trueResidualRel"] < 1.01e-8
     # stated error against the FP64 solve: both within tol * cond of the exact solution
     assert relerr(xmx.download(), x64.download()) < 1e-6
+
+
+def test_graph_solve_matches_plain_launches(rsd, ctx, monkeypatch):
+    # The CG solve runs as one CUDA graph (device-side WHILE loop, IF node for the FP64 residual
+    # replacement); the plain launch sequence runs the same kernels, so both give the same iterates.
+    h = make_heat(rsd, ctx, 3, 1, 2, [30, 26, 22], [0, 0, 0], [1, 1, 1], src_expr="1 + x", dirichlet={0: "0", 2: "y"})
+    n = h.n
+    h.assemble_matrix(1.0, 200.0)
+    F = ctx.array(n)
+    h.assemble_vector(0, F)
+    for prec in (rsd.FP64, rsd.MIXED):
+        outs = []
+        for mode in ("1", "0", "1"):            # graph, plain, graph again (cached graph reused)
+            monkeypatch.setenv("RSD_CG_GRAPH", mode)
+            x = ctx.array(n).zero()
+            rep = rsd.solve(ctx, h.K, F, x, type=rsd.CG, precision=prec, tol=1e-9, max_iters=5000)
+            assert rep["converged"]
+            outs.append((rep["iterations"], rep["trueResidualRel"], x.download()))
+        for it, tr, xv in outs[1:]:
+            assert it == outs[0][0] and tr == outs[0][1] and np.array_equal(xv, outs[0][2])
+        # a different right-hand side buffer rebuilds the graph; the answer follows the new b
+        G = ctx.to_device(2.0 * F.download())
+        x2 = ctx.array(n).zero()
+        monkeypatch.setenv("RSD_CG_GRAPH", "1")
+        rep = rsd.solve(ctx, h.K, G, x2, type=rsd.CG, precision=prec, tol=1e-9, max_iters=5000)
+        assert rep["converged"] and relerr(x2.download(), 2.0 * outs[0][2]) < 1e-6
+    # max_iters reached inside the graph: not converged, iteration count as the plain path reports
+    for mode in ("1", "0"):
+        monkeypatch.setenv("RSD_CG_GRAPH", mode)
+        x = ctx.array(n).zero()
+        rep = rsd.solve(ctx, h.K, F, x, type=rsd.CG, tol=1e-14, max_iters=7)
+        assert not rep["converged"] and rep["iterations"] == 7
 
 
 def test_edge_cases(rsd, ctx):
