@@ -67,7 +67,7 @@ typedef struct rsd_solver_cfg {
 	double tol;
 	int64_t max_iters;
 	int64_t krylov_dim;          /* GMRES restart length m */
-	double reliable_delta;       /* mixed CG: FP64 residual replacement when |r| falls by this factor (0: 0.1) */
+	double reliable_delta;       /* mixed CG: FP64 residual replacement when |r| falls by this factor (0: 1e-3) */
 } rsd_solver_cfg;
 
 /* ---- lifetime (linalg/types/backend/CUDA.hpp:23-73 has no context; these give it one) ---- */
@@ -207,6 +207,20 @@ int rsd_heat_be_step(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver_cfg*
  * solver/stage/SteadyStage.hpp:89-116): R = F - K(T)T, J = K + K_T, J dU = R, U += dU */
 int rsd_heat_newton(rsd_ctx* ctx, rsd_heat* h, double abs_tol, double rel_tol, int64_t max_iters,
                     const rsd_solver_cfg* linear, double* U, rsd_report* report);
+
+/* ---- adjoint pair, in the shape of an autograd Function (no counterpart in the reference) ----
+ * Steady linear heat with per-element conductivity k_e = k_const * exp(theta_e) (rsd_heat_desc's
+ * k_expr must be unset).  theta: device, one value per element; T, dJdT: device, free DOFs;
+ * dJdtheta: device, one value per element.
+ * forward:  sets k_e from theta, assembles K(theta), F and the Dirichlet lift, solves K T = F
+ *           (T holds the warm start on entry).
+ * backward: rebuilds K(theta) (nothing is saved between the calls), solves the adjoint system
+ *           K lambda = dJ/dT, and returns dJ/dtheta_e = -k_e * int_e grad(lambda) . grad(T) with T
+ *           carrying its Dirichlet values.  For J = 0.5 ||T - T_obs||^2 pass dJdT = T - T_obs. */
+int rsd_heat_forward(rsd_ctx* ctx, rsd_heat* h, const double* theta, const rsd_solver_cfg* cfg, double* T,
+                     rsd_report* report);
+int rsd_heat_backward(rsd_ctx* ctx, rsd_heat* h, const double* theta, const double* T, const double* dJdT,
+                      const rsd_solver_cfg* cfg, double* dJdtheta, rsd_report* report);
 
 #ifdef __cplusplus
 }

@@ -113,6 +113,8 @@ SIGNATURES = {
     "rsd_heat_steady": [_P, _P, C.POINTER(SolverConfig), _P, C.POINTER(Report)],
     "rsd_heat_be_step": [_P, _P, _D, C.POINTER(SolverConfig), _P, _P, C.POINTER(Report), C.POINTER(_D)],
     "rsd_heat_newton": [_P, _P, _D, _D, _I64, C.POINTER(SolverConfig), _P, C.POINTER(Report)],
+    "rsd_heat_forward": [_P, _P, _P, C.POINTER(SolverConfig), _P, C.POINTER(Report)],
+    "rsd_heat_backward": [_P, _P, _P, _P, _P, C.POINTER(SolverConfig), _P, C.POINTER(Report)],
 }
 
 
@@ -224,7 +226,14 @@ class DeviceArray:
 
 
 def _ptr(a):
-    return None if a is None else (a.ptr if isinstance(a, DeviceArray) else a)
+    """Device pointer of a DeviceArray, a torch CUDA tensor (data_ptr), or a raw pointer."""
+    if a is None:
+        return None
+    if isinstance(a, DeviceArray):
+        return a.ptr
+    if hasattr(a, "data_ptr"):
+        return C.c_void_p(a.data_ptr())
+    return a
 
 
 class CSR:
@@ -404,6 +413,22 @@ class Heat:
         d = rep.as_dict()
         d["residualNorm"] = res.value
         return d
+
+    def forward(self, theta, T, cfg=None, **kw):
+        """Adjoint pair, forward: k_e = k_const exp(theta_e), solve K(theta) T = F (T: warm start in,
+        solution out).  theta, T: device arrays (DeviceArray or anything with .ptr / data_ptr())."""
+        cfg = cfg or SolverConfig.make(**kw)
+        rep = Report()
+        check(lib().rsd_heat_forward(self.ctx.h, self.h, _ptr(theta), C.byref(cfg), _ptr(T), C.byref(rep)))
+        return rep.as_dict()
+
+    def backward(self, theta, T, dJdT, dJdtheta, cfg=None, **kw):
+        """Adjoint pair, backward: solve K lambda = dJ/dT and write dJ/dtheta per element."""
+        cfg = cfg or SolverConfig.make(**kw)
+        rep = Report()
+        check(lib().rsd_heat_backward(self.ctx.h, self.h, _ptr(theta), _ptr(T), _ptr(dJdT), C.byref(cfg),
+                                      _ptr(dJdtheta), C.byref(rep)))
+        return rep.as_dict()
 
     def newton(self, U, abs_tol=1e-10, rel_tol=1e-10, max_iters=50, cfg=None, **kw):
         cfg = cfg or SolverConfig.make(type=GMRES, **kw)

@@ -51,6 +51,17 @@ __global__ void k_be_rate(int64_t n, double inv_dt, const double* __restrict__ U
 }
 // |F - R| with the deterministic grid reduction: axpby(1, -1, F, R) then norm(R)
 // (BackwardEulerStage.hpp:120-122), without storing F - R
+// k_e = exp(theta_e): the per-element conductivity multiplier of the adjoint pair
+__global__ void k_exp_theta(int64_t ne, const double* __restrict__ theta, double* __restrict__ kElem) {
+	for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne; e += (int64_t)gridDim.x * blockDim.x)
+		kElem[e] = exp(theta[e]);
+}
+// dJ/dtheta_e = -(dk_e/dtheta_e) * k0 * g_e with dk_e/dtheta_e = k_e and g_e = int_e grad(lambda) . grad(T)
+__global__ void k_adjoint_scale(int64_t ne, const double* __restrict__ kElem, double k0, double* __restrict__ g) {
+	for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne; e += (int64_t)gridDim.x * blockDim.x)
+		g[e] = -(kElem[e] * k0) * g[e];
+}
+
 __global__ void k_diff_norm(int64_t n, const double* __restrict__ F, const double* __restrict__ R, double* partials,
                             unsigned* ticket, double* out) {
 	double v[1] = {0.0};
@@ -274,6 +285,52 @@ int rsd_heat_newton(rsd_ctx* ctx, rsd_heat* h, double abs_tol, double rel_tol, i
 		if (it == max_iters - 1) R.iterations = max_iters;
 	}
 	if (rep) *rep = R;
+	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+	return RSD_OK;
+}
+
+// ---- adjoint pair (no counterpart in the reference; the gradient's element loop follows
+// DiffusionForm::computeElementLevelMatrix, equation/heateq/form/DiffusionForm.hpp:11-52) ----
+static int adjoint_check(rsd_ctx* ctx, rsd_heat* h, const double* theta, const rsd_solver_cfg* cfg) {
+	if (!ctx || !h || !theta || !cfg) return set_error(RSD_EINVAL, "null argument");
+	if (h->kExpr.n) return set_error(RSD_EINVAL, "the adjoint pair needs a constant conductivity (k_expr unset)");
+	if (!h->kElem) RSD_CUDA(cudaMalloc(&h->kElem, sizeof(double) * std::max<int64_t>(h->m->nelem, 1)));
+	const int64_t ne = h->m->nelem;
+	if (ne) {
+		k_exp_theta<<<vec_grid(ctx, ne), 256, 0, ctx->stream>>>(ne, theta, h->kElem);
+		RSD_CUDA(cudaGetLastError());
+	}
+	return RSD_OK;
+}
+
+int rsd_heat_forward(rsd_ctx* ctx, rsd_heat* h, const double* theta, const rsd_solver_cfg* cfg, double* T, rsd_report* rep) {
+	if (!T) return set_error(RSD_EINVAL, "null argument");
+	RSD_CHECK(adjoint_check(ctx, h, theta, cfg));
+	RSD_CHECK(assemble_matrix(ctx, h, 1.0, 0.0, 0.0, 0.0, T, nullptr, h->K));
+	RSD_CHECK(assemble_vector(ctx, h, 0, 0.0, T, nullptr, nullptr, h->F, 1.0, false));
+	RSD_CHECK(assemble_lift(ctx, h, 1.0, 0.0, h->F));
+	RSD_CHECK(solve(ctx, h->K, cfg, h->F, T, rep));
+	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+	return RSD_OK;
+}
+
+int rsd_heat_backward(rsd_ctx* ctx, rsd_heat* h, const double* theta, const double* T, const double* dJdT,
+                      const rsd_solver_cfg* cfg, double* dJdtheta, rsd_report* rep) {
+	if (!T || !dJdT || !dJdtheta) return set_error(RSD_EINVAL, "null argument");
+	RSD_CHECK(adjoint_check(ctx, h, theta, cfg));
+	// K(theta) again (the forward's matrix may have been overwritten since); K is symmetric, so the
+	// adjoint system K^T lambda = dJ/dT is solved with the same matrix
+	RSD_CHECK(assemble_matrix(ctx, h, 1.0, 0.0, 0.0, 0.0, T, nullptr, h->K));
+	const int64_t n = h->n, ne = h->m->nelem;
+	double* lam = h->dU;
+	RSD_CUDA(cudaMemsetAsync(lam, 0, sizeof(double) * std::max<int64_t>(n, 1), ctx->stream));
+	RSD_CHECK(solve(ctx, h->K, cfg, dJdT, lam, rep));
+	// g_e = int_e grad(lambda) . grad(T) (T with its Dirichlet values, lambda zero there), then scale
+	RSD_CHECK(assemble_vector(ctx, h, 6, 0.0, T, nullptr, lam, dJdtheta, 1.0, false));
+	if (ne) {
+		k_adjoint_scale<<<vec_grid(ctx, ne), 256, 0, ctx->stream>>>(ne, h->kElem, h->k_const, dJdtheta);
+		RSD_CUDA(cudaGetLastError());
+	}
 	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
 	return RSD_OK;
 }

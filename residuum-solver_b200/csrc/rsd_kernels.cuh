@@ -71,6 +71,51 @@ __device__ __forceinline__ void sth(float* a, float v, uint64_t pol) {
 	asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(a), "f"(v), "l"(pol) : "memory");
 }
 
+// 16-byte packets for the element-wise Krylov kernels (4 floats or 2 doubles per load/store)
+template <typename T> struct Pk;
+template <> struct Pk<float> { static constexpr int W = 4; float v[4]; };
+template <> struct Pk<double> { static constexpr int W = 2; double v[2]; };
+__device__ __forceinline__ Pk<float> ldp(const float* a, uint64_t pol) {
+	Pk<float> r;
+	asm volatile("ld.global.nc.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"
+	             : "=f"(r.v[0]), "=f"(r.v[1]), "=f"(r.v[2]), "=f"(r.v[3]) : "l"(a), "l"(pol));
+	return r;
+}
+__device__ __forceinline__ Pk<float> ldp_rw(const float* a, uint64_t pol) {
+	Pk<float> r;
+	asm volatile("ld.global.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"
+	             : "=f"(r.v[0]), "=f"(r.v[1]), "=f"(r.v[2]), "=f"(r.v[3]) : "l"(a), "l"(pol));
+	return r;
+}
+__device__ __forceinline__ void stp(float* a, const Pk<float>& r, uint64_t pol) {
+	asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1,%2,%3,%4}, %5;"
+	             ::"l"(a), "f"(r.v[0]), "f"(r.v[1]), "f"(r.v[2]), "f"(r.v[3]), "l"(pol) : "memory");
+}
+__device__ __forceinline__ Pk<double> ldp(const double* a, uint64_t pol) {
+	Pk<double> r;
+	asm volatile("ld.global.nc.L2::cache_hint.v2.f64 {%0,%1}, [%2], %3;" : "=d"(r.v[0]), "=d"(r.v[1]) : "l"(a), "l"(pol));
+	return r;
+}
+__device__ __forceinline__ Pk<double> ldp_rw(const double* a, uint64_t pol) {
+	Pk<double> r;
+	asm volatile("ld.global.L2::cache_hint.v2.f64 {%0,%1}, [%2], %3;" : "=d"(r.v[0]), "=d"(r.v[1]) : "l"(a), "l"(pol));
+	return r;
+}
+__device__ __forceinline__ void stp(double* a, const Pk<double>& r, uint64_t pol) {
+	asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1,%2}, %3;" ::"l"(a), "d"(r.v[0]), "d"(r.v[1]), "l"(pol) : "memory");
+}
+
+// Element-wise loop over [0, n): f(i0, W) on 16-byte packets (i0 a multiple of W) when `vec`, the
+// scalar tail (and everything when !vec) as f(i, 1).  f must handle both widths.
+template <typename T, typename F>
+__device__ __forceinline__ void packet_loop(int64_t n, bool vec, F f) {
+	constexpr int W = Pk<T>::W;
+	const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, nth = (int64_t)gridDim.x * blockDim.x;
+	const int64_t nv = vec ? n / W : 0;
+	for (int64_t iv = tid; iv < nv; iv += nth) f(iv * W, W);
+	for (int64_t i = nv * W + tid; i < n; i += nth) f(i, 1);
+}
+
 template <int W, typename T>
 __device__ __forceinline__ T group_sum(T v) {
 #pragma unroll

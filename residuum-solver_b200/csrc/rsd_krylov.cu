@@ -109,19 +109,36 @@ __global__ void __launch_bounds__(256) k_cg_spmv_dot(int64_t n, MatView<double> 
 __global__ void __launch_bounds__(256) k_cg_update(int64_t n, double* __restrict__ x, double* __restrict__ r,
                                                    const double* __restrict__ p, const double* __restrict__ Ap,
                                                    const double* __restrict__ invD, CgScal* S, double* partials, double tol,
-                                                   int relMode, int64_t maxIters) {
+                                                   int relMode, int64_t maxIters, int vec) {
 	if (is_done(S)) return;
 	const double alpha = S->alpha;
 	const L2Pol pol = make_l2pol();
+	const uint64_t h = pol.last;
 	double v[2] = {0.0, 0.0};
-	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-		sth(x + i, ldh_rw(x + i, pol.last) + alpha * ldh(p + i, pol.last), pol.last);
-		const double ri = ldh_rw(r + i, pol.last) + (-alpha) * ldh(Ap + i, pol.last);
-		sth(r + i, ri, pol.last);
-		const double zi = invD ? ri * ldh(invD + i, pol.last) : ri;
-		v[0] += ri * ri;
-		v[1] += ri * zi;
-	}
+	packet_loop<double>(n, vec, [&](int64_t i, int w) {
+		if (w > 1) {
+			Pk<double> X = ldp_rw(x + i, h), P = ldp(p + i, h), R = ldp_rw(r + i, h), Q = ldp(Ap + i, h), D;
+			if (invD) D = ldp(invD + i, h);
+#pragma unroll
+			for (int k = 0; k < Pk<double>::W; ++k) {
+				X.v[k] = X.v[k] + alpha * P.v[k];
+				const double ri = R.v[k] + (-alpha) * Q.v[k];
+				R.v[k] = ri;
+				const double zi = invD ? ri * D.v[k] : ri;
+				v[0] += ri * ri;
+				v[1] += ri * zi;
+			}
+			stp(x + i, X, h);
+			stp(r + i, R, h);
+		} else {
+			sth(x + i, ldh_rw(x + i, h) + alpha * ldh(p + i, h), h);
+			const double ri = ldh_rw(r + i, h) + (-alpha) * ldh(Ap + i, h);
+			sth(r + i, ri, h);
+			const double zi = invD ? ri * ldh(invD + i, h) : ri;
+			v[0] += ri * ri;
+			v[1] += ri * zi;
+		}
+	});
 	if (grid_sum<2>(v, partials, &S->ticket)) {
 		const int64_t k = S->iter + 1;
 		const double res = sqrt(v[0]);
@@ -142,11 +159,20 @@ __global__ void __launch_bounds__(256) k_cg_pupdate(int64_t n, double* __restric
 	if (is_done(S)) return;
 	const double beta = S->beta;
 	const L2Pol pol = make_l2pol();
-	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-		const double ri = ldh(r + i, pol.last);
-		const double zi = invD ? ri * ldh(invD + i, pol.last) : ri;
-		sth(p + i, ldh_rw(p + i, pol.last) * beta + 1.0 * zi, pol.last);   // the next SpMV gathers p
-	}
+	const uint64_t h = pol.last;   // the next SpMV gathers p
+	packet_loop<double>(n, true, [&](int64_t i, int w) {
+		if (w > 1) {
+			Pk<double> P = ldp_rw(p + i, h), R = ldp(r + i, h), D;
+			if (invD) D = ldp(invD + i, h);
+#pragma unroll
+			for (int k = 0; k < Pk<double>::W; ++k) P.v[k] = P.v[k] * beta + 1.0 * (invD ? R.v[k] * D.v[k] : R.v[k]);
+			stp(p + i, P, h);
+		} else {
+			const double ri = ldh(r + i, h);
+			const double zi = invD ? ri * ldh(invD + i, h) : ri;
+			sth(p + i, ldh_rw(p + i, h) * beta + 1.0 * zi, h);
+		}
+	});
 }
 
 // ---- mixed precision PCG: FP32 matrix, vectors and recurrence; FP64 x, reductions and residual
@@ -213,15 +239,32 @@ __global__ void __launch_bounds__(256) k_mx_update(int64_t n, float* __restrict_
 	if (is_done(S)) return;
 	const float alpha = (float)S->alpha;
 	const L2Pol pol = make_l2pol();
+	const uint64_t h = pol.last;
 	double v[2] = {0.0, 0.0};
-	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-		sth(y + i, ldh_rw(y + i, pol.last) + alpha * ldh(p + i, pol.last), pol.last);
-		const float ri = ldh_rw(r + i, pol.last) - alpha * ldh(Ap + i, pol.last);
-		sth(r + i, ri, pol.last);
-		const float zi = invD ? ri * ldh(invD + i, pol.last) : ri;
-		v[0] += (double)ri * (double)ri;
-		v[1] += (double)ri * (double)zi;
-	}
+	packet_loop<float>(n, true, [&](int64_t i, int w) {
+		if (w > 1) {
+			Pk<float> Y = ldp_rw(y + i, h), P = ldp(p + i, h), R = ldp_rw(r + i, h), Q = ldp(Ap + i, h), D;
+			if (invD) D = ldp(invD + i, h);
+#pragma unroll
+			for (int k = 0; k < Pk<float>::W; ++k) {
+				Y.v[k] = Y.v[k] + alpha * P.v[k];
+				const float ri = R.v[k] - alpha * Q.v[k];
+				R.v[k] = ri;
+				const float zi = invD ? ri * D.v[k] : ri;
+				v[0] += (double)ri * (double)ri;
+				v[1] += (double)ri * (double)zi;
+			}
+			stp(y + i, Y, h);
+			stp(r + i, R, h);
+		} else {
+			sth(y + i, ldh_rw(y + i, h) + alpha * ldh(p + i, h), h);
+			const float ri = ldh_rw(r + i, h) - alpha * ldh(Ap + i, h);
+			sth(r + i, ri, h);
+			const float zi = invD ? ri * ldh(invD + i, h) : ri;
+			v[0] += (double)ri * (double)ri;
+			v[1] += (double)ri * (double)zi;
+		}
+	});
 	if (grid_sum<2>(v, partials, &S->ticket)) {
 		const int64_t k = S->iter + 1;
 		const double res = sqrt(v[0]);
@@ -284,17 +327,27 @@ __global__ void __launch_bounds__(256) k_mx_pupdate(int64_t n, double* __restric
 	if (!apply && done) return;
 	const float beta = (float)S->beta;
 	const L2Pol pol = make_l2pol();
-	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-		if (apply) {
-			sth(x + i, ldh_rw(x + i, pol.last) + (double)ldh_rw(y + i, pol.last), pol.last);
-			sth(y + i, 0.0f, pol.last);
-		}
-		if (!done) {
-			const float ri = ldh(r + i, pol.last);
-			const float zi = invD ? ri * ldh(invD + i, pol.last) : ri;
-			sth(p + i, ldh_rw(p + i, pol.last) * beta + zi, pol.last);   // the next SpMV gathers p
+	const uint64_t h = pol.last;
+	if (apply) {   // after a residual replacement: fold the FP32 correction into the FP64 iterate
+		for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+			sth(x + i, ldh_rw(x + i, h) + (double)ldh_rw(y + i, h), h);
+			sth(y + i, 0.0f, h);
 		}
 	}
+	if (done) return;
+	packet_loop<float>(n, true, [&](int64_t i, int w) {   // the next SpMV gathers p
+		if (w > 1) {
+			Pk<float> P = ldp_rw(p + i, h), R = ldp(r + i, h), D;
+			if (invD) D = ldp(invD + i, h);
+#pragma unroll
+			for (int k = 0; k < Pk<float>::W; ++k) P.v[k] = P.v[k] * beta + (invD ? R.v[k] * D.v[k] : R.v[k]);
+			stp(p + i, P, h);
+		} else {
+			const float ri = ldh(r + i, h);
+			const float zi = invD ? ri * ldh(invD + i, h) : ri;
+			sth(p + i, ldh_rw(p + i, h) * beta + zi, h);
+		}
+	});
 }
 
 __global__ void k_invdiag32(int64_t n, const int32_t* __restrict__ dpos, const double* __restrict__ val, float* __restrict__ d) {
@@ -543,6 +596,7 @@ static int cg_fp64(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const do
 	double* p = r + ns;
 	double* Ap = p + ns;
 	double* invD = cfg->precond == RSD_JACOBI ? Ap + ns : nullptr;
+	const int xvec = reinterpret_cast<uintptr_t>(x) % 16 == 0;   // 16-byte packets on x too
 	CgScal* S = scal_slot(ctx, 0);
 	CgScal* S1 = scal_slot(ctx, 1);
 	double* partials = ctx->s.partials;
@@ -560,7 +614,7 @@ static int cg_fp64(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const do
 	};
 	auto body_a = [&](GraphCtl) -> int {
 		RSD_DISPATCH_L(L, (k_cg_spmv_dot<LL><<<RG(k_cg_spmv_dot<LL>), 256, 0, st>>>(n, V, p, Ap, S, partials)));
-		k_cg_update<<<VG(k_cg_update), 256, 0, st>>>(n, x, r, p, Ap, invD, S, partials, tol, rel, maxIt);
+		k_cg_update<<<VG(k_cg_update), 256, 0, st>>>(n, x, r, p, Ap, invD, S, partials, tol, rel, maxIt, xvec);
 		RSD_CUDA(cudaGetLastError());
 		return RSD_OK;
 	};
@@ -603,7 +657,7 @@ static int cg_fp64(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const do
 				RSD_DISPATCH_L(L, (k_cg_spmv_dot<LL><<<RG(k_cg_spmv_dot<LL>), 256, 0, st>>>(n, V, p, Ap, S, partials)));
 				prof_end(ctx, pr);
 				int pu = prof_begin(ctx, PF_CG_UPDATE);
-				k_cg_update<<<VG(k_cg_update), 256, 0, st>>>(n, x, r, p, Ap, invD, S, partials, tol, rel, maxIt);
+				k_cg_update<<<VG(k_cg_update), 256, 0, st>>>(n, x, r, p, Ap, invD, S, partials, tol, rel, maxIt, xvec);
 				prof_end(ctx, pu);
 				int pp = prof_begin(ctx, PF_CG_PUPDATE);
 				k_cg_pupdate<<<VG(k_cg_pupdate), 256, 0, st>>>(n, p, r, invD, S, off);
@@ -641,7 +695,7 @@ static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const d
 	CgScal* S = scal_slot(ctx, 0);
 	double* partials = ctx->s.partials;
 	const int rel = cfg->tol_type == RSD_TOL_RELATIVE;
-	const double delta = cfg->reliable_delta > 0 ? cfg->reliable_delta : 0.1;
+	const double delta = cfg->reliable_delta > 0 ? cfg->reliable_delta : 1e-3;
 	const double tol = cfg->tol;
 	const int64_t maxIt = cfg->max_iters;
 	cudaStream_t st = ctx->stream;
@@ -919,6 +973,7 @@ static int cg_fp64_static(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, c
 	double* p = r + ns;
 	double* Ap = p + ns;
 	double* invD = cfg->precond == RSD_JACOBI ? Ap + ns : nullptr;
+	const int xvec = reinterpret_cast<uintptr_t>(x) % 16 == 0;
 	// the reduction tickets and the done/converged flags must start at zero on every call
 	RSD_CUDA(cudaMemsetAsync(base, 0, 2 * sizeof(DevScalars), ctx->stream));
 	RSD_CHECK(exec_sync(ctx, A));
@@ -932,7 +987,7 @@ static int cg_fp64_static(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, c
 	for (int64_t it = 0; it < cfg->max_iters + 2 * chunk; it += chunk) {
 		for (int c = 0; c < chunk; ++c) {
 			RSD_DISPATCH_L(L, (k_cg_spmv_dot<LL><<<RG(k_cg_spmv_dot<LL>), 256, 0, ctx->stream>>>(n, V, p, Ap, S, partials)));
-			k_cg_update<<<VG(k_cg_update), 256, 0, ctx->stream>>>(n, x, r, p, Ap, invD, S, partials, cfg->tol, rel, cfg->max_iters);
+			k_cg_update<<<VG(k_cg_update), 256, 0, ctx->stream>>>(n, x, r, p, Ap, invD, S, partials, cfg->tol, rel, cfg->max_iters, xvec);
 			k_cg_pupdate<<<VG(k_cg_pupdate), 256, 0, ctx->stream>>>(n, p, r, invD, S, GraphCtl{0, 0, 0, 0});
 		}
 		RSD_CUDA(cudaGetLastError());

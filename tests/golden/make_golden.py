@@ -1,6 +1,6 @@
 """Generate the golden fixtures in this folder from the reference's own templates.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [main] [adjoint]
 
 Every array comes from oracle/_ref/libresiduum_ref.so, i.e. the unmodified Residuum templates
 (Assembler<CPU>, BoundaryApplicator<CPU>, TopologicalDOF, cg/gmres::Solver, SteadyStage,
@@ -82,7 +82,41 @@ def main():
     save("newton_q2_hex_3.npz", U=U, iterations=rep["iterations"], finalResidual=rep["finalResidual"])
 
 
+def adjoint():
+    # adjoint pair: 3D Q1 6x5x4 on the unit cube, k_e = exp(theta_e), f = 1, T = 0 on every face but
+    # x = 1 (T = 0.5, so the gradient carries the lift's dependence on k); forward and adjoint solves
+    # by the reference CG + Jacobi to 1e-14, the element gradient by the reference DiffusionForm
+    rng = np.random.default_rng(55)
+    theta = 0.5 * rng.standard_normal(6 * 5 * 4)
+    r = oracle.Reference(3, 1, 2, [6, 5, 4], [0, 0, 0], [1, 1, 1], list(range(6)), bc_kind=0, bc_val={1: 0.5},
+                         src_kind=0, src_c=1.0, k_elem=np.exp(theta))
+    T, rep = r.steady(0, 1, 1e-14, 10000)
+    Tobs = 0.05 * np.sin(1.7 * np.arange(r.n))
+    rp, col = r.pattern()
+    K = r.assemble_matrix("K")
+    lam, lrep = oracle.ref_csr_solve(rp, col, K, T - Tobs, tol=1e-14, maxit=10000)
+    g = r.adjoint_gradient(T, lam)
+    grad = -np.exp(theta) * g
+    # central differences of J through the reference forward solve, as a check of the generator
+    d = rng.standard_normal(theta.size)
+    d /= np.linalg.norm(d)
+    h = 1e-6
+
+    def J(th):
+        rr = oracle.Reference(3, 1, 2, [6, 5, 4], [0, 0, 0], [1, 1, 1], list(range(6)), bc_kind=0, bc_val={1: 0.5},
+                              src_kind=0, src_c=1.0, k_elem=np.exp(th))
+        Tt, _ = rr.steady(0, 1, 1e-14, 10000)
+        return 0.5 * np.sum((Tt - Tobs) ** 2)
+
+    fd = (J(theta + h * d) - J(theta - h * d)) / (2 * h)
+    assert abs(fd - grad @ d) <= 1e-6 * abs(fd), (fd, grad @ d)
+    save("adjoint_q1_hex_6x5x4.npz", theta=theta, T=T, Tobs=Tobs, lam=lam, g=g, grad=grad, fd_dir=d, fd=fd)
+
+
+GROUPS = {"main": main, "adjoint": adjoint}
+
 if __name__ == "__main__":
     if not oracle.reference_available():
         sys.exit("oracle/_ref/libresiduum_ref.so is missing: run make -C oracle (needs the reference tree)")
-    main()
+    for name in sys.argv[1:] or list(GROUPS):
+        GROUPS[name]()
