@@ -73,6 +73,51 @@ class MT19937_64:
         return a + int(self.uniform() * (b - a + 1))
 
 
+_MT_U, _MT_L, _MT_A = np.uint64(0xFFFFFFFF80000000), np.uint64(0x7FFFFFFF), np.uint64(0xB5026F5AA96619E9)
+
+
+def mt19937_64_stream(seed, count):
+    """The first `count` outputs of std::mt19937_64(seed), the twist and tempering vectorized with
+    numpy (the twist splits into the three index ranges whose inputs are already final)."""
+    mt = np.array(MT19937_64(seed).mt, dtype=np.uint64)
+    out = np.empty(count, np.uint64)
+    done = 0
+    one = np.uint64(1)
+    with np.errstate(over="ignore"):
+        while done < count:
+            for lo, hi, src in ((0, 156, 156), (156, 311, -156)):
+                i = np.arange(lo, hi)
+                x = (mt[i] & _MT_U) | (mt[i + 1] & _MT_L)
+                mt[i] = mt[i + src] ^ (x >> one) ^ np.where((x & one) == one, _MT_A, np.uint64(0))
+            x = (mt[311] & _MT_U) | (mt[0] & _MT_L)
+            mt[311] = mt[155] ^ (x >> one) ^ (_MT_A if int(x) & 1 else np.uint64(0))
+            y = mt.copy()
+            y ^= (y >> np.uint64(29)) & np.uint64(0x5555555555555555)
+            y ^= (y << np.uint64(17)) & np.uint64(0x71D67FFFEDA60000)
+            y ^= (y << np.uint64(37)) & np.uint64(0xFFF7EEE000000000)
+            y ^= y >> np.uint64(43)
+            k = min(312, count - done)
+            out[done:done + k] = y[:k]
+            done += k
+    return out
+
+
+def uniforms(bits):
+    """uniform doubles in [0, 1): (x >> 11) * 2^-53"""
+    return (bits >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def batch_problem(p):
+    """Problem p of the batched workload: stream mt19937_64(4000 + p); Nx, Ny ~ U{32..256}; then per
+    element, in element order, z_e ~ N(0, 1) by Box-Muller (cos branch) from two uniforms u1, u2 as
+    sqrt(-2 ln(1 - u1)) cos(2 pi u2); k_e = exp(z_e)."""
+    head = uniforms(mt19937_64_stream(4000 + p, 2))
+    nx, ny = (32 + int(u * 225) for u in head)
+    u = uniforms(mt19937_64_stream(4000 + p, 2 + 2 * nx * ny)[2:]).reshape(-1, 2)
+    z = np.sqrt(-2.0 * np.log1p(-u[:, 0])) * np.cos(2.0 * np.pi * u[:, 1])
+    return nx, ny, np.exp(z)
+
+
 def sine_modes(seed=2, modes=8):
     """T0(x) = sum_m 0.1 sin(a_m . x + b_m), a_m = pi * i_m with i_m ~ U{1..8}^3, b_m ~ U[0, 2pi);
     per mode the three integers are drawn before the phase."""
@@ -209,6 +254,63 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line))
 
 
+def run_batch(rsd, ctx, stream, count, reps, peak):
+    """The batched workload: `count` unit-square Q1 problems (Nx, Ny ~ U{32..256}, log-normal
+    per-element conductivity, unit source, T = 0 on the boundary) solved together by
+    rsd_batch_solve, CG + Jacobi to 1e-8 (mixed: FP64-checked), x0 = 0."""
+    import torch
+    from importlib import import_module
+    bm = import_module("residuum_solver_b200.blockmesh")
+    t0 = time.time()
+    probs = []
+    for p in range(count):
+        nx, ny, ke = batch_problem(p)
+        xyz, ien, rg = bm.block_mesh(2, [nx, ny], [0, 0], [1, 1], 1)
+        h = rsd.Heat(ctx, rsd.Mesh(ctx, 2, 1, xyz, ien, rg), 2, k_elem=ke, src_expr="1",
+                     dirichlet={t: "0" for t in range(4)})
+        h.assemble_matrix(1.0)
+        F = ctx.array(h.n)
+        h.assemble_vector(0, F)
+        probs.append((h, F))
+    setup_s = time.time() - t0
+    B = rsd.Batch(ctx, [h.K for h, _ in probs])
+    xs = [ctx.array(h.n) for h, _ in probs]
+    ns = np.array([h.n for h, _ in probs], dtype=np.float64)
+    nnzs = np.array([h.nnz for h, _ in probs], dtype=np.float64)
+    out = {"problems": count, "rows": int(ns.sum()), "nnz": int(nnzs.sum()), "setup_s": round(setup_s, 2)}
+    for key, prec in (("mixed", rsd.MIXED), ("fp64", rsd.FP64)):
+        cfg = rsd.SolverConfig.make(precision=prec, tol=1e-8, max_iters=100000)
+        ts = []
+        for r in range(reps + 1):
+            for x in xs:
+                x.zero()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rr = B.solve([F for _, F in probs], xs, cfg)
+            e1.record(stream)
+            e1.synchronize()
+            if r:
+                ts.append(e0.elapsed_time(e1))
+        its = np.array([q["iterations"] for q in rr], dtype=np.float64)
+        refs = np.array([q["refinements"] for q in rr], dtype=np.float64)
+        s = 4 if key == "mixed" else 8
+        # PCG+Jacobi per iteration: SpMV nnz(s+4) + 4(n+1) + 2ns, and 11 vector passes of n*s;
+        # each FP64 residual replacement one FP64 SpMV plus 4 n*8
+        byts = float(np.sum(its * (nnzs * (s + 4) + 4 * (ns + 1) + 2 * ns * s + 11 * ns * s)
+                            + refs * (nnzs * 12 + 4 * (ns + 1) + 2 * ns * 8 + 4 * ns * 8)))
+        ms = float(np.median(ts))
+        out[key] = {"ms": ms, "problems_per_s": count / (ms * 1e-3), "all_converged": all(q["converged"] for q in rr),
+                    "iterations_total": int(its.sum()), "iterations_max": int(its.max()),
+                    "refinements_total": int(refs.sum()),
+                    "max_true_residual_rel": max(q["trueResidualRel"] for q in rr),
+                    "algorithmic_gbs": byts / (ms * 1e-3) / 1e9, "frac_of_measured_hbm": byts / (ms * 1e-3) / 1e9 / peak}
+    out["speedup_mixed_vs_fp64"] = out["fp64"]["ms"] / out["mixed"]["ms"]
+    out["how"] = ("one rsd_batch_solve call (one persistent launch), CUDA events around the call, median of "
+                  f"{reps}; setup (meshes, patterns, assembly) outside the timed region")
+    del B
+    return out
+
+
 METRIC = "time to a 1e-8 FP64-checked relative residual per Backward-Euler step, mixed FP32/FP64 CG+Jacobi (FP64 CG alongside)"
 WORKLOAD = ("3D transient heat, unit cube, {S}^3 Q1 hexes, k = rho*cp = 1, Backward Euler dt = 1e-3, "
             "T0 = 8 seeded sine modes (amplitude 0.1, seed 2), Dirichlet T = 0 on all faces")
@@ -224,6 +326,7 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=48)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--reliable-delta", type=float, default=0.0)
+    ap.add_argument("--batch", type=int, default=256, help="problems in the batched workload (0: skip it)")
     ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
                     help="run one solver path only (no e2e, no CPU leg): for profiler captures")
     args = ap.parse_args()
@@ -341,6 +444,10 @@ def main():
         solve_it[key] = r["iterations"]
         solve_tr[key] = r["trueResidualRel"]
 
+    batch = None
+    if args.batch > 0:
+        batch = run_batch(rsd, ctx, stream, args.batch, 3, measured_peak_hbm()[0])
+
     # end to end through the public API with host buffers: H2D of the step's state from pinned
     # host memory, the step, D2H of the new state, every step
     hU = torch.from_numpy(U0.copy()).pin_memory()
@@ -432,6 +539,7 @@ def main():
         "kernel_ms_per_step": {k: v[1] / args.steps for k, v in prof_mx.items()},
         "kernel_ms_per_step_fp64": {k: v[1] / args.steps for k, v in prof_64.items()},
         "clocks_fp64": clk64,
+        "batch": batch,
         "cpu_baseline": cpu,
         "e2e": {"value": ms_e2e, "unit": "ms", "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 8 * n},
         "gpu_launches": gpu_launches,

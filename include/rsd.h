@@ -208,6 +208,20 @@ int rsd_heat_be_step(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver_cfg*
 int rsd_heat_newton(rsd_ctx* ctx, rsd_heat* h, double abs_tol, double rel_tol, int64_t max_iters,
                     const rsd_solver_cfg* linear, double* U, rsd_report* report);
 
+/* ---- batched solves (no counterpart in the reference, whose solvers take one system): many
+ *      independent systems A_i x_i = b_i of any sizes in one persistent launch.  Each CTA takes the
+ *      next problem from a device queue (largest first) and runs the whole CG+Jacobi for it.
+ *      cfg->type must be RSD_CG; RSD_MIXED gives FP32 inner iterations with FP64 residual
+ *      replacement (convergence on the FP64 residual), RSD_FP64 plain FP64 PCG.  The batch keeps
+ *      the matrices by reference: they must outlive it and keep their patterns. ---- */
+typedef struct rsd_batch rsd_batch;
+int rsd_batch_create(rsd_ctx* ctx, int32_t count, rsd_csr* const* A, rsd_batch** out);
+int rsd_batch_destroy(rsd_batch* batch);
+/* b, x: host arrays of count device pointers (x holds the initial guesses on entry);
+ * reports: host array of count reports, or NULL */
+int rsd_batch_solve(rsd_ctx* ctx, rsd_batch* batch, const rsd_solver_cfg* cfg, const double* const* b,
+                    double* const* x, rsd_report* reports);
+
 /* ---- adjoint pair, in the shape of an autograd Function (no counterpart in the reference) ----
  * Steady linear heat with per-element conductivity k_e = k_const * exp(theta_e) (rsd_heat_desc's
  * k_expr must be unset).  theta: device, one value per element; T, dJdT: device, free DOFs;

@@ -113,6 +113,9 @@ SIGNATURES = {
     "rsd_heat_steady": [_P, _P, C.POINTER(SolverConfig), _P, C.POINTER(Report)],
     "rsd_heat_be_step": [_P, _P, _D, C.POINTER(SolverConfig), _P, _P, C.POINTER(Report), C.POINTER(_D)],
     "rsd_heat_newton": [_P, _P, _D, _D, _I64, C.POINTER(SolverConfig), _P, C.POINTER(Report)],
+    "rsd_batch_create": [_P, _I32, _P, C.POINTER(_P)],
+    "rsd_batch_destroy": [_P],
+    "rsd_batch_solve": [_P, _P, C.POINTER(SolverConfig), _P, _P, _P],
     "rsd_heat_forward": [_P, _P, _P, C.POINTER(SolverConfig), _P, C.POINTER(Report)],
     "rsd_heat_backward": [_P, _P, _P, _P, _P, C.POINTER(SolverConfig), _P, C.POINTER(Report)],
 }
@@ -309,6 +312,34 @@ def solve(ctx, A, b, x, cfg=None, **kw):
     rep = Report()
     check(lib().rsd_solve(ctx.h, A.h, C.byref(cfg), _ptr(b), _ptr(x), C.byref(rep)))
     return rep.as_dict()
+
+
+class Batch:
+    """rsd_batch: independent systems solved together in one persistent launch."""
+
+    def __init__(self, ctx, mats):
+        self.ctx, self.mats = ctx, list(mats)
+        hs = (_P * max(len(self.mats), 1))(*[m.h for m in self.mats])
+        h = _P()
+        check(lib().rsd_batch_create(ctx.h, len(self.mats), hs, C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().rsd_batch_destroy(self.h)
+        except Exception:
+            pass
+
+    def solve(self, bs, xs, cfg=None, **kw):
+        """bs, xs: sequences of device vectors; returns one report dict per system."""
+        cfg = cfg or SolverConfig.make(**kw)
+        n = len(self.mats)
+        pb = (_P * max(n, 1))(*[_ptr(b) for b in bs])
+        px = (_P * max(n, 1))(*[_ptr(x) for x in xs])
+        reps = (Report * max(n, 1))()
+        check(lib().rsd_batch_solve(self.ctx.h, self.h, C.byref(cfg), pb, px, reps))
+        return [reps[i].as_dict() for i in range(n)]
 
 
 def solve_static(ctx, A, b, x, cfg=None, **kw):

@@ -1,0 +1,331 @@
+// Batched solves of many independent, uneven systems in one persistent launch (a "CSR of CSRs":
+// the batch indexes its problems, each problem is an rsd_csr in its SELL-32 execution layout).
+//
+// Each CTA takes the next problem from a device-side queue (problems ordered by size, largest
+// first, so the longest solves start first), runs the whole preconditioned CG for it with
+// block-level reductions and __syncthreads between phases, writes the problem's report and takes
+// the next one.  No CTA ever waits for another, so the launch cannot deadlock, and the loop of every
+// solve is bounded by max_iters.
+//
+// Precision: TI = float is the mixed scheme of the single-system solver (FP32 matrix and vectors,
+// FP64 reductions, FP64 residual replacement when the recurrence residual falls by delta or claims
+// convergence, convergence declared on the FP64 residual); TI = double is plain FP64 PCG
+// (cg/Solver.tpp:13-119 per problem).
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <vector>
+
+#include "rsd_kernels.cuh"
+
+struct rsd_batch {
+	int32_t count = 0;
+	std::vector<rsd_csr*> A;
+	std::vector<int32_t> order;        // problems by nnz, descending
+	void* desc = nullptr;              // device BatchProb[count]
+	void* out = nullptr;               // device BatchOut[count]
+	int32_t* dorder = nullptr;         // device order[count]
+	int32_t* next = nullptr;           // device queue head
+	void* ws = nullptr;                // device workspace, 5 vectors per problem
+	size_t wsBytes = 0;
+};
+
+namespace rsd {
+namespace {
+
+constexpr int kBT = 1024;              // threads per CTA: 32 warps keep enough gathers in flight
+constexpr int kBW = kBT / 32;
+
+template <typename TI>
+struct BatchProb {
+	int64_t n, nslices;
+	MatView<TI> A;                     // execution layout, inner precision
+	MatView<double> A64;               // FP64 values (residuals)
+	const int32_t* sDiag;
+	const double* b;
+	double* x;
+	TI *r, *p, *Ap, *y, *invD;
+};
+
+struct BatchOut {
+	int64_t iterations, refinements;
+	double res0, res, trueRel;
+	int32_t converged, status;
+};
+
+// block-wide sums of NCH doubles; every thread receives the totals (fixed order: deterministic)
+template <int NCH>
+__device__ __forceinline__ void bsum(double (&v)[NCH], double (*sm)[kBW]) {
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+	for (int c = 0; c < NCH; ++c) v[c] = group_sum<32>(v[c]);
+	if (lane == 0)
+#pragma unroll
+		for (int c = 0; c < NCH; ++c) sm[c][warp] = v[c];
+	__syncthreads();
+#pragma unroll
+	for (int c = 0; c < NCH; ++c) {
+		double t = 0.0;
+		for (int w = 0; w < kBW; ++w) t += sm[c][w];
+		v[c] = t;
+	}
+	__syncthreads();
+}
+
+// rows of one problem, one SELL slice per warp at a time; f(row, rowSum) for the rows < n
+template <int L, typename T, typename XF, typename F>
+__device__ __forceinline__ void slice_rows(const MatView<T>& A, int64_t n, int64_t nslices, const L2Pol& pol, XF xf, F f) {
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	for (int64_t sl = warp; sl < nslices; sl += kBW) {
+		const int64_t row = sl * 32 + lane;
+		const double s = (double)row_sum<L, T, T>(A, row, n, 0, pol, xf);
+		if (row < n) f(row, s);
+	}
+}
+
+template <typename TI, int L>
+__device__ void solve_one(const BatchProb<TI>& P, BatchOut* out, double tol, int relMode, int64_t maxIt, double delta,
+                          double (*sm)[kBW]) {
+	constexpr bool kMixed = sizeof(TI) == 4;
+	const int64_t n = P.n;
+	const L2Pol pol = make_l2pol();
+	TI* __restrict__ r = P.r;
+	TI* __restrict__ p = P.p;
+	TI* __restrict__ Ap = P.Ap;
+	TI* __restrict__ y = P.y;
+	TI* __restrict__ invD = P.invD;
+	double* __restrict__ x = P.x;
+	const int tid = threadIdx.x;
+	// Jacobi::update (Jacobi.hpp:31-34); z = M r through zr()
+	for (int64_t i = tid; i < n; i += kBT) {
+		if (invD) {
+			const int32_t q = P.sDiag[i];
+			const double d = q >= 0 ? P.A64.val[q] : 0.0;
+			invD[i] = (TI)(fabs(d) > 1e-300 ? 1.0 / d : 1.0);
+		}
+		y[i] = (TI)0;
+	}
+	__syncthreads();
+	auto zr = [&](int64_t i, TI ri) -> TI { return invD ? ri * invD[i] : ri; };
+	// r = b - A64 x; z = M r; p = z
+	auto residual64 = [&](double (&v)[2]) {
+		v[0] = v[1] = 0.0;
+		slice_rows<L, double>(P.A64, n, P.nslices, pol, [&](int c) { return x[c] + (double)y[c]; }, [&](int64_t i, double ax) {
+			const double r64 = P.b[i] - ax;
+			const TI ri = (TI)r64;
+			const TI zi = zr(i, ri);
+			r[i] = ri;
+			v[0] += r64 * r64;
+			v[1] += (double)ri * (double)zi;
+		});
+	};
+	double v[2];
+	residual64(v);
+	bsum<2>(v, sm);
+	for (int64_t i = tid; i < n; i += kBT) p[i] = zr(i, r[i]);
+	__syncthreads();
+	const double res0 = sqrt(v[0]);
+	double rz = v[1], res = res0, rmax = res0, trueRel = 1.0;
+	int64_t it = 0, refinements = 0;
+	int32_t converged = 0, status = 0;
+	auto crit = [&](double rr) { return relMode ? rr / (res0 + 1e-50) : rr; };
+	if (crit(res0) < tol || n == 0) converged = 1;
+	while (!converged && !status && it < maxIt - 1) {
+		// Ap = A p, alpha = r.z / p.Ap
+		double w[1] = {0.0};
+		slice_rows<L, TI>(P.A, n, P.nslices, pol, [&](int c) { return (TI)p[c]; }, [&](int64_t i, double s) {
+			Ap[i] = (TI)s;
+			w[0] += (double)p[i] * (double)(TI)s;
+		});
+		bsum<1>(w, sm);
+		const double alpha = rz / w[0];
+		if (!isfinite(alpha)) { status = RSD_EBREAKDOWN; break; }
+		const TI a = (TI)alpha;
+		double u[2] = {0.0, 0.0};
+		for (int64_t i = tid; i < n; i += kBT) {
+			if (kMixed) y[i] = y[i] + a * p[i];
+			else x[i] = x[i] + alpha * (double)p[i];    // FP64: x += alpha p as cg/Solver.tpp:74-76
+			const TI ri = r[i] - a * Ap[i];
+			r[i] = ri;
+			const TI zi = zr(i, ri);
+			u[0] += (double)ri * (double)ri;
+			u[1] += (double)ri * (double)zi;
+		}
+		bsum<2>(u, sm);
+		++it;
+		res = sqrt(u[0]);
+		if (!isfinite(res)) { status = RSD_ENAN; break; }
+		double rzNew = u[1];
+		const bool replace = kMixed && (crit(res) < tol || res < delta * rmax || it + 1 >= maxIt);
+		if (replace) {
+			// FP64 residual replacement: r = b - A64 (x + y), then fold y into x
+			residual64(v);
+			bsum<2>(v, sm);
+			for (int64_t i = tid; i < n; i += kBT) { x[i] += (double)y[i]; y[i] = (TI)0; }
+			res = sqrt(v[0]);
+			rmax = res;
+			trueRel = res / (res0 + 1e-50);
+			rzNew = v[1];
+			++refinements;
+			if (crit(res) < tol) { converged = 1; break; }
+		} else if (!kMixed && crit(res) < tol) {
+			converged = 1;
+			break;
+		}
+		const TI beta = (TI)(rzNew / rz);
+		rz = rzNew;
+		__syncthreads();
+		for (int64_t i = tid; i < n; i += kBT) p[i] = p[i] * beta + zr(i, r[i]);
+		__syncthreads();
+	}
+	if (kMixed && !converged) {
+		// stopped early: fold the remaining FP32 correction into the FP64 iterate
+		__syncthreads();
+		for (int64_t i = tid; i < n; i += kBT) { x[i] += (double)y[i]; y[i] = (TI)0; }
+	}
+	if (!kMixed) trueRel = res / (res0 + 1e-50);
+	if (tid == 0) {
+		out->iterations = converged ? it : (status ? it : maxIt);
+		out->refinements = refinements;
+		out->res0 = res0;
+		out->res = res;
+		out->trueRel = trueRel;
+		out->converged = converged;
+		out->status = status;
+	}
+	__syncthreads();
+}
+
+template <typename TI>
+__global__ void __launch_bounds__(kBT) k_batch_cg(const BatchProb<TI>* probs, const int32_t* order, int32_t count,
+                                                  int32_t* next, BatchOut* outs, double tol, int relMode,
+                                                  int64_t maxIt, double delta) {
+	__shared__ double sm[2][kBW];
+	__shared__ int32_t job;
+	for (;;) {
+		if (threadIdx.x == 0) job = atomicAdd(next, 1);
+		__syncthreads();
+		const int32_t j = job;
+		__syncthreads();
+		if (j >= count) return;
+		const int32_t pi = order[j];
+		const BatchProb<TI> P = probs[pi];
+		if (P.A.col16) solve_one<TI, -1>(P, outs + pi, tol, relMode, maxIt, delta, sm);
+		else solve_one<TI, 0>(P, outs + pi, tol, relMode, maxIt, delta, sm);
+	}
+}
+
+int64_t pad_len(int64_t n) { return (n + 63) & ~int64_t(63); }
+
+}  // namespace
+}  // namespace rsd
+
+using namespace rsd;
+
+extern "C" {
+
+int rsd_batch_create(rsd_ctx* ctx, int32_t count, rsd_csr* const* A, rsd_batch** out) {
+	if (!ctx || !out || count < 0 || (count && !A)) return set_error(RSD_EINVAL, "null argument");
+	for (int32_t i = 0; i < count; ++i)
+		if (!A[i]) return set_error(RSD_EINVAL, "null matrix in the batch");
+	RSD_CUDA(cudaSetDevice(ctx->device));
+	rsd_batch* B = new rsd_batch();
+	B->count = count;
+	B->A.assign(A, A + count);
+	B->order.resize(count);
+	std::iota(B->order.begin(), B->order.end(), 0);
+	std::stable_sort(B->order.begin(), B->order.end(), [&](int32_t a, int32_t b) { return A[a]->nnz > A[b]->nnz; });
+	size_t floats = 0;
+	for (int32_t i = 0; i < count; ++i) floats += 5 * (size_t)pad_len(A[i]->n);
+	B->wsBytes = std::max<size_t>(floats * sizeof(double), 256);   // room for FP64 inner vectors too
+	const size_t descBytes = std::max<size_t>(sizeof(BatchProb<double>) * count, 64);
+	cudaError_t e;
+	if ((e = cudaMalloc(&B->ws, B->wsBytes)) != cudaSuccess || (e = cudaMalloc(&B->desc, descBytes)) != cudaSuccess ||
+	    (e = cudaMalloc(&B->out, sizeof(BatchOut) * std::max(count, 1))) != cudaSuccess ||
+	    (e = cudaMalloc(&B->dorder, sizeof(int32_t) * std::max(count, 1))) != cudaSuccess ||
+	    (e = cudaMalloc(&B->next, sizeof(int32_t))) != cudaSuccess) {
+		cudaFree(B->ws); cudaFree(B->desc); cudaFree(B->out); cudaFree(B->dorder); cudaFree(B->next);
+		delete B;
+		return cuda_error(e, "cudaMalloc (batch)");
+	}
+	if (count) RSD_CUDA(cudaMemcpy(B->dorder, B->order.data(), sizeof(int32_t) * count, cudaMemcpyHostToDevice));
+	*out = B;
+	return RSD_OK;
+}
+
+int rsd_batch_destroy(rsd_batch* B) {
+	if (!B) return RSD_OK;
+	cudaFree(B->ws); cudaFree(B->desc); cudaFree(B->out); cudaFree(B->dorder); cudaFree(B->next);
+	delete B;
+	return RSD_OK;
+}
+
+int rsd_batch_solve(rsd_ctx* ctx, rsd_batch* B, const rsd_solver_cfg* cfg, const double* const* b, double* const* x,
+                    rsd_report* reports) {
+	if (!ctx || !B || !cfg || (B->count && (!b || !x))) return set_error(RSD_EINVAL, "null argument");
+	if (cfg->type != RSD_CG) return set_error(RSD_EINVAL, "the batched solver runs CG");
+	if (cfg->max_iters < 0 || !(cfg->tol >= 0)) return set_error(RSD_EINVAL, "bad solver configuration");
+	const int32_t count = B->count;
+	if (!count) return RSD_OK;
+	RSD_CUDA(cudaSetDevice(ctx->device));
+	const bool mixed = cfg->precision == RSD_MIXED;
+	const bool jacobi = cfg->precond == RSD_JACOBI;
+	const double delta = cfg->reliable_delta > 0 ? cfg->reliable_delta : 1e-3;
+	const int rel = cfg->tol_type == RSD_TOL_RELATIVE;
+	auto fill = [&](auto tag) -> int {
+		using TI = decltype(tag);
+		std::vector<BatchProb<TI>> d(count);
+		TI* w = static_cast<TI*>(B->ws);
+		for (int32_t i = 0; i < count; ++i) {
+			rsd_csr* A = B->A[i];
+			if (!b[i] || !x[i]) return set_error(RSD_EINVAL, "null vector in the batch");
+			A->format = 0;                                      // the persistent kernel reads SELL-32
+			if (mixed) RSD_CHECK(f32_sync(ctx, A)); else RSD_CHECK(sell_sync(ctx, A));
+			BatchProb<TI>& P = d[i];
+			P.n = A->n;
+			P.nslices = A->nslices;
+			P.A = MatView<TI>{A->sStart, A->sCol, mixed ? (const TI*)A->val32 : (const TI*)A->sVal, A->sCol16, A->sBase};
+			P.A64 = MatView<double>{A->sStart, A->sCol, A->sVal, A->sCol16, A->sBase};
+			P.sDiag = A->sDiag;
+			P.b = b[i];
+			P.x = x[i];
+			const int64_t ns = pad_len(A->n);
+			P.r = w; P.p = w + ns; P.Ap = w + 2 * ns; P.y = w + 3 * ns; P.invD = jacobi ? w + 4 * ns : nullptr;
+			w += 5 * ns;
+		}
+		RSD_CUDA(cudaMemcpyAsync(B->desc, d.data(), sizeof(BatchProb<TI>) * count, cudaMemcpyHostToDevice, ctx->stream));
+		return RSD_OK;
+	};
+	RSD_CHECK(mixed ? fill(float()) : fill(double()));
+	RSD_CUDA(cudaMemsetAsync(B->next, 0, sizeof(int32_t), ctx->stream));
+	int occ = 0;
+	const void* kern = mixed ? (const void*)k_batch_cg<float> : (const void*)k_batch_cg<double>;
+	RSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kBT, 0));
+	const int grid = std::max(1, std::min(count, ctx->num_sms * std::max(occ, 1)));
+	if (mixed)
+		k_batch_cg<float><<<grid, kBT, 0, ctx->stream>>>((const BatchProb<float>*)B->desc, B->dorder, count, B->next,
+		                                                (BatchOut*)B->out, cfg->tol, rel, cfg->max_iters, delta);
+	else
+		k_batch_cg<double><<<grid, kBT, 0, ctx->stream>>>((const BatchProb<double>*)B->desc, B->dorder, count, B->next,
+		                                                 (BatchOut*)B->out, cfg->tol, rel, cfg->max_iters, delta);
+	RSD_CUDA(cudaGetLastError());
+	std::vector<BatchOut> h(count);
+	RSD_CUDA(cudaMemcpyAsync(h.data(), B->out, sizeof(BatchOut) * count, cudaMemcpyDeviceToHost, ctx->stream));
+	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+	if (reports)
+		for (int32_t i = 0; i < count; ++i) {
+			rsd_report& R = reports[i];
+			R = rsd_report{};
+			R.converged = h[i].converged;
+			R.status = h[i].status;
+			R.iterations = h[i].iterations;
+			R.initialResidual = h[i].res0;
+			R.finalResidual = mixed ? h[i].trueRel * h[i].res0 : h[i].res;
+			R.finalResidualRel = mixed ? h[i].trueRel : h[i].res / (h[i].res0 + 1e-50);
+			R.trueResidualRel = h[i].trueRel;
+			R.refinements = h[i].refinements;
+		}
+	return RSD_OK;
+}
+
+}  // extern "C"
