@@ -311,6 +311,127 @@ def run_batch(rsd, ctx, stream, count, reps, peak):
     return out
 
 
+def run_newton(rsd, ctx, stream, S):
+    """Steady nonlinear heat on S^3 Q2 hexes: k(T) = 1 + 0.5 T, f = 10, T = 0 on x = 0 and 1 on x = 1,
+    zero flux elsewhere; Newton to 1e-10 (absolute or relative) with GMRES(30) + Jacobi inner solves
+    to 1e-12, x0 = 0.  Checked against the 1D closed form T = 2(sqrt(1 + u) - 1), u = 6.25 x - 5 x^2."""
+    import torch
+    from importlib import import_module
+    bm = import_module("residuum_solver_b200.blockmesh")
+    t0 = time.time()
+    xyz, ien, rg = bm.block_mesh(3, [S] * 3, [0, 0, 0], [1, 1, 1], 2)
+    h = rsd.Heat(ctx, rsd.Mesh(ctx, 3, 2, xyz, ien, rg), 3, k_expr="1 + 0.5*T", dk_expr="0.5", src_expr="10",
+                 dirichlet={0: "0", 1: "1"})
+    setup_s = time.time() - t0
+    U = ctx.array(h.n)
+    cfg = rsd.SolverConfig.make(type=rsd.GMRES, krylov_dim=30, tol=1e-12, max_iters=100000)
+    U.zero()
+    h.newton(U, 1e-10, 1e-10, 50, cfg)          # warm-up (workspace setup)
+    U.zero()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    rep = h.newton(U, 1e-10, 1e-10, 50, cfg)
+    e1.record(stream)
+    e1.synchronize()
+    t2a, a2t = h.dofmap()
+    x = xyz.reshape(-1, 3)[a2t, 0]
+    exact = 2.0 * (np.sqrt(1.0 + 6.25 * x - 5.0 * x * x) - 1.0)
+    err = float(np.max(np.abs(U.download() - exact)))
+    return {"workload": f"{S}^3 Q2 hexes, k(T) = 1 + 0.5T, f = 10, Newton 1e-10, GMRES(30) + Jacobi 1e-12",
+            "n_free": h.n, "nnz": h.nnz, "setup_s": round(setup_s, 2), "ms": e0.elapsed_time(e1),
+            "newton_iterations": rep["iterations"], "gmres_iterations_total": rep["refinements"],
+            "converged": bool(rep["converged"]), "final_residual": rep["finalResidual"],
+            "max_error_vs_1d_closed_form": err}
+
+
+def fourier_theta(xyz, ien, npe, seed, modes=16, amp=0.5):
+    """theta_e = sum_m amp sin(2 pi k_m . c_e + phi_m) at element centroids c_e; stream mt19937_64(seed),
+    per mode the three integers k_m ~ U{1..4} and then phi_m ~ U[0, 2 pi)."""
+    u = uniforms(mt19937_64_stream(seed, 4 * modes)).reshape(modes, 4)
+    c = xyz.reshape(-1, 3)[ien.reshape(-1, npe)].mean(axis=1)
+    th = np.zeros(len(c))
+    for m in range(modes):
+        k = 1 + np.floor(u[m, :3] * 4.0)
+        th += amp * np.sin(2.0 * np.pi * (c @ k) + 2.0 * np.pi * u[m, 3])
+    return th
+
+
+def run_adjoint(rsd, ctx, stream, S, ndir):
+    """Adjoint gradient on S^3 Q1 hexes: k_e = exp(theta_e) (16 seeded Fourier modes, seed 5), f = 1,
+    T = 0 on the boundary, J = 0.5 ||T(theta) - T_obs||^2 over the free nodes with T_obs from a second
+    theta (seed 55); forward and adjoint CG + Jacobi to 1e-13; central differences (h = 1e-6) along
+    `ndir` directions d ~ N(0, 1) per element (seed 555, Box-Muller), normalised."""
+    import torch
+    from importlib import import_module
+    bm = import_module("residuum_solver_b200.blockmesh")
+    xyz, ien, rg = bm.block_mesh(3, [S] * 3, [0, 0, 0], [1, 1, 1], 1)
+    h = rsd.Heat(ctx, rsd.Mesh(ctx, 3, 1, xyz, ien, rg), 2, src_expr="1", dirichlet={t: "0" for t in range(6)})
+    ne, n = S ** 3, h.n
+    th = fourier_theta(xyz, ien, 8, 5)
+    cfg = rsd.SolverConfig.make(tol=1e-13, max_iters=100000)
+    Tobs = ctx.array(n).zero()
+    h.forward(ctx.to_device(fourier_theta(xyz, ien, 8, 55)), Tobs, cfg)
+    tobs = Tobs.download()
+    theta, T, grad, dJdT = ctx.to_device(th), ctx.array(n), ctx.array(ne), ctx.array(n)
+    times = []
+    for _ in range(3):
+        T.zero()
+        e0, e1, e2, e3 = (torch.cuda.Event(enable_timing=True) for _ in range(4))
+        e0.record(stream)
+        rf = h.forward(theta, T, cfg)
+        e1.record(stream)
+        dJdT.upload(T.download() - tobs)
+        e2.record(stream)
+        rb = h.backward(theta, T, dJdT, grad, cfg)
+        e3.record(stream)
+        e3.synchronize()
+        times.append((e0.elapsed_time(e1), e2.elapsed_time(e3)))
+    g = grad.download()
+    u = uniforms(mt19937_64_stream(555, 2 * ne * ndir)).reshape(ndir, ne, 2)
+    dirs = np.sqrt(-2.0 * np.log1p(-u[..., 0])) * np.cos(2.0 * np.pi * u[..., 1])
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+
+    # each perturbed forward solve starts from T(theta) and reduces the O(h) initial residual by 1e-8
+    # (about 1e-15 of ||F||); the quotient is formed from T+ - T-, not from J+ - J-, so that no
+    # cancellation between two nearly equal sums limits it:
+    #   J(th + h d) - J(th - h d) = 0.5 sum (T+ - T-) (T+ + T- - 2 T_obs)
+    t_base = T.download()
+    fd_cfg = rsd.SolverConfig.make(tol=1e-8, max_iters=20000)
+
+    def Tof(t):
+        Tt = ctx.to_device(t_base)
+        h.forward(ctx.to_device(t), Tt, fd_cfg)
+        return Tt.download()
+
+    errs = []
+    for d in dirs:
+        tp, tm = Tof(th + 1e-6 * d), Tof(th - 1e-6 * d)
+        fd = 0.5 * float(np.sum((tp - tm) * (tp + tm - 2.0 * tobs))) / 2e-6
+        errs.append(abs(fd - g @ d) / abs(fd))
+    # the same directional derivatives without differencing (tangent-linear solve):
+    # K dT = -(dK/dtheta . d) T, with (dK/dtheta . d) T the diffusion operator of the element
+    # multipliers k_e d_e applied to T; dJ . d = (T - T_obs) . dT
+    ke = np.exp(th)
+    v, dT = ctx.array(n), ctx.array(n)
+    terrs = []
+    for d in dirs:
+        h.set_k_elem(ctx.to_device(ke * d))
+        h.assemble_vector(1, v, U=T)
+        h.set_k_elem(ctx.to_device(ke))
+        h.assemble_matrix(1.0)
+        rhs = ctx.to_device(-v.download())
+        dT.zero()
+        rsd.solve(ctx, h.K, rhs, dT, cfg)
+        tl = float((t_base - tobs) @ dT.download())
+        terrs.append(abs(tl - g @ d) / abs(tl))
+    fwd, bwd = (float(np.median([t[i] for t in times])) for i in (0, 1))
+    return {"workload": f"{S}^3 Q1 hexes, k_e = exp(theta_e), J = 0.5||T - T_obs||^2, CG + Jacobi 1e-13",
+            "n_free": n, "elements": ne, "forward_ms": fwd, "backward_ms": bwd,
+            "forward_iterations": rf["iterations"], "adjoint_iterations": rb["iterations"],
+            "fd_directions": ndir, "fd_max_rel_error": max(errs), "fd_median_rel_error": float(np.median(errs)),
+            "tangent_linear_max_rel_error": max(terrs), "tangent_linear_median_rel_error": float(np.median(terrs))}
+
+
 METRIC = "time to a 1e-8 FP64-checked relative residual per Backward-Euler step, mixed FP32/FP64 CG+Jacobi (FP64 CG alongside)"
 WORKLOAD = ("3D transient heat, unit cube, {S}^3 Q1 hexes, k = rho*cp = 1, Backward Euler dt = 1e-3, "
             "T0 = 8 seeded sine modes (amplitude 0.1, seed 2), Dirichlet T = 0 on all faces")
@@ -327,6 +448,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--reliable-delta", type=float, default=0.0)
     ap.add_argument("--batch", type=int, default=256, help="problems in the batched workload (0: skip it)")
+    ap.add_argument("--newton", type=int, default=48, help="Q2 mesh size of the Newton workload (0: skip it)")
+    ap.add_argument("--adjoint", type=int, default=96, help="mesh size of the adjoint workload (0: skip it)")
+    ap.add_argument("--fd-directions", type=int, default=20)
     ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
                     help="run one solver path only (no e2e, no CPU leg): for profiler captures")
     args = ap.parse_args()
@@ -447,6 +571,8 @@ def main():
     batch = None
     if args.batch > 0:
         batch = run_batch(rsd, ctx, stream, args.batch, 3, measured_peak_hbm()[0])
+    newton = run_newton(rsd, ctx, stream, args.newton) if args.newton > 0 else None
+    adjoint = run_adjoint(rsd, ctx, stream, args.adjoint, args.fd_directions) if args.adjoint > 0 else None
 
     # end to end through the public API with host buffers: H2D of the step's state from pinned
     # host memory, the step, D2H of the new state, every step
@@ -540,6 +666,8 @@ def main():
         "kernel_ms_per_step_fp64": {k: v[1] / args.steps for k, v in prof_64.items()},
         "clocks_fp64": clk64,
         "batch": batch,
+        "newton": newton,
+        "adjoint": adjoint,
         "cpu_baseline": cpu,
         "e2e": {"value": ms_e2e, "unit": "ms", "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 8 * n},
         "gpu_launches": gpu_launches,

@@ -85,7 +85,7 @@ __device__ __forceinline__ void slice_rows(const MatView<T>& A, int64_t n, int64
 
 template <typename TI, int L>
 __device__ void solve_one(const BatchProb<TI>& P, BatchOut* out, double tol, int relMode, int64_t maxIt, double delta,
-                          double (*sm)[kBW]) {
+                          int adaptive, double (*sm)[kBW]) {
 	constexpr bool kMixed = sizeof(TI) == 4;
 	const int64_t n = P.n;
 	const L2Pol pol = make_l2pol();
@@ -162,7 +162,9 @@ __device__ void solve_one(const BatchProb<TI>& P, BatchOut* out, double tol, int
 			residual64(v);
 			bsum<2>(v, sm);
 			for (int64_t i = tid; i < n; i += kBT) { x[i] += (double)y[i]; y[i] = (TI)0; }
+			const double recurrence = res;
 			res = sqrt(v[0]);
+			if (adaptive) delta = next_delta(delta, recurrence, res);
 			rmax = res;
 			trueRel = res / (res0 + 1e-50);
 			rzNew = v[1];
@@ -199,7 +201,7 @@ __device__ void solve_one(const BatchProb<TI>& P, BatchOut* out, double tol, int
 template <typename TI>
 __global__ void __launch_bounds__(kBT) k_batch_cg(const BatchProb<TI>* probs, const int32_t* order, int32_t count,
                                                   int32_t* next, BatchOut* outs, double tol, int relMode,
-                                                  int64_t maxIt, double delta) {
+                                                  int64_t maxIt, double delta, int adaptive) {
 	__shared__ double sm[2][kBW];
 	__shared__ int32_t job;
 	for (;;) {
@@ -210,8 +212,8 @@ __global__ void __launch_bounds__(kBT) k_batch_cg(const BatchProb<TI>* probs, co
 		if (j >= count) return;
 		const int32_t pi = order[j];
 		const BatchProb<TI> P = probs[pi];
-		if (P.A.col16) solve_one<TI, -1>(P, outs + pi, tol, relMode, maxIt, delta, sm);
-		else solve_one<TI, 0>(P, outs + pi, tol, relMode, maxIt, delta, sm);
+		if (P.A.col16) solve_one<TI, -1>(P, outs + pi, tol, relMode, maxIt, delta, adaptive, sm);
+		else solve_one<TI, 0>(P, outs + pi, tol, relMode, maxIt, delta, adaptive, sm);
 	}
 }
 
@@ -270,7 +272,8 @@ int rsd_batch_solve(rsd_ctx* ctx, rsd_batch* B, const rsd_solver_cfg* cfg, const
 	RSD_CUDA(cudaSetDevice(ctx->device));
 	const bool mixed = cfg->precision == RSD_MIXED;
 	const bool jacobi = cfg->precond == RSD_JACOBI;
-	const double delta = cfg->reliable_delta > 0 ? cfg->reliable_delta : 1e-3;
+	const int adaptive = !(cfg->reliable_delta > 0);
+	const double delta = adaptive ? 0.1 : cfg->reliable_delta;
 	const int rel = cfg->tol_type == RSD_TOL_RELATIVE;
 	auto fill = [&](auto tag) -> int {
 		using TI = decltype(tag);
@@ -284,8 +287,8 @@ int rsd_batch_solve(rsd_ctx* ctx, rsd_batch* B, const rsd_solver_cfg* cfg, const
 			BatchProb<TI>& P = d[i];
 			P.n = A->n;
 			P.nslices = A->nslices;
-			P.A = MatView<TI>{A->sStart, A->sCol, mixed ? (const TI*)A->val32 : (const TI*)A->sVal, A->sCol16, A->sBase};
-			P.A64 = MatView<double>{A->sStart, A->sCol, A->sVal, A->sCol16, A->sBase};
+			P.A = MatView<TI>{A->sStart, A->sCol, mixed ? (const TI*)A->val32 : (const TI*)A->sVal, A->sCol16, A->sBase, A->sUni, A->sOffs};
+			P.A64 = MatView<double>{A->sStart, A->sCol, A->sVal, A->sCol16, A->sBase, A->sUni, A->sOffs};
 			P.sDiag = A->sDiag;
 			P.b = b[i];
 			P.x = x[i];
@@ -304,10 +307,10 @@ int rsd_batch_solve(rsd_ctx* ctx, rsd_batch* B, const rsd_solver_cfg* cfg, const
 	const int grid = std::max(1, std::min(count, ctx->num_sms * std::max(occ, 1)));
 	if (mixed)
 		k_batch_cg<float><<<grid, kBT, 0, ctx->stream>>>((const BatchProb<float>*)B->desc, B->dorder, count, B->next,
-		                                                (BatchOut*)B->out, cfg->tol, rel, cfg->max_iters, delta);
+		                                                (BatchOut*)B->out, cfg->tol, rel, cfg->max_iters, delta, adaptive);
 	else
 		k_batch_cg<double><<<grid, kBT, 0, ctx->stream>>>((const BatchProb<double>*)B->desc, B->dorder, count, B->next,
-		                                                 (BatchOut*)B->out, cfg->tol, rel, cfg->max_iters, delta);
+		                                                 (BatchOut*)B->out, cfg->tol, rel, cfg->max_iters, delta, adaptive);
 	RSD_CUDA(cudaGetLastError());
 	std::vector<BatchOut> h(count);
 	RSD_CUDA(cudaMemcpyAsync(h.data(), B->out, sizeof(BatchOut) * count, cudaMemcpyDeviceToHost, ctx->stream));

@@ -236,7 +236,7 @@ int resident_blocks(const void* kernel, int block) {
 
 static void free_csr_arrays(rsd_csr* A) {
 	cudaFree(A->rowPtr); cudaFree(A->col); cudaFree(A->val); cudaFree(A->diag);
-	cudaFree(A->sStart); cudaFree(A->sCol); cudaFree(A->sVal); cudaFree(A->val32); cudaFree(A->sSrc); cudaFree(A->sDiag); cudaFree(A->sCol16); cudaFree(A->sBase);
+	cudaFree(A->sStart); cudaFree(A->sCol); cudaFree(A->sVal); cudaFree(A->val32); cudaFree(A->sSrc); cudaFree(A->sDiag); cudaFree(A->sCol16); cudaFree(A->sBase); cudaFree(A->sUni); cudaFree(A->sOffs);
 }
 
 static int upload_csr(rsd_ctx* ctx, int64_t n, const std::vector<int32_t>& rp, const std::vector<int32_t>& col,
@@ -283,6 +283,38 @@ static int upload_csr(rsd_ctx* ctx, int64_t n, const std::vector<int32_t>& rp, c
 			sMax[s] = len ? hi : 0;
 		}
 	});
+	// stencil slices: a full slice whose 32 rows have the same length and the same column offsets
+	// (column - row) stores that pattern once, in a table of distinct patterns
+	std::vector<int32_t> sUni(std::max<int64_t>(ns, 1), -1), offTable;
+	{
+		std::vector<std::vector<int32_t>> pat(ns);
+		parallel_for(ns, [&](int64_t b, int64_t e) {
+			for (int64_t s = b; s < e; ++s) {
+				const int64_t r0 = 32 * s, len = (start[s + 1] - start[s]) / 32;
+				if (r0 + 32 > n || len == 0) continue;
+				bool uni = true;
+				for (int64_t l = 0; l < 32 && uni; ++l) uni = rp[r0 + l + 1] - rp[r0 + l] == len;
+				for (int64_t j = 0; j < len && uni; ++j) {
+					const int32_t off = col[rp[r0] + j] - (int32_t)r0;
+					for (int64_t l = 1; l < 32 && uni; ++l) uni = col[rp[r0 + l] + j] - (int32_t)(r0 + l) == off;
+				}
+				if (!uni) continue;
+				pat[s].resize(len);
+				for (int64_t j = 0; j < len; ++j) pat[s][j] = col[rp[r0] + j] - (int32_t)r0;
+			}
+		});
+		std::map<std::vector<int32_t>, int32_t> seen;
+		for (int64_t s = 0; s < ns; ++s) {
+			if (pat[s].empty()) continue;
+			auto it = seen.find(pat[s]);
+			if (it == seen.end()) {
+				it = seen.emplace(pat[s], (int32_t)offTable.size()).first;
+				offTable.insert(offTable.end(), pat[s].begin(), pat[s].end());
+			}
+			sUni[s] = it->second;
+		}
+	}
+	const bool stencil = !offTable.empty();
 	// 16-bit columns: every slice's columns within 65,535 of the slice's smallest one
 	bool narrow = ssize > 0;
 	for (int64_t s = 0; s < ns && narrow; ++s) narrow = (int64_t)sMax[s] - sMin[s] <= 65535;
@@ -315,6 +347,12 @@ static int upload_csr(rsd_ctx* ctx, int64_t n, const std::vector<int32_t>& rp, c
 	if ((e = cudaMemcpyAsync(A->sCol, sCol.data(), sizeof(int32_t) * S, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload sCol");
 	if ((e = cudaMemcpyAsync(A->sSrc, sSrc.data(), sizeof(int32_t) * S, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload sSrc");
 	if ((e = cudaMemcpyAsync(A->sDiag, sDiag.data(), sizeof(int32_t) * std::max<int64_t>(n, 1), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload sDiag");
+	if (stencil) {
+		if ((e = cudaMalloc(&A->sUni, sizeof(int32_t) * ns)) != cudaSuccess) return fail(e, "cudaMalloc sUni");
+		if ((e = cudaMalloc(&A->sOffs, sizeof(int32_t) * offTable.size())) != cudaSuccess) return fail(e, "cudaMalloc sOffs");
+		if ((e = cudaMemcpyAsync(A->sUni, sUni.data(), sizeof(int32_t) * ns, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload sUni");
+		if ((e = cudaMemcpyAsync(A->sOffs, offTable.data(), sizeof(int32_t) * offTable.size(), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload sOffs");
+	}
 	if (narrow) {
 		if ((e = cudaMalloc(&A->sCol16, sizeof(uint16_t) * ssize)) != cudaSuccess) return fail(e, "cudaMalloc sCol16");
 		if ((e = cudaMalloc(&A->sBase, sizeof(int32_t) * ns)) != cudaSuccess) return fail(e, "cudaMalloc sBase");

@@ -106,6 +106,10 @@ struct rsd_csr {
 	// lie within 65,535 of its smallest (then the SELL kernels read 2 instead of 4 bytes per slot)
 	uint16_t* sCol16 = nullptr;    // ssize
 	int32_t* sBase = nullptr;      // nslices
+	// stencil slices: sUni[s] >= 0 when the 32 rows of slice s share one pattern of column offsets,
+	// sOffs[sUni[s] + j] = column - row of entry j; the slice's columns are then not read
+	int32_t* sUni = nullptr;       // nslices (or null when no slice qualifies)
+	int32_t* sOffs = nullptr;      // distinct patterns, concatenated
 	bool csrValid = true, sellValid = false;
 	int format = 0;                // SpMV layout: 0 SELL-32 (narrow columns when present), 1 CSR vector with `lanes` lanes per row
 	int lanes = 0;                 // CSR SpMV lanes per row (0: default from nnz/row)

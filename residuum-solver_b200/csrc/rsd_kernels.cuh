@@ -180,6 +180,8 @@ struct MatView {
 	const T* __restrict__ val;
 	const uint16_t* __restrict__ col16 = nullptr;   // SELL-32 narrow columns (L == -1)
 	const int32_t* __restrict__ base = nullptr;
+	const int32_t* __restrict__ uni = nullptr;      // SELL-32 stencil slices (L <= 0), or null
+	const int32_t* __restrict__ offs = nullptr;
 };
 
 // sum over one row of val * xf(column).  L == 0: SELL-32, one thread per row (entries 32 slots
@@ -192,33 +194,42 @@ __device__ __forceinline__ AccT row_sum(const MatView<T>& A, int64_t row, int64_
 	AccT s = AccT(0);
 	if (row < n) {
 		if constexpr (L <= 0) {
-			// the slice's length is the same for the whole warp; loads are issued four slots at a
-			// time (values, columns, then the gathers) and summed in row order
+			// the slice's length is the same for the whole warp
 			const int64_t sl = row >> 5;
 			const int s0 = A.ptr[sl];
 			const int len = (A.ptr[sl + 1] - s0) >> 5;
 			const int q0 = s0 + (int)(row & 31);
 			const T* __restrict__ vp = A.val + q0;
-			int cb = 0;
-			const int32_t* __restrict__ cp32 = nullptr;
-			const uint16_t* __restrict__ cp16 = nullptr;
-			if constexpr (L < 0) { cb = A.base[sl]; cp16 = A.col16 + q0; } else { cp32 = A.col + q0; }
-			auto colat = [&](int j) -> int {
-				if constexpr (L < 0) return cb + (int)ldh(cp16 + 32 * j, pol.first);
-				else return ldh(cp32 + 32 * j, pol.first);
+			// loads four slots at a time: values, columns, then the gathers; summed in row order
+			auto run = [&](auto colat) {
+				int j = 0;
+				for (; j + 4 <= len; j += 4) {
+					const T v0 = ldh(vp + 32 * j, pol.first), v1 = ldh(vp + 32 * (j + 1), pol.first);
+					const T v2 = ldh(vp + 32 * (j + 2), pol.first), v3 = ldh(vp + 32 * (j + 3), pol.first);
+					const int c0 = colat(j), c1 = colat(j + 1), c2 = colat(j + 2), c3 = colat(j + 3);
+					const AccT x0 = xf(c0), x1 = xf(c1), x2 = xf(c2), x3 = xf(c3);
+					s += (AccT)v0 * x0;
+					s += (AccT)v1 * x1;
+					s += (AccT)v2 * x2;
+					s += (AccT)v3 * x3;
+				}
+				for (; j < len; ++j) s += (AccT)ldh(vp + 32 * j, pol.first) * xf(colat(j));
 			};
-			int j = 0;
-			for (; j + 4 <= len; j += 4) {
-				const T v0 = ldh(vp + 32 * j, pol.first), v1 = ldh(vp + 32 * (j + 1), pol.first);
-				const T v2 = ldh(vp + 32 * (j + 2), pol.first), v3 = ldh(vp + 32 * (j + 3), pol.first);
-				const int c0 = colat(j), c1 = colat(j + 1), c2 = colat(j + 2), c3 = colat(j + 3);
-				const AccT x0 = xf(c0), x1 = xf(c1), x2 = xf(c2), x3 = xf(c3);
-				s += (AccT)v0 * x0;
-				s += (AccT)v1 * x1;
-				s += (AccT)v2 * x2;
-				s += (AccT)v3 * x3;
+			// a stencil slice (the branch is uniform over the warp, which holds the slice): the column
+			// of entry j is row + offset j, read once per warp from the shared pattern
+			const int u = A.uni ? A.uni[sl] : -1;
+			if (u >= 0) {
+				const int32_t* __restrict__ op = A.offs + u;
+				const int r = (int)row;
+				run([&](int j) { return r + ldh(op + j, pol.last); });
+			} else if constexpr (L < 0) {
+				const int cb = A.base[sl];
+				const uint16_t* __restrict__ cp16 = A.col16 + q0;
+				run([&](int j) { return cb + (int)ldh(cp16 + 32 * j, pol.first); });
+			} else {
+				const int32_t* __restrict__ cp32 = A.col + q0;
+				run([&](int j) { return ldh(cp32 + 32 * j, pol.first); });
 			}
-			for (; j < len; ++j) s += (AccT)ldh(vp + 32 * j, pol.first) * xf(colat(j));
 		} else {
 			const int e = A.ptr[row + 1];
 #pragma unroll 4
@@ -249,6 +260,17 @@ struct RowLoop {
 		step = ((int64_t)gridDim.x * blockDim.x) / G;
 	}
 };
+
+// Adaptive replacement threshold of the mixed-precision solvers.  The FP32 recurrence residual drifts
+// from the true one by roughly eps32 * cond(A) * ||A|| ||x|| whatever the current residual is, so its
+// relative error grows in proportion to the reduction since the last replacement.  With d the
+// relative gap seen at this replacement (threshold delta), the threshold that keeps the next gap
+// near 1% is 100 d delta, kept within [1e-3, 0.1]: well-conditioned systems replace rarely,
+// ill-conditioned ones often.
+__host__ __device__ __forceinline__ double next_delta(double delta, double recurrence, double true_res) {
+	const double d = fabs(recurrence - true_res) / fmax(true_res, 1e-300);
+	return fmin(0.1, fmax(1e-3, 100.0 * d * delta));
+}
 
 // expression stack machine (bytecode from compile_expr)
 __device__ __forceinline__ double eval_expr(const DevExpr& e, double t, double x, double y, double z, double T) {
@@ -283,12 +305,17 @@ __device__ __forceinline__ double eval_expr(const DevExpr& e, double t, double x
 // the CSR group size
 inline int exec_lanes(const rsd_csr* A) { return A->format == 0 ? (A->sCol16 ? -1 : 0) : default_lanes(A); }
 inline MatView<double> view64(const rsd_csr* A) {
-	return A->format == 0 ? MatView<double>{A->sStart, A->sCol, A->sVal, A->sCol16, A->sBase}
+	return A->format == 0 ? MatView<double>{A->sStart, A->sCol, A->sVal, A->sCol16, A->sBase, A->sUni, A->sOffs}
 	                      : MatView<double>{A->rowPtr, A->col, A->val};
 }
 inline MatView<float> view32(const rsd_csr* A) {
-	return A->format == 0 ? MatView<float>{A->sStart, A->sCol, A->val32, A->sCol16, A->sBase}
+	return A->format == 0 ? MatView<float>{A->sStart, A->sCol, A->val32, A->sCol16, A->sBase, A->sUni, A->sOffs}
 	                      : MatView<float>{A->rowPtr, A->col, A->val32};
+}
+template <typename T>
+inline MatView<T> exec_view(const rsd_csr* A) {
+	if constexpr (sizeof(T) == 4) return view32(A);
+	else return view64(A);
 }
 // diagonal position and values of the execution layout
 inline const int32_t* exec_diag(const rsd_csr* A) { return A->format == 0 ? A->sDiag : A->diag; }

@@ -22,8 +22,9 @@ namespace {
 
 struct CgScal {
 	double rz, pAp, alpha, beta, res0, res, rel, rmax, res64, trueRel;
-	int64_t iter, refinements;
-	int32_t done, converged, reliable, apply_xy, status, pad;
+	double dcur;                      // mixed: current replacement threshold
+	int64_t iter;
+	int32_t refinements, done, converged, reliable, apply_xy, status, pad;
 	unsigned ticket;
 };
 static_assert(sizeof(CgScal) <= sizeof(DevScalars), "CgScal must fit a DevScalars slot");
@@ -87,7 +88,7 @@ __global__ void __launch_bounds__(256) k_cg_init(int64_t n, MatView<double> A, c
 
 // Ap = A p; alpha = rz / p.Ap   (Solver.tpp:69-73)
 template <int L>
-__global__ void __launch_bounds__(256) k_cg_spmv_dot(int64_t n, MatView<double> A, const double* __restrict__ p,
+__global__ void __launch_bounds__(256, 8) k_cg_spmv_dot(int64_t n, MatView<double> A, const double* __restrict__ p,
                                                      double* __restrict__ Ap, CgScal* S, double* partials) {
 	if (is_done(S)) return;
 	const L2Pol pol = make_l2pol();
@@ -185,7 +186,7 @@ template <int L>
 __global__ void __launch_bounds__(256) k_mx_init(int64_t n, MatView<double> A, const double* __restrict__ b,
                                                  const double* __restrict__ x, float* __restrict__ r, float* __restrict__ p,
                                                  float* __restrict__ y, const float* __restrict__ invD, CgScal* S,
-                                                 double* partials, double tol, int relMode, int64_t maxIters) {
+                                                 double* partials, double tol, int relMode, int64_t maxIters, double delta) {
 	const L2Pol pol = make_l2pol();
 	const RowLoop<L> rl;
 	double v[2] = {0.0, 0.0};
@@ -205,6 +206,7 @@ __global__ void __launch_bounds__(256) k_mx_init(int64_t n, MatView<double> A, c
 		const double res0 = sqrt(v[0]);
 		S->res0 = res0; S->rmax = res0; S->res = res0; S->res64 = res0; S->rel = 1.0; S->trueRel = 1.0;
 		S->rz = v[1]; S->iter = 0; S->refinements = 0; S->reliable = 0; S->apply_xy = 0; S->status = 0;
+		S->dcur = delta;
 		const double crit = relMode ? res0 / (res0 + 1e-50) : res0;
 		if (crit < tol) { S->done = 1; S->converged = 1; }
 		else if (maxIters <= 1) { S->done = 1; S->converged = 0; S->iter = maxIters; }
@@ -213,7 +215,7 @@ __global__ void __launch_bounds__(256) k_mx_init(int64_t n, MatView<double> A, c
 }
 
 template <int L>
-__global__ void __launch_bounds__(256) k_mx_spmv_dot(int64_t n, MatView<float> A, const float* __restrict__ p,
+__global__ void __launch_bounds__(256, 8) k_mx_spmv_dot(int64_t n, MatView<float> A, const float* __restrict__ p,
                                                      float* __restrict__ Ap, CgScal* S, double* partials) {
 	if (is_done(S)) return;
 	if (blockIdx.x == 0 && threadIdx.x == 0) { S->reliable = 0; S->apply_xy = 0; }
@@ -235,7 +237,7 @@ __global__ void __launch_bounds__(256) k_mx_spmv_dot(int64_t n, MatView<float> A
 __global__ void __launch_bounds__(256) k_mx_update(int64_t n, float* __restrict__ y, float* __restrict__ r,
                                                    const float* __restrict__ p, const float* __restrict__ Ap,
                                                    const float* __restrict__ invD, CgScal* S, double* partials, double tol,
-                                                   int relMode, int64_t maxIters, double delta, GraphCtl gc) {
+                                                   int relMode, int64_t maxIters, GraphCtl gc) {
 	if (is_done(S)) return;
 	const float alpha = (float)S->alpha;
 	const L2Pol pol = make_l2pol();
@@ -271,7 +273,7 @@ __global__ void __launch_bounds__(256) k_mx_update(int64_t n, float* __restrict_
 		S->res = res; S->iter = k;
 		const double crit = relMode ? res / (S->res0 + 1e-50) : res;
 		if (!isfinite(res)) { S->done = 1; S->converged = 0; S->status = RSD_ENAN; return; }
-		if (crit < tol || res < delta * S->rmax || k + 1 >= maxIters) {
+		if (crit < tol || res < S->dcur * S->rmax || k + 1 >= maxIters) {
 			S->reliable = 1;                    // FP64 residual replacement next
 		} else {
 			S->beta = v[1] / S->rz; S->rz = v[1];
@@ -285,7 +287,7 @@ template <int L>
 __global__ void __launch_bounds__(256) k_mx_reliable(int64_t n, MatView<double> A, const double* __restrict__ b,
                                                      const double* __restrict__ x, const float* __restrict__ y,
                                                      float* __restrict__ r, const float* __restrict__ invD, CgScal* S,
-                                                     double* partials, double tol, int relMode, int64_t maxIters) {
+                                                     double* partials, double tol, int relMode, int64_t maxIters, int adaptive) {
 	if (is_done(S) || !*((volatile const int32_t*)&S->reliable)) return;
 	const L2Pol pol = make_l2pol();
 	const RowLoop<L> rl;
@@ -306,6 +308,7 @@ __global__ void __launch_bounds__(256) k_mx_reliable(int64_t n, MatView<double> 
 	if (grid_sum<2>(v, partials, &S->ticket)) {
 		const double res = sqrt(v[0]);
 		const double rel = res / (S->res0 + 1e-50);
+		if (adaptive) S->dcur = next_delta(S->dcur, S->res, res);
 		S->res64 = res; S->trueRel = rel; S->rmax = res; S->res = res; S->rel = rel;
 		S->refinements += 1;
 		S->apply_xy = 1;
@@ -400,6 +403,9 @@ static int get_ws(rsd_ctx* ctx, size_t bytes, void** out) {
 	return RSD_OK;
 }
 
+// The SpMV kernels are capped at 32 registers (8 blocks of 256 per SM): they are latency-bound on
+// the value/column -> gather chain, and full occupancy measured 20-25% faster than the 40-register
+// build.
 // grids of the row kernels (n rows, max(L,1) threads each) and vector kernels (n entries): one
 // full wave of each kernel's resident blocks; used inside functions that define ctx, n and L
 #define RG(kern) wave_blocks(ctx, kern, 256, n * std::max(L, 1))
@@ -695,25 +701,27 @@ static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const d
 	CgScal* S = scal_slot(ctx, 0);
 	double* partials = ctx->s.partials;
 	const int rel = cfg->tol_type == RSD_TOL_RELATIVE;
-	const double delta = cfg->reliable_delta > 0 ? cfg->reliable_delta : 1e-3;
+	// a fixed threshold when the configuration gives one, else adaptive from 0.1
+	const int adaptive = !(cfg->reliable_delta > 0);
+	const double delta = adaptive ? 0.1 : cfg->reliable_delta;
 	const double tol = cfg->tol;
 	const int64_t maxIt = cfg->max_iters;
 	cudaStream_t st = ctx->stream;
 	auto prologue = [&]() -> int {
 		RSD_CUDA(cudaMemsetAsync(S, 0, sizeof(CgScal), st));
 		if (invD) k_invdiag32<<<VG(k_invdiag32), 256, 0, st>>>(n, exec_diag(A), exec_val(A), invD);
-		RSD_DISPATCH_L(L, (k_mx_init<LL><<<RG(k_mx_init<LL>), 256, 0, st>>>(n, V, b, x, r, p, y, invD, S, partials, tol, rel, maxIt)));
+		RSD_DISPATCH_L(L, (k_mx_init<LL><<<RG(k_mx_init<LL>), 256, 0, st>>>(n, V, b, x, r, p, y, invD, S, partials, tol, rel, maxIt, delta)));
 		RSD_CUDA(cudaGetLastError());
 		return RSD_OK;
 	};
 	auto body_a = [&](GraphCtl gc) -> int {
 		RSD_DISPATCH_L(L, (k_mx_spmv_dot<LL><<<RG(k_mx_spmv_dot<LL>), 256, 0, st>>>(n, V32, p, Ap, S, partials)));
-		k_mx_update<<<VG(k_mx_update), 256, 0, st>>>(n, y, r, p, Ap, invD, S, partials, tol, rel, maxIt, delta, gc);
+		k_mx_update<<<VG(k_mx_update), 256, 0, st>>>(n, y, r, p, Ap, invD, S, partials, tol, rel, maxIt, gc);
 		RSD_CUDA(cudaGetLastError());
 		return RSD_OK;
 	};
 	auto reliable = [&]() -> int {
-		RSD_DISPATCH_L(L, (k_mx_reliable<LL><<<RG(k_mx_reliable<LL>), 256, 0, st>>>(n, V, b, x, y, r, invD, S, partials, tol, rel, maxIt)));
+		RSD_DISPATCH_L(L, (k_mx_reliable<LL><<<RG(k_mx_reliable<LL>), 256, 0, st>>>(n, V, b, x, y, r, invD, S, partials, tol, rel, maxIt, adaptive)));
 		RSD_CUDA(cudaGetLastError());
 		return RSD_OK;
 	};
@@ -730,7 +738,7 @@ static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const d
 		const int64_t ints[] = {n, L, maxIt, rel};
 		std::copy(std::begin(ints), std::end(ints), key.i);
 		key.d[0] = tol;
-		key.d[1] = delta;
+		key.d[1] = adaptive ? -1.0 : delta;
 		if (!G.valid || !(G.key == key)) {
 			RSD_CHECK(build_cg_graph(ctx, true, body_limit(maxIt), prologue, body_a, reliable, body_b, [] { return RSD_OK; }, &G));
 			G.key = key;
@@ -751,7 +759,7 @@ static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const d
 				RSD_DISPATCH_L(L, (k_mx_spmv_dot<LL><<<RG(k_mx_spmv_dot<LL>), 256, 0, st>>>(n, V32, p, Ap, S, partials)));
 				prof_end(ctx, pr);
 				int pu = prof_begin(ctx, PF_CG_UPDATE);
-				k_mx_update<<<VG(k_mx_update), 256, 0, st>>>(n, y, r, p, Ap, invD, S, partials, tol, rel, maxIt, delta, off);
+				k_mx_update<<<VG(k_mx_update), 256, 0, st>>>(n, y, r, p, Ap, invD, S, partials, tol, rel, maxIt, off);
 				prof_end(ctx, pu);
 				int pq = prof_begin(ctx, PF_RELIABLE);
 				RSD_CHECK(reliable());
@@ -784,71 +792,158 @@ void free_graph_cache(rsd_ctx* ctx) {
 namespace {
 
 // ---- GMRES(m): linalg/solver/iterative/gmres/Solver.tpp:3-170 ---------------------------------
-// Device: SpMV, preconditioner, the MGS dot/axpy pairs (each h_ij stays on the device), norms and
-// scalings.  Host: the (m+1) x m Hessenberg, Givens rotations and back substitution, as the
-// reference keeps them (gmres/Workspace.hpp:26-31); one column is read back per Arnoldi step.
-__global__ void k_dot_to(int64_t n, const double* __restrict__ a, const double* __restrict__ b, double* partials,
-                         unsigned* ticket, double* out, int sqrtOut) {
-	double v[1] = {0.0};
-	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) v[0] += a[i] * b[i];
-	if (grid_sum<1>(v, partials, ticket)) *out = sqrtOut ? sqrt(v[0]) : v[0];
-}
-// w += (-h) q, h read from the device
-__global__ void k_axpy_neg_dev(int64_t n, const double* __restrict__ h, const double* __restrict__ q, double* __restrict__ w) {
-	const double a = -(*h);
-	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) w[i] += a * q[i];
-}
-// q = w * (1/hn) unless breakdown (hn <= 1e-14)
-__global__ void k_scale_copy(int64_t n, const double* __restrict__ w, const double* __restrict__ hn, double* __restrict__ q) {
-	const double h = *hn;
-	if (h <= 1e-14) return;
-	const double s = 1.0 / h;
-	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) q[i] = w[i] * s;
-}
-__global__ void k_prec(int64_t n, const double* __restrict__ invD, const double* __restrict__ r, double* __restrict__ z) {
-	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) z[i] = invD ? r[i] * invD[i] : r[i];
-}
-__global__ void k_resid(int64_t n, const double* __restrict__ b, const double* __restrict__ Ax, double* __restrict__ r) {
-	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) r[i] = b[i] + (-1.0) * Ax[i];
-}
-__global__ void k_scal_dev(int64_t n, double a, double* __restrict__ x) {
-	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) x[i] *= a;
-}
-// z = sum_i y_i Q_i (accumulated in basis order, as the reference's axpy sequence)
-__global__ void k_combine(int64_t n, int m, const double* __restrict__ Q, const double* __restrict__ yv, double* __restrict__ z) {
-	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-		double s = 0.0;
-		for (int k = 0; k < m; ++k) s += yv[k] * Q[(int64_t)k * n + i];
-		z[i] = s;
+// Right-preconditioned restarted GMRES.  Device: the preconditioned SpMV (Jacobi folded into the
+// gather, w = A (M^-1 q)), the orthogonalization and the scalings; host: the (m+1) x m Hessenberg,
+// Givens rotations and back substitution, as the reference keeps them (gmres/Workspace.hpp:26-31),
+// with one read-back of the new column per Arnoldi step.
+// Orthogonalization is classical Gram-Schmidt applied twice (CGS2): each pass is one kernel for
+// all j+1 projections Q^T w and one for w -= Q h.  In exact arithmetic it equals the reference's
+// modified Gram-Schmidt; in floating point CGS2 keeps the basis orthogonal to working precision as
+// MGS does, with 4 launches per step instead of 2(j+1).
+// T = double is FP64 GMRES; T = float is the mixed variant: FP32 matrix and Krylov basis, FP64
+// reductions, x and the restart residual r = b - A64 x, convergence declared on that FP64 residual.
+
+// w = A (M^-1 q) with M^-1 = diag(invD) (identity when invD is null)
+template <int L, typename T>
+__global__ void __launch_bounds__(256, 8) k_gm_spmv(int64_t n, MatView<T> A, const T* __restrict__ q,
+                                                 const T* __restrict__ invD, T* __restrict__ w) {
+	const L2Pol pol = make_l2pol();
+	const RowLoop<L> rl;
+	for (int64_t base = rl.base; base < n; base += rl.step) {
+		const int64_t row = base + rl.sub;
+		const T s = row_sum<L, T, T>(A, row, n, rl.lane, pol, [&](int c) {
+			return invD ? ldh(invD + c, pol.last) * ldh(q + c, pol.last) : ldh(q + c, pol.last);
+		});
+		if (rl.lane == 0 && row < n) sth(w + row, s, pol.last);
 	}
 }
 
-static int gmres_fp64(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const double* b, double* x, rsd_report* rep) {
+// h[i] = Q_i . w for i = blockIdx.y (FP64 accumulation; last-block-done reduction per i)
+template <typename T>
+__global__ void k_gm_mdot(int64_t n, const T* __restrict__ Q, int64_t ldq, const T* __restrict__ w, double* partials,
+                          unsigned* tickets, double* h) {
+	const int i = blockIdx.y;
+	const T* __restrict__ qi = Q + (int64_t)i * ldq;
+	double v[1] = {0.0};
+	for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+		v[0] += (double)qi[e] * (double)w[e];
+	if (grid_sum<1>(v, partials + (size_t)i * kMaxPartials, tickets + i)) h[i] = v[0];
+}
+
+// w -= sum_{i<k} h[i] Q_i (basis order)
+template <typename T>
+__global__ void k_gm_mupdate(int64_t n, const T* __restrict__ Q, int64_t ldq, int k, const double* __restrict__ h,
+                             T* __restrict__ w) {
+	for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+		double s = (double)w[e];
+		for (int i = 0; i < k; ++i) s -= h[i] * (double)Q[(int64_t)i * ldq + e];
+		w[e] = (T)s;
+	}
+}
+
+// out = ||w||
+template <typename T>
+__global__ void k_gm_nrm2(int64_t n, const T* __restrict__ w, double* partials, unsigned* ticket, double* out) {
+	double v[1] = {0.0};
+	for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+		v[0] += (double)w[e] * (double)w[e];
+	if (grid_sum<1>(v, partials, ticket)) *out = sqrt(v[0]);
+}
+
+// q = w / hn unless breakdown (hn <= 1e-14)
+template <typename T>
+__global__ void k_gm_scale(int64_t n, const T* __restrict__ w, const double* __restrict__ hn, T* __restrict__ q) {
+	const double h = *hn;
+	if (h <= 1e-14) return;
+	const double s = 1.0 / h;
+	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+		q[i] = (T)((double)w[i] * s);
+}
+
+// q0 = (b - Ax) / beta in T, with beta read from the device
+template <typename T>
+__global__ void k_gm_start(int64_t n, const double* __restrict__ b, const double* __restrict__ Ax,
+                           const double* __restrict__ beta, T* __restrict__ q) {
+	const double s = 1.0 / *beta;
+	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+		q[i] = (T)((b[i] + (-1.0) * Ax[i]) * s);
+}
+
+// ||b - Ax||
+__global__ void k_gm_resnorm(int64_t n, const double* __restrict__ b, const double* __restrict__ Ax, double* partials,
+                             unsigned* ticket, double* out) {
+	double v[1] = {0.0};
+	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+		const double r = b[i] + (-1.0) * Ax[i];
+		v[0] += r * r;
+	}
+	if (grid_sum<1>(v, partials, ticket)) *out = sqrt(v[0]);
+}
+
+// x += M^-1 (sum_i y_i Q_i), accumulated in basis order in FP64
+template <typename T>
+__global__ void k_gm_update_x(int64_t n, int m, const T* __restrict__ Q, int64_t ldq, const double* __restrict__ yv,
+                              const T* __restrict__ invD, double* __restrict__ x) {
+	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+		double s = 0.0;
+		for (int k = 0; k < m; ++k) s += yv[k] * (double)Q[(int64_t)k * ldq + i];
+		x[i] += invD ? (double)invD[i] * s : s;
+	}
+}
+
+template <typename T>
+__global__ void k_gm_invdiag(int64_t n, const int32_t* __restrict__ dpos, const double* __restrict__ val, T* __restrict__ d) {
+	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+		const int32_t q = dpos[i];
+		const double v = q >= 0 ? val[q] : 0.0;
+		d[i] = (T)((fabs(v) > 1e-300) ? 1.0 / v : 1.0);
+	}
+}
+
+template <typename T>
+static int gmres_run(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const double* b, double* x, rsd_report* rep) {
+	constexpr bool kMixed = sizeof(T) == 4;
 	const int64_t n = A->n;
 	const int64_t m = std::max<int64_t>(1, cfg->krylov_dim);
+	if (m + 1 > 255) return set_error(RSD_EINVAL, "GMRES krylov_dim above 254");
+	if (kMixed) RSD_CHECK(f32_sync(ctx, A)); else RSD_CHECK(exec_sync(ctx, A));
+	const int L = exec_lanes(A);
+	const MatView<T> V = exec_view<T>(A);
+	const int64_t ns = pad_len(n);
+	// workspace: Q (m+1 vectors), w, invD in T; Ax in FP64; partials for m+1 reductions; tickets; H columns
+	const size_t qBytes = sizeof(T) * (size_t)(m + 3) * ns;
+	const size_t axBytes = sizeof(double) * (size_t)ns;
+	const size_t pBytes = sizeof(double) * (size_t)(m + 1) * kMaxPartials;
+	const size_t hBytes = sizeof(double) * (size_t)(4 * (m + 2) + 8);
+	const size_t tBytes = sizeof(unsigned) * (size_t)(m + 2);
 	void* wsv;
-	RSD_CHECK(get_ws(ctx, sizeof(double) * ((m + 4) * n + 4 * (m + 2) + 64), &wsv));
-	double* Q = (double*)wsv;
-	double* w = Q + (m + 1) * n;
-	double* z = w + n;
-	double* invD = cfg->precond == RSD_JACOBI ? z + n : nullptr;
-	double* dH = z + 2 * n;          // device column buffer: h_0..h_{j+1}, plus y
-	double* dY = dH + (m + 2);
+	RSD_CHECK(get_ws(ctx, qBytes + axBytes + pBytes + hBytes + tBytes + 1024, &wsv));
+	char* base = (char*)wsv;
+	T* Q = (T*)base;
+	T* w = Q + (m + 1) * ns;
+	T* invD = cfg->precond == RSD_JACOBI ? w + ns : nullptr;
+	double* Ax = (double*)(base + qBytes);
+	double* parts = (double*)(base + qBytes + axBytes);
+	double* dH1 = (double*)(base + qBytes + axBytes + pBytes);
+	double* dH2 = dH1 + (m + 2);
+	double* dY = dH2 + (m + 2);
+	double* dNorm = dY + (m + 2);
+	unsigned* tickets = (unsigned*)(base + qBytes + axBytes + pBytes + hBytes);
+	cudaStream_t st = ctx->stream;
+	RSD_CUDA(cudaMemsetAsync(tickets, 0, tBytes, st));
 	const int gv = vec_grid(ctx, n), grd = red_grid(ctx, n);
-	unsigned* ticket = &scal_slot(ctx, 2)->ticket;
 	const bool relMode = cfg->tol_type == RSD_TOL_RELATIVE;
 	const double breakdownTol = 1e-14, eps = 1e-50;
-	std::vector<double> H((m + 1) * m, 0.0), cs(m), sn(m), g(m + 1), yv(m), col(m + 2);
+	std::vector<double> H((m + 1) * m, 0.0), cs(m), sn(m), g(m + 1), yv(m), col(2 * (m + 2));
 	auto Hat = [&](int64_t i, int64_t j) -> double& { return H[j * (m + 1) + i]; };
-	RSD_CHECK(exec_sync(ctx, A));
-	if (invD) k_invdiag64<<<gv, 256, 0, ctx->stream>>>(n, exec_diag(A), exec_val(A), invD);
+	if (invD) k_gm_invdiag<T><<<gv, 256, 0, st>>>(n, exec_diag(A), exec_val(A), invD);
+	// FP64 residual of the current x; q0 = r / beta
 	auto residual = [&](double* beta) -> int {
-		RSD_CHECK(spmv_f64(ctx, A, x, w));
-		k_resid<<<gv, 256, 0, ctx->stream>>>(n, b, w, Q);
-		k_dot_to<<<grd, kReduceThreads, 0, ctx->stream>>>(n, Q, Q, ctx->s.partials, ticket, dH, 1);
+		RSD_CHECK(spmv_f64(ctx, A, x, Ax));
+		k_gm_resnorm<<<grd, kReduceThreads, 0, st>>>(n, b, Ax, parts, tickets + m + 1, dNorm);
 		RSD_CUDA(cudaGetLastError());
-		RSD_CUDA(cudaMemcpyAsync(ctx->s.hbuf, dH, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-		RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+		RSD_CUDA(cudaMemcpyAsync(ctx->s.hbuf, dNorm, sizeof(double), cudaMemcpyDeviceToHost, st));
+		RSD_CUDA(cudaStreamSynchronize(st));
 		*beta = ctx->s.hbuf[0];
 		return RSD_OK;
 	};
@@ -862,29 +957,31 @@ static int gmres_fp64(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const
 		if (rep) *rep = R;
 		return RSD_OK;
 	}
-	int64_t total = 0;
+	int64_t total = 0, cycles = 0;
 	double beta = res0;
 	while (total < cfg->max_iters) {
-		k_scal_dev<<<gv, 256, 0, ctx->stream>>>(n, 1.0 / beta, Q);
+		k_gm_start<T><<<gv, 256, 0, st>>>(n, b, Ax, dNorm, Q);
+		++cycles;
 		g[0] = beta;
 		for (int64_t i = 1; i <= m; ++i) g[i] = 0.0;
 		int64_t mLocal = 0;
 		bool breakdown = false;
 		for (int64_t j = 0; j < m; ++j) {
-			double* qj = Q + j * n;
-			k_prec<<<gv, 256, 0, ctx->stream>>>(n, invD, qj, z);
-			RSD_CHECK(spmv_f64(ctx, A, z, w));
-			for (int64_t i = 0; i <= j; ++i) {
-				k_dot_to<<<grd, kReduceThreads, 0, ctx->stream>>>(n, Q + i * n, w, ctx->s.partials, ticket, dH + i, 0);
-				k_axpy_neg_dev<<<gv, 256, 0, ctx->stream>>>(n, dH + i, Q + i * n, w);
+			const T* qj = Q + j * ns;
+			RSD_DISPATCH_L(L, (k_gm_spmv<LL, T><<<wave_blocks(ctx, k_gm_spmv<LL, T>, 256, n * std::max(LL, 1)), 256, 0, st>>>(n, V, qj, invD, w)));
+			const int k = (int)(j + 1);
+			for (double* dh : {dH1, dH2}) {
+				k_gm_mdot<T><<<dim3(grd, k), kReduceThreads, 0, st>>>(n, Q, ns, w, parts, tickets, dh);
+				k_gm_mupdate<T><<<gv, 256, 0, st>>>(n, Q, ns, k, dh, w);
 			}
-			k_dot_to<<<grd, kReduceThreads, 0, ctx->stream>>>(n, w, w, ctx->s.partials, ticket, dH + j + 1, 1);
-			k_scale_copy<<<gv, 256, 0, ctx->stream>>>(n, w, dH + j + 1, Q + (j + 1) * n);
+			k_gm_nrm2<T><<<grd, kReduceThreads, 0, st>>>(n, w, parts, tickets + m + 1, dNorm);
+			k_gm_scale<T><<<gv, 256, 0, st>>>(n, w, dNorm, Q + (j + 1) * ns);
 			RSD_CUDA(cudaGetLastError());
-			RSD_CUDA(cudaMemcpyAsync(col.data(), dH, sizeof(double) * (j + 2), cudaMemcpyDeviceToHost, ctx->stream));
-			RSD_CUDA(cudaStreamSynchronize(ctx->stream));
-			for (int64_t i = 0; i <= j; ++i) Hat(i, j) = col[i];
-			const double hNext = col[j + 1];
+			RSD_CUDA(cudaMemcpyAsync(col.data(), dH1, sizeof(double) * 2 * (m + 2), cudaMemcpyDeviceToHost, st));
+			double hNext = 0.0;
+			RSD_CUDA(cudaMemcpyAsync(&hNext, dNorm, sizeof(double), cudaMemcpyDeviceToHost, st));
+			RSD_CUDA(cudaStreamSynchronize(st));
+			for (int64_t i = 0; i <= j; ++i) Hat(i, j) = col[i] + col[(m + 2) + i];
 			++total;
 			breakdown = hNext <= breakdownTol;
 			for (int64_t i = 0; i < j; ++i) {
@@ -910,18 +1007,18 @@ static int gmres_fp64(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const
 			for (int64_t k = i + 1; k < mLocal; ++k) s -= Hat(i, k) * yv[k];
 			yv[i] = s / Hat(i, i);
 		}
-		RSD_CUDA(cudaMemcpyAsync(dY, yv.data(), sizeof(double) * mLocal, cudaMemcpyHostToDevice, ctx->stream));
-		k_combine<<<gv, 256, 0, ctx->stream>>>(n, (int)mLocal, Q, dY, z);
-		k_prec<<<gv, 256, 0, ctx->stream>>>(n, invD, z, w);
-		RSD_CHECK(rsd_axpy(ctx, n, 1.0, w, x));
+		RSD_CUDA(cudaMemcpyAsync(dY, yv.data(), sizeof(double) * mLocal, cudaMemcpyHostToDevice, st));
+		k_gm_update_x<T><<<gv, 256, 0, st>>>(n, (int)mLocal, Q, ns, dY, invD, x);
 		RSD_CHECK(residual(&beta));
-		if (R.status || converged(beta) || breakdown || total >= cfg->max_iters) break;
+		if (R.status || converged(beta) || total >= cfg->max_iters) break;
+		if (breakdown && !kMixed) break;   // FP64: the Krylov space is exhausted; mixed: restart in FP64
 	}
 	R.converged = R.status ? 0 : converged(beta);
 	R.finalResidual = beta;
 	R.finalResidualRel = beta / (res0 + eps);
 	R.iterations = total;
 	R.trueResidualRel = beta / (res0 + eps);
+	R.refinements = kMixed ? cycles : 0;
 	if (rep) *rep = R;
 	return RSD_OK;
 }
@@ -1018,7 +1115,7 @@ int solve(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const double* b, 
 	if (cfg->type == RSD_CG) return cfg->precision == RSD_MIXED ? cg_mixed(ctx, A, cfg, b, x, rep) : cg_fp64(ctx, A, cfg, b, x, rep);
 	if (cfg->type == RSD_GMRES) {
 		if (cfg->krylov_dim <= 0) return set_error(RSD_EINVAL, "GMRES needs krylov_dim >= 1");
-		return gmres_fp64(ctx, A, cfg, b, x, rep);
+		return cfg->precision == RSD_MIXED ? gmres_run<float>(ctx, A, cfg, b, x, rep) : gmres_run<double>(ctx, A, cfg, b, x, rep);
 	}
 	return set_error(RSD_EINVAL, "unknown solver type");
 }

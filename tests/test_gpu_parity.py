@@ -121,6 +121,28 @@ def test_newton_gmres_matches_reference(rsd, ctx):
     assert relerr(U.download(), g["U"]) <= 1e-11
 
 
+def test_mixed_gmres_and_newton(rsd, ctx):
+    # FP32 Arnoldi with FP64 restart residuals: converges on the FP64 residual, and a Newton solve
+    # with mixed inner GMRES reaches the FP64 Newton solution
+    h = make_heat(rsd, ctx, 3, 2, 3, [6, 5, 4], [0, 0, 0], [1, 1, 1], src_expr="10", k_expr="1 + 0.5*T", dk_expr="0.5",
+                  dirichlet={0: "0", 1: "1"})
+    U64, Umx = ctx.array(h.n).zero(), ctx.array(h.n).zero()
+    r64 = h.newton(U64, 1e-10, 1e-10, 50, cfg=rsd.SolverConfig.make(type=rsd.GMRES, tol=1e-12, max_iters=5000, krylov_dim=30))
+    rmx = h.newton(Umx, 1e-10, 1e-10, 50, cfg=rsd.SolverConfig.make(type=rsd.GMRES, precision=rsd.MIXED, tol=1e-12,
+                                                                    max_iters=5000, krylov_dim=30))
+    assert r64["converged"] and rmx["converged"]
+    assert relerr(Umx.download(), U64.download()) <= 1e-9
+    # one linear solve with the Jacobian: the reported residual is the FP64 one
+    h.assemble_matrix(1.0, 0.0, 1.0, 0.0, U=U64)
+    F = ctx.to_device(np.random.default_rng(2).standard_normal(h.n))
+    x = ctx.array(h.n).zero()
+    rep = rsd.solve(ctx, h.K, F, x, type=rsd.GMRES, precision=rsd.MIXED, tol=1e-10, max_iters=5000, krylov_dim=20)
+    rp, col = h.K.pattern()
+    r = F.download() - oracle.spmv(rp, col, h.K.values(), x.download())
+    assert rep["converged"] and np.linalg.norm(r) / np.linalg.norm(F.download()) < 1e-10
+    assert rep["refinements"] >= 1
+
+
 def random_csr(n, per_row, seed):
     rng = np.random.default_rng(seed)
     rows = []
