@@ -139,45 +139,57 @@ def initial_condition(xyz, a2t, seed=2):
 # clocks during the timed region
 # ---------------------------------------------------------------------------------------------
 class ClockSampler:
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and clock-event reasons sampled by NVML (read-only queries) every 2 ms in a thread
+    while the timed region runs; nvidia-smi's 100 ms minimum interval is longer than a timed region
+    of a few steps.  Reports the median SM clock under load, the maximum SM clock and the reasons
+    seen active."""
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"), ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"), ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
+               ("hw_power_brake", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
 
     def __init__(self, device):
         self.device = device
-        self.path = tempfile.mktemp(suffix=".csv")
-        self.proc = None
+        self.thread = None
+        self.samples, self.reasons = [], set()
+        self.err = None
+
+    def _run(self):
+        import pynvml
+        h = pynvml.nvmlDeviceGetHandleByIndex(self.device)
+        while not self.stop_flag:
+            try:
+                self.samples.append(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+                r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                for name, const in self.REASONS:
+                    if r & getattr(pynvml, const, 0):
+                        self.reasons.add(name)
+            except Exception as e:  # noqa: BLE001
+                self.err = str(e)
+                break
+            time.sleep(0.002)
 
     def start(self):
+        import threading
         try:
-            self.f = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.QUERY,
-                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
-                                         stderr=subprocess.DEVNULL)
-        except Exception:
-            self.proc = None
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.device)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+        except Exception as e:  # noqa: BLE001
+            self.err = f"nvml unavailable: {e}"
+            return
+        self.stop_flag = False
+        self.thread = threading.Thread(target=self._run, daemon=True)
+        self.thread.start()
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        self.proc.wait()
-        self.f.close()
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
-            p = [x.strip() for x in line.split(",")]
-            if len(p) < 9:
-                continue
-            try:
-                sm.append(float(p[1])); mx.append(float(p[2]))
-            except ValueError:
-                continue
-            for nm, v in zip(names, p[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        os.unlink(self.path)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        if self.thread is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [self.err or "not sampled"], "samples": 0}
+        self.stop_flag = True
+        self.thread.join()
+        sm = self.samples
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": float(self.max_mhz),
+                "reasons": sorted(self.reasons), "samples": len(sm), "source": "nvml, 2 ms"}
 
 
 def measured_peak_hbm():
@@ -314,7 +326,8 @@ def run_batch(rsd, ctx, stream, count, reps, peak):
 def run_newton(rsd, ctx, stream, S):
     """Steady nonlinear heat on S^3 Q2 hexes: k(T) = 1 + 0.5 T, f = 10, T = 0 on x = 0 and 1 on x = 1,
     zero flux elsewhere; Newton to 1e-10 (absolute or relative) with GMRES(30) + Jacobi inner solves
-    to 1e-12, x0 = 0.  Checked against the 1D closed form T = 2(sqrt(1 + u) - 1), u = 6.25 x - 5 x^2."""
+    to 1e-12, x0 = 0, inner GMRES in FP64 and mixed (FP32 Arnoldi, FP64 restart residuals).  Checked
+    against the 1D closed form T = 2(sqrt(1 + u) - 1), u = 6.25 x - 5 x^2."""
     import torch
     from importlib import import_module
     bm = import_module("residuum_solver_b200.blockmesh")
@@ -324,24 +337,30 @@ def run_newton(rsd, ctx, stream, S):
                  dirichlet={0: "0", 1: "1"})
     setup_s = time.time() - t0
     U = ctx.array(h.n)
-    cfg = rsd.SolverConfig.make(type=rsd.GMRES, krylov_dim=30, tol=1e-12, max_iters=100000)
-    U.zero()
-    h.newton(U, 1e-10, 1e-10, 50, cfg)          # warm-up (workspace setup)
-    U.zero()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    rep = h.newton(U, 1e-10, 1e-10, 50, cfg)
-    e1.record(stream)
-    e1.synchronize()
     t2a, a2t = h.dofmap()
     x = xyz.reshape(-1, 3)[a2t, 0]
     exact = 2.0 * (np.sqrt(1.0 + 6.25 * x - 5.0 * x * x) - 1.0)
-    err = float(np.max(np.abs(U.download() - exact)))
-    return {"workload": f"{S}^3 Q2 hexes, k(T) = 1 + 0.5T, f = 10, Newton 1e-10, GMRES(30) + Jacobi 1e-12",
-            "n_free": h.n, "nnz": h.nnz, "setup_s": round(setup_s, 2), "ms": e0.elapsed_time(e1),
-            "newton_iterations": rep["iterations"], "gmres_iterations_total": rep["refinements"],
-            "converged": bool(rep["converged"]), "final_residual": rep["finalResidual"],
-            "max_error_vs_1d_closed_form": err}
+    out = {"workload": f"{S}^3 Q2 hexes, k(T) = 1 + 0.5T, f = 10, Newton 1e-10, GMRES(30) + Jacobi 1e-12",
+           "n_free": h.n, "nnz": h.nnz, "setup_s": round(setup_s, 2)}
+    sols = {}
+    for key, prec in (("fp64", rsd.FP64), ("mixed", rsd.MIXED)):
+        cfg = rsd.SolverConfig.make(type=rsd.GMRES, krylov_dim=30, tol=1e-12, max_iters=100000, precision=prec)
+        U.zero()
+        h.newton(U, 1e-10, 1e-10, 50, cfg)          # warm-up (workspace setup)
+        U.zero()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rep = h.newton(U, 1e-10, 1e-10, 50, cfg)
+        e1.record(stream)
+        e1.synchronize()
+        sols[key] = U.download()
+        out[key] = {"ms": e0.elapsed_time(e1), "newton_iterations": rep["iterations"],
+                    "gmres_iterations_total": rep["refinements"], "converged": bool(rep["converged"]),
+                    "final_residual": rep["finalResidual"],
+                    "max_error_vs_1d_closed_form": float(np.max(np.abs(sols[key] - exact)))}
+    out["speedup_mixed_vs_fp64"] = out["fp64"]["ms"] / out["mixed"]["ms"]
+    out["mixed_vs_fp64_max_rel_diff"] = float(np.max(np.abs(sols["mixed"] - sols["fp64"])) / np.max(np.abs(sols["fp64"])))
+    return out
 
 
 def fourier_theta(xyz, ien, npe, seed, modes=16, amp=0.5):

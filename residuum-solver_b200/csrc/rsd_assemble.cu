@@ -108,8 +108,9 @@ __device__ __forceinline__ void stage_tables(const AsmParams& prm, double* sm) {
 	__syncthreads();
 }
 
-// phase 2: one quadrature point, all inputs from the staged node data
-template <int NSD, int P>
+// phase 2: one quadrature point, all inputs from the staged node data.  GRAD = false (mass and load
+// terms only): no inverse Jacobian, no gradients and no conductivity model are evaluated.
+template <int NSD, int P, bool GRAD>
 __device__ __forceinline__ void eval_point(const AsmParams& prm, const Needs& nd, const double* tq, double w,
                                            const double* nodes, double ke, double* rec) {
 	using E = Elem<NSD, P>;
@@ -126,15 +127,16 @@ __device__ __forceinline__ void eval_point(const AsmParams& prm, const Needs& nd
 		for (int i = 0; i < NSD; ++i)
 #pragma unroll
 			for (int al = 0; al < NSD; ++al) J[i * NSD + al] += t[1 + al] * nb[N_X + i];
-		if (nd.state) {
+		if (GRAD && nd.state) {
 			Tq += t[0] * nb[N_U];
 #pragma unroll
 			for (int al = 0; al < NSD; ++al) dT[al] += t[1 + al] * nb[N_U];
 		}
 		if (nd.field) {
 			Vq += t[0] * nb[N_V];
+			if (GRAD)
 #pragma unroll
-			for (int al = 0; al < NSD; ++al) dV[al] += t[1 + al] * nb[N_V];
+				for (int al = 0; al < NSD; ++al) dV[al] += t[1 + al] * nb[N_V];
 		}
 		if (nd.field2) Wq += t[0] * nb[N_W];
 		if (nd.load)
@@ -145,6 +147,15 @@ __device__ __forceinline__ void eval_point(const AsmParams& prm, const Needs& nd
 	if (NSD == 2) {
 		const double g0 = J[0] * J[0] + J[2] * J[2], g1 = J[0] * J[1] + J[2] * J[3], g3 = J[1] * J[1] + J[3] * J[3];
 		detg = g0 * g3 - g1 * g1;
+		if (!GRAD) {
+			rec[R_WM] = sqrt(detg) * w;
+			if (nd.field) rec[R_V] = Vq;
+			if (nd.field2) rec[R_W] = Wq;
+			rec[R_K] = 0.0;
+			rec[R_DK] = 0.0;
+			if (nd.load) rec[R_F] = prm.srcExpr.n ? eval_expr(prm.srcExpr, prm.time, xq[0], xq[1], 0.0, 0.0) : 0.0;
+			return;
+		}
 		const double di = 1.0 / (J[0] * J[3] - J[1] * J[2]);
 		inv[0] = di * J[3]; inv[1] = -di * J[1]; inv[2] = -di * J[2]; inv[3] = di * J[0];
 	} else {
@@ -154,6 +165,15 @@ __device__ __forceinline__ void eval_point(const AsmParams& prm, const Needs& nd
 #pragma unroll
 			for (int a = 0; a < 3; ++a) gm[b * 3 + a] = J[a] * J[b] + J[3 + a] * J[3 + b] + J[6 + a] * J[6 + b];
 		detg = gm[0] * (gm[4] * gm[8] - gm[5] * gm[7]) - gm[1] * (gm[3] * gm[8] - gm[5] * gm[6]) + gm[2] * (gm[3] * gm[7] - gm[4] * gm[6]);
+		if (!GRAD) {
+			rec[R_WM] = sqrt(detg) * w;
+			if (nd.field) rec[R_V] = Vq;
+			if (nd.field2) rec[R_W] = Wq;
+			rec[R_K] = 0.0;
+			rec[R_DK] = 0.0;
+			if (nd.load) rec[R_F] = prm.srcExpr.n ? eval_expr(prm.srcExpr, prm.time, xq[0], xq[1], xq[2], 0.0) : 0.0;
+			return;
+		}
 		const double detJ = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) + J[2] * (J[3] * J[7] - J[4] * J[6]);
 		const double di = 1.0 / detJ;
 		inv[0] = di * (J[4] * J[8] - J[5] * J[7]);
@@ -245,7 +265,7 @@ __device__ __forceinline__ void node_grad(const double* rec, const double* ta, d
 		__syncwarp();                                                                            \
 		if (inRange)                                                                             \
 			for (int q = a; q < prm.nq; q += G)                                                  \
-				eval_point<NSD, P>(prm, nd, tab + q * TS, wq[q], nodes, ke, recs + q * REC);     \
+				eval_point<NSD, P, kGrad>(prm, nd, tab + q * TS, wq[q], nodes, ke, recs + q * REC);     \
 		__syncwarp();
 
 #define RSD_ELEMENT_LOOP_END                                                                     \
@@ -258,6 +278,7 @@ __device__ __forceinline__ void node_grad(const double* rec, const double* ta, d
 // ---------------------------------------------------------------------------------------------
 template <int NSD, int P>
 __global__ void __launch_bounds__(kAsmThreads) k_asm_matrix(const AsmParams prm) {
+	constexpr bool kGrad = true;
 	Needs nd{};
 	nd.state = prm.kExpr.n || prm.dkExpr.n || prm.cTDiff != 0.0;
 	RSD_ELEMENT_LOOP_BEGIN
@@ -368,9 +389,11 @@ __global__ void k_build_slots(int64_t nelem, const int32_t* __restrict__ ien, co
 // sum_b (dN_a/dx . dN_b/dx) V_b = dN_a/dx . grad V and sum_b N_a N_b V_b = N_a V(x_q), with V and
 // grad V evaluated once per point in phase 2.
 // ---------------------------------------------------------------------------------------------
-template <int NSD, int P>
+template <int NSD, int P, int W>
 __global__ void __launch_bounds__(kAsmThreads) k_asm_vector(const AsmParams prm) {
-	const int which = prm.which;
+	constexpr int which = W;
+	// the diffusion-type terms need gradients; load and mass terms only the measure
+	constexpr bool kGrad = W == 1 || W == 4 || W == 5 || W == 6 || W == 8 || W == 9;
 	Needs nd{};
 	nd.load = which == 0 || which == 7 || which == 9;
 	nd.field = which != 0;
@@ -413,12 +436,15 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_vector(const AsmParams prm)
 			}
 			if (nd.load) Fa += (rec[R_F] * Na) * wm;
 			if (which == 0) continue;
-			double dx[3];
-			node_grad<NSD>(rec, ta, dx);
-			double dd = 0.0;
+			double kd = 0.0;
+			if constexpr (kGrad) {
+				double dx[3];
+				node_grad<NSD>(rec, ta, dx);
+				double dd = 0.0;
 #pragma unroll
-			for (int i = 0; i < NSD; ++i) dd += dx[i] * rec[R_GV + i];
-			const double kd = rec[R_K] * dd;               // per-element factor included
+				for (int i = 0; i < NSD; ++i) dd += dx[i] * rec[R_GV + i];
+				kd = rec[R_K] * dd;                        // per-element factor included
+			}
 			const double mass = prm.rho * prm.cp * Na * rec[R_V];
 			switch (which) {
 				case 1: Fa += kd * wm; break;
@@ -443,6 +469,7 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_vector(const AsmParams prm)
 // Assembler::assembleDiagonal (Assembler.tpp:142-197) for c_diff*Diffusion + c_mass*Mass
 template <int NSD, int P>
 __global__ void __launch_bounds__(kAsmThreads) k_asm_diag(const AsmParams prm) {
+	constexpr bool kGrad = true;
 	Needs nd{};
 	nd.state = prm.kExpr.n != 0;
 	RSD_ELEMENT_LOOP_BEGIN
@@ -585,8 +612,40 @@ static int launch_one(void (*kern)(const AsmParams), dim3 gr, size_t smem, rsd_c
 	}
 
 RSD_ASM_DISPATCH(k_asm_matrix)
-RSD_ASM_DISPATCH(k_asm_vector)
 RSD_ASM_DISPATCH(k_asm_diag)
+
+// the vector kernel is specialised per operand mode, so that each mode compiles only its terms
+template <int NSD, int P>
+static int launch_vector_mode(rsd_ctx* ctx, dim3 gr, size_t smem, const AsmParams& p) {
+	switch (p.which) {
+		case 0: return launch_one(k_asm_vector<NSD, P, 0>, gr, smem, ctx, p);
+		case 1: return launch_one(k_asm_vector<NSD, P, 1>, gr, smem, ctx, p);
+		case 2: return launch_one(k_asm_vector<NSD, P, 2>, gr, smem, ctx, p);
+		case 3: return launch_one(k_asm_vector<NSD, P, 3>, gr, smem, ctx, p);
+		case 4: return launch_one(k_asm_vector<NSD, P, 4>, gr, smem, ctx, p);
+		case 5: return launch_one(k_asm_vector<NSD, P, 5>, gr, smem, ctx, p);
+		case 6: return launch_one(k_asm_vector<NSD, P, 6>, gr, smem, ctx, p);
+		case 7: return launch_one(k_asm_vector<NSD, P, 7>, gr, smem, ctx, p);
+		case 8: return launch_one(k_asm_vector<NSD, P, 8>, gr, smem, ctx, p);
+		case 9: return launch_one(k_asm_vector<NSD, P, 9>, gr, smem, ctx, p);
+		default: return set_error(RSD_EINVAL, "unknown vector assembly mode");
+	}
+}
+
+static int launch_k_asm_vector(rsd_ctx* ctx, const rsd_heat* h, const AsmParams& p) {
+	const int nsd = h->m->nsd, ord = h->m->order, G = group_width(h->m->npe);
+	const size_t smem = asm_smem_bytes(h->m->npe, h->nq);
+	const int epb = kAsmWarps * (32 / G);
+	int64_t blocks = (p.nelem + epb - 1) / epb;
+	blocks = std::min<int64_t>(blocks, (int64_t)ctx->num_sms * 16);
+	dim3 gr((unsigned)std::max<int64_t>(blocks, 1));
+	if (nsd == 2 && ord == 1) return launch_vector_mode<2, 1>(ctx, gr, smem, p);
+	if (nsd == 2 && ord == 2) return launch_vector_mode<2, 2>(ctx, gr, smem, p);
+	if (nsd == 2 && ord == 3) return launch_vector_mode<2, 3>(ctx, gr, smem, p);
+	if (nsd == 3 && ord == 1) return launch_vector_mode<3, 1>(ctx, gr, smem, p);
+	if (nsd == 3 && ord == 2) return launch_vector_mode<3, 2>(ctx, gr, smem, p);
+	return set_error(RSD_EINVAL, "unsupported element");
+}
 
 // Build the element -> CSR slot map for h's pattern (once).  Skipped, leaving the binary-search
 // scatter, when RSD_SLOT_MAP=0 or when the map would take more than a quarter of free memory.
