@@ -266,16 +266,46 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line))
 
 
-def run_batch(rsd, ctx, stream, count, reps, peak):
+def batch_share(count, world, rank):
+    """The problems of the batched workload that rank `rank` of `world` solves: largest first, each to
+    the rank with the fewest rows so far (ties to the lower rank).  Independent problems need no
+    exchange, so ranks share nothing but the final timing."""
+    rows = []
+    for p in range(count):
+        head = uniforms(mt19937_64_stream(4000 + p, 2))
+        nx, ny = (32 + int(u * 225) for u in head)
+        rows.append(((nx - 1) * (ny - 1), p))
+    load = [0] * world
+    mine = []
+    for r, p in sorted(rows, key=lambda t: (-t[0], t[1])):
+        k = min(range(world), key=lambda i: (load[i], i))
+        load[k] += r
+        if k == rank:
+            mine.append(p)
+    return sorted(mine)
+
+
+def ranks_reduce(value, op, dist, device):
+    """max or sum of a float over the ranks (the value itself on one rank)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def run_batch(rsd, ctx, stream, count, reps, peak, rank=0, world=1, dist=None, device="cuda"):
     """The batched workload: `count` unit-square Q1 problems (Nx, Ny ~ U{32..256}, log-normal
     per-element conductivity, unit source, T = 0 on the boundary) solved together by
-    rsd_batch_solve, CG + Jacobi to 1e-8 (mixed: FP64-checked), x0 = 0."""
+    rsd_batch_solve, CG + Jacobi to 1e-8 (mixed: FP64-checked), x0 = 0.  With several ranks each
+    solves its share (batch_share) and the time is the slowest rank's."""
     import torch
     from importlib import import_module
     bm = import_module("residuum_solver_b200.blockmesh")
     t0 = time.time()
     probs = []
-    for p in range(count):
+    for p in batch_share(count, world, rank):
         nx, ny, ke = batch_problem(p)
         xyz, ien, rg = bm.block_mesh(2, [nx, ny], [0, 0], [1, 1], 1)
         h = rsd.Heat(ctx, rsd.Mesh(ctx, 2, 1, xyz, ien, rg), 2, k_elem=ke, src_expr="1",
@@ -289,13 +319,17 @@ def run_batch(rsd, ctx, stream, count, reps, peak):
     xs = [ctx.array(h.n) for h, _ in probs]
     ns = np.array([h.n for h, _ in probs], dtype=np.float64)
     nnzs = np.array([h.nnz for h, _ in probs], dtype=np.float64)
-    out = {"problems": count, "rows": int(ns.sum()), "nnz": int(nnzs.sum()), "setup_s": round(setup_s, 2)}
+    out = {"problems": count, "rows": int(ranks_reduce(ns.sum(), "sum", dist, device)),
+           "nnz": int(ranks_reduce(nnzs.sum(), "sum", dist, device)), "setup_s": round(setup_s, 2), "ranks": world}
     for key, prec in (("mixed", rsd.MIXED), ("fp64", rsd.FP64)):
         cfg = rsd.SolverConfig.make(precision=prec, tol=1e-8, max_iters=100000)
         ts = []
         for r in range(reps + 1):
             for x in xs:
                 x.zero()
+            torch.cuda.synchronize()
+            if dist is not None:
+                dist.barrier()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             rr = B.solve([F for _, F in probs], xs, cfg)
@@ -310,12 +344,16 @@ def run_batch(rsd, ctx, stream, count, reps, peak):
         # each FP64 residual replacement one FP64 SpMV plus 4 n*8
         byts = float(np.sum(its * (nnzs * (s + 4) + 4 * (ns + 1) + 2 * ns * s + 11 * ns * s)
                             + refs * (nnzs * 12 + 4 * (ns + 1) + 2 * ns * 8 + 4 * ns * 8)))
-        ms = float(np.median(ts))
-        out[key] = {"ms": ms, "problems_per_s": count / (ms * 1e-3), "all_converged": all(q["converged"] for q in rr),
-                    "iterations_total": int(its.sum()), "iterations_max": int(its.max()),
-                    "refinements_total": int(refs.sum()),
-                    "max_true_residual_rel": max(q["trueResidualRel"] for q in rr),
-                    "algorithmic_gbs": byts / (ms * 1e-3) / 1e9, "frac_of_measured_hbm": byts / (ms * 1e-3) / 1e9 / peak}
+        ms = ranks_reduce(float(np.median(ts)), "max", dist, device)
+        byts = ranks_reduce(byts, "sum", dist, device)
+        conv = ranks_reduce(0.0 if all(q["converged"] for q in rr) else 1.0, "max", dist, device) == 0.0
+        out[key] = {"ms": ms, "problems_per_s": count / (ms * 1e-3), "all_converged": conv,
+                    "iterations_total": int(ranks_reduce(its.sum(), "sum", dist, device)),
+                    "iterations_max": int(ranks_reduce(its.max() if len(its) else 0, "max", dist, device)),
+                    "refinements_total": int(ranks_reduce(refs.sum(), "sum", dist, device)),
+                    "max_true_residual_rel": ranks_reduce(max([q["trueResidualRel"] for q in rr] or [0.0]), "max", dist, device),
+                    "algorithmic_gbs": byts / (ms * 1e-3) / 1e9,
+                    "frac_of_measured_hbm": byts / (ms * 1e-3) / 1e9 / (peak * world)}
     out["speedup_mixed_vs_fp64"] = out["fp64"]["ms"] / out["mixed"]["ms"]
     out["how"] = ("one rsd_batch_solve call (one persistent launch), CUDA events around the call, median of "
                   f"{reps}; setup (meshes, patterns, assembly) outside the timed region")
@@ -589,7 +627,7 @@ def main():
 
     batch = None
     if args.batch > 0:
-        batch = run_batch(rsd, ctx, stream, args.batch, 3, measured_peak_hbm()[0])
+        batch = run_batch(rsd, ctx, stream, args.batch, 3, measured_peak_hbm()[0], rank, world, dist, f"cuda:{local}")
     newton = run_newton(rsd, ctx, stream, args.newton) if args.newton > 0 else None
     adjoint = run_adjoint(rsd, ctx, stream, args.adjoint, args.fd_directions) if args.adjoint > 0 else None
 
@@ -617,11 +655,7 @@ def main():
     ms_e2e = e0.elapsed_time(e1) / args.steps
 
     def reduce_max(v):
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return ranks_reduce(v, "max", dist, f"cuda:{local}")
 
     ms_mx, ms_64, ms_e2e = reduce_max(ms_mx), reduce_max(ms_64), reduce_max(ms_e2e)
     solve_t = {k: reduce_max(v) for k, v in solve_t.items()}
