@@ -196,8 +196,7 @@ struct rsd_heat {
 	int64_t nbElems = 0;
 	double* gPrev = nullptr;        // device: Dirichlet values at the previous time (time-dependent BCs)
 	bool gPrevValid = false;
-	int32_t* slots = nullptr;       // device: element -> CSR position map for K's pattern
-	int32_t slotStride = 0;
+	uint8_t* ranks = nullptr;       // device: element -> column-rank map for K's pattern
 	bool slotsTried = false;
 	// stage scratch
 	double *F = nullptr, *R = nullptr, *Udot = nullptr, *ms = nullptr, *dU = nullptr;
