@@ -19,6 +19,7 @@
 // Geometry follows JacobianTransform (fem/geometry/JacobianTransform.tpp): measure = sqrt(det(J^T J)),
 // 2D gradient transform with the true inverse, 3D with the cofactor/det layout (:160-185).
 #include <cmath>
+#include <vector>
 
 #include "rsd_kernels.cuh"
 
@@ -51,8 +52,9 @@ struct AsmParams {
 	const int32_t* __restrict__ col;
 	const int32_t* __restrict__ sStart;
 	double* __restrict__ val;
-	const int32_t* __restrict__ slots;  // element -> SELL slot map [e][a][b] (row stride slotStride), or null
-	int32_t slotStride;
+	// element -> column-rank map [e][a][b]: the position of column t2a[node_b] within row t2a[node_a]
+	// (0xFF when either DOF is constrained), rows of (NPE rounded up to 8) bytes; or null
+	const uint8_t* __restrict__ ranks;
 	double cDiff, cMass, cTDiff, cTMass;
 	// vectors
 	const double* __restrict__ U;
@@ -230,6 +232,7 @@ __device__ __forceinline__ void node_grad(const double* rec, const double* ta, d
 }
 
 // the warp-uniform element loop shared by every kernel: EPW elements per warp per trip
+// the warp-uniform element loop shared by every kernel: EPW elements per warp per trip
 #define RSD_ELEMENT_LOOP_BEGIN                                                                   \
 	using E = Elem<NSD, P>;                                                                      \
 	constexpr int NPE = E::NPE, G = E::G, EPW = E::EPW;                                           \
@@ -321,15 +324,20 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_matrix(const AsmParams prm)
 			}
 		}
 	}
-	// scatter row a (free rows only) into the SELL-32 values
-	if (prm.slots) {
-		// precomputed positions: one contiguous run of NPE slots per lane, -1 for constrained pairs
-		const int32_t* sl = prm.slots + ((int64_t)e * NPE + a) * prm.slotStride;
+	// scatter row a (free rows only) into the SELL-32 values: entry j of row r sits at
+	// sStart[r / 32] + 32 j + r % 32, and the rank map gives j for each element column
+	if (prm.ranks) {
+		constexpr int RB = (NPE + 7) & ~7;
+		if (has && row >= 0) {
+			const unsigned long long* rk = reinterpret_cast<const unsigned long long*>(prm.ranks + ((int64_t)e * NPE + a) * RB);
+			unsigned long long w[RB / 8];
 #pragma unroll
-		for (int b = 0; b < NPE; ++b) {
-			if (has && row >= 0) {
-				const int32_t s = __ldcs(sl + b);
-				if (s >= 0) atomicAdd(prm.val + s, Ke[b]);
+			for (int k = 0; k < RB / 8; ++k) w[k] = __ldcs(rk + k);
+			double* rowBase = prm.val + prm.sStart[row >> 5] + (row & 31);
+#pragma unroll
+			for (int b = 0; b < NPE; ++b) {
+				const int j = (int)((w[b >> 3] >> (8 * (b & 7))) & 0xFF);
+				if (j != 0xFF) atomicAdd(rowBase + 32 * j, Ke[b]);
 			}
 		}
 	} else {
@@ -351,12 +359,13 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_matrix(const AsmParams prm)
 	RSD_ELEMENT_LOOP_END
 }
 
-// element -> SELL-32 slot map, built once per pattern: slot[e][a][b] = slot of column t2a[node_b]
-// in row t2a[node_a], -1 when either DOF is constrained
+// element -> column-rank map, built once per pattern: rank[e][a][b] = position of column
+// t2a[node_b] within row t2a[node_a] (rows hold at most 254 entries), 0xFF when either DOF is
+// constrained
 template <int NSD, int P>
 __global__ void k_build_slots(int64_t nelem, const int32_t* __restrict__ ien, const int32_t* __restrict__ t2a,
                               const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
-                              const int32_t* __restrict__ sStart, int32_t* __restrict__ slots, int32_t stride) {
+                              uint8_t* __restrict__ ranks, int32_t stride) {
 	using E = Elem<NSD, P>;
 	constexpr int NPE = E::NPE;
 	const int64_t total = nelem * NPE;
@@ -364,10 +373,10 @@ __global__ void k_build_slots(int64_t nelem, const int32_t* __restrict__ ien, co
 		const int64_t e = t / NPE;
 		const int a = (int)(t % NPE);
 		const int32_t row = t2a[ien[e * NPE + a]];
-		int32_t* out = slots + t * stride;
+		uint8_t* out = ranks + t * stride;
 		for (int b = 0; b < NPE; ++b) {
 			const int32_t cb = t2a[ien[e * NPE + b]];
-			int32_t s = -1;
+			int32_t s = 0xFF;
 			if (row >= 0 && cb >= 0) {
 				const int end = rp[row + 1];
 				int lo = rp[row], hi = end;
@@ -375,11 +384,11 @@ __global__ void k_build_slots(int64_t nelem, const int32_t* __restrict__ ien, co
 					const int mid = (lo + hi) >> 1;
 					if (col[mid] < cb) lo = mid + 1; else hi = mid;
 				}
-				if (lo < end && col[lo] == cb) s = sell_slot(sStart, rp, row, lo);
+				if (lo < end && col[lo] == cb) s = lo - rp[row];
 			}
-			out[b] = s;
+			out[b] = (uint8_t)s;
 		}
-		for (int b = NPE; b < stride; ++b) out[b] = -1;
+		for (int b = NPE; b < stride; ++b) out[b] = 0xFF;
 	}
 }
 
@@ -647,26 +656,32 @@ static int launch_k_asm_vector(rsd_ctx* ctx, const rsd_heat* h, const AsmParams&
 	return set_error(RSD_EINVAL, "unsupported element");
 }
 
-// Build the element -> CSR slot map for h's pattern (once).  Skipped, leaving the binary-search
-// scatter, when RSD_SLOT_MAP=0 or when the map would take more than a quarter of free memory.
+// Build the element -> column-rank map for h's pattern (once).  Skipped, leaving the binary-search
+// scatter, when RSD_SLOT_MAP=0, when a row holds more than 254 entries, or when the map would take
+// more than a quarter of free memory.
 static int ensure_slots(rsd_ctx* ctx, rsd_heat* h) {
-	if (h->slots || h->slotsTried) return RSD_OK;
+	if (h->ranks || h->slotsTried) return RSD_OK;
 	h->slotsTried = true;
 	const char* env = getenv("RSD_SLOT_MAP");
 	if (env && env[0] == '0') return RSD_OK;
+	const rsd_csr* K = h->K;
+	// the longest row is the longest slice of the SELL-32 layout
+	std::vector<int32_t> st(K->nslices + 1);
+	RSD_CUDA(cudaMemcpyAsync(st.data(), K->sStart, sizeof(int32_t) * st.size(), cudaMemcpyDeviceToHost, ctx->stream));
+	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+	for (int64_t i = 0; i < K->nslices; ++i)
+		if ((st[i + 1] - st[i]) / 32 > 254) return RSD_OK;
 	const int npe = h->m->npe;
-	const int stride = (npe + 3) & ~3;
-	const size_t bytes = sizeof(int32_t) * (size_t)h->m->nelem * npe * stride;
+	const int stride = (npe + 7) & ~7;
+	const size_t bytes = (size_t)h->m->nelem * npe * stride;
 	size_t freeB = 0, totalB = 0;
 	RSD_CUDA(cudaMemGetInfo(&freeB, &totalB));
 	if (bytes > freeB / 4) return RSD_OK;
-	if (cudaMalloc(&h->slots, bytes) != cudaSuccess) { cudaGetLastError(); h->slots = nullptr; return RSD_OK; }
-	h->slotStride = stride;
+	if (cudaMalloc(&h->ranks, std::max<size_t>(bytes, 8)) != cudaSuccess) { cudaGetLastError(); h->ranks = nullptr; return RSD_OK; }
 	const int64_t total = h->m->nelem * npe;
 	const int blocks = (int)std::min<int64_t>((total + 255) / 256, (int64_t)ctx->num_sms * 8);
 	const int nsd = h->m->nsd, ord = h->m->order;
-	const rsd_csr* K = h->K;
-#define RSD_SLOTS(D, Q) k_build_slots<D, Q><<<std::max(blocks, 1), 256, 0, ctx->stream>>>(h->m->nelem, h->m->ien, h->t2a, K->rowPtr, K->col, K->sStart, h->slots, stride)
+#define RSD_SLOTS(D, Q) k_build_slots<D, Q><<<std::max(blocks, 1), 256, 0, ctx->stream>>>(h->m->nelem, h->m->ien, h->t2a, K->rowPtr, K->col, h->ranks, stride)
 	if (nsd == 2 && ord == 1) RSD_SLOTS(2, 1);
 	else if (nsd == 2 && ord == 2) RSD_SLOTS(2, 2);
 	else if (nsd == 2 && ord == 3) RSD_SLOTS(2, 3);
@@ -684,7 +699,7 @@ int assemble_matrix(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, doubl
 	AsmParams p = params_for(h);
 	p.rp = A->rowPtr; p.col = A->col; p.sStart = A->sStart; p.val = A->sVal;
 	// the slot map indexes h's pattern; another matrix of equal size may differ, so it searches
-	if (A == h->K || A->rowPtr == h->K->rowPtr) { p.slots = h->slots; p.slotStride = h->slotStride; }
+	if (A == h->K || A->rowPtr == h->K->rowPtr) p.ranks = h->ranks;
 	p.cDiff = cDiff; p.cMass = cMass; p.cTDiff = cTDiff; p.cTMass = cTMass;
 	p.U = U; p.Udot = Udot;
 	RSD_CUDA(cudaMemsetAsync(A->sVal, 0, sizeof(double) * std::max<int64_t>(A->ssize, 1), ctx->stream));
