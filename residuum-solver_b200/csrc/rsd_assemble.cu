@@ -27,7 +27,8 @@ namespace rsd {
 
 // SELL-32 slot of CSR position q of row `row`
 __device__ __forceinline__ int32_t sell_slot(const int32_t* sStart, const int32_t* rp, int32_t row, int32_t q) {
-	return sStart[row >> 5] + 32 * (q - rp[row]) + (row & 31);
+	const int32_t j = q - rp[row];
+	return sStart[row >> 5] + 64 * (j >> 1) + 2 * (row & 31) + (j & 1);
 }
 
 struct AsmParams {
@@ -325,7 +326,7 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_matrix(const AsmParams prm)
 		}
 	}
 	// scatter row a (free rows only) into the SELL-32 values: entry j of row r sits at
-	// sStart[r / 32] + 32 j + r % 32, and the rank map gives j for each element column
+	// sStart[r / 32] + 64 (j / 2) + 2 (r % 32) + j % 2, and the rank map gives j for each element column
 	if (prm.ranks) {
 		constexpr int RB = (NPE + 7) & ~7;
 		if (has && row >= 0) {
@@ -333,11 +334,11 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_matrix(const AsmParams prm)
 			unsigned long long w[RB / 8];
 #pragma unroll
 			for (int k = 0; k < RB / 8; ++k) w[k] = __ldcs(rk + k);
-			double* rowBase = prm.val + prm.sStart[row >> 5] + (row & 31);
+			double* rowBase = prm.val + prm.sStart[row >> 5] + 2 * (row & 31);
 #pragma unroll
 			for (int b = 0; b < NPE; ++b) {
 				const int j = (int)((w[b >> 3] >> (8 * (b & 7))) & 0xFF);
-				if (j != 0xFF) atomicAdd(rowBase + 32 * j, Ke[b]);
+				if (j != 0xFF) atomicAdd(rowBase + 64 * (j >> 1) + (j & 1), Ke[b]);
 			}
 		}
 	} else {

@@ -247,14 +247,17 @@ static int upload_csr(rsd_ctx* ctx, int64_t n, const std::vector<int32_t>& rp, c
 	A->nnz = nnz;
 	std::vector<int32_t> d(n);
 	diag_index(n, rp.data(), col.data(), d.data());
-	// SELL-32 layout: slice s holds rows 32s..32s+31, padded to its longest row
+	// SELL-32 layout: slice s holds rows 32s..32s+31, padded to its longest row rounded up to even;
+	// entries are stored in pairs, entry j of lane l at start[s] + 64 (j / 2) + 2 l + (j % 2), so that a
+	// lane reads two consecutive entries of its row with one 8- or 16-byte load
 	const int64_t ns = (n + 31) / 32;
 	std::vector<int64_t> start(ns + 1, 0);
 	for (int64_t s = 0; s < ns; ++s) {
 		int32_t len = 0;
 		for (int64_t i = 32 * s; i < std::min<int64_t>(n, 32 * s + 32); ++i) len = std::max(len, rp[i + 1] - rp[i]);
-		start[s + 1] = start[s] + 32 * (int64_t)len;
+		start[s + 1] = start[s] + 32 * (int64_t)((len + 1) & ~1);
 	}
+	auto pos = [&](int64_t s, int64_t l, int64_t j) { return start[s] + 64 * (j >> 1) + 2 * l + (j & 1); };
 	const int64_t ssize = start[ns];
 	if (ssize > INT32_MAX) { delete A; return set_error(RSD_EINVAL, "padded SELL layout has 2^31 or more slots"); }
 	std::vector<int32_t> sStart(ns + 1), sCol(std::max<int64_t>(ssize, 1)), sSrc(std::max<int64_t>(ssize, 1), -1), sDiag(std::max<int64_t>(n, 1), -1);
@@ -271,13 +274,13 @@ static int upload_csr(rsd_ctx* ctx, int64_t n, const std::vector<int32_t>& rp, c
 				const int64_t i = r0 + l;
 				const int32_t pad = i < n ? (rp[i] < rp[i + 1] ? col[rp[i + 1] - 1] : (int32_t)i) : pad0;
 				for (int64_t j = 0; j < len; ++j) {
-					const int64_t slot = start[s] + 32 * j + l;
+					const int64_t slot = pos(s, l, j);
 					if (i < n && rp[i] + j < rp[i + 1]) { sCol[slot] = col[rp[i] + j]; sSrc[slot] = (int32_t)(rp[i] + j); }
 					else sCol[slot] = pad;
 					lo = std::min(lo, sCol[slot]);
 					hi = std::max(hi, sCol[slot]);
 				}
-				if (i < n && d[i] >= 0) sDiag[i] = (int32_t)(start[s] + 32 * (d[i] - rp[i]) + l);
+				if (i < n && d[i] >= 0) sDiag[i] = (int32_t)pos(s, l, d[i] - rp[i]);
 			}
 			sMin[s] = len ? lo : 0;
 			sMax[s] = len ? hi : 0;
@@ -290,17 +293,19 @@ static int upload_csr(rsd_ctx* ctx, int64_t n, const std::vector<int32_t>& rp, c
 		std::vector<std::vector<int32_t>> pat(ns);
 		parallel_for(ns, [&](int64_t b, int64_t e) {
 			for (int64_t s = b; s < e; ++s) {
-				const int64_t r0 = 32 * s, len = (start[s + 1] - start[s]) / 32;
-				if (r0 + 32 > n || len == 0) continue;
-				bool uni = true;
+				const int64_t r0 = 32 * s, len2 = (start[s + 1] - start[s]) / 32;
+				if (r0 + 32 > n || len2 == 0) continue;
+				const int64_t len = rp[r0 + 1] - rp[r0];
+				bool uni = len > 0;
 				for (int64_t l = 0; l < 32 && uni; ++l) uni = rp[r0 + l + 1] - rp[r0 + l] == len;
 				for (int64_t j = 0; j < len && uni; ++j) {
 					const int32_t off = col[rp[r0] + j] - (int32_t)r0;
 					for (int64_t l = 1; l < 32 && uni; ++l) uni = col[rp[r0 + l] + j] - (int32_t)(r0 + l) == off;
 				}
 				if (!uni) continue;
-				pat[s].resize(len);
-				for (int64_t j = 0; j < len; ++j) pat[s][j] = col[rp[r0] + j] - (int32_t)r0;
+				// the pattern covers the padded length; a padding entry repeats the last column
+				pat[s].resize(len2);
+				for (int64_t j = 0; j < len2; ++j) pat[s][j] = col[rp[r0] + std::min(j, len - 1)] - (int32_t)r0;
 			}
 		});
 		std::map<std::vector<int32_t>, int32_t> seen;

@@ -85,10 +85,11 @@ int prof_flush(rsd_ctx* ctx);   // fold recorded pairs into the totals (synchron
 }  // namespace rsd
 
 // A CSR matrix (the API's storage, CSRMatrix's layout with 32-bit indices) plus its SELL-32
-// execution layout: rows in slices of 32, each slice stored column-major and padded to its
-// longest row, so that a warp's loads of values and columns are contiguous and consecutive rows'
-// gathers of x are neighbours.  Entry j of row i lives at sStart[i/32] + 32 j + i%32; padding has
-// value 0 and the row's own column.  Values may be current in either layout (csrValid/sellValid).
+// execution layout: rows in slices of 32, each slice padded to its longest row rounded up to even
+// and stored as column-major pairs, so that each lane reads two consecutive entries of its row in
+// one load, a warp's loads are contiguous and consecutive rows' gathers of x are neighbours.  Entry
+// j of row i lives at sStart[i/32] + 64 (j/2) + 2 (i%32) + j%2; padding has value 0 and repeats a
+// column of the row.  Values may be current in either layout (csrValid/sellValid).
 struct rsd_csr {
 	int64_t n = 0, nnz = 0;
 	int32_t* rowPtr = nullptr;     // n+1

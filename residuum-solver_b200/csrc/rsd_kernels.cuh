@@ -48,6 +48,27 @@ __device__ __forceinline__ uint16_t ldh(const uint16_t* a, uint64_t pol) {
 	asm volatile("ld.global.nc.L2::cache_hint.u16 %0, [%1], %2;" : "=h"(v) : "l"(a), "l"(pol));
 	return v;
 }
+__device__ __forceinline__ uint32_t ldh(const uint32_t* a, uint64_t pol) {
+	uint32_t v;
+	asm volatile("ld.global.nc.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
+	return v;
+}
+// pairs of consecutive entries (8- or 16-byte aligned)
+__device__ __forceinline__ float2 ldh2(const float* a, uint64_t pol) {
+	float2 v;
+	asm volatile("ld.global.nc.L2::cache_hint.v2.f32 {%0,%1}, [%2], %3;" : "=f"(v.x), "=f"(v.y) : "l"(a), "l"(pol));
+	return v;
+}
+__device__ __forceinline__ double2 ldh2(const double* a, uint64_t pol) {
+	double2 v;
+	asm volatile("ld.global.nc.L2::cache_hint.v2.f64 {%0,%1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(a), "l"(pol));
+	return v;
+}
+__device__ __forceinline__ int2 ldh2(const int32_t* a, uint64_t pol) {
+	int2 v;
+	asm volatile("ld.global.nc.L2::cache_hint.v2.s32 {%0,%1}, [%2], %3;" : "=r"(v.x), "=r"(v.y) : "l"(a), "l"(pol));
+	return v;
+}
 __device__ __forceinline__ int32_t ldh(const int32_t* a, uint64_t pol) {
 	int32_t v;
 	asm volatile("ld.global.nc.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
@@ -194,26 +215,37 @@ __device__ __forceinline__ AccT row_sum(const MatView<T>& A, int64_t row, int64_
 	AccT s = AccT(0);
 	if (row < n) {
 		if constexpr (L <= 0) {
-			// the slice's length is the same for the whole warp
+			// the slice's (even) length is the same for the whole warp; a lane reads its row in pairs
+			// of consecutive entries, two pairs at a time (values, columns, then the gathers), and sums
+			// them in row order
 			const int64_t sl = row >> 5;
 			const int s0 = A.ptr[sl];
-			const int len = (A.ptr[sl + 1] - s0) >> 5;
-			const int q0 = s0 + (int)(row & 31);
+			const int npair = (A.ptr[sl + 1] - s0) >> 6;
+			const int q0 = s0 + 2 * (int)(row & 31);
 			const T* __restrict__ vp = A.val + q0;
-			// loads four slots at a time: values, columns, then the gathers; summed in row order
-			auto run = [&](auto colat) {
-				int j = 0;
-				for (; j + 4 <= len; j += 4) {
-					const T v0 = ldh(vp + 32 * j, pol.first), v1 = ldh(vp + 32 * (j + 1), pol.first);
-					const T v2 = ldh(vp + 32 * (j + 2), pol.first), v3 = ldh(vp + 32 * (j + 3), pol.first);
-					const int c0 = colat(j), c1 = colat(j + 1), c2 = colat(j + 2), c3 = colat(j + 3);
-					const AccT x0 = xf(c0), x1 = xf(c1), x2 = xf(c2), x3 = xf(c3);
-					s += (AccT)v0 * x0;
-					s += (AccT)v1 * x1;
-					s += (AccT)v2 * x2;
-					s += (AccT)v3 * x3;
+			auto run = [&](auto colpair) {
+				int jp = 0;
+				// FP32 rows take two pairs per step; FP64 pairs are already 16-byte loads, and a second
+				// pair in flight would spill under the SpMV kernels' 32-register budget
+				constexpr int kStep = sizeof(T) == 4 ? 2 : 1;
+				if constexpr (kStep == 2) {
+					for (; jp + 2 <= npair; jp += 2) {
+						const auto va = ldh2(vp + 64 * jp, pol.first), vb = ldh2(vp + 64 * (jp + 1), pol.first);
+						const int2 ca = colpair(jp), cb = colpair(jp + 1);
+						const AccT x0 = xf(ca.x), x1 = xf(ca.y), x2 = xf(cb.x), x3 = xf(cb.y);
+						s += (AccT)va.x * x0;
+						s += (AccT)va.y * x1;
+						s += (AccT)vb.x * x2;
+						s += (AccT)vb.y * x3;
+					}
 				}
-				for (; j < len; ++j) s += (AccT)ldh(vp + 32 * j, pol.first) * xf(colat(j));
+				for (; jp < npair; ++jp) {
+					const auto va = ldh2(vp + 64 * jp, pol.first);
+					const int2 ca = colpair(jp);
+					const AccT x0 = xf(ca.x), x1 = xf(ca.y);
+					s += (AccT)va.x * x0;
+					s += (AccT)va.y * x1;
+				}
 			};
 			// a stencil slice (the branch is uniform over the warp, which holds the slice): the column
 			// of entry j is row + offset j, read once per warp from the shared pattern
@@ -221,14 +253,20 @@ __device__ __forceinline__ AccT row_sum(const MatView<T>& A, int64_t row, int64_
 			if (u >= 0) {
 				const int32_t* __restrict__ op = A.offs + u;
 				const int r = (int)row;
-				run([&](int j) { return r + ldh(op + j, pol.last); });
+				run([&](int jp) {
+					const int2 o = ldh2(op + 2 * jp, pol.last);
+					return make_int2(r + o.x, r + o.y);
+				});
 			} else if constexpr (L < 0) {
 				const int cb = A.base[sl];
 				const uint16_t* __restrict__ cp16 = A.col16 + q0;
-				run([&](int j) { return cb + (int)ldh(cp16 + 32 * j, pol.first); });
+				run([&](int jp) {
+					const uint32_t w = ldh(reinterpret_cast<const uint32_t*>(cp16 + 64 * jp), pol.first);
+					return make_int2(cb + (int)(w & 0xFFFFu), cb + (int)(w >> 16));
+				});
 			} else {
 				const int32_t* __restrict__ cp32 = A.col + q0;
-				run([&](int j) { return ldh(cp32 + 32 * j, pol.first); });
+				run([&](int jp) { return ldh2(cp32 + 64 * jp, pol.first); });
 			}
 		} else {
 			const int e = A.ptr[row + 1];
