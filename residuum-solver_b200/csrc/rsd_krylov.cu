@@ -30,7 +30,7 @@ struct CgScal {
 	double rz, pAp, alpha, beta, res0, res, rel, rmax, res64, trueRel;
 	double dcur;                      // mixed: current replacement threshold
 	int64_t iter;
-	int32_t refinements, done, converged, reliable, apply_xy, status, pad;
+	int32_t refinements, done, converged, reliable, status, pad0, pad;
 	unsigned ticket;
 };
 static_assert(sizeof(CgScal) <= sizeof(DevScalars), "CgScal must fit a DevScalars slot");
@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(256) k_cg_init(int64_t n, MatView<double> A, c
 	if (grid_sum<2>(v, partials, &S->ticket)) {
 		const double res0 = sqrt(v[0]);
 		S->res0 = res0; S->rz = v[1]; S->iter = 0; S->res = res0; S->rel = 1.0;
-		S->refinements = 0; S->reliable = 0; S->apply_xy = 0; S->status = 0;
+		S->refinements = 0; S->reliable = 0; S->status = 0;
 		const double crit = relMode ? res0 / (res0 + 1e-50) : res0;
 		if (crit < tol) { S->done = 1; S->converged = 1; }
 		else if (maxIters <= 1) { S->done = 1; S->converged = 0; S->iter = maxIters; S->rel = res0 / (res0 + 1e-50); }
@@ -184,9 +184,9 @@ __global__ void __launch_bounds__(kVT) k_cg_pupdate(int64_t n, double* __restric
 
 // ---- mixed precision PCG: FP32 matrix, vectors and recurrence; FP64 x, reductions and residual
 // replacement (reliable updates, Sleijpen & van der Vorst 1996): whenever the FP32 recurrence
-// residual drops by `delta` since the last replacement, or claims convergence, the true residual
-// r = b - A64 (x + y) is recomputed in FP64 and replaces the recurrence residual; the FP32
-// correction y is folded into x.  Convergence is declared on the FP64 residual only.
+// residual drops by `delta` since the last replacement, or claims convergence, the FP32
+// correction y is folded into x (x += y, y = 0) and the true residual r = b - A64 x is recomputed
+// in FP64 to replace the recurrence residual.  Convergence is declared on the FP64 residual only.
 // r0 = b - A64 x in FP64
 template <int L>
 __global__ void __launch_bounds__(256) k_mx_init(int64_t n, MatView<double> A, const double* __restrict__ b,
@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(256) k_mx_init(int64_t n, MatView<double> A, c
 	if (grid_sum<2>(v, partials, &S->ticket)) {
 		const double res0 = sqrt(v[0]);
 		S->res0 = res0; S->rmax = res0; S->res = res0; S->res64 = res0; S->rel = 1.0; S->trueRel = 1.0;
-		S->rz = v[1]; S->iter = 0; S->refinements = 0; S->reliable = 0; S->apply_xy = 0; S->status = 0;
+		S->rz = v[1]; S->iter = 0; S->refinements = 0; S->reliable = 0; S->status = 0;
 		S->dcur = delta;
 		const double crit = relMode ? res0 / (res0 + 1e-50) : res0;
 		if (crit < tol) { S->done = 1; S->converged = 1; }
@@ -224,7 +224,7 @@ template <int L>
 __global__ void __launch_bounds__(kST, 2048 / kST) k_mx_spmv_dot(int64_t n, MatView<float> A, const float* __restrict__ p,
                                                      float* __restrict__ Ap, CgScal* S, double* partials) {
 	if (is_done(S)) return;
-	if (blockIdx.x == 0 && threadIdx.x == 0) { S->reliable = 0; S->apply_xy = 0; }
+	if (blockIdx.x == 0 && threadIdx.x == 0) S->reliable = 0;
 	const L2Pol pol = make_l2pol();
 	const RowLoop<L> rl;
 	double v[1] = {0.0};
@@ -288,22 +288,32 @@ __global__ void __launch_bounds__(kVT) k_mx_update(int64_t n, float* __restrict_
 	}
 }
 
-// reliable update: r64 = b - A64 (x + y), r = (float) r64, rz with the new r
+// before a replacement: fold the FP32 correction into the FP64 iterate, x += y, y = 0
+__global__ void __launch_bounds__(kVT) k_mx_fold(int64_t n, double* __restrict__ x, float* __restrict__ y, const CgScal* S) {
+	if (is_done(S) || !*((volatile const int32_t*)&S->reliable)) return;
+	const L2Pol pol = make_l2pol();
+	const uint64_t h = pol.last;
+	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+		sth(x + i, ldh_rw(x + i, h) + (double)ldh_rw(y + i, h), h);
+		sth(y + i, 0.0f, h);
+	}
+}
+
+// reliable update (after the fold): r64 = b - A64 x, r = (float) r64, rz with the new r
 template <int L>
-__global__ void __launch_bounds__(256) k_mx_reliable(int64_t n, MatView<double> A, const double* __restrict__ b,
-                                                     const double* __restrict__ x, const float* __restrict__ y,
-                                                     float* __restrict__ r, const float* __restrict__ invD, CgScal* S,
-                                                     double* partials, double tol, int relMode, int64_t maxIters, int adaptive) {
+__global__ void __launch_bounds__(kST, 2048 / kST) k_mx_reliable(int64_t n, MatView<double> A, const double* __restrict__ b,
+                                                     const double* __restrict__ x, float* __restrict__ r,
+                                                     const float* __restrict__ invD, CgScal* S, double* partials,
+                                                     double tol, int relMode, int64_t maxIters, int adaptive) {
 	if (is_done(S) || !*((volatile const int32_t*)&S->reliable)) return;
 	const L2Pol pol = make_l2pol();
 	const RowLoop<L> rl;
 	double v[2] = {0.0, 0.0};
 	for (int64_t base = rl.base; base < n; base += rl.step) {
 		const int64_t row = base + rl.sub;
-		const double s = row_sum<L, double, double>(A, row, n, rl.lane, pol,
-		                                            [&](int c) { return ldh(x + c, pol.last) + (double)ldh(y + c, pol.last); });
+		const double ax = row_dot<L, double, double>(A, x, row, n, rl.lane, pol);
 		if (rl.lane == 0 && row < n) {
-			const double r64 = ldh(b + row, pol.first) - s;
+			const double r64 = ldh(b + row, pol.first) - ax;
 			const float ri = (float)r64;
 			const float zi = invD ? ri * ldh(invD + row, pol.last) : ri;
 			sth(r + row, ri, pol.last);
@@ -317,7 +327,6 @@ __global__ void __launch_bounds__(256) k_mx_reliable(int64_t n, MatView<double> 
 		if (adaptive) S->dcur = next_delta(S->dcur, S->res, res);
 		S->res64 = res; S->trueRel = rel; S->rmax = res; S->res = res; S->rel = rel;
 		S->refinements += 1;
-		S->apply_xy = 1;
 		const double crit = relMode ? rel : res;
 		if (!isfinite(res)) { S->done = 1; S->converged = 0; S->status = RSD_ENAN; }
 		else if (crit < tol) { S->done = 1; S->converged = 1; }
@@ -326,24 +335,14 @@ __global__ void __launch_bounds__(256) k_mx_reliable(int64_t n, MatView<double> 
 	}
 }
 
-// fold y into x after a replacement; p = beta p + z
-__global__ void __launch_bounds__(kVT) k_mx_pupdate(int64_t n, double* __restrict__ x, float* __restrict__ y,
-                                                    float* __restrict__ p, const float* __restrict__ r,
+// p = beta p + z
+__global__ void __launch_bounds__(kVT) k_mx_pupdate(int64_t n, float* __restrict__ p, const float* __restrict__ r,
                                                     const float* __restrict__ invD, CgScal* S, GraphCtl gc) {
 	if (gc.on && blockIdx.x == 0 && threadIdx.x == 0) graph_continue(S, gc);
-	const int apply = *((volatile const int32_t*)&S->apply_xy);
-	const int done = is_done(S);
-	if (!apply && done) return;
+	if (is_done(S)) return;
 	const float beta = (float)S->beta;
 	const L2Pol pol = make_l2pol();
 	const uint64_t h = pol.last;
-	if (apply) {   // after a residual replacement: fold the FP32 correction into the FP64 iterate
-		for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-			sth(x + i, ldh_rw(x + i, h) + (double)ldh_rw(y + i, h), h);
-			sth(y + i, 0.0f, h);
-		}
-	}
-	if (done) return;
 	packet_loop<float>(n, true, [&](int64_t i, int w) {   // the next SpMV gathers p
 		if (w > 1) {
 			Pk<float> P = ldp_rw(p + i, h), R = ldp(r + i, h), D;
@@ -729,12 +728,13 @@ static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const d
 		return RSD_OK;
 	};
 	auto reliable = [&]() -> int {
-		RSD_DISPATCH_L(L, (k_mx_reliable<LL><<<RG(k_mx_reliable<LL>), 256, 0, st>>>(n, V, b, x, y, r, invD, S, partials, tol, rel, maxIt, adaptive)));
+		k_mx_fold<<<VGB(k_mx_fold, kVT), kVT, 0, st>>>(n, x, y, S);
+		RSD_DISPATCH_L(L, (k_mx_reliable<LL><<<RGB(k_mx_reliable<LL>, kST), kST, 0, st>>>(n, V, b, x, r, invD, S, partials, tol, rel, maxIt, adaptive)));
 		RSD_CUDA(cudaGetLastError());
 		return RSD_OK;
 	};
 	auto body_b = [&](GraphCtl gc) -> int {
-		k_mx_pupdate<<<VGB(k_mx_pupdate, kVT), kVT, 0, st>>>(n, x, y, p, r, invD, S, gc);
+		k_mx_pupdate<<<VGB(k_mx_pupdate, kVT), kVT, 0, st>>>(n, p, r, invD, S, gc);
 		RSD_CUDA(cudaGetLastError());
 		return RSD_OK;
 	};
@@ -773,7 +773,7 @@ static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const d
 				RSD_CHECK(reliable());
 				prof_end(ctx, pq);
 				int pp = prof_begin(ctx, PF_CG_PUPDATE);
-				k_mx_pupdate<<<VGB(k_mx_pupdate, kVT), kVT, 0, st>>>(n, x, y, p, r, invD, S, off);
+				k_mx_pupdate<<<VGB(k_mx_pupdate, kVT), kVT, 0, st>>>(n, p, r, invD, S, off);
 				prof_end(ctx, pp);
 				if (pr >= 0) { pairs.push_back(pr); pairs.push_back(pu); pairs.push_back(pq); pairs.push_back(pp); }
 			}
