@@ -25,9 +25,28 @@
 
 namespace rsd {
 
-// SELL-32 slot of CSR position q of row `row`
-__device__ __forceinline__ int32_t sell_slot(const int32_t* sStart, const int32_t* rp, int32_t row, int32_t q) {
-	const int32_t j = q - rp[row];
+// Position j of CSR entry q (column c) of row `row` in its SELL-32 slice: the rank within the row,
+// or in a stencil slice the index of the offset c - row in the slice's sorted pattern (whose padding
+// repeats the last offset, so the first match is the entry)
+__device__ __forceinline__ int32_t sell_rank(const int32_t* sStart, const int32_t* sUni, const int32_t* sOffs,
+                                             const int32_t* rp, int32_t row, int32_t q, int32_t c) {
+	const int32_t sl = row >> 5;
+	const int32_t u = sUni ? sUni[sl] : -1;
+	if (u < 0) return q - rp[row];
+	const int32_t* pat = sOffs + u;
+	const int32_t off = c - row;
+	int lo = 0, hi = (sStart[sl + 1] - sStart[sl]) >> 5;
+	while (lo < hi) {
+		const int mid = (lo + hi) >> 1;
+		if (pat[mid] < off) lo = mid + 1; else hi = mid;
+	}
+	return lo;
+}
+
+// SELL-32 slot of CSR entry q (column c) of row `row`
+__device__ __forceinline__ int32_t sell_slot(const int32_t* sStart, const int32_t* sUni, const int32_t* sOffs,
+                                             const int32_t* rp, int32_t row, int32_t q, int32_t c) {
+	const int32_t j = sell_rank(sStart, sUni, sOffs, rp, row, q, c);
 	return sStart[row >> 5] + 64 * (j >> 1) + 2 * (row & 31) + (j & 1);
 }
 
@@ -52,9 +71,11 @@ struct AsmParams {
 	const int32_t* __restrict__ rp;
 	const int32_t* __restrict__ col;
 	const int32_t* __restrict__ sStart;
+	const int32_t* __restrict__ sUni;   // stencil slices (pattern start per slice, -1 for none), or null
+	const int32_t* __restrict__ sOffs;
 	double* __restrict__ val;
-	// element -> column-rank map [e][a][b]: the position of column t2a[node_b] within row t2a[node_a]
-	// (0xFF when either DOF is constrained), rows of (NPE rounded up to 8) bytes; or null
+	// element -> column-rank map [e][a][b]: the SELL-32 position j (sell_rank) of column t2a[node_b] in
+	// row t2a[node_a] (0xFF when either DOF is constrained), rows of (NPE rounded up to 8) bytes; or null
 	const uint8_t* __restrict__ ranks;
 	double cDiff, cMass, cTDiff, cTMass;
 	// vectors
@@ -353,7 +374,8 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_matrix(const AsmParams prm)
 					const int mid = (lo + hi) >> 1;
 					if (prm.col[mid] < cb) lo = mid + 1; else hi = mid;
 				}
-				if (lo < end && prm.col[lo] == cb) atomicAdd(prm.val + sell_slot(prm.sStart, prm.rp, row, lo), Ke[b]);
+				if (lo < end && prm.col[lo] == cb)
+					atomicAdd(prm.val + sell_slot(prm.sStart, prm.sUni, prm.sOffs, prm.rp, row, lo, cb), Ke[b]);
 			}
 		}
 	}
@@ -366,7 +388,8 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_matrix(const AsmParams prm)
 template <int NSD, int P>
 __global__ void k_build_slots(int64_t nelem, const int32_t* __restrict__ ien, const int32_t* __restrict__ t2a,
                               const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
-                              uint8_t* __restrict__ ranks, int32_t stride) {
+                              const int32_t* __restrict__ sStart, const int32_t* __restrict__ sUni,
+                              const int32_t* __restrict__ sOffs, uint8_t* __restrict__ ranks, int32_t stride) {
 	using E = Elem<NSD, P>;
 	constexpr int NPE = E::NPE;
 	const int64_t total = nelem * NPE;
@@ -385,7 +408,7 @@ __global__ void k_build_slots(int64_t nelem, const int32_t* __restrict__ ien, co
 					const int mid = (lo + hi) >> 1;
 					if (col[mid] < cb) lo = mid + 1; else hi = mid;
 				}
-				if (lo < end && col[lo] == cb) s = lo - rp[row];
+				if (lo < end && col[lo] == cb) s = sell_rank(sStart, sUni, sOffs, rp, row, lo, cb);
 			}
 			out[b] = (uint8_t)s;
 		}
@@ -682,7 +705,7 @@ static int ensure_slots(rsd_ctx* ctx, rsd_heat* h) {
 	const int64_t total = h->m->nelem * npe;
 	const int blocks = (int)std::min<int64_t>((total + 255) / 256, (int64_t)ctx->num_sms * 8);
 	const int nsd = h->m->nsd, ord = h->m->order;
-#define RSD_SLOTS(D, Q) k_build_slots<D, Q><<<std::max(blocks, 1), 256, 0, ctx->stream>>>(h->m->nelem, h->m->ien, h->t2a, K->rowPtr, K->col, h->ranks, stride)
+#define RSD_SLOTS(D, Q) k_build_slots<D, Q><<<std::max(blocks, 1), 256, 0, ctx->stream>>>(h->m->nelem, h->m->ien, h->t2a, K->rowPtr, K->col, K->sStart, K->sUni, K->sOffs, h->ranks, stride)
 	if (nsd == 2 && ord == 1) RSD_SLOTS(2, 1);
 	else if (nsd == 2 && ord == 2) RSD_SLOTS(2, 2);
 	else if (nsd == 2 && ord == 3) RSD_SLOTS(2, 3);
@@ -698,7 +721,7 @@ int assemble_matrix(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, doubl
 	if (A->n != h->n || A->nnz != h->K->nnz) return set_error(RSD_EINVAL, "matrix does not have the problem's pattern");
 	RSD_CHECK(ensure_slots(ctx, h));
 	AsmParams p = params_for(h);
-	p.rp = A->rowPtr; p.col = A->col; p.sStart = A->sStart; p.val = A->sVal;
+	p.rp = A->rowPtr; p.col = A->col; p.sStart = A->sStart; p.sUni = A->sUni; p.sOffs = A->sOffs; p.val = A->sVal;
 	// the slot map indexes h's pattern; another matrix of equal size may differ, so it searches
 	if (A == h->K || A->rowPtr == h->K->rowPtr) p.ranks = h->ranks;
 	p.cDiff = cDiff; p.cMass = cMass; p.cTDiff = cTDiff; p.cTMass = cTMass;

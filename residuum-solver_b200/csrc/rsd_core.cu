@@ -286,26 +286,34 @@ static int upload_csr(rsd_ctx* ctx, int64_t n, const std::vector<int32_t>& rp, c
 			sMax[s] = len ? hi : 0;
 		}
 	});
-	// stencil slices: a full slice whose 32 rows have the same length and the same column offsets
-	// (column - row) stores that pattern once, in a table of distinct patterns
+	// stencil slices: a full slice whose rows' column offsets (column - row) all belong to one sorted
+	// pattern no longer than the slice's padded length stores that pattern once.  Entry j of every row
+	// of the slice is then the pattern's offset j: a row without that column holds a zero there (its
+	// column row + offset must lie in [0, n), so that the gather stays in range), and the padding
+	// repeats the last offset.  Rows that differ only by missing neighbours (the ends of grid lines)
+	// thus share the slice pattern, and the slice reads no column bytes.
 	std::vector<int32_t> sUni(std::max<int64_t>(ns, 1), -1), offTable;
 	{
 		std::vector<std::vector<int32_t>> pat(ns);
 		parallel_for(ns, [&](int64_t b, int64_t e) {
+			std::vector<int32_t> u;
 			for (int64_t s = b; s < e; ++s) {
 				const int64_t r0 = 32 * s, len2 = (start[s + 1] - start[s]) / 32;
 				if (r0 + 32 > n || len2 == 0) continue;
-				const int64_t len = rp[r0 + 1] - rp[r0];
-				bool uni = len > 0;
-				for (int64_t l = 0; l < 32 && uni; ++l) uni = rp[r0 + l + 1] - rp[r0 + l] == len;
-				for (int64_t j = 0; j < len && uni; ++j) {
-					const int32_t off = col[rp[r0] + j] - (int32_t)r0;
-					for (int64_t l = 1; l < 32 && uni; ++l) uni = col[rp[r0 + l] + j] - (int32_t)(r0 + l) == off;
-				}
-				if (!uni) continue;
-				// the pattern covers the padded length; a padding entry repeats the last column
-				pat[s].resize(len2);
-				for (int64_t j = 0; j < len2; ++j) pat[s][j] = col[rp[r0] + std::min(j, len - 1)] - (int32_t)r0;
+				u.clear();
+				bool sorted = true;   // rows in increasing column order (the re-lay below matches in order)
+				for (int64_t i = r0; i < r0 + 32; ++i)
+					for (int32_t q = rp[i]; q < rp[i + 1]; ++q) {
+						u.push_back(col[q] - (int32_t)i);
+						sorted = sorted && (q == rp[i] || col[q - 1] < col[q]);
+					}
+				if (!sorted) continue;
+				std::sort(u.begin(), u.end());
+				u.erase(std::unique(u.begin(), u.end()), u.end());
+				if (u.empty() || (int64_t)u.size() > len2) continue;
+				if (r0 + u.front() < 0 || r0 + 31 + (int64_t)u.back() >= n) continue;
+				pat[s] = u;
+				pat[s].resize(len2, u.back());
 			}
 		});
 		std::map<std::vector<int32_t>, int32_t> seen;
@@ -318,6 +326,35 @@ static int upload_csr(rsd_ctx* ctx, int64_t n, const std::vector<int32_t>& rp, c
 			}
 			sUni[s] = it->second;
 		}
+		// re-lay the stencil slices by pattern position (the CSR rank order above holds for the rest)
+		parallel_for(ns, [&](int64_t b, int64_t e) {
+			for (int64_t s = b; s < e; ++s) {
+				if (sUni[s] < 0) continue;
+				const int32_t* off = offTable.data() + sUni[s];
+				const int64_t len = (start[s + 1] - start[s]) / 32;
+				int32_t lo = INT32_MAX, hi = INT32_MIN;
+				for (int64_t l = 0; l < 32; ++l) {
+					const int64_t i = 32 * s + l;
+					int32_t q = rp[i];
+					sDiag[i] = -1;
+					for (int64_t j = 0; j < len; ++j) {
+						const int64_t slot = pos(s, l, j);
+						const int32_t c = (int32_t)i + off[j];
+						sCol[slot] = c;
+						sSrc[slot] = -1;
+						if (q < rp[i + 1] && col[q] == c) {
+							sSrc[slot] = q;
+							if (q == d[i]) sDiag[i] = (int32_t)slot;
+							++q;
+						}
+						lo = std::min(lo, c);
+						hi = std::max(hi, c);
+					}
+				}
+				sMin[s] = lo;
+				sMax[s] = hi;
+			}
+		});
 	}
 	const bool stencil = !offTable.empty();
 	// 16-bit columns: every slice's columns within 65,535 of the slice's smallest one

@@ -340,10 +340,50 @@ def test_larger_case_against_restatement(rsd, ctx):
     orp, ocol = o.pattern()
     assert (rp == orp).all() and (col == ocol).all()
     h.assemble_matrix(1.0, 1000.0)
-    assert relerr(h.K.values(), o.assemble_matrix(1.0, 1000.0)) <= REL
+    v = o.assemble_matrix(1.0, 1000.0)
+    assert relerr(h.K.values(), v) <= REL
     F = ctx.array(h.n)
     h.assemble_vector(0, F)
     assert relerr(F.download(), o.assemble_vector(0)) <= REL
+    # grid lines of 19 rows: most slices hold a line end, whose rows miss neighbours of the slice's
+    # stencil pattern (zeros in the execution layout); products, diagonal and FP32 copy see none of it
+    x = np.random.default_rng(8).standard_normal(h.n)
+    xd, yd, d = ctx.to_device(x), ctx.array(h.n), ctx.array(h.n)
+    h.K.spmv(xd, yd)
+    assert relerr(yd.download(), oracle.spmv(rp, col, v, x)) <= REL
+    h.K.diagonal(d)
+    vd = h.K.values()
+    assert relerr(d.download(), np.array([vd[rp[i]:rp[i + 1]][col[rp[i]:rp[i + 1]] == i][0] for i in range(h.n)])) == 0.0
+    h.K.sync_f32()
+    x32, y32 = ctx.to_device(x.astype(np.float32)), ctx.array(h.n, np.float32)
+    h.K.spmv_f32(x32, y32)
+    assert relerr(y32.download(), oracle.spmv(rp, col, v, x)) <= 1e-5
+
+
+@pytest.mark.parametrize("nx,ny", [(50, 37), (32, 8), (7, 40)])
+def test_spmv_grid_with_line_ends(rsd, ctx, nx, ny):
+    # 9-point stencil on an nx x ny grid with no boundary rows removed: rows at line ends and on the
+    # first and last lines miss neighbours, and rows near both ends of the matrix have offsets that
+    # would leave [0, n) -- the layout must keep those slices apart
+    n = nx * ny
+    rows = []
+    for j in range(ny):
+        for i in range(nx):
+            rows.append(sorted((j + b) * nx + (i + a) for b in (-1, 0, 1) for a in (-1, 0, 1)
+                               if 0 <= i + a < nx and 0 <= j + b < ny))
+    rp = np.zeros(n + 1, np.int64)
+    rp[1:] = np.cumsum([len(r) for r in rows])
+    col = np.concatenate(rows).astype(np.int64)
+    val = np.random.default_rng(nx).standard_normal(len(col))
+    A = rsd.CSR.from_host(ctx, rp, col, val)
+    x = np.random.default_rng(ny).standard_normal(n)
+    xd, yd = ctx.to_device(x), ctx.array(n)
+    A.spmv(xd, yd)
+    assert relerr(yd.download(), oracle.spmv(rp, col, val, x)) <= 1e-13
+    assert relerr(A.values(), val) == 0.0
+    A.set_values(2.0 * val)
+    A.spmv(xd, yd)
+    assert relerr(yd.download(), oracle.spmv(rp, col, 2.0 * val, x)) <= 1e-13
 
 
 def test_size_independent_properties_at_scale(rsd, ctx):
