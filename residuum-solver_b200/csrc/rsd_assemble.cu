@@ -77,6 +77,11 @@ struct AsmParams {
 	// element -> column-rank map [e][a][b]: the SELL-32 position j (sell_rank) of column t2a[node_b] in
 	// row t2a[node_a] (0xFF when either DOF is constrained), rows of (NPE rounded up to 8) bytes; or null
 	const uint8_t* __restrict__ ranks;
+	// affine fast path (launch-uniform `fast`): per-element flags and the reference integrals
+	int32_t fast;
+	const uint8_t* __restrict__ affine;
+	const double* __restrict__ geo;     // per affine element: the 6 coefficients of the tables, |J|, 0
+	const double* __restrict__ ktab;
 	double cDiff, cMass, cTDiff, cTMass;
 	// vectors
 	const double* __restrict__ U;
@@ -105,11 +110,16 @@ constexpr int N_X = 0, N_U = 3, N_V = 4, N_W = 5, NREC = 6;
 __host__ __device__ inline int table_stride(int G) { return G * 4 + 1; }                      // odd: no bank conflicts across q
 __host__ __device__ inline int node_area(int npe) { return npe * NREC + 1; }
 __host__ __device__ inline int point_area(int nq) { return nq * REC + 1; }
+// reference-integral tables of the affine path: NT gradient-product tables and the mass table, rows
+// of npe entries padded to an odd stride (a group's lanes read distinct rows without bank conflicts)
+__host__ __device__ inline int ktab_count(int nsd) { return nsd == 3 ? 7 : 4; }
+__host__ __device__ inline int ktab_stride(int npe) { return npe | 1; }
 
-size_t asm_smem_bytes(int npe, int nq) {
+size_t asm_smem_bytes(int npe, int nq, int nsd, bool fast) {
 	const int G = npe <= 4 ? 4 : npe <= 8 ? 8 : npe <= 16 ? 16 : 32;
 	const int EPW = 32 / G;
-	return sizeof(double) * ((size_t)nq * table_stride(G) + nq + (size_t)kAsmWarps * EPW * (node_area(npe) + point_area(nq)));
+	const size_t kt = fast ? (size_t)ktab_count(nsd) * npe * ktab_stride(npe) : 0;
+	return sizeof(double) * ((size_t)nq * table_stride(G) + nq + (size_t)kAsmWarps * EPW * (node_area(npe) + point_area(nq)) + kt);
 }
 
 // what phase 2 must evaluate
@@ -130,6 +140,42 @@ __device__ __forceinline__ void stage_tables(const AsmParams& prm, double* sm) {
 	}
 	for (int i = threadIdx.x; i < prm.nq; i += blockDim.x) sm[prm.nq * TS + i] = prm.tables[prm.nq * E::G * 4 + i];
 	__syncthreads();
+}
+
+// Geometry of one point from its Jacobian J[i * NSD + al] = dx_i/dxi_al: returns det(J^T J) (the
+// squared measure) and, when INV, the inverse layout inv[i * NSD + al] = (J^-T)_{i al}.
+template <int NSD, bool INV>
+__device__ __forceinline__ double jac_geom(const double (&J)[9], double (&inv)[9]) {
+	double detg;
+	if (NSD == 2) {
+		const double g0 = J[0] * J[0] + J[2] * J[2], g1 = J[0] * J[1] + J[2] * J[3], g3 = J[1] * J[1] + J[3] * J[3];
+		detg = g0 * g3 - g1 * g1;
+		if (INV) {
+			const double di = 1.0 / (J[0] * J[3] - J[1] * J[2]);
+			inv[0] = di * J[3]; inv[1] = -di * J[1]; inv[2] = -di * J[2]; inv[3] = di * J[0];
+		}
+	} else {
+		double gm[9];
+#pragma unroll
+		for (int b = 0; b < 3; ++b)
+#pragma unroll
+			for (int a = 0; a < 3; ++a) gm[b * 3 + a] = J[a] * J[b] + J[3 + a] * J[3 + b] + J[6 + a] * J[6 + b];
+		detg = gm[0] * (gm[4] * gm[8] - gm[5] * gm[7]) - gm[1] * (gm[3] * gm[8] - gm[5] * gm[6]) + gm[2] * (gm[3] * gm[7] - gm[4] * gm[6]);
+		if (INV) {
+			const double detJ = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) + J[2] * (J[3] * J[7] - J[4] * J[6]);
+			const double di = 1.0 / detJ;
+			inv[0] = di * (J[4] * J[8] - J[5] * J[7]);
+			inv[1] = -di * (J[3] * J[8] - J[5] * J[6]);
+			inv[2] = di * (J[3] * J[7] - J[4] * J[6]);
+			inv[3] = -di * (J[1] * J[8] - J[2] * J[7]);
+			inv[4] = di * (J[0] * J[8] - J[2] * J[6]);
+			inv[5] = -di * (J[0] * J[7] - J[1] * J[6]);
+			inv[6] = di * (J[1] * J[5] - J[2] * J[4]);
+			inv[7] = -di * (J[0] * J[5] - J[2] * J[3]);
+			inv[8] = di * (J[0] * J[4] - J[1] * J[3]);
+		}
+	}
+	return detg;
 }
 
 // phase 2: one quadrature point, all inputs from the staged node data.  GRAD = false (mass and load
@@ -167,48 +213,16 @@ __device__ __forceinline__ void eval_point(const AsmParams& prm, const Needs& nd
 #pragma unroll
 			for (int i = 0; i < NSD; ++i) xq[i] += t[0] * nb[N_X + i];
 	}
-	double inv[9], detg;
-	if (NSD == 2) {
-		const double g0 = J[0] * J[0] + J[2] * J[2], g1 = J[0] * J[1] + J[2] * J[3], g3 = J[1] * J[1] + J[3] * J[3];
-		detg = g0 * g3 - g1 * g1;
-		if (!GRAD) {
-			rec[R_WM] = sqrt(detg) * w;
-			if (nd.field) rec[R_V] = Vq;
-			if (nd.field2) rec[R_W] = Wq;
-			rec[R_K] = 0.0;
-			rec[R_DK] = 0.0;
-			if (nd.load) rec[R_F] = prm.srcExpr.n ? eval_expr(prm.srcExpr, prm.time, xq[0], xq[1], 0.0, 0.0) : 0.0;
-			return;
-		}
-		const double di = 1.0 / (J[0] * J[3] - J[1] * J[2]);
-		inv[0] = di * J[3]; inv[1] = -di * J[1]; inv[2] = -di * J[2]; inv[3] = di * J[0];
-	} else {
-		double gm[9];
-#pragma unroll
-		for (int b = 0; b < 3; ++b)
-#pragma unroll
-			for (int a = 0; a < 3; ++a) gm[b * 3 + a] = J[a] * J[b] + J[3 + a] * J[3 + b] + J[6 + a] * J[6 + b];
-		detg = gm[0] * (gm[4] * gm[8] - gm[5] * gm[7]) - gm[1] * (gm[3] * gm[8] - gm[5] * gm[6]) + gm[2] * (gm[3] * gm[7] - gm[4] * gm[6]);
-		if (!GRAD) {
-			rec[R_WM] = sqrt(detg) * w;
-			if (nd.field) rec[R_V] = Vq;
-			if (nd.field2) rec[R_W] = Wq;
-			rec[R_K] = 0.0;
-			rec[R_DK] = 0.0;
-			if (nd.load) rec[R_F] = prm.srcExpr.n ? eval_expr(prm.srcExpr, prm.time, xq[0], xq[1], xq[2], 0.0) : 0.0;
-			return;
-		}
-		const double detJ = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) + J[2] * (J[3] * J[7] - J[4] * J[6]);
-		const double di = 1.0 / detJ;
-		inv[0] = di * (J[4] * J[8] - J[5] * J[7]);
-		inv[1] = -di * (J[3] * J[8] - J[5] * J[6]);
-		inv[2] = di * (J[3] * J[7] - J[4] * J[6]);
-		inv[3] = -di * (J[1] * J[8] - J[2] * J[7]);
-		inv[4] = di * (J[0] * J[8] - J[2] * J[6]);
-		inv[5] = -di * (J[0] * J[7] - J[1] * J[6]);
-		inv[6] = di * (J[1] * J[5] - J[2] * J[4]);
-		inv[7] = -di * (J[0] * J[5] - J[2] * J[3]);
-		inv[8] = di * (J[0] * J[4] - J[1] * J[3]);
+	double inv[9];
+	const double detg = jac_geom<NSD, GRAD>(J, inv);
+	if (!GRAD) {
+		rec[R_WM] = sqrt(detg) * w;
+		if (nd.field) rec[R_V] = Vq;
+		if (nd.field2) rec[R_W] = Wq;
+		rec[R_K] = 0.0;
+		rec[R_DK] = 0.0;
+		if (nd.load) rec[R_F] = prm.srcExpr.n ? eval_expr(prm.srcExpr, prm.time, xq[0], xq[1], NSD == 3 ? xq[2] : 0.0, 0.0) : 0.0;
+		return;
 	}
 #pragma unroll
 	for (int i = 0; i < NSD * NSD; ++i) rec[R_INV + i] = inv[i];
@@ -253,7 +267,49 @@ __device__ __forceinline__ void node_grad(const double* rec, const double* ta, d
 	}
 }
 
-// the warp-uniform element loop shared by every kernel: EPW elements per warp per trip
+// Affine elements: with J constant, sum_q w_q |J| (J^-T dN_a).(J^-T dN_b) = |J| sum_{al,be} C_{al be}
+// S^{al be}_ab with C = J^-1 J^-T and S the reference integrals sum_q w_q dN_a/dxi_al dN_b/dxi_be.
+// C is symmetric, so the tables hold S^{al al} and S^{al be} + S^{be al} (al < be): coefficient k of
+// table k in the order (00, 11, [22,] 01, [02, 12]).
+template <int NSD>
+__device__ __forceinline__ void coefs_from_inv(const double (&inv)[9], double (&c)[6]) {
+	auto C = [&](int al, int be) {
+		double t = 0.0;
+#pragma unroll
+		for (int i = 0; i < NSD; ++i) t += inv[i * NSD + al] * inv[i * NSD + be];
+		return t;
+	};
+	if (NSD == 3) { c[0] = C(0, 0); c[1] = C(1, 1); c[2] = C(2, 2); c[3] = C(0, 1); c[4] = C(0, 2); c[5] = C(1, 2); }
+	else { c[0] = C(0, 0); c[1] = C(1, 1); c[2] = C(0, 1); c[3] = c[4] = c[5] = 0.0; }
+}
+
+// row a of the affine element's gradient form applied to v: sum_k c_k sum_b T_k[a][b] v_b
+template <int NSD, int NPE, int KS>
+__device__ __forceinline__ double affine_grad_row(const double* kt, const double (&c)[6], int a, const double* v, int vstride) {
+	constexpr int NT = NSD == 3 ? 6 : 3;
+	double s = 0.0;
+#pragma unroll
+	for (int k = 0; k < NT; ++k) {
+		const double* row = kt + (k * NPE + a) * KS;
+		double t = 0.0;
+#pragma unroll 9
+		for (int b = 0; b < NPE; ++b) t += row[b] * v[b * vstride];
+		s += c[k] * t;
+	}
+	return s;
+}
+
+// row a of the reference mass matrix applied to v
+template <int NSD, int NPE, int KS>
+__device__ __forceinline__ double affine_mass_row(const double* kt, int a, const double* v, int vstride) {
+	constexpr int NT = NSD == 3 ? 6 : 3;
+	const double* row = kt + (NT * NPE + a) * KS;
+	double t = 0.0;
+#pragma unroll 9
+	for (int b = 0; b < NPE; ++b) t += row[b] * v[b * vstride];
+	return t;
+}
+
 // the warp-uniform element loop shared by every kernel: EPW elements per warp per trip
 #define RSD_ELEMENT_LOOP_BEGIN                                                                   \
 	using E = Elem<NSD, P>;                                                                      \
@@ -269,10 +325,18 @@ __device__ __forceinline__ void node_grad(const double* rec, const double* ta, d
 	double* recs = nodes + node_area(NPE);                                                       \
 	const int64_t warpId = (int64_t)blockIdx.x * kAsmWarps + warp;                               \
 	const int64_t warpStride = (int64_t)gridDim.x * kAsmWarps;                                   \
+	constexpr int KS = NPE | 1;                                                                  \
+	double* kt = sm + prm.nq * TS + prm.nq + (size_t)kAsmWarps * EPW * (node_area(NPE) + point_area(prm.nq)); \
+	if (prm.fast) {                                                                              \
+		for (int i = threadIdx.x; i < ktab_count(NSD) * NPE * NPE; i += blockDim.x)              \
+			kt[(i / NPE) * KS + i % NPE] = prm.ktab[i];                                          \
+		__syncthreads();                                                                         \
+	}                                                                                            \
 	for (int64_t eb = warpId * EPW; eb < prm.nelem; eb += warpStride * EPW) {                    \
 		const int64_t idx = eb + slot;                                                           \
 		const bool inRange = idx < prm.nelem;                                                    \
 		const int64_t e = inRange ? (prm.elist ? (int64_t)prm.elist[idx] : idx) : 0;             \
+		const bool aff = prm.fast && inRange && prm.affine[e];                                   \
 		const bool has = inRange && a < NPE;                                                     \
 		int32_t node = 0, row = -1;                                                              \
 		if (has) {                                                                               \
@@ -284,11 +348,12 @@ __device__ __forceinline__ void node_grad(const double* rec, const double* ta, d
 #define RSD_STAGE_NODE(Uv, Vv, Wv)                                                               \
 		if (has) {                                                                               \
 			double* nb = nodes + a * NREC;                                                       \
-			_Pragma("unroll") for (int i = 0; i < NSD; ++i) nb[N_X + i] = prm.xyz[(int64_t)node * NSD + i]; \
+			if (!aff)   /* an affine element's geometry is precomputed */                        \
+				_Pragma("unroll") for (int i = 0; i < NSD; ++i) nb[N_X + i] = prm.xyz[(int64_t)node * NSD + i]; \
 			nb[N_U] = (Uv); nb[N_V] = (Vv); nb[N_W] = (Wv);                                      \
 		}                                                                                        \
 		__syncwarp();                                                                            \
-		if (inRange)                                                                             \
+		if (!aff && inRange)                                                                     \
 			for (int q = a; q < prm.nq; q += G)                                                  \
 				eval_point<NSD, P, kGrad>(prm, nd, tab + q * TS, wq[q], nodes, ke, recs + q * REC);     \
 		__syncwarp();
@@ -312,7 +377,23 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_matrix(const AsmParams prm)
 	double Ke[NPE];
 #pragma unroll
 	for (int b = 0; b < NPE; ++b) Ke[b] = 0.0;
-	if (has) {
+	if (has && aff) {
+		// c_diff k |J| sum_k c_k T_k + c_mass rho cp |J| M, from the reference integrals
+		const double* gp = prm.geo + e * 8;
+		double c[6];
+#pragma unroll
+		for (int k = 0; k < 6; ++k) c[k] = gp[k];
+		const double cd = prm.cDiff * ke * prm.kConst * gp[6];
+		const double cm = prm.cMass * prm.rho * prm.cp * gp[6];
+		constexpr int NT = NSD == 3 ? 6 : 3;
+#pragma unroll
+		for (int b = 0; b < NPE; ++b) {
+			double g = 0.0;
+#pragma unroll
+			for (int k = 0; k < NT; ++k) g += c[k] * kt[(k * NPE + a) * KS + b];
+			Ke[b] = cd * g + cm * kt[(NT * NPE + a) * KS + b];
+		}
+	} else if (has) {
 		for (int q = 0; q < prm.nq; ++q) {
 			const double* rec = recs + q * REC;
 			const double* tq = tab + q * TS;
@@ -451,7 +532,31 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_vector(const AsmParams prm)
 	}
 	RSD_STAGE_NODE(Ua, Va, Wa)
 	double Fa = 0.0, ge = 0.0;
-	if (has) {
+	if (has && aff) {
+		// reference integrals (no load term and no state here: the host enables this path only then;
+		// without state the conductivity model is evaluated at T = 0, as on the quadrature path)
+		const double* gp = prm.geo + e * 8;
+		const double detJ = gp[6];
+		double kdV = 0.0;
+		if constexpr (kGrad) {
+			double c[6];
+#pragma unroll
+			for (int k = 0; k < 6; ++k) c[k] = gp[k];
+			const double k0 = prm.kExpr.n ? eval_expr(prm.kExpr, 0.0, 0.0, 0.0, 0.0, 0.0) : prm.kConst;
+			kdV = ke * k0 * detJ * affine_grad_row<NSD, NPE, KS>(kt, c, a, nodes + N_V, NREC);
+		}
+		const double massV = prm.rho * prm.cp * detJ * affine_mass_row<NSD, NPE, KS>(kt, a, nodes + N_V, NREC);
+		switch (which) {
+			case 1: Fa = kdV; break;
+			case 2: case 3: Fa = massV; break;
+			case 4: Fa = kdV + prm.coef * massV; break;
+			case 5: Fa = prm.cDiff * kdV + prm.cMass * massV; break;
+			case 7: Fa = prm.coef * massV; break;
+			case 8: Fa = kdV + prm.rho * prm.cp * detJ * affine_mass_row<NSD, NPE, KS>(kt, a, nodes + N_W, NREC); break;
+			case 9: Fa = -kdV; break;
+			default: break;
+		}
+	} else if (has) {
 		for (int q = 0; q < prm.nq; ++q) {
 			const double* rec = recs + q * REC;
 			const double* ta = tab + q * TS + a * 4;
@@ -568,7 +673,7 @@ int build_tables(rsd_heat* h) {
 	double gx[5], gw[5];
 	gauss_legendre(q1, gx, gw);
 	const int nq = nsd == 3 ? q1 * q1 * q1 : q1 * q1;
-	if (asm_smem_bytes(h->m->npe, nq) > 227 * 1024) return set_error(RSD_EINVAL, "too many quadrature points for this element");
+	if (asm_smem_bytes(h->m->npe, nq, nsd, false) > 227 * 1024) return set_error(RSD_EINVAL, "too many quadrature points for this element");
 	std::vector<double> t(nq * G * 4 + nq, 0.0);
 	int q = 0;
 	for (int k = 0; k < (nsd == 3 ? q1 : 1); ++k)
@@ -597,6 +702,114 @@ int build_tables(rsd_heat* h) {
 	if (h->tables) cudaFree(h->tables);
 	RSD_CUDA(cudaMalloc(&h->tables, sizeof(double) * t.size()));
 	RSD_CUDA(cudaMemcpy(h->tables, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice));
+	// reference integrals of the affine path, by the same quadrature: the gradient products
+	// (00, 11, [22,] 01, [02, 12]; off-diagonal pairs symmetrised) and the mass
+	const int npe = h->m->npe, nt = ktab_count(nsd) - 1;
+	const int pairs[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
+	const int pairs2[3][2] = {{0, 0}, {1, 1}, {0, 1}};
+	std::vector<double> kt((size_t)(nt + 1) * npe * npe, 0.0);
+	for (int k = 0; k <= nt; ++k)
+		for (int a = 0; a < npe; ++a)
+			for (int b = 0; b < npe; ++b) {
+				double sum = 0.0;
+				for (int qq = 0; qq < nq; ++qq) {
+					const double w = t[(size_t)nq * G * 4 + qq];
+					const double* ta = &t[((size_t)qq * G + a) * 4];
+					const double* tb = &t[((size_t)qq * G + b) * 4];
+					if (k == nt) { sum += w * ta[0] * tb[0]; continue; }
+					const int al = nsd == 3 ? pairs[k][0] : pairs2[k][0], be = nsd == 3 ? pairs[k][1] : pairs2[k][1];
+					sum += w * ta[1 + al] * tb[1 + be];
+					if (al != be) sum += w * ta[1 + be] * tb[1 + al];
+				}
+				kt[((size_t)k * npe + a) * npe + b] = sum;
+			}
+	if (h->ktab) cudaFree(h->ktab);
+	RSD_CUDA(cudaMalloc(&h->ktab, sizeof(double) * kt.size()));
+	RSD_CUDA(cudaMemcpy(h->ktab, kt.data(), sizeof(double) * kt.size(), cudaMemcpyHostToDevice));
+	return RSD_OK;
+}
+
+// An element is affine when its Jacobian is the same at every quadrature point, to 1e-13 of its
+// largest entry (rounding of the node coordinates stays well below that on regular meshes).
+template <int NSD, int P>
+__global__ void k_affine(int64_t nelem, const int32_t* __restrict__ ien, const double* __restrict__ xyz,
+                         const double* __restrict__ tables, int nq, uint8_t* __restrict__ flag, double* __restrict__ geo,
+                         unsigned* count) {
+	using E = Elem<NSD, P>;
+	constexpr int NPE = E::NPE, G = E::G;
+	const int64_t total = ((nelem + 31) / 32) * 32;
+	for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+		bool ok = false;
+		if (e < nelem) {
+			auto jac = [&](int q, double (&J)[9]) {
+#pragma unroll
+				for (int i = 0; i < 9; ++i) J[i] = 0.0;
+				for (int b = 0; b < NPE; ++b) {
+					const int64_t node = ien[e * NPE + b];
+					const double* t = tables + ((size_t)q * G + b) * 4;
+#pragma unroll
+					for (int i = 0; i < NSD; ++i)
+#pragma unroll
+						for (int al = 0; al < NSD; ++al) J[i * NSD + al] += t[1 + al] * xyz[node * NSD + i];
+				}
+			};
+			double J0[9], Jq[9];
+			jac(0, J0);
+			double jmax = 0.0;
+#pragma unroll
+			for (int i = 0; i < NSD * NSD; ++i) jmax = fmax(jmax, fabs(J0[i]));
+			ok = jmax > 0.0;
+			for (int q = 1; q < nq && ok; ++q) {
+				jac(q, Jq);
+#pragma unroll
+				for (int i = 0; i < NSD * NSD; ++i) ok = ok && fabs(Jq[i] - J0[i]) <= 1e-13 * jmax;
+			}
+			flag[e] = ok ? 1 : 0;
+			// the element's geometry from its first point, as the quadrature path evaluates it
+			double inv[9], c[6];
+			const double meas = sqrt(jac_geom<NSD, true>(J0, inv));
+			coefs_from_inv<NSD>(inv, c);
+			double* gp = geo + e * 8;
+#pragma unroll
+			for (int k = 0; k < 6; ++k) gp[k] = c[k];
+			gp[6] = meas;
+			gp[7] = 0.0;
+		}
+		const unsigned votes = __ballot_sync(0xffffffffu, ok);
+		if ((threadIdx.x & 31) == 0 && votes) atomicAdd(count, (unsigned)__popc(votes));
+	}
+}
+
+// Per-element affine flags (once per problem).  RSD_AFFINE=0 leaves every element on the
+// quadrature path.
+static int ensure_affine(rsd_ctx* ctx, rsd_heat* h) {
+	if (h->affineTried) return RSD_OK;
+	h->affineTried = true;
+	const char* env = getenv("RSD_AFFINE");
+	if (env && env[0] == '0') return RSD_OK;
+	if (asm_smem_bytes(h->m->npe, h->nq, h->m->nsd, true) > 227 * 1024 || !h->ktab) return RSD_OK;
+	const int64_t ne = h->m->nelem;
+	RSD_CUDA(cudaMalloc(&h->affine, std::max<int64_t>(ne, 1)));
+	RSD_CUDA(cudaMalloc(&h->geo, sizeof(double) * 8 * std::max<int64_t>(ne, 1)));
+	unsigned hcnt = 0;
+	unsigned* dcnt = nullptr;
+	RSD_CUDA(cudaMalloc(&dcnt, sizeof(unsigned)));
+	RSD_CUDA(cudaMemsetAsync(dcnt, 0, sizeof(unsigned), ctx->stream));
+	const int blocks = (int)std::min<int64_t>((ne + 255) / 256, (int64_t)ctx->num_sms * 8);
+	const int nsd = h->m->nsd, ord = h->m->order;
+#define RSD_AFF(D, Q) k_affine<D, Q><<<std::max(blocks, 1), 256, 0, ctx->stream>>>(ne, h->m->ien, h->m->xyz, h->tables, h->nq, h->affine, h->geo, dcnt)
+	if (nsd == 2 && ord == 1) RSD_AFF(2, 1);
+	else if (nsd == 2 && ord == 2) RSD_AFF(2, 2);
+	else if (nsd == 2 && ord == 3) RSD_AFF(2, 3);
+	else if (nsd == 3 && ord == 1) RSD_AFF(3, 1);
+	else RSD_AFF(3, 2);
+#undef RSD_AFF
+	cudaError_t e = cudaGetLastError();
+	if (e == cudaSuccess) e = cudaMemcpyAsync(&hcnt, dcnt, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream);
+	if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+	cudaFree(dcnt);
+	if (e != cudaSuccess) return cuda_error(e, "affine element flags");
+	h->anyAffine = hcnt > 0;
 	return RSD_OK;
 }
 
@@ -622,6 +835,7 @@ static AsmParams params_for(const rsd_heat* h) {
 }
 
 static int launch_one(void (*kern)(const AsmParams), dim3 gr, size_t smem, rsd_ctx* ctx, const AsmParams& p) {
+	if (p.fast && !(p.affine && p.geo && p.ktab)) return set_error(RSD_EINVAL, "affine assembly path without its tables");
 	if (smem > 48 * 1024) RSD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 	kern<<<gr, kAsmThreads, smem, ctx->stream>>>(p);
 	RSD_CUDA(cudaGetLastError());
@@ -631,7 +845,7 @@ static int launch_one(void (*kern)(const AsmParams), dim3 gr, size_t smem, rsd_c
 #define RSD_ASM_DISPATCH(KERNEL)                                                              \
 	static int launch_##KERNEL(rsd_ctx* ctx, const rsd_heat* h, const AsmParams& p) {         \
 		const int nsd = h->m->nsd, ord = h->m->order, G = group_width(h->m->npe);             \
-		const size_t smem = asm_smem_bytes(h->m->npe, h->nq);                                 \
+		const size_t smem = asm_smem_bytes(h->m->npe, h->nq, nsd, p.fast != 0);              \
 		const int epb = kAsmWarps * (32 / G);                                                 \
 		int64_t blocks = (p.nelem + epb - 1) / epb;                                           \
 		blocks = std::min<int64_t>(blocks, (int64_t)ctx->num_sms * 16);                       \
@@ -667,7 +881,7 @@ static int launch_vector_mode(rsd_ctx* ctx, dim3 gr, size_t smem, const AsmParam
 
 static int launch_k_asm_vector(rsd_ctx* ctx, const rsd_heat* h, const AsmParams& p) {
 	const int nsd = h->m->nsd, ord = h->m->order, G = group_width(h->m->npe);
-	const size_t smem = asm_smem_bytes(h->m->npe, h->nq);
+	const size_t smem = asm_smem_bytes(h->m->npe, h->nq, nsd, p.fast != 0);
 	const int epb = kAsmWarps * (32 / G);
 	int64_t blocks = (p.nelem + epb - 1) / epb;
 	blocks = std::min<int64_t>(blocks, (int64_t)ctx->num_sms * 16);
@@ -725,6 +939,9 @@ int assemble_matrix(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, doubl
 	// the slot map indexes h's pattern; another matrix of equal size may differ, so it searches
 	if (A == h->K || A->rowPtr == h->K->rowPtr) p.ranks = h->ranks;
 	p.cDiff = cDiff; p.cMass = cMass; p.cTDiff = cTDiff; p.cTMass = cTMass;
+	// reference integrals for the affine elements when the coefficients are constant per element
+	RSD_CHECK(ensure_affine(ctx, h));
+	if (h->anyAffine && h->kExpr.n == 0 && h->dkExpr.n == 0 && cTDiff == 0.0) { p.fast = 1; p.affine = h->affine; p.geo = h->geo; p.ktab = h->ktab; }
 	p.U = U; p.Udot = Udot;
 	RSD_CUDA(cudaMemsetAsync(A->sVal, 0, sizeof(double) * std::max<int64_t>(A->ssize, 1), ctx->stream));
 	A->sellValid = true;
@@ -736,11 +953,23 @@ int assemble_matrix(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, doubl
 	return rc;
 }
 
+// the affine path of the vector kernels: every mode but the adjoint, with no state-dependent
+// conductivity and no load term (both are evaluated per quadrature point)
+static int affine_vector(rsd_ctx* ctx, rsd_heat* h, AsmParams& p) {
+	RSD_CHECK(ensure_affine(ctx, h));
+	const int w = p.which;
+	const bool load = w == 0 || w == 7 || w == 9;
+	const bool state = h->kExpr.n != 0 && (w == 1 || w == 4 || w == 8 || w == 9);
+	if (h->anyAffine && w != 6 && !state && !(load && h->srcExpr.n != 0)) { p.fast = 1; p.affine = h->affine; p.geo = h->geo; p.ktab = h->ktab; }
+	return RSD_OK;
+}
+
 int assemble_vector(rsd_ctx* ctx, rsd_heat* h, int which, double coef, const double* U, const double* Udot,
                     const double* operand, double* out, double outScale, bool accumulate) {
 	AsmParams p = params_for(h);
 	p.which = which; p.coef = coef; p.U = U; p.Udot = Udot; p.V = operand; p.out = out; p.outScale = outScale;
 	if (which == 7 && h->gPrevValid) p.gPrev = h->gPrev;
+	RSD_CHECK(affine_vector(ctx, h, p));
 	if (!accumulate) {
 		const int64_t len = which == 6 ? h->m->nelem : h->n;
 		RSD_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * std::max<int64_t>(len, 1), ctx->stream));
@@ -757,6 +986,7 @@ int assemble_lift(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, double*
 	AsmParams p = params_for(h);
 	p.which = 5; p.cDiff = cDiff; p.cMass = cMass; p.out = F; p.outScale = -1.0;
 	p.elist = h->bElems; p.nelem = h->nbElems;
+	RSD_CHECK(affine_vector(ctx, h, p));
 	const int pr = prof_begin(ctx, PF_ASM_VECTOR);
 	const int rc = launch_k_asm_vector(ctx, h, p);
 	prof_end(ctx, pr);

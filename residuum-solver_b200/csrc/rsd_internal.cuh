@@ -199,6 +199,12 @@ struct rsd_heat {
 	bool gPrevValid = false;
 	uint8_t* ranks = nullptr;       // device: element -> column-rank map for K's pattern
 	bool slotsTried = false;
+	// affine elements (constant Jacobian): flag per element, and the reference-element integrals
+	// [NT + 1][npe][npe] of the gradient products and of the mass (NT = 3 in 2D, 6 in 3D)
+	uint8_t* affine = nullptr;      // device, per element
+	double* geo = nullptr;          // device, 8 per element: table coefficients (6), |J|, 0
+	bool affineTried = false, anyAffine = false;
+	double* ktab = nullptr;         // device
 	// stage scratch
 	double *F = nullptr, *R = nullptr, *Udot = nullptr, *ms = nullptr, *dU = nullptr;
 	double dt = 0.0;

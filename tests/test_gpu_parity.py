@@ -83,6 +83,66 @@ def test_element_loops_match_reference(rsd, ctx, name, nsd, order, nq, nel, lo, 
     assert relerr(out.download(), g["diag"]) <= REL
 
 
+def distorted_mesh(nsd, order, nel, seed):
+    # block mesh with the nodes of the left half moved at random (the restatement's own copy is
+    # moved too): elements there are not affine, those on the right stay affine, so one launch
+    # takes both the quadrature path and the reference-integral path
+    m = oracle.BlockMesh(nsd, nel, [0] * nsd, [1] * nsd, order)
+    X = np.ctypeslib.as_array(m._m.xyz, shape=(m.nnodes, nsd))
+    rng = np.random.default_rng(seed)
+    move = ((X > 1e-9) & (X < 1 - 1e-9)).all(1) & (X[:, 0] < 0.45)
+    X[move] += (0.2 / (order * max(nel))) * rng.uniform(-1.0, 1.0, (int(move.sum()), nsd))
+    m.xyz = X.reshape(-1).copy()
+    return m
+
+
+@pytest.mark.parametrize("nsd,order,nq,nel", [(3, 1, 2, [6, 5, 4]), (2, 2, 3, [5, 3]), (3, 2, 3, [3, 2, 2])])
+def test_distorted_and_affine_elements_match_reference(rsd, ctx, nsd, order, nq, nel):
+    m = distorted_mesh(nsd, order, nel, 11)
+    bc = {0: "x", 1: "0"}
+    o = oracle.Oracle(m, nq, rho=1.5, cp=2.0, bc=bc)
+    h = rsd.Heat(ctx, rsd.Mesh(ctx, nsd, order, m.xyz, m.ien, m.rng), nq, rho=1.5, cp=2.0, dirichlet=bc)
+    n = h.n
+    rng = np.random.default_rng(3)
+    Uh, Udh = rng.standard_normal(n), rng.standard_normal(n)
+    U, Ud = ctx.to_device(Uh), ctx.to_device(Udh)
+    h.assemble_matrix(1.0, 7.5)
+    assert relerr(h.K.values(), o.assemble_matrix(1.0, 7.5)) <= REL
+    out = ctx.array(n)
+    h.assemble_vector(1, out, U=U)
+    assert relerr(out.download(), o.assemble_vector(1, U=Uh)) <= REL
+    h.assemble_vector(2, out, U=U)
+    assert relerr(out.download(), o.assemble_vector(2, U=Uh)) <= REL
+    h.assemble_vector(3, out, Udot=Ud)
+    assert relerr(out.download(), o.assemble_vector(3, Udot=Udh)) <= REL
+    h.assemble_vector(4, out, coef=2.5, operand=Ud)
+    assert relerr(out.download(), o.assemble_vector(4, coef=2.5, operand=Udh)) <= REL
+    F = np.zeros(n)
+    Fd = ctx.to_device(F)
+    h.lift(Fd, 1.0, 7.5)
+    assert relerr(Fd.download(), o.lift(F, 1.0, 7.5)) <= REL
+
+
+def test_affine_path_matches_quadrature_path(rsd, ctx, monkeypatch):
+    # the same problem on an undistorted mesh with the reference-integral path and without it
+    def run():
+        h = make_heat(rsd, ctx, 3, 1, 2, [7, 6, 5], [0, 0, 0], [1, 2, 3], k_elem=np.linspace(1, 2, 210),
+                      dirichlet={0: "0", 3: "1"})
+        U = ctx.to_device(np.random.default_rng(1).standard_normal(h.n))
+        h.assemble_matrix(1.0, 4.0)
+        out = ctx.array(h.n)
+        res = [h.K.values()]
+        for which, kw in ((1, dict(U=U)), (2, dict(U=U)), (4, dict(coef=0.5, operand=U))):
+            h.assemble_vector(which, out, **kw)
+            res.append(out.download())
+        return res
+    fast = run()
+    monkeypatch.setenv("RSD_AFFINE", "0")
+    slow = run()
+    for a, b in zip(fast, slow):
+        assert relerr(a, b) <= 1e-13
+
+
 def test_steady_cg_and_gmres_match_reference(rsd, ctx):
     h = make_heat(rsd, ctx, 2, 1, 2, [16, 16], [0, 0], [1, 1], dirichlet={t: "(1-x)*(1-y)" for t in range(4)})
     g = golden("steady_q1_quad_16.npz")
