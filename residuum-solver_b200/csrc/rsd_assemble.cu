@@ -53,6 +53,7 @@ __device__ __forceinline__ int32_t sell_slot(const int32_t* sStart, const int32_
 struct AsmParams {
 	int64_t nelem;
 	int32_t nq;
+	int32_t pts;   // per-point records staged per element: nq, or 0 when every element of the launch is affine
 	// vector kernels: 0 load, 1 diffusion(U), 2 mass(U), 3 mass(Udot), 4 operator(V), 5 lift, 6 adjoint,
 	// 7 Backward-Euler right-hand side load + coef*mass(U), 8 stage residual diffusion(U) + mass(Udot),
 	// 9 Newton residual load - diffusion(U)
@@ -115,11 +116,11 @@ __host__ __device__ inline int point_area(int nq) { return nq * REC + 1; }
 __host__ __device__ inline int ktab_count(int nsd) { return nsd == 3 ? 7 : 4; }
 __host__ __device__ inline int ktab_stride(int npe) { return npe | 1; }
 
-size_t asm_smem_bytes(int npe, int nq, int nsd, bool fast) {
+size_t asm_smem_bytes(int npe, int nq, int nsd, bool fast, int pts) {
 	const int G = npe <= 4 ? 4 : npe <= 8 ? 8 : npe <= 16 ? 16 : 32;
 	const int EPW = 32 / G;
 	const size_t kt = fast ? (size_t)ktab_count(nsd) * npe * ktab_stride(npe) : 0;
-	return sizeof(double) * ((size_t)nq * table_stride(G) + nq + (size_t)kAsmWarps * EPW * (node_area(npe) + point_area(nq)) + kt);
+	return sizeof(double) * ((size_t)nq * table_stride(G) + nq + (size_t)kAsmWarps * EPW * (node_area(npe) + point_area(pts)) + kt);
 }
 
 // what phase 2 must evaluate
@@ -320,13 +321,13 @@ __device__ __forceinline__ double affine_mass_row(const double* kt, int a, const
 	const double* tab = sm;                                                                      \
 	const double* wq = sm + prm.nq * TS;                                                         \
 	const int lane = threadIdx.x & 31, a = lane % G, slot = lane / G, warp = threadIdx.x >> 5;   \
-	double* wbase = sm + prm.nq * TS + prm.nq + (size_t)warp * EPW * (node_area(NPE) + point_area(prm.nq)); \
-	double* nodes = wbase + slot * (node_area(NPE) + point_area(prm.nq));                        \
+	double* wbase = sm + prm.nq * TS + prm.nq + (size_t)warp * EPW * (node_area(NPE) + point_area(prm.pts)); \
+	double* nodes = wbase + slot * (node_area(NPE) + point_area(prm.pts));                       \
 	double* recs = nodes + node_area(NPE);                                                       \
 	const int64_t warpId = (int64_t)blockIdx.x * kAsmWarps + warp;                               \
 	const int64_t warpStride = (int64_t)gridDim.x * kAsmWarps;                                   \
 	constexpr int KS = NPE | 1;                                                                  \
-	double* kt = sm + prm.nq * TS + prm.nq + (size_t)kAsmWarps * EPW * (node_area(NPE) + point_area(prm.nq)); \
+	double* kt = sm + prm.nq * TS + prm.nq + (size_t)kAsmWarps * EPW * (node_area(NPE) + point_area(prm.pts)); \
 	if (prm.fast) {                                                                              \
 		for (int i = threadIdx.x; i < ktab_count(NSD) * NPE * NPE; i += blockDim.x)              \
 			kt[(i / NPE) * KS + i % NPE] = prm.ktab[i];                                          \
@@ -336,7 +337,7 @@ __device__ __forceinline__ double affine_mass_row(const double* kt, int a, const
 		const int64_t idx = eb + slot;                                                           \
 		const bool inRange = idx < prm.nelem;                                                    \
 		const int64_t e = inRange ? (prm.elist ? (int64_t)prm.elist[idx] : idx) : 0;             \
-		const bool aff = prm.fast && inRange && prm.affine[e];                                   \
+		const bool aff = prm.fast && inRange && (prm.pts == 0 || prm.affine[e]);                \
 		const bool has = inRange && a < NPE;                                                     \
 		int32_t node = 0, row = -1;                                                              \
 		if (has) {                                                                               \
@@ -673,7 +674,7 @@ int build_tables(rsd_heat* h) {
 	double gx[5], gw[5];
 	gauss_legendre(q1, gx, gw);
 	const int nq = nsd == 3 ? q1 * q1 * q1 : q1 * q1;
-	if (asm_smem_bytes(h->m->npe, nq, nsd, false) > 227 * 1024) return set_error(RSD_EINVAL, "too many quadrature points for this element");
+	if (asm_smem_bytes(h->m->npe, nq, nsd, false, nq) > 227 * 1024) return set_error(RSD_EINVAL, "too many quadrature points for this element");
 	std::vector<double> t(nq * G * 4 + nq, 0.0);
 	int q = 0;
 	for (int k = 0; k < (nsd == 3 ? q1 : 1); ++k)
@@ -787,7 +788,7 @@ static int ensure_affine(rsd_ctx* ctx, rsd_heat* h) {
 	h->affineTried = true;
 	const char* env = getenv("RSD_AFFINE");
 	if (env && env[0] == '0') return RSD_OK;
-	if (asm_smem_bytes(h->m->npe, h->nq, h->m->nsd, true) > 227 * 1024 || !h->ktab) return RSD_OK;
+	if (asm_smem_bytes(h->m->npe, h->nq, h->m->nsd, true, h->nq) > 227 * 1024 || !h->ktab) return RSD_OK;
 	const int64_t ne = h->m->nelem;
 	RSD_CUDA(cudaMalloc(&h->affine, std::max<int64_t>(ne, 1)));
 	RSD_CUDA(cudaMalloc(&h->geo, sizeof(double) * 8 * std::max<int64_t>(ne, 1)));
@@ -810,6 +811,7 @@ static int ensure_affine(rsd_ctx* ctx, rsd_heat* h) {
 	cudaFree(dcnt);
 	if (e != cudaSuccess) return cuda_error(e, "affine element flags");
 	h->anyAffine = hcnt > 0;
+	h->allAffine = (int64_t)hcnt == ne;
 	return RSD_OK;
 }
 
@@ -817,6 +819,7 @@ static AsmParams params_for(const rsd_heat* h) {
 	AsmParams p{};
 	p.nelem = h->m->nelem;
 	p.nq = h->nq;
+	p.pts = h->nq;
 	p.xyz = h->m->xyz;
 	p.ien = h->m->ien;
 	p.t2a = h->t2a;
@@ -845,7 +848,7 @@ static int launch_one(void (*kern)(const AsmParams), dim3 gr, size_t smem, rsd_c
 #define RSD_ASM_DISPATCH(KERNEL)                                                              \
 	static int launch_##KERNEL(rsd_ctx* ctx, const rsd_heat* h, const AsmParams& p) {         \
 		const int nsd = h->m->nsd, ord = h->m->order, G = group_width(h->m->npe);             \
-		const size_t smem = asm_smem_bytes(h->m->npe, h->nq, nsd, p.fast != 0);              \
+		const size_t smem = asm_smem_bytes(h->m->npe, h->nq, nsd, p.fast != 0, p.pts);       \
 		const int epb = kAsmWarps * (32 / G);                                                 \
 		int64_t blocks = (p.nelem + epb - 1) / epb;                                           \
 		blocks = std::min<int64_t>(blocks, (int64_t)ctx->num_sms * 16);                       \
@@ -881,7 +884,7 @@ static int launch_vector_mode(rsd_ctx* ctx, dim3 gr, size_t smem, const AsmParam
 
 static int launch_k_asm_vector(rsd_ctx* ctx, const rsd_heat* h, const AsmParams& p) {
 	const int nsd = h->m->nsd, ord = h->m->order, G = group_width(h->m->npe);
-	const size_t smem = asm_smem_bytes(h->m->npe, h->nq, nsd, p.fast != 0);
+	const size_t smem = asm_smem_bytes(h->m->npe, h->nq, nsd, p.fast != 0, p.pts);
 	const int epb = kAsmWarps * (32 / G);
 	int64_t blocks = (p.nelem + epb - 1) / epb;
 	blocks = std::min<int64_t>(blocks, (int64_t)ctx->num_sms * 16);
@@ -941,7 +944,7 @@ int assemble_matrix(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, doubl
 	p.cDiff = cDiff; p.cMass = cMass; p.cTDiff = cTDiff; p.cTMass = cTMass;
 	// reference integrals for the affine elements when the coefficients are constant per element
 	RSD_CHECK(ensure_affine(ctx, h));
-	if (h->anyAffine && h->kExpr.n == 0 && h->dkExpr.n == 0 && cTDiff == 0.0) { p.fast = 1; p.affine = h->affine; p.geo = h->geo; p.ktab = h->ktab; }
+	if (h->anyAffine && h->kExpr.n == 0 && h->dkExpr.n == 0 && cTDiff == 0.0) { p.fast = 1; p.affine = h->affine; p.geo = h->geo; p.ktab = h->ktab; if (h->allAffine) p.pts = 0; }
 	p.U = U; p.Udot = Udot;
 	RSD_CUDA(cudaMemsetAsync(A->sVal, 0, sizeof(double) * std::max<int64_t>(A->ssize, 1), ctx->stream));
 	A->sellValid = true;
@@ -960,7 +963,7 @@ static int affine_vector(rsd_ctx* ctx, rsd_heat* h, AsmParams& p) {
 	const int w = p.which;
 	const bool load = w == 0 || w == 7 || w == 9;
 	const bool state = h->kExpr.n != 0 && (w == 1 || w == 4 || w == 8 || w == 9);
-	if (h->anyAffine && w != 6 && !state && !(load && h->srcExpr.n != 0)) { p.fast = 1; p.affine = h->affine; p.geo = h->geo; p.ktab = h->ktab; }
+	if (h->anyAffine && w != 6 && !state && !(load && h->srcExpr.n != 0)) { p.fast = 1; p.affine = h->affine; p.geo = h->geo; p.ktab = h->ktab; if (h->allAffine) p.pts = 0; }
 	return RSD_OK;
 }
 

@@ -203,7 +203,7 @@ struct rsd_heat {
 	// [NT + 1][npe][npe] of the gradient products and of the mass (NT = 3 in 2D, 6 in 3D)
 	uint8_t* affine = nullptr;      // device, per element
 	double* geo = nullptr;          // device, 8 per element: table coefficients (6), |J|, 0
-	bool affineTried = false, anyAffine = false;
+	bool affineTried = false, anyAffine = false, allAffine = false;
 	double* ktab = nullptr;         // device
 	// stage scratch
 	double *F = nullptr, *R = nullptr, *Udot = nullptr, *ms = nullptr, *dU = nullptr;
