@@ -467,6 +467,76 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_matrix(const AsmParams prm)
 // element -> column-rank map, built once per pattern: rank[e][a][b] = position of column
 // t2a[node_b] within row t2a[node_a] (rows hold at most 254 entries), 0xFF when either DOF is
 // constrained
+// Assembler::assembleMatrix when every element of the launch is affine, gathered by row: a warp owns
+// a SELL-32 slice and lane l its row 32 s + l.  The lane adds row a of every adjacent element (e, a),
+// in element order, into its column of a shared-memory image of the slice [entry][lane], which the
+// warp then writes out in the pair layout.  Every value is written once: no zero fill, no atomics,
+// and the sums are deterministic.
+constexpr int kRowWarps = 4;
+template <int NSD, int P>
+__global__ void __launch_bounds__(32 * kRowWarps) k_asm_matrix_rows(const AsmParams prm, const int32_t* __restrict__ adjPtr,
+                                                                     const int32_t* __restrict__ adj, int64_t n, int32_t maxLen) {
+	using E = Elem<NSD, P>;
+	constexpr int NPE = E::NPE, KS = NPE | 1, NT = NSD == 3 ? 6 : 3, RB = (NPE + 7) & ~7;
+	extern __shared__ double sm[];
+	double* kt = sm;
+	for (int i = threadIdx.x; i < ktab_count(NSD) * NPE * NPE; i += blockDim.x) kt[(i / NPE) * KS + i % NPE] = prm.ktab[i];
+	__syncthreads();
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	double* acc = sm + ktab_count(NSD) * NPE * KS + (size_t)warp * maxLen * 32 + lane;   // this lane's column
+	const int64_t ns = (n + 31) >> 5;
+	for (int64_t s = (int64_t)blockIdx.x * kRowWarps + warp; s < ns; s += (int64_t)gridDim.x * kRowWarps) {
+		const int32_t s0 = prm.sStart[s];
+		const int len = (prm.sStart[s + 1] - s0) >> 5;
+		for (int j = 0; j < len; ++j) acc[j * 32] = 0.0;
+		const int64_t row = 32 * s + lane;
+		if (row < n) {
+			// elements in batches of ABATCH: all their loads first, then the sums (in element order)
+			constexpr int ABATCH = 4;
+			const int32_t q1 = adjPtr[row + 1];
+			for (int32_t q0 = adjPtr[row]; q0 < q1; q0 += ABATCH) {
+				int32_t ea[ABATCH];
+				double gk[ABATCH][8];
+				unsigned long long w[ABATCH][RB / 8];
+#pragma unroll
+				for (int k = 0; k < ABATCH; ++k) ea[k] = q0 + k < q1 ? adj[q0 + k] : -1;
+#pragma unroll
+				for (int k = 0; k < ABATCH; ++k) {
+					if (ea[k] < 0) continue;
+					const int32_t e = ea[k] / NPE;
+					const double2* gp = reinterpret_cast<const double2*>(prm.geo + (int64_t)e * 8);
+#pragma unroll
+					for (int i = 0; i < 4; ++i) { const double2 v = gp[i]; gk[k][2 * i] = v.x; gk[k][2 * i + 1] = v.y; }
+					gk[k][7] = prm.kElem ? prm.kElem[e] : 1.0;   // slot 7 of the record is spare
+					const unsigned long long* rk = reinterpret_cast<const unsigned long long*>(prm.ranks + (int64_t)ea[k] * RB);
+#pragma unroll
+					for (int i = 0; i < RB / 8; ++i) w[k][i] = __ldcs(rk + i);
+				}
+#pragma unroll
+				for (int k = 0; k < ABATCH; ++k) {
+					if (ea[k] < 0) continue;
+					const int32_t a = ea[k] - (ea[k] / NPE) * NPE;
+					const double cd = prm.cDiff * gk[k][7] * prm.kConst * gk[k][6];
+					const double cm = prm.cMass * prm.rho * prm.cp * gk[k][6];
+#pragma unroll
+					for (int b = 0; b < NPE; ++b) {
+						const int j = (int)((w[k][b >> 3] >> (8 * (b & 7))) & 0xFF);
+						if (j != 0xFF) {
+							double g = 0.0;
+#pragma unroll
+							for (int t = 0; t < NT; ++t) g += gk[k][t] * kt[(t * NPE + a) * KS + b];
+							acc[j * 32] += cd * g + cm * kt[(NT * NPE + a) * KS + b];
+						}
+					}
+				}
+			}
+		}
+		// pair jp of lane l sits at s0 + 64 jp + 2 l; a lane reads only its own column of the image
+		double2* out = reinterpret_cast<double2*>(prm.val + s0) + lane;
+		for (int jp = 0; jp < (len >> 1); ++jp) out[32 * jp] = make_double2(acc[(2 * jp) * 32], acc[(2 * jp + 1) * 32]);
+	}
+}
+
 template <int NSD, int P>
 __global__ void k_build_slots(int64_t nelem, const int32_t* __restrict__ ien, const int32_t* __restrict__ t2a,
                               const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
@@ -669,7 +739,7 @@ static int group_width(int npe) { return npe <= 4 ? 4 : npe <= 8 ? 8 : npe <= 16
 
 // tensor-product tables in quadrature-point order (x fastest, GaussQuadratureHex.tpp:4-49) and
 // node order (x fastest, LagrangeHex.tpp:4-55): [nq][G][4] = (N, dN/dxi, dN/deta, dN/dzeta), then w[nq]
-int build_tables(rsd_heat* h) {
+int build_tables(rsd_ctx* ctx, rsd_heat* h) {
 	const int nsd = h->m->nsd, p = h->m->order, q1 = h->nq1, G = group_width(h->m->npe);
 	double gx[5], gw[5];
 	gauss_legendre(q1, gx, gw);
@@ -702,7 +772,7 @@ int build_tables(rsd_heat* h) {
 	h->nq = nq;
 	if (h->tables) cudaFree(h->tables);
 	RSD_CUDA(cudaMalloc(&h->tables, sizeof(double) * t.size()));
-	RSD_CUDA(cudaMemcpy(h->tables, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice));
+	RSD_CUDA(cudaMemcpyAsync(h->tables, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice, ctx->stream));
 	// reference integrals of the affine path, by the same quadrature: the gradient products
 	// (00, 11, [22,] 01, [02, 12]; off-diagonal pairs symmetrised) and the mass
 	const int npe = h->m->npe, nt = ktab_count(nsd) - 1;
@@ -726,7 +796,10 @@ int build_tables(rsd_heat* h) {
 			}
 	if (h->ktab) cudaFree(h->ktab);
 	RSD_CUDA(cudaMalloc(&h->ktab, sizeof(double) * kt.size()));
-	RSD_CUDA(cudaMemcpy(h->ktab, kt.data(), sizeof(double) * kt.size(), cudaMemcpyHostToDevice));
+	RSD_CUDA(cudaMemcpyAsync(h->ktab, kt.data(), sizeof(double) * kt.size(), cudaMemcpyHostToDevice, ctx->stream));
+	// uploads go on the context stream (a pageable copy on the legacy stream may still be in flight when
+	// it returns, unordered with the non-blocking context stream); the host tables die here
+	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
 	return RSD_OK;
 }
 
@@ -910,8 +983,8 @@ static int ensure_slots(rsd_ctx* ctx, rsd_heat* h) {
 	std::vector<int32_t> st(K->nslices + 1);
 	RSD_CUDA(cudaMemcpyAsync(st.data(), K->sStart, sizeof(int32_t) * st.size(), cudaMemcpyDeviceToHost, ctx->stream));
 	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
-	for (int64_t i = 0; i < K->nslices; ++i)
-		if ((st[i + 1] - st[i]) / 32 > 254) return RSD_OK;
+	for (int64_t i = 0; i < K->nslices; ++i) h->maxSlice = std::max<int32_t>(h->maxSlice, (st[i + 1] - st[i]) / 32);
+	if (h->maxSlice > 254) return RSD_OK;
 	const int npe = h->m->npe;
 	const int stride = (npe + 7) & ~7;
 	const size_t bytes = (size_t)h->m->nelem * npe * stride;
@@ -933,6 +1006,64 @@ static int ensure_slots(rsd_ctx* ctx, rsd_heat* h) {
 	return RSD_OK;
 }
 
+// Row -> (element, local node) adjacency of the free rows (once per problem), for the row-gather
+// assembly: built on the host in element order, so that every row sums its elements in that order.
+static int ensure_adjacency(rsd_ctx* ctx, rsd_heat* h) {
+	if (h->adjTried) return RSD_OK;
+	h->adjTried = true;
+	const int64_t ne = h->m->nelem, n = h->n;
+	const int npe = h->m->npe;
+	if (ne * npe >= INT32_MAX) return RSD_OK;
+	std::vector<int32_t> ptr(n + 1, 0);
+	for (int64_t t = 0; t < ne * npe; ++t) {
+		const int32_t r = h->h_t2a[h->m->h_ien[t]];
+		if (r >= 0) ++ptr[r + 1];
+	}
+	for (int64_t i = 0; i < n; ++i) ptr[i + 1] += ptr[i];
+	std::vector<int32_t> pos(ptr.begin(), ptr.end() - 1), adj(std::max<int32_t>(ptr[n], 1));
+	for (int64_t t = 0; t < ne * npe; ++t) {
+		const int32_t r = h->h_t2a[h->m->h_ien[t]];
+		if (r >= 0) adj[pos[r]++] = (int32_t)t;
+	}
+	cudaError_t e;
+	if ((e = cudaMalloc(&h->adjPtr, sizeof(int32_t) * (n + 1))) != cudaSuccess ||
+	    (e = cudaMalloc(&h->adj, sizeof(int32_t) * adj.size())) != cudaSuccess ||
+	    (e = cudaMemcpyAsync(h->adjPtr, ptr.data(), sizeof(int32_t) * (n + 1), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess ||
+	    (e = cudaMemcpyAsync(h->adj, adj.data(), sizeof(int32_t) * adj.size(), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess ||
+	    (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) {
+		cudaGetLastError();
+		cudaFree(h->adjPtr); cudaFree(h->adj);
+		h->adjPtr = nullptr; h->adj = nullptr;
+	}
+	return RSD_OK;
+}
+
+// the row-gather kernel for an all-affine launch with the slot map (RSD_ROW_ASM=0: the scatter)
+static int launch_matrix_rows(rsd_ctx* ctx, rsd_heat* h, const AsmParams& p, bool* done) {
+	*done = false;
+	const char* env = getenv("RSD_ROW_ASM");
+	if ((env && env[0] == '0') || !p.fast || p.pts != 0 || !p.ranks || h->maxSlice > 64) return RSD_OK;
+	RSD_CHECK(ensure_adjacency(ctx, h));
+	if (!h->adj) return RSD_OK;
+	const int nsd = h->m->nsd, ord = h->m->order, npe = h->m->npe;
+	const size_t smem = sizeof(double) * ((size_t)ktab_count(nsd) * npe * ktab_stride(npe) + (size_t)kRowWarps * h->maxSlice * 32);
+	const int64_t ns = (h->n + 31) / 32;
+	const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((ns + kRowWarps - 1) / kRowWarps, (int64_t)ctx->num_sms * 32));
+	auto go = [&](auto kern) -> int {
+		if (smem > 48 * 1024) RSD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+		kern<<<blocks, 32 * kRowWarps, smem, ctx->stream>>>(p, h->adjPtr, h->adj, h->n, h->maxSlice);
+		RSD_CUDA(cudaGetLastError());
+		*done = true;
+		return RSD_OK;
+	};
+	if (nsd == 2 && ord == 1) return go(k_asm_matrix_rows<2, 1>);
+	if (nsd == 2 && ord == 2) return go(k_asm_matrix_rows<2, 2>);
+	if (nsd == 2 && ord == 3) return go(k_asm_matrix_rows<2, 3>);
+	if (nsd == 3 && ord == 1) return go(k_asm_matrix_rows<3, 1>);
+	if (nsd == 3 && ord == 2) return go(k_asm_matrix_rows<3, 2>);
+	return RSD_OK;
+}
+
 int assemble_matrix(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, double cTDiff, double cTMass,
                     const double* U, const double* Udot, rsd_csr* A) {
 	if (A->n != h->n || A->nnz != h->K->nnz) return set_error(RSD_EINVAL, "matrix does not have the problem's pattern");
@@ -946,12 +1077,16 @@ int assemble_matrix(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, doubl
 	RSD_CHECK(ensure_affine(ctx, h));
 	if (h->anyAffine && h->kExpr.n == 0 && h->dkExpr.n == 0 && cTDiff == 0.0) { p.fast = 1; p.affine = h->affine; p.geo = h->geo; p.ktab = h->ktab; if (h->allAffine) p.pts = 0; }
 	p.U = U; p.Udot = Udot;
-	RSD_CUDA(cudaMemsetAsync(A->sVal, 0, sizeof(double) * std::max<int64_t>(A->ssize, 1), ctx->stream));
 	A->sellValid = true;
 	A->csrValid = false;
 	A->version++;
 	const int pr = prof_begin(ctx, PF_ASM_MATRIX);
-	const int rc = launch_k_asm_matrix(ctx, h, p);
+	bool rows = false;
+	int rc = launch_matrix_rows(ctx, h, p, &rows);
+	if (rc == RSD_OK && !rows) {
+		RSD_CUDA(cudaMemsetAsync(A->sVal, 0, sizeof(double) * std::max<int64_t>(A->ssize, 1), ctx->stream));
+		rc = launch_k_asm_matrix(ctx, h, p);
+	}
 	prof_end(ctx, pr);
 	return rc;
 }

@@ -250,7 +250,10 @@ int rsd_batch_create(rsd_ctx* ctx, int32_t count, rsd_csr* const* A, rsd_batch**
 		delete B;
 		return cuda_error(e, "cudaMalloc (batch)");
 	}
-	if (count) RSD_CUDA(cudaMemcpy(B->dorder, B->order.data(), sizeof(int32_t) * count, cudaMemcpyHostToDevice));
+	if (count) {   // on the context stream, which the solves run on (B->order outlives the copy)
+		RSD_CUDA(cudaMemcpyAsync(B->dorder, B->order.data(), sizeof(int32_t) * count, cudaMemcpyHostToDevice, ctx->stream));
+		RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+	}
 	*out = B;
 	return RSD_OK;
 }

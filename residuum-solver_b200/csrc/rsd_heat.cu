@@ -7,7 +7,7 @@
 
 namespace rsd {
 
-int build_tables(rsd_heat* h);
+int build_tables(rsd_ctx* ctx, rsd_heat* h);
 int assemble_lift(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, double* F);
 
 static bool uses_time(const DevExpr& e) {
@@ -74,7 +74,7 @@ __global__ void k_diff_norm(int64_t n, const double* __restrict__ F, const doubl
 
 static void free_heat(rsd_heat* h) {
 	cudaFree(h->t2a); cudaFree(h->g); cudaFree(h->kElem); cudaFree(h->tables); cudaFree(h->bElems); cudaFree(h->gPrev);
-	cudaFree(h->ranks); cudaFree(h->affine); cudaFree(h->geo); cudaFree(h->ktab);
+	cudaFree(h->ranks); cudaFree(h->affine); cudaFree(h->geo); cudaFree(h->ktab); cudaFree(h->adjPtr); cudaFree(h->adj);
 	cudaFree(h->F); cudaFree(h->R); cudaFree(h->Udot); cudaFree(h->ms); cudaFree(h->dU);
 	if (h->K) rsd_csr_destroy(h->K);
 	delete h;
@@ -136,7 +136,7 @@ int rsd_heat_create(rsd_ctx* ctx, const rsd_mesh* m, const rsd_heat_desc* d, rsd
 		}
 		if ((e = cudaMalloc(&h->gPrev, sizeof(double) * nn)) != cudaSuccess) { free_heat(h); return cuda_error(e, "allocation"); }
 	}
-	if ((rc = build_tables(h)) || (rc = upload_bc_values(ctx, h)) || (rc = build_pattern(ctx, h, &h->K))) { free_heat(h); return rc; }
+	if ((rc = build_tables(ctx, h)) || (rc = upload_bc_values(ctx, h)) || (rc = build_pattern(ctx, h, &h->K))) { free_heat(h); return rc; }
 	*out = h;
 	return RSD_OK;
 }

@@ -205,6 +205,11 @@ struct rsd_heat {
 	double* geo = nullptr;          // device, 8 per element: table coefficients (6), |J|, 0
 	bool affineTried = false, anyAffine = false, allAffine = false;
 	double* ktab = nullptr;         // device
+	// row -> (element, local node) adjacency of the free rows, element order (row-gather assembly)
+	int32_t* adjPtr = nullptr;      // device, n + 1
+	int32_t* adj = nullptr;         // device, e * npe + a
+	bool adjTried = false;
+	int32_t maxSlice = 0;           // longest SELL-32 slice of K, in entries per row
 	// stage scratch
 	double *F = nullptr, *R = nullptr, *Udot = nullptr, *ms = nullptr, *dU = nullptr;
 	double dt = 0.0;
@@ -220,5 +225,5 @@ int assemble_vector(rsd_ctx* ctx, rsd_heat* h, int which, double coef, const dou
                     const double* operand, double* out, double outScale, bool accumulate);
 int assemble_diagonal(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, const double* U, double* d);
 int assemble_lift(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, double* F);
-int build_tables(rsd_heat* h);
+int build_tables(rsd_ctx* ctx, rsd_heat* h);
 }  // namespace rsd

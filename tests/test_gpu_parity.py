@@ -124,7 +124,8 @@ def test_distorted_and_affine_elements_match_reference(rsd, ctx, nsd, order, nq,
 
 
 def test_affine_path_matches_quadrature_path(rsd, ctx, monkeypatch):
-    # the same problem on an undistorted mesh with the reference-integral path and without it
+    # the same problem on an undistorted mesh: matrix by row gather (default), by the affine scatter,
+    # and everything by quadrature
     def run():
         h = make_heat(rsd, ctx, 3, 1, 2, [7, 6, 5], [0, 0, 0], [1, 2, 3], k_elem=np.linspace(1, 2, 210),
                       dirichlet={0: "0", 3: "1"})
@@ -136,11 +137,26 @@ def test_affine_path_matches_quadrature_path(rsd, ctx, monkeypatch):
             h.assemble_vector(which, out, **kw)
             res.append(out.download())
         return res
-    fast = run()
+    rows = run()
+    assert relerr(rows[0], run()[0]) == 0.0   # the matrix gather is deterministic (the vectors use atomics)
+    monkeypatch.setenv("RSD_ROW_ASM", "0")
+    scatter = run()
     monkeypatch.setenv("RSD_AFFINE", "0")
-    slow = run()
-    for a, b in zip(fast, slow):
-        assert relerr(a, b) <= 1e-13
+    quad = run()
+    for a, b, c in zip(rows, scatter, quad):
+        assert relerr(a, c) <= 1e-13 and relerr(b, c) <= 1e-13
+
+
+def test_first_assembly_after_setup(rsd, ctx):
+    # the first assembly of a problem builds its lazily made tables (slot map, affine flags and
+    # geometry, row adjacency) and must see them complete: a small problem first, then a larger one
+    small = make_heat(rsd, ctx, 3, 1, 2, [7, 6, 5], [0, 0, 0], [1, 1, 1], dirichlet={0: "0", 1: "0", 4: "0"})
+    small.assemble_matrix(1.0, 50.0)
+    bc = {t: "0" for t in range(6)}
+    h = make_heat(rsd, ctx, 3, 1, 2, [40, 36, 30], [0, 0, 0], [1, 1, 1], dirichlet=bc)
+    h.assemble_matrix(1.0, 50.0)
+    o = oracle.Oracle(oracle.BlockMesh(3, [40, 36, 30], [0, 0, 0], [1, 1, 1], 1), 2, bc=bc)
+    assert relerr(h.K.values(), o.assemble_matrix(1.0, 50.0)) <= REL
 
 
 def test_steady_cg_and_gmres_match_reference(rsd, ctx):
