@@ -217,8 +217,9 @@ def reference_sample(sample_size, nsteps, warmup):
     if not oracle.reference_available():
         return None
     r = oracle.Reference(3, 1, 2, [sample_size] * 3, [0, 0, 0], [1, 1, 1], list(range(6)), bc_kind=0, rho=1.0, cp=1.0)
-    from importlib import import_module
-    xyz = import_module("residuum_solver_b200.blockmesh").block_mesh(3, [sample_size] * 3, [0, 0, 0], [1, 1, 1], 1)[0]
+    # node coordinates from the oracle's block mesh (the reference's numbering): nothing of the
+    # device package runs on this arm
+    xyz = oracle.BlockMesh(3, [sample_size] * 3, [0, 0, 0], [1, 1, 1], 1).xyz
     t2a, a2t = r.dofmap()
     U0 = initial_condition(xyz, a2t)
     _, _, rc, st = r.backward_euler(1e-3, warmup + nsteps, U0, tol=1e-8, maxit=100000, stats=True)
