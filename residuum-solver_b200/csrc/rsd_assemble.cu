@@ -75,6 +75,7 @@ struct AsmParams {
 	const int32_t* __restrict__ sUni;   // stencil slices (pattern start per slice, -1 for none), or null
 	const int32_t* __restrict__ sOffs;
 	double* __restrict__ val;
+	float* __restrict__ val32;          // row-gather assembly: the FP32 copy written alongside, or null
 	// element -> column-rank map [e][a][b]: the SELL-32 position j (sell_rank) of column t2a[node_b] in
 	// row t2a[node_a] (0xFF when either DOF is constrained), rows of (NPE rounded up to 8) bytes; or null
 	const uint8_t* __restrict__ ranks;
@@ -534,6 +535,11 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_asm_matrix_rows(const AsmPar
 		// pair jp of lane l sits at s0 + 64 jp + 2 l; a lane reads only its own column of the image
 		double2* out = reinterpret_cast<double2*>(prm.val + s0) + lane;
 		for (int jp = 0; jp < (len >> 1); ++jp) out[32 * jp] = make_double2(acc[(2 * jp) * 32], acc[(2 * jp + 1) * 32]);
+		if (prm.val32) {   // the mixed solver's copy, rounded as the conversion kernel rounds
+			float2* out32 = reinterpret_cast<float2*>(prm.val32 + s0) + lane;
+			for (int jp = 0; jp < (len >> 1); ++jp)
+				out32[32 * jp] = make_float2((float)acc[(2 * jp) * 32], (float)acc[(2 * jp + 1) * 32]);
+		}
 	}
 }
 
@@ -1082,7 +1088,10 @@ int assemble_matrix(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, doubl
 	A->version++;
 	const int pr = prof_begin(ctx, PF_ASM_MATRIX);
 	bool rows = false;
+	// a matrix that already has an FP32 copy in the SELL layout gets it written by the row gather too
+	if (A->val32 && A->format == 0) p.val32 = A->val32;
 	int rc = launch_matrix_rows(ctx, h, p, &rows);
+	if (rc == RSD_OK && rows && p.val32) { A->version32 = A->version; A->fmt32 = 0; }
 	if (rc == RSD_OK && !rows) {
 		RSD_CUDA(cudaMemsetAsync(A->sVal, 0, sizeof(double) * std::max<int64_t>(A->ssize, 1), ctx->stream));
 		rc = launch_k_asm_matrix(ctx, h, p);

@@ -159,6 +159,28 @@ def test_first_assembly_after_setup(rsd, ctx):
     assert relerr(h.K.values(), o.assemble_matrix(1.0, 50.0)) <= REL
 
 
+def test_fp32_copy_written_by_row_assembly(rsd, ctx):
+    # once a matrix has an FP32 copy, the row-gather assembly writes it alongside the FP64 values;
+    # it must equal the copy that converting the FP64 values afresh gives, bit for bit
+    bc = {0: "0", 1: "0"}
+    h = make_heat(rsd, ctx, 3, 1, 2, [9, 8, 7], [0, 0, 0], [1, 1, 1], dirichlet=bc)
+    h.assemble_matrix(1.0, 2.0)
+    h.K.sync_f32()
+    h.assemble_matrix(1.0, 50.0)
+    n = h.n
+    x = np.random.default_rng(6).standard_normal(n)
+    x32, y32 = ctx.to_device(x.astype(np.float32)), ctx.array(n, np.float32)
+    h.K.spmv_f32(x32, y32)
+    fused = y32.download()
+    v = h.K.values()
+    h.K.set_values(v)                  # the same values through CSR: the copy is converted again
+    h.K.spmv_f32(x32, y32)
+    assert np.array_equal(fused, y32.download())
+    rp, col = h.K.pattern()
+    o = oracle.Oracle(oracle.BlockMesh(3, [9, 8, 7], [0, 0, 0], [1, 1, 1], 1), 2, bc=bc)
+    assert relerr(fused, oracle.spmv(rp, col, o.assemble_matrix(1.0, 50.0), x)) <= 1e-5
+
+
 def test_steady_cg_and_gmres_match_reference(rsd, ctx):
     h = make_heat(rsd, ctx, 2, 1, 2, [16, 16], [0, 0], [1, 1], dirichlet={t: "(1-x)*(1-y)" for t in range(4)})
     g = golden("steady_q1_quad_16.npz")
