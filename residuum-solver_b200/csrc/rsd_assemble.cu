@@ -681,6 +681,86 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_vector(const AsmParams prm)
 	RSD_ELEMENT_LOOP_END
 }
 
+// The vector modes of k_asm_vector for problems whose elements are all affine, with one thread per
+// element (4- and 8-node elements): a warp keeps 32 elements' gathers in flight instead of 32 / G,
+// and the reference integrals (staged in shared memory, rows of npe) are read by all lanes at once.
+// Each element's rows are formed as in the group kernel's affine branch, in the same order.
+template <int NSD, int P, int W>
+__global__ void __launch_bounds__(256) k_asm_vector_elem(const AsmParams prm) {
+	using E = Elem<NSD, P>;
+	constexpr int NPE = E::NPE, NT = NSD == 3 ? 6 : 3;
+	constexpr bool kGrad = W == 1 || W == 4 || W == 5 || W == 8 || W == 9;
+	static_assert(NPE == 4 || NPE == 8, "one thread per element for 4- and 8-node elements");
+	extern __shared__ double kt[];
+	for (int i = threadIdx.x; i < (NT + 1) * NPE * NPE; i += blockDim.x) kt[i] = prm.ktab[i];
+	__syncthreads();
+	const double k0 = kGrad ? (prm.kExpr.n ? eval_expr(prm.kExpr, 0.0, 0.0, 0.0, 0.0, 0.0) : prm.kConst) : 0.0;
+	for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < prm.nelem; idx += (int64_t)gridDim.x * blockDim.x) {
+		const int64_t e = prm.elist ? (int64_t)prm.elist[idx] : idx;
+		double gk[8];
+		const double2* gp2 = reinterpret_cast<const double2*>(prm.geo + e * 8);
+#pragma unroll
+		for (int i = 0; i < 4; ++i) { const double2 v = gp2[i]; gk[2 * i] = v.x; gk[2 * i + 1] = v.y; }
+		const double ke = prm.kElem ? prm.kElem[e] : 1.0;
+		int32_t rows[NPE];
+		double V[NPE], Wv[NPE];
+#pragma unroll
+		for (int a = 0; a < NPE; ++a) {
+			const int32_t node = prm.ien[e * NPE + a];
+			const int32_t row = prm.t2a[node];
+			rows[a] = row;
+			double Va = 0.0;
+			switch (W) {
+				case 1: case 2: case 8: case 9: Va = row >= 0 ? (prm.U ? prm.U[row] : 0.0) : prm.g[node]; break;
+				case 3: Va = (row >= 0 && prm.Udot) ? prm.Udot[row] : 0.0; break;
+				case 4: Va = (row >= 0 && prm.V) ? prm.V[row] : 0.0; break;
+				case 5: Va = row >= 0 ? 0.0 : prm.g[node]; break;
+				case 7: Va = row >= 0 ? (prm.U ? prm.U[row] : 0.0) : (prm.gPrev ? prm.gPrev[node] : prm.g[node]); break;
+				default: break;
+			}
+			V[a] = Va;
+			Wv[a] = (W == 8 && row >= 0 && prm.Udot) ? prm.Udot[row] : 0.0;
+		}
+		const double detJ = gk[6];
+#pragma unroll
+		for (int a = 0; a < NPE; ++a) {
+			double kdV = 0.0;
+			if constexpr (kGrad) {
+				double g = 0.0;
+#pragma unroll
+				for (int k = 0; k < NT; ++k) {
+					const double* row = kt + (k * NPE + a) * NPE;
+					double t = 0.0;
+#pragma unroll
+					for (int b = 0; b < NPE; ++b) t += row[b] * V[b];
+					g += gk[k] * t;
+				}
+				kdV = ke * k0 * detJ * g;
+			}
+			const double* mrow = kt + (NT * NPE + a) * NPE;
+			double mv = 0.0, mw = 0.0;
+#pragma unroll
+			for (int b = 0; b < NPE; ++b) {
+				mv += mrow[b] * V[b];
+				if (W == 8) mw += mrow[b] * Wv[b];
+			}
+			const double massV = prm.rho * prm.cp * detJ * mv;
+			double Fa = 0.0;
+			switch (W) {
+				case 1: Fa = kdV; break;
+				case 2: case 3: Fa = massV; break;
+				case 4: Fa = kdV + prm.coef * massV; break;
+				case 5: Fa = prm.cDiff * kdV + prm.cMass * massV; break;
+				case 7: Fa = prm.coef * massV; break;
+				case 8: Fa = kdV + prm.rho * prm.cp * detJ * mw; break;
+				case 9: Fa = -kdV; break;
+				default: break;
+			}
+			if (rows[a] >= 0) atomicAdd(prm.out + rows[a], prm.outScale * Fa);
+		}
+	}
+}
+
 // Assembler::assembleDiagonal (Assembler.tpp:142-197) for c_diff*Diffusion + c_mass*Mass
 template <int NSD, int P>
 __global__ void __launch_bounds__(kAsmThreads) k_asm_diag(const AsmParams prm) {
@@ -961,8 +1041,37 @@ static int launch_vector_mode(rsd_ctx* ctx, dim3 gr, size_t smem, const AsmParam
 	}
 }
 
+// one thread per element for all-affine problems of 4- and 8-node elements (RSD_ELEM_VEC=0: the
+// group kernel)
+template <int NSD, int P>
+static int launch_vector_elem(rsd_ctx* ctx, const AsmParams& p) {
+	constexpr int NPE = Elem<NSD, P>::NPE, NT = NSD == 3 ? 6 : 3;
+	const size_t smem = sizeof(double) * (NT + 1) * NPE * NPE;
+	const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((p.nelem + 255) / 256, (int64_t)ctx->num_sms * 16));
+	auto go = [&](auto kern) -> int {
+		kern<<<blocks, 256, smem, ctx->stream>>>(p);
+		RSD_CUDA(cudaGetLastError());
+		return RSD_OK;
+	};
+	switch (p.which) {
+		case 1: return go(k_asm_vector_elem<NSD, P, 1>);
+		case 2: return go(k_asm_vector_elem<NSD, P, 2>);
+		case 3: return go(k_asm_vector_elem<NSD, P, 3>);
+		case 4: return go(k_asm_vector_elem<NSD, P, 4>);
+		case 5: return go(k_asm_vector_elem<NSD, P, 5>);
+		case 7: return go(k_asm_vector_elem<NSD, P, 7>);
+		case 8: return go(k_asm_vector_elem<NSD, P, 8>);
+		case 9: return go(k_asm_vector_elem<NSD, P, 9>);
+		default: return set_error(RSD_EINVAL, "vector mode without a per-element affine kernel");
+	}
+}
+
 static int launch_k_asm_vector(rsd_ctx* ctx, const rsd_heat* h, const AsmParams& p) {
 	const int nsd = h->m->nsd, ord = h->m->order, G = group_width(h->m->npe);
+	if (p.fast && p.pts == 0 && ord == 1 && p.which != 0 && p.which != 6 && p.nelem > 0) {
+		const char* env = getenv("RSD_ELEM_VEC");
+		if (!(env && env[0] == '0')) return nsd == 3 ? launch_vector_elem<3, 1>(ctx, p) : launch_vector_elem<2, 1>(ctx, p);
+	}
 	const size_t smem = asm_smem_bytes(h->m->npe, h->nq, nsd, p.fast != 0, p.pts);
 	const int epb = kAsmWarps * (32 / G);
 	int64_t blocks = (p.nelem + epb - 1) / epb;

@@ -123,27 +123,34 @@ def test_distorted_and_affine_elements_match_reference(rsd, ctx, nsd, order, nq,
     assert relerr(Fd.download(), o.lift(F, 1.0, 7.5)) <= REL
 
 
-def test_affine_path_matches_quadrature_path(rsd, ctx, monkeypatch):
-    # the same problem on an undistorted mesh: matrix by row gather (default), by the affine scatter,
-    # and everything by quadrature
+@pytest.mark.parametrize("nsd,nel,hi", [(3, [7, 6, 5], [1, 2, 3]), (2, [9, 7], [1, 2])])
+def test_affine_path_matches_quadrature_path(rsd, ctx, monkeypatch, nsd, nel, hi):
+    # the same problem on an undistorted mesh: matrix by row gather and vectors one thread per element
+    # (default), both by the affine group kernels, and everything by quadrature
+    ne = int(np.prod(nel))
     def run():
-        h = make_heat(rsd, ctx, 3, 1, 2, [7, 6, 5], [0, 0, 0], [1, 2, 3], k_elem=np.linspace(1, 2, 210),
+        h = make_heat(rsd, ctx, nsd, 1, 2, nel, [0] * nsd, hi, k_elem=np.linspace(1, 2, ne), rho=1.5, cp=2.0,
                       dirichlet={0: "0", 3: "1"})
-        U = ctx.to_device(np.random.default_rng(1).standard_normal(h.n))
+        rng = np.random.default_rng(1)
+        U, Ud = ctx.to_device(rng.standard_normal(h.n)), ctx.to_device(rng.standard_normal(h.n))
         h.assemble_matrix(1.0, 4.0)
         out = ctx.array(h.n)
         res = [h.K.values()]
-        for which, kw in ((1, dict(U=U)), (2, dict(U=U)), (4, dict(coef=0.5, operand=U))):
+        for which, kw in ((1, dict(U=U)), (2, dict(U=U)), (3, dict(Udot=Ud)), (4, dict(coef=0.5, operand=U))):
             h.assemble_vector(which, out, **kw)
             res.append(out.download())
+        F = ctx.to_device(np.zeros(h.n))
+        h.lift(F, 1.0, 7.5)
+        res.append(F.download())
         return res
-    rows = run()
-    assert relerr(rows[0], run()[0]) == 0.0   # the matrix gather is deterministic (the vectors use atomics)
+    fast = run()
+    assert relerr(fast[0], run()[0]) == 0.0   # the matrix gather is deterministic (the vectors use atomics)
     monkeypatch.setenv("RSD_ROW_ASM", "0")
-    scatter = run()
+    monkeypatch.setenv("RSD_ELEM_VEC", "0")
+    group = run()
     monkeypatch.setenv("RSD_AFFINE", "0")
     quad = run()
-    for a, b, c in zip(rows, scatter, quad):
+    for a, b, c in zip(fast, group, quad):
         assert relerr(a, c) <= 1e-13 and relerr(b, c) <= 1e-13
 
 
