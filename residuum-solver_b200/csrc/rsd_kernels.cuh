@@ -253,10 +253,27 @@ __device__ __forceinline__ AccT row_sum(const MatView<T>& A, int64_t row, int64_
 			if (u >= 0) {
 				const int32_t* __restrict__ op = A.offs + u;
 				const int r = (int)row;
-				run([&](int jp) {
-					const int2 o = ldh2(op + 2 * jp, pol.last);
-					return make_int2(r + o.x, r + o.y);
-				});
+				auto by_load = [&]() {
+					run([&](int jp) {
+						const int2 o = ldh2(op + 2 * jp, pol.last);
+						return make_int2(r + o.x, r + o.y);
+					});
+				};
+				if constexpr (sizeof(T) == 4) {
+					// FP32 values: a stencil slice fills the warp, so lane k holds pattern entry k (read once
+					// per slice) and the offsets come by shuffle instead of a load per pair (for FP64 values
+					// the extra register spills under the 32-register budget, so those keep the loads)
+					if (npair <= 16) {
+						const int mine = __ldg(op + min((int)(row & 31), 2 * npair - 1));
+						run([&](int jp) {
+							return make_int2(r + __shfl_sync(0xffffffffu, mine, 2 * jp), r + __shfl_sync(0xffffffffu, mine, 2 * jp + 1));
+						});
+					} else {
+						by_load();
+					}
+				} else {
+					by_load();
+				}
 			} else if constexpr (L < 0) {
 				const int cb = A.base[sl];
 				const uint16_t* __restrict__ cp16 = A.col16 + q0;
