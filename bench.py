@@ -675,10 +675,11 @@ def main():
     it_64 = [r["iterations"] for r in reps_64]
     solve_mx = sum(prof_mx[f][1] for f in ("spmv_dot_f32", "cg_update", "cg_pupdate", "reliable_update")) / args.steps
     solve_64 = sum(prof_64[f][1] for f in ("spmv_dot_f64", "cg_update", "cg_pupdate")) / args.steps
-    # kernels run in the timed mixed steps: per step 9 outside the solve (Udot, K + M/dt, right-hand side,
-    # lift, FP32 value copy, inverse diagonal, initial residual, stage residual, its norm), per CG
-    # iteration 3 (SpMV + p.Ap, update, p update) and one per FP64 residual replacement
-    gpu_launches = int(sum(9 + 3 * r["iterations"] + r["refinements"] for r in reps_mx))
+    # kernels run in the timed mixed steps: per step 8 outside the solve (Udot, K + M/dt with its FP32
+    # copy, right-hand side, lift, inverse diagonal, initial residual, stage residual, its norm); in the
+    # solve 2 per loop body (SpMV + z.Az, vector pass) and 2 per replacement node (fold, FP64
+    # residual), with one idle body and replacement node after the converged one
+    gpu_launches = int(sum(8 + 2 * (r["iterations"] + 1) + 2 * (r["refinements"] + 1) for r in reps_mx))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

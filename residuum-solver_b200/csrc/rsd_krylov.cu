@@ -27,7 +27,7 @@ constexpr int kST = 512;
 constexpr int kVT = 1024;
 
 struct CgScal {
-	double rz, pAp, alpha, beta, res0, res, rel, rmax, res64, trueRel;
+	double rz, pAp, alpha, beta, res0, res, rhoPrev, rmax, res64, trueRel;   // mixed: rhoPrev = previous r.z
 	double dcur;                      // mixed: current replacement threshold
 	int64_t iter;
 	int32_t refinements, done, converged, reliable, status, pad0, pad;
@@ -83,11 +83,11 @@ __global__ void __launch_bounds__(256) k_cg_init(int64_t n, MatView<double> A, c
 	}
 	if (grid_sum<2>(v, partials, &S->ticket)) {
 		const double res0 = sqrt(v[0]);
-		S->res0 = res0; S->rz = v[1]; S->iter = 0; S->res = res0; S->rel = 1.0;
+		S->res0 = res0; S->rz = v[1]; S->iter = 0; S->res = res0;
 		S->refinements = 0; S->reliable = 0; S->status = 0;
 		const double crit = relMode ? res0 / (res0 + 1e-50) : res0;
 		if (crit < tol) { S->done = 1; S->converged = 1; }
-		else if (maxIters <= 1) { S->done = 1; S->converged = 0; S->iter = maxIters; S->rel = res0 / (res0 + 1e-50); }
+		else if (maxIters <= 1) { S->done = 1; S->converged = 0; S->iter = maxIters; }
 		else { S->done = 0; S->converged = 0; }
 	}
 }
@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(kVT) k_cg_update(int64_t n, double* __restrict
 		const int64_t k = S->iter + 1;
 		const double res = sqrt(v[0]);
 		const double rel = res / (S->res0 + 1e-50);
-		S->res = res; S->rel = rel; S->iter = k;
+		S->res = res; S->iter = k;
 		const double crit = relMode ? rel : res;
 		if (!isfinite(res)) { S->done = 1; S->converged = 0; S->status = RSD_ENAN; }
 		else if (crit < tol) { S->done = 1; S->converged = 1; }
@@ -187,10 +187,11 @@ __global__ void __launch_bounds__(kVT) k_cg_pupdate(int64_t n, double* __restric
 // residual drops by `delta` since the last replacement, or claims convergence, the FP32
 // correction y is folded into x (x += y, y = 0) and the true residual r = b - A64 x is recomputed
 // in FP64 to replace the recurrence residual.  Convergence is declared on the FP64 residual only.
-// r0 = b - A64 x in FP64
+// The iteration is the single-reduction form (k_mx_step): one SpMV and one vector pass.
+// r0 = b - A64 x in FP64, z0 = M r0, y = 0
 template <int L>
 __global__ void __launch_bounds__(256) k_mx_init(int64_t n, MatView<double> A, const double* __restrict__ b,
-                                                 const double* __restrict__ x, float* __restrict__ r, float* __restrict__ p,
+                                                 const double* __restrict__ x, float* __restrict__ r, float* __restrict__ z,
                                                  float* __restrict__ y, const float* __restrict__ invD, CgScal* S,
                                                  double* partials, double tol, int relMode, int64_t maxIters, double delta) {
 	const L2Pol pol = make_l2pol();
@@ -203,14 +204,14 @@ __global__ void __launch_bounds__(256) k_mx_init(int64_t n, MatView<double> A, c
 			const double r64 = ldh(b + row, pol.first) - ax;
 			const float ri = (float)r64;
 			const float zi = invD ? ri * ldh(invD + row, pol.last) : ri;
-			sth(r + row, ri, pol.last); sth(p + row, zi, pol.last); sth(y + row, 0.0f, pol.last);
+			sth(r + row, ri, pol.last); sth(z + row, zi, pol.last); sth(y + row, 0.0f, pol.last);
 			v[0] += r64 * r64;
 			v[1] += (double)ri * (double)zi;
 		}
 	}
 	if (grid_sum<2>(v, partials, &S->ticket)) {
 		const double res0 = sqrt(v[0]);
-		S->res0 = res0; S->rmax = res0; S->res = res0; S->res64 = res0; S->rel = 1.0; S->trueRel = 1.0;
+		S->res0 = res0; S->rmax = res0; S->res = res0; S->res64 = res0; S->rhoPrev = 0.0; S->trueRel = 1.0;
 		S->rz = v[1]; S->iter = 0; S->refinements = 0; S->reliable = 0; S->status = 0;
 		S->dcur = delta;
 		const double crit = relMode ? res0 / (res0 + 1e-50) : res0;
@@ -220,9 +221,10 @@ __global__ void __launch_bounds__(256) k_mx_init(int64_t n, MatView<double> A, c
 	}
 }
 
+// w = A32 z and mu = z.w (FP64 sum)
 template <int L>
-__global__ void __launch_bounds__(kST, 2048 / kST) k_mx_spmv_dot(int64_t n, MatView<float> A, const float* __restrict__ p,
-                                                     float* __restrict__ Ap, CgScal* S, double* partials) {
+__global__ void __launch_bounds__(kST, 2048 / kST) k_mx_spmv_dot(int64_t n, MatView<float> A, const float* __restrict__ z,
+                                                     float* __restrict__ w, CgScal* S, double* partials) {
 	if (is_done(S)) return;
 	if (blockIdx.x == 0 && threadIdx.x == 0) S->reliable = 0;
 	const L2Pol pol = make_l2pol();
@@ -230,45 +232,66 @@ __global__ void __launch_bounds__(kST, 2048 / kST) k_mx_spmv_dot(int64_t n, MatV
 	double v[1] = {0.0};
 	for (int64_t base = rl.base; base < n; base += rl.step) {
 		const int64_t row = base + rl.sub;
-		const float s = row_dot<L, float, float>(A, p, row, n, rl.lane, pol);
-		if (rl.lane == 0 && row < n) { sth(Ap + row, s, pol.last); v[0] += (double)ldh(p + row, pol.last) * (double)s; }
+		const float s = row_dot<L, float, float>(A, z, row, n, rl.lane, pol);
+		if (rl.lane == 0 && row < n) { sth(w + row, s, pol.last); v[0] += (double)ldh(z + row, pol.last) * (double)s; }
 	}
-	if (grid_sum<1>(v, partials, &S->ticket)) {
-		S->pAp = v[0];
-		S->alpha = S->rz / v[0];
-		if (!isfinite(S->alpha)) { S->done = 1; S->converged = 0; S->status = RSD_EBREAKDOWN; }
-	}
+	if (grid_sum<1>(v, partials, &S->ticket)) S->pAp = v[0];
 }
 
-__global__ void __launch_bounds__(kVT) k_mx_update(int64_t n, float* __restrict__ y, float* __restrict__ r,
-                                                   const float* __restrict__ p, const float* __restrict__ Ap,
-                                                   const float* __restrict__ invD, CgScal* S, double* partials, double tol,
-                                                   int relMode, int64_t maxIters, GraphCtl gc) {
+// The vector pass of the single-reduction iteration (Chronopoulos & Gear 1989): with rho = r.z,
+// mu = z.Az and the previous rho and alpha on the device, beta = rho / rho_prev and
+// alpha = rho / (mu - beta rho / alpha_prev) (the first pass: beta = 0, alpha = rho / mu); then
+// p = z + beta p, s = w + beta s (s = A p by recurrence, w = A z), y += alpha p, r -= alpha s,
+// z = M r, and rho = r.z and |r| in one reduction.  In exact arithmetic these are the iterates of
+// the two-reduction PCG; the pass replaces its update and p-update kernels and one grid-wide
+// reduction per iteration.  In graph mode its first thread also sets the loop condition from the
+// done flag as the previous body left it (replacement included), so a solve ends one idle body after
+// the body that finished it, with no extra node per iteration.
+__global__ void __launch_bounds__(kVT) k_mx_step(int64_t n, float* __restrict__ y, float* __restrict__ r,
+                                                 float* __restrict__ z, float* __restrict__ p, float* __restrict__ s,
+                                                 const float* __restrict__ w, const float* __restrict__ invD, CgScal* S,
+                                                 double* partials, double tol, int relMode, int64_t maxIters, GraphCtl gc) {
+	if (gc.on && blockIdx.x == 0 && threadIdx.x == 0) graph_continue(S, gc);
 	if (is_done(S)) return;
-	const float alpha = (float)S->alpha;
+	const double rho = S->rz, mu = S->pAp, rhoPrev = S->rhoPrev;
+	const bool first = !(rhoPrev != 0.0);
+	const double beta = first ? 0.0 : rho / rhoPrev;
+	const double alpha = first ? rho / mu : rho / (mu - beta * rho / S->alpha);
+	const float fa = (float)alpha, fb = (float)beta;
 	const L2Pol pol = make_l2pol();
 	const uint64_t h = pol.last;
 	double v[2] = {0.0, 0.0};
-	packet_loop<float>(n, true, [&](int64_t i, int w) {
-		if (w > 1) {
-			Pk<float> Y = ldp_rw(y + i, h), P = ldp(p + i, h), R = ldp_rw(r + i, h), Q = ldp(Ap + i, h), D;
+	packet_loop<float>(n, true, [&](int64_t i, int wd) {
+		if (wd > 1) {
+			Pk<float> Z = ldp_rw(z + i, h), W = ldp(w + i, h), Y = ldp_rw(y + i, h), R = ldp_rw(r + i, h), P, Q, D;
+			if (first) { P = Z; Q = W; }
+			else {
+				P = ldp_rw(p + i, h); Q = ldp_rw(s + i, h);
+#pragma unroll
+				for (int k = 0; k < Pk<float>::W; ++k) { P.v[k] = Z.v[k] + fb * P.v[k]; Q.v[k] = W.v[k] + fb * Q.v[k]; }
+			}
 			if (invD) D = ldp(invD + i, h);
 #pragma unroll
 			for (int k = 0; k < Pk<float>::W; ++k) {
-				Y.v[k] = Y.v[k] + alpha * P.v[k];
-				const float ri = R.v[k] - alpha * Q.v[k];
+				Y.v[k] = Y.v[k] + fa * P.v[k];
+				const float ri = R.v[k] - fa * Q.v[k];
 				R.v[k] = ri;
 				const float zi = invD ? ri * D.v[k] : ri;
+				Z.v[k] = zi;
 				v[0] += (double)ri * (double)ri;
 				v[1] += (double)ri * (double)zi;
 			}
-			stp(y + i, Y, h);
-			stp(r + i, R, h);
+			stp(p + i, P, h); stp(s + i, Q, h); stp(y + i, Y, h); stp(r + i, R, h); stp(z + i, Z, h);
 		} else {
-			sth(y + i, ldh_rw(y + i, h) + alpha * ldh(p + i, h), h);
-			const float ri = ldh_rw(r + i, h) - alpha * ldh(Ap + i, h);
+			const float zo = ldh_rw(z + i, h), wo = ldh(w + i, h);
+			const float pi = first ? zo : zo + fb * ldh_rw(p + i, h);
+			const float si = first ? wo : wo + fb * ldh_rw(s + i, h);
+			sth(p + i, pi, h); sth(s + i, si, h);
+			sth(y + i, ldh_rw(y + i, h) + fa * pi, h);
+			const float ri = ldh_rw(r + i, h) - fa * si;
 			sth(r + i, ri, h);
 			const float zi = invD ? ri * ldh(invD + i, h) : ri;
+			sth(z + i, zi, h);
 			v[0] += (double)ri * (double)ri;
 			v[1] += (double)ri * (double)zi;
 		}
@@ -277,12 +300,12 @@ __global__ void __launch_bounds__(kVT) k_mx_update(int64_t n, float* __restrict_
 		const int64_t k = S->iter + 1;
 		const double res = sqrt(v[0]);
 		S->res = res; S->iter = k;
-		const double crit = relMode ? res / (S->res0 + 1e-50) : res;
-		if (!isfinite(res)) { S->done = 1; S->converged = 0; S->status = RSD_ENAN; return; }
-		if (crit < tol || res < S->dcur * S->rmax || k + 1 >= maxIters) {
-			S->reliable = 1;                    // FP64 residual replacement next
-		} else {
-			S->beta = v[1] / S->rz; S->rz = v[1];
+		if (!isfinite(alpha)) { S->done = 1; S->converged = 0; S->status = RSD_EBREAKDOWN; }
+		else if (!isfinite(res)) { S->done = 1; S->converged = 0; S->status = RSD_ENAN; }
+		else {
+			S->alpha = alpha; S->beta = beta; S->rhoPrev = rho; S->rz = v[1];
+			const double crit = relMode ? res / (S->res0 + 1e-50) : res;
+			if (crit < tol || res < S->dcur * S->rmax || k + 1 >= maxIters) S->reliable = 1;   // FP64 replacement next
 		}
 		if (gc.on) cudaGraphSetConditional(gc.hr, S->reliable ? 1u : 0u);
 	}
@@ -299,11 +322,12 @@ __global__ void __launch_bounds__(kVT) k_mx_fold(int64_t n, double* __restrict__
 	}
 }
 
-// reliable update (after the fold): r64 = b - A64 x, r = (float) r64, rz with the new r
+// reliable update (after the fold): r64 = b - A64 x, r = (float) r64, z = M r, rho = r.z with the new
+// r (p, s and the previous rho and alpha carry on)
 template <int L>
 __global__ void __launch_bounds__(kST, 2048 / kST) k_mx_reliable(int64_t n, MatView<double> A, const double* __restrict__ b,
                                                      const double* __restrict__ x, float* __restrict__ r,
-                                                     const float* __restrict__ invD, CgScal* S, double* partials,
+                                                     float* __restrict__ z, const float* __restrict__ invD, CgScal* S, double* partials,
                                                      double tol, int relMode, int64_t maxIters, int adaptive) {
 	if (is_done(S) || !*((volatile const int32_t*)&S->reliable)) return;
 	const L2Pol pol = make_l2pol();
@@ -317,6 +341,7 @@ __global__ void __launch_bounds__(kST, 2048 / kST) k_mx_reliable(int64_t n, MatV
 			const float ri = (float)r64;
 			const float zi = invD ? ri * ldh(invD + row, pol.last) : ri;
 			sth(r + row, ri, pol.last);
+			sth(z + row, zi, pol.last);
 			v[0] += r64 * r64;
 			v[1] += (double)ri * (double)zi;
 		}
@@ -325,37 +350,14 @@ __global__ void __launch_bounds__(kST, 2048 / kST) k_mx_reliable(int64_t n, MatV
 		const double res = sqrt(v[0]);
 		const double rel = res / (S->res0 + 1e-50);
 		if (adaptive) S->dcur = next_delta(S->dcur, S->res, res);
-		S->res64 = res; S->trueRel = rel; S->rmax = res; S->res = res; S->rel = rel;
+		S->res64 = res; S->trueRel = rel; S->rmax = res; S->res = res;
 		S->refinements += 1;
 		const double crit = relMode ? rel : res;
 		if (!isfinite(res)) { S->done = 1; S->converged = 0; S->status = RSD_ENAN; }
 		else if (crit < tol) { S->done = 1; S->converged = 1; }
 		else if (S->iter + 1 >= maxIters) { S->done = 1; S->converged = 0; S->iter = maxIters; }
-		else { S->beta = v[1] / S->rz; S->rz = v[1]; }
+		else S->rz = v[1];
 	}
-}
-
-// p = beta p + z
-__global__ void __launch_bounds__(kVT) k_mx_pupdate(int64_t n, float* __restrict__ p, const float* __restrict__ r,
-                                                    const float* __restrict__ invD, CgScal* S, GraphCtl gc) {
-	if (gc.on && blockIdx.x == 0 && threadIdx.x == 0) graph_continue(S, gc);
-	if (is_done(S)) return;
-	const float beta = (float)S->beta;
-	const L2Pol pol = make_l2pol();
-	const uint64_t h = pol.last;
-	packet_loop<float>(n, true, [&](int64_t i, int w) {   // the next SpMV gathers p
-		if (w > 1) {
-			Pk<float> P = ldp_rw(p + i, h), R = ldp(r + i, h), D;
-			if (invD) D = ldp(invD + i, h);
-#pragma unroll
-			for (int k = 0; k < Pk<float>::W; ++k) P.v[k] = P.v[k] * beta + (invD ? R.v[k] * D.v[k] : R.v[k]);
-			stp(p + i, P, h);
-		} else {
-			const float ri = ldh(r + i, h);
-			const float zi = invD ? ri * ldh(invD + i, h) : ri;
-			sth(p + i, ldh_rw(p + i, h) * beta + zi, h);
-		}
-	});
 }
 
 __global__ void k_invdiag32(int64_t n, const int32_t* __restrict__ dpos, const double* __restrict__ val, float* __restrict__ d) {
@@ -699,11 +701,13 @@ static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const d
 	const MatView<float> V32 = view32(A);
 	void* wsv;
 	const int64_t ns = pad_len(n);
-	RSD_CHECK(get_ws(ctx, sizeof(float) * 5 * ns, &wsv));
+	RSD_CHECK(get_ws(ctx, sizeof(float) * 7 * ns, &wsv));
 	float* r = (float*)wsv;
-	float* p = r + ns;
-	float* Ap = p + ns;
-	float* y = Ap + ns;
+	float* z = r + ns;       // M r, the vector the SpMV multiplies
+	float* p = z + ns;
+	float* sv = p + ns;      // A p, by recurrence
+	float* w = sv + ns;      // A z
+	float* y = w + ns;
 	float* invD = cfg->precond == RSD_JACOBI ? y + ns : nullptr;
 	CgScal* S = scal_slot(ctx, 0);
 	double* partials = ctx->s.partials;
@@ -717,27 +721,30 @@ static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const d
 	auto prologue = [&]() -> int {
 		RSD_CUDA(cudaMemsetAsync(S, 0, sizeof(CgScal), st));
 		if (invD) k_invdiag32<<<VG(k_invdiag32), 256, 0, st>>>(n, exec_diag(A), exec_val(A), invD);
-		RSD_DISPATCH_L(L, (k_mx_init<LL><<<RG(k_mx_init<LL>), 256, 0, st>>>(n, V, b, x, r, p, y, invD, S, partials, tol, rel, maxIt, delta)));
+		RSD_DISPATCH_L(L, (k_mx_init<LL><<<RG(k_mx_init<LL>), 256, 0, st>>>(n, V, b, x, r, z, y, invD, S, partials, tol, rel, maxIt, delta)));
 		RSD_CUDA(cudaGetLastError());
 		return RSD_OK;
 	};
+	// one iteration: w = A z with mu = z.w, then the single-reduction vector pass
+	auto spmv = [&]() {
+		RSD_DISPATCH_L(L, (k_mx_spmv_dot<LL><<<RGB(k_mx_spmv_dot<LL>, kST), kST, 0, st>>>(n, V32, z, w, S, partials)));
+	};
+	auto step = [&](GraphCtl gc) {
+		k_mx_step<<<VGB(k_mx_step, kVT), kVT, 0, st>>>(n, y, r, z, p, sv, w, invD, S, partials, tol, rel, maxIt, gc);
+	};
 	auto body_a = [&](GraphCtl gc) -> int {
-		RSD_DISPATCH_L(L, (k_mx_spmv_dot<LL><<<RGB(k_mx_spmv_dot<LL>, kST), kST, 0, st>>>(n, V32, p, Ap, S, partials)));
-		k_mx_update<<<VGB(k_mx_update, kVT), kVT, 0, st>>>(n, y, r, p, Ap, invD, S, partials, tol, rel, maxIt, gc);
+		spmv();
+		step(gc);
 		RSD_CUDA(cudaGetLastError());
 		return RSD_OK;
 	};
 	auto reliable = [&]() -> int {
 		k_mx_fold<<<VGB(k_mx_fold, kVT), kVT, 0, st>>>(n, x, y, S);
-		RSD_DISPATCH_L(L, (k_mx_reliable<LL><<<RGB(k_mx_reliable<LL>, kST), kST, 0, st>>>(n, V, b, x, r, invD, S, partials, tol, rel, maxIt, adaptive)));
+		RSD_DISPATCH_L(L, (k_mx_reliable<LL><<<RGB(k_mx_reliable<LL>, kST), kST, 0, st>>>(n, V, b, x, r, z, invD, S, partials, tol, rel, maxIt, adaptive)));
 		RSD_CUDA(cudaGetLastError());
 		return RSD_OK;
 	};
-	auto body_b = [&](GraphCtl gc) -> int {
-		k_mx_pupdate<<<VGB(k_mx_pupdate, kVT), kVT, 0, st>>>(n, p, r, invD, S, gc);
-		RSD_CUDA(cudaGetLastError());
-		return RSD_OK;
-	};
+	auto body_b = [&](GraphCtl) -> int { return RSD_OK; };   // the step kernel sets the loop condition
 	if (graph_mode(ctx)) {
 		CgGraph& G = graph_cache(ctx)->cg[1];
 		CgKey key{};
@@ -764,24 +771,21 @@ static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const d
 		for (int64_t it = 0; it < maxIt + 2 * chunk && !fin; it += chunk) {
 			for (int c = 0; c < chunk; ++c) {
 				int pr = prof_begin(ctx, PF_SPMV_DOT_F32);
-				RSD_DISPATCH_L(L, (k_mx_spmv_dot<LL><<<RGB(k_mx_spmv_dot<LL>, kST), kST, 0, st>>>(n, V32, p, Ap, S, partials)));
+				spmv();
 				prof_end(ctx, pr);
 				int pu = prof_begin(ctx, PF_CG_UPDATE);
-				k_mx_update<<<VGB(k_mx_update, kVT), kVT, 0, st>>>(n, y, r, p, Ap, invD, S, partials, tol, rel, maxIt, off);
+				step(off);
 				prof_end(ctx, pu);
 				int pq = prof_begin(ctx, PF_RELIABLE);
 				RSD_CHECK(reliable());
 				prof_end(ctx, pq);
-				int pp = prof_begin(ctx, PF_CG_PUPDATE);
-				k_mx_pupdate<<<VGB(k_mx_pupdate, kVT), kVT, 0, st>>>(n, p, r, invD, S, off);
-				prof_end(ctx, pp);
-				if (pr >= 0) { pairs.push_back(pr); pairs.push_back(pu); pairs.push_back(pq); pairs.push_back(pp); }
+				if (pr >= 0) { pairs.push_back(pr); pairs.push_back(pu); pairs.push_back(pq); }
 			}
 			RSD_CUDA(cudaGetLastError());
 			RSD_CHECK(poll.post(&fin));
 		}
 		RSD_CHECK(finish_report(ctx, S, rep));
-		discard_idle(ctx, pairs, 4, rep ? rep->iterations : 0);
+		discard_idle(ctx, pairs, 3, rep ? rep->iterations : 0);
 	}
 	if (rep) { rep->finalResidual = rep->trueResidualRel * rep->initialResidual; rep->finalResidualRel = rep->trueResidualRel; }
 	return RSD_OK;
