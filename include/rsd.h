@@ -68,7 +68,8 @@ typedef struct rsd_solver_cfg {
 	int64_t max_iters;
 	int64_t krylov_dim;          /* GMRES restart length m */
 	double reliable_delta;       /* mixed CG: FP64 residual replacement when |r| falls by this factor; 0: adaptive,
-	                                from 0.1, set at each replacement from the recurrence/true residual gap, in [1e-3, 0.1] */
+	                                from 0.1, set at each replacement from the recurrence/true residual gap, in [1e-4, 0.1]
+	                                (the batched solver: [1e-3, 0.1]) */
 } rsd_solver_cfg;
 
 /* ---- lifetime (linalg/types/backend/CUDA.hpp:23-73 has no context; these give it one) ---- */

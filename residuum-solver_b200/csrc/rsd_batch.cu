@@ -164,7 +164,7 @@ __device__ void solve_one(const BatchProb<TI>& P, BatchOut* out, double tol, int
 			for (int64_t i = tid; i < n; i += kBT) { x[i] += (double)y[i]; y[i] = (TI)0; }
 			const double recurrence = res;
 			res = sqrt(v[0]);
-			if (adaptive) delta = next_delta(delta, recurrence, res);
+			if (adaptive) delta = next_delta(delta, recurrence, res, kDeltaFloorBatch);
 			rmax = res;
 			trueRel = res / (res0 + 1e-50);
 			rzNew = v[1];

@@ -320,11 +320,13 @@ struct RowLoop {
 // from the true one by roughly eps32 * cond(A) * ||A|| ||x|| whatever the current residual is, so its
 // relative error grows in proportion to the reduction since the last replacement.  With d the
 // relative gap seen at this replacement (threshold delta), the threshold that keeps the next gap
-// near 1% is 100 d delta, kept within [1e-3, 0.1]: well-conditioned systems replace rarely,
-// ill-conditioned ones often.
-__host__ __device__ __forceinline__ double next_delta(double delta, double recurrence, double true_res) {
+// near 1% is 100 d delta, kept within [lo, 0.1]: well-conditioned systems replace rarely,
+// ill-conditioned ones often.  The floor is the solver's (measured): the single CG solve takes
+// kDeltaFloorCg, the batched solver kDeltaFloorBatch, where a lower floor cost iterations.
+constexpr double kDeltaFloorCg = 1e-4, kDeltaFloorBatch = 1e-3;
+__host__ __device__ __forceinline__ double next_delta(double delta, double recurrence, double true_res, double lo) {
 	const double d = fabs(recurrence - true_res) / fmax(true_res, 1e-300);
-	return fmin(0.1, fmax(1e-3, 100.0 * d * delta));
+	return fmin(0.1, fmax(lo, 100.0 * d * delta));
 }
 
 // expression stack machine (bytecode from compile_expr)

@@ -349,7 +349,7 @@ __global__ void __launch_bounds__(kST, 2048 / kST) k_mx_reliable(int64_t n, MatV
 	if (grid_sum<2>(v, partials, &S->ticket)) {
 		const double res = sqrt(v[0]);
 		const double rel = res / (S->res0 + 1e-50);
-		if (adaptive) S->dcur = next_delta(S->dcur, S->res, res);
+		if (adaptive) S->dcur = next_delta(S->dcur, S->res, res, kDeltaFloorCg);
 		S->res64 = res; S->trueRel = rel; S->rmax = res; S->res = res;
 		S->refinements += 1;
 		const double crit = relMode ? rel : res;
