@@ -694,6 +694,27 @@ def main():
         except Exception as e:  # noqa: BLE001
             cpu = {"value": None, "unit": "ms", "cores": 1, "kind": "reference", "sample": f"failed: {e}"}
 
+    # element assembly roofline of K + M/dt (the survey's accounting): bytes = CSR values written
+    # once + coordinates + connectivity, flops = E nq npe^2 (2d + 2) diffusion + E nq npe^2 3 mass,
+    # against the measured HBM copy peak and the measured FP64 FMA rate; the bound that binds is the
+    # larger time
+    import ctypes
+    fp64 = ctypes.c_double()
+    rsd.check(rsd.lib().rsd_measure_fp64_rate(ctx.h, ctypes.byref(fp64)))
+    n_elem, n_nodes = S ** 3, (S + 1) ** 3
+    asm_bytes = nnz * 8 + n_nodes * 3 * 8 + n_elem * 8 * 4
+    asm_flops = n_elem * 8 * 64 * (2 * 3 + 2 + 3)
+    t_hbm = asm_bytes / (peak * 1e9) * 1e3
+    t_fp64 = asm_flops / (fp64.value * 1e12) * 1e3
+    asm_ms = prof_mx["assemble_matrix"][1] / max(prof_mx["assemble_matrix"][0], 1) if "assemble_matrix" in prof_mx else None
+    asm_roof = {"kernel": "k_asm_matrix_rows (K + M/dt, one launch per step)", "bytes": asm_bytes, "flops": asm_flops,
+                "hbm_ms": t_hbm, "fp64_ms": t_fp64, "bound": "fp64" if t_fp64 > t_hbm else "hbm",
+                "roofline_ms": max(t_hbm, t_fp64), "achieved_ms": asm_ms,
+                "frac": max(t_hbm, t_fp64) / asm_ms if asm_ms else None,
+                "fp64_tflops": fp64.value, "fp64_peak_kind": "measured (FMA chains, rsd_measure_fp64_rate)",
+                "note": "flops as the quadrature form counts them; affine elements take the same integrals from "
+                        "reference-element tables with about a tenth of those flops"}
+
     line = {
         "metric": METRIC, "value": ms_mx, "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_mx, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
@@ -716,6 +737,7 @@ def main():
                      "avg_launch_us": avg_ms * 1e3, "launches": launches, "traffic": traffic,
                      "fp64_spmv": {"achieved": achieved64, "frac": achieved64 / peak if achieved64 else None,
                                    "algorithmic_bytes": bytes_spmv64, "avg_launch_us": 1e3 * t64 / max(l64, 1)}},
+        "assembly_roofline": asm_roof,
         "kernel_ms_per_step": {k: v[1] / args.steps for k, v in prof_mx.items()},
         "kernel_ms_per_step_fp64": {k: v[1] / args.steps for k, v in prof_64.items()},
         "clocks_fp64": clk64,

@@ -133,6 +133,10 @@ int rsd_jacobi_setup(rsd_ctx* ctx, const rsd_csr* A, double* inv_diag);
  * 0 for the default.  The autotuner times every choice and keeps the fastest. */
 int rsd_csr_set_launch(rsd_csr* A, int32_t lanes_per_row, int32_t block_threads);
 int rsd_csr_autotune(rsd_ctx* ctx, rsd_csr* A, int32_t* lanes_per_row, int32_t* block_threads, double* best_us);
+/* Measured FP64 FMA throughput of the device (non-tensor pipe), in TFLOP/s, for the element
+ * assembly's roofline: independent FMA chains on every SM, timed with CUDA events.  No counterpart
+ * in the reference (a measurement helper). */
+int rsd_measure_fp64_rate(rsd_ctx* ctx, double* tflops);
 
 /* ---- Krylov solves: CGRunner / GMRESRunner::solve (linalg/solver/iterative/cg/Solver.tpp:13-119,
  *      gmres/Solver.tpp:3-170) through LinearSolverRunner::solve(b, x, report)

@@ -95,6 +95,7 @@ SIGNATURES = {
     "rsd_jacobi_setup": [_P, _P, _P],
     "rsd_csr_set_launch": [_P, _I32, _I32],
     "rsd_csr_autotune": [_P, _P, C.POINTER(_I32), C.POINTER(_I32), C.POINTER(_D)],
+    "rsd_measure_fp64_rate": [_P, C.POINTER(_D)],
     "rsd_solve": [_P, _P, C.POINTER(SolverConfig), _P, _P, C.POINTER(Report)],
     "rsd_cg_solve_static": [_P, _P, C.POINTER(SolverConfig), _P, _P, C.POINTER(Report)],
     "rsd_mesh_create": [_P, _I32, _I32, _I64, _I64, _P, _P, _P, C.POINTER(_P)],

@@ -294,6 +294,49 @@ int rsd_csr_lump(rsd_ctx* c, const rsd_csr* Ac, double* d) {
 	return RSD_OK;
 }
 
+}  // extern "C" (reopened below)
+
+namespace rsd {
+// eight independent FMA chains per thread; the sum is stored only under a condition the host never
+// meets, so that the chains are not removed
+__global__ void __launch_bounds__(256) k_fma64(double* out, int iters, double a, double b) {
+	double x[8];
+#pragma unroll
+	for (int k = 0; k < 8; ++k) x[k] = 1.0 + 1e-3 * (threadIdx.x + k);
+	for (int i = 0; i < iters; ++i)
+#pragma unroll
+		for (int k = 0; k < 8; ++k) x[k] = fma(x[k], a, b);
+	double s = 0.0;
+#pragma unroll
+	for (int k = 0; k < 8; ++k) s += x[k];
+	if (s == -1.0) out[0] = s;
+}
+}  // namespace rsd
+
+extern "C" {
+
+int rsd_measure_fp64_rate(rsd_ctx* c, double* tflops) {
+	if (!c || !tflops) return set_error(RSD_EINVAL, "null argument");
+	const int iters = 4096, threads = 256, blocks = c->num_sms * 8;
+	cudaEvent_t e0, e1;
+	RSD_CUDA(cudaEventCreate(&e0));
+	RSD_CUDA(cudaEventCreate(&e1));
+	float best = 1e30f;
+	for (int rep = 0; rep < 4; ++rep) {
+		RSD_CUDA(cudaEventRecord(e0, c->stream));
+		k_fma64<<<blocks, threads, 0, c->stream>>>(c->s.partials, iters, 0.9999999, 1e-9);
+		RSD_CUDA(cudaEventRecord(e1, c->stream));
+		RSD_CUDA(cudaEventSynchronize(e1));
+		float ms = 0.0f;
+		RSD_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+		if (rep > 0) best = std::min(best, ms);   // the first launch warms up
+	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	*tflops = 2.0 * 8.0 * iters * (double)threads * blocks / (best * 1e-3) / 1e12;
+	return RSD_OK;
+}
+
 // SpMV launch autotuner: times SELL-32 and CSR-vector with 2..32 lanes per row, each at 128, 256
 // and 512 threads per block, with CUDA events (median of 5 launches after 2 warm-ups), and keeps
 // the fastest in A's launch settings.
