@@ -296,7 +296,50 @@ def ranks_reduce(value, op, dist, device):
     return float(t.item())
 
 
-def run_batch(rsd, ctx, stream, count, reps, peak, rank=0, world=1, dist=None, device="cuda"):
+def _batch_cpu_worker(ps):
+    """One process of the batched workload's CPU baseline: problems `ps` through the reference's own
+    templates (oracle/_ref), each assembled (untimed) and then solved by the reference's FP64
+    CG + Jacobi to 1e-8 from x0 = 0 (timed).  Returns (solve seconds, iterations)."""
+    import oracle
+    solve_s, iters = 0.0, 0
+    for p in ps:
+        nx, ny, ke = batch_problem(p)
+        r = oracle.Reference(2, 1, 2, [nx, ny], [0, 0], [1, 1], [0, 1, 2, 3], bc_kind=0, src_kind=0, src_c=1.0, k_elem=ke)
+        val = r.assemble_matrix("K")
+        F = r.assemble_vector(0)
+        rp, col = r.pattern()
+        t0 = time.perf_counter()
+        _, rep = oracle.ref_csr_solve(rp, col, val, F, tol=1e-8, maxit=100000)
+        solve_s += time.perf_counter() - t0
+        iters += int(rep["iterations"])
+    return solve_s, iters
+
+
+def batch_cpu_baseline(count):
+    """The reference CPU solver over the whole batch with P = min(cores, 32) spawned processes (the
+    reference is single-threaded), each taking every P-th problem of the largest-first order: the
+    slowest process's solve seconds are the time for the batch at P cores."""
+    import multiprocessing as mp
+    import oracle
+    if not oracle.reference_available():
+        return None
+    rows = []
+    for p in range(count):
+        head = uniforms(mt19937_64_stream(4000 + p, 2))
+        nx, ny = (32 + int(u * 225) for u in head)
+        rows.append(((nx - 1) * (ny - 1), p))
+    order = [p for _, p in sorted(rows, key=lambda t: (-t[0], t[1]))]
+    procs = max(1, min(os.cpu_count() or 1, 32))
+    with mp.get_context("spawn").Pool(procs) as pool:
+        res = pool.map(_batch_cpu_worker, [order[i::procs] for i in range(procs)])
+    slowest = max(t for t, _ in res)
+    return {"value": 1e3 * slowest, "unit": "ms", "cores": procs, "kind": "reference",
+            "problems_per_s": count / slowest, "iterations_total": int(sum(i for _, i in res)),
+            "sample": f"all {count} problems, FP64 CG + Jacobi to 1e-8 through the reference templates "
+                      f"(oracle/_ref), {procs} spawned processes, solve time of the slowest (assembly untimed)"}
+
+
+def run_batch(rsd, ctx, stream, count, reps, peak, rank=0, world=1, dist=None, device="cuda", cpu=False):
     """The batched workload: `count` unit-square Q1 problems (Nx, Ny ~ U{32..256}, log-normal
     per-element conductivity, unit source, T = 0 on the boundary) solved together by
     rsd_batch_solve, CG + Jacobi to 1e-8 (mixed: FP64-checked), x0 = 0.  With several ranks each
@@ -356,10 +399,34 @@ def run_batch(rsd, ctx, stream, count, reps, peak, rank=0, world=1, dist=None, d
                     "algorithmic_gbs": byts / (ms * 1e-3) / 1e9,
                     "frac_of_measured_hbm": byts / (ms * 1e-3) / 1e9 / (peak * world)}
     out["speedup_mixed_vs_fp64"] = out["fp64"]["ms"] / out["mixed"]["ms"]
+    if cpu and rank == 0 and world == 1:
+        try:
+            out["cpu_baseline"] = batch_cpu_baseline(count)
+        except Exception as e:  # noqa: BLE001
+            out["cpu_baseline"] = {"value": None, "sample": f"failed: {e}"}
     out["how"] = ("one rsd_batch_solve call (one persistent launch), CUDA events around the call, median of "
                   f"{reps}; setup (meshes, patterns, assembly) outside the timed region")
     del B
     return out
+
+
+def newton_cpu_baseline(rsd, ctx, stream, m):
+    """The reference's own Newton (oracle/_ref: its NewtonRunner over SteadyStage with GMRES(30) +
+    Jacobi, 1 core) on an m^3 Q2 sample of the Newton workload, beside this library's Newton on the
+    same sample."""
+    import oracle
+    if not oracle.reference_available():
+        return None
+    r = oracle.Reference(3, 2, 3, [m] * 3, [0, 0, 0], [1, 1, 1], [0, 1], bc_kind=0, bc_val={0: 0.0, 1: 1.0},
+                         src_kind=0, src_c=10.0, k_a=1.0, k_b=0.5)
+    t0 = time.perf_counter()
+    _, rep = r.newton(1e-10, 1e-10, 50, solver=1, precond=1, tol=1e-12, lin_maxit=100000, krylov=30)
+    cpu_ms = 1e3 * (time.perf_counter() - t0)
+    dev = run_newton(rsd, ctx, stream, m)
+    return {"value": cpu_ms, "unit": "ms", "cores": 1, "kind": "reference", "newton_iterations": rep["iterations"],
+            "device_same_sample_ms": {"fp64": dev["fp64"]["ms"], "mixed": dev["mixed"]["ms"]},
+            "sample": f"the whole Newton solve on {m}^3 Q2 hexes ({r.n} rows) through the reference templates "
+                      f"(oracle/_ref), 1 core; the device times are this library's Newton on the same mesh"}
 
 
 def run_newton(rsd, ctx, stream, S):
@@ -412,6 +479,42 @@ def fourier_theta(xyz, ien, npe, seed, modes=16, amp=0.5):
         k = 1 + np.floor(u[m, :3] * 4.0)
         th += amp * np.sin(2.0 * np.pi * (c @ k) + 2.0 * np.pi * u[m, 3])
     return th
+
+
+def adjoint_cpu_baseline(rsd, ctx, stream, m):
+    """One forward solve of the adjoint workload (k_e = exp(theta_e), f = 1, T = 0 on the boundary,
+    CG + Jacobi to 1e-13) through the reference's own SteadyStage (oracle/_ref, 1 core) on an m^3
+    sample, beside this library's forward solve on the same sample."""
+    import torch
+    import oracle
+    from importlib import import_module
+    if not oracle.reference_available():
+        return None
+    bm = import_module("residuum_solver_b200.blockmesh")
+    xyz, ien, rg = bm.block_mesh(3, [m] * 3, [0, 0, 0], [1, 1, 1], 1)
+    th = fourier_theta(xyz, ien, 8, 5)
+    r = oracle.Reference(3, 1, 2, [m] * 3, [0, 0, 0], [1, 1, 1], list(range(6)), bc_kind=0, src_kind=0, src_c=1.0,
+                         k_elem=np.exp(th))
+    t0 = time.perf_counter()
+    _, rep = r.steady(solver=0, precond=1, tol=1e-13, maxit=100000)
+    cpu_ms = 1e3 * (time.perf_counter() - t0)
+    h = rsd.Heat(ctx, rsd.Mesh(ctx, 3, 1, xyz, ien, rg), 2, src_expr="1", dirichlet={t: "0" for t in range(6)})
+    cfg = rsd.SolverConfig.make(tol=1e-13, max_iters=100000)
+    theta, T = ctx.to_device(th), ctx.array(h.n)
+    ts = []
+    for _ in range(3):
+        T.zero()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        h.forward(theta, T, cfg)
+        e1.record(stream)
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return {"value": cpu_ms, "unit": "ms", "cores": 1, "kind": "reference", "cg_iterations": rep["iterations"],
+            "device_same_sample_ms": float(np.median(ts)),
+            "sample": f"one forward solve (assembly, lift, CG + Jacobi to 1e-13) on {m}^3 Q1 hexes ({r.n} rows) through "
+                      f"the reference templates (oracle/_ref), 1 core; the device time is this library's forward "
+                      f"solve on the same mesh"}
 
 
 def run_adjoint(rsd, ctx, stream, S, ndir):
@@ -628,9 +731,20 @@ def main():
 
     batch = None
     if args.batch > 0:
-        batch = run_batch(rsd, ctx, stream, args.batch, 3, measured_peak_hbm()[0], rank, world, dist, f"cuda:{local}")
+        batch = run_batch(rsd, ctx, stream, args.batch, 3, measured_peak_hbm()[0], rank, world, dist, f"cuda:{local}",
+                          cpu=not args.no_cpu)
     newton = run_newton(rsd, ctx, stream, args.newton) if args.newton > 0 else None
+    if newton is not None and rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            newton["cpu_baseline"] = newton_cpu_baseline(rsd, ctx, stream, 16)
+        except Exception as e:  # noqa: BLE001
+            newton["cpu_baseline"] = {"value": None, "sample": f"failed: {e}"}
     adjoint = run_adjoint(rsd, ctx, stream, args.adjoint, args.fd_directions) if args.adjoint > 0 else None
+    if adjoint is not None and rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            adjoint["cpu_baseline"] = adjoint_cpu_baseline(rsd, ctx, stream, 48)
+        except Exception as e:  # noqa: BLE001
+            adjoint["cpu_baseline"] = {"value": None, "sample": f"failed: {e}"}
 
     # end to end through the public API with host buffers, every step: H2D of the state from pinned
     # host memory, the step (its previous state is the state it starts from: BackwardEulerRunner::step
