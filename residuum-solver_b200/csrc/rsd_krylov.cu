@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(kVT) k_cg_pupdate(int64_t n, double* __restric
 // r0 = b - A64 x in FP64, z0 = M r0, y = 0
 template <int L>
 __global__ void __launch_bounds__(256) k_mx_init(int64_t n, MatView<double> A, const double* __restrict__ b,
-                                                 const double* __restrict__ x, float* __restrict__ r, float* __restrict__ z,
+                                                 const double* __restrict__ x, float* __restrict__ z,
                                                  float* __restrict__ y, const float* __restrict__ invD, CgScal* S,
                                                  double* partials, double tol, int relMode, int64_t maxIters, double delta) {
 	const L2Pol pol = make_l2pol();
@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(256) k_mx_init(int64_t n, MatView<double> A, c
 			const double r64 = ldh(b + row, pol.first) - ax;
 			const float ri = (float)r64;
 			const float zi = invD ? ri * ldh(invD + row, pol.last) : ri;
-			sth(r + row, ri, pol.last); sth(z + row, zi, pol.last); sth(y + row, 0.0f, pol.last);
+			sth(z + row, zi, pol.last); sth(y + row, 0.0f, pol.last);
 			v[0] += r64 * r64;
 			v[1] += (double)ri * (double)zi;
 		}
@@ -241,13 +241,14 @@ __global__ void __launch_bounds__(kST, 2048 / kST) k_mx_spmv_dot(int64_t n, MatV
 // The vector pass of the single-reduction iteration (Chronopoulos & Gear 1989): with rho = r.z,
 // mu = z.Az and the previous rho and alpha on the device, beta = rho / rho_prev and
 // alpha = rho / (mu - beta rho / alpha_prev) (the first pass: beta = 0, alpha = rho / mu); then
-// p = z + beta p, s = w + beta s (s = A p by recurrence, w = A z), y += alpha p, r -= alpha s,
-// z = M r, and rho = r.z and |r| in one reduction.  In exact arithmetic these are the iterates of
+// p = z + beta p, s = w + beta s (s = A p by recurrence, w = A z), y += alpha p, and the residual
+// update carried on z alone (Jacobi: r = D z, so z -= alpha M s and r = z / M for the sums), with
+// rho = r.z and |r| in one reduction.  In exact arithmetic these are the iterates of
 // the two-reduction PCG; the pass replaces its update and p-update kernels and one grid-wide
 // reduction per iteration.  In graph mode its first thread also sets the loop condition from the
 // done flag as the previous body left it (replacement included), so a solve ends one idle body after
 // the body that finished it, with no extra node per iteration.
-__global__ void __launch_bounds__(kVT) k_mx_step(int64_t n, float* __restrict__ y, float* __restrict__ r,
+__global__ void __launch_bounds__(kVT) k_mx_step(int64_t n, float* __restrict__ y,
                                                  float* __restrict__ z, float* __restrict__ p, float* __restrict__ s,
                                                  const float* __restrict__ w, const float* __restrict__ invD, CgScal* S,
                                                  double* partials, double tol, int relMode, int64_t maxIters, GraphCtl gc) {
@@ -263,7 +264,7 @@ __global__ void __launch_bounds__(kVT) k_mx_step(int64_t n, float* __restrict__ 
 	double v[2] = {0.0, 0.0};
 	packet_loop<float>(n, true, [&](int64_t i, int wd) {
 		if (wd > 1) {
-			Pk<float> Z = ldp_rw(z + i, h), W = ldp(w + i, h), Y = ldp_rw(y + i, h), R = ldp_rw(r + i, h), P, Q, D;
+			Pk<float> Z = ldp_rw(z + i, h), W = ldp(w + i, h), Y = ldp_rw(y + i, h), P, Q, D;
 			if (first) { P = Z; Q = W; }
 			else {
 				P = ldp_rw(p + i, h); Q = ldp_rw(s + i, h);
@@ -274,23 +275,22 @@ __global__ void __launch_bounds__(kVT) k_mx_step(int64_t n, float* __restrict__ 
 #pragma unroll
 			for (int k = 0; k < Pk<float>::W; ++k) {
 				Y.v[k] = Y.v[k] + fa * P.v[k];
-				const float ri = R.v[k] - fa * Q.v[k];
-				R.v[k] = ri;
-				const float zi = invD ? ri * D.v[k] : ri;
+				const float zi = invD ? Z.v[k] - fa * (Q.v[k] * D.v[k]) : Z.v[k] - fa * Q.v[k];
+				const float ri = invD ? zi / D.v[k] : zi;
 				Z.v[k] = zi;
 				v[0] += (double)ri * (double)ri;
 				v[1] += (double)ri * (double)zi;
 			}
-			stp(p + i, P, h); stp(s + i, Q, h); stp(y + i, Y, h); stp(r + i, R, h); stp(z + i, Z, h);
+			stp(p + i, P, h); stp(s + i, Q, h); stp(y + i, Y, h); stp(z + i, Z, h);
 		} else {
 			const float zo = ldh_rw(z + i, h), wo = ldh(w + i, h);
 			const float pi = first ? zo : zo + fb * ldh_rw(p + i, h);
 			const float si = first ? wo : wo + fb * ldh_rw(s + i, h);
 			sth(p + i, pi, h); sth(s + i, si, h);
 			sth(y + i, ldh_rw(y + i, h) + fa * pi, h);
-			const float ri = ldh_rw(r + i, h) - fa * si;
-			sth(r + i, ri, h);
-			const float zi = invD ? ri * ldh(invD + i, h) : ri;
+			const float di = invD ? ldh(invD + i, h) : 1.0f;
+			const float zi = invD ? zo - fa * (si * di) : zo - fa * si;
+			const float ri = invD ? zi / di : zi;
 			sth(z + i, zi, h);
 			v[0] += (double)ri * (double)ri;
 			v[1] += (double)ri * (double)zi;
@@ -322,11 +322,11 @@ __global__ void __launch_bounds__(kVT) k_mx_fold(int64_t n, double* __restrict__
 	}
 }
 
-// reliable update (after the fold): r64 = b - A64 x, r = (float) r64, z = M r, rho = r.z with the new
-// r (p, s and the previous rho and alpha carry on)
+// reliable update (after the fold): r64 = b - A64 x, z = M (float) r64, rho = r.z with the new r
+// (p, s and the previous rho and alpha carry on)
 template <int L>
 __global__ void __launch_bounds__(kST, 2048 / kST) k_mx_reliable(int64_t n, MatView<double> A, const double* __restrict__ b,
-                                                     const double* __restrict__ x, float* __restrict__ r,
+                                                     const double* __restrict__ x,
                                                      float* __restrict__ z, const float* __restrict__ invD, CgScal* S, double* partials,
                                                      double tol, int relMode, int64_t maxIters, int adaptive) {
 	if (is_done(S) || !*((volatile const int32_t*)&S->reliable)) return;
@@ -340,7 +340,6 @@ __global__ void __launch_bounds__(kST, 2048 / kST) k_mx_reliable(int64_t n, MatV
 			const double r64 = ldh(b + row, pol.first) - ax;
 			const float ri = (float)r64;
 			const float zi = invD ? ri * ldh(invD + row, pol.last) : ri;
-			sth(r + row, ri, pol.last);
 			sth(z + row, zi, pol.last);
 			v[0] += r64 * r64;
 			v[1] += (double)ri * (double)zi;
@@ -701,9 +700,9 @@ static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const d
 	const MatView<float> V32 = view32(A);
 	void* wsv;
 	const int64_t ns = pad_len(n);
-	RSD_CHECK(get_ws(ctx, sizeof(float) * 7 * ns, &wsv));
-	float* r = (float*)wsv;
-	float* z = r + ns;       // M r, the vector the SpMV multiplies
+	RSD_CHECK(get_ws(ctx, sizeof(float) * 6 * ns, &wsv));
+	// the residual is carried as z = M r alone (r = D z for the reductions)
+	float* z = (float*)wsv;  // M r, the vector the SpMV multiplies
 	float* p = z + ns;
 	float* sv = p + ns;      // A p, by recurrence
 	float* w = sv + ns;      // A z
@@ -721,7 +720,7 @@ static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const d
 	auto prologue = [&]() -> int {
 		RSD_CUDA(cudaMemsetAsync(S, 0, sizeof(CgScal), st));
 		if (invD) k_invdiag32<<<VG(k_invdiag32), 256, 0, st>>>(n, exec_diag(A), exec_val(A), invD);
-		RSD_DISPATCH_L(L, (k_mx_init<LL><<<RG(k_mx_init<LL>), 256, 0, st>>>(n, V, b, x, r, z, y, invD, S, partials, tol, rel, maxIt, delta)));
+		RSD_DISPATCH_L(L, (k_mx_init<LL><<<RG(k_mx_init<LL>), 256, 0, st>>>(n, V, b, x, z, y, invD, S, partials, tol, rel, maxIt, delta)));
 		RSD_CUDA(cudaGetLastError());
 		return RSD_OK;
 	};
@@ -730,7 +729,7 @@ static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const d
 		RSD_DISPATCH_L(L, (k_mx_spmv_dot<LL><<<RGB(k_mx_spmv_dot<LL>, kST), kST, 0, st>>>(n, V32, z, w, S, partials)));
 	};
 	auto step = [&](GraphCtl gc) {
-		k_mx_step<<<VGB(k_mx_step, kVT), kVT, 0, st>>>(n, y, r, z, p, sv, w, invD, S, partials, tol, rel, maxIt, gc);
+		k_mx_step<<<VGB(k_mx_step, kVT), kVT, 0, st>>>(n, y, z, p, sv, w, invD, S, partials, tol, rel, maxIt, gc);
 	};
 	auto body_a = [&](GraphCtl gc) -> int {
 		spmv();
@@ -740,7 +739,7 @@ static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const d
 	};
 	auto reliable = [&]() -> int {
 		k_mx_fold<<<VGB(k_mx_fold, kVT), kVT, 0, st>>>(n, x, y, S);
-		RSD_DISPATCH_L(L, (k_mx_reliable<LL><<<RGB(k_mx_reliable<LL>, kST), kST, 0, st>>>(n, V, b, x, r, z, invD, S, partials, tol, rel, maxIt, adaptive)));
+		RSD_DISPATCH_L(L, (k_mx_reliable<LL><<<RGB(k_mx_reliable<LL>, kST), kST, 0, st>>>(n, V, b, x, z, invD, S, partials, tol, rel, maxIt, adaptive)));
 		RSD_CUDA(cudaGetLastError());
 		return RSD_OK;
 	};
@@ -748,7 +747,7 @@ static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const d
 	if (graph_mode(ctx)) {
 		CgGraph& G = graph_cache(ctx)->cg[1];
 		CgKey key{};
-		const void* ptrs[] = {A, V.ptr, V.col, V.val, V32.val, exec_diag(A), b, x, r, invD, S, partials};
+		const void* ptrs[] = {A, V.ptr, V.col, V.val, V32.val, exec_diag(A), b, x, z, invD, S, partials};
 		std::copy(std::begin(ptrs), std::end(ptrs), key.p);
 		const int64_t ints[] = {n, L, maxIt, rel};
 		std::copy(std::begin(ints), std::end(ints), key.i);
