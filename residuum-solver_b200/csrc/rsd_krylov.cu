@@ -1,10 +1,12 @@
 // Krylov solvers on the device: PCG (FP64, and FP32-inner with FP64 reliable updates) and
-// restarted right-preconditioned GMRES(m) with modified Gram-Schmidt.
+// restarted right-preconditioned GMRES(m) with classical Gram-Schmidt applied twice.
 //
-// PCG keeps every scalar (alpha, beta, r.z, |r|) in device memory: each iteration is three
-// kernels on one stream (SpMV + p.Ap, update + r.r/r.z, p update), each grid reduction finishing
-// in its last block, so no iteration waits on the host.  The host only polls the done flag once
-// per chunk of iterations; kernels of an already-finished solve return immediately.
+// PCG keeps every scalar (alpha, beta, r.z, |r|) in device memory: an FP64 iteration is three
+// kernels on one stream (SpMV + p.Ap, update + r.r/r.z, p update), a mixed one two (SpMV + z.Az,
+// then one vector pass of the single-reduction form), each grid reduction finishing in its last
+// block, so no iteration waits on the host.  A solve is one CUDA graph (a device-side WHILE loop);
+// with plain launches the host polls the done flag once per chunk of iterations, and kernels of an
+// already-finished solve return immediately.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
