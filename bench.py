@@ -552,28 +552,38 @@ def run_adjoint(rsd, ctx, stream, S, ndir):
     dirs = np.sqrt(-2.0 * np.log1p(-u[..., 0])) * np.cos(2.0 * np.pi * u[..., 1])
     dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
 
-    # each perturbed forward solve starts from T(theta) and reduces the O(h) initial residual by 1e-8
-    # (about 1e-15 of ||F||); the quotient is formed from T+ - T-, not from J+ - J-, so that no
-    # cancellation between two nearly equal sums limits it:
-    #   J(th + h d) - J(th - h d) = 0.5 sum (T+ - T-) (T+ + T- - 2 T_obs)
+    # central differences J(th + h d) - J(th - h d) from the increments delta = T(th +- h d) - T(th),
+    # solved directly: K(th +- h d) delta = -(K(th +- h d) - K(th)) T, the right-hand side being the
+    # diffusion operator of the conductivity differences k_e (exp(+-h d_e) - 1) applied to T.  Nothing
+    # is formed as a difference of two nearly equal solutions (T+ - T- loses about cond(K) eps / h of
+    # its digits at this conductivity contrast), and T + delta solves the perturbed system exactly
+    # when T solves the base one; then
+    #   J(th + h d) - J(th - h d) = 0.5 sum (d+ - d-) (d+ + d- + 2 (T - T_obs))
     t_base = T.download()
-    fd_cfg = rsd.SolverConfig.make(tol=1e-8, max_iters=20000)
+    ke = np.exp(th)
+    v, dl = ctx.array(n), ctx.array(n)
+    hstep = 1e-6
 
-    def Tof(t):
-        Tt = ctx.to_device(t_base)
-        h.forward(ctx.to_device(t), Tt, fd_cfg)
-        return Tt.download()
+    def increment(d, sgn):
+        h.set_k_elem(ctx.to_device(ke * np.expm1(sgn * hstep * d)))
+        h.assemble_vector(1, v, U=T)
+        h.set_k_elem(ctx.to_device(ke * np.exp(sgn * hstep * d)))
+        h.assemble_matrix(1.0)
+        rhs = ctx.to_device(-v.download())
+        dl.zero()
+        rsd.solve(ctx, h.K, rhs, dl, cfg)
+        return dl.download()
 
     errs = []
     for d in dirs:
-        tp, tm = Tof(th + 1e-6 * d), Tof(th - 1e-6 * d)
-        fd = 0.5 * float(np.sum((tp - tm) * (tp + tm - 2.0 * tobs))) / 2e-6
+        dp, dm = increment(d, 1.0), increment(d, -1.0)
+        fd = 0.5 * float(np.sum((dp - dm) * (dp + dm + 2.0 * (t_base - tobs)))) / (2.0 * hstep)
         errs.append(abs(fd - g @ d) / abs(fd))
+    h.set_k_elem(ctx.to_device(ke))
     # the same directional derivatives without differencing (tangent-linear solve):
     # K dT = -(dK/dtheta . d) T, with (dK/dtheta . d) T the diffusion operator of the element
     # multipliers k_e d_e applied to T; dJ . d = (T - T_obs) . dT
-    ke = np.exp(th)
-    v, dT = ctx.array(n), ctx.array(n)
+    dT = ctx.array(n)
     terrs = []
     for d in dirs:
         h.set_k_elem(ctx.to_device(ke * d))
