@@ -756,6 +756,24 @@ def main():
         except Exception as e:  # noqa: BLE001
             adjoint["cpu_baseline"] = {"value": None, "sample": f"failed: {e}"}
 
+    # the configured run once: 50 steps from T0 with each solver, final states compared
+    full_run = {}
+    finals = {}
+    for key in ("mixed", "fp64"):
+        U.upload(U0); Up.upload(U0)
+        heat.set_time(0.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        reps50 = [heat.be_step(dt, U, Up, cfgs[key]) for _ in range(50)]
+        e1.record(stream)
+        e1.synchronize()
+        finals[key] = U.download()
+        full_run[key] = {"ms": e0.elapsed_time(e1), "all_converged": all(r["converged"] for r in reps50),
+                         "iterations_total": int(sum(r["iterations"] for r in reps50)),
+                         "max_true_residual_rel": max(r["trueResidualRel"] for r in reps50)}
+    full_run["final_state_max_rel_diff"] = float(np.max(np.abs(finals["mixed"] - finals["fp64"])) / np.max(np.abs(finals["fp64"])))
+    full_run["how"] = "50 Backward-Euler steps (dt = 1e-3) from T0, one CUDA-event pair around all of them, each solver"
+
     # end to end through the public API with host buffers, every step: H2D of the state from pinned
     # host memory, the step (its previous state is the state it starts from: BackwardEulerRunner::step
     # keeps Uprev = U between steps, so it is set on the device), D2H of the new state
@@ -865,6 +883,7 @@ def main():
         "kernel_ms_per_step": {k: v[1] / args.steps for k, v in prof_mx.items()},
         "kernel_ms_per_step_fp64": {k: v[1] / args.steps for k, v in prof_64.items()},
         "clocks_fp64": clk64,
+        "full_run_50_steps": full_run,
         "batch": batch,
         "newton": newton,
         "adjoint": adjoint,
