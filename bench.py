@@ -836,7 +836,7 @@ def main():
         except Exception as e:  # noqa: BLE001
             cpu = {"value": None, "unit": "ms", "cores": 1, "kind": "reference", "sample": f"failed: {e}"}
 
-    # element assembly roofline of K + M/dt (the survey's accounting): bytes = CSR values written
+    # element assembly roofline of K + M/dt (bytes and flops as the path's roofline counts them): bytes = CSR values written
     # once + coordinates + connectivity, flops = E nq npe^2 (2d + 2) diffusion + E nq npe^2 3 mass,
     # against the measured HBM copy peak and the measured FP64 FMA rate; the bound that binds is the
     # larger time
