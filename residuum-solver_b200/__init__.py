@@ -113,6 +113,7 @@ SIGNATURES = {
     "rsd_assemble_diagonal": [_P, _P, _D, _D, _P, _P],
     "rsd_heat_steady": [_P, _P, C.POINTER(SolverConfig), _P, C.POINTER(Report)],
     "rsd_heat_be_step": [_P, _P, _D, C.POINTER(SolverConfig), _P, _P, C.POINTER(Report), C.POINTER(_D)],
+    "rsd_heat_be_step_host": [_P, _P, _D, C.POINTER(SolverConfig), _P, C.POINTER(Report), C.POINTER(_D)],
     "rsd_heat_newton": [_P, _P, _D, _D, _I64, C.POINTER(SolverConfig), _P, C.POINTER(Report)],
     "rsd_batch_create": [_P, _I32, _P, C.POINTER(_P)],
     "rsd_batch_destroy": [_P],
@@ -442,6 +443,25 @@ class Heat:
         cfg = cfg or SolverConfig.make(**kw)
         rep, res = Report(), _D()
         check(lib().rsd_heat_be_step(self.ctx.h, self.h, dt, C.byref(cfg), _ptr(U), _ptr(Uprev), C.byref(rep), C.byref(res)))
+        d = rep.as_dict()
+        d["residualNorm"] = res.value
+        return d
+
+    def be_step_host(self, dt, U_host, cfg=None, **kw):
+        """The step with the state in host memory: U_host (a C-contiguous float64 numpy array or CPU
+        torch tensor, pinned for full-speed copies) holds the state on entry and the new state on
+        return."""
+        cfg = cfg or SolverConfig.make(**kw)
+        rep, res = Report(), _D()
+        if hasattr(U_host, "ctypes"):
+            if U_host.dtype != np.float64 or not U_host.flags["C_CONTIGUOUS"] or U_host.size != self.n:
+                raise ValueError("U_host must be a C-contiguous float64 array of the problem's size")
+            ptr = U_host.ctypes.data_as(_P)
+        else:
+            if U_host.dtype != __import__("torch").float64 or U_host.is_cuda or U_host.numel() != self.n:
+                raise ValueError("U_host must be a float64 CPU tensor of the problem's size")
+            ptr = C.c_void_p(U_host.data_ptr())
+        check(lib().rsd_heat_be_step_host(self.ctx.h, self.h, dt, C.byref(cfg), ptr, C.byref(rep), C.byref(res)))
         d = rep.as_dict()
         d["residualNorm"] = res.value
         return d

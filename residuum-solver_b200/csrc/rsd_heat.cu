@@ -75,6 +75,7 @@ __global__ void k_diff_norm(int64_t n, const double* __restrict__ F, const doubl
 static void free_heat(rsd_heat* h) {
 	cudaFree(h->t2a); cudaFree(h->g); cudaFree(h->kElem); cudaFree(h->tables); cudaFree(h->bElems); cudaFree(h->gPrev);
 	cudaFree(h->ranks); cudaFree(h->affine); cudaFree(h->geo); cudaFree(h->ktab); cudaFree(h->adjPtr); cudaFree(h->adj);
+	cudaFree(h->hostU); cudaFree(h->hostUprev);
 	cudaFree(h->F); cudaFree(h->R); cudaFree(h->Udot); cudaFree(h->ms); cudaFree(h->dU);
 	if (h->K) rsd_csr_destroy(h->K);
 	delete h;
@@ -225,9 +226,13 @@ int rsd_heat_steady(rsd_ctx* ctx, rsd_heat* h, const rsd_solver_cfg* cfg, double
 
 // one BackwardEulerRunner::step, linear mode (solver/timestepper/BackwardEuler.hpp:32-70 over
 // solver/stage/BackwardEulerStage.hpp:71-124)
-int rsd_heat_be_step(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver_cfg* cfg, double* U, double* Uprev,
-                     rsd_report* rep, double* residual_norm) {
-	if (!ctx || !h || !cfg || !U || !Uprev || !(dt > 0)) return set_error(RSD_EINVAL, "bad argument");
+}  // extern "C" (reopened below)
+
+namespace rsd {
+// BackwardEulerRunner::step on device vectors U, Uprev; with host_out the new U is also copied to that
+// host buffer before the one synchronization at the end
+static int be_step(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver_cfg* cfg, double* U, double* Uprev,
+                   rsd_report* rep, double* residual_norm, double* host_out) {
 	const int64_t n = h->n;
 	const double t = h->time + dt, inv = 1.0 / dt;
 	const int gv = vec_grid(ctx, n);
@@ -251,9 +256,42 @@ int rsd_heat_be_step(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver_cfg*
 		RSD_CUDA(cudaMemcpyAsync(ctx->s.hbuf + 8, dres, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
 	}
 	RSD_CUDA(cudaMemcpyAsync(Uprev, U, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));   // advance()
+	if (host_out) RSD_CUDA(cudaMemcpyAsync(host_out, U, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
 	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
 	if (residual_norm) *residual_norm = ctx->s.hbuf[8];
 	return RSD_OK;
+}
+}  // namespace rsd
+
+extern "C" {
+
+int rsd_heat_be_step(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver_cfg* cfg, double* U, double* Uprev,
+                     rsd_report* rep, double* residual_norm) {
+	if (!ctx || !h || !cfg || !U || !Uprev || !(dt > 0)) return set_error(RSD_EINVAL, "bad argument");
+	return be_step(ctx, h, dt, cfg, U, Uprev, rep, residual_norm, nullptr);
+}
+
+// The same step for a caller whose state lives in host memory: the state is uploaded to device
+// vectors the problem keeps (allocated on the first call), the step's previous state is that same
+// state (BackwardEulerRunner::step keeps Uprev = U between steps), and the new state is copied back,
+// everything on the context stream with one synchronization.  Pinned host memory makes the copies
+// run at full link speed.
+int rsd_heat_be_step_host(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver_cfg* cfg, double* U_host,
+                          rsd_report* rep, double* residual_norm) {
+	if (!ctx || !h || !cfg || !U_host || !(dt > 0)) return set_error(RSD_EINVAL, "bad argument");
+	const int64_t n = h->n;
+	const size_t bytes = sizeof(double) * std::max<int64_t>(n, 1);
+	if (!h->hostU) {
+		cudaError_t e;
+		if ((e = cudaMalloc(&h->hostU, bytes)) != cudaSuccess || (e = cudaMalloc(&h->hostUprev, bytes)) != cudaSuccess) {
+			cudaFree(h->hostU);
+			h->hostU = nullptr;
+			return cuda_error(e, "device state for host-buffer steps");
+		}
+	}
+	RSD_CUDA(cudaMemcpyAsync(h->hostU, U_host, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+	RSD_CUDA(cudaMemcpyAsync(h->hostUprev, h->hostU, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+	return be_step(ctx, h, dt, cfg, h->hostU, h->hostUprev, rep, residual_norm, U_host);
 }
 
 // NewtonRunner::solve over SteadyStage nonlinear mode (solver/nonlinear/Newton.hpp:32-83)

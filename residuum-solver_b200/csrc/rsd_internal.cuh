@@ -212,6 +212,7 @@ struct rsd_heat {
 	int32_t maxSlice = 0;           // longest SELL-32 slice of K, in entries per row
 	// stage scratch
 	double *F = nullptr, *R = nullptr, *Udot = nullptr, *ms = nullptr, *dU = nullptr;
+	double *hostU = nullptr, *hostUprev = nullptr;   // device state of rsd_heat_be_step_host
 	double dt = 0.0;
 };
 

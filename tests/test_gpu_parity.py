@@ -215,6 +215,25 @@ def test_backward_euler_matches_reference(rsd, ctx):
     assert relerr(res, g["residual"]) <= 1e-9   # norms of residuals ~1e-8 of their parts: cancellation
 
 
+def test_be_step_with_host_state_matches_device_steps(rsd, ctx):
+    # the host-buffer step runs the same kernels on device copies of the state (the right-hand side
+    # and residual passes add with atomics, so the last bits may differ between two problems)
+    g = golden("be_q1_hex_6x5x4.npz")
+    kw = dict(type=rsd.CG, precond=rsd.JACOBI, tol=1e-8, max_iters=1000)
+    h1 = make_heat(rsd, ctx, 3, 1, 2, [6, 5, 4], [0, 0, 0], [1, 1, 1], dirichlet={t: "0" for t in range(6)})
+    U, Up = ctx.to_device(g["U0"]), ctx.to_device(g["U0"])
+    dev = [h1.be_step(1e-2, U, Up, **kw) for _ in range(5)]
+    h2 = make_heat(rsd, ctx, 3, 1, 2, [6, 5, 4], [0, 0, 0], [1, 1, 1], dirichlet={t: "0" for t in range(6)})
+    Uh = np.array(g["U0"], dtype=np.float64)
+    host = [h2.be_step_host(1e-2, Uh, **kw) for _ in range(5)]
+    assert relerr(Uh, U.download()) <= REL
+    assert relerr([r["residualNorm"] for r in host], [r["residualNorm"] for r in dev]) <= 1e-9
+    assert all(abs(a["iterations"] - b["iterations"]) <= 1 for a, b in zip(host, dev))
+    assert relerr(Uh, g["U"]) <= REL
+    with pytest.raises(ValueError):
+        h2.be_step_host(1e-2, np.zeros(h2.n, np.float32), **kw)
+
+
 def test_newton_gmres_matches_reference(rsd, ctx):
     g = golden("newton_q2_hex_3.npz")
     h = make_heat(rsd, ctx, 3, 2, 3, [3, 3, 3], [0, 0, 0], [1, 1, 1], src_expr="10", k_expr="1 + 0.5*T", dk_expr="0.5",
