@@ -573,6 +573,8 @@ int rsd_ctx_destroy(rsd_ctx* c) {
 	cudaFree(c->s.scal);
 	cudaFreeHost(c->s.hscal);
 	cudaFreeHost(c->s.hbuf);
+	if (c->copy) { cudaStreamSynchronize(c->copy); cudaStreamDestroy(c->copy); }
+	if (c->copyReady) cudaEventDestroy(c->copyReady);
 	if (c->stream) cudaStreamDestroy(c->stream);
 	delete c;
 	return RSD_OK;

@@ -246,6 +246,16 @@ static int be_step(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver_cfg* c
 	RSD_CHECK(assemble_vector(ctx, h, 7, inv, Uprev, nullptr, nullptr, h->F, 1.0, false));  // load + (1/dt) M Uprev
 	RSD_CHECK(assemble_lift(ctx, h, 1.0, inv, h->F));                                      // F -= (K + M/dt) G
 	RSD_CHECK(solve(ctx, h->K, cfg, h->F, U, rep));
+	if (host_out) {
+		// the new state is final: copy it to the host on the second stream while the residual pass runs
+		if (!ctx->copy) {
+			RSD_CUDA(cudaStreamCreateWithFlags(&ctx->copy, cudaStreamNonBlocking));
+			RSD_CUDA(cudaEventCreateWithFlags(&ctx->copyReady, cudaEventDisableTiming));
+		}
+		RSD_CUDA(cudaEventRecord(ctx->copyReady, ctx->stream));
+		RSD_CUDA(cudaStreamWaitEvent(ctx->copy, ctx->copyReady, 0));
+		RSD_CUDA(cudaMemcpyAsync(host_out, U, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->copy));
+	}
 	if (residual_norm) {
 		// BackwardEulerStage::residualNorm (:113-124) with the Udot of this step's assemble():
 		// K U (Full) + M Udot in one element pass, then |F - R|
@@ -256,8 +266,8 @@ static int be_step(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver_cfg* c
 		RSD_CUDA(cudaMemcpyAsync(ctx->s.hbuf + 8, dres, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
 	}
 	RSD_CUDA(cudaMemcpyAsync(Uprev, U, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));   // advance()
-	if (host_out) RSD_CUDA(cudaMemcpyAsync(host_out, U, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
 	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+	if (host_out) RSD_CUDA(cudaStreamSynchronize(ctx->copy));
 	if (residual_norm) *residual_norm = ctx->s.hbuf[8];
 	return RSD_OK;
 }

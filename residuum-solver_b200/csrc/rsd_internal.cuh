@@ -72,6 +72,8 @@ struct rsd_ctx {
 	int device = 0;
 	int num_sms = 148;
 	cudaStream_t stream = nullptr;
+	cudaStream_t copy = nullptr;       // second stream: D2H of a step's state beside its residual pass (lazy)
+	cudaEvent_t copyReady = nullptr;
 	rsd::rsd_scratch s;
 	rsd::Profiler prof;
 	void* graphs = nullptr;        // cached CG solve graphs (rsd_krylov.cu)
