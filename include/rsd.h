@@ -211,8 +211,9 @@ int rsd_heat_be_step(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver_cfg*
                      rsd_report* report, double* residual_norm);
 /* The same step for a caller whose state U_host lives in host memory (in: the state to advance from,
  * also the step's previous state; out: the new state): uploaded to device vectors h keeps (allocated
- * on the first call), stepped, and copied back, with one synchronization.  Pinned host memory gives
- * full-speed copies.  No counterpart in the reference (its CUDA tag keeps vectors on the device). */
+ * on the first call), stepped, and copied back, with one synchronization; the copies overlap the
+ * matrix assembly and the residual pass on a second stream.  Pinned host memory gives full-speed
+ * copies.  No counterpart in the reference (its CUDA tag keeps vectors on the device). */
 int rsd_heat_be_step_host(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver_cfg* cfg, double* U_host,
                           rsd_report* report, double* residual_norm);
 /* NewtonRunner::solve over SteadyStage nonlinear mode (solver/nonlinear/Newton.hpp:32-83,

@@ -575,6 +575,7 @@ int rsd_ctx_destroy(rsd_ctx* c) {
 	cudaFreeHost(c->s.hbuf);
 	if (c->copy) { cudaStreamSynchronize(c->copy); cudaStreamDestroy(c->copy); }
 	if (c->copyReady) cudaEventDestroy(c->copyReady);
+	if (c->uploaded) cudaEventDestroy(c->uploaded);
 	if (c->stream) cudaStreamDestroy(c->stream);
 	delete c;
 	return RSD_OK;

@@ -229,29 +229,45 @@ int rsd_heat_steady(rsd_ctx* ctx, rsd_heat* h, const rsd_solver_cfg* cfg, double
 }  // extern "C" (reopened below)
 
 namespace rsd {
-// BackwardEulerRunner::step on device vectors U, Uprev; with host_out the new U is also copied to that
-// host buffer before the one synchronization at the end
+static int ensure_copy_stream(rsd_ctx* ctx) {
+	if (ctx->copy) return RSD_OK;
+	RSD_CUDA(cudaStreamCreateWithFlags(&ctx->copy, cudaStreamNonBlocking));
+	RSD_CUDA(cudaEventCreateWithFlags(&ctx->copyReady, cudaEventDisableTiming));
+	RSD_CUDA(cudaEventCreateWithFlags(&ctx->uploaded, cudaEventDisableTiming));
+	return RSD_OK;
+}
+
+// BackwardEulerRunner::step on device vectors U, Uprev.  With host_in the state is first uploaded
+// into U and Uprev on the second stream, and a matrix that does not depend on the state (no k(T))
+// is assembled meanwhile; with host_out the new U is copied to that host buffer on the second stream
+// beside the residual pass.  One synchronization at the end.
 static int be_step(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver_cfg* cfg, double* U, double* Uprev,
-                   rsd_report* rep, double* residual_norm, double* host_out) {
+                   rsd_report* rep, double* residual_norm, const double* host_in, double* host_out) {
 	const int64_t n = h->n;
 	const double t = h->time + dt, inv = 1.0 / dt;
 	const int gv = vec_grid(ctx, n);
+	if (host_in || host_out) RSD_CHECK(ensure_copy_stream(ctx));
+	if (host_in) {
+		RSD_CUDA(cudaMemcpyAsync(U, host_in, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->copy));
+		RSD_CUDA(cudaMemcpyAsync(Uprev, U, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->copy));
+		RSD_CUDA(cudaEventRecord(ctx->uploaded, ctx->copy));
+	}
+	// K + M/dt reads the state only through k(T); without it, it goes first while the state uploads
+	const bool early = host_in && h->kExpr.n == 0 && h->dkExpr.n == 0;
 	h->dt = dt;
 	RSD_CHECK(set_time(ctx, h, t));
 	// Dirichlet values at t - dt for the mass right-hand side (gathered Full at currentTime_ - dt_)
 	h->gPrevValid = bc_time_dependent(h);
 	if (h->gPrevValid) RSD_CHECK(bc_values_to(ctx, h, t - dt, h->gPrev));
+	if (early) RSD_CHECK(assemble_matrix(ctx, h, 1.0, inv, 0.0, 0.0, U, h->Udot, h->K));      // K + M/dt
+	if (host_in) RSD_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->uploaded, 0));
 	k_be_rate<<<gv, 256, 0, ctx->stream>>>(n, inv, U, Uprev, h->Udot);
-	RSD_CHECK(assemble_matrix(ctx, h, 1.0, inv, 0.0, 0.0, U, h->Udot, h->K));                 // K + M/dt
+	if (!early) RSD_CHECK(assemble_matrix(ctx, h, 1.0, inv, 0.0, 0.0, U, h->Udot, h->K));    // K + M/dt
 	RSD_CHECK(assemble_vector(ctx, h, 7, inv, Uprev, nullptr, nullptr, h->F, 1.0, false));  // load + (1/dt) M Uprev
 	RSD_CHECK(assemble_lift(ctx, h, 1.0, inv, h->F));                                      // F -= (K + M/dt) G
 	RSD_CHECK(solve(ctx, h->K, cfg, h->F, U, rep));
 	if (host_out) {
 		// the new state is final: copy it to the host on the second stream while the residual pass runs
-		if (!ctx->copy) {
-			RSD_CUDA(cudaStreamCreateWithFlags(&ctx->copy, cudaStreamNonBlocking));
-			RSD_CUDA(cudaEventCreateWithFlags(&ctx->copyReady, cudaEventDisableTiming));
-		}
 		RSD_CUDA(cudaEventRecord(ctx->copyReady, ctx->stream));
 		RSD_CUDA(cudaStreamWaitEvent(ctx->copy, ctx->copyReady, 0));
 		RSD_CUDA(cudaMemcpyAsync(host_out, U, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->copy));
@@ -267,7 +283,7 @@ static int be_step(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver_cfg* c
 	}
 	RSD_CUDA(cudaMemcpyAsync(Uprev, U, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));   // advance()
 	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
-	if (host_out) RSD_CUDA(cudaStreamSynchronize(ctx->copy));
+	if (host_in || host_out) RSD_CUDA(cudaStreamSynchronize(ctx->copy));
 	if (residual_norm) *residual_norm = ctx->s.hbuf[8];
 	return RSD_OK;
 }
@@ -278,7 +294,7 @@ extern "C" {
 int rsd_heat_be_step(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver_cfg* cfg, double* U, double* Uprev,
                      rsd_report* rep, double* residual_norm) {
 	if (!ctx || !h || !cfg || !U || !Uprev || !(dt > 0)) return set_error(RSD_EINVAL, "bad argument");
-	return be_step(ctx, h, dt, cfg, U, Uprev, rep, residual_norm, nullptr);
+	return be_step(ctx, h, dt, cfg, U, Uprev, rep, residual_norm, nullptr, nullptr);
 }
 
 // The same step for a caller whose state lives in host memory: the state is uploaded to device
@@ -299,9 +315,7 @@ int rsd_heat_be_step_host(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver
 			return cuda_error(e, "device state for host-buffer steps");
 		}
 	}
-	RSD_CUDA(cudaMemcpyAsync(h->hostU, U_host, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
-	RSD_CUDA(cudaMemcpyAsync(h->hostUprev, h->hostU, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));
-	return be_step(ctx, h, dt, cfg, h->hostU, h->hostUprev, rep, residual_norm, U_host);
+	return be_step(ctx, h, dt, cfg, h->hostU, h->hostUprev, rep, residual_norm, U_host, U_host);
 }
 
 // NewtonRunner::solve over SteadyStage nonlinear mode (solver/nonlinear/Newton.hpp:32-83)

@@ -73,7 +73,7 @@ struct rsd_ctx {
 	int num_sms = 148;
 	cudaStream_t stream = nullptr;
 	cudaStream_t copy = nullptr;       // second stream: D2H of a step's state beside its residual pass (lazy)
-	cudaEvent_t copyReady = nullptr;
+	cudaEvent_t copyReady = nullptr, uploaded = nullptr;
 	rsd::rsd_scratch s;
 	rsd::Profiler prof;
 	void* graphs = nullptr;        // cached CG solve graphs (rsd_krylov.cu)
