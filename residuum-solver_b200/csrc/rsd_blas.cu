@@ -105,7 +105,7 @@ int f32_sync(rsd_ctx* ctx, rsd_csr* A) {
 // a warp per slice) or CSR-vector (L lanes per row)
 // ---------------------------------------------------------------------------------------------
 template <int L, typename T>
-__global__ void __launch_bounds__(512, 4) k_spmv(int64_t n, MatView<T> A, const T* __restrict__ x, T* __restrict__ y) {
+__global__ void __launch_bounds__(512, kRowBlocks) k_spmv(int64_t n, MatView<T> A, const T* __restrict__ x, T* __restrict__ y) {
 	const L2Pol pol = make_l2pol();
 	RowLoop<L> rl;
 	for (int64_t base = rl.base; base < n; base += rl.step) {

@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(256) k_cg_init(int64_t n, MatView<double> A, c
 
 // Ap = A p; alpha = rz / p.Ap   (Solver.tpp:69-73)
 template <int L>
-__global__ void __launch_bounds__(kST, 2048 / kST) k_cg_spmv_dot(int64_t n, MatView<double> A, const double* __restrict__ p,
+__global__ void __launch_bounds__(kST, kRowBlocks) k_cg_spmv_dot(int64_t n, MatView<double> A, const double* __restrict__ p,
                                                      double* __restrict__ Ap, CgScal* S, double* partials) {
 	if (is_done(S)) return;
 	const L2Pol pol = make_l2pol();
@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(256) k_mx_init(int64_t n, MatView<double> A, c
 
 // w = A32 z and mu = z.w (FP64 sum)
 template <int L>
-__global__ void __launch_bounds__(kST, 2048 / kST) k_mx_spmv_dot(int64_t n, MatView<float> A, const float* __restrict__ z,
+__global__ void __launch_bounds__(kST, kRowBlocks) k_mx_spmv_dot(int64_t n, MatView<float> A, const float* __restrict__ z,
                                                      float* __restrict__ w, CgScal* S, double* partials) {
 	if (is_done(S)) return;
 	if (blockIdx.x == 0 && threadIdx.x == 0) S->reliable = 0;
@@ -327,7 +327,7 @@ __global__ void __launch_bounds__(kVT) k_mx_fold(int64_t n, double* __restrict__
 // reliable update (after the fold): r64 = b - A64 x, z = M (float) r64, rho = r.z with the new r
 // (p, s and the previous rho and alpha carry on)
 template <int L>
-__global__ void __launch_bounds__(kST, 2048 / kST) k_mx_reliable(int64_t n, MatView<double> A, const double* __restrict__ b,
+__global__ void __launch_bounds__(kST, kRowBlocks) k_mx_reliable(int64_t n, MatView<double> A, const double* __restrict__ b,
                                                      const double* __restrict__ x,
                                                      float* __restrict__ z, const float* __restrict__ invD, CgScal* S, double* partials,
                                                      double tol, int relMode, int64_t maxIters, int adaptive) {
@@ -818,7 +818,7 @@ namespace {
 
 // w = A (M^-1 q) with M^-1 = diag(invD) (identity when invD is null)
 template <int L, typename T>
-__global__ void __launch_bounds__(256, 8) k_gm_spmv(int64_t n, MatView<T> A, const T* __restrict__ q,
+__global__ void __launch_bounds__(256, 2 * kRowBlocks) k_gm_spmv(int64_t n, MatView<T> A, const T* __restrict__ q,
                                                  const T* __restrict__ invD, T* __restrict__ w) {
 	const L2Pol pol = make_l2pol();
 	const RowLoop<L> rl;
