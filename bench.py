@@ -872,6 +872,8 @@ def main():
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak if achieved else None,
                      "frac_nominal_8tbs": achieved / 8000.0 if achieved else None, "algorithmic_bytes": bytes_spmv32,
                      "avg_launch_us": avg_ms * 1e3, "launches": launches, "traffic": traffic,
+                     "traffic_gbs": traffic / (avg_ms * 1e6) if traffic and avg_ms else None,
+                     "traffic_frac": traffic / (avg_ms * 1e6) / peak if traffic and avg_ms else None,
                      "fp64_spmv": {"achieved": achieved64, "frac": achieved64 / peak if achieved64 else None,
                                    "algorithmic_bytes": bytes_spmv64, "avg_launch_us": 1e3 * t64 / max(l64, 1)}},
         "assembly_roofline": asm_roof,

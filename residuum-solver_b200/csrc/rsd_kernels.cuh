@@ -205,10 +205,11 @@ struct MatView {
 	const int32_t* __restrict__ offs = nullptr;
 };
 
-// Resident blocks of 512 threads per SM the SELL-32 row-sum kernels are compiled for: 3 leaves about
-// 40 registers per thread, enough for the four pairs in flight of row_sum (measured at 128^3: FP32
-// SpMV 53 us against 58 us with two pairs at 4 blocks, 65 us with four pairs at 4 blocks)
-constexpr int kRowBlocks = 3;
+// Resident blocks of 512 threads per SM the SELL-32 row-sum kernels are compiled for: 2 leaves 64
+// registers per thread, enough for the 64 bytes of values in flight per lane of row_sum (eight FP32
+// pairs or four FP64 pairs).  Measured at 128^3: FP32 SpMV 49 us and FP64 85 us, against 53 / 90 us
+// with four pairs at 3 blocks, 58 us (FP32) with two pairs at 4 blocks
+constexpr int kRowBlocks = 2;
 
 // sum over one row of val * xf(column).  L == 0: SELL-32, one thread per row (entries 32 slots
 // apart, so a warp's value/column loads are contiguous); L == -1: SELL-32 with 16-bit column
@@ -230,8 +231,28 @@ __device__ __forceinline__ AccT row_sum(const MatView<T>& A, int64_t row, int64_
 			const T* __restrict__ vp = A.val + q0;
 			auto run = [&](auto colpair) {
 				int jp = 0;
-				// four pairs per step (their value loads, pattern offsets and gathers issued together),
-				// then two, then one; the SpMV kernels get the registers for it (kRowBlocks)
+				// 64 bytes of values per step (eight FP32 pairs or four FP64 pairs: their value loads,
+				// pattern offsets and gathers issued together), then two pairs, then one; the SpMV
+				// kernels get the registers for it (kRowBlocks)
+				if constexpr (sizeof(T) == 4) {
+					for (; jp + 8 <= npair; jp += 8) {
+						decltype(ldh2(vp, pol.first)) vv[8];
+						AccT xv[16];
+#pragma unroll
+						for (int k = 0; k < 8; ++k) vv[k] = ldh2(vp + 64 * (jp + k), pol.first);
+#pragma unroll
+						for (int k = 0; k < 8; ++k) {
+							const int2 c = colpair(jp + k);
+							xv[2 * k] = xf(c.x);
+							xv[2 * k + 1] = xf(c.y);
+						}
+#pragma unroll
+						for (int k = 0; k < 8; ++k) {
+							s += (AccT)vv[k].x * xv[2 * k];
+							s += (AccT)vv[k].y * xv[2 * k + 1];
+						}
+					}
+				}
 				for (; jp + 4 <= npair; jp += 4) {
 					const auto va = ldh2(vp + 64 * jp, pol.first), vb = ldh2(vp + 64 * (jp + 1), pol.first);
 					const auto vc = ldh2(vp + 64 * (jp + 2), pol.first), vd = ldh2(vp + 64 * (jp + 3), pol.first);
