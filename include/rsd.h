@@ -45,6 +45,8 @@ enum { RSD_CG = 0, RSD_GMRES = 1 };
 enum { RSD_IDENTITY = 0, RSD_JACOBI = 1 };
 enum { RSD_FP64 = 0, RSD_MIXED = 1 };
 enum { RSD_TOL_RELATIVE = 0, RSD_TOL_ABSOLUTE = 1 };
+/* LinearSolverConfig::OperatorType (include/solver/config/LinearSolverConfig.hpp:49-56) */
+enum { RSD_OP_CSR = 0, RSD_OP_FEM = 1 };
 
 /* SolverReport (include/linalg/solver/base/SolverReport.hpp:12-28) plus device-path extras */
 typedef struct rsd_report {
@@ -70,6 +72,10 @@ typedef struct rsd_solver_cfg {
 	double reliable_delta;       /* mixed CG: FP64 residual replacement when |r| falls by this factor; 0: adaptive,
 	                                from 0.1, set at each replacement from the recurrence/true residual gap, in [1e-4, 0.1]
 	                                (the batched solver: [1e-3, 0.1]) */
+	int32_t operator_type;       /* RSD_OP_CSR, or RSD_OP_FEM: the heat stages assemble no matrix and solve with the
+	                                matrix-free operator (FEMOperator: element-kernel products, Jacobi from the
+	                                element diagonal; CG in FP64).  rsd_solve and rsd_batch_solve take RSD_OP_CSR. */
+	int32_t reserved;            /* zero */
 } rsd_solver_cfg;
 
 /* ---- lifetime (linalg/types/backend/CUDA.hpp:23-73 has no context; these give it one) ---- */
@@ -195,13 +201,23 @@ int rsd_assemble_matrix(rsd_ctx* ctx, rsd_heat* h, double c_diff, double c_mass,
  * 3: rho*cp*Mass on Udot (Free); 4: Diffusion + coef*Mass on operand (Free; FEMOperator::apply) */
 int rsd_assemble_vector(rsd_ctx* ctx, rsd_heat* h, int32_t which, double coef, const double* U, const double* Udot,
                         const double* operand, double* out);
+/* The LinearSolverRunner HeatProblem::makeLinearRunner builds for OperatorType::FEM
+ * (application/heateq/problem/HeatProblem.tpp:274-289) over FEMOperator (linalg/operator/FEMOperator.hpp:39-56)
+ * with the forms Diffusion + c_mass*Mass: solves A x = b without a matrix, every product an element
+ * pass (rsd_assemble_vector mode 4 with the iterate as the k(T) state), Jacobi from the element
+ * diagonal (Assembler::assembleDiagonal).  cfg: type RSD_CG, precision RSD_FP64; operator_type is not
+ * read.  b, x device vectors of num_free entries; x holds the initial guess. */
+int rsd_heat_solve_fem(rsd_ctx* ctx, rsd_heat* h, double c_mass, const rsd_solver_cfg* cfg, const double* b, double* x,
+                       rsd_report* report);
 /* BoundaryApplicator::applyEssentialBCs (fem/boundary/backend/cpu/BoundaryApplicator.tpp:7-64) */
 int rsd_apply_dirichlet_lift(rsd_ctx* ctx, rsd_heat* h, double c_diff, double c_mass, double* F);
 /* Assembler::assembleDiagonal (Assembler.tpp:142-197) */
 int rsd_assemble_diagonal(rsd_ctx* ctx, rsd_heat* h, double c_diff, double c_mass, const double* U, double* d);
 
 /* ---- stages ---- */
-/* SteadyStage linear assemble + solve (solver/stage/SteadyStage.hpp:60-84); U device in/out */
+/* SteadyStage linear assemble + solve (solver/stage/SteadyStage.hpp:60-84); U device in/out.
+ * With cfg->operator_type RSD_OP_FEM the stages assemble no matrix (the stages' needsK() is false
+ * for a matrix-free operator) and solve as rsd_heat_solve_fem does. */
 int rsd_heat_steady(rsd_ctx* ctx, rsd_heat* h, const rsd_solver_cfg* cfg, double* U, rsd_report* report);
 /* BackwardEulerRunner::step over BackwardEulerStage, linear mode
  * (solver/timestepper/BackwardEuler.hpp:32-70, solver/stage/BackwardEulerStage.hpp:71-124):
@@ -217,7 +233,8 @@ int rsd_heat_be_step(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver_cfg*
 int rsd_heat_be_step_host(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver_cfg* cfg, double* U_host,
                           rsd_report* report, double* residual_norm);
 /* NewtonRunner::solve over SteadyStage nonlinear mode (solver/nonlinear/Newton.hpp:32-83,
- * solver/stage/SteadyStage.hpp:89-116): R = F - K(T)T, J = K + K_T, J dU = R, U += dU */
+ * solver/stage/SteadyStage.hpp:89-116): R = F - K(T)T, J = K + K_T, J dU = R, U += dU.
+ * linear->operator_type: RSD_OP_CSR (the Jacobian forms have no matrix-free product here). */
 int rsd_heat_newton(rsd_ctx* ctx, rsd_heat* h, double abs_tol, double rel_tol, int64_t max_iters,
                     const rsd_solver_cfg* linear, double* U, rsd_report* report);
 

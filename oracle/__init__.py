@@ -93,6 +93,8 @@ def oracle_lib():
         L.ro_backward_euler.argtypes = [_P, _D, _I64, _I32, _I32, _D, _I64, _I64, _P, _P, _P]
         L.ro_newton.argtypes = [_P, _D, _D, _I64, _I32, _I32, _D, _I64, _I64, _P, C.POINTER(Report)]
         L.ro_expr_eval.argtypes = [C.c_char_p, _D, _D, _D, _D, _D, C.POINTER(_D)]
+        L.ro_fem_solve.argtypes = [_P, _D, _I32, _P, _P, _D, _I64, C.POINTER(Report)]
+        L.ro_set_operator.argtypes = [_P, _I32]
         _olib = L
     return _olib
 
@@ -207,6 +209,17 @@ class Oracle:
         oracle_lib().ro_adjoint_gradient(self.h, _ptr(_f64(T)), _ptr(_f64(lam)), _ptr(g))
         return g
 
+    def set_operator(self, op):
+        """Operator of the stages' linear solves: "csr" (assembled matrix) or "fem" (matrix-free, CG)."""
+        oracle_lib().ro_set_operator(self.h, {"csr": 0, "fem": 1}[op])
+
+    def fem_solve(self, b, x0, coef=0.0, precond=1, tol=1e-10, maxit=1000):
+        """(Diffusion + coef Mass) x = b by CG over element-pass products (FEMOperator)."""
+        x = np.array(x0, dtype=np.float64)
+        rep = Report()
+        oracle_lib().ro_fem_solve(self.h, coef, precond, _ptr(np.asarray(b, np.float64)), _ptr(x), tol, maxit, C.byref(rep))
+        return x, rep.as_dict()
+
     def steady(self, solver=0, precond=1, tol=1e-10, maxit=1000, krylov=30, U=None):
         U = np.zeros(self.n) if U is None else np.array(U, dtype=np.float64)
         rep = Report()
@@ -291,6 +304,7 @@ def ref_lib():
         L.ref_adjoint_gradient.argtypes = [_P, _P, _P, _P]
         L.ref_csr_solve.argtypes = [C.c_int, C.c_int, _I64, _P, _P, _P, _P, _P, _D, _I64, _I64, C.POINTER(Report)]
         L.ref_spmv.argtypes = [_I64, _P, _P, _P, _P, _P]
+        L.ref_set_operator.argtypes = [_P, C.c_int]
         _rlib = L
     return _rlib
 
@@ -373,6 +387,10 @@ class Reference:
         d = np.zeros(self.n)
         ref_lib().ref_diagonal(self.h, self.FORMSETS[formset], c, _ptr(_f64(U)), _ptr(d))
         return d
+
+    def set_operator(self, op):
+        """LinearSolverConfig::OperatorType of the stages' linear solves: "csr" or "fem" (FEMOperator)."""
+        ref_lib().ref_set_operator(self.h, {"csr": 0, "fem": 1}[op])
 
     def steady(self, solver=0, precond=1, tol=1e-10, maxit=1000, krylov=30, U=None):
         U = np.zeros(self.n) if U is None else np.array(U, dtype=np.float64)

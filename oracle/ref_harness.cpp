@@ -35,6 +35,7 @@
 #include "linalg/operations/VectorOps.hpp"
 #include "linalg/operations/MatrixOps.hpp"
 #include "linalg/operator/CSROperator.hpp"
+#include "linalg/operator/FEMOperator.hpp"
 #include "linalg/solver/iterative/cg/Solver.hpp"
 #include "linalg/solver/iterative/gmres/Solver.hpp"
 #include "linalg/solver/preconditioner/Jacobi.hpp"
@@ -221,6 +222,7 @@ struct Base {
 	virtual int newton(double absTol, double relTol, int64_t maxit, int solverType, int precond, double tol, int64_t linMaxit, int64_t krylov, double* U, ref_report* rep) = 0;
 	virtual int backwardEuler(double dt, int64_t nsteps, int solverType, int precond, double tol, int64_t maxit, int64_t krylov, double* U, double* residualPerStep, double* stepStats) = 0;
 	virtual void adjointGradient(const double* T, const double* lam, double* grad) = 0;
+	int opType = 0;   // LinearSolverConfig::OperatorType of the stages' linear solves: 0 CSR, 1 FEM
 };
 
 template<int NSD>
@@ -264,6 +266,8 @@ struct RefHeatProblem final : Base {
 	OpModelT opModel_;
 	equation::heateq::evaluator::DefaultModel<EvalQP> defaultModel_;
 	Diff diff_;
+	std::unique_ptr<StiffnessForms> stiff_;
+	fem::assembly::Assembler<CPU> assembler_;
 	SourceForms sourceForms_;
 
 	// linear / nonlinear / time-stepper configuration consumed by the reference stages
@@ -294,6 +298,7 @@ struct RefHeatProblem final : Base {
 		diff_.ienBase = mesh_.data.ien.data();
 		diff_.npe = mesh_.data.nodesPerElement;
 		diff_.kElem = d.k_elem;
+		stiff_ = std::make_unique<StiffnessForms>(diff_);
 		const int ntags = (NSD == 2) ? 4 : 6;
 		for (int t = 0; t < ntags; ++t) {
 			if (!(desc.ess_mask & (1 << t))) continue;
@@ -311,7 +316,8 @@ struct RefHeatProblem final : Base {
 	}
 
 	// ---- Problem concept (solver/problem/Problem.hpp:16-50) -----------------------------------
-	StiffnessForms stiffnessForms() const { return StiffnessForms(diff_); }
+	// a reference to one instance: FEMOperator keeps the forms it is given by reference
+	const StiffnessForms& stiffnessForms() const { return *stiff_; }
 	const OpModelT& stiffnessModel() const { return opModel_; }
 	TangentDiffusionForms tangentStiffnessForms() const { return {}; }
 	MassForms massForms() const { return {}; }
@@ -364,10 +370,15 @@ struct RefHeatProblem final : Base {
 	linalg::solver::SolverReport<VecT> lastReport_;
 	double lastSolveSeconds_ = 0.0;
 	template<typename FormsT, typename ModelT>
-	std::unique_ptr<linalg::solver::LinearSolverRunner<VecT>> makeLinearRunner(const Real*, const FormsT&, const ModelT&, StateVectorT&, MatT& K) {
+	std::unique_ptr<linalg::solver::LinearSolverRunner<VecT>> makeLinearRunner(const Real* time, const FormsT& forms, const ModelT& model, StateVectorT& state, MatT& K) {
 		using Op = linalg::op::CSROperator<MatT>;
+		using FemOp = linalg::op::FEMOperator<fem::assembly::Assembler<CPU>, topology::TopologicalDOF<1>, EvalEle, EvalQP, ModelT, FormsT, typename Fam::Quad, StateVectorT, VecT>;
 		auto r = std::make_unique<ReportingRunner>();
-		r->inner = solver::linear::makeLinearSolverRunner<Op, VecT>(Op(K), topo_->numFreeDOFs(), *inst_.linear, logCfg_.linear, equationLabel(), dofNames(), topo_->numFreeDOFs(), fem::dof::DOFOrdering::Interleaved);
+		// HeatProblem.tpp:274-289: the operator type of the linear solver config picks CSR or matrix-free
+		if (inst_.linear->operatorType == solver::config::LinearSolverConfig::OperatorType::FEM)
+			r->inner = solver::linear::makeLinearSolverRunner<FemOp, VecT>(FemOp(assembler_, mesh_, *topo_, time, model, forms, evalEle_, quad_, &ess_, state), topo_->numFreeDOFs(), *inst_.linear, logCfg_.linear, equationLabel(), dofNames(), topo_->numFreeDOFs(), fem::dof::DOFOrdering::Interleaved);
+		else
+			r->inner = solver::linear::makeLinearSolverRunner<Op, VecT>(Op(K), topo_->numFreeDOFs(), *inst_.linear, logCfg_.linear, equationLabel(), dofNames(), topo_->numFreeDOFs(), fem::dof::DOFOrdering::Interleaved);
 		r->sink = &lastReport_;
 		r->seconds = &lastSolveSeconds_;
 		return r;
@@ -474,7 +485,7 @@ struct RefHeatProblem final : Base {
 
 	void setLinear(int solverType, int precond, double tol, int64_t maxit, int64_t krylov) {
 		linCfg_.type = solverType == 0 ? solver::config::LinearSolverConfig::Type::CG : solver::config::LinearSolverConfig::Type::GMRES;
-		linCfg_.operatorType = solver::config::LinearSolverConfig::OperatorType::CSR;
+		linCfg_.operatorType = opType ? solver::config::LinearSolverConfig::OperatorType::FEM : solver::config::LinearSolverConfig::OperatorType::CSR;
 		linCfg_.preconditioner.type = precond ? solver::config::PreconditionerConfig::Type::Jacobi : solver::config::PreconditionerConfig::Type::Identity;
 		linCfg_.tolerance = tol;
 		linCfg_.maxIterations = (Index)maxit;
@@ -593,6 +604,7 @@ void* ref_create(const ref_desc* d) {
 	return nullptr;
 }
 void ref_destroy(void* h) { delete static_cast<Base*>(h); }
+void ref_set_operator(void* h, int op) { static_cast<Base*>(h)->opType = op; }
 int64_t ref_num_nodes(void* h) { return (int64_t)static_cast<Base*>(h)->numNodes(); }
 int64_t ref_num_elems(void* h) { return (int64_t)static_cast<Base*>(h)->numElems(); }
 int64_t ref_num_free(void* h) { return (int64_t)static_cast<Base*>(h)->numFree(); }

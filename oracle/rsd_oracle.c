@@ -221,6 +221,7 @@ struct ro_problem {
 	double N[RO_MAXQ][RO_MAXN], dNdxi[RO_MAXQ][RO_MAXN * 3], qxi[RO_MAXQ][3], qw[RO_MAXQ];
 	double time;
 	double* g;                 /* Dirichlet value per node at the current time (constrained nodes) */
+	int32_t opType;            /* LinearSolverConfig::OperatorType of the stages: 0 CSR, 1 FEM */
 };
 
 int64_t ro_num_free(const ro_problem* p) { return p->n; }
@@ -802,16 +803,71 @@ int ro_csr_solve(int32_t solverType, int32_t precond, int64_t n, const int64_t* 
 	return solverType == 0 ? cg_solve(&A, precond, b, x, tol, maxit, rep) : gmres_solve(&A, precond, b, x, tol, maxit, krylov, rep);
 }
 
+/* The LinearSolverRunner HeatProblem::makeLinearRunner builds for OperatorType::FEM
+ * (application/heateq/problem/HeatProblem.tpp:274-289): cg/Solver.tpp:13-119 over FEMOperator
+ * (linalg/operator/FEMOperator.hpp:39-56).  Every product is the element pass of which 4
+ * (Diffusion + coef*Mass on the operand, gathered Free) with the state, read through k(T), being the
+ * iterate x itself (the stages bind their state to the vector the solver updates); Jacobi::update
+ * (preconditioner/Jacobi.hpp:23-33) inverts the element diagonal at the initial x. */
+int ro_fem_solve(ro_problem* P, double coef, int32_t precond, const double* b, double* x, double tol, int64_t maxit,
+                 ro_report* rep) {
+	const int64_t n = P->n;
+	memset(rep, 0, sizeof *rep);
+	double* r = malloc(sizeof(double) * n); double* p = malloc(sizeof(double) * n);
+	double* Ap = malloc(sizeof(double) * n); double* z = malloc(sizeof(double) * n); double* invD = malloc(sizeof(double) * n);
+	if (precond) {
+		ro_diagonal(P, 1.0, coef, x, invD);
+		for (int64_t i = 0; i < n; ++i) invD[i] = (fabs(invD[i]) > 1e-300) ? 1.0 / invD[i] : 1.0;
+	} else {
+		for (int64_t i = 0; i < n; ++i) invD[i] = 1.0;
+	}
+	ro_assemble_vector(P, 4, coef, x, NULL, x, Ap);
+	for (int64_t i = 0; i < n; ++i) r[i] = b[i];
+	axpy(n, -1.0, Ap, r);
+	const double res0 = sqrt(dot(n, r, r));
+	int ok = 0; int64_t it = 0; double res = res0;
+	rep->initialResidual = res0;
+	if (res0 / (res0 + 1e-50) < tol) { ok = 1; rep->finalResidual = res0; rep->finalResidualRel = 1.0; goto done; }
+	prec_apply(n, precond, invD, r, z);
+	memcpy(p, z, sizeof(double) * n);
+	double rz = dot(n, r, z);
+	for (int64_t k = 1; k < maxit; ++k) {
+		ro_assemble_vector(P, 4, coef, x, NULL, p, Ap);
+		const double alpha = rz / dot(n, p, Ap);
+		axpy(n, alpha, p, x);
+		axpy(n, -alpha, Ap, r);
+		res = sqrt(dot(n, r, r));
+		const double rel = res / (res0 + 1e-50);
+		if (rel < tol) { ok = 1; it = k; rep->finalResidual = res; rep->finalResidualRel = rel; goto done; }
+		prec_apply(n, precond, invD, r, z);
+		const double rzn = dot(n, r, z);
+		const double beta = rzn / rz;
+		for (int64_t i = 0; i < n; ++i) p[i] *= beta;
+		axpy(n, 1.0, z, p);
+		rz = rzn;
+	}
+	res = sqrt(dot(n, r, r));
+	it = maxit; rep->finalResidual = res; rep->finalResidualRel = res / (res0 + 1e-50);
+done:
+	rep->converged = ok; rep->iterations = it;
+	free(r); free(p); free(Ap); free(z); free(invD);
+	return ok ? 0 : 1;
+}
+
+void ro_set_operator(ro_problem* P, int32_t op) { P->opType = op; }
+
 /* ============================================================================================
  * stages
  * ========================================================================================== */
 /* SteadyStage linear (solver/stage/SteadyStage.hpp:60-84, HeatProblem.tpp:217-270) */
 int ro_steady(ro_problem* P, int32_t solverType, int32_t precond, double tol, int64_t maxit, int64_t krylov, double* U, ro_report* rep) {
 	double* val = malloc(sizeof(double) * P->nnz); double* F = malloc(sizeof(double) * P->n);
-	ro_assemble_matrix(P, 1.0, 0.0, 0.0, 0.0, U, NULL, val);
+	if (P->opType && solverType != 0) { free(val); free(F); snprintf(g_err, sizeof g_err, "matrix-free operator: CG only"); return 2; }
+	if (!P->opType) ro_assemble_matrix(P, 1.0, 0.0, 0.0, 0.0, U, NULL, val);
 	ro_assemble_vector(P, 0, 0.0, U, NULL, NULL, F);
 	ro_lift(P, 1.0, 0.0, F);
-	int rc = ro_csr_solve(solverType, precond, P->n, P->rowPtr, P->col, val, F, U, tol, maxit, krylov, rep);
+	int rc = P->opType ? ro_fem_solve(P, 0.0, precond, F, U, tol, maxit, rep)
+	                   : ro_csr_solve(solverType, precond, P->n, P->rowPtr, P->col, val, F, U, tol, maxit, krylov, rep);
 	free(val); free(F);
 	return rc;
 }
@@ -830,12 +886,13 @@ int ro_backward_euler(ro_problem* P, double dt, int64_t nsteps, int32_t solverTy
 	memcpy(Uprev, U, sizeof(double) * n);
 	double time = 0.0; const double tf = dt * (double)nsteps;
 	int rc = 0;
+	if (P->opType && solverType != 0) { snprintf(g_err, sizeof g_err, "matrix-free operator: CG only"); rc = 2; nsteps = 0; }
 	for (int64_t s = 0; s < nsteps && !(time >= tf - 1e-9); ++s) {
 		double h = dt < tf - time ? dt : tf - time;
 		const double t = time + h;
 		for (int64_t i = 0; i < n; ++i) Udot[i] = (-1.0 / h) * Uprev[i] + (1.0 / h) * U[i];
 		ro_set_time(P, t);
-		ro_assemble_matrix(P, 1.0, 1.0 / h, 0.0, 0.0, U, Udot, val);
+		if (!P->opType) ro_assemble_matrix(P, 1.0, 1.0 / h, 0.0, 0.0, U, Udot, val);
 		ro_assemble_vector(P, 0, 0.0, U, Udot, NULL, F);
 		ro_set_time(P, t - h);
 		ro_assemble_vector(P, 2, 0.0, Uprev, NULL, NULL, ms);
@@ -843,7 +900,9 @@ int ro_backward_euler(ro_problem* P, double dt, int64_t nsteps, int32_t solverTy
 		axpy(n, 1.0 / h, ms, F);
 		ro_lift(P, 1.0, 1.0 / h, F);
 		ro_report rep;
-		if (ro_csr_solve(solverType, precond, n, P->rowPtr, P->col, val, F, U, tol, maxit, krylov, &rep)) { rc = 1; break; }
+		const int src = P->opType ? ro_fem_solve(P, 1.0 / h, precond, F, U, tol, maxit, &rep)
+		                          : ro_csr_solve(solverType, precond, n, P->rowPtr, P->col, val, F, U, tol, maxit, krylov, &rep);
+		if (src) { rc = 1; break; }
 		if (itersPerStep) itersPerStep[s] = rep.iterations;
 		ro_assemble_vector(P, 1, 0.0, U, Udot, NULL, R);
 		ro_assemble_vector(P, 3, 0.0, U, Udot, NULL, ms);

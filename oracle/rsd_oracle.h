@@ -76,6 +76,12 @@ int ro_csr_solve(int32_t solverType, int32_t precond, int64_t n, const int64_t* 
                  const double* val, const double* b, double* x, double tol, int64_t maxit, int64_t krylov,
                  ro_report* rep);
 
+/* the matrix-free operator (LinearSolverConfig operator type "fem"): CG over element-pass products */
+int ro_fem_solve(ro_problem* p, double coef, int32_t precond, const double* b, double* x, double tol, int64_t maxit,
+                 ro_report* rep);
+/* 0: the stages solve with the assembled matrix (CSR); 1: with the matrix-free operator (CG only) */
+void ro_set_operator(ro_problem* p, int32_t op);
+
 /* stages */
 int ro_steady(ro_problem* p, int32_t solverType, int32_t precond, double tol, int64_t maxit, int64_t krylov,
               double* U, ro_report* rep);

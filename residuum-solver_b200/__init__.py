@@ -20,6 +20,7 @@ CG, GMRES = 0, 1
 IDENTITY, JACOBI = 0, 1
 FP64, MIXED = 0, 1
 RELATIVE, ABSOLUTE = 0, 1
+OP_CSR, OP_FEM = 0, 1      # LinearSolverConfig::OperatorType
 
 ERRORS = {-1: "RSD_EINVAL", -2: "RSD_ENOMEM", -3: "RSD_ECUDA", -5: "RSD_EBREAKDOWN", -6: "RSD_ENAN",
           -7: "RSD_EPARSE", -8: "RSD_ETIMEOUT"}
@@ -42,12 +43,13 @@ class Report(C.Structure):
 
 class SolverConfig(C.Structure):
     _fields_ = [("type", _I32), ("precond", _I32), ("precision", _I32), ("tol_type", _I32), ("tol", _D),
-                ("max_iters", _I64), ("krylov_dim", _I64), ("reliable_delta", _D)]
+                ("max_iters", _I64), ("krylov_dim", _I64), ("reliable_delta", _D), ("operator_type", _I32),
+                ("reserved", _I32)]
 
     @classmethod
     def make(cls, type=CG, precond=JACOBI, precision=FP64, tol=1e-10, max_iters=1000, krylov_dim=30,
-             tol_type=RELATIVE, reliable_delta=0.0):
-        return cls(type, precond, precision, tol_type, tol, max_iters, krylov_dim, reliable_delta)
+             tol_type=RELATIVE, reliable_delta=0.0, operator_type=OP_CSR):
+        return cls(type, precond, precision, tol_type, tol, max_iters, krylov_dim, reliable_delta, operator_type, 0)
 
 
 class HeatDesc(C.Structure):
@@ -111,6 +113,7 @@ SIGNATURES = {
     "rsd_assemble_vector": [_P, _P, _I32, _D, _P, _P, _P, _P],
     "rsd_apply_dirichlet_lift": [_P, _P, _D, _D, _P],
     "rsd_assemble_diagonal": [_P, _P, _D, _D, _P, _P],
+    "rsd_heat_solve_fem": [_P, _P, _D, C.POINTER(SolverConfig), _P, _P, C.POINTER(Report)],
     "rsd_heat_steady": [_P, _P, C.POINTER(SolverConfig), _P, C.POINTER(Report)],
     "rsd_heat_be_step": [_P, _P, _D, C.POINTER(SolverConfig), _P, _P, C.POINTER(Report), C.POINTER(_D)],
     "rsd_heat_be_step_host": [_P, _P, _D, C.POINTER(SolverConfig), _P, C.POINTER(Report), C.POINTER(_D)],
@@ -432,6 +435,14 @@ class Heat:
 
     def diagonal(self, d, c_diff=1.0, c_mass=0.0, U=None):
         check(lib().rsd_assemble_diagonal(self.ctx.h, self.h, c_diff, c_mass, _ptr(U), _ptr(d)))
+
+    def solve_fem(self, b, x, c_mass=0.0, cfg=None, **kw):
+        """(Diffusion + c_mass Mass) x = b without a matrix: the LinearSolverRunner the reference builds
+        for operator type `fem` (FEMOperator), CG + Jacobi in FP64; x holds the initial guess."""
+        cfg = cfg or SolverConfig.make(**kw)
+        rep = Report()
+        check(lib().rsd_heat_solve_fem(self.ctx.h, self.h, c_mass, C.byref(cfg), _ptr(b), _ptr(x), C.byref(rep)))
+        return rep.as_dict()
 
     def steady(self, U, cfg=None, **kw):
         cfg = cfg or SolverConfig.make(**kw)

@@ -92,6 +92,8 @@ struct AsmParams {
 	double coef;
 	double* __restrict__ out;
 	double outScale;
+	// vector kernels: the whole launch returns at once when *skip != 0 (a finished solve's flag), or null
+	const int32_t* __restrict__ skip;
 };
 
 template <int NSD, int P>
@@ -591,6 +593,7 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_vector(const AsmParams prm)
 	nd.field2 = which == 8;
 	// k(T): diffusion of U takes T from U itself (staged as V, mirrored into U), the operator from the state
 	nd.state = (prm.kExpr.n != 0 && (which == 1 || which == 4 || which == 8 || which == 9)) || which == 6;
+	if (prm.skip && *(volatile const int32_t*)prm.skip) return;   // uniform over the launch
 	RSD_ELEMENT_LOOP_BEGIN
 	double Va = 0.0, Wa = 0.0, Ua = 0.0;
 	if (has) {
@@ -691,6 +694,7 @@ __global__ void __launch_bounds__(256) k_asm_vector_elem(const AsmParams prm) {
 	constexpr int NPE = E::NPE, NT = NSD == 3 ? 6 : 3;
 	constexpr bool kGrad = W == 1 || W == 4 || W == 5 || W == 8 || W == 9;
 	static_assert(NPE == 4 || NPE == 8, "one thread per element for 4- and 8-node elements");
+	if (prm.skip && *(volatile const int32_t*)prm.skip) return;   // uniform over the launch
 	extern __shared__ double kt[];
 	for (int i = threadIdx.x; i < (NT + 1) * NPE * NPE; i += blockDim.x) kt[i] = prm.ktab[i];
 	__syncthreads();
@@ -1230,6 +1234,21 @@ int assemble_vector(rsd_ctx* ctx, rsd_heat* h, int which, double coef, const dou
 		const int64_t len = which == 6 ? h->m->nelem : h->n;
 		RSD_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * std::max<int64_t>(len, 1), ctx->stream));
 	}
+	const int pr = prof_begin(ctx, PF_ASM_VECTOR);
+	const int rc = launch_k_asm_vector(ctx, h, p);
+	prof_end(ctx, pr);
+	return rc;
+}
+
+// FEMOperator::apply (linalg/operator/FEMOperator.hpp:39-43) for the forms Diffusion + coef * Mass:
+// out = A(U) V over the free DOFs, the operand gathered Free (zero on constrained nodes) and the state
+// U (Full) read only through k(T).  With skip, the element kernel returns at once once *skip != 0.
+int apply_operator(rsd_ctx* ctx, rsd_heat* h, double coef, const double* U, const double* V, double* out,
+                   const int32_t* skip) {
+	AsmParams p = params_for(h);
+	p.which = 4; p.coef = coef; p.U = U; p.V = V; p.out = out; p.skip = skip;
+	RSD_CHECK(affine_vector(ctx, h, p));
+	RSD_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * std::max<int64_t>(h->n, 1), ctx->stream));
 	const int pr = prof_begin(ctx, PF_ASM_VECTOR);
 	const int rc = launch_k_asm_vector(ctx, h, p);
 	prof_end(ctx, pr);

@@ -270,6 +270,7 @@ int rsd_batch_solve(rsd_ctx* ctx, rsd_batch* B, const rsd_solver_cfg* cfg, const
 	if (!ctx || !B || !cfg || (B->count && (!b || !x))) return set_error(RSD_EINVAL, "null argument");
 	if (cfg->type != RSD_CG) return set_error(RSD_EINVAL, "the batched solver runs CG");
 	if (cfg->max_iters < 0 || !(cfg->tol >= 0)) return set_error(RSD_EINVAL, "bad solver configuration");
+	if (cfg->operator_type != RSD_OP_CSR) return set_error(RSD_EINVAL, "the batched solver takes operator_type RSD_OP_CSR");
 	const int32_t count = B->count;
 	if (!count) return RSD_OK;
 	RSD_CUDA(cudaSetDevice(ctx->device));

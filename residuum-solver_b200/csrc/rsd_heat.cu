@@ -201,6 +201,12 @@ int rsd_assemble_vector(rsd_ctx* ctx, rsd_heat* h, int32_t which, double coef, c
 	return RSD_OK;
 }
 
+int rsd_heat_solve_fem(rsd_ctx* ctx, rsd_heat* h, double c_mass, const rsd_solver_cfg* cfg, const double* b, double* x,
+                       rsd_report* rep) {
+	if (!ctx || !h || !cfg) return set_error(RSD_EINVAL, "null argument");
+	return solve_fem(ctx, h, c_mass, cfg, b, x, rep);
+}
+
 int rsd_apply_dirichlet_lift(rsd_ctx* ctx, rsd_heat* h, double cd, double cm, double* F) {
 	if (!ctx || !h || !F) return set_error(RSD_EINVAL, "null argument");
 	RSD_CHECK(assemble_lift(ctx, h, cd, cm, F));
@@ -218,10 +224,11 @@ int rsd_assemble_diagonal(rsd_ctx* ctx, rsd_heat* h, double cd, double cm, const
 // SteadyStage linear: assemble K, load, lift; solve K U = F (solver/stage/SteadyStage.hpp:60-84)
 int rsd_heat_steady(rsd_ctx* ctx, rsd_heat* h, const rsd_solver_cfg* cfg, double* U, rsd_report* rep) {
 	if (!ctx || !h || !cfg || !U) return set_error(RSD_EINVAL, "null argument");
-	RSD_CHECK(assemble_matrix(ctx, h, 1.0, 0.0, 0.0, 0.0, U, nullptr, h->K));
+	const bool fem = cfg->operator_type == RSD_OP_FEM;   // isSparse() false: no K (SteadyStage.hpp:62-64)
+	if (!fem) RSD_CHECK(assemble_matrix(ctx, h, 1.0, 0.0, 0.0, 0.0, U, nullptr, h->K));
 	RSD_CHECK(assemble_vector(ctx, h, 0, 0.0, U, nullptr, nullptr, h->F, 1.0, false));
 	RSD_CHECK(assemble_lift(ctx, h, 1.0, 0.0, h->F));
-	return solve(ctx, h->K, cfg, h->F, U, rep);
+	return fem ? solve_fem(ctx, h, 0.0, cfg, h->F, U, rep) : solve(ctx, h->K, cfg, h->F, U, rep);
 }
 
 // one BackwardEulerRunner::step, linear mode (solver/timestepper/BackwardEuler.hpp:32-70 over
@@ -252,8 +259,10 @@ static int be_step(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver_cfg* c
 		RSD_CUDA(cudaMemcpyAsync(Uprev, U, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->copy));
 		RSD_CUDA(cudaEventRecord(ctx->uploaded, ctx->copy));
 	}
-	// K + M/dt reads the state only through k(T); without it, it goes first while the state uploads
-	const bool early = host_in && h->kExpr.n == 0 && h->dkExpr.n == 0;
+	// K + M/dt reads the state only through k(T); without it, it goes first while the state uploads.
+	// A matrix-free operator needs no K (BackwardEulerStage::needsK, BackwardEulerStage.hpp:76-78).
+	const bool fem = cfg->operator_type == RSD_OP_FEM;
+	const bool early = !fem && host_in && h->kExpr.n == 0 && h->dkExpr.n == 0;
 	h->dt = dt;
 	RSD_CHECK(set_time(ctx, h, t));
 	// Dirichlet values at t - dt for the mass right-hand side (gathered Full at currentTime_ - dt_)
@@ -262,10 +271,11 @@ static int be_step(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver_cfg* c
 	if (early) RSD_CHECK(assemble_matrix(ctx, h, 1.0, inv, 0.0, 0.0, U, h->Udot, h->K));      // K + M/dt
 	if (host_in) RSD_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->uploaded, 0));
 	k_be_rate<<<gv, 256, 0, ctx->stream>>>(n, inv, U, Uprev, h->Udot);
-	if (!early) RSD_CHECK(assemble_matrix(ctx, h, 1.0, inv, 0.0, 0.0, U, h->Udot, h->K));    // K + M/dt
+	if (!early && !fem) RSD_CHECK(assemble_matrix(ctx, h, 1.0, inv, 0.0, 0.0, U, h->Udot, h->K));    // K + M/dt
 	RSD_CHECK(assemble_vector(ctx, h, 7, inv, Uprev, nullptr, nullptr, h->F, 1.0, false));  // load + (1/dt) M Uprev
 	RSD_CHECK(assemble_lift(ctx, h, 1.0, inv, h->F));                                      // F -= (K + M/dt) G
-	RSD_CHECK(solve(ctx, h->K, cfg, h->F, U, rep));
+	if (fem) RSD_CHECK(solve_fem(ctx, h, inv, cfg, h->F, U, rep));
+	else RSD_CHECK(solve(ctx, h->K, cfg, h->F, U, rep));
 	if (host_out) {
 		// the new state is final: copy it to the host on the second stream while the residual pass runs
 		RSD_CUDA(cudaEventRecord(ctx->copyReady, ctx->stream));
@@ -322,6 +332,7 @@ int rsd_heat_be_step_host(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver
 int rsd_heat_newton(rsd_ctx* ctx, rsd_heat* h, double abs_tol, double rel_tol, int64_t max_iters,
                     const rsd_solver_cfg* lin, double* U, rsd_report* rep) {
 	if (!ctx || !h || !lin || !U) return set_error(RSD_EINVAL, "bad argument");
+	if (lin->operator_type != RSD_OP_CSR) return set_error(RSD_EINVAL, "Newton takes operator_type RSD_OP_CSR");
 	const int64_t n = h->n;
 	rsd_report R{};
 	double res0 = 0.0;

@@ -228,5 +228,9 @@ int assemble_vector(rsd_ctx* ctx, rsd_heat* h, int which, double coef, const dou
                     const double* operand, double* out, double outScale, bool accumulate);
 int assemble_diagonal(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, const double* U, double* d);
 int assemble_lift(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, double* F);
+int apply_operator(rsd_ctx* ctx, rsd_heat* h, double coef, const double* U, const double* V, double* out,
+                   const int32_t* skip);
+int solve_fem(rsd_ctx* ctx, rsd_heat* h, double coef, const rsd_solver_cfg* cfg, const double* b, double* x,
+              rsd_report* rep);
 int build_tables(rsd_ctx* ctx, rsd_heat* h);
 }  // namespace rsd

@@ -792,7 +792,137 @@ static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const d
 	return RSD_OK;
 }
 
+// ---- PCG over the matrix-free operator: cg/Solver.tpp:13-119 with the operator products of
+// FEMOperator::apply (linalg/operator/FEMOperator.hpp:39-43) and Jacobi::update over
+// FEMOperator::diagonal (FEMOperator.hpp:49-51).  The products are element passes (apply_operator),
+// the rest the FP64 CG kernels above. ------------------------------------------------------------
+
+// Jacobi::update's inversion (preconditioner/Jacobi.hpp:29-32): d = 1/d where |d| > 1e-300, else 1
+__global__ void k_inv_guarded(int64_t n, double* __restrict__ d) {
+	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+		const double v = d[i];
+		d[i] = (fabs(v) > 1e-300) ? 1.0 / v : 1.0;
+	}
+}
+
+// r holds A x on entry: r = b - A x; z = M r; p = z; rz = r.z; res0 = |r|   (Solver.tpp:31-63)
+__global__ void __launch_bounds__(256) k_fem_init(int64_t n, const double* __restrict__ b, double* __restrict__ r,
+                                                  double* __restrict__ p, const double* __restrict__ invD, CgScal* S,
+                                                  double* partials, double tol, int relMode, int64_t maxIters) {
+	double v[2] = {0.0, 0.0};
+	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+		const double ri = b[i] + (-1.0) * r[i];
+		const double zi = invD ? ri * invD[i] : ri;
+		r[i] = ri;
+		p[i] = zi;
+		v[0] += ri * ri;
+		v[1] += ri * zi;
+	}
+	if (grid_sum<2>(v, partials, &S->ticket)) {
+		const double res0 = sqrt(v[0]);
+		S->res0 = res0; S->rz = v[1]; S->iter = 0; S->res = res0;
+		S->refinements = 0; S->reliable = 0; S->status = 0;
+		const double crit = relMode ? res0 / (res0 + 1e-50) : res0;
+		if (crit < tol) { S->done = 1; S->converged = 1; }
+		else if (maxIters <= 1) { S->done = 1; S->converged = 0; S->iter = maxIters; }
+		else { S->done = 0; S->converged = 0; }
+	}
+}
+
+// alpha = rz / p.Ap   (Solver.tpp:69-73), Ap from the element pass
+__global__ void __launch_bounds__(256) k_fem_alpha(int64_t n, const double* __restrict__ p, const double* __restrict__ Ap,
+                                                   CgScal* S, double* partials) {
+	if (is_done(S)) return;
+	double v[1] = {0.0};
+	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+		v[0] += p[i] * Ap[i];
+	if (grid_sum<1>(v, partials, &S->ticket)) {
+		S->pAp = v[0];
+		S->alpha = S->rz / v[0];
+		if (!isfinite(S->alpha)) { S->done = 1; S->converged = 0; S->status = RSD_EBREAKDOWN; }
+	}
+}
+
+// |b - A x| into *out, A x in ax
+__global__ void __launch_bounds__(256) k_fem_true_res(int64_t n, const double* __restrict__ b, const double* __restrict__ ax,
+                                                      double* partials, unsigned* ticket, double* out) {
+	double v[1] = {0.0};
+	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+		const double d = b[i] + (-1.0) * ax[i];
+		v[0] += d * d;
+	}
+	if (grid_sum<1>(v, partials, ticket)) *out = sqrt(v[0]);
+}
+
+// Plain launches in chunks of 8 iterations behind a done-flag poll; after the solve has finished the
+// remaining launches of a chunk return at once (the element pass through its skip flag).
+static int cg_fem(rsd_ctx* ctx, rsd_heat* h, double coef, const rsd_solver_cfg* cfg, const double* b, double* x,
+                  rsd_report* rep) {
+	const int64_t n = h->n;
+	void* wsv;
+	const int64_t ns = pad_len(n);
+	RSD_CHECK(get_ws(ctx, sizeof(double) * 4 * ns, &wsv));
+	double* r = (double*)wsv;
+	double* p = r + ns;
+	double* Ap = p + ns;
+	double* invD = cfg->precond == RSD_JACOBI ? Ap + ns : nullptr;
+	const int xvec = reinterpret_cast<uintptr_t>(x) % 16 == 0;
+	CgScal* S = scal_slot(ctx, 0);
+	CgScal* S1 = scal_slot(ctx, 1);
+	double* partials = ctx->s.partials;
+	const int rel = cfg->tol_type == RSD_TOL_RELATIVE;
+	const double tol = cfg->tol;
+	const int64_t maxIt = cfg->max_iters;
+	cudaStream_t st = ctx->stream;
+	RSD_CUDA(cudaMemsetAsync(S, 0, sizeof(CgScal), st));
+	// Jacobi::update on every solve (cg/Solver.tpp:22); the operator's state is the iterate x
+	if (invD) {
+		RSD_CHECK(assemble_diagonal(ctx, h, 1.0, coef, x, invD));
+		k_inv_guarded<<<vec_grid(ctx, n), 256, 0, st>>>(n, invD);
+	}
+	RSD_CHECK(apply_operator(ctx, h, coef, x, x, r, nullptr));
+	k_fem_init<<<VG(k_fem_init), 256, 0, st>>>(n, b, r, p, invD, S, partials, tol, rel, maxIt);
+	RSD_CUDA(cudaGetLastError());
+	Poller poll{ctx, S, (int32_t*)ctx->s.hbuf};
+	RSD_CHECK(poll.init());
+	const int chunk = 8;
+	bool fin = false;
+	const GraphCtl off{0, 0, 0, 0};
+	for (int64_t it = 0; it < maxIt + 2 * chunk && !fin; it += chunk) {
+		for (int c = 0; c < chunk; ++c) {
+			RSD_CHECK(apply_operator(ctx, h, coef, x, p, Ap, &S->done));
+			k_fem_alpha<<<VG(k_fem_alpha), 256, 0, st>>>(n, p, Ap, S, partials);
+			k_cg_update<<<VGB(k_cg_update, kVT), kVT, 0, st>>>(n, x, r, p, Ap, invD, S, partials, tol, rel, maxIt, xvec);
+			k_cg_pupdate<<<VGB(k_cg_pupdate, kVT), kVT, 0, st>>>(n, p, r, invD, S, off);
+		}
+		RSD_CUDA(cudaGetLastError());
+		RSD_CHECK(poll.post(&fin));
+	}
+	RSD_CHECK(finish_report(ctx, S, rep));
+	// FP64 check of the final iterate: ||b - A x||
+	RSD_CHECK(apply_operator(ctx, h, coef, x, x, Ap, nullptr));
+	k_fem_true_res<<<VG(k_fem_true_res), 256, 0, st>>>(n, b, Ap, partials, &S1->ticket, &S1->res);
+	RSD_CUDA(cudaGetLastError());
+	double hres = 0.0;
+	RSD_CUDA(cudaMemcpyAsync(&hres, &S1->res, sizeof(double), cudaMemcpyDeviceToHost, st));
+	RSD_CUDA(cudaStreamSynchronize(st));
+	if (rep) rep->trueResidualRel = hres / (rep->initialResidual + 1e-50);
+	return RSD_OK;
+}
+
 }  // namespace
+
+int solve_fem(rsd_ctx* ctx, rsd_heat* h, double coef, const rsd_solver_cfg* cfg, const double* b, double* x,
+              rsd_report* rep) {
+	if (!ctx || !h || !cfg || (h->n && (!b || !x))) return set_error(RSD_EINVAL, "null argument");
+	if (cfg->max_iters < 0 || !(cfg->tol >= 0)) return set_error(RSD_EINVAL, "bad solver configuration");
+	if (cfg->type != RSD_CG) return set_error(RSD_EINVAL, "the matrix-free operator solves with CG (type RSD_CG)");
+	if (cfg->precision != RSD_FP64) return set_error(RSD_EINVAL, "the matrix-free operator solves in FP64 (precision RSD_FP64)");
+	if (rep) *rep = rsd_report{};
+	if (h->n == 0) { if (rep) rep->converged = 1; return RSD_OK; }
+	RSD_CUDA(cudaSetDevice(ctx->device));
+	return cg_fem(ctx, h, coef, cfg, b, x, rep);
+}
 
 void free_graph_cache(rsd_ctx* ctx) {
 	if (!ctx->graphs) return;
@@ -1122,6 +1252,8 @@ static int cg_fp64_static(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, c
 int solve(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const double* b, double* x, rsd_report* rep) {
 	if (!ctx || !A || !cfg || (A->n && (!b || !x))) return set_error(RSD_EINVAL, "null argument");
 	if (cfg->max_iters < 0 || !(cfg->tol >= 0)) return set_error(RSD_EINVAL, "bad solver configuration");
+	if (cfg->operator_type != RSD_OP_CSR)
+		return set_error(RSD_EINVAL, "a matrix solve takes operator_type RSD_OP_CSR (the matrix-free operator is rsd_heat_solve_fem)");
 	if (rep) *rep = rsd_report{};
 	if (A->n == 0) { if (rep) rep->converged = 1; return RSD_OK; }
 	RSD_CUDA(cudaSetDevice(ctx->device));
@@ -1143,8 +1275,8 @@ extern "C" int rsd_cg_solve_static(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cf
                                    rsd_report* rep) {
 	using namespace rsd;
 	if (!ctx || !A || !cfg || (A->n && (!b || !x))) return set_error(RSD_EINVAL, "null argument");
-	if (cfg->type != RSD_CG || cfg->precision != RSD_FP64)
-		return set_error(RSD_EINVAL, "rsd_cg_solve_static runs FP64 CG only (type RSD_CG, precision RSD_FP64)");
+	if (cfg->type != RSD_CG || cfg->precision != RSD_FP64 || cfg->operator_type != RSD_OP_CSR)
+		return set_error(RSD_EINVAL, "rsd_cg_solve_static runs FP64 CG on a matrix only (type RSD_CG, precision RSD_FP64, operator_type RSD_OP_CSR)");
 	if (cfg->max_iters < 0 || !(cfg->tol >= 0)) return set_error(RSD_EINVAL, "bad solver configuration");
 	if (A->n > kStaticMaxRows) {
 		char msg[160];

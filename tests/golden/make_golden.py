@@ -1,6 +1,6 @@
 """Generate the golden fixtures in this folder from the reference's own templates.
 
-    python tests/golden/make_golden.py [main] [adjoint]
+    python tests/golden/make_golden.py [main] [adjoint] [fem]
 
 Every array comes from oracle/_ref/libresiduum_ref.so, i.e. the unmodified Residuum templates
 (Assembler<CPU>, BoundaryApplicator<CPU>, TopologicalDOF, cg/gmres::Solver, SteadyStage,
@@ -113,7 +113,40 @@ def adjoint():
     save("adjoint_q1_hex_6x5x4.npz", theta=theta, T=T, Tobs=Tobs, lam=lam, g=g, grad=grad, fd_dir=d, fd=fd)
 
 
-GROUPS = {"main": main, "adjoint": adjoint}
+def fem():
+    # the matrix-free operator (LinearSolverConfig operator type "fem": FEMOperator, CG + Jacobi from
+    # the element diagonal) through the reference's own stages
+    r = oracle.Reference(3, 1, 2, [6, 5, 4], [0, 0, 0], [1, 1, 1], [0, 1, 2, 3], bc_kind=1, src_kind=1, src_c=1.0)
+    r.set_operator("fem")
+    U, rep = r.steady(0, 1, 1e-10, 1000)
+    save("fem_steady_q1_hex_6x5x4.npz", U=U, iterations=rep["iterations"], initialResidual=rep["initialResidual"],
+         finalResidual=rep["finalResidual"])
+    r = oracle.Reference(3, 1, 2, [6, 5, 4], [0, 0, 0], [1, 1, 1], list(range(6)), bc_kind=0)
+    r.set_operator("fem")
+    U0 = np.sin(np.arange(r.n) * 0.37)
+    U, res, rc, st = r.backward_euler(1e-2, 5, U0, tol=1e-8, stats=True)
+    assert rc == 0
+    save("fem_be_q1_hex_6x5x4.npz", U0=U0, U=U, residual=res, iterations=st[:, 2].astype(np.int64))
+    ke = np.exp(np.random.default_rng(7).standard_normal(15))
+    r = oracle.Reference(2, 2, 3, [5, 3], [0, 0], [1, 1], [0, 1, 2, 3], bc_kind=2, src_kind=0, src_c=1.0, k_elem=ke)
+    r.set_operator("fem")
+    U, rep = r.steady(0, 1, 1e-10, 1000)
+    save("fem_steady_q2_quad_kelem.npz", k_elem=ke, U=U, iterations=rep["iterations"])
+    r = oracle.Reference(3, 2, 3, [3, 3, 2], [0, 0, 0], [1, 1, 1], [0, 1], bc_kind=0, bc_val={0: 0.0, 1: 1.0},
+                         src_kind=0, src_c=10.0)
+    r.set_operator("fem")
+    U, rep = r.steady(0, 1, 1e-10, 1000)
+    save("fem_steady_q2_hex_3x3x2.npz", U=U, iterations=rep["iterations"])
+    # k(T) = 1 + 0.5 T in a linear stage: the operator's state is the solve's own iterate (the stage
+    # binds its state to U, which the solver updates in place), so the operator changes as CG runs
+    r = oracle.Reference(3, 2, 3, [3, 3, 2], [0, 0, 0], [1, 1, 1], [0, 1], bc_kind=0, bc_val={0: 0.0, 1: 1.0},
+                         src_kind=0, src_c=10.0, k_a=1.0, k_b=0.5)
+    r.set_operator("fem")
+    U, rep = r.steady(0, 1, 1e-12, 1000)
+    save("fem_steady_q2_hex_kT.npz", U=U, iterations=rep["iterations"], converged=rep["converged"])
+
+
+GROUPS = {"main": main, "adjoint": adjoint, "fem": fem}
 
 if __name__ == "__main__":
     if not oracle.reference_available():

@@ -193,6 +193,52 @@ def test_restatement_matches_reference_bcs_time_dependent():
     assert (Uo == Ur).all() and (reso == resr).all()
 
 
+def test_restatement_matrix_free_operator_matches_golden():
+    # the reference stages with operator type "fem" (FEMOperator): steady, Backward Euler and a
+    # state-dependent k(T) whose operator follows the CG iterate; the restatement is bit-exact
+    m = oracle.BlockMesh(3, [6, 5, 4], [0, 0, 0], [1, 1, 1], 1)
+    o = oracle.Oracle(m, 2, bc={t: "x" for t in range(4)}, src_expr="x*y*z")
+    o.set_operator("fem")
+    U, rep = o.steady(tol=1e-10)
+    g = golden("fem_steady_q1_hex_6x5x4.npz")
+    assert rep["iterations"] == g["iterations"] and (U == g["U"]).all()
+    o = oracle.Oracle(m, 2, bc={t: "0" for t in range(6)})
+    o.set_operator("fem")
+    g = golden("fem_be_q1_hex_6x5x4.npz")
+    U, res, its, rc = o.backward_euler(1e-2, 5, g["U0"], tol=1e-8)
+    assert rc == 0 and (its == g["iterations"]).all() and (U == g["U"]).all() and (res == g["residual"]).all()
+    g = golden("fem_steady_q2_quad_kelem.npz")
+    m2 = oracle.BlockMesh(2, [5, 3], [0, 0], [1, 1], 2)
+    o = oracle.Oracle(m2, 3, bc={t: "(1-x)*(1-y)" for t in range(4)}, src_expr="1", k_elem=g["k_elem"])
+    o.set_operator("fem")
+    U, rep = o.steady(tol=1e-10)
+    assert rep["iterations"] == g["iterations"] and (U == g["U"]).all()
+    m3 = oracle.BlockMesh(3, [3, 3, 2], [0, 0, 0], [1, 1, 1], 2)
+    for name, kw, tol in (("fem_steady_q2_hex_3x3x2.npz", {}, 1e-10),
+                          ("fem_steady_q2_hex_kT.npz", dict(k_expr="1 + 0.5*T", dk_expr="0.5"), 1e-12)):
+        g = golden(name)
+        o = oracle.Oracle(m3, 3, bc={0: "0", 1: "1"}, src_expr="10", **kw)
+        o.set_operator("fem")
+        U, rep = o.steady(tol=tol)
+        assert rep["iterations"] == g["iterations"] and (U == g["U"]).all()
+    # matrix-free and assembled operators solve the same constant-k system
+    o = oracle.Oracle(m, 2, bc={0: "0", 1: "1"}, src_expr="1")
+    Uc, rc_ = o.steady(tol=1e-12)
+    o.set_operator("fem")
+    Uf, rf = o.steady(tol=1e-12)
+    assert abs(rc_["iterations"] - rf["iterations"]) <= 1
+    assert np.max(np.abs(Uf - Uc)) <= 1e-12 * np.max(np.abs(Uc))
+
+
+@pytest.mark.skipif(not oracle.reference_available(), reason="oracle/_ref not built (reference tree absent)")
+def test_matrix_free_fixtures_reproduce_from_reference():
+    r = oracle.Reference(3, 1, 2, [6, 5, 4], [0, 0, 0], [1, 1, 1], list(range(6)), bc_kind=0)
+    r.set_operator("fem")
+    g = golden("fem_be_q1_hex_6x5x4.npz")
+    U, res, rc = r.backward_euler(1e-2, 5, g["U0"], tol=1e-8)
+    assert rc == 0 and (U == g["U"]).all() and (res == g["residual"]).all()
+
+
 def test_blockmesh_generator_matches_restatement():
     rsd = load_package()
     from importlib import import_module
