@@ -94,6 +94,7 @@ struct AsmParams {
 	double outScale;
 	// vector kernels: the whole launch returns at once when *skip != 0 (a finished solve's flag), or null
 	const int32_t* __restrict__ skip;
+	const int32_t* __restrict__ erow;   // [e][a]: the free row of node a of element e (-1: constrained), or null
 };
 
 template <int NSD, int P>
@@ -765,6 +766,297 @@ __global__ void __launch_bounds__(256) k_asm_vector_elem(const AsmParams prm) {
 	}
 }
 
+// 1D Lagrange values and derivatives at the Gauss points, [q][j] = N_j(xi_q), N_j'(xi_q), and the
+// Gauss weights: the factors of the tensor-product shape functions and quadrature
+struct Tab1D {
+	double B[4][4], D[4][4], w[4];
+};
+
+// The operator product (which 4: Diffusion + coef*Mass on the operand, gathered Free) of an all-affine
+// mesh of tensor-product elements with P+1 Gauss points per direction, by sum factorization.  A
+// group of G lanes holds one element, lane a on node a = ix + N1 iy + N1^2 iz, which is also
+// quadrature point (ix, iy, iz).  Reference gradients and values at the points come from 1D
+// contractions along x, y, z (the values of the other lanes along one axis by shuffle); the flux
+// w |J| k C grad (C = J^-1 J^-T from the element's coefficients, the same integrals as the tables of
+// the affine path, evaluated by the same Gauss rule) and the mass term go back by the transposed
+// contractions.  Per element that is 2 x (1 + 2 + 3) contractions of N1 shuffles in 3D instead of
+// NPE^2 table entries per form.
+template <int NSD, int P>
+__global__ void __launch_bounds__(256) k_apply_sumfac(const AsmParams prm, const Tab1D tab) {
+	using E = Elem<NSD, P>;
+	constexpr int N1 = P + 1, NPE = E::NPE, G = E::G, EPW = 32 / G;
+	static_assert(NPE <= 32, "one element per group of at most 32 lanes");
+	if (prm.skip && *(volatile const int32_t*)prm.skip) return;   // uniform over the launch
+	__shared__ Tab1D st;
+	if (threadIdx.x == 0) st = tab;
+	__syncthreads();
+	const int lane = threadIdx.x & 31, a = lane % G, base = lane - a;
+	const bool act = a < NPE;
+	const int ax = act ? a % N1 : 0, ay = act ? (a / N1) % N1 : 0, az = (act && NSD == 3) ? a / (N1 * N1) : 0;
+	// the lane's rows (forward) and columns (backward) of the 1D factors, read from shared memory
+	const double* Bx = st.B[ax];
+	const double* Dx = st.D[ax];
+	const double* By = st.B[ay];
+	const double* Dy = st.D[ay];
+	const double* Bz = st.B[az];
+	const double* Dz = st.D[az];
+	auto BT = [&](int q, int i) { return st.B[q][i]; };
+	auto DT = [&](int q, int i) { return st.D[q][i]; };
+	const double wq = st.w[ax] * st.w[ay] * (NSD == 3 ? st.w[az] : 1.0);
+	const double k0 = prm.kExpr.n ? eval_expr(prm.kExpr, 0.0, 0.0, 0.0, 0.0, 0.0) : prm.kConst;
+	const double massc = prm.coef * prm.rho * prm.cp;
+	// the value of lane (i, j, k) of this group
+	auto at = [&](double v, int i, int j, int k) { return __shfl_sync(0xffffffffu, v, base + i + N1 * j + N1 * N1 * k); };
+	const int64_t warpId = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const int64_t step = (((int64_t)gridDim.x * blockDim.x) >> 5) * EPW;
+	auto rowOf = [&](int64_t ee) -> int32_t { return (act && ee < prm.nelem) ? prm.erow[ee * NPE + a] : -1; };
+	auto valOf = [&](int32_t r) -> double { return (r >= 0 && prm.V) ? prm.V[r] : 0.0; };
+	// loads run ahead of the element being computed: its operand values one element ahead, the rows two
+	const int64_t e0 = warpId * EPW + lane / G;
+	int32_t rowCur = rowOf(e0), rowNext = rowOf(e0 + step);
+	double uCur = valOf(rowCur);
+	for (int64_t eb = warpId * EPW; eb < prm.nelem; eb += step) {
+		const int64_t e = eb + lane / G;
+		const bool in = e < prm.nelem;
+		const int32_t row = rowCur;
+		const double u = uCur;
+		uCur = valOf(rowNext);
+		rowCur = rowNext;
+		rowNext = rowOf(e + 2 * step);
+		double c[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, detJ = 0.0, ke = 1.0;
+		if (in) {
+			const double2* gp2 = reinterpret_cast<const double2*>(prm.geo + e * 8);
+			const double2 g0 = gp2[0], g1 = gp2[1], g2 = gp2[2], g3 = gp2[3];
+			c[0] = g0.x; c[1] = g0.y; c[2] = g1.x; c[3] = g1.y; c[4] = g2.x; c[5] = g2.y; detJ = g3.x;
+			if (prm.kElem) ke = prm.kElem[e];
+		}
+		double F = 0.0;
+		if constexpr (NSD == 3) {
+			// forward: x, then y, then z
+			double xb = 0.0, xd = 0.0;
+#pragma unroll
+			for (int j = 0; j < N1; ++j) { const double v = at(u, j, ay, az); xb += Bx[j] * v; xd += Dx[j] * v; }
+			double ybb = 0.0, ydb = 0.0, ybd = 0.0;
+#pragma unroll
+			for (int j = 0; j < N1; ++j) {
+				const double vb = at(xb, ax, j, az), vd = at(xd, ax, j, az);
+				ybb += By[j] * vb; ydb += Dy[j] * vb; ybd += By[j] * vd;
+			}
+			double val = 0.0, gz = 0.0, gy = 0.0, gx = 0.0;
+#pragma unroll
+			for (int j = 0; j < N1; ++j) {
+				const double vbb = at(ybb, ax, ay, j), vdb = at(ydb, ax, ay, j), vbd = at(ybd, ax, ay, j);
+				val += Bz[j] * vbb; gz += Dz[j] * vbb; gy += Bz[j] * vdb; gx += Bz[j] * vbd;
+			}
+			// the point's flux and mass term (c: C00, C11, C22, C01, C02, C12)
+			const double s = ke * k0 * detJ * wq;
+			const double fx = s * (c[0] * gx + c[3] * gy + c[4] * gz);
+			const double fy = s * (c[3] * gx + c[1] * gy + c[5] * gz);
+			const double fz = s * (c[4] * gx + c[5] * gy + c[2] * gz);
+			const double m = massc * detJ * wq * val;
+			// backward: z, then y, then x (transposed factors)
+			double A1 = 0.0, A2 = 0.0, A3 = 0.0;
+#pragma unroll
+			for (int q = 0; q < N1; ++q) {
+				const double vx = at(fx, ax, ay, q), vy = at(fy, ax, ay, q), vz = at(fz, ax, ay, q), vm = at(m, ax, ay, q);
+				const double bq = BT(q, az);
+				A1 += bq * vx; A2 += bq * vy; A3 += DT(q, az) * vz + bq * vm;
+			}
+			double C1 = 0.0, C2 = 0.0;
+#pragma unroll
+			for (int q = 0; q < N1; ++q) {
+				const double v1 = at(A1, ax, q, az), v2 = at(A2, ax, q, az), v3 = at(A3, ax, q, az);
+				const double bq = BT(q, ay);
+				C1 += bq * v1; C2 += DT(q, ay) * v2 + bq * v3;
+			}
+#pragma unroll
+			for (int q = 0; q < N1; ++q) {
+				const double v1 = at(C1, q, ay, az), v2 = at(C2, q, ay, az);
+				F += DT(q, ax) * v1 + BT(q, ax) * v2;
+			}
+		} else {
+			double xb = 0.0, xd = 0.0;
+#pragma unroll
+			for (int j = 0; j < N1; ++j) { const double v = at(u, j, ay, 0); xb += Bx[j] * v; xd += Dx[j] * v; }
+			double val = 0.0, gy = 0.0, gx = 0.0;
+#pragma unroll
+			for (int j = 0; j < N1; ++j) {
+				const double vb = at(xb, ax, j, 0), vd = at(xd, ax, j, 0);
+				val += By[j] * vb; gy += Dy[j] * vb; gx += By[j] * vd;
+			}
+			// c: C00, C11, C01
+			const double s = ke * k0 * detJ * wq;
+			const double fx = s * (c[0] * gx + c[2] * gy);
+			const double fy = s * (c[2] * gx + c[1] * gy);
+			const double m = massc * detJ * wq * val;
+			double A1 = 0.0, A2 = 0.0;
+#pragma unroll
+			for (int q = 0; q < N1; ++q) {
+				const double vx = at(fx, ax, q, 0), vy = at(fy, ax, q, 0), vm = at(m, ax, q, 0);
+				const double bq = BT(q, ay);
+				A1 += bq * vx; A2 += DT(q, ay) * vy + bq * vm;
+			}
+#pragma unroll
+			for (int q = 0; q < N1; ++q) {
+				const double v1 = at(A1, q, ay, 0), v2 = at(A2, q, ay, 0);
+				F += DT(q, ax) * v1 + BT(q, ax) * v2;
+			}
+		}
+		if (row >= 0) atomicAdd(prm.out + row, prm.outScale * F);
+	}
+}
+
+// The same product for 27-node hexahedra with one lane per grid line of the element: a warp holds 3
+// elements, lane (p, r) of an element owns the line of 3 values along the axis of the current stage,
+// so each 1D contraction is local to the lane (its 3x3 factors are compile-time indices into the
+// kernel's parameters) and values cross lanes only between stages, through shared memory: 6 line
+// exchanges per element instead of a shuffle per value and factor.
+__global__ void __launch_bounds__(256) k_apply_hex27_lines(const AsmParams prm, const Tab1D t) {
+	// shared-memory layout of one element's arrays: point (x, y, z) at x + 4y + 11z, 33 entries per
+	// array, 3 arrays per element; within an element the 9 lanes of every exchange (a fixed x, y or z)
+	// then fall in distinct banks, and the third element of a warp is shifted by 11 entries to reduce
+	// the conflicts with the second one in the same half-warp
+	constexpr int EPW = 3, NPE = 27, WPB = 8, ARR = 33, SLOT = 3 * ARR, WARPBUF = EPW * SLOT + 11;
+	if (prm.skip && *(volatile const int32_t*)prm.skip) return;   // uniform over the launch
+	__shared__ double sbuf[WPB * WARPBUF];
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	const bool act = lane < EPW * 9;   // lanes 27-31 compute along but write nothing
+	const int slot = act ? lane / 9 : 0, l = lane % 9, p = l % 3, r = l / 3;
+	double* buf = sbuf + warp * WARPBUF + slot * SLOT + (slot == 2 ? 11 : 0);
+	// buffer entry of array k (0..2) at point (x, y, z)
+	auto at = [&](int k, int x, int y, int z) -> double& { return buf[k * ARR + x + 4 * y + 11 * z]; };
+	const double k0 = prm.kExpr.n ? eval_expr(prm.kExpr, 0.0, 0.0, 0.0, 0.0, 0.0) : prm.kConst;
+	const double massc = prm.coef * prm.rho * prm.cp;
+	const int64_t warpId = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const int64_t step = (((int64_t)gridDim.x * blockDim.x) >> 5) * EPW;
+	// the rows and operand values of this lane's x-line (nodes (i, p, r)) of element ee
+	auto load = [&](int64_t ee, int32_t (&rw)[3], double (&uv)[3]) {
+#pragma unroll
+		for (int i = 0; i < 3; ++i) rw[i] = (act && ee < prm.nelem) ? prm.erow[ee * NPE + i + 3 * p + 9 * r] : -1;
+#pragma unroll
+		for (int i = 0; i < 3; ++i) uv[i] = (rw[i] >= 0 && prm.V) ? prm.V[rw[i]] : 0.0;
+	};
+	int32_t rowN[3];
+	double uN[3];
+	load(warpId * EPW + slot, rowN, uN);
+	for (int64_t eb = warpId * EPW; eb < prm.nelem; eb += step) {
+		const int64_t e = eb + slot;
+		const bool in = act && e < prm.nelem;
+		int32_t row[3];
+		double u[3];
+#pragma unroll
+		for (int i = 0; i < 3; ++i) { row[i] = rowN[i]; u[i] = uN[i]; }
+		load(e + step, rowN, uN);   // the next element's line, in flight during this one
+		double c[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, detJ = 0.0, ke = 1.0;
+		if (in) {
+			const double2* gp2 = reinterpret_cast<const double2*>(prm.geo + e * 8);
+			const double2 g0 = gp2[0], g1 = gp2[1], g2 = gp2[2], g3 = gp2[3];
+			c[0] = g0.x; c[1] = g0.y; c[2] = g1.x; c[3] = g1.y; c[4] = g2.x; c[5] = g2.y; detJ = g3.x;
+			if (prm.kElem) ke = prm.kElem[e];
+		}
+		// x: lane (p, r) = line (y, z); B and D of u along x
+		{
+			double xb[3], xd[3];
+#pragma unroll
+			for (int q = 0; q < 3; ++q) {
+				xb[q] = t.B[q][0] * u[0] + t.B[q][1] * u[1] + t.B[q][2] * u[2];
+				xd[q] = t.D[q][0] * u[0] + t.D[q][1] * u[1] + t.D[q][2] * u[2];
+			}
+			__syncwarp();
+#pragma unroll
+			for (int q = 0; q < 3; ++q) if (act) { at(0, q, p, r) = xb[q]; at(1, q, p, r) = xd[q]; }
+			__syncwarp();
+		}
+		// y: lane (p, r) = line (x, z)
+		{
+			double vb[3], vd[3];
+#pragma unroll
+			for (int j = 0; j < 3; ++j) { vb[j] = at(0, p, j, r); vd[j] = at(1, p, j, r); }
+			double bb[3], db[3], bd[3];
+#pragma unroll
+			for (int q = 0; q < 3; ++q) {
+				bb[q] = t.B[q][0] * vb[0] + t.B[q][1] * vb[1] + t.B[q][2] * vb[2];
+				db[q] = t.D[q][0] * vb[0] + t.D[q][1] * vb[1] + t.D[q][2] * vb[2];
+				bd[q] = t.B[q][0] * vd[0] + t.B[q][1] * vd[1] + t.B[q][2] * vd[2];
+			}
+			__syncwarp();
+#pragma unroll
+			for (int q = 0; q < 3; ++q) if (act) { at(0, p, q, r) = bb[q]; at(1, p, q, r) = db[q]; at(2, p, q, r) = bd[q]; }
+			__syncwarp();
+		}
+		// z: lane (p, r) = line (x, y); values and reference gradients at the points (p, r, q), the
+		// flux and mass term there, and back along z
+		{
+			double vbb[3], vdb[3], vbd[3];
+#pragma unroll
+			for (int j = 0; j < 3; ++j) { vbb[j] = at(0, p, r, j); vdb[j] = at(1, p, r, j); vbd[j] = at(2, p, r, j); }
+			double fx[3], fy[3], fz[3], m[3];
+			const double s0 = ke * k0 * detJ * t.w[p] * t.w[r];
+			const double m0 = massc * detJ * t.w[p] * t.w[r];
+#pragma unroll
+			for (int q = 0; q < 3; ++q) {
+				const double val = t.B[q][0] * vbb[0] + t.B[q][1] * vbb[1] + t.B[q][2] * vbb[2];
+				const double gz = t.D[q][0] * vbb[0] + t.D[q][1] * vbb[1] + t.D[q][2] * vbb[2];
+				const double gy = t.B[q][0] * vdb[0] + t.B[q][1] * vdb[1] + t.B[q][2] * vdb[2];
+				const double gx = t.B[q][0] * vbd[0] + t.B[q][1] * vbd[1] + t.B[q][2] * vbd[2];
+				const double s = s0 * t.w[q];
+				fx[q] = s * (c[0] * gx + c[3] * gy + c[4] * gz);
+				fy[q] = s * (c[3] * gx + c[1] * gy + c[5] * gz);
+				fz[q] = s * (c[4] * gx + c[5] * gy + c[2] * gz);
+				m[q] = m0 * t.w[q] * val;
+			}
+			double A1[3], A2[3], A3[3];
+#pragma unroll
+			for (int k = 0; k < 3; ++k) {
+				A1[k] = t.B[0][k] * fx[0] + t.B[1][k] * fx[1] + t.B[2][k] * fx[2];
+				A2[k] = t.B[0][k] * fy[0] + t.B[1][k] * fy[1] + t.B[2][k] * fy[2];
+				A3[k] = t.D[0][k] * fz[0] + t.D[1][k] * fz[1] + t.D[2][k] * fz[2]
+				      + t.B[0][k] * m[0] + t.B[1][k] * m[1] + t.B[2][k] * m[2];
+			}
+			__syncwarp();
+#pragma unroll
+			for (int k = 0; k < 3; ++k) if (act) { at(0, p, r, k) = A1[k]; at(1, p, r, k) = A2[k]; at(2, p, r, k) = A3[k]; }
+			__syncwarp();
+		}
+		// y back: lane (p, r) = line (x, z)
+		{
+			double v1[3], v2[3], v3[3];
+#pragma unroll
+			for (int q = 0; q < 3; ++q) { v1[q] = at(0, p, q, r); v2[q] = at(1, p, q, r); v3[q] = at(2, p, q, r); }
+			double C1[3], C2[3];
+#pragma unroll
+			for (int k = 0; k < 3; ++k) {
+				C1[k] = t.B[0][k] * v1[0] + t.B[1][k] * v1[1] + t.B[2][k] * v1[2];
+				C2[k] = t.D[0][k] * v2[0] + t.D[1][k] * v2[1] + t.D[2][k] * v2[2]
+				      + t.B[0][k] * v3[0] + t.B[1][k] * v3[1] + t.B[2][k] * v3[2];
+			}
+			__syncwarp();
+#pragma unroll
+			for (int k = 0; k < 3; ++k) if (act) { at(0, p, k, r) = C1[k]; at(1, p, k, r) = C2[k]; }
+			__syncwarp();
+		}
+		// x back: lane (p, r) = line (y, z), the nodes of its x-line
+		{
+			double v1[3], v2[3];
+#pragma unroll
+			for (int q = 0; q < 3; ++q) { v1[q] = at(0, q, p, r); v2[q] = at(1, q, p, r); }
+#pragma unroll
+			for (int k = 0; k < 3; ++k) {
+				const double F = t.D[0][k] * v1[0] + t.D[1][k] * v1[1] + t.D[2][k] * v1[2]
+				               + t.B[0][k] * v2[0] + t.B[1][k] * v2[1] + t.B[2][k] * v2[2];
+				if (row[k] >= 0) atomicAdd(prm.out + row[k], prm.outScale * F);
+			}
+		}
+	}
+}
+
+// erow[e][a] = t2a[ien[e][a]]
+__global__ void k_build_erow(int64_t count, const int32_t* __restrict__ ien, const int32_t* __restrict__ t2a,
+                             int32_t* __restrict__ erow) {
+	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
+		erow[i] = t2a[ien[i]];
+}
+
 // Assembler::assembleDiagonal (Assembler.tpp:142-197) for c_diff*Diffusion + c_mass*Mass
 template <int NSD, int P>
 __global__ void __launch_bounds__(kAsmThreads) k_asm_diag(const AsmParams prm) {
@@ -1213,6 +1505,9 @@ int assemble_matrix(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, doubl
 	return rc;
 }
 
+int apply_operator(rsd_ctx* ctx, rsd_heat* h, double coef, const double* U, const double* V, double* out,
+                   const int32_t* skip);
+
 // the affine path of the vector kernels: every mode but the adjoint, with no state-dependent
 // conductivity and no load term (both are evaluated per quadrature point)
 static int affine_vector(rsd_ctx* ctx, rsd_heat* h, AsmParams& p) {
@@ -1226,6 +1521,7 @@ static int affine_vector(rsd_ctx* ctx, rsd_heat* h, AsmParams& p) {
 
 int assemble_vector(rsd_ctx* ctx, rsd_heat* h, int which, double coef, const double* U, const double* Udot,
                     const double* operand, double* out, double outScale, bool accumulate) {
+	if (which == 4 && !accumulate && outScale == 1.0) return apply_operator(ctx, h, coef, U, operand, out, nullptr);
 	AsmParams p = params_for(h);
 	p.which = which; p.coef = coef; p.U = U; p.Udot = Udot; p.V = operand; p.out = out; p.outScale = outScale;
 	if (which == 7 && h->gPrevValid) p.gPrev = h->gPrev;
@@ -1243,6 +1539,9 @@ int assemble_vector(rsd_ctx* ctx, rsd_heat* h, int which, double coef, const dou
 // FEMOperator::apply (linalg/operator/FEMOperator.hpp:39-43) for the forms Diffusion + coef * Mass:
 // out = A(U) V over the free DOFs, the operand gathered Free (zero on constrained nodes) and the state
 // U (Full) read only through k(T).  With skip, the element kernel returns at once once *skip != 0.
+// Meshes of order 2 and 3 whose elements are all affine, with P+1 Gauss points per direction and at
+// most 32 nodes per element, take the sum-factorized kernel (RSD_SUMFAC=0: the table kernels);
+// 4- and 8-node elements keep the one-thread-per-element table kernel, which measured faster for them.
 int apply_operator(rsd_ctx* ctx, rsd_heat* h, double coef, const double* U, const double* V, double* out,
                    const int32_t* skip) {
 	AsmParams p = params_for(h);
@@ -1250,7 +1549,51 @@ int apply_operator(rsd_ctx* ctx, rsd_heat* h, double coef, const double* U, cons
 	RSD_CHECK(affine_vector(ctx, h, p));
 	RSD_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * std::max<int64_t>(h->n, 1), ctx->stream));
 	const int pr = prof_begin(ctx, PF_ASM_VECTOR);
-	const int rc = launch_k_asm_vector(ctx, h, p);
+	const int nsd = h->m->nsd, ord = h->m->order;
+	const int n1 = ord + 1, nq1 = h->nq1;
+	const char* env = getenv("RSD_SUMFAC");
+	int rc;
+	if (p.fast && p.pts == 0 && nq1 == n1 && ord >= 2 && h->m->npe <= 32 && p.nelem > 0 && !(env && env[0] == '0')) {
+		if (!h->erow) {
+			// the element -> free-row map, once per problem
+			const int64_t cnt = h->m->nelem * h->m->npe;
+			int32_t* er = nullptr;
+			RSD_CUDA(cudaMalloc(&er, sizeof(int32_t) * std::max<int64_t>(cnt, 1)));
+			h->erow = er;
+			k_build_erow<<<vec_grid(ctx, cnt), 256, 0, ctx->stream>>>(cnt, h->m->ien, h->t2a, h->erow);
+			RSD_CUDA(cudaGetLastError());
+		}
+		p.erow = h->erow;
+		Tab1D t{};
+		double xq[5], wq[5], N[4], dN[4];
+		gauss_legendre(n1, xq, wq);
+		for (int q = 0; q < n1; ++q) {
+			lagrange1d(ord, xq[q], N, dN);
+			for (int j = 0; j < n1; ++j) { t.B[q][j] = N[j]; t.D[q][j] = dN[j]; }
+			t.w[q] = wq[q];
+		}
+		const int epw = 32 / group_width(h->m->npe);
+		const int64_t warpsNeeded = (p.nelem + epw - 1) / epw;
+		const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((warpsNeeded + 7) / 8, (int64_t)ctx->num_sms * 8));
+		auto go = [&](auto kern) -> int {
+			kern<<<blocks, 256, 0, ctx->stream>>>(p, t);
+			RSD_CUDA(cudaGetLastError());
+			return RSD_OK;
+		};
+		const char* lines = getenv("RSD_SUMFAC_LINES");
+		if (nsd == 2 && ord == 2) rc = go(k_apply_sumfac<2, 2>);
+		else if (nsd == 2 && ord == 3) rc = go(k_apply_sumfac<2, 3>);
+		else if (lines && lines[0] == '0') rc = go(k_apply_sumfac<3, 2>);
+		else {
+			const int64_t wn = (p.nelem + 2) / 3;
+			const int b = (int)std::max<int64_t>(1, std::min<int64_t>((wn + 7) / 8, (int64_t)ctx->num_sms * 8));
+			k_apply_hex27_lines<<<b, 256, 0, ctx->stream>>>(p, t);
+			RSD_CUDA(cudaGetLastError());
+			rc = RSD_OK;
+		}
+	} else {
+		rc = launch_k_asm_vector(ctx, h, p);
+	}
 	prof_end(ctx, pr);
 	return rc;
 }

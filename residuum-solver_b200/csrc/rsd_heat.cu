@@ -74,7 +74,7 @@ __global__ void k_diff_norm(int64_t n, const double* __restrict__ F, const doubl
 
 static void free_heat(rsd_heat* h) {
 	cudaFree(h->t2a); cudaFree(h->g); cudaFree(h->kElem); cudaFree(h->tables); cudaFree(h->bElems); cudaFree(h->gPrev);
-	cudaFree(h->ranks); cudaFree(h->affine); cudaFree(h->geo); cudaFree(h->ktab); cudaFree(h->adjPtr); cudaFree(h->adj);
+	cudaFree(h->ranks); cudaFree(h->affine); cudaFree(h->geo); cudaFree(h->ktab); cudaFree(h->adjPtr); cudaFree(h->adj); cudaFree(h->erow);
 	cudaFree(h->hostU); cudaFree(h->hostUprev);
 	cudaFree(h->F); cudaFree(h->R); cudaFree(h->Udot); cudaFree(h->ms); cudaFree(h->dU);
 	if (h->K) rsd_csr_destroy(h->K);

@@ -210,6 +210,7 @@ struct rsd_heat {
 	// row -> (element, local node) adjacency of the free rows, element order (row-gather assembly)
 	int32_t* adjPtr = nullptr;      // device, n + 1
 	int32_t* adj = nullptr;         // device, e * npe + a
+	int32_t* erow = nullptr;        // device, [e][a]: t2a[ien[e][a]] (sum-factorized operator products), or null
 	bool adjTried = false;
 	int32_t maxSlice = 0;           // longest SELL-32 slice of K, in entries per row
 	// stage scratch

@@ -107,6 +107,41 @@ def test_matrix_free_solve_matches_csr_solve(rsd, ctx, nsd, order, nq, nel):
     assert relerr(d2.download(), d1.download()) <= REL
 
 
+@pytest.mark.parametrize("nsd,order,nel", [(2, 1, [13, 9]), (2, 2, [7, 5]), (2, 3, [5, 4]), (3, 1, [7, 6, 5]),
+                                           (3, 2, [4, 3, 3])])
+def test_sum_factorized_product_matches_tables_and_matrix(rsd, ctx, monkeypatch, nsd, order, nel):
+    # all-affine meshes with P+1 points per direction take the sum-factorized kernel; the table
+    # kernel (RSD_SUMFAC=0) and the assembled matrix give the same product
+    lo, hi = [0.0] * nsd, [1.0, 2.0, 1.5][:nsd]
+    rng = np.random.default_rng(5)
+    ke = np.exp(rng.standard_normal(int(np.prod(nel))))
+    h = make_heat(rsd, ctx, nsd, order, order + 1, nel, lo, hi, k_elem=ke, rho=1.3, cp=0.7, k_const=2.5,
+                  dirichlet={0: "0", 2: "1"})
+    c = 11.0
+    v = ctx.to_device(rng.standard_normal(h.n))
+    y1, y2, y3 = ctx.array(h.n), ctx.array(h.n), ctx.array(h.n)
+    h.assemble_matrix(1.0, c)
+    h.K.spmv(v, y1)
+    h.assemble_vector(4, y2, coef=c, operand=v)
+    monkeypatch.setenv("RSD_SUMFAC", "0")
+    h.assemble_vector(4, y3, coef=c, operand=v)
+    assert relerr(y2.download(), y1.download()) <= REL
+    assert relerr(y3.download(), y1.download()) <= REL
+    if nsd == 3 and order == 2:
+        # the 27-node kernel by lanes per node (shuffles) instead of lanes per grid line
+        monkeypatch.setenv("RSD_SUMFAC", "1")
+        monkeypatch.setenv("RSD_SUMFAC_LINES", "0")
+        h.assemble_vector(4, y3, coef=c, operand=v)
+        assert relerr(y3.download(), y1.download()) <= REL
+        monkeypatch.delenv("RSD_SUMFAC_LINES")
+    # the diffusion operator alone (coef 0)
+    monkeypatch.delenv("RSD_SUMFAC")
+    h.assemble_matrix(1.0, 0.0)
+    h.K.spmv(v, y1)
+    h.assemble_vector(4, y2, coef=0.0, operand=v)
+    assert relerr(y2.download(), y1.download()) <= REL
+
+
 def test_identity_preconditioner_and_limits(rsd, ctx):
     h = make_heat(rsd, ctx, 3, 1, 2, [6, 5, 4], [0, 0, 0], [1, 1, 1], src_expr="1", dirichlet={t: "0" for t in range(6)})
     F = ctx.array(h.n)
