@@ -469,6 +469,105 @@ def run_newton(rsd, ctx, stream, S):
     return out
 
 
+def fem_steady(rsd, ctx, stream, S, op, reps=3):
+    """Steady linear heat on S^3 Q2 hexes (k = 1, f = 10, T = 0 on x = 0 and 1 on x = 1), CG + Jacobi
+    in FP64 to 1e-8 from x0 = 0 with the assembled matrix (op CSR: assembly + solve) or the matrix-free
+    operator (op FEM: the solve's products are element passes); median of reps event-timed stages."""
+    import torch
+    from importlib import import_module
+    bm = import_module("residuum_solver_b200.blockmesh")
+    xyz, ien, rg = bm.block_mesh(3, [S] * 3, [0, 0, 0], [1, 1, 1], 2)
+    h = rsd.Heat(ctx, rsd.Mesh(ctx, 3, 2, xyz, ien, rg), 3, src_expr="10", dirichlet={0: "0", 1: "1"})
+    cfg = rsd.SolverConfig.make(type=rsd.CG, precond=rsd.JACOBI, precision=rsd.FP64, tol=1e-8, max_iters=100000,
+                                operator_type=op)
+    U = ctx.array(h.n).zero()
+    h.steady(U, cfg=cfg)            # warm-up (tables, maps, workspace)
+    ts = []
+    for _ in range(reps):
+        U.zero()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rep = h.steady(U, cfg=cfg)
+        e1.record(stream)
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return h, U.download(), rep, float(np.median(ts))
+
+
+def run_fem_operator(rsd, ctx, stream, S):
+    """The matrix-free operator (operator type fem) against the assembled matrix on S^3 Q2 hexes: the
+    whole steady stage both ways, and one operator product (sum-factorized element pass against the
+    FP64 SpMV of the assembled K)."""
+    import torch
+    out = {"workload": f"{S}^3 Q2 hexes, k = 1, f = 10, T = 0 / 1 on x = 0 / 1, steady, CG + Jacobi FP64 to 1e-8"}
+    sol = {}
+    for key, op in (("csr", rsd.OP_CSR), ("fem", rsd.OP_FEM)):
+        h, sol[key], rep, ms = fem_steady(rsd, ctx, stream, S, op)
+        out[key] = {"ms": ms, "iterations": rep["iterations"], "converged": bool(rep["converged"]),
+                    "true_residual_rel": rep["trueResidualRel"]}
+    out["n_free"], out["nnz"], out["elements"] = h.n, h.nnz, S ** 3
+    out["speedup_fem_vs_csr"] = out["csr"]["ms"] / out["fem"]["ms"]
+    out["fem_vs_csr_max_rel_diff"] = float(np.max(np.abs(sol["fem"] - sol["csr"])) / np.max(np.abs(sol["csr"])))
+    # one product each way, 20 back to back per event pair, median of 5
+    v = ctx.to_device(np.random.default_rng(1).standard_normal(h.n))
+    y = ctx.array(h.n)
+    h.assemble_matrix(1.0, 0.0)
+
+    def per_product(fn):
+        ts = []
+        for i in range(6):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(20):
+                fn()
+            e1.record(stream)
+            e1.synchronize()
+            if i:
+                ts.append(e0.elapsed_time(e1) * 1e3 / 20)
+        return float(np.median(ts))
+    spmv_us = per_product(lambda: h.K.spmv(v, y))
+    fem_us = per_product(lambda: h.assemble_vector(4, y, coef=0.0, operand=v))
+    import ctypes
+    rate = ctypes.c_double()
+    rsd.check(rsd.lib().rsd_measure_fp64_rate(ctx.h, ctypes.byref(rate)))
+    fp64_rate = rate.value   # TFLOP/s, measured on this GPU
+    E = S ** 3
+    # bytes: per element the 27 free rows (4 B) and the geometry record (64 B), the operand read and
+    # the result written once; flops: 210 multiply-adds per lane of the kernel, 9 lanes per element
+    fem_bytes = E * (27 * 4 + 64) + 16 * h.n
+    fem_flops = E * 9 * 210 * 2
+    t_hbm = fem_bytes / (measured_peak_hbm()[0] * 1e3)
+    t_fp64 = fem_flops / (fp64_rate * 1e6) if fp64_rate else None
+    bound = max(t_hbm, t_fp64 or 0.0)
+    out["product_us"] = {"csr_spmv_fp64": spmv_us, "fem_sum_factorized": fem_us, "speedup": spmv_us / fem_us}
+    out["product_roofline"] = {"kernel": "k_apply_hex27_lines", "bytes": fem_bytes, "flops": fem_flops,
+                               "hbm_us": t_hbm, "fp64_us": t_fp64, "bound": "fp64" if (t_fp64 or 0) > t_hbm else "hbm",
+                               "roofline_us": bound, "achieved_us": fem_us, "frac": bound / fem_us,
+                               "fp64_tflops": fp64_rate, "hbm_peak_gbs": measured_peak_hbm()[0],
+                               "csr_bytes": h.nnz * 12 + 4 * (h.n + 1) + 16 * h.n,
+                               "note": "shared-memory line exchanges bound the kernel (ncu: L1/shared pipe ~90% busy)"}
+    return out
+
+
+def fem_cpu_baseline(rsd, ctx, stream, m):
+    """The reference's steady stage with operator type fem (FEMOperator + cg::Solver + Jacobi, 1 core)
+    on an m^3 Q2 sample, beside this library's matrix-free stage on the same sample."""
+    import oracle
+    if not oracle.reference_available():
+        return None
+    r = oracle.Reference(3, 2, 3, [m] * 3, [0, 0, 0], [1, 1, 1], [0, 1], bc_kind=0, bc_val={0: 0.0, 1: 1.0},
+                         src_kind=0, src_c=10.0)
+    r.set_operator("fem")
+    t0 = time.perf_counter()
+    _, rep = r.steady(0, 1, 1e-8, 100000)
+    cpu_ms = 1e3 * (time.perf_counter() - t0)
+    _, _, drep, dev_ms = fem_steady(rsd, ctx, stream, m, rsd.OP_FEM)
+    return {"value": cpu_ms, "unit": "ms", "cores": 1, "kind": "reference", "cg_iterations": rep["iterations"],
+            "device_same_sample_ms": dev_ms, "device_iterations": drep["iterations"],
+            "sample": f"the whole steady stage with the matrix-free operator on {m}^3 Q2 hexes ({r.n} rows) through "
+                      f"the reference templates (oracle/_ref), 1 core; the device time is this library's on the same mesh"}
+
+
 def fourier_theta(xyz, ien, npe, seed, modes=16, amp=0.5):
     """theta_e = sum_m amp sin(2 pi k_m . c_e + phi_m) at element centroids c_e; stream mt19937_64(seed),
     per mode the three integers k_m ~ U{1..4} and then phi_m ~ U[0, 2 pi)."""
@@ -621,6 +720,7 @@ def main():
     ap.add_argument("--batch", type=int, default=256, help="problems in the batched workload (0: skip it)")
     ap.add_argument("--newton", type=int, default=48, help="Q2 mesh size of the Newton workload (0: skip it)")
     ap.add_argument("--adjoint", type=int, default=96, help="mesh size of the adjoint workload (0: skip it)")
+    ap.add_argument("--fem", type=int, default=48, help="Q2 mesh size of the matrix-free operator workload (0: skip it)")
     ap.add_argument("--fd-directions", type=int, default=20)
     ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
                     help="run one solver path only (no e2e, no CPU leg): for profiler captures")
@@ -756,6 +856,15 @@ def main():
         except Exception as e:  # noqa: BLE001
             adjoint["cpu_baseline"] = {"value": None, "sample": f"failed: {e}"}
 
+    fem_op = None
+    if args.fem > 0:
+        fem_op = run_fem_operator(rsd, ctx, stream, args.fem)
+        if rank == 0 and world == 1 and not args.no_cpu:
+            try:
+                fem_op["cpu_baseline"] = fem_cpu_baseline(rsd, ctx, stream, 16)
+            except Exception as e:  # noqa: BLE001
+                fem_op["cpu_baseline"] = {"value": None, "sample": f"failed: {e}"}
+
     # the configured run once: 50 steps from T0 with each solver, final states compared
     full_run = {}
     finals = {}
@@ -883,6 +992,7 @@ def main():
         "full_run_50_steps": full_run,
         "batch": batch,
         "newton": newton,
+        "fem_operator": fem_op,
         "adjoint": adjoint,
         "cpu_baseline": cpu,
         "e2e": {"value": ms_e2e, "unit": "ms", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
