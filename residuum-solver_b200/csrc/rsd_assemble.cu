@@ -920,8 +920,10 @@ __global__ void __launch_bounds__(256) k_apply_hex27_lines(const AsmParams prm, 
 	if (prm.skip && *(volatile const int32_t*)prm.skip) return;   // uniform over the launch
 	__shared__ double sbuf[WPB * WARPBUF];
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	const bool act = lane < EPW * 9;   // lanes 27-31 compute along but write nothing
-	const int slot = act ? lane / 9 : 0, l = lane % 9, p = l % 3, r = l / 3;
+	// lanes 27-31 compute along but write nothing; they read the addresses of lanes 18-22 (the same
+	// half-warp: broadcasts, no extra bank wavefronts)
+	const bool act = lane < EPW * 9;
+	const int slot = act ? lane / 9 : 2, l = act ? lane % 9 : lane - 27, p = l % 3, r = l / 3;
 	double* buf = sbuf + warp * WARPBUF + slot * SLOT + (slot == 2 ? 11 : 0);
 	// buffer entry of array k (0..2) at point (x, y, z)
 	auto at = [&](int k, int x, int y, int z) -> double& { return buf[k * ARR + x + 4 * y + 11 * z]; };
