@@ -722,8 +722,9 @@ def main():
     ap.add_argument("--adjoint", type=int, default=96, help="mesh size of the adjoint workload (0: skip it)")
     ap.add_argument("--fem", type=int, default=48, help="Q2 mesh size of the matrix-free operator workload (0: skip it)")
     ap.add_argument("--fd-directions", type=int, default=20)
-    ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
-                    help="run one solver path only (no e2e, no CPU leg): for profiler captures")
+    ap.add_argument("--only", choices=["mixed", "fp64", "fem-product"], default=None,
+                    help="run one solver path only (no e2e, no CPU leg), or 4 matrix-free products on the "
+                         "--fem Q2 mesh: for profiler captures")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -748,6 +749,24 @@ def main():
     bm = import_module("residuum_solver_b200.blockmesh")
     ctx = rsd.Context(local)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=local)
+
+    if args.only == "fem-product":
+        # the matrix-free workload's problem and 4 operator products on a seeded operand
+        F = args.fem
+        xq, iq, rq = bm.block_mesh(3, [F] * 3, [0, 0, 0], [1, 1, 1], 2)
+        hq = rsd.Heat(ctx, rsd.Mesh(ctx, 3, 2, xq, iq, rq), 3, src_expr="10", dirichlet={0: "0", 1: "1"})
+        v = ctx.to_device(np.random.default_rng(1).standard_normal(hq.n))
+        y = ctx.array(hq.n)
+        for _ in range(4):
+            hq.assemble_vector(4, y, coef=0.0, operand=v)
+        ctx.sync()
+        if rank == 0:
+            print(json.dumps({"only": args.only, "n_free": hq.n, "elements": F ** 3}))
+        del hq
+        ctx.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return
 
     S = args.size
     xyz, ien, rng = bm.block_mesh(3, [S, S, S], [0, 0, 0], [1, 1, 1], 1)
