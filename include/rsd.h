@@ -209,6 +209,13 @@ int rsd_assemble_vector(rsd_ctx* ctx, rsd_heat* h, int32_t which, double coef, c
  * read.  b, x device vectors of num_free entries; x holds the initial guess. */
 int rsd_heat_solve_fem(rsd_ctx* ctx, rsd_heat* h, double c_mass, const rsd_solver_cfg* cfg, const double* b, double* x,
                        rsd_report* report);
+/* A flux boundary condition given by one expression per spatial component, q(t, x, y, z), on a
+ * boundary tag (HeatProblem.tpp:98-105, FluxBoundaryForm); flux_expr NULL clears the tag's flux.
+ * The stages then add its integrals to the right-hand side as HeatProblem::applyNatural does. */
+int rsd_heat_set_flux(rsd_ctx* ctx, rsd_heat* h, int32_t tag, const char* const* flux_expr);
+/* BoundaryApplicator::applyNaturalBCs (fem/boundary/backend/cpu/BoundaryApplicator.tpp:66-140) at the
+ * problem's current time: F += sum over flux faces of the integral of (q . n) N_a, scattered Free */
+int rsd_apply_natural(rsd_ctx* ctx, rsd_heat* h, double* F);
 /* BoundaryApplicator::applyEssentialBCs (fem/boundary/backend/cpu/BoundaryApplicator.tpp:7-64) */
 int rsd_apply_dirichlet_lift(rsd_ctx* ctx, rsd_heat* h, double c_diff, double c_mass, double* F);
 /* Assembler::assembleDiagonal (Assembler.tpp:142-197) */

@@ -95,6 +95,8 @@ def oracle_lib():
         L.ro_expr_eval.argtypes = [C.c_char_p, _D, _D, _D, _D, _D, C.POINTER(_D)]
         L.ro_fem_solve.argtypes = [_P, _D, _I32, _P, _P, _D, _I64, C.POINTER(Report)]
         L.ro_set_operator.argtypes = [_P, _I32]
+        L.ro_set_flux.argtypes = [_P, _I32, C.POINTER(C.c_char_p)]
+        L.ro_natural.argtypes = [_P, _P]
         _olib = L
     return _olib
 
@@ -135,7 +137,7 @@ class Oracle:
     """The restatement for one mesh + model: dof map, pattern, element loops, solvers, stages."""
 
     def __init__(self, mesh, nq, k_const=1.0, k_expr=None, dk_expr=None, k_elem=None, rho=1.0, cp=1.0,
-                 src_expr=None, bc=None):
+                 src_expr=None, bc=None, flux=None):
         L = oracle_lib()
         self.mesh = mesh
         self._kelem = None if k_elem is None else _f64(k_elem)
@@ -155,6 +157,10 @@ class Oracle:
             raise ValueError(L.ro_last_error().decode())
         self.n = L.ro_num_free(self.h)
         self.nnz = L.ro_nnz(self.h)
+        for tag, exprs in (flux or {}).items():
+            arr = (C.c_char_p * len(exprs))(*[e.encode() for e in exprs])
+            if L.ro_set_flux(self.h, tag, arr):
+                raise ValueError(L.ro_last_error().decode())
 
     def __del__(self):
         try:
@@ -197,6 +203,12 @@ class Oracle:
     def lift(self, F, c_diff=1.0, c_mass=0.0):
         F = np.array(F, dtype=np.float64)
         oracle_lib().ro_lift(self.h, c_diff, c_mass, _ptr(F))
+        return F
+
+    def natural(self, F):
+        """F plus the flux boundary integrals (applyNaturalBCs) at the current time."""
+        F = np.array(F, dtype=np.float64)
+        oracle_lib().ro_natural(self.h, _ptr(F))
         return F
 
     def diagonal(self, c_diff=1.0, c_mass=0.0, U=None):

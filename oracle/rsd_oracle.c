@@ -222,6 +222,8 @@ struct ro_problem {
 	double time;
 	double* g;                 /* Dirichlet value per node at the current time (constrained nodes) */
 	int32_t opType;            /* LinearSolverConfig::OperatorType of the stages: 0 CSR, 1 FEM */
+	ro_prog fluxP[6][3];       /* flux boundary conditions: per tag, one expression per component */
+	int hasFlux[6];
 };
 
 int64_t ro_num_free(const ro_problem* p) { return p->n; }
@@ -644,6 +646,88 @@ void ro_diagonal(ro_problem* P, double cDiff, double cMass, const double* U, dou
 	}
 }
 
+/* HeatProblem's flux boundary condition, one expression per spatial component
+ * (application/heateq/problem/HeatProblem.tpp:98-105); NULL clears the tag */
+int ro_set_flux(ro_problem* P, int32_t tag, const char* const* exprs) {
+	if (tag < 0 || tag >= 2 * P->m->nsd) { snprintf(g_err, sizeof g_err, "boundary tag out of range"); return 1; }
+	if (!exprs) { P->hasFlux[tag] = 0; return 0; }
+	for (int d = 0; d < P->m->nsd; ++d) if (compile_expr(exprs[d], &P->fluxP[tag][d])) return 1;
+	P->hasFlux[tag] = 1;
+	return 0;
+}
+
+/* BoundaryApplicator<CPU>::applyNaturalBCs (fem/boundary/backend/cpu/BoundaryApplicator.tpp:66-140)
+ * with FluxBoundaryForm (equation/heateq/form/FluxBoundaryForm.hpp:22-34) and the boundary
+ * quadrature point of equation/heateq/evaluator/EvalQuadraturePointBoundary.hpp:74-103: for each
+ * element face whose tag carries a flux, the face point is mapped into the element
+ * (LagrangeQuad/Hex::mapFaceToElement), x and J from all element nodes, n = cof(J) nRef
+ * (JacobianTransform::computeBoundaryNormal, nRef = +-e_axis by getFaceTopology), and
+ * Fe[a] += (q_i N_a) n_i w over the face nodes (getFaceNodes), w the reference face weight; the
+ * face vector is scattered Free with +1. */
+void ro_natural(ro_problem* P, double* F) {
+	const ro_mesh* m = P->m;
+	const int S = m->nsd, p = m->order, q1 = p + 1, npe = m->npe, nf = m->nfaces;
+	int any = 0;
+	for (int t = 0; t < 6; ++t) any |= P->hasFlux[t];
+	if (!any) return;
+	int nb = 0;
+	for (int i = 1; i <= 5; ++i) if ((int)round(pow((double)P->nq, 1.0 / S)) == i) nb = i;
+	double gx[5], gw[5];
+	gauss1d(nb, gx, gw);
+	double coords[RO_MAXN * 3];
+	int64_t fn[RO_MAXN];
+	for (int64_t e = 0; e < m->nelem; ++e) {
+		const int64_t* nodes = m->ien + e * npe;
+		for (int f = 0; f < nf; ++f) {
+			const int32_t tag = m->rng[e * nf + f];
+			if (tag < 0 || tag >= 6 || !P->hasFlux[tag]) continue;
+			coords_of(P, nodes, coords);
+			const int npf = face_nodes(S, p, f, fn);
+			const int axis = f / 2;
+			const double side = (f & 1) ? 1.0 : -1.0;
+			double Fe[RO_MAXN];
+			memset(Fe, 0, sizeof Fe);
+			const int nqf = S == 3 ? nb * nb : nb;
+			for (int q = 0; q < nqf; ++q) {
+				const int qs = q % nb, qt = q / nb;
+				const double w = S == 3 ? gw[qs] * gw[qt] : gw[qs];
+				double xi[3] = {0, 0, 0};
+				xi[axis] = side;
+				int k = 0;
+				for (int d = 0; d < S; ++d) if (d != axis) xi[d] = (k++ == 0) ? gx[qs] : gx[qt];
+				double Nd[3][4], dNd[3][4];
+				for (int d = 0; d < S; ++d) lag1d(p, xi[d], Nd[d], dNd[d]);
+				double N[RO_MAXN], x[3] = {0, 0, 0}, J[9] = {0};
+				for (int a = 0; a < npe; ++a) {
+					const int ix = a % q1, iy = (a / q1) % q1, iz = S == 3 ? a / (q1 * q1) : 0;
+					double g[3];
+					N[a] = Nd[0][ix] * Nd[1][iy] * (S == 3 ? Nd[2][iz] : 1.0);
+					g[0] = dNd[0][ix] * Nd[1][iy] * (S == 3 ? Nd[2][iz] : 1.0);
+					g[1] = Nd[0][ix] * dNd[1][iy] * (S == 3 ? Nd[2][iz] : 1.0);
+					g[2] = S == 3 ? Nd[0][ix] * Nd[1][iy] * dNd[2][iz] : 0.0;
+					for (int i = 0; i < S; ++i) {
+						x[i] += N[a] * coords[a * S + i];
+						for (int al = 0; al < S; ++al) J[i * S + al] += g[al] * coords[a * S + i];
+					}
+				}
+				double cof[9], nrm[3];
+				if (S == 2) { cof[0] = J[3]; cof[1] = -J[2]; cof[2] = -J[1]; cof[3] = J[0]; }
+				else {
+					cof[0] = (J[4] * J[8] - J[5] * J[7]); cof[1] = -(J[3] * J[8] - J[5] * J[6]); cof[2] = (J[3] * J[7] - J[4] * J[6]);
+					cof[3] = -(J[1] * J[8] - J[2] * J[7]); cof[4] = (J[0] * J[8] - J[2] * J[6]); cof[5] = -(J[0] * J[7] - J[1] * J[6]);
+					cof[6] = (J[1] * J[5] - J[2] * J[4]); cof[7] = -(J[0] * J[5] - J[2] * J[3]); cof[8] = (J[0] * J[4] - J[1] * J[3]);
+				}
+				for (int i = 0; i < S; ++i) nrm[i] = cof[i * S + axis] * side;
+				double val[3];
+				for (int d = 0; d < S; ++d) val[d] = run_expr(&P->fluxP[tag][d], P->time, x[0], x[1], S == 3 ? x[2] : 0.0, 0.0);
+				for (int b = 0; b < npf; ++b)
+					for (int d = 0; d < S; ++d) Fe[b] += (val[d] * N[fn[b]]) * nrm[d] * w;
+			}
+			for (int b = 0; b < npf; ++b) { const int32_t r = P->t2a[nodes[fn[b]]]; if (r >= 0) F[r] += Fe[b]; }
+		}
+	}
+}
+
 /* adjoint: grad_e = lam_e^T Khat_e T_e with Khat_e the unit-conductivity element stiffness,
  * T_e gathered Full (Dirichlet values), lam_e gathered Free */
 void ro_adjoint_gradient(ro_problem* P, const double* T, const double* lam, double* grad) {
@@ -865,6 +949,7 @@ int ro_steady(ro_problem* P, int32_t solverType, int32_t precond, double tol, in
 	if (P->opType && solverType != 0) { free(val); free(F); snprintf(g_err, sizeof g_err, "matrix-free operator: CG only"); return 2; }
 	if (!P->opType) ro_assemble_matrix(P, 1.0, 0.0, 0.0, 0.0, U, NULL, val);
 	ro_assemble_vector(P, 0, 0.0, U, NULL, NULL, F);
+	ro_natural(P, F);
 	ro_lift(P, 1.0, 0.0, F);
 	int rc = P->opType ? ro_fem_solve(P, 0.0, precond, F, U, tol, maxit, rep)
 	                   : ro_csr_solve(solverType, precond, P->n, P->rowPtr, P->col, val, F, U, tol, maxit, krylov, rep);
@@ -898,6 +983,7 @@ int ro_backward_euler(ro_problem* P, double dt, int64_t nsteps, int32_t solverTy
 		ro_assemble_vector(P, 2, 0.0, Uprev, NULL, NULL, ms);
 		ro_set_time(P, t);
 		axpy(n, 1.0 / h, ms, F);
+		ro_natural(P, F);
 		ro_lift(P, 1.0, 1.0 / h, F);
 		ro_report rep;
 		const int src = P->opType ? ro_fem_solve(P, 1.0 / h, precond, F, U, tol, maxit, &rep)
@@ -927,6 +1013,7 @@ int ro_newton(ro_problem* P, double absTol, double relTol, int64_t maxit, int32_
 	memset(rep, 0, sizeof *rep);
 	for (int64_t it = 0; it < maxit; ++it) {
 		ro_assemble_vector(P, 0, 0.0, U, NULL, NULL, F);
+		ro_natural(P, F);
 		ro_assemble_vector(P, 1, 0.0, U, NULL, NULL, R);
 		for (int64_t i = 0; i < n; ++i) R[i] = -1.0 * R[i] + 1.0 * F[i];
 		const double res = sqrt(dot(n, R, R));

@@ -67,6 +67,8 @@ void ro_assemble_matrix(ro_problem* p, double cDiff, double cMass, double cTDiff
 void ro_assemble_vector(ro_problem* p, int32_t which, double coef, const double* U, const double* Udot,
                         const double* operand, double* out);
 void ro_lift(ro_problem* p, double cDiff, double cMass, double* F);
+int ro_set_flux(ro_problem* p, int32_t tag, const char* const* exprs);
+void ro_natural(ro_problem* p, double* F);
 void ro_diagonal(ro_problem* p, double cDiff, double cMass, const double* U, double* d);
 void ro_adjoint_gradient(ro_problem* p, const double* T, const double* lam, double* grad);
 

@@ -114,6 +114,8 @@ SIGNATURES = {
     "rsd_apply_dirichlet_lift": [_P, _P, _D, _D, _P],
     "rsd_assemble_diagonal": [_P, _P, _D, _D, _P, _P],
     "rsd_heat_solve_fem": [_P, _P, _D, C.POINTER(SolverConfig), _P, _P, C.POINTER(Report)],
+    "rsd_heat_set_flux": [_P, _P, _I32, C.POINTER(C.c_char_p)],
+    "rsd_apply_natural": [_P, _P, _P],
     "rsd_heat_steady": [_P, _P, C.POINTER(SolverConfig), _P, C.POINTER(Report)],
     "rsd_heat_be_step": [_P, _P, _D, C.POINTER(SolverConfig), _P, _P, C.POINTER(Report), C.POINTER(_D)],
     "rsd_heat_be_step_host": [_P, _P, _D, C.POINTER(SolverConfig), _P, C.POINTER(Report), C.POINTER(_D)],
@@ -382,7 +384,7 @@ class Heat:
     """rsd_heat: the heat problem (dof map, pattern, element loops, stages) on the device."""
 
     def __init__(self, ctx, mesh, nq, k_const=1.0, k_expr=None, dk_expr=None, k_elem=None, rho=1.0, cp=1.0,
-                 src_expr=None, dirichlet=None):
+                 src_expr=None, dirichlet=None, flux=None):
         self.ctx, self.mesh = ctx, mesh
         d = HeatDesc()
         d.nq, d.k_const, d.rho, d.cp = nq, k_const, rho, cp
@@ -401,6 +403,8 @@ class Heat:
         a = _P()
         check(lib().rsd_heat_matrix(self.h, C.byref(a)))
         self.K = CSR(ctx, a, owned=False)
+        for tag, exprs in (flux or {}).items():
+            self.set_flux(tag, exprs)
 
     def __del__(self):
         try:
@@ -435,6 +439,17 @@ class Heat:
 
     def diagonal(self, d, c_diff=1.0, c_mass=0.0, U=None):
         check(lib().rsd_assemble_diagonal(self.ctx.h, self.h, c_diff, c_mass, _ptr(U), _ptr(d)))
+
+    def set_flux(self, tag, exprs):
+        """Flux boundary condition on `tag`: one expression per spatial component (None clears it)."""
+        if exprs is None:
+            check(lib().rsd_heat_set_flux(self.ctx.h, self.h, tag, None))
+            return
+        arr = (C.c_char_p * len(exprs))(*[e.encode() for e in exprs])
+        check(lib().rsd_heat_set_flux(self.ctx.h, self.h, tag, arr))
+
+    def apply_natural(self, F):
+        check(lib().rsd_apply_natural(self.ctx.h, self.h, _ptr(F)))
 
     def solve_fem(self, b, x, c_mass=0.0, cfg=None, **kw):
         """(Diffusion + c_mass Mass) x = b without a matrix: the LinearSolverRunner the reference builds

@@ -1085,11 +1085,127 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_diag(const AsmParams prm) {
 	RSD_ELEMENT_LOOP_END
 }
 
+// 1D Gauss rule of the boundary quadrature (points and weights, up to 5 points)
+struct FaceRule {
+	double x[5], w[5];
+	int n;
+};
+
+__host__ __device__ static inline void lagrange1d(int p, double xi, double* N, double* dN);
+
+// BoundaryApplicator::applyNaturalBCs (fem/boundary/backend/cpu/BoundaryApplicator.tpp:66-140) with
+// FluxBoundaryForm (equation/heateq/form/FluxBoundaryForm.hpp:22-34): for every boundary face whose
+// tag carries a flux q(t, x), F_a += sum_q sum_i (q_i(t, x_q) N_a(q)) n_i(q) w_q over the face's nodes,
+// with the point mapped into the element (LagrangeQuad/Hex::mapFaceToElement), n = cof(J) nRef
+// (JacobianTransform::computeBoundaryNormal), w the reference face weight, scattered Free.  One
+// thread per face; faces holds (element, face, tag) triplets.
+template <int NSD, int P>
+__global__ void __launch_bounds__(128) k_natural(int64_t nfaces, const int32_t* __restrict__ faces,
+                                                 const double* __restrict__ xyz, const int32_t* __restrict__ ien,
+                                                 const int32_t* __restrict__ t2a, const DevExpr* __restrict__ flux,
+                                                 double time, FaceRule rule, double* __restrict__ F) {
+	constexpr int N1 = P + 1, NPE = (NSD == 3) ? N1 * N1 * N1 : N1 * N1, NFN = (NSD == 3) ? N1 * N1 : N1;
+	const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+	if (i >= nfaces) return;
+	const int64_t e = faces[3 * i];
+	const int f = faces[3 * i + 1], tag = faces[3 * i + 2];
+	const int axis = f / 2;                       // the reference axis normal to the face
+	const double side = (f & 1) ? 1.0 : -1.0;     // its reference coordinate on the face
+	const int32_t* en = ien + e * NPE;
+	double Fe[NFN];
+#pragma unroll
+	for (int a = 0; a < NFN; ++a) Fe[a] = 0.0;
+	const int nqf = (NSD == 3) ? rule.n * rule.n : rule.n;
+	for (int q = 0; q < nqf; ++q) {
+		const int qs = q % rule.n, qt = q / rule.n;
+		const double s = rule.x[qs], t = NSD == 3 ? rule.x[qt] : 0.0;
+		const double w = NSD == 3 ? rule.w[qs] * rule.w[qt] : rule.w[qs];
+		// element coordinates of the point: the face axis fixed, (s, t) on the others in order
+		double xi[3] = {0.0, 0.0, 0.0};
+		xi[axis] = side;
+		{
+			int k = 0;
+#pragma unroll
+			for (int d = 0; d < NSD; ++d)
+				if (d != axis) xi[d] = (k++ == 0) ? s : t;
+		}
+		double Nd[3][4], dNd[3][4];
+#pragma unroll
+		for (int d = 0; d < NSD; ++d) lagrange1d(P, xi[d], Nd[d], dNd[d]);
+		// x = sum N_a x_a, J[i][al] = sum dN_a/dxi_al x_a,i (JacobianTransform::mapToPhysical, computeJacobian)
+		double x[3] = {0.0, 0.0, 0.0}, J[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+		for (int a = 0; a < NPE; ++a) {
+			const int ix = a % N1, iy = (a / N1) % N1, iz = NSD == 3 ? a / (N1 * N1) : 0;
+			double Na = Nd[0][ix] * Nd[1][iy], g[3];
+			g[0] = dNd[0][ix] * Nd[1][iy];
+			g[1] = Nd[0][ix] * dNd[1][iy];
+			if (NSD == 3) { g[0] *= Nd[2][iz]; g[1] *= Nd[2][iz]; g[2] = Nd[0][ix] * Nd[1][iy] * dNd[2][iz]; Na *= Nd[2][iz]; }
+			const double* xa = xyz + (int64_t)en[a] * NSD;
+#pragma unroll
+			for (int d = 0; d < NSD; ++d) {
+				const double c = xa[d];
+				x[d] += Na * c;
+#pragma unroll
+				for (int al = 0; al < NSD; ++al) J[d * NSD + al] += g[al] * c;
+			}
+		}
+		// n = cof(J) nRef with nRef = side e_axis (JacobianTransform::computeMatrixCofactor)
+		double n[3];
+		if constexpr (NSD == 2) {
+			const double cof[4] = {J[3], -J[2], -J[1], J[0]};
+#pragma unroll
+			for (int d = 0; d < 2; ++d) n[d] = cof[d * 2 + axis] * side;
+		} else {
+			const double cof[9] = {J[4] * J[8] - J[5] * J[7], -(J[3] * J[8] - J[5] * J[6]), J[3] * J[7] - J[4] * J[6],
+			                       -(J[1] * J[8] - J[2] * J[7]), J[0] * J[8] - J[2] * J[6], -(J[0] * J[7] - J[1] * J[6]),
+			                       J[1] * J[5] - J[2] * J[4], -(J[0] * J[5] - J[2] * J[3]), J[0] * J[4] - J[1] * J[3]};
+#pragma unroll
+			for (int d = 0; d < 3; ++d) n[d] = cof[d * 3 + axis] * side;
+		}
+		double val[3];
+#pragma unroll
+		for (int d = 0; d < NSD; ++d)
+			val[d] = eval_expr(flux[tag * 3 + d], time, x[0], x[1], NSD == 3 ? x[2] : 0.0, 0.0);
+		// the face's nodes: the face axis at its end, the other axes in order
+#pragma unroll
+		for (int b = 0; b < NFN; ++b) {
+			const int u = b % N1, v = b / N1;
+			int id[3];
+			id[axis] = (f & 1) ? P : 0;
+			{
+				int k = 0;
+#pragma unroll
+				for (int d = 0; d < NSD; ++d)
+					if (d != axis) id[d] = (k++ == 0) ? u : v;
+			}
+			double Nb = Nd[0][id[0]] * Nd[1][id[1]];
+			if (NSD == 3) Nb *= Nd[2][id[2]];
+#pragma unroll
+			for (int d = 0; d < NSD; ++d) Fe[b] += (val[d] * Nb) * n[d] * w;
+		}
+	}
+#pragma unroll
+	for (int b = 0; b < NFN; ++b) {
+		const int u = b % N1, v = b / N1;
+		int id[3] = {0, 0, 0};
+		id[axis] = (f & 1) ? P : 0;
+		{
+			int k = 0;
+#pragma unroll
+			for (int d = 0; d < NSD; ++d)
+				if (d != axis) id[d] = (k++ == 0) ? u : v;
+		}
+		const int a = id[0] + N1 * id[1] + (NSD == 3 ? N1 * N1 * id[2] : 0);
+		const int32_t row = t2a[en[a]];
+		if (row >= 0) atomicAdd(F + row, Fe[b]);
+	}
+}
+
 // ---------------------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------------------
 // Lagrange1D::eval / evalFirstDerivative (fem/basis/Lagrange1D.tpp:4-51)
-static void lagrange1d(int p, double xi, double* N, double* dN) {
+__host__ __device__ static inline void lagrange1d(int p, double xi, double* N, double* dN) {
 	if (p == 1) { N[0] = 0.5 * (1.0 - xi); N[1] = 0.5 * (1.0 + xi); dN[0] = -0.5; dN[1] = 0.5; }
 	else if (p == 2) {
 		N[0] = 0.5 * xi * (xi - 1.0); N[1] = (1.0 - xi) * (1.0 + xi); N[2] = 0.5 * xi * (xi + 1.0);
@@ -1611,6 +1727,63 @@ int assemble_lift(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, double*
 	const int rc = launch_k_asm_vector(ctx, h, p);
 	prof_end(ctx, pr);
 	return rc;
+}
+
+// HeatProblem's flux boundary condition with an expression per spatial component
+// (application/heateq/problem/HeatProblem.tpp:98-105): registers or clears tag's flux and rebuilds
+// the list of boundary faces that carry one
+int set_flux(rsd_ctx* ctx, rsd_heat* h, int tag, const char* const* exprs) {
+	const rsd_mesh* m = h->m;
+	if (tag < 0 || tag >= 2 * m->nsd) return set_error(RSD_EINVAL, "boundary tag out of range");
+	if (exprs) {
+		DevExpr c[3];
+		for (int d = 0; d < m->nsd; ++d) {
+			if (!exprs[d]) return set_error(RSD_EINVAL, "a flux needs one expression per spatial component");
+			RSD_CHECK(compile_expr(exprs[d], &c[d]));
+		}
+		for (int d = 0; d < 3; ++d) h->fluxExpr[tag * 3 + d] = d < m->nsd ? c[d] : DevExpr{};
+		h->hasFlux[tag] = true;
+	} else {
+		h->hasFlux[tag] = false;
+	}
+	std::vector<int32_t> fl;
+	for (int64_t e = 0; e < m->nelem; ++e)
+		for (int f = 0; f < m->nfaces; ++f) {
+			const int32_t t = m->h_rng[e * m->nfaces + f];
+			if (t >= 0 && t < 6 && h->hasFlux[t]) { fl.push_back((int32_t)e); fl.push_back(f); fl.push_back(t); }
+		}
+	cudaFree(h->nFaces);
+	h->nFaces = nullptr;
+	h->nnFaces = (int64_t)fl.size() / 3;
+	if (!h->dFlux) RSD_CUDA(cudaMalloc(&h->dFlux, sizeof(DevExpr) * 18));
+	RSD_CUDA(cudaMemcpyAsync(h->dFlux, h->fluxExpr, sizeof(DevExpr) * 18, cudaMemcpyHostToDevice, ctx->stream));
+	if (h->nnFaces) {
+		RSD_CUDA(cudaMalloc(&h->nFaces, sizeof(int32_t) * fl.size()));
+		RSD_CUDA(cudaMemcpyAsync(h->nFaces, fl.data(), sizeof(int32_t) * fl.size(), cudaMemcpyHostToDevice, ctx->stream));
+	}
+	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+	return RSD_OK;
+}
+
+// HeatProblem::applyNatural (HeatProblem.tpp:234-238) at the problem's current time: F += the flux
+// integrals of every registered flux boundary
+int apply_natural(rsd_ctx* ctx, rsd_heat* h, double* F) {
+	if (h->nnFaces == 0) return RSD_OK;
+	FaceRule r{};
+	r.n = h->nq1;
+	gauss_legendre(r.n, r.x, r.w);
+	const int nsd = h->m->nsd, ord = h->m->order;
+	const int blocks = (int)((h->nnFaces + 127) / 128);
+#define RSD_NAT(D, Q) k_natural<D, Q><<<blocks, 128, 0, ctx->stream>>>(h->nnFaces, h->nFaces, h->m->xyz, h->m->ien, h->t2a, h->dFlux, h->time, r, F)
+	if (nsd == 2 && ord == 1) RSD_NAT(2, 1);
+	else if (nsd == 2 && ord == 2) RSD_NAT(2, 2);
+	else if (nsd == 2 && ord == 3) RSD_NAT(2, 3);
+	else if (nsd == 3 && ord == 1) RSD_NAT(3, 1);
+	else if (nsd == 3 && ord == 2) RSD_NAT(3, 2);
+	else return set_error(RSD_EINVAL, "unsupported element");
+#undef RSD_NAT
+	RSD_CUDA(cudaGetLastError());
+	return RSD_OK;
 }
 
 int assemble_diagonal(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, const double* U, double* d) {

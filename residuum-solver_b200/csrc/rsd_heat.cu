@@ -74,7 +74,7 @@ __global__ void k_diff_norm(int64_t n, const double* __restrict__ F, const doubl
 
 static void free_heat(rsd_heat* h) {
 	cudaFree(h->t2a); cudaFree(h->g); cudaFree(h->kElem); cudaFree(h->tables); cudaFree(h->bElems); cudaFree(h->gPrev);
-	cudaFree(h->ranks); cudaFree(h->affine); cudaFree(h->geo); cudaFree(h->ktab); cudaFree(h->adjPtr); cudaFree(h->adj); cudaFree(h->erow);
+	cudaFree(h->ranks); cudaFree(h->affine); cudaFree(h->geo); cudaFree(h->ktab); cudaFree(h->adjPtr); cudaFree(h->adj); cudaFree(h->erow); cudaFree(h->dFlux); cudaFree(h->nFaces);
 	cudaFree(h->hostU); cudaFree(h->hostUprev);
 	cudaFree(h->F); cudaFree(h->R); cudaFree(h->Udot); cudaFree(h->ms); cudaFree(h->dU);
 	if (h->K) rsd_csr_destroy(h->K);
@@ -201,6 +201,18 @@ int rsd_assemble_vector(rsd_ctx* ctx, rsd_heat* h, int32_t which, double coef, c
 	return RSD_OK;
 }
 
+int rsd_heat_set_flux(rsd_ctx* ctx, rsd_heat* h, int32_t tag, const char* const* flux_expr) {
+	if (!ctx || !h) return set_error(RSD_EINVAL, "null argument");
+	return set_flux(ctx, h, tag, flux_expr);
+}
+
+int rsd_apply_natural(rsd_ctx* ctx, rsd_heat* h, double* F) {
+	if (!ctx || !h || (h->n && !F)) return set_error(RSD_EINVAL, "null argument");
+	RSD_CHECK(apply_natural(ctx, h, F));
+	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+	return RSD_OK;
+}
+
 int rsd_heat_solve_fem(rsd_ctx* ctx, rsd_heat* h, double c_mass, const rsd_solver_cfg* cfg, const double* b, double* x,
                        rsd_report* rep) {
 	if (!ctx || !h || !cfg) return set_error(RSD_EINVAL, "null argument");
@@ -227,6 +239,7 @@ int rsd_heat_steady(rsd_ctx* ctx, rsd_heat* h, const rsd_solver_cfg* cfg, double
 	const bool fem = cfg->operator_type == RSD_OP_FEM;   // isSparse() false: no K (SteadyStage.hpp:62-64)
 	if (!fem) RSD_CHECK(assemble_matrix(ctx, h, 1.0, 0.0, 0.0, 0.0, U, nullptr, h->K));
 	RSD_CHECK(assemble_vector(ctx, h, 0, 0.0, U, nullptr, nullptr, h->F, 1.0, false));
+	RSD_CHECK(apply_natural(ctx, h, h->F));                                                  // applyNatural
 	RSD_CHECK(assemble_lift(ctx, h, 1.0, 0.0, h->F));
 	return fem ? solve_fem(ctx, h, 0.0, cfg, h->F, U, rep) : solve(ctx, h->K, cfg, h->F, U, rep);
 }
@@ -273,6 +286,7 @@ static int be_step(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver_cfg* c
 	k_be_rate<<<gv, 256, 0, ctx->stream>>>(n, inv, U, Uprev, h->Udot);
 	if (!early && !fem) RSD_CHECK(assemble_matrix(ctx, h, 1.0, inv, 0.0, 0.0, U, h->Udot, h->K));    // K + M/dt
 	RSD_CHECK(assemble_vector(ctx, h, 7, inv, Uprev, nullptr, nullptr, h->F, 1.0, false));  // load + (1/dt) M Uprev
+	RSD_CHECK(apply_natural(ctx, h, h->F));                                                  // applyNatural
 	RSD_CHECK(assemble_lift(ctx, h, 1.0, inv, h->F));                                      // F -= (K + M/dt) G
 	if (fem) RSD_CHECK(solve_fem(ctx, h, inv, cfg, h->F, U, rep));
 	else RSD_CHECK(solve(ctx, h->K, cfg, h->F, U, rep));
@@ -339,6 +353,7 @@ int rsd_heat_newton(rsd_ctx* ctx, rsd_heat* h, double abs_tol, double rel_tol, i
 	for (int64_t it = 0; it < max_iters; ++it) {
 		// assembleLoad and assembleResidual (K(T) T, Full gather) in one element pass: R = F - K(T) T
 		RSD_CHECK(assemble_vector(ctx, h, 9, 0.0, U, nullptr, nullptr, h->R, 1.0, false));
+		RSD_CHECK(apply_natural(ctx, h, h->R));   // F includes the natural boundary terms
 		double rr = 0.0;
 		RSD_CHECK(dot_device(ctx, n, h->R, h->R, &rr));
 		const double res = std::sqrt(rr);
@@ -381,6 +396,7 @@ int rsd_heat_forward(rsd_ctx* ctx, rsd_heat* h, const double* theta, const rsd_s
 	RSD_CHECK(adjoint_check(ctx, h, theta, cfg));
 	RSD_CHECK(assemble_matrix(ctx, h, 1.0, 0.0, 0.0, 0.0, T, nullptr, h->K));
 	RSD_CHECK(assemble_vector(ctx, h, 0, 0.0, T, nullptr, nullptr, h->F, 1.0, false));
+	RSD_CHECK(apply_natural(ctx, h, h->F));
 	RSD_CHECK(assemble_lift(ctx, h, 1.0, 0.0, h->F));
 	RSD_CHECK(solve(ctx, h->K, cfg, h->F, T, rep));
 	RSD_CUDA(cudaStreamSynchronize(ctx->stream));

@@ -211,6 +211,11 @@ struct rsd_heat {
 	int32_t* adjPtr = nullptr;      // device, n + 1
 	int32_t* adj = nullptr;         // device, e * npe + a
 	int32_t* erow = nullptr;        // device, [e][a]: t2a[ien[e][a]] (sum-factorized operator products), or null
+	rsd::DevExpr fluxExpr[18];      // flux boundary conditions: [tag][component]
+	bool hasFlux[6] = {false, false, false, false, false, false};
+	rsd::DevExpr* dFlux = nullptr;  // device copy of fluxExpr
+	int32_t* nFaces = nullptr;      // device: (element, face, tag) of the faces whose tag carries a flux
+	int64_t nnFaces = 0;
 	bool adjTried = false;
 	int32_t maxSlice = 0;           // longest SELL-32 slice of K, in entries per row
 	// stage scratch
@@ -231,6 +236,8 @@ int assemble_diagonal(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, con
 int assemble_lift(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, double* F);
 int apply_operator(rsd_ctx* ctx, rsd_heat* h, double coef, const double* U, const double* V, double* out,
                    const int32_t* skip);
+int set_flux(rsd_ctx* ctx, rsd_heat* h, int tag, const char* const* exprs);
+int apply_natural(rsd_ctx* ctx, rsd_heat* h, double* F);
 int solve_fem(rsd_ctx* ctx, rsd_heat* h, double coef, const rsd_solver_cfg* cfg, const double* b, double* x,
               rsd_report* rep);
 int build_tables(rsd_ctx* ctx, rsd_heat* h);

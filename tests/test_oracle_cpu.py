@@ -239,6 +239,33 @@ def test_matrix_free_fixtures_reproduce_from_reference():
     assert rc == 0 and (U == g["U"]).all() and (res == g["residual"]).all()
 
 
+def test_natural_bcs_known_answers():
+    # tests/integration/fem/heateq/cpu/HeatEquationMinimal2D.cpp:96-112, 355-392: flux h = (0, x) on
+    # BOTTOM adds -1, -2, -3 to the three free bottom nodes, then the lift
+    m = oracle.BlockMesh(2, [4, 4], [0, 0], [4, 4], 1)
+    o = oracle.Oracle(m, 2, src_expr="x*y", bc={0: "x", 1: "x", 3: "x"}, flux={2: ("0", "x")})
+    F = o.lift(o.natural(o.assemble_vector(0)), 1.0, 0.0)
+    expect = [1 / 6 - 1, 1 / 3 - 2, 1 / 2 - 3 + 2, 1, 2, 3 + 4, 2, 4, 6 + 4, 3 + 1, 6 + 2, 9 + 17 / 3]
+    assert np.max(np.abs(F - expect)) <= TOL
+    # HeatEquationMinimal3D.cpp:288-337: flux (0, 0, x) on BOTTOM/TOP adds -i / +i on the k = 0 / 4 layers
+    m = oracle.BlockMesh(3, [4, 4, 4], [0, 0, 0], [4, 4, 4], 1)
+    o = oracle.Oracle(m, 2, src_expr="x*y*z", bc={t: "x" for t in range(4)}, flux={4: ("0", "0", "x"), 5: ("0", "0", "x")})
+    t2a, _, _ = o.dofmap()
+    F0 = o.assemble_vector(0)
+    F1 = o.natural(F0)
+    Sz = [1 / 6, 1, 2, 3, 11 / 6]
+    for i in range(1, 4):
+        for j in range(1, 4):
+            for k in range(5):
+                a = t2a[i + 5 * j + 25 * k]
+                e = i * j * Sz[k] + (-i if k == 0 else i if k == 4 else 0)
+                assert abs(F1[a] - e) <= TOL
+    F2 = o.lift(F1, 1.0, 0.0)
+    node = lambda i, j, k: t2a[i + 5 * j + 25 * k]
+    for (i, j, k), e in (((1, 1, 0), -1 / 3), ((1, 1, 1), 2.0), ((1, 1, 4), 10 / 3), ((2, 2, 2), 8.0), ((3, 1, 1), 26 / 3)):
+        assert abs(F2[node(i, j, k)] - e) <= TOL
+
+
 def test_blockmesh_generator_matches_restatement():
     rsd = load_package()
     from importlib import import_module
