@@ -17,16 +17,42 @@ static bool uses_time(const DevExpr& e) {
 
 // Dirichlet value per constrained node at time t: the constraint tag's expression at the node's
 // coordinates, as gatherElementVector evaluates it (fem/assembly/backend/cpu/ElementMap.tpp:55-65)
-static int bc_values_to(rsd_ctx* ctx, const rsd_heat* h, double t, double* dst) {
-	const rsd_mesh* m = h->m;
-	std::vector<double> g(m->nnodes, 0.0);
-	for (int64_t i = 0; i < m->nnodes; ++i) {
-		if (h->h_t2a[i] >= 0) continue;
-		const double* x = &m->h_xyz[i * m->nsd];
-		g[i] = eval_expr_host(h->bcExpr[h->h_ctag[i]], t, x[0], x[1], m->nsd == 3 ? x[2] : 0.0, 0.0);
+// g[node] = the Dirichlet expression of the node's constraint tag at (t, x) for every constrained node
+__global__ void k_bc_values(int64_t nc, const int32_t* __restrict__ nodes, const int32_t* __restrict__ tags,
+                            const double* __restrict__ xyz, int nsd, const DevExpr* __restrict__ bc, double t,
+                            double* __restrict__ g) {
+	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nc; i += (int64_t)gridDim.x * blockDim.x) {
+		const int32_t v = nodes[i];
+		const double* x = xyz + (int64_t)v * nsd;
+		g[v] = eval_expr(bc[tags[i]], t, x[0], x[1], nsd == 3 ? x[2] : 0.0, 0.0);
 	}
-	RSD_CUDA(cudaMemcpyAsync(dst, g.data(), sizeof(double) * m->nnodes, cudaMemcpyHostToDevice, ctx->stream));
-	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+// gatherElementVector's Dirichlet values (fem/assembly/backend/cpu/ElementMap.tpp:55-65) for every
+// constrained node at time t, evaluated on the device into dst (free nodes keep zero); the constrained
+// node list and the compiled expressions go to the device on the first call
+static int bc_values_to(rsd_ctx* ctx, rsd_heat* h, double t, double* dst) {
+	const rsd_mesh* m = h->m;
+	if (!h->dBc) {
+		std::vector<int32_t> cn, ct;
+		for (int64_t i = 0; i < m->nnodes; ++i)
+			if (h->h_t2a[i] < 0) { cn.push_back((int32_t)i); ct.push_back(h->h_ctag[i]); }
+		h->ncNodes = (int64_t)cn.size();
+		RSD_CUDA(cudaMalloc(&h->dBc, sizeof(DevExpr) * 6));
+		RSD_CUDA(cudaMalloc(&h->cNodes, sizeof(int32_t) * 2 * std::max<int64_t>(h->ncNodes, 1)));
+		RSD_CUDA(cudaMemcpyAsync(h->dBc, h->bcExpr, sizeof(DevExpr) * 6, cudaMemcpyHostToDevice, ctx->stream));
+		if (h->ncNodes) {
+			RSD_CUDA(cudaMemcpyAsync(h->cNodes, cn.data(), sizeof(int32_t) * cn.size(), cudaMemcpyHostToDevice, ctx->stream));
+			RSD_CUDA(cudaMemcpyAsync(h->cNodes + h->ncNodes, ct.data(), sizeof(int32_t) * ct.size(), cudaMemcpyHostToDevice, ctx->stream));
+		}
+		RSD_CUDA(cudaStreamSynchronize(ctx->stream));   // the host lists go out of scope
+	}
+	if (dst != h->g && dst != h->gPrev) return set_error(RSD_EINVAL, "Dirichlet values go to g or gPrev");
+	if (h->ncNodes) {
+		k_bc_values<<<vec_grid(ctx, h->ncNodes), 256, 0, ctx->stream>>>(h->ncNodes, h->cNodes, h->cNodes + h->ncNodes,
+		                                                                m->xyz, m->nsd, h->dBc, t, dst);
+		RSD_CUDA(cudaGetLastError());
+	}
 	return RSD_OK;
 }
 
@@ -74,7 +100,7 @@ __global__ void k_diff_norm(int64_t n, const double* __restrict__ F, const doubl
 
 static void free_heat(rsd_heat* h) {
 	cudaFree(h->t2a); cudaFree(h->g); cudaFree(h->kElem); cudaFree(h->tables); cudaFree(h->bElems); cudaFree(h->gPrev);
-	cudaFree(h->ranks); cudaFree(h->affine); cudaFree(h->geo); cudaFree(h->ktab); cudaFree(h->adjPtr); cudaFree(h->adj); cudaFree(h->erow); cudaFree(h->dFlux); cudaFree(h->nFaces);
+	cudaFree(h->ranks); cudaFree(h->affine); cudaFree(h->geo); cudaFree(h->ktab); cudaFree(h->adjPtr); cudaFree(h->adj); cudaFree(h->erow); cudaFree(h->dFlux); cudaFree(h->nFaces); cudaFree(h->dBc); cudaFree(h->cNodes);
 	cudaFree(h->hostU); cudaFree(h->hostUprev);
 	cudaFree(h->F); cudaFree(h->R); cudaFree(h->Udot); cudaFree(h->ms); cudaFree(h->dU);
 	if (h->K) rsd_csr_destroy(h->K);
@@ -136,6 +162,9 @@ int rsd_heat_create(rsd_ctx* ctx, const rsd_mesh* m, const rsd_heat_desc* d, rsd
 			return cuda_error(e, "boundary element list");
 		}
 		if ((e = cudaMalloc(&h->gPrev, sizeof(double) * nn)) != cudaSuccess) { free_heat(h); return cuda_error(e, "allocation"); }
+		// Dirichlet values are written for the constrained nodes only: the free nodes' entries stay zero
+		if ((e = cudaMemsetAsync(h->g, 0, sizeof(double) * nn, ctx->stream)) != cudaSuccess ||
+		    (e = cudaMemsetAsync(h->gPrev, 0, sizeof(double) * nn, ctx->stream)) != cudaSuccess) { free_heat(h); return cuda_error(e, "allocation"); }
 	}
 	if ((rc = build_tables(ctx, h)) || (rc = upload_bc_values(ctx, h)) || (rc = build_pattern(ctx, h, &h->K))) { free_heat(h); return rc; }
 	*out = h;

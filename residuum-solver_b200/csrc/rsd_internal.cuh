@@ -216,6 +216,9 @@ struct rsd_heat {
 	rsd::DevExpr* dFlux = nullptr;  // device copy of fluxExpr
 	int32_t* nFaces = nullptr;      // device: (element, face, tag) of the faces whose tag carries a flux
 	int64_t nnFaces = 0;
+	rsd::DevExpr* dBc = nullptr;    // device copy of bcExpr
+	int32_t* cNodes = nullptr;      // device: the constrained nodes, then their constraint tags
+	int64_t ncNodes = 0;
 	bool adjTried = false;
 	int32_t maxSlice = 0;           // longest SELL-32 slice of K, in entries per row
 	// stage scratch

@@ -530,3 +530,18 @@ def test_size_independent_properties_at_scale(rsd, ctx):
     assert np.abs(k1.download()[interior]).max() < 1e-12
     # symmetry via x.Ay == y.Ax
     assert abs(x @ ay.download() - y @ ax.download()) < 1e-10 * abs(x @ ax.download())
+
+
+def test_time_dependent_dirichlet_values(rsd, ctx):
+    # Dirichlet expressions of t and x evaluated on the device at each step's time (and at t - dt for
+    # the mass right-hand side) against the restatement's host evaluation
+    bc = {0: "sin(3*t + x) + y", 1: "t*y", 3: "0.25"}
+    m = oracle.BlockMesh(2, [9, 7], [0, 0], [1, 1], 2)
+    o = oracle.Oracle(m, 3, bc=bc, src_expr="1 + t")
+    h = rsd.Heat(ctx, rsd.Mesh(ctx, 2, 2, m.xyz, m.ien, m.rng), 3, src_expr="1 + t", dirichlet=bc)
+    U0 = np.sin(np.arange(o.n) * 0.11)
+    Uo, reso, _, _ = o.backward_euler(0.04, 5, U0, tol=1e-11)
+    U, Up = ctx.to_device(U0), ctx.to_device(U0)
+    res = [h.be_step(0.04, U, Up, type=rsd.CG, precond=rsd.JACOBI, tol=1e-11)["residualNorm"] for _ in range(5)]
+    assert relerr(U.download(), Uo) <= REL
+    assert relerr(res, reso) <= 1e-9
