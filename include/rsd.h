@@ -216,6 +216,13 @@ int rsd_heat_set_flux(rsd_ctx* ctx, rsd_heat* h, int32_t tag, const char* const*
 /* BoundaryApplicator::applyNaturalBCs (fem/boundary/backend/cpu/BoundaryApplicator.tpp:66-140) at the
  * problem's current time: F += sum over flux faces of the integral of (q . n) N_a, scattered Free */
 int rsd_apply_natural(rsd_ctx* ctx, rsd_heat* h, double* F);
+/* HeatProblem::computeNodalField (application/heateq/problem/HeatProblem.tpp:293-303) through
+ * QuantityEvaluator::evaluateNodalField with SimpleAverageRecovery (fem/quantity/backend/cpu/
+ * QuantityEvaluator.tpp:205-257): field RSD_FIELD_HEAT_FLUX (HeatFluxField, Q = -k grad T, nsd
+ * components per node) or RSD_FIELD_CONDUCTIVITY (ConductivityField, 1 per node) from the free-DOF
+ * temperature U (device); out: device, nnodes * components (node-major); scratch: device, nnodes. */
+enum { RSD_FIELD_HEAT_FLUX = 0, RSD_FIELD_CONDUCTIVITY = 1 };
+int rsd_heat_nodal_field(rsd_ctx* ctx, rsd_heat* h, int32_t field, const double* U, double* out, double* scratch);
 /* BoundaryApplicator::applyEssentialBCs (fem/boundary/backend/cpu/BoundaryApplicator.tpp:7-64) */
 int rsd_apply_dirichlet_lift(rsd_ctx* ctx, rsd_heat* h, double c_diff, double c_mass, double* F);
 /* Assembler::assembleDiagonal (Assembler.tpp:142-197) */

@@ -97,6 +97,7 @@ def oracle_lib():
         L.ro_set_operator.argtypes = [_P, _I32]
         L.ro_set_flux.argtypes = [_P, _I32, C.POINTER(C.c_char_p)]
         L.ro_natural.argtypes = [_P, _P]
+        L.ro_nodal_field.argtypes = [_P, _I32, _P, _P]
         _olib = L
     return _olib
 
@@ -204,6 +205,14 @@ class Oracle:
         F = np.array(F, dtype=np.float64)
         oracle_lib().ro_lift(self.h, c_diff, c_mass, _ptr(F))
         return F
+
+    def nodal_field(self, U, field="heat_flux"):
+        """Nodal recovery (SimpleAverageRecovery) of the heat flux (nnodes x nsd) or the conductivity."""
+        f = {"heat_flux": 0, "conductivity": 1}[field]
+        nc = self.mesh.nsd if f == 0 else 1
+        out = np.zeros(self.mesh.nnodes * nc)
+        oracle_lib().ro_nodal_field(self.h, f, _ptr(_f64(U)), _ptr(out))
+        return out.reshape(-1, nc) if nc > 1 else out
 
     def natural(self, F):
         """F plus the flux boundary integrals (applyNaturalBCs) at the current time."""
@@ -317,6 +326,7 @@ def ref_lib():
         L.ref_csr_solve.argtypes = [C.c_int, C.c_int, _I64, _P, _P, _P, _P, _P, _D, _I64, _I64, C.POINTER(Report)]
         L.ref_spmv.argtypes = [_I64, _P, _P, _P, _P, _P]
         L.ref_set_operator.argtypes = [_P, C.c_int]
+        L.ref_nodal_field.argtypes = [_P, C.c_int, _P, _P]
         _rlib = L
     return _rlib
 
@@ -350,6 +360,7 @@ class Reference:
         self.h = L.ref_create(C.byref(d))
         if not self.h:
             raise ValueError(L.ref_last_error().decode())
+        self.nsd = nsd
         self.nnodes = L.ref_num_nodes(self.h)
         self.nelem = L.ref_num_elems(self.h)
         self.n = L.ref_num_free(self.h)
@@ -399,6 +410,14 @@ class Reference:
         d = np.zeros(self.n)
         ref_lib().ref_diagonal(self.h, self.FORMSETS[formset], c, _ptr(_f64(U)), _ptr(d))
         return d
+
+    def nodal_field(self, U, field="heat_flux"):
+        """The reference's QuantityEvaluator::evaluateNodalField (SimpleAverageRecovery)."""
+        f = {"heat_flux": 0, "conductivity": 1}[field]
+        nc = self.nsd if f == 0 else 1
+        out = np.zeros(self.nnodes * nc)
+        ref_lib().ref_nodal_field(self.h, f, _ptr(_f64(U)), _ptr(out))
+        return out.reshape(-1, nc) if nc > 1 else out
 
     def set_operator(self, op):
         """LinearSolverConfig::OperatorType of the stages' linear solves: "csr" or "fem" (FEMOperator)."""

@@ -36,6 +36,10 @@
 #include "linalg/operations/MatrixOps.hpp"
 #include "linalg/operator/CSROperator.hpp"
 #include "linalg/operator/FEMOperator.hpp"
+#include "fem/quantity/QuantityEvaluator.hpp"
+#include "fem/quantity/recovery/SimpleAverageRecovery.hpp"
+#include "equation/heateq/evaluator/HeatFluxField.hpp"
+#include "equation/heateq/evaluator/ConductivityField.hpp"
 #include "linalg/solver/iterative/cg/Solver.hpp"
 #include "linalg/solver/iterative/gmres/Solver.hpp"
 #include "linalg/solver/preconditioner/Jacobi.hpp"
@@ -223,6 +227,7 @@ struct Base {
 	virtual int backwardEuler(double dt, int64_t nsteps, int solverType, int precond, double tol, int64_t maxit, int64_t krylov, double* U, double* residualPerStep, double* stepStats) = 0;
 	virtual void adjointGradient(const double* T, const double* lam, double* grad) = 0;
 	int opType = 0;   // LinearSolverConfig::OperatorType of the stages' linear solves: 0 CSR, 1 FEM
+	virtual void nodalField(int field, const double* U, double* out) = 0;
 };
 
 template<int NSD>
@@ -552,6 +557,20 @@ struct RefHeatProblem final : Base {
 		return rc;
 	}
 
+	// HeatProblem::computeNodalField (HeatProblem.tpp:293-303): the reference QuantityEvaluator with
+	// SimpleAverageRecovery over the operator model; field 0 HeatFluxField, 1 ConductivityField
+	void nodalField(int field, const double* U, double* out) override {
+		loadState(U, nullptr);
+		StateVectorT state;
+		state.valueSource = U_.get();
+		auto run = [&](auto fld) {
+			using FieldT = decltype(fld);
+			fem::quantity::QuantityEvaluator<CPU>::template evaluateNodalField<1, EvalEle, EvalQP, OpModelT, FieldT, typename Fam::Quad, fem::quantity::recovery::SimpleAverageRecovery, StateVectorT>(mesh_, *topo_, ess_, 0.0, opModel_, fld, evalEle_, quad_, state, fem::quantity::recovery::SimpleAverageRecovery{}, out);
+		};
+		if (field == 0) run(equation::heateq::evaluator::HeatFluxField<NSD>{});
+		else run(equation::heateq::evaluator::ConductivityField{});
+	}
+
 	// dJ/dk_e contribution lam_e^T Khat_e T_e for every element, with Khat_e the unit-conductivity
 	// element stiffness built by the reference QP evaluator and DiffusionForm; T and lam are free
 	// vectors (constrained entries contribute their Dirichlet value for T and zero for lam).
@@ -605,6 +624,7 @@ void* ref_create(const ref_desc* d) {
 }
 void ref_destroy(void* h) { delete static_cast<Base*>(h); }
 void ref_set_operator(void* h, int op) { static_cast<Base*>(h)->opType = op; }
+void ref_nodal_field(void* h, int field, const double* U, double* out) { static_cast<Base*>(h)->nodalField(field, U, out); }
 int64_t ref_num_nodes(void* h) { return (int64_t)static_cast<Base*>(h)->numNodes(); }
 int64_t ref_num_elems(void* h) { return (int64_t)static_cast<Base*>(h)->numElems(); }
 int64_t ref_num_free(void* h) { return (int64_t)static_cast<Base*>(h)->numFree(); }

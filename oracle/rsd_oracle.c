@@ -728,6 +728,38 @@ void ro_natural(ro_problem* P, double* F) {
 	}
 }
 
+/* QuantityEvaluator::evaluateNodalField (fem/quantity/backend/cpu/QuantityEvaluator.tpp:205-257) with
+ * SimpleAverageRecovery: per element and point, the field value (0: HeatFluxField, -k grad T;
+ * 1: ConductivityField, k) is accumulated at every element node with weight N_a * measure * w, and
+ * divided by the summed weights; T gathered Full.  out: nnodes * components. */
+void ro_nodal_field(ro_problem* P, int32_t field, const double* U, double* out) {
+	const int S = P->m->nsd, npe = P->m->npe, nc = field == 0 ? S : 1;
+	const int64_t nn = P->m->nnodes;
+	double* wsum = calloc((size_t)nn, sizeof(double));
+	memset(out, 0, sizeof(double) * nn * nc);
+	double Ue[RO_MAXN], Z[RO_MAXN] = {0}, coords[RO_MAXN * 3];
+	for (int64_t e = 0; e < P->m->nelem; ++e) {
+		const int64_t* nodes = P->m->ien + e * npe;
+		gather(P, nodes, G_FULL, U, P->g, Ue);
+		coords_of(P, nodes, coords);
+		const double ke = P->kElem ? P->kElem[e] : 1.0;
+		for (int q = 0; q < P->nq; ++q) {
+			ro_qp Q; qp_eval(P, q, coords, &Q); qp_state(P, &Q, Ue, Z);
+			const double k = ke * Q.k;
+			double val[3];
+			if (field == 0) for (int i = 0; i < S; ++i) val[i] = -(k * Q.gradT[i]);
+			else val[0] = k;
+			for (int a = 0; a < npe; ++a) {
+				const double wa = Q.N[a] * Q.measure * Q.w;
+				for (int c = 0; c < nc; ++c) out[nodes[a] * nc + c] += wa * val[c];
+				wsum[nodes[a]] += wa;
+			}
+		}
+	}
+	for (int64_t v = 0; v < nn; ++v) for (int c = 0; c < nc; ++c) out[v * nc + c] /= wsum[v];
+	free(wsum);
+}
+
 /* adjoint: grad_e = lam_e^T Khat_e T_e with Khat_e the unit-conductivity element stiffness,
  * T_e gathered Full (Dirichlet values), lam_e gathered Free */
 void ro_adjoint_gradient(ro_problem* P, const double* T, const double* lam, double* grad) {

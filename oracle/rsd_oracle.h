@@ -69,6 +69,7 @@ void ro_assemble_vector(ro_problem* p, int32_t which, double coef, const double*
 void ro_lift(ro_problem* p, double cDiff, double cMass, double* F);
 int ro_set_flux(ro_problem* p, int32_t tag, const char* const* exprs);
 void ro_natural(ro_problem* p, double* F);
+void ro_nodal_field(ro_problem* p, int32_t field, const double* U, double* out);
 void ro_diagonal(ro_problem* p, double cDiff, double cMass, const double* U, double* d);
 void ro_adjoint_gradient(ro_problem* p, const double* T, const double* lam, double* grad);
 

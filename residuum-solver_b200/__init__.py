@@ -116,6 +116,7 @@ SIGNATURES = {
     "rsd_heat_solve_fem": [_P, _P, _D, C.POINTER(SolverConfig), _P, _P, C.POINTER(Report)],
     "rsd_heat_set_flux": [_P, _P, _I32, C.POINTER(C.c_char_p)],
     "rsd_apply_natural": [_P, _P, _P],
+    "rsd_heat_nodal_field": [_P, _P, _I32, _P, _P, _P],
     "rsd_heat_steady": [_P, _P, C.POINTER(SolverConfig), _P, C.POINTER(Report)],
     "rsd_heat_be_step": [_P, _P, _D, C.POINTER(SolverConfig), _P, _P, C.POINTER(Report), C.POINTER(_D)],
     "rsd_heat_be_step_host": [_P, _P, _D, C.POINTER(SolverConfig), _P, C.POINTER(Report), C.POINTER(_D)],
@@ -447,6 +448,16 @@ class Heat:
             return
         arr = (C.c_char_p * len(exprs))(*[e.encode() for e in exprs])
         check(lib().rsd_heat_set_flux(self.ctx.h, self.h, tag, arr))
+
+    def nodal_field(self, U, field="heat_flux"):
+        """Nodal recovery of the heat flux (nnodes x nsd) or the conductivity (nnodes) from U."""
+        f = {"heat_flux": 0, "conductivity": 1}[field]
+        nc = self.mesh.nsd if f == 0 else 1
+        out = self.ctx.array(self.mesh.nnodes * nc)
+        scratch = self.ctx.array(self.mesh.nnodes)
+        check(lib().rsd_heat_nodal_field(self.ctx.h, self.h, f, _ptr(U), _ptr(out), _ptr(scratch)))
+        a = out.download()
+        return a.reshape(-1, nc) if nc > 1 else a
 
     def apply_natural(self, F):
         check(lib().rsd_apply_natural(self.ctx.h, self.h, _ptr(F)))

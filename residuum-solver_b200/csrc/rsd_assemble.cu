@@ -1201,6 +1201,73 @@ __global__ void __launch_bounds__(128) k_natural(int64_t nfaces, const int32_t* 
 	}
 }
 
+// QuantityEvaluator::evaluateNodalField (fem/quantity/backend/cpu/QuantityEvaluator.tpp:205-257) with
+// SimpleAverageRecovery (fem/quantity/recovery/SimpleAverageRecovery.hpp): at every quadrature point of
+// every element the field's value is added to each of the element's nodes with weight
+// N_a |J| w, and the weights themselves are summed; k_nodal_finish divides.  field 0: HeatFluxField
+// (Q = -K grad T, K = k(T) I times the element factor, equation/heateq/evaluator/HeatFluxField.hpp),
+// 1: ConductivityField (K[0]).  The temperature is gathered Full (Dirichlet values on constrained
+// nodes).  One thread per element.
+template <int NSD, int P>
+__global__ void __launch_bounds__(128) k_nodal_field(const AsmParams prm, int field, int G, double* __restrict__ acc,
+                                                     double* __restrict__ wsum) {
+	using E = Elem<NSD, P>;
+	constexpr int NPE = E::NPE;
+	const int NC = field == 0 ? NSD : 1;
+	const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+	if (e >= prm.nelem) return;
+	const int32_t* en = prm.ien + e * NPE;
+	double Ue[NPE];
+#pragma unroll
+	for (int a = 0; a < NPE; ++a) {
+		const int32_t v = en[a], r = prm.t2a[v];
+		Ue[a] = r >= 0 ? (prm.U ? prm.U[r] : 0.0) : prm.g[v];
+	}
+	const double ke = prm.kElem ? prm.kElem[e] : 1.0;
+	const double* wq = prm.tables + (size_t)prm.nq * G * 4;
+	for (int q = 0; q < prm.nq; ++q) {
+		const double* tq = prm.tables + (size_t)q * G * 4;
+		double J[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, gxi[3] = {0.0, 0.0, 0.0}, T = 0.0;
+		for (int a = 0; a < NPE; ++a) {
+			const double* ta = tq + a * 4;
+			const double* xa = prm.xyz + (int64_t)en[a] * NSD;
+			T += ta[0] * Ue[a];
+#pragma unroll
+			for (int al = 0; al < NSD; ++al) {
+				gxi[al] += ta[1 + al] * Ue[a];
+#pragma unroll
+				for (int i = 0; i < NSD; ++i) J[i * NSD + al] += ta[1 + al] * xa[i];
+			}
+		}
+		double inv[9];
+		const double meas = sqrt(jac_geom<NSD, true>(J, inv));
+		const double k = ke * (prm.kExpr.n ? eval_expr(prm.kExpr, 0.0, 0.0, 0.0, 0.0, T) : prm.kConst);
+		double val[3];
+		if (field == 0) {
+#pragma unroll
+			for (int i = 0; i < NSD; ++i) {
+				double gi = 0.0;
+#pragma unroll
+				for (int al = 0; al < NSD; ++al) gi += inv[i * NSD + al] * gxi[al];
+				val[i] = -(k * gi);
+			}
+		} else {
+			val[0] = k;
+		}
+		for (int a = 0; a < NPE; ++a) {
+			const double wa = tq[a * 4] * meas * wq[q];
+			const int64_t v = en[a];
+			for (int c = 0; c < NC; ++c) atomicAdd(acc + v * NC + c, wa * val[c]);
+			atomicAdd(wsum + v, wa);
+		}
+	}
+}
+
+__global__ void k_nodal_finish(int64_t nnodes, int nc, const double* __restrict__ wsum, double* __restrict__ acc) {
+	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nnodes * nc; i += (int64_t)gridDim.x * blockDim.x)
+		acc[i] /= wsum[i / nc];
+}
+
 // ---------------------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------------------
@@ -1782,6 +1849,28 @@ int apply_natural(rsd_ctx* ctx, rsd_heat* h, double* F) {
 	else if (nsd == 3 && ord == 2) RSD_NAT(3, 2);
 	else return set_error(RSD_EINVAL, "unsupported element");
 #undef RSD_NAT
+	RSD_CUDA(cudaGetLastError());
+	return RSD_OK;
+}
+
+// HeatProblem::computeNodalField (HeatProblem.tpp:293-303) for the heat flux (field 0, nsd components
+// per node) or the conductivity (field 1): out has nnodes * components entries; scratch nnodes
+int nodal_field(rsd_ctx* ctx, rsd_heat* h, int field, const double* U, double* out, double* scratch) {
+	AsmParams p = params_for(h);
+	p.U = U;
+	const int nsd = h->m->nsd, ord = h->m->order, nc = field == 0 ? nsd : 1, G = group_width(h->m->npe);
+	RSD_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * h->m->nnodes * nc, ctx->stream));
+	RSD_CUDA(cudaMemsetAsync(scratch, 0, sizeof(double) * h->m->nnodes, ctx->stream));
+	const int blocks = (int)std::max<int64_t>(1, (h->m->nelem + 127) / 128);
+#define RSD_NF(D, Q) k_nodal_field<D, Q><<<blocks, 128, 0, ctx->stream>>>(p, field, G, out, scratch)
+	if (nsd == 2 && ord == 1) RSD_NF(2, 1);
+	else if (nsd == 2 && ord == 2) RSD_NF(2, 2);
+	else if (nsd == 2 && ord == 3) RSD_NF(2, 3);
+	else if (nsd == 3 && ord == 1) RSD_NF(3, 1);
+	else if (nsd == 3 && ord == 2) RSD_NF(3, 2);
+	else return set_error(RSD_EINVAL, "unsupported element");
+#undef RSD_NF
+	k_nodal_finish<<<vec_grid(ctx, h->m->nnodes * nc), 256, 0, ctx->stream>>>(h->m->nnodes, nc, scratch, out);
 	RSD_CUDA(cudaGetLastError());
 	return RSD_OK;
 }

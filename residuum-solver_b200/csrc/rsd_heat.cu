@@ -242,6 +242,14 @@ int rsd_apply_natural(rsd_ctx* ctx, rsd_heat* h, double* F) {
 	return RSD_OK;
 }
 
+int rsd_heat_nodal_field(rsd_ctx* ctx, rsd_heat* h, int32_t field, const double* U, double* out, double* scratch) {
+	if (!ctx || !h || !out || !scratch || (h->n && !U)) return set_error(RSD_EINVAL, "null argument");
+	if (field != RSD_FIELD_HEAT_FLUX && field != RSD_FIELD_CONDUCTIVITY) return set_error(RSD_EINVAL, "unknown nodal field");
+	RSD_CHECK(nodal_field(ctx, h, field, U, out, scratch));
+	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+	return RSD_OK;
+}
+
 int rsd_heat_solve_fem(rsd_ctx* ctx, rsd_heat* h, double c_mass, const rsd_solver_cfg* cfg, const double* b, double* x,
                        rsd_report* rep) {
 	if (!ctx || !h || !cfg) return set_error(RSD_EINVAL, "null argument");

@@ -241,6 +241,7 @@ int apply_operator(rsd_ctx* ctx, rsd_heat* h, double coef, const double* U, cons
                    const int32_t* skip);
 int set_flux(rsd_ctx* ctx, rsd_heat* h, int tag, const char* const* exprs);
 int apply_natural(rsd_ctx* ctx, rsd_heat* h, double* F);
+int nodal_field(rsd_ctx* ctx, rsd_heat* h, int field, const double* U, double* out, double* scratch);
 int solve_fem(rsd_ctx* ctx, rsd_heat* h, double coef, const rsd_solver_cfg* cfg, const double* b, double* x,
               rsd_report* rep);
 int build_tables(rsd_ctx* ctx, rsd_heat* h);

@@ -266,6 +266,21 @@ def test_natural_bcs_known_answers():
         assert abs(F2[node(i, j, k)] - e) <= TOL
 
 
+@pytest.mark.skipif(not oracle.reference_available(), reason="oracle/_ref not built (reference tree absent)")
+def test_nodal_field_recovery_matches_reference():
+    # QuantityEvaluator::evaluateNodalField with SimpleAverageRecovery (heat flux, conductivity):
+    # the restatement is bit-exact with the reference's own evaluator
+    for nsd, order, nq, nel, kw, rk in [(2, 1, 2, [5, 4], {}, {}), (3, 1, 2, [4, 3, 3], {}, {}),
+                                        (3, 2, 3, [3, 2, 2], dict(k_expr="1 + 0.5*T"), dict(k_a=1.0, k_b=0.5))]:
+        r = oracle.Reference(nsd, order, nq, nel, [0] * nsd, [1] * nsd, [0, 1], bc_kind=0, bc_val={0: 0.0, 1: 1.0},
+                             src_kind=0, src_c=1.0, **rk)
+        m = oracle.BlockMesh(nsd, nel, [0] * nsd, [1] * nsd, order)
+        o = oracle.Oracle(m, nq, bc={0: "0", 1: "1"}, src_expr="1", **kw)
+        U = np.sin(np.arange(o.n) * 0.7)
+        assert (r.nodal_field(U) == o.nodal_field(U)).all()
+        assert (r.nodal_field(U, "conductivity") == o.nodal_field(U, "conductivity")).all()
+
+
 def test_blockmesh_generator_matches_restatement():
     rsd = load_package()
     from importlib import import_module
