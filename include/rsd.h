@@ -74,7 +74,7 @@ typedef struct rsd_solver_cfg {
 	                                (the batched solver: [1e-3, 0.1]) */
 	int32_t operator_type;       /* RSD_OP_CSR, or RSD_OP_FEM: the heat stages assemble no matrix and solve with the
 	                                matrix-free operator (FEMOperator: element-kernel products, Jacobi from the
-	                                element diagonal; CG in FP64).  rsd_solve and rsd_batch_solve take RSD_OP_CSR. */
+	                                element diagonal; CG or GMRES in FP64).  rsd_solve and rsd_batch_solve take RSD_OP_CSR. */
 	int32_t reserved;            /* zero */
 } rsd_solver_cfg;
 
@@ -205,8 +205,8 @@ int rsd_assemble_vector(rsd_ctx* ctx, rsd_heat* h, int32_t which, double coef, c
  * (application/heateq/problem/HeatProblem.tpp:274-289) over FEMOperator (linalg/operator/FEMOperator.hpp:39-56)
  * with the forms Diffusion + c_mass*Mass: solves A x = b without a matrix, every product an element
  * pass (rsd_assemble_vector mode 4 with the iterate as the k(T) state), Jacobi from the element
- * diagonal (Assembler::assembleDiagonal).  cfg: type RSD_CG, precision RSD_FP64; operator_type is not
- * read.  b, x device vectors of num_free entries; x holds the initial guess. */
+ * diagonal (Assembler::assembleDiagonal).  cfg: type RSD_CG or RSD_GMRES, precision RSD_FP64;
+ * operator_type is not read.  b, x device vectors of num_free entries; x holds the initial guess. */
 int rsd_heat_solve_fem(rsd_ctx* ctx, rsd_heat* h, double c_mass, const rsd_solver_cfg* cfg, const double* b, double* x,
                        rsd_report* report);
 /* A flux boundary condition given by one expression per spatial component, q(t, x, y, z), on a

@@ -912,17 +912,6 @@ static int cg_fem(rsd_ctx* ctx, rsd_heat* h, double coef, const rsd_solver_cfg* 
 
 }  // namespace
 
-int solve_fem(rsd_ctx* ctx, rsd_heat* h, double coef, const rsd_solver_cfg* cfg, const double* b, double* x,
-              rsd_report* rep) {
-	if (!ctx || !h || !cfg || (h->n && (!b || !x))) return set_error(RSD_EINVAL, "null argument");
-	if (cfg->max_iters < 0 || !(cfg->tol >= 0)) return set_error(RSD_EINVAL, "bad solver configuration");
-	if (cfg->type != RSD_CG) return set_error(RSD_EINVAL, "the matrix-free operator solves with CG (type RSD_CG)");
-	if (cfg->precision != RSD_FP64) return set_error(RSD_EINVAL, "the matrix-free operator solves in FP64 (precision RSD_FP64)");
-	if (rep) *rep = rsd_report{};
-	if (h->n == 0) { if (rep) rep->converged = 1; return RSD_OK; }
-	RSD_CUDA(cudaSetDevice(ctx->device));
-	return cg_fem(ctx, h, coef, cfg, b, x, rep);
-}
 
 void free_graph_cache(rsd_ctx* ctx) {
 	if (!ctx->graphs) return;
@@ -1043,18 +1032,66 @@ __global__ void k_gm_invdiag(int64_t n, const int32_t* __restrict__ dpos, const 
 	}
 }
 
+// The operator of a GMRES solve: an assembled matrix (CSR/SELL, FP64 or its FP32 copy) ...
 template <typename T>
-static int gmres_run(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const double* b, double* x, rsd_report* rep) {
+struct GmCsrOp {
+	rsd_ctx* ctx;
+	rsd_csr* A;
+	int64_t n;
+	int prepare() { return sizeof(T) == 4 ? f32_sync(ctx, A) : exec_sync(ctx, A); }
+	int invdiag(T* invD, const double*) {
+		k_gm_invdiag<T><<<vec_grid(ctx, n), 256, 0, ctx->stream>>>(n, exec_diag(A), exec_val(A), invD);
+		RSD_CUDA(cudaGetLastError());
+		return RSD_OK;
+	}
+	// w = A (M^-1 q)
+	int prec_apply(const T* q, const T* invD, T* w, T*, const double*) {
+		const int L = exec_lanes(A);
+		const MatView<T> V = exec_view<T>(A);
+		RSD_DISPATCH_L(L, (k_gm_spmv<LL, T><<<wave_blocks(ctx, k_gm_spmv<LL, T>, 256, n * std::max(LL, 1)), 256, 0, ctx->stream>>>(n, V, q, invD, w)));
+		RSD_CUDA(cudaGetLastError());
+		return RSD_OK;
+	}
+	int apply64(const double* x, double* Ax) { return spmv_f64(ctx, A, x, Ax); }
+};
+
+// ... or the matrix-free operator (FEMOperator, FP64): every product an element pass with the
+// iterate as the k(T) state, Jacobi from the element diagonal at the initial iterate
+__global__ void k_gm_scale_by(int64_t n, const double* __restrict__ q, const double* __restrict__ d, double* __restrict__ out) {
+	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+		out[i] = d ? q[i] * d[i] : q[i];
+}
+struct GmFemOp {
+	rsd_ctx* ctx;
+	rsd_heat* h;
+	double coef;
+	int64_t n;
+	int prepare() { return RSD_OK; }
+	int invdiag(double* invD, const double* x) {
+		RSD_CHECK(assemble_diagonal(ctx, h, 1.0, coef, x, invD));
+		k_inv_guarded<<<vec_grid(ctx, n), 256, 0, ctx->stream>>>(n, invD);
+		RSD_CUDA(cudaGetLastError());
+		return RSD_OK;
+	}
+	int prec_apply(const double* q, const double* invD, double* w, double* tmp, const double* x) {
+		k_gm_scale_by<<<vec_grid(ctx, n), 256, 0, ctx->stream>>>(n, q, invD, tmp);
+		RSD_CUDA(cudaGetLastError());
+		return apply_operator(ctx, h, coef, x, tmp, w, nullptr);
+	}
+	int apply64(const double* x, double* Ax) { return apply_operator(ctx, h, coef, x, x, Ax, nullptr); }
+};
+
+template <typename T, typename Op>
+static int gmres_core(rsd_ctx* ctx, Op& op, const rsd_solver_cfg* cfg, const double* b, double* x, rsd_report* rep) {
 	constexpr bool kMixed = sizeof(T) == 4;
-	const int64_t n = A->n;
+	const int64_t n = op.n;
 	const int64_t m = std::max<int64_t>(1, cfg->krylov_dim);
 	if (m + 1 > 255) return set_error(RSD_EINVAL, "GMRES krylov_dim above 254");
-	if (kMixed) RSD_CHECK(f32_sync(ctx, A)); else RSD_CHECK(exec_sync(ctx, A));
-	const int L = exec_lanes(A);
-	const MatView<T> V = exec_view<T>(A);
+	RSD_CHECK(op.prepare());
 	const int64_t ns = pad_len(n);
-	// workspace: Q (m+1 vectors), w, invD in T; Ax in FP64; partials for m+1 reductions; tickets; H columns
-	const size_t qBytes = sizeof(T) * (size_t)(m + 3) * ns;
+	// workspace: Q (m+1 vectors), w, invD and a scratch vector in T; Ax in FP64; partials for m+1
+	// reductions; tickets; H columns
+	const size_t qBytes = sizeof(T) * (size_t)(m + 4) * ns;
 	const size_t axBytes = sizeof(double) * (size_t)ns;
 	const size_t pBytes = sizeof(double) * (size_t)(m + 1) * kMaxPartials;
 	const size_t hBytes = sizeof(double) * (size_t)(4 * (m + 2) + 8);
@@ -1065,6 +1102,7 @@ static int gmres_run(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const 
 	T* Q = (T*)base;
 	T* w = Q + (m + 1) * ns;
 	T* invD = cfg->precond == RSD_JACOBI ? w + ns : nullptr;
+	T* tmp = w + 2 * ns;
 	double* Ax = (double*)(base + qBytes);
 	double* parts = (double*)(base + qBytes + axBytes);
 	double* dH1 = (double*)(base + qBytes + axBytes + pBytes);
@@ -1079,10 +1117,10 @@ static int gmres_run(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const 
 	const double breakdownTol = 1e-14, eps = 1e-50;
 	std::vector<double> H((m + 1) * m, 0.0), cs(m), sn(m), g(m + 1), yv(m), col(2 * (m + 2));
 	auto Hat = [&](int64_t i, int64_t j) -> double& { return H[j * (m + 1) + i]; };
-	if (invD) k_gm_invdiag<T><<<gv, 256, 0, st>>>(n, exec_diag(A), exec_val(A), invD);
+	if (invD) RSD_CHECK(op.invdiag(invD, x));
 	// FP64 residual of the current x; q0 = r / beta
 	auto residual = [&](double* beta) -> int {
-		RSD_CHECK(spmv_f64(ctx, A, x, Ax));
+		RSD_CHECK(op.apply64(x, Ax));
 		k_gm_resnorm<<<grd, kReduceThreads, 0, st>>>(n, b, Ax, parts, tickets + m + 1, dNorm);
 		RSD_CUDA(cudaGetLastError());
 		RSD_CUDA(cudaMemcpyAsync(ctx->s.hbuf, dNorm, sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -1111,7 +1149,7 @@ static int gmres_run(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const 
 		bool breakdown = false;
 		for (int64_t j = 0; j < m; ++j) {
 			const T* qj = Q + j * ns;
-			RSD_DISPATCH_L(L, (k_gm_spmv<LL, T><<<wave_blocks(ctx, k_gm_spmv<LL, T>, 256, n * std::max(LL, 1)), 256, 0, st>>>(n, V, qj, invD, w)));
+			RSD_CHECK(op.prec_apply(qj, invD, w, tmp, x));
 			const int k = (int)(j + 1);
 			for (double* dh : {dH1, dH2}) {
 				k_gm_mdot<T><<<dim3(grd, k), kReduceThreads, 0, st>>>(n, Q, ns, w, parts, tickets, dh);
@@ -1164,6 +1202,12 @@ static int gmres_run(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const 
 	R.refinements = kMixed ? cycles : 0;
 	if (rep) *rep = R;
 	return RSD_OK;
+}
+
+template <typename T>
+static int gmres_run(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const double* b, double* x, rsd_report* rep) {
+	GmCsrOp<T> op{ctx, A, A->n};
+	return gmres_core<T>(ctx, op, cfg, b, x, rep);
 }
 
 // ---- FP64 PCG over a static device scratch ---------------------------------------------------
@@ -1248,6 +1292,23 @@ static int cg_fp64_static(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, c
 }
 
 }  // namespace
+
+int solve_fem(rsd_ctx* ctx, rsd_heat* h, double coef, const rsd_solver_cfg* cfg, const double* b, double* x,
+              rsd_report* rep) {
+	if (!ctx || !h || !cfg || (h->n && (!b || !x))) return set_error(RSD_EINVAL, "null argument");
+	if (cfg->max_iters < 0 || !(cfg->tol >= 0)) return set_error(RSD_EINVAL, "bad solver configuration");
+	if (cfg->type != RSD_CG && cfg->type != RSD_GMRES) return set_error(RSD_EINVAL, "unknown solver type");
+	if (cfg->precision != RSD_FP64) return set_error(RSD_EINVAL, "the matrix-free operator solves in FP64 (precision RSD_FP64)");
+	if (cfg->type == RSD_GMRES && cfg->krylov_dim <= 0) return set_error(RSD_EINVAL, "GMRES needs krylov_dim >= 1");
+	if (rep) *rep = rsd_report{};
+	if (h->n == 0) { if (rep) rep->converged = 1; return RSD_OK; }
+	RSD_CUDA(cudaSetDevice(ctx->device));
+	if (cfg->type == RSD_GMRES) {
+		GmFemOp op{ctx, h, coef, h->n};
+		return gmres_core<double>(ctx, op, cfg, b, x, rep);
+	}
+	return cg_fem(ctx, h, coef, cfg, b, x, rep);
+}
 
 int solve(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const double* b, double* x, rsd_report* rep) {
 	if (!ctx || !A || !cfg || (A->n && (!b || !x))) return set_error(RSD_EINVAL, "null argument");

@@ -137,6 +137,11 @@ def fem():
     r.set_operator("fem")
     U, rep = r.steady(0, 1, 1e-10, 1000)
     save("fem_steady_q2_hex_3x3x2.npz", U=U, iterations=rep["iterations"])
+    # GMRES(7) + Jacobi over the matrix-free operator, the 16x16 Q1 steady problem
+    r = oracle.Reference(2, 1, 2, [16, 16], [0, 0], [1, 1], [0, 1, 2, 3], bc_kind=2)
+    r.set_operator("fem")
+    U, rep = r.steady(1, 1, 1e-10, 1000, 7)
+    save("fem_steady_gmres7_q1_quad_16.npz", U=U, iterations=rep["iterations"], finalResidual=rep["finalResidual"])
     # k(T) = 1 + 0.5 T in a linear stage: the operator's state is the solve's own iterate (the stage
     # binds its state to U, which the solver updates in place), so the operator changes as CG runs
     r = oracle.Reference(3, 2, 3, [3, 3, 2], [0, 0, 0], [1, 1, 1], [0, 1], bc_kind=0, bc_val={0: 0.0, 1: 1.0},

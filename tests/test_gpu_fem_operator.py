@@ -157,10 +157,23 @@ def test_identity_preconditioner_and_limits(rsd, ctx):
     assert not r["converged"] and r["iterations"] == 5
 
 
+def test_gmres_over_the_operator_matches_reference(rsd, ctx):
+    g = golden("fem_steady_gmres7_q1_quad_16.npz")
+    h = make_heat(rsd, ctx, 2, 1, 2, [16, 16], [0, 0], [1, 1], dirichlet={t: "(1-x)*(1-y)" for t in range(4)})
+    U = ctx.array(h.n).zero()
+    rep = h.steady(U, cfg=fem_cfg(rsd, type=rsd.GMRES, krylov_dim=7))
+    assert rep["converged"] and rep["iterations"] == g["iterations"]
+    assert relerr(U.download(), g["U"]) <= REL
+    # the same system through the assembled matrix
+    U2 = ctx.array(h.n).zero()
+    rep2 = h.steady(U2, type=rsd.GMRES, precond=rsd.JACOBI, tol=1e-10, max_iters=1000, krylov_dim=7)
+    assert rep2["iterations"] == rep["iterations"] and relerr(U.download(), U2.download()) <= REL
+
+
 def test_configurations_the_operator_does_not_take(rsd, ctx):
     h = make_heat(rsd, ctx, 2, 1, 2, [4, 4], [0, 0], [1, 1], src_expr="1", dirichlet={0: "0"})
     U, b = ctx.array(h.n).zero(), ctx.array(h.n).zero()
-    for kw in (dict(type=rsd.GMRES), dict(precision=rsd.MIXED)):
+    for kw in (dict(precision=rsd.MIXED), dict(type=rsd.GMRES, krylov_dim=0)):
         with pytest.raises(rsd.RsdError, match="RSD_EINVAL"):
             h.steady(U, cfg=fem_cfg(rsd, **kw))
         with pytest.raises(rsd.RsdError, match="RSD_EINVAL"):
