@@ -464,7 +464,7 @@ class Heat:
 
     def solve_fem(self, b, x, c_mass=0.0, cfg=None, **kw):
         """(Diffusion + c_mass Mass) x = b without a matrix: the LinearSolverRunner the reference builds
-        for operator type `fem` (FEMOperator), CG + Jacobi in FP64; x holds the initial guess."""
+        for operator type `fem` (FEMOperator), CG or GMRES(m) + Jacobi in FP64; x holds the initial guess."""
         cfg = cfg or SolverConfig.make(**kw)
         rep = Report()
         check(lib().rsd_heat_solve_fem(self.ctx.h, self.h, c_mass, C.byref(cfg), _ptr(b), _ptr(x), C.byref(rep)))
