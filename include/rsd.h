@@ -198,7 +198,8 @@ int rsd_assemble_matrix(rsd_ctx* ctx, rsd_heat* h, double c_diff, double c_mass,
                         const double* U, const double* Udot, rsd_csr* A);
 /* Assembler::assembleVector (Assembler.tpp:199-255) with the stages' form/operand pairings:
  * which 0: load (SourceForm); 1: Diffusion on U (Full); 2: rho*cp*Mass on U (Full);
- * 3: rho*cp*Mass on Udot (Free); 4: Diffusion + coef*Mass on operand (Free; FEMOperator::apply) */
+ * 3: rho*cp*Mass on Udot (Free); 4: Diffusion + coef*Mass on operand (Free; FEMOperator::apply);
+ * 10: Diffusion + TangentDiffusion + coef*Mass on operand at the state U (the Jacobian's product) */
 int rsd_assemble_vector(rsd_ctx* ctx, rsd_heat* h, int32_t which, double coef, const double* U, const double* Udot,
                         const double* operand, double* out);
 /* The LinearSolverRunner HeatProblem::makeLinearRunner builds for OperatorType::FEM
@@ -248,7 +249,9 @@ int rsd_heat_be_step_host(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver
                           rsd_report* report, double* residual_norm);
 /* NewtonRunner::solve over SteadyStage nonlinear mode (solver/nonlinear/Newton.hpp:32-83,
  * solver/stage/SteadyStage.hpp:89-116): R = F - K(T)T, J = K + K_T, J dU = R, U += dU.
- * linear->operator_type: RSD_OP_CSR (the Jacobian forms have no matrix-free product here). */
+ * linear->operator_type RSD_OP_FEM: J is not assembled; each product of the linear solve is an element
+ * pass of Diffusion + TangentDiffusion at the Newton state (the reference's FEMOperator over the
+ * Jacobian forms), Jacobi from that operator's element diagonal. */
 int rsd_heat_newton(rsd_ctx* ctx, rsd_heat* h, double abs_tol, double rel_tol, int64_t max_iters,
                     const rsd_solver_cfg* linear, double* U, rsd_report* report);
 

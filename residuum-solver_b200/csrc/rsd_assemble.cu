@@ -587,13 +587,13 @@ template <int NSD, int P, int W>
 __global__ void __launch_bounds__(kAsmThreads) k_asm_vector(const AsmParams prm) {
 	constexpr int which = W;
 	// the diffusion-type terms need gradients; load and mass terms only the measure
-	constexpr bool kGrad = W == 1 || W == 4 || W == 5 || W == 6 || W == 8 || W == 9;
+	constexpr bool kGrad = W == 1 || W == 4 || W == 5 || W == 6 || W == 8 || W == 9 || W == 10;
 	Needs nd{};
 	nd.load = which == 0 || which == 7 || which == 9;
 	nd.field = which != 0;
 	nd.field2 = which == 8;
 	// k(T): diffusion of U takes T from U itself (staged as V, mirrored into U), the operator from the state
-	nd.state = (prm.kExpr.n != 0 && (which == 1 || which == 4 || which == 8 || which == 9)) || which == 6;
+	nd.state = (prm.kExpr.n != 0 && (which == 1 || which == 4 || which == 8 || which == 9)) || which == 6 || which == 10;
 	if (prm.skip && *(volatile const int32_t*)prm.skip) return;   // uniform over the launch
 	RSD_ELEMENT_LOOP_BEGIN
 	double Va = 0.0, Wa = 0.0, Ua = 0.0;
@@ -602,14 +602,14 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_vector(const AsmParams prm)
 		switch (which) {
 			case 1: case 2: case 8: case 9: Va = fullU; break;                          // GatherMode::Full
 			case 3: Va = (row >= 0 && prm.Udot) ? prm.Udot[row] : 0.0; break;           // Free
-			case 4: Va = (row >= 0 && prm.V) ? prm.V[row] : 0.0; break;                 // Free
+			case 4: case 10: Va = (row >= 0 && prm.V) ? prm.V[row] : 0.0; break;        // Free
 			case 5: Va = row >= 0 ? 0.0 : prm.g[node]; break;                           // Constrained
 			case 6: Va = (row >= 0 && prm.V) ? prm.V[row] : 0.0; break;                 // lambda (Free)
 			case 7: Va = row >= 0 ? (prm.U ? prm.U[row] : 0.0) : (prm.gPrev ? prm.gPrev[node] : prm.g[node]); break;
 			default: break;
 		}
 		if (which == 8) Wa = (row >= 0 && prm.Udot) ? prm.Udot[row] : 0.0;
-		Ua = (which == 4 || which == 6) ? fullU : Va;
+		Ua = (which == 4 || which == 6 || which == 10) ? fullU : Va;
 	}
 	RSD_STAGE_NODE(Ua, Va, Wa)
 	double Fa = 0.0, ge = 0.0;
@@ -655,7 +655,7 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_vector(const AsmParams prm)
 			}
 			if (nd.load) Fa += (rec[R_F] * Na) * wm;
 			if (which == 0) continue;
-			double kd = 0.0;
+			double kd = 0.0, tg = 0.0;
 			if constexpr (kGrad) {
 				double dx[3];
 				node_grad<NSD>(rec, ta, dx);
@@ -663,12 +663,16 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_vector(const AsmParams prm)
 #pragma unroll
 				for (int i = 0; i < NSD; ++i) dd += dx[i] * rec[R_GV + i];
 				kd = rec[R_K] * dd;                        // per-element factor included
+				if (which == 10)                           // TangentDiffusionForm: grad N_a . dk/dT grad T
+#pragma unroll
+					for (int i = 0; i < NSD; ++i) tg += dx[i] * rec[R_DK] * rec[R_GT + i];
 			}
 			const double mass = prm.rho * prm.cp * Na * rec[R_V];
 			switch (which) {
 				case 1: Fa += kd * wm; break;
 				case 2: case 3: Fa += mass * wm; break;
 				case 4: Fa += (kd + prm.coef * mass) * wm; break;
+				case 10: Fa += (kd + tg * rec[R_V] + prm.coef * mass) * wm; break;
 				case 5: Fa += (prm.cDiff * kd + prm.cMass * mass) * wm; break;
 				case 7: Fa += prm.coef * mass * wm; break;
 				case 8: Fa += (kd + prm.rho * prm.cp * Na * rec[R_W]) * wm; break;
@@ -1064,7 +1068,7 @@ template <int NSD, int P>
 __global__ void __launch_bounds__(kAsmThreads) k_asm_diag(const AsmParams prm) {
 	constexpr bool kGrad = true;
 	Needs nd{};
-	nd.state = prm.kExpr.n != 0;
+	nd.state = prm.kExpr.n != 0 || prm.cTDiff != 0.0;
 	RSD_ELEMENT_LOOP_BEGIN
 	const double Ua = (has && nd.state) ? (row >= 0 ? (prm.U ? prm.U[row] : 0.0) : prm.g[node]) : 0.0;
 	RSD_STAGE_NODE(Ua, 0.0, 0.0)
@@ -1078,7 +1082,11 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_diag(const AsmParams prm) {
 			double dd = 0.0;
 #pragma unroll
 			for (int i = 0; i < NSD; ++i) dd += dx[i] * dx[i];
-			Da += (prm.cDiff * rec[R_K] * dd + prm.cMass * prm.rho * prm.cp * ta[0] * ta[0]) * rec[R_WM];
+			double tg = 0.0;
+			if (prm.cTDiff != 0.0)
+#pragma unroll
+				for (int i = 0; i < NSD; ++i) tg += dx[i] * rec[R_DK] * rec[R_GT + i];
+			Da += (prm.cDiff * rec[R_K] * dd + prm.cMass * prm.rho * prm.cp * ta[0] * ta[0] + prm.cTDiff * tg * ta[0]) * rec[R_WM];
 		}
 	}
 	if (has && row >= 0) atomicAdd(prm.out + row, Da);
@@ -1518,6 +1526,7 @@ static int launch_vector_mode(rsd_ctx* ctx, dim3 gr, size_t smem, const AsmParam
 		case 7: return launch_one(k_asm_vector<NSD, P, 7>, gr, smem, ctx, p);
 		case 8: return launch_one(k_asm_vector<NSD, P, 8>, gr, smem, ctx, p);
 		case 9: return launch_one(k_asm_vector<NSD, P, 9>, gr, smem, ctx, p);
+		case 10: return launch_one(k_asm_vector<NSD, P, 10>, gr, smem, ctx, p);
 		default: return set_error(RSD_EINVAL, "unknown vector assembly mode");
 	}
 }
@@ -1691,7 +1700,7 @@ int assemble_matrix(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, doubl
 }
 
 int apply_operator(rsd_ctx* ctx, rsd_heat* h, double coef, const double* U, const double* V, double* out,
-                   const int32_t* skip);
+                   const int32_t* skip, int which);
 
 // the affine path of the vector kernels: every mode but the adjoint, with no state-dependent
 // conductivity and no load term (both are evaluated per quadrature point)
@@ -1699,14 +1708,14 @@ static int affine_vector(rsd_ctx* ctx, rsd_heat* h, AsmParams& p) {
 	RSD_CHECK(ensure_affine(ctx, h));
 	const int w = p.which;
 	const bool load = w == 0 || w == 7 || w == 9;
-	const bool state = h->kExpr.n != 0 && (w == 1 || w == 4 || w == 8 || w == 9);
+	const bool state = (h->kExpr.n != 0 && (w == 1 || w == 4 || w == 8 || w == 9)) || w == 10;
 	if (h->anyAffine && w != 6 && !state && !(load && h->srcExpr.n != 0)) { p.fast = 1; p.affine = h->affine; p.geo = h->geo; p.ktab = h->ktab; if (h->allAffine) p.pts = 0; }
 	return RSD_OK;
 }
 
 int assemble_vector(rsd_ctx* ctx, rsd_heat* h, int which, double coef, const double* U, const double* Udot,
                     const double* operand, double* out, double outScale, bool accumulate) {
-	if (which == 4 && !accumulate && outScale == 1.0) return apply_operator(ctx, h, coef, U, operand, out, nullptr);
+	if (which == 4 && !accumulate && outScale == 1.0) return apply_operator(ctx, h, coef, U, operand, out, nullptr, 4);
 	AsmParams p = params_for(h);
 	p.which = which; p.coef = coef; p.U = U; p.Udot = Udot; p.V = operand; p.out = out; p.outScale = outScale;
 	if (which == 7 && h->gPrevValid) p.gPrev = h->gPrev;
@@ -1728,9 +1737,9 @@ int assemble_vector(rsd_ctx* ctx, rsd_heat* h, int which, double coef, const dou
 // most 32 nodes per element, take the sum-factorized kernel (RSD_SUMFAC=0: the table kernels);
 // 4- and 8-node elements keep the one-thread-per-element table kernel, which measured faster for them.
 int apply_operator(rsd_ctx* ctx, rsd_heat* h, double coef, const double* U, const double* V, double* out,
-                   const int32_t* skip) {
+                   const int32_t* skip, int which) {
 	AsmParams p = params_for(h);
-	p.which = 4; p.coef = coef; p.U = U; p.V = V; p.out = out; p.skip = skip;
+	p.which = which; p.coef = coef; p.U = U; p.V = V; p.out = out; p.skip = skip;
 	RSD_CHECK(affine_vector(ctx, h, p));
 	RSD_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * std::max<int64_t>(h->n, 1), ctx->stream));
 	const int pr = prof_begin(ctx, PF_ASM_VECTOR);
@@ -1875,9 +1884,9 @@ int nodal_field(rsd_ctx* ctx, rsd_heat* h, int field, const double* U, double* o
 	return RSD_OK;
 }
 
-int assemble_diagonal(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, const double* U, double* d) {
+int assemble_diagonal(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, const double* U, double* d, double cTDiff) {
 	AsmParams p = params_for(h);
-	p.cDiff = cDiff; p.cMass = cMass; p.U = U; p.out = d;
+	p.cDiff = cDiff; p.cMass = cMass; p.cTDiff = cTDiff; p.U = U; p.out = d;
 	RSD_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * std::max<int64_t>(h->n, 1), ctx->stream));
 	return launch_k_asm_diag(ctx, h, p);
 }

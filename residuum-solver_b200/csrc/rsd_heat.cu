@@ -224,7 +224,7 @@ int rsd_assemble_matrix(rsd_ctx* ctx, rsd_heat* h, double cd, double cm, double 
 
 int rsd_assemble_vector(rsd_ctx* ctx, rsd_heat* h, int32_t which, double coef, const double* U, const double* Udot,
                         const double* operand, double* out) {
-	if (!ctx || !h || !out || which < 0 || which > 4) return set_error(RSD_EINVAL, "bad argument");
+	if (!ctx || !h || !out || which < 0 || (which > 4 && which != 10)) return set_error(RSD_EINVAL, "bad argument");
 	RSD_CHECK(assemble_vector(ctx, h, which, coef, U, Udot, operand, out, 1.0, false));
 	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
 	return RSD_OK;
@@ -383,7 +383,7 @@ int rsd_heat_be_step_host(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver
 int rsd_heat_newton(rsd_ctx* ctx, rsd_heat* h, double abs_tol, double rel_tol, int64_t max_iters,
                     const rsd_solver_cfg* lin, double* U, rsd_report* rep) {
 	if (!ctx || !h || !lin || !U) return set_error(RSD_EINVAL, "bad argument");
-	if (lin->operator_type != RSD_OP_CSR) return set_error(RSD_EINVAL, "Newton takes operator_type RSD_OP_CSR");
+	const bool fem = lin->operator_type == RSD_OP_FEM;   // needsJ() false: J is applied, not assembled
 	const int64_t n = h->n;
 	rsd_report R{};
 	double res0 = 0.0;
@@ -400,10 +400,11 @@ int rsd_heat_newton(rsd_ctx* ctx, rsd_heat* h, double abs_tol, double rel_tol, i
 		R.initialResidual = res0; R.finalResidual = res; R.finalResidualRel = rel; R.trueResidualRel = rel;
 		if (!std::isfinite(res)) { R.status = RSD_ENAN; break; }
 		if (res < abs_tol || rel < rel_tol) { R.converged = 1; break; }
-		RSD_CHECK(assemble_matrix(ctx, h, 1.0, 0.0, 1.0, 0.0, U, nullptr, h->K));             // J = K + K_T
+		if (!fem) RSD_CHECK(assemble_matrix(ctx, h, 1.0, 0.0, 1.0, 0.0, U, nullptr, h->K));   // J = K + K_T
 		RSD_CUDA(cudaMemsetAsync(h->dU, 0, sizeof(double) * n, ctx->stream));
 		rsd_report lr;
-		RSD_CHECK(solve(ctx, h->K, lin, h->R, h->dU, &lr));
+		if (fem) RSD_CHECK(solve_fem(ctx, h, 0.0, lin, h->R, h->dU, &lr, 10, U));           // J(U) applied per product
+		else RSD_CHECK(solve(ctx, h->K, lin, h->R, h->dU, &lr));
 		R.refinements += lr.iterations;                                                      // total inner iterations
 		if (!lr.converged) { R.status = lr.status; break; }
 		RSD_CHECK(rsd_axpy(ctx, n, 1.0, h->dU, U));                                           // U += dU

@@ -235,14 +235,18 @@ int assemble_matrix(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, doubl
                     const double* U, const double* Udot, rsd_csr* A);
 int assemble_vector(rsd_ctx* ctx, rsd_heat* h, int which, double coef, const double* U, const double* Udot,
                     const double* operand, double* out, double outScale, bool accumulate);
-int assemble_diagonal(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, const double* U, double* d);
+int assemble_diagonal(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, const double* U, double* d,
+                      double cTDiff = 0.0);
 int assemble_lift(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, double* F);
+// which 4: Diffusion + coef Mass (the stages' operator); 10: Diffusion + TangentDiffusion + coef Mass
+// (Newton's Jacobian), both with the state U read through k(T), dk/dT and grad T
 int apply_operator(rsd_ctx* ctx, rsd_heat* h, double coef, const double* U, const double* V, double* out,
-                   const int32_t* skip);
+                   const int32_t* skip, int which = 4);
 int set_flux(rsd_ctx* ctx, rsd_heat* h, int tag, const char* const* exprs);
 int apply_natural(rsd_ctx* ctx, rsd_heat* h, double* F);
 int nodal_field(rsd_ctx* ctx, rsd_heat* h, int field, const double* U, double* out, double* scratch);
+// state null: the iterate x is the state (the stages' linear solves); which as for apply_operator
 int solve_fem(rsd_ctx* ctx, rsd_heat* h, double coef, const rsd_solver_cfg* cfg, const double* b, double* x,
-              rsd_report* rep);
+              rsd_report* rep, int which = 4, const double* state = nullptr);
 int build_tables(rsd_ctx* ctx, rsd_heat* h);
 }  // namespace rsd

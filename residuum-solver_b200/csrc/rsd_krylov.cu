@@ -857,7 +857,8 @@ __global__ void __launch_bounds__(256) k_fem_true_res(int64_t n, const double* _
 // Plain launches in chunks of 8 iterations behind a done-flag poll; after the solve has finished the
 // remaining launches of a chunk return at once (the element pass through its skip flag).
 static int cg_fem(rsd_ctx* ctx, rsd_heat* h, double coef, const rsd_solver_cfg* cfg, const double* b, double* x,
-                  rsd_report* rep) {
+                  rsd_report* rep, int which, const double* state) {
+	const double* U = state ? state : x;   // the operator's state
 	const int64_t n = h->n;
 	void* wsv;
 	const int64_t ns = pad_len(n);
@@ -877,10 +878,10 @@ static int cg_fem(rsd_ctx* ctx, rsd_heat* h, double coef, const rsd_solver_cfg* 
 	RSD_CUDA(cudaMemsetAsync(S, 0, sizeof(CgScal), st));
 	// Jacobi::update on every solve (cg/Solver.tpp:22); the operator's state is the iterate x
 	if (invD) {
-		RSD_CHECK(assemble_diagonal(ctx, h, 1.0, coef, x, invD));
+		RSD_CHECK(assemble_diagonal(ctx, h, 1.0, coef, U, invD, which == 10 ? 1.0 : 0.0));
 		k_inv_guarded<<<vec_grid(ctx, n), 256, 0, st>>>(n, invD);
 	}
-	RSD_CHECK(apply_operator(ctx, h, coef, x, x, r, nullptr));
+	RSD_CHECK(apply_operator(ctx, h, coef, U, x, r, nullptr, which));
 	k_fem_init<<<VG(k_fem_init), 256, 0, st>>>(n, b, r, p, invD, S, partials, tol, rel, maxIt);
 	RSD_CUDA(cudaGetLastError());
 	Poller poll{ctx, S, (int32_t*)ctx->s.hbuf};
@@ -890,7 +891,7 @@ static int cg_fem(rsd_ctx* ctx, rsd_heat* h, double coef, const rsd_solver_cfg* 
 	const GraphCtl off{0, 0, 0, 0};
 	for (int64_t it = 0; it < maxIt + 2 * chunk && !fin; it += chunk) {
 		for (int c = 0; c < chunk; ++c) {
-			RSD_CHECK(apply_operator(ctx, h, coef, x, p, Ap, &S->done));
+			RSD_CHECK(apply_operator(ctx, h, coef, U, p, Ap, &S->done, which));
 			k_fem_alpha<<<VG(k_fem_alpha), 256, 0, st>>>(n, p, Ap, S, partials);
 			k_cg_update<<<VGB(k_cg_update, kVT), kVT, 0, st>>>(n, x, r, p, Ap, invD, S, partials, tol, rel, maxIt, xvec);
 			k_cg_pupdate<<<VGB(k_cg_pupdate, kVT), kVT, 0, st>>>(n, p, r, invD, S, off);
@@ -900,7 +901,7 @@ static int cg_fem(rsd_ctx* ctx, rsd_heat* h, double coef, const rsd_solver_cfg* 
 	}
 	RSD_CHECK(finish_report(ctx, S, rep));
 	// FP64 check of the final iterate: ||b - A x||
-	RSD_CHECK(apply_operator(ctx, h, coef, x, x, Ap, nullptr));
+	RSD_CHECK(apply_operator(ctx, h, coef, U, x, Ap, nullptr, which));
 	k_fem_true_res<<<VG(k_fem_true_res), 256, 0, st>>>(n, b, Ap, partials, &S1->ticket, &S1->res);
 	RSD_CUDA(cudaGetLastError());
 	double hres = 0.0;
@@ -1066,9 +1067,11 @@ struct GmFemOp {
 	rsd_heat* h;
 	double coef;
 	int64_t n;
+	int which;
+	const double* state;   // null: the iterate
 	int prepare() { return RSD_OK; }
 	int invdiag(double* invD, const double* x) {
-		RSD_CHECK(assemble_diagonal(ctx, h, 1.0, coef, x, invD));
+		RSD_CHECK(assemble_diagonal(ctx, h, 1.0, coef, state ? state : x, invD, which == 10 ? 1.0 : 0.0));
 		k_inv_guarded<<<vec_grid(ctx, n), 256, 0, ctx->stream>>>(n, invD);
 		RSD_CUDA(cudaGetLastError());
 		return RSD_OK;
@@ -1076,9 +1079,9 @@ struct GmFemOp {
 	int prec_apply(const double* q, const double* invD, double* w, double* tmp, const double* x) {
 		k_gm_scale_by<<<vec_grid(ctx, n), 256, 0, ctx->stream>>>(n, q, invD, tmp);
 		RSD_CUDA(cudaGetLastError());
-		return apply_operator(ctx, h, coef, x, tmp, w, nullptr);
+		return apply_operator(ctx, h, coef, state ? state : x, tmp, w, nullptr, which);
 	}
-	int apply64(const double* x, double* Ax) { return apply_operator(ctx, h, coef, x, x, Ax, nullptr); }
+	int apply64(const double* x, double* Ax) { return apply_operator(ctx, h, coef, state ? state : x, x, Ax, nullptr, which); }
 };
 
 template <typename T, typename Op>
@@ -1294,7 +1297,7 @@ static int cg_fp64_static(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, c
 }  // namespace
 
 int solve_fem(rsd_ctx* ctx, rsd_heat* h, double coef, const rsd_solver_cfg* cfg, const double* b, double* x,
-              rsd_report* rep) {
+              rsd_report* rep, int which, const double* state) {
 	if (!ctx || !h || !cfg || (h->n && (!b || !x))) return set_error(RSD_EINVAL, "null argument");
 	if (cfg->max_iters < 0 || !(cfg->tol >= 0)) return set_error(RSD_EINVAL, "bad solver configuration");
 	if (cfg->type != RSD_CG && cfg->type != RSD_GMRES) return set_error(RSD_EINVAL, "unknown solver type");
@@ -1304,10 +1307,10 @@ int solve_fem(rsd_ctx* ctx, rsd_heat* h, double coef, const rsd_solver_cfg* cfg,
 	if (h->n == 0) { if (rep) rep->converged = 1; return RSD_OK; }
 	RSD_CUDA(cudaSetDevice(ctx->device));
 	if (cfg->type == RSD_GMRES) {
-		GmFemOp op{ctx, h, coef, h->n};
+		GmFemOp op{ctx, h, coef, h->n, which, state};
 		return gmres_core<double>(ctx, op, cfg, b, x, rep);
 	}
-	return cg_fem(ctx, h, coef, cfg, b, x, rep);
+	return cg_fem(ctx, h, coef, cfg, b, x, rep, which, state);
 }
 
 int solve(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const double* b, double* x, rsd_report* rep) {

@@ -142,6 +142,12 @@ def fem():
     r.set_operator("fem")
     U, rep = r.steady(1, 1, 1e-10, 1000, 7)
     save("fem_steady_gmres7_q1_quad_16.npz", U=U, iterations=rep["iterations"], finalResidual=rep["finalResidual"])
+    # Newton + GMRES(30) + Jacobi with the Jacobian forms applied matrix-free (the Newton fixture's problem)
+    r = oracle.Reference(3, 2, 3, [3, 3, 3], [0, 0, 0], [1, 1, 1], [0, 1], bc_kind=0, bc_val={0: 0.0, 1: 1.0},
+                         src_kind=0, src_c=10.0, k_a=1.0, k_b=0.5)
+    r.set_operator("fem")
+    U, rep = r.newton(1e-10, 1e-10, 50, 1, 1, 1e-12, 1000, 30)
+    save("fem_newton_q2_hex_3.npz", U=U, iterations=rep["iterations"], finalResidual=rep["finalResidual"])
     # k(T) = 1 + 0.5 T in a linear stage: the operator's state is the solve's own iterate (the stage
     # binds its state to U, which the solver updates in place), so the operator changes as CG runs
     r = oracle.Reference(3, 2, 3, [3, 3, 2], [0, 0, 0], [1, 1, 1], [0, 1], bc_kind=0, bc_val={0: 0.0, 1: 1.0},

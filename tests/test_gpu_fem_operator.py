@@ -170,6 +170,30 @@ def test_gmres_over_the_operator_matches_reference(rsd, ctx):
     assert rep2["iterations"] == rep["iterations"] and relerr(U.download(), U2.download()) <= REL
 
 
+def test_newton_with_the_jacobian_applied_matches_reference(rsd, ctx):
+    # J = Diffusion + TangentDiffusion at the Newton state, never assembled; GMRES(30) + Jacobi from
+    # its element diagonal, against the reference's Newton with operator type fem
+    g = golden("fem_newton_q2_hex_3.npz")
+    h = make_heat(rsd, ctx, 3, 2, 3, [3, 3, 3], [0, 0, 0], [1, 1, 1], src_expr="10", k_expr="1 + 0.5*T", dk_expr="0.5",
+                  dirichlet={0: "0", 1: "1"})
+    U = ctx.array(h.n).zero()
+    cfg = rsd.SolverConfig.make(type=rsd.GMRES, precond=rsd.JACOBI, tol=1e-12, max_iters=1000, krylov_dim=30,
+                                operator_type=rsd.OP_FEM)
+    rep = h.newton(U, 1e-10, 1e-10, 50, cfg=cfg)
+    assert rep["converged"] and rep["iterations"] == g["iterations"]
+    assert relerr(U.download(), g["U"]) <= 1e-11
+    # the Jacobian product and diagonal against the assembled J = K + K_T
+    rng = np.random.default_rng(9)
+    Us = ctx.to_device(0.3 * rng.standard_normal(h.n))
+    h.assemble_matrix(1.0, 0.0, 1.0, 0.0, U=Us)
+    v = ctx.to_device(rng.standard_normal(h.n))
+    y1 = ctx.array(h.n)
+    h.K.spmv(v, y1)
+    y2 = ctx.array(h.n)
+    h.assemble_vector(10, y2, U=Us, operand=v)
+    assert relerr(y2.download(), y1.download()) <= REL
+
+
 def test_configurations_the_operator_does_not_take(rsd, ctx):
     h = make_heat(rsd, ctx, 2, 1, 2, [4, 4], [0, 0], [1, 1], src_expr="1", dirichlet={0: "0"})
     U, b = ctx.array(h.n).zero(), ctx.array(h.n).zero()
@@ -178,9 +202,7 @@ def test_configurations_the_operator_does_not_take(rsd, ctx):
             h.steady(U, cfg=fem_cfg(rsd, **kw))
         with pytest.raises(rsd.RsdError, match="RSD_EINVAL"):
             h.solve_fem(b, U, **dict(dict(type=rsd.CG, tol=1e-8), **kw))
-    # a matrix solve, the batched solver and Newton take the CSR operator only
+    # a matrix solve and the batched solver take the CSR operator only
     h.assemble_matrix(1.0, 0.0)
     with pytest.raises(rsd.RsdError, match="RSD_EINVAL"):
         rsd.solve(ctx, h.K, b, U, fem_cfg(rsd))
-    with pytest.raises(rsd.RsdError, match="RSD_EINVAL"):
-        h.newton(U, 1e-10, 1e-10, 5, cfg=fem_cfg(rsd))
