@@ -210,59 +210,67 @@ def ncu_traffic(kernel):
 
 
 # ---------------------------------------------------------------------------------------------
-# reference CPU path (oracle/_ref: the reference templates compiled unmodified), bounded sample
+# reference CPU path (oracle/_ref: the reference templates compiled unmodified) on the full workload
 # ---------------------------------------------------------------------------------------------
-def reference_sample(sample_size, nsteps, warmup):
+def reference_steps(S, nsteps):
+    """`nsteps` Backward-Euler steps of the S^3 workload from T0 through the reference's own
+    BackwardEulerStage + BackwardEulerRunner (oracle/_ref, one core: the reference is
+    single-threaded).  Returns the state after the last step, the per-step wall seconds of
+    runner.step() and of its linear solve, the CG iterations per step, and the seconds spent before
+    the first step (mesh, DOF map, CSR pattern, the stage's first matrix assembly in setDt)."""
     import oracle
     if not oracle.reference_available():
         return None
-    r = oracle.Reference(3, 1, 2, [sample_size] * 3, [0, 0, 0], [1, 1, 1], list(range(6)), bc_kind=0, rho=1.0, cp=1.0)
+    t0 = time.perf_counter()
+    r = oracle.Reference(3, 1, 2, [S] * 3, [0, 0, 0], [1, 1, 1], list(range(6)), bc_kind=0, rho=1.0, cp=1.0)
     # node coordinates from the oracle's block mesh (the reference's numbering): nothing of the
-    # device package runs on this arm
-    xyz = oracle.BlockMesh(3, [sample_size] * 3, [0, 0, 0], [1, 1, 1], 1).xyz
+    # device package runs on this path
+    xyz = oracle.BlockMesh(3, [S] * 3, [0, 0, 0], [1, 1, 1], 1).xyz
     t2a, a2t = r.dofmap()
     U0 = initial_condition(xyz, a2t)
-    _, _, rc, st = r.backward_euler(1e-3, warmup + nsteps, U0, tol=1e-8, maxit=100000, stats=True)
-    st = st[warmup:]
-    return {"n": r.n, "nnz": r.nnz, "elements": r.nelem, "step_s": st[:, 0], "solve_s": st[:, 1], "iters": st[:, 2], "rc": rc}
+    setup = time.perf_counter() - t0
+    t1 = time.perf_counter()
+    U, _, rc, st = r.backward_euler(1e-3, nsteps, U0, tol=1e-8, maxit=100000, stats=True)
+    total = time.perf_counter() - t1
+    return {"U": U, "U0": U0, "n": r.n, "nnz": r.nnz, "elements": r.nelem, "rc": rc, "step_s": st[:, 0],
+            "solve_s": st[:, 1], "iters": st[:, 2], "setup_s": setup + total - float(st[:, 0].sum())}
 
 
-def extrapolate(ref, n_elem, nnz, iters):
-    """Scale a reference sample to the full workload: element loops by the element count, the CG
-    solve by nnz x iterations (the reference runs the same CG as the device FP64 path, so the
-    device's FP64 iteration count is the reference's at full size)."""
-    step = float(np.median(ref["step_s"]))
-    solve = float(np.median(ref["solve_s"]))
-    it = float(np.median(ref["iters"]))
-    loops = (step - solve) * (n_elem / ref["elements"])
-    cg = solve * (nnz / ref["nnz"]) * (iters / max(it, 1.0))
-    return 1e3 * (loops + cg), step * 1e3
+def reference_config(S):
+    """The workload description both arms print (the reference arm computes the sizes itself)."""
+    n, nnz = (S - 1) ** 3, (3 * S - 5) ** 3
+    return {"workload": WORKLOAD.format(S=S), "n_free": n, "nnz": nnz, "elements": S ** 3, "parallelism": "replicas",
+            "l2": "inputs larger than L2 (CSR FP64 values + columns %.2f GB)" % (nnz * 12 / 1e9)}
 
 
 def run_reference_arm(args, rank, world):
+    """bench.py --impl reference: the reference's own Backward-Euler steps on the same 128^3 workload,
+    timed on the host (one core), `--ref-steps` of them (each about half a minute) so that the arm
+    ends within a few minutes whatever --steps asks for; the steps timed are the line's `steps`."""
     if rank != 0:
         return
+    S = args.size
+    nsteps = max(1, min(args.steps, args.ref_steps))
     try:
         import oracle
         if not oracle.reference_available():
             print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libresiduum_ref.so not built (reference tree absent at build time)"}))
             return
-        ref = reference_sample(args.cpu_sample, args.steps, args.warmup)
+        ref = reference_steps(S, nsteps)
     except Exception as e:  # noqa: BLE001
-        print(json.dumps({"impl": "reference", "unavailable": f"reference sample failed: {e}"}))
+        print(json.dumps({"impl": "reference", "unavailable": f"reference run failed: {e}"}))
         return
-    # without the device run at hand, scale CG by nnz and by the sample's own iteration growth
-    # (iterations ~ h^-1 for BE-preconditioned CG at fixed dt: a documented estimate)
-    S = args.size
-    n_elem, nnz = S ** 3, (3 * S - 5) ** 3
-    iters = float(np.median(ref["iters"])) * (S / args.cpu_sample)
-    ms, sample_ms = extrapolate(ref, n_elem, nnz, iters)
-    line = {"impl": "reference", "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD.format(S=S), "parallelism": "replicas"},
-            "cpu_baseline": {"value": ms, "unit": "ms", "cores": 1, "kind": "reference",
-                             "sample": f"{args.steps} Backward-Euler steps of the {args.cpu_sample}^3 problem through the reference templates (oracle/_ref), median {sample_ms:.0f} ms per step, scaled to {S}^3: element loops by elements, CG by nnz x iterations"},
+    ms = 1e3 * float(np.median(ref["step_s"]))
+    sample = (f"{nsteps} Backward-Euler step(s) of the {S}^3 workload from T0 (dt = 1e-3, FP64 CG + Jacobi to 1e-8) "
+              f"through the reference templates (oracle/_ref: BackwardEulerStage + BackwardEulerRunner::step), 1 core, "
+              f"median of runner.step() wall times; CG iterations {[int(i) for i in ref['iters']]}; "
+              f"setup before the first step {ref['setup_s']:.1f} s untimed")
+    line = {"impl": "reference", "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": world, "steps": nsteps,
+            "warmup": 0, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "config": reference_config(S),
+            "requested": {"steps": args.steps, "warmup": args.warmup},
+            "step_ms": [1e3 * float(t) for t in ref["step_s"]], "solve_ms": [1e3 * float(t) for t in ref["solve_s"]],
+            "cpu_baseline": {"value": ms, "unit": "ms", "cores": 1, "kind": "reference", "sample": sample},
             "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -714,7 +722,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--size", type=int, default=128)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cpu-sample", type=int, default=48)
+    ap.add_argument("--ref-steps", type=int, default=2, help="reference Backward-Euler steps the reference arm times")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--reliable-delta", type=float, default=0.0)
     ap.add_argument("--batch", type=int, default=256, help="problems in the batched workload (0: skip it)")
@@ -946,39 +954,88 @@ def main():
     # residual), with one idle body and replacement node after the converged one
     gpu_launches = int(sum(8 + 2 * (r["iterations"] + 1) + 2 * (r["refinements"] + 1) for r in reps_mx))
 
+    # the reference's own first step of the same workload (one core), timed on the host, and parity
+    # at the configured size: the device's first step from T0 in FP64 and mixed precision against it
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu:
+        first = {}
+        for key in ("fp64", "mixed"):
+            U.upload(U0); Up.upload(U0)
+            heat.set_time(0.0)
+            rep1 = heat.be_step(dt, U, Up, cfgs[key])
+            first[key] = (U.download(), rep1)
         try:
-            ref = reference_sample(args.cpu_sample, 2, 1)
+            ref = reference_steps(S, 1)
             if ref is not None:
-                est, sample_ms = extrapolate(ref, S ** 3, nnz, float(np.median(it_64)))
-                cpu = {"value": est, "unit": "ms", "cores": 1, "kind": "reference",
-                       "sample": (f"2 Backward-Euler steps (after 1 warm-up) of the {args.cpu_sample}^3 problem through the "
-                                  f"reference templates (oracle/_ref), median {sample_ms:.0f} ms per step; scaled to {S}^3 "
-                                  f"by elements for the element loops and by nnz x the device FP64 iteration count for CG")}
+                step_ms = 1e3 * float(ref["step_s"][0])
+                cpu = {"value": step_ms, "unit": "ms", "cores": 1, "kind": "reference",
+                       "sample": (f"the first Backward-Euler step of the {S}^3 workload from T0 through the reference "
+                                  f"templates (oracle/_ref: BackwardEulerRunner::step), 1 core; its linear solve "
+                                  f"{1e3 * float(ref['solve_s'][0]):.0f} ms, {int(ref['iters'][0])} CG iterations; setup before "
+                                  f"the step {ref['setup_s']:.1f} s untimed")}
+                uref = ref["U"]
+                scale = float(np.max(np.abs(uref)))
+                parity = {"reference_iterations": int(ref["iters"][0]),
+                          "initial_state_identical": bool(np.array_equal(ref["U0"], U0)),
+                          "how": "one step from T0, the device's state against the reference's state after its first step, max |diff| / max |ref|"}
+                for key in ("fp64", "mixed"):
+                    ud, rp = first[key]
+                    parity[key] = {"max_rel_diff_vs_reference": float(np.max(np.abs(ud - uref))) / scale,
+                                   "iterations": int(rp["iterations"]), "true_residual_rel": rp["trueResidualRel"]}
+                parity["fp64"]["iterations_equal"] = parity["fp64"]["iterations"] == parity["reference_iterations"]
         except Exception as e:  # noqa: BLE001
             cpu = {"value": None, "unit": "ms", "cores": 1, "kind": "reference", "sample": f"failed: {e}"}
 
-    # element assembly roofline of K + M/dt (bytes and flops as the path's roofline counts them): bytes = CSR values written
-    # once + coordinates + connectivity, flops = E nq npe^2 (2d + 2) diffusion + E nq npe^2 3 mass,
-    # against the measured HBM copy peak and the measured FP64 FMA rate; the bound that binds is the
-    # larger time
+    # element assembly roofline of K + M/dt.  The all-affine row-gather kernel (k_asm_matrix_rows) forms
+    # each entry from the reference-element integrals: per (element, row a, column b) NT + 1 = 7
+    # multiply-adds and one more add (3D), E npe^2 17 flops, so it is HBM-bound.  Its bytes: the SELL
+    # values written once in FP64 and in FP32 (slots x 12), per (element, row) the adjacency entry (4)
+    # and the column-rank record (8), per element the geometry record (64), the row pointers (n x 4).
+    # The path's own byte count (CSR values + coordinates + connectivity) is given beside it.
     import ctypes
     fp64 = ctypes.c_double()
     rsd.check(rsd.lib().rsd_measure_fp64_rate(ctx.h, ctypes.byref(fp64)))
     n_elem, n_nodes = S ** 3, (S + 1) ** 3
-    asm_bytes = nnz * 8 + n_nodes * 3 * 8 + n_elem * 8 * 4
-    asm_flops = n_elem * 8 * 64 * (2 * 3 + 2 + 3)
+    lay = heat.K.layout()
+    slots = lay["sell_slots"]
+    asm_bytes = slots * 12 + n_elem * 8 * (4 + 8) + n_elem * 64 + 4 * n
+    path_bytes = nnz * 8 + n_nodes * 3 * 8 + n_elem * 8 * 4
+    asm_flops = n_elem * 64 * 17
     t_hbm = asm_bytes / (peak * 1e9) * 1e3
     t_fp64 = asm_flops / (fp64.value * 1e12) * 1e3
     asm_ms = prof_mx["assemble_matrix"][1] / max(prof_mx["assemble_matrix"][0], 1) if "assemble_matrix" in prof_mx else None
-    asm_roof = {"kernel": "k_asm_matrix_rows (K + M/dt, one launch per step)", "bytes": asm_bytes, "flops": asm_flops,
-                "hbm_ms": t_hbm, "fp64_ms": t_fp64, "bound": "fp64" if t_fp64 > t_hbm else "hbm",
-                "roofline_ms": max(t_hbm, t_fp64), "achieved_ms": asm_ms,
-                "frac": max(t_hbm, t_fp64) / asm_ms if asm_ms else None,
-                "fp64_tflops": fp64.value, "fp64_peak_kind": "measured (FMA chains, rsd_measure_fp64_rate)",
-                "note": "flops as the quadrature form counts them; affine elements take the same integrals from "
-                        "reference-element tables with about a tenth of those flops"}
+    asm_roof = {"kernel": "k_asm_matrix_rows (K + M/dt with its FP32 copy, one launch per step)", "bound": "hbm",
+                "bytes": asm_bytes, "flops": asm_flops, "hbm_ms": t_hbm, "fp64_ms": t_fp64,
+                "achieved_ms": asm_ms, "achieved_gbs": asm_bytes / (asm_ms * 1e6) if asm_ms else None,
+                "frac": t_hbm / asm_ms if asm_ms else None, "peak_gbs": peak, "peak_kind": peak_kind,
+                "path_bytes": path_bytes, "fp64_tflops": fp64.value, "layout": lay,
+                "note": "frac = kernel bytes / measured HBM copy peak / event-timed duration; the executed flops "
+                        "(reference-element integrals) need 3% of the duration at the measured FP64 rate"}
+
+    # the dominant kernel's roofline on the bytes it moves: DRAM traffic per launch from the ncu
+    # capture of this workload (dram__bytes_read.sum + dram__bytes_write.sum) over the event-timed
+    # average launch.  The path's algorithmic byte count charges 4-byte column indices, which the
+    # stencil-slice layout does not read, and a gathered vector that stays in L2: its figure is kept
+    # beside it as an equivalent rate, not as a fraction of the HBM roofline.
+    if traffic and avg_ms:
+        achieved_dram = traffic / (avg_ms * 1e6)
+    else:
+        achieved_dram = None
+    roofline = {"kernel": "k_mx_spmv_dot (FP32 SELL-32 SpMV + z.w)", "bound": "hbm",
+                "achieved": achieved_dram, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                "frac": achieved_dram / peak if achieved_dram else None,
+                "frac_nominal_8tbs": achieved_dram / 8000.0 if achieved_dram else None,
+                "traffic": traffic, "avg_launch_us": avg_ms * 1e3, "launches": launches,
+                "algorithmic_bytes": bytes_spmv32, "algorithmic_equiv_gbs": achieved,
+                "algorithmic_equiv_frac": achieved / peak if achieved else None,
+                "note": "achieved = ncu DRAM bytes per launch / CUDA-event average launch time on the solve stream",
+                "fp64_spmv": {"kernel": "k_cg_spmv_dot", "traffic": ncu_traffic("k_cg_spmv_dot"),
+                              "avg_launch_us": 1e3 * t64 / max(l64, 1),
+                              "achieved": (ncu_traffic("k_cg_spmv_dot") / (t64 / max(l64, 1) * 1e6)) if ncu_traffic("k_cg_spmv_dot") and l64 else None,
+                              "algorithmic_bytes": bytes_spmv64, "algorithmic_equiv_gbs": achieved64}}
+    if roofline["fp64_spmv"]["achieved"]:
+        roofline["fp64_spmv"]["frac"] = roofline["fp64_spmv"]["achieved"] / peak
 
     line = {
         "metric": METRIC, "value": ms_mx, "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -996,14 +1053,7 @@ def main():
         "iterations": {"mixed": it_mx, "fp64": it_64},
         "reliable_updates": [r["refinements"] for r in reps_mx],
         "true_residual_rel": {"mixed": max(r["trueResidualRel"] for r in reps_mx), "fp64": max(r["trueResidualRel"] for r in reps_64)},
-        "roofline": {"kernel": "k_mx_spmv_dot (FP32 CSR SpMV + p.Ap)", "bound": "hbm", "achieved": achieved, "peak": peak,
-                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak if achieved else None,
-                     "frac_nominal_8tbs": achieved / 8000.0 if achieved else None, "algorithmic_bytes": bytes_spmv32,
-                     "avg_launch_us": avg_ms * 1e3, "launches": launches, "traffic": traffic,
-                     "traffic_gbs": traffic / (avg_ms * 1e6) if traffic and avg_ms else None,
-                     "traffic_frac": traffic / (avg_ms * 1e6) / peak if traffic and avg_ms else None,
-                     "fp64_spmv": {"achieved": achieved64, "frac": achieved64 / peak if achieved64 else None,
-                                   "algorithmic_bytes": bytes_spmv64, "avg_launch_us": 1e3 * t64 / max(l64, 1)}},
+        "roofline": roofline,
         "assembly_roofline": asm_roof,
         "kernel_ms_per_step": {k: v[1] / args.steps for k, v in prof_mx.items()},
         "kernel_ms_per_step_fp64": {k: v[1] / args.steps for k, v in prof_64.items()},
@@ -1014,6 +1064,7 @@ def main():
         "fem_operator": fem_op,
         "adjoint": adjoint,
         "cpu_baseline": cpu,
+        "parity_at_size": parity,
         "e2e": {"value": ms_e2e, "unit": "ms", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
         "gpu_launches": gpu_launches,
         "clocks": clk,

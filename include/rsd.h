@@ -96,6 +96,12 @@ int rsd_ctx_profile_get(rsd_ctx* ctx, const char* family, int64_t* launches, dou
 /* ---- memory: CUDA::alloc / copy / zero / set (linalg/types/backend/CUDA.hpp:30-71) ---- */
 int rsd_alloc(rsd_ctx* ctx, size_t bytes, void** dptr);
 int rsd_free(rsd_ctx* ctx, void* dptr);
+/* Device memory that host code may also read (managed memory, resident on the device): the backend
+ * tag's vectors use it because the reference's NewtonRunner reads the stage residual's entries on the
+ * host (solver/nonlinear/Newton.hpp:45, fem/dof/DOFResidualNorms.hpp:13-24); read it only after the
+ * context's stream has finished with it.  Freed with rsd_free.  No counterpart in the reference's
+ * CUDA tag, which allocates with cudaMalloc (linalg/types/backend/CUDA.hpp:30-37). */
+int rsd_alloc_managed(rsd_ctx* ctx, size_t bytes, void** dptr);
 int rsd_memcpy(rsd_ctx* ctx, void* dst, const void* src, size_t bytes, int32_t kind);
 int rsd_memset_zero(rsd_ctx* ctx, void* dptr, size_t bytes);
 int rsd_fill_f64(rsd_ctx* ctx, double* x, int64_t n, double value);
@@ -118,6 +124,10 @@ int rsd_csr_create(rsd_ctx* ctx, int64_t nrows, int64_t nnz, const int64_t* row_
                    const double* values, rsd_csr** out);
 int rsd_csr_destroy(rsd_csr* A);
 int rsd_csr_info(const rsd_csr* A, int64_t* nrows, int64_t* nnz);
+/* The execution layout's size (no counterpart in the reference, whose CSR has one layout): SELL-32
+ * slots (entries including padding), slices of 32 rows, and the slices stored as stencil slices
+ * (no column indices); any output may be NULL. */
+int rsd_csr_layout(const rsd_csr* A, int64_t* sell_slots, int64_t* slices, int64_t* stencil_slices);
 /* device pointer to the CSR-order values (writes through it are allowed until the next call on A) */
 int rsd_csr_values(rsd_ctx* ctx, rsd_csr* A, double** dvalues);
 int rsd_csr_set_values(rsd_ctx* ctx, rsd_csr* A, const double* host_values);
@@ -175,9 +185,24 @@ typedef struct rsd_heat_desc {
 	const char* k_expr;              /* k(T), or NULL */
 	const char* dk_expr;             /* dk/dT(T), or NULL (0) */
 	const double* k_elem;            /* host, one multiplier per element, or NULL */
-	double rho, cp;                  /* density, specific heat */
+	double rho, cp;                  /* density, specific heat (cp when cp_expr is NULL) */
 	const char* src_expr;            /* volumetric source f(t,x,y,z), or NULL (0) */
-	const char* dirichlet_expr[6];   /* Dirichlet value per boundary tag; NULL = tag not essential */
+	const char* dirichlet_expr[6];   /* Dirichlet value per boundary tag 0..5; NULL = tag not essential */
+	/* ConductivityModel (equation/heateq/evaluator/ConductivityModel.hpp:60-96) with an anisotropic
+	 * shape: K = k * k_tensor, k being k_const or k(T) (set k_const = 1 for the reference's constant
+	 * Anisotropic type); host, nsd x nsd row-major, or NULL for the isotropic K = k I */
+	const double* k_tensor;
+	/* SpecificHeatModel (equation/heateq/evaluator/SpecificHeatModel.hpp:35-61), TemperatureDependent:
+	 * cp(T) and dcp/dT(T) (the latter feeds TangentMassForm), or NULL for the constant cp */
+	const char* cp_expr;
+	const char* dcp_expr;
+	/* further essential tags of any value >= 0 (EssentialBoundaryRegistry takes any tag,
+	 * fem/boundary/EssentialBoundaryRegistry.hpp:15-59): num_dirichlet pairs of a tag and its
+	 * Dirichlet expression, registered after the dirichlet_expr entries (a tag given twice keeps the
+	 * later expression) */
+	int32_t num_dirichlet;
+	const int32_t* dirichlet_tags;
+	const char* const* dirichlet_exprs;
 } rsd_heat_desc;
 
 /* constructor + TopologicalDOF::buildConstraints + Assembler::createMatrix
@@ -187,6 +212,13 @@ int rsd_heat_destroy(rsd_heat* h);
 int rsd_heat_info(const rsd_heat* h, int64_t* num_free, int64_t* nnz);
 int rsd_heat_dofmap(rsd_ctx* ctx, const rsd_heat* h, int32_t* host_topo_to_alg, int32_t* host_alg_to_topo);
 int rsd_heat_matrix(rsd_heat* h, rsd_csr** A);       /* the problem's K/J storage (owned by h) */
+/* HeatProblem::createMatrix (HeatProblem.hpp:62, Assembler::createMatrix): a new matrix with h's
+ * pattern, sharing h's pattern arrays, with zero values of its own; destroy it with rsd_csr_destroy
+ * before h. */
+int rsd_heat_create_matrix(rsd_ctx* ctx, rsd_heat* h, rsd_csr** A);
+/* HeatProblem::loadNodalField, Expression mode (HeatProblem.tpp:185-205): U[free dof of node v] =
+ * expr(t, x_v, y_v, z_v) for every free node (the initial condition); U device, num_free entries */
+int rsd_heat_eval_nodal(rsd_ctx* ctx, rsd_heat* h, const char* expr, double t, double* U);
 int rsd_heat_set_time(rsd_ctx* ctx, rsd_heat* h, double t);   /* re-evaluates Dirichlet node values */
 int rsd_heat_set_k_elem(rsd_ctx* ctx, rsd_heat* h, const double* k_elem_device);
 
@@ -210,8 +242,16 @@ int rsd_assemble_vector(rsd_ctx* ctx, rsd_heat* h, int32_t which, double coef, c
  * operator_type is not read.  b, x device vectors of num_free entries; x holds the initial guess. */
 int rsd_heat_solve_fem(rsd_ctx* ctx, rsd_heat* h, double c_mass, const rsd_solver_cfg* cfg, const double* b, double* x,
                        rsd_report* report);
+/* The LinearSolverRunner HeatProblem::makeLinearRunner builds for OperatorType::FEM with any of the
+ * stages' form compositions (SteadyStage.hpp:37, BackwardEulerStage.hpp:43-46): Diffusion
+ * + c_tdiff TangentDiffusion + c_mass Mass + c_tmass TangentMass, models at the state U (Full gather)
+ * and the rate Udot (TangentMass); U NULL or U == x binds the state to the iterate, as the linear
+ * stages do.  Jacobi from the same forms' element diagonal.  cfg as for rsd_heat_solve_fem. */
+int rsd_heat_solve_fem_forms(rsd_ctx* ctx, rsd_heat* h, double c_tdiff, double c_mass, double c_tmass, const double* U,
+                             const double* Udot, const rsd_solver_cfg* cfg, const double* b, double* x, rsd_report* report);
 /* A flux boundary condition given by one expression per spatial component, q(t, x, y, z), on a
- * boundary tag (HeatProblem.tpp:98-105, FluxBoundaryForm); flux_expr NULL clears the tag's flux.
+ * boundary tag of any value >= 0 (HeatProblem.tpp:98-105, FluxBoundaryForm); flux_expr NULL clears
+ * the tag's flux.
  * The stages then add its integrals to the right-hand side as HeatProblem::applyNatural does. */
 int rsd_heat_set_flux(rsd_ctx* ctx, rsd_heat* h, int32_t tag, const char* const* flux_expr);
 /* BoundaryApplicator::applyNaturalBCs (fem/boundary/backend/cpu/BoundaryApplicator.tpp:66-140) at the

@@ -14,7 +14,8 @@
 //     reference's CPU and CUDA tags (linalg/types/backend/CPU.hpp:15-40, CUDA.hpp:23-73), on one
 //     process-wide rsd context (device 0 unless B200::use() names another);
 //   * CSRMatrix<T, B200>: a device CSR matrix (an rsd_csr: 32-bit indices, SELL-32 execution layout),
-//     built from the reference's host CSRMatrix<T, CPU> (linalg/types/CSRMatrix.hpp:14-88);
+//     built from the reference's host CSRMatrix<T, CPU> (linalg/types/CSRMatrix.hpp:14-88) or taken
+//     over from the C ABI (the heat problem's createMatrix);
 //   * explicit specializations of operations::dot/axpy/axpby/scal/copy/multiply/norm
 //     (linalg/operations/VectorOps.hpp:10-36) and operations::matvec/lump (MatrixOps.hpp:10-16) for
 //     the tag's vector and matrix;
@@ -22,6 +23,7 @@
 //     Jacobi<Vector<double, B200>> (linalg/solver/preconditioner/Jacobi.hpp:15-50), whose reference
 //     versions read matrix entries on the host.
 // Errors throw std::runtime_error with the library's message, as the reference's CUDA tag throws.
+// The heat problem itself on the tag is in rsd_residuum_heat.hpp.
 #pragma once
 
 #include <memory>
@@ -66,10 +68,13 @@ public:
 	template <typename T>
 	using Ptr = std::unique_ptr<T, Deleter<T>>;
 
+	// vectors live in device-resident managed memory: the reference's NewtonRunner reads the stage
+	// residual's entries on the host (solver/nonlinear/Newton.hpp:45), which plain device memory
+	// would not allow; kernels see ordinary device memory
 	template <typename T>
 	static Ptr<T> alloc(Index n) {
 		void* p = nullptr;
-		check(rsd_alloc(ctx(), sizeof(T) * (n ? n : 1), &p));
+		check(rsd_alloc_managed(ctx(), sizeof(T) * (n ? n : 1), &p));
 		return Ptr<T>(static_cast<T*>(p));
 	}
 	template <typename T>
@@ -107,6 +112,16 @@ public:
 	using value_type = T;
 	using backend_type = rsd::residuum::B200;
 
+	// an empty matrix (the stages' MatrixT(0, 0) when no matrix is assembled)
+	CSRMatrix(Index nRows, Index nCols) : nRows_(nRows), nCols_(nCols) {}
+	// takes ownership of a device matrix from the C ABI (rsd_heat_create_matrix, rsd_csr_create)
+	explicit CSRMatrix(rsd_csr* A) {
+		int64_t n = 0, nnz = 0;
+		rsd::residuum::check(rsd_csr_info(A, &n, &nnz));
+		nRows_ = nCols_ = (Index)n;
+		nNnz_ = (Index)nnz;
+		A_.reset(A);
+	}
 	explicit CSRMatrix(const CSRMatrix<T, backend::CPU>& host) : nRows_(host.nRows()), nCols_(host.nCols()) {
 		const Index nnz = host.rowPtr()[nRows_];
 		std::vector<int64_t> rp(nRows_ + 1), col(nnz ? nnz : 1);

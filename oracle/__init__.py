@@ -25,11 +25,17 @@ _I32 = C.c_int32
 _I64 = C.c_int64
 
 
-def build(ref_root="/root/reference"):
-    """Compile the restatement and, when the reference checkout exists, the reference harness."""
-    env = dict(os.environ)
-    targets = ["all"] if os.path.isdir(ref_root) else [os.path.join(HERE, "_build", "librsd_oracle.so")]
-    subprocess.run(["make", "-s", "-C", HERE, "REF=" + ref_root] + targets, check=True, env=env)
+def build(ref_root=None):
+    """Compile the restatement and, when `ref_root` names the reference checkout, the reference
+    harness from the sources there."""
+    targets = ["all"]
+    args = []
+    if ref_root:
+        if not os.path.isdir(ref_root):
+            raise FileNotFoundError(f"reference checkout {ref_root!r} does not exist")
+        targets.append("ref")
+        args.append("REF=" + ref_root)
+    subprocess.run(["make", "-s", "-C", HERE] + args + targets, check=True)
 
 
 def _ptr(a):
@@ -462,3 +468,165 @@ def ref_csr_solve(rowPtr, col, val, b, x0=None, solver=0, precond=1, tol=1e-10, 
     ref_lib().ref_csr_solve(solver, precond, n, _ptr(rowPtr), _ptr(col), _ptr(_f64(val)), _ptr(_f64(b)), _ptr(x),
                             tol, maxit, krylov, C.byref(rep))
     return x, rep.as_dict()
+
+
+# ---------------------------------------------------------------------------------------------
+# the reference's application layer (ref_problem.cpp): HeatProblem<CPU, HeatEquation> from a config
+# ---------------------------------------------------------------------------------------------
+class _RefpDesc(C.Structure):
+    _fields_ = [("nsd", _I32), ("order", _I32), ("nq", _I32), ("nel", _I32 * 3), ("lo", _D * 3), ("hi", _D * 3),
+                ("tag_map", _I32 * 6), ("k_type", _I32), ("k_value", _D), ("k_tensor", _D * 9),
+                ("k_expr", C.c_char_p), ("dk_expr", C.c_char_p), ("rho", _D), ("cp_type", _I32), ("cp_value", _D),
+                ("cp_expr", C.c_char_p), ("dcp_expr", C.c_char_p), ("source", C.c_char_p), ("initial", C.c_char_p),
+                ("nbc", _I32), ("bc_tag", _I32 * 16), ("bc_flux", _I32 * 16), ("bc_expr", (C.c_char_p * 3) * 16),
+                ("transient", _I32), ("nonlinear", _I32), ("nl_abs", _D), ("nl_rel", _D), ("nl_maxit", _I64),
+                ("lin_type", _I32), ("precond", _I32), ("op_type", _I32), ("lin_tol", _D), ("lin_maxit", _I64),
+                ("krylov", _I64), ("t0", _D), ("tf", _D), ("dt", _D)]
+
+
+_refp_bound = False
+
+
+def _refp_lib():
+    global _refp_bound
+    L = ref_lib()
+    if not _refp_bound:
+        L.refp_create.argtypes = [C.POINTER(_RefpDesc)]; L.refp_create.restype = _P
+        L.refp_destroy.argtypes = [_P]
+        L.refp_last_error.restype = C.c_char_p
+        L.refp_num_free.argtypes = [_P]; L.refp_num_free.restype = _I64
+        L.refp_num_nodes.argtypes = [_P]; L.refp_num_nodes.restype = _I64
+        L.refp_nnz.argtypes = [_P]; L.refp_nnz.restype = _I64
+        L.refp_mesh.argtypes = [_P, _P, _P]
+        L.refp_dofmap.argtypes = [_P, _P]
+        L.refp_run.argtypes = [_P, _P]
+        L.refp_pattern.argtypes = [_P, _P, _P]
+        L.refp_assemble_matrix.argtypes = [_P, C.c_int, _D, _D, _P, _P, _P]
+        L.refp_assemble_vector.argtypes = [_P, C.c_int, _D, _P, _P, _P]
+        _refp_bound = True
+    return L
+
+
+class RefProblem:
+    """The reference's HeatProblem<CPU, HeatEquation<nsd, nsd, Quad|Hex>> on a block mesh, built from
+    a HeatConfig with its own models, and solved by its own stages and drivers.
+
+    conductivity: ("constant", k) | ("anisotropic", tensor) | ("k(T)", k_expr, dk_expr)
+                  | ("k(T) tensor", tensor, k_expr, dk_expr)
+    specific_heat: ("constant", cp) | ("cp(T)", cp_expr, dcp_expr)   (transient runs only)
+    bcs: list of (tag, "value", expr) or (tag, "flux", [expr per component])
+    tag_map: {block tag: new tag} renumbers the block mesh's boundary tags
+    solver: dict(type "cg"|"gmres", precond "jacobi"|"identity", operator "csr"|"fem", tol, maxit, krylov,
+                 newton=(abs, rel, maxit) or None, transient=(t0, tf, dt) or None)
+    """
+
+    def __init__(self, nsd, order, nq, nel, lo, hi, conductivity=("constant", 1.0), rho=1.0,
+                 specific_heat=("constant", 1.0), source="0", initial="0", bcs=(), tag_map=None, solver=None):
+        L = _refp_lib()
+        d = _RefpDesc()
+        self._keep = []
+
+        def s(x):
+            if x is None:
+                return None
+            b = x.encode()
+            self._keep.append(b)
+            return b
+        d.nsd, d.order, d.nq = nsd, order, nq
+        nel = list(nel) + [1] * (3 - len(nel))
+        for i in range(3):
+            d.nel[i] = nel[i]
+        for i in range(nsd):
+            d.lo[i], d.hi[i] = lo[i], hi[i]
+        for t in range(6):
+            d.tag_map[t] = (tag_map or {}).get(t, -1)
+        kind = conductivity[0]
+        d.k_type = {"constant": 0, "anisotropic": 1, "k(T)": 2, "k(T) tensor": 3}[kind]
+        if kind == "constant":
+            d.k_value = conductivity[1]
+        if kind in ("anisotropic", "k(T) tensor"):
+            t = np.asarray(conductivity[1], dtype=np.float64).reshape(nsd, nsd)
+            for i in range(nsd * nsd):
+                d.k_tensor[i] = t.flat[i]
+        if kind in ("k(T)", "k(T) tensor"):
+            d.k_expr, d.dk_expr = s(conductivity[-2]), s(conductivity[-1])
+        d.rho = rho
+        if specific_heat[0] == "constant":
+            d.cp_type, d.cp_value = 0, specific_heat[1]
+        else:
+            d.cp_type, d.cp_expr, d.dcp_expr = 1, s(specific_heat[1]), s(specific_heat[2])
+        d.source, d.initial = s(source), s(initial)
+        d.nbc = len(bcs)
+        for b, (tag, kind, ex) in enumerate(bcs):
+            d.bc_tag[b] = tag
+            d.bc_flux[b] = 1 if kind == "flux" else 0
+            exprs = [ex] if kind != "flux" else list(ex)
+            for i, e in enumerate(exprs):
+                d.bc_expr[b][i] = s(e)
+        sv = dict(type="cg", precond="jacobi", operator="csr", tol=1e-10, maxit=1000, krylov=30, newton=None, transient=None)
+        sv.update(solver or {})
+        d.lin_type = 1 if sv["type"] == "gmres" else 0
+        d.precond = 1 if sv["precond"] == "jacobi" else 0
+        d.op_type = 1 if sv["operator"] == "fem" else 0
+        d.lin_tol, d.lin_maxit, d.krylov = sv["tol"], sv["maxit"], sv["krylov"]
+        if sv["newton"]:
+            d.nonlinear = 1
+            d.nl_abs, d.nl_rel, d.nl_maxit = sv["newton"]
+        if sv["transient"]:
+            d.transient = 1
+            d.t0, d.tf, d.dt = sv["transient"]
+        self.nsd = nsd
+        self.h = L.refp_create(C.byref(d))
+        if not self.h:
+            raise ValueError(L.refp_last_error().decode())
+        self.n = L.refp_num_free(self.h)
+        self.nnodes = L.refp_num_nodes(self.h)
+
+    def __del__(self):
+        try:
+            _refp_lib().refp_destroy(self.h)
+        except Exception:
+            pass
+
+    def mesh(self, nelem, nfaces):
+        xyz = np.zeros(self.nnodes * self.nsd)
+        rng = np.zeros(nelem * nfaces, np.int32)
+        _refp_lib().refp_mesh(self.h, _ptr(xyz), _ptr(rng))
+        return xyz, rng
+
+    def dofmap(self):
+        t2a = np.zeros(self.nnodes, np.int32)
+        _refp_lib().refp_dofmap(self.h, _ptr(t2a))
+        return t2a
+
+    def run(self):
+        """The configured solve from the configured initial condition: (U over the free DOFs, converged)."""
+        U = np.zeros(self.n)
+        rc = _refp_lib().refp_run(self.h, _ptr(U))
+        if rc < 0:
+            raise RuntimeError(_refp_lib().refp_last_error().decode())
+        return U, rc == 0
+
+    def pattern(self):
+        L = _refp_lib()
+        nnz = L.refp_nnz(self.h)
+        rp = np.zeros(self.n + 1, np.int64)
+        col = np.zeros(max(nnz, 1), np.int64)
+        L.refp_pattern(self.h, _ptr(rp), _ptr(col))
+        return rp, col[:nnz]
+
+    def assemble_matrix(self, formset, c=0.0, t=0.0, U=None, Udot=None):
+        """formset 0 K; 1 K + c M; 2 K + K_T; 3 K + K_T + c M + M_T, with the problem's models."""
+        L = _refp_lib()
+        val = np.zeros(max(L.refp_nnz(self.h), 1))
+        if L.refp_assemble_matrix(self.h, formset, c, t, _ptr(_f64(U)), _ptr(_f64(Udot)), _ptr(val)):
+            raise RuntimeError(L.refp_last_error().decode())
+        return val[:L.refp_nnz(self.h)]
+
+    def assemble_vector(self, which, t=0.0, U=None, Udot=None):
+        """which 0: load + natural BCs at t; 1: stiffness residual K(U) U (Full gather); 2: mass forms on Udot."""
+        L = _refp_lib()
+        out = np.zeros(self.n)
+        if L.refp_assemble_vector(self.h, which, t, _ptr(_f64(U)), _ptr(_f64(Udot)), _ptr(out)):
+            raise RuntimeError(L.refp_last_error().decode())
+        return out

@@ -2,7 +2,7 @@
 hot path (declared in include/rsd.h).
 
 This is the binding a Python caller (tests, bench.py, a PyTorch autograd wrapper) uses; C++ callers
-use the header layer in residuum_cuda/.  There is no CPU fallback: every call goes to the CUDA
+use the backend tag in include/rsd_residuum.hpp.  There is no CPU fallback: every call goes to the CUDA
 library, and importing raises if the library is missing.
 """
 import ctypes as C
@@ -54,7 +54,9 @@ class SolverConfig(C.Structure):
 
 class HeatDesc(C.Structure):
     _fields_ = [("nq", _I32), ("k_const", _D), ("k_expr", C.c_char_p), ("dk_expr", C.c_char_p), ("k_elem", _P),
-                ("rho", _D), ("cp", _D), ("src_expr", C.c_char_p), ("dirichlet_expr", C.c_char_p * 6)]
+                ("rho", _D), ("cp", _D), ("src_expr", C.c_char_p), ("dirichlet_expr", C.c_char_p * 6),
+                ("k_tensor", _P), ("cp_expr", C.c_char_p), ("dcp_expr", C.c_char_p), ("num_dirichlet", _I32),
+                ("dirichlet_tags", _P), ("dirichlet_exprs", _P)]
 
 
 _lib = None
@@ -71,6 +73,7 @@ SIGNATURES = {
     "rsd_ctx_profile_get": [_P, C.c_char_p, C.POINTER(_I64), C.POINTER(_D)],
     "rsd_alloc": [_P, _SZ, C.POINTER(_P)],
     "rsd_free": [_P, _P],
+    "rsd_alloc_managed": [_P, _SZ, C.POINTER(_P)],
     "rsd_memcpy": [_P, _P, _P, _SZ, _I32],
     "rsd_memset_zero": [_P, _P, _SZ],
     "rsd_fill_f64": [_P, _P, _I64, _D],
@@ -85,6 +88,7 @@ SIGNATURES = {
     "rsd_csr_create": [_P, _I64, _I64, _P, _P, _P, C.POINTER(_P)],
     "rsd_csr_destroy": [_P],
     "rsd_csr_info": [_P, C.POINTER(_I64), C.POINTER(_I64)],
+    "rsd_csr_layout": [_P, C.POINTER(_I64), C.POINTER(_I64), C.POINTER(_I64)],
     "rsd_csr_values": [_P, _P, C.POINTER(_P)],
     "rsd_csr_set_values": [_P, _P, _P],
     "rsd_csr_get_values": [_P, _P, _P],
@@ -107,6 +111,8 @@ SIGNATURES = {
     "rsd_heat_info": [_P, C.POINTER(_I64), C.POINTER(_I64)],
     "rsd_heat_dofmap": [_P, _P, _P, _P],
     "rsd_heat_matrix": [_P, C.POINTER(_P)],
+    "rsd_heat_create_matrix": [_P, _P, C.POINTER(_P)],
+    "rsd_heat_eval_nodal": [_P, _P, C.c_char_p, _D, _P],
     "rsd_heat_set_time": [_P, _P, _D],
     "rsd_heat_set_k_elem": [_P, _P, _P],
     "rsd_assemble_matrix": [_P, _P, _D, _D, _D, _D, _P, _P, _P],
@@ -114,6 +120,7 @@ SIGNATURES = {
     "rsd_apply_dirichlet_lift": [_P, _P, _D, _D, _P],
     "rsd_assemble_diagonal": [_P, _P, _D, _D, _P, _P],
     "rsd_heat_solve_fem": [_P, _P, _D, C.POINTER(SolverConfig), _P, _P, C.POINTER(Report)],
+    "rsd_heat_solve_fem_forms": [_P, _P, _D, _D, _D, _P, _P, C.POINTER(SolverConfig), _P, _P, C.POINTER(Report)],
     "rsd_heat_set_flux": [_P, _P, _I32, C.POINTER(C.c_char_p)],
     "rsd_apply_natural": [_P, _P, _P],
     "rsd_heat_nodal_field": [_P, _P, _I32, _P, _P, _P],
@@ -282,6 +289,12 @@ class CSR:
         v = np.ascontiguousarray(v, np.float64)
         check(lib().rsd_csr_set_values(self.ctx.h, self.h, v.ctypes.data_as(_P)))
 
+    def layout(self):
+        """SELL-32 slots (padding included), slices and stencil slices of the execution layout."""
+        a, b, c = _I64(), _I64(), _I64()
+        check(lib().rsd_csr_layout(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return {"sell_slots": a.value, "slices": b.value, "stencil_slices": c.value}
+
     def pattern(self):
         rp = np.empty(self.n + 1, np.int64)
         col = np.empty(self.nnz, np.int64)
@@ -385,17 +398,32 @@ class Heat:
     """rsd_heat: the heat problem (dof map, pattern, element loops, stages) on the device."""
 
     def __init__(self, ctx, mesh, nq, k_const=1.0, k_expr=None, dk_expr=None, k_elem=None, rho=1.0, cp=1.0,
-                 src_expr=None, dirichlet=None, flux=None):
+                 src_expr=None, dirichlet=None, flux=None, k_tensor=None, cp_expr=None, dcp_expr=None):
+        """dirichlet: {tag: expression} for boundary tags of any value >= 0; k_tensor: the conductivity's
+        nsd x nsd anisotropic shape (K = k * k_tensor); cp_expr / dcp_expr: cp(T) and dcp/dT."""
         self.ctx, self.mesh = ctx, mesh
         d = HeatDesc()
         d.nq, d.k_const, d.rho, d.cp = nq, k_const, rho, cp
         d.k_expr = k_expr.encode() if k_expr else None
         d.dk_expr = dk_expr.encode() if dk_expr else None
         d.src_expr = src_expr.encode() if src_expr else None
+        d.cp_expr = cp_expr.encode() if cp_expr else None
+        d.dcp_expr = dcp_expr.encode() if dcp_expr else None
         ke = None if k_elem is None else np.ascontiguousarray(k_elem, np.float64)
         d.k_elem = None if ke is None else ke.ctypes.data_as(_P)
+        kt = None if k_tensor is None else np.ascontiguousarray(k_tensor, np.float64).reshape(-1)
+        if kt is not None and kt.size != mesh.nsd * mesh.nsd:
+            raise ValueError("k_tensor must hold nsd x nsd entries")
+        d.k_tensor = None if kt is None else kt.ctypes.data_as(_P)
+        extra = [(tag, ex) for tag, ex in (dirichlet or {}).items() if not 0 <= tag < 6]
         for tag, ex in (dirichlet or {}).items():
-            d.dirichlet_expr[tag] = ex.encode()
+            if 0 <= tag < 6:
+                d.dirichlet_expr[tag] = ex.encode()
+        tags = np.array([t for t, _ in extra], dtype=np.int32)
+        exprs = (C.c_char_p * max(len(extra), 1))(*[ex.encode() for _, ex in extra])
+        d.num_dirichlet = len(extra)
+        d.dirichlet_tags = tags.ctypes.data_as(_P) if extra else None
+        d.dirichlet_exprs = C.cast(exprs, _P) if extra else None
         self.h = _P()
         check(lib().rsd_heat_create(ctx.h, mesh.h, C.byref(d), C.byref(self.h)))
         n, nnz = _I64(), _I64()
@@ -422,6 +450,27 @@ class Heat:
 
     def set_time(self, t):
         check(lib().rsd_heat_set_time(self.ctx.h, self.h, t))
+
+    def create_matrix(self):
+        """A new matrix with the problem's pattern (shared) and zero values (HeatProblem::createMatrix)."""
+        a = _P()
+        check(lib().rsd_heat_create_matrix(self.ctx.h, self.h, C.byref(a)))
+        m = CSR(self.ctx, a, owned=True)
+        m._owner = self   # the pattern belongs to the problem: keep it alive
+        return m
+
+    def eval_nodal(self, expr, U, t=0.0):
+        """U = expr(t, x) at the free nodes (the initial condition's Expression mode)."""
+        check(lib().rsd_heat_eval_nodal(self.ctx.h, self.h, expr.encode(), t, _ptr(U)))
+        return U
+
+    def solve_fem_forms(self, b, x, c_tdiff=0.0, c_mass=0.0, c_tmass=0.0, U=None, Udot=None, cfg=None, **kw):
+        """Diffusion + c_tdiff TangentDiffusion + c_mass Mass + c_tmass TangentMass without a matrix."""
+        cfg = cfg or SolverConfig.make(**kw)
+        rep = Report()
+        check(lib().rsd_heat_solve_fem_forms(self.ctx.h, self.h, c_tdiff, c_mass, c_tmass, _ptr(U), _ptr(Udot), C.byref(cfg),
+                                             _ptr(b), _ptr(x), C.byref(rep)))
+        return rep.as_dict()
 
     def set_k_elem(self, k_dev):
         check(lib().rsd_heat_set_k_elem(self.ctx.h, self.h, _ptr(k_dev)))

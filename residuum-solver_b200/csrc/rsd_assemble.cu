@@ -19,6 +19,7 @@
 // Geometry follows JacobianTransform (fem/geometry/JacobianTransform.tpp): measure = sqrt(det(J^T J)),
 // 2D gradient transform with the true inverse, 3D with the cofactor/det layout (:160-185).
 #include <cmath>
+#include <map>
 #include <vector>
 
 #include "rsd_kernels.cuh"
@@ -68,6 +69,9 @@ struct AsmParams {
 	const double* __restrict__ tables;  // [nq][G][4] (N, dxi, deta, dzeta) then w[nq]
 	double kConst, rho, cp, time;
 	DevExpr kExpr, dkExpr, srcExpr;
+	DevExpr cpExpr, dcpExpr;            // cp(T), dcp/dT (n = 0: the constant cp)
+	int32_t aniso;                      // K = k kS (anisotropic shape), else k I
+	double kS[9];                       // row-major, stride 3
 	// matrix: CSR pattern for the column search, SELL-32 slice starts and values for the scatter
 	const int32_t* __restrict__ rp;
 	const int32_t* __restrict__ col;
@@ -107,10 +111,11 @@ struct Elem {
 constexpr int kAsmThreads = 128;
 constexpr int kAsmWarps = kAsmThreads / 32;
 
-// per-point record: inverse layout (9), w*measure, k, dk, grad T (3), V, grad V (3), W, f, spare
-constexpr int R_INV = 0, R_WM = 9, R_K = 10, R_DK = 11, R_GT = 12, R_V = 15, R_GV = 16, R_W = 19, R_F = 20, REC = 22;
-// per-node staging: x (3), U, V, W
-constexpr int N_X = 0, N_U = 3, N_V = 4, N_W = 5, NREC = 6;
+// per-point record: inverse layout (9), w*measure, k, dk, grad T (3), V, grad V (3), W, f, cp, dcp/dT, T rate
+constexpr int R_INV = 0, R_WM = 9, R_K = 10, R_DK = 11, R_GT = 12, R_V = 15, R_GV = 16, R_W = 19, R_F = 20, R_CP = 21,
+              R_DCP = 22, R_TR = 23, REC = 24;
+// per-node staging: x (3), U, V, W, rate of U
+constexpr int N_X = 0, N_U = 3, N_V = 4, N_W = 5, N_R = 6, NREC = 7;
 
 __host__ __device__ inline int table_stride(int G) { return G * 4 + 1; }                      // odd: no bank conflicts across q
 __host__ __device__ inline int node_area(int npe) { return npe * NREC + 1; }
@@ -129,11 +134,55 @@ size_t asm_smem_bytes(int npe, int nq, int nsd, bool fast, int pts) {
 
 // what phase 2 must evaluate
 struct Needs {
-	bool state;    // T, grad T (k(T), tangents)
+	bool state;    // T, grad T (k(T), cp(T), tangents)
 	bool field;    // V, grad V
 	bool field2;   // W (second operand, mass only)
 	bool load;     // x_q and f(t, x_q)
+	bool rate;     // the rate of T (TangentMassForm)
 };
+
+// the conductivity's shape applied to a vector: out = kS v (anisotropic) or v
+template <int NSD>
+__device__ __forceinline__ void shape_apply(const AsmParams& prm, const double* v, double* out) {
+	if (!prm.aniso) {
+#pragma unroll
+		for (int i = 0; i < NSD; ++i) out[i] = v[i];
+		return;
+	}
+#pragma unroll
+	for (int i = 0; i < NSD; ++i) {
+		double s = 0.0;
+#pragma unroll
+		for (int j = 0; j < NSD; ++j) s += prm.kS[i * 3 + j] * v[j];
+		out[i] = s;
+	}
+}
+// out = kS^T v
+template <int NSD>
+__device__ __forceinline__ void shape_apply_t(const AsmParams& prm, const double* v, double* out) {
+	if (!prm.aniso) {
+#pragma unroll
+		for (int i = 0; i < NSD; ++i) out[i] = v[i];
+		return;
+	}
+#pragma unroll
+	for (int j = 0; j < NSD; ++j) {
+		double s = 0.0;
+#pragma unroll
+		for (int i = 0; i < NSD; ++i) s += prm.kS[i * 3 + j] * v[i];
+		out[j] = s;
+	}
+}
+// grad N_a . K grad V / k with K = k kS: the diffusion integrand's direction part
+template <int NSD>
+__device__ __forceinline__ double shape_dot(const AsmParams& prm, const double* ga, const double* gv) {
+	double sv[3];
+	shape_apply<NSD>(prm, gv, sv);
+	double s = 0.0;
+#pragma unroll
+	for (int i = 0; i < NSD; ++i) s += ga[i] * sv[i];
+	return s;
+}
 
 template <int NSD, int P>
 __device__ __forceinline__ void stage_tables(const AsmParams& prm, double* sm) {
@@ -193,7 +242,7 @@ __device__ __forceinline__ void eval_point(const AsmParams& prm, const Needs& nd
 	double J[9];
 #pragma unroll
 	for (int i = 0; i < NSD * NSD; ++i) J[i] = 0.0;
-	double Tq = 0.0, Vq = 0.0, Wq = 0.0, xq[3] = {0.0, 0.0, 0.0}, dT[3] = {0.0, 0.0, 0.0}, dV[3] = {0.0, 0.0, 0.0};
+	double Tq = 0.0, Rq = 0.0, Vq = 0.0, Wq = 0.0, xq[3] = {0.0, 0.0, 0.0}, dT[3] = {0.0, 0.0, 0.0}, dV[3] = {0.0, 0.0, 0.0};
 #pragma unroll 4
 	for (int b = 0; b < NPE; ++b) {
 		const double* t = tq + b * 4;
@@ -202,11 +251,13 @@ __device__ __forceinline__ void eval_point(const AsmParams& prm, const Needs& nd
 		for (int i = 0; i < NSD; ++i)
 #pragma unroll
 			for (int al = 0; al < NSD; ++al) J[i * NSD + al] += t[1 + al] * nb[N_X + i];
-		if (GRAD && nd.state) {
+		if (nd.state) {
 			Tq += t[0] * nb[N_U];
+			if (GRAD)
 #pragma unroll
-			for (int al = 0; al < NSD; ++al) dT[al] += t[1 + al] * nb[N_U];
+				for (int al = 0; al < NSD; ++al) dT[al] += t[1 + al] * nb[N_U];
 		}
+		if (nd.rate) Rq += t[0] * nb[N_R];
 		if (nd.field) {
 			Vq += t[0] * nb[N_V];
 			if (GRAD)
@@ -220,6 +271,10 @@ __device__ __forceinline__ void eval_point(const AsmParams& prm, const Needs& nd
 	}
 	double inv[9];
 	const double detg = jac_geom<NSD, GRAD>(J, inv);
+	// SpecificHeatModel (SpecificHeatModel.hpp:35-61): cp and dcp/dT at the point's T
+	rec[R_CP] = prm.cpExpr.n ? eval_expr(prm.cpExpr, 0.0, 0.0, 0.0, 0.0, nd.state ? Tq : 0.0) : prm.cp;
+	rec[R_DCP] = prm.dcpExpr.n ? eval_expr(prm.dcpExpr, 0.0, 0.0, 0.0, 0.0, nd.state ? Tq : 0.0) : 0.0;
+	rec[R_TR] = Rq;
 	if (!GRAD) {
 		rec[R_WM] = sqrt(detg) * w;
 		if (nd.field) rec[R_V] = Vq;
@@ -350,12 +405,13 @@ __device__ __forceinline__ double affine_mass_row(const double* kt, int a, const
 		}                                                                                        \
 		const double ke = (prm.kElem && inRange) ? prm.kElem[e] : 1.0;
 
-#define RSD_STAGE_NODE(Uv, Vv, Wv)                                                               \
+#define RSD_STAGE_NODE(Uv, Vv, Wv) RSD_STAGE_NODE_R(Uv, Vv, Wv, 0.0)
+#define RSD_STAGE_NODE_R(Uv, Vv, Wv, Rv)                                                         \
 		if (has) {                                                                               \
 			double* nb = nodes + a * NREC;                                                       \
 			if (!aff)   /* an affine element's geometry is precomputed */                        \
 				_Pragma("unroll") for (int i = 0; i < NSD; ++i) nb[N_X + i] = prm.xyz[(int64_t)node * NSD + i]; \
-			nb[N_U] = (Uv); nb[N_V] = (Vv); nb[N_W] = (Wv);                                      \
+			nb[N_U] = (Uv); nb[N_V] = (Vv); nb[N_W] = (Wv); nb[N_R] = (Rv);                      \
 		}                                                                                        \
 		__syncwarp();                                                                            \
 		if (!aff && inRange)                                                                     \
@@ -369,16 +425,19 @@ __device__ __forceinline__ double affine_mass_row(const double* kt, int a, const
 
 // ---------------------------------------------------------------------------------------------
 // Assembler::assembleMatrix (fem/assembly/backend/cpu/Assembler.tpp:86-140):
-// c_diff*Diffusion + c_mass*Mass + c_tdiff*TangentDiffusion (+ TangentMass, zero for constant cp)
+// c_diff*Diffusion + c_mass*Mass + c_tdiff*TangentDiffusion + c_tmass*TangentMass, the models at the
+// state U (Full gather) and the rate Udot (Free gather; TangentMassForm reads it)
 // ---------------------------------------------------------------------------------------------
 template <int NSD, int P>
 __global__ void __launch_bounds__(kAsmThreads) k_asm_matrix(const AsmParams prm) {
 	constexpr bool kGrad = true;
 	Needs nd{};
-	nd.state = prm.kExpr.n || prm.dkExpr.n || prm.cTDiff != 0.0;
+	nd.state = prm.kExpr.n || prm.dkExpr.n || prm.cTDiff != 0.0 || (prm.cpExpr.n && (prm.cMass != 0.0 || prm.cTMass != 0.0));
+	nd.rate = prm.cTMass != 0.0 && prm.dcpExpr.n != 0;
 	RSD_ELEMENT_LOOP_BEGIN
 	const double Ua = (has && nd.state) ? (row >= 0 ? (prm.U ? prm.U[row] : 0.0) : prm.g[node]) : 0.0;
-	RSD_STAGE_NODE(Ua, 0.0, 0.0)
+	const double Ra = (has && nd.rate && row >= 0 && prm.Udot) ? prm.Udot[row] : 0.0;
+	RSD_STAGE_NODE_R(Ua, 0.0, 0.0, Ra)
 	double Ke[NPE];
 #pragma unroll
 	for (int b = 0; b < NPE; ++b) Ke[b] = 0.0;
@@ -403,25 +462,24 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_matrix(const AsmParams prm)
 			const double* rec = recs + q * REC;
 			const double* tq = tab + q * TS;
 			const double* ta = tq + a * 4;
-			double dx[3];
+			double dx[3], ky[3];
 			node_grad<NSD>(rec, ta, dx);
+			// DiffusionForm: grad N_a . kS grad N_b = (kS^T grad N_a) . J^-T dN_b/dxi
+			shape_apply_t<NSD>(prm, dx, ky);
 			double Ga[3];
 #pragma unroll
 			for (int al = 0; al < NSD; ++al) {
 				double s = 0.0;
 #pragma unroll
-				for (int i = 0; i < NSD; ++i) s += rec[R_INV + i * NSD + al] * dx[i];
+				for (int i = 0; i < NSD; ++i) s += rec[R_INV + i * NSD + al] * ky[i];
 				Ga[al] = s;
 			}
 			const double wm = rec[R_WM];
 			const double cd = prm.cDiff * rec[R_K] * wm;
-			double cm = prm.cMass * prm.rho * prm.cp * ta[0] * wm;
-			if (prm.cTDiff != 0.0) {
-				double s = 0.0;
-#pragma unroll
-				for (int i = 0; i < NSD; ++i) s += dx[i] * rec[R_DK] * rec[R_GT + i];
-				cm += prm.cTDiff * s * wm;
-			}
+			// MassForm rho cp(T) N_a N_b, TangentMassForm rho dcp/dT T_rate N_a N_b
+			double cm = (prm.cMass * prm.rho * rec[R_CP] + prm.cTMass * prm.rho * rec[R_DCP] * rec[R_TR]) * ta[0] * wm;
+			if (prm.cTDiff != 0.0)   // TangentDiffusionForm: grad N_a . dk/dT kS grad T N_b
+				cm += prm.cTDiff * rec[R_DK] * shape_dot<NSD>(prm, dx, rec + R_GT) * wm;
 #pragma unroll
 			for (int b = 0; b < NPE; ++b) {
 				const double* tb = tq + b * 4;   // one address for the whole warp: broadcast
@@ -592,8 +650,12 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_vector(const AsmParams prm)
 	nd.load = which == 0 || which == 7 || which == 9;
 	nd.field = which != 0;
 	nd.field2 = which == 8;
-	// k(T): diffusion of U takes T from U itself (staged as V, mirrored into U), the operator from the state
-	nd.state = (prm.kExpr.n != 0 && (which == 1 || which == 4 || which == 8 || which == 9)) || which == 6 || which == 10;
+	// k(T): diffusion of U takes T from U itself (staged as V, mirrored into U), the operator from the state;
+	// cp(T): every mass term takes T from the state (the mass right-hand side's state is U_prev itself)
+	constexpr bool kMass = W == 2 || W == 3 || W == 4 || W == 7 || W == 8 || W == 10;
+	nd.state = (prm.kExpr.n != 0 && (which == 1 || which == 4 || which == 8 || which == 9)) || which == 6 || which == 10 ||
+	           (kMass && prm.cpExpr.n != 0);
+	nd.rate = W == 10 && prm.cTMass != 0.0 && prm.dcpExpr.n != 0;
 	if (prm.skip && *(volatile const int32_t*)prm.skip) return;   // uniform over the launch
 	RSD_ELEMENT_LOOP_BEGIN
 	double Va = 0.0, Wa = 0.0, Ua = 0.0;
@@ -609,9 +671,10 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_vector(const AsmParams prm)
 			default: break;
 		}
 		if (which == 8) Wa = (row >= 0 && prm.Udot) ? prm.Udot[row] : 0.0;
-		Ua = (which == 4 || which == 6 || which == 10) ? fullU : Va;
+		Ua = (which == 3 || which == 4 || which == 6 || which == 10) ? fullU : Va;
 	}
-	RSD_STAGE_NODE(Ua, Va, Wa)
+	const double Ra = (has && nd.rate && row >= 0 && prm.Udot) ? prm.Udot[row] : 0.0;
+	RSD_STAGE_NODE_R(Ua, Va, Wa, Ra)
 	double Fa = 0.0, ge = 0.0;
 	if (has && aff) {
 		// reference integrals (no load term and no state here: the host enables this path only then;
@@ -644,13 +707,8 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_vector(const AsmParams prm)
 			const double wm = rec[R_WM];
 			const double Na = ta[0];
 			if (which == 6) {
-				// adjoint: grad lambda . grad T with unit conductivity, summed once per point
-				if (a == 0) {
-					double s = 0.0;
-#pragma unroll
-					for (int i = 0; i < NSD; ++i) s += rec[R_GV + i] * rec[R_GT + i];
-					ge += s * wm;
-				}
+				// adjoint: grad lambda . kS grad T with unit conductivity, summed once per point
+				if (a == 0) ge += shape_dot<NSD>(prm, rec + R_GV, rec + R_GT) * wm;
 				continue;
 			}
 			if (nd.load) Fa += (rec[R_F] * Na) * wm;
@@ -659,23 +717,21 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_vector(const AsmParams prm)
 			if constexpr (kGrad) {
 				double dx[3];
 				node_grad<NSD>(rec, ta, dx);
-				double dd = 0.0;
-#pragma unroll
-				for (int i = 0; i < NSD; ++i) dd += dx[i] * rec[R_GV + i];
-				kd = rec[R_K] * dd;                        // per-element factor included
-				if (which == 10)                           // TangentDiffusionForm: grad N_a . dk/dT grad T
-#pragma unroll
-					for (int i = 0; i < NSD; ++i) tg += dx[i] * rec[R_DK] * rec[R_GT + i];
+				kd = rec[R_K] * shape_dot<NSD>(prm, dx, rec + R_GV);      // per-element factor included
+				if (which == 10)                           // TangentDiffusionForm: grad N_a . dk/dT kS grad T
+					tg = rec[R_DK] * shape_dot<NSD>(prm, dx, rec + R_GT);
 			}
-			const double mass = prm.rho * prm.cp * Na * rec[R_V];
+			const double mass = prm.rho * rec[R_CP] * Na * rec[R_V];
 			switch (which) {
 				case 1: Fa += kd * wm; break;
 				case 2: case 3: Fa += mass * wm; break;
 				case 4: Fa += (kd + prm.coef * mass) * wm; break;
-				case 10: Fa += (kd + tg * rec[R_V] + prm.coef * mass) * wm; break;
+				case 10:   // + c_tdiff TangentDiffusionForm + c_tmass TangentMassForm (rho dcp/dT T_rate N_a V)
+					Fa += (kd + prm.cTDiff * tg * rec[R_V] + prm.coef * mass + prm.cTMass * prm.rho * rec[R_DCP] * rec[R_TR] * Na * rec[R_V]) * wm;
+					break;
 				case 5: Fa += (prm.cDiff * kd + prm.cMass * mass) * wm; break;
 				case 7: Fa += prm.coef * mass * wm; break;
-				case 8: Fa += (kd + prm.rho * prm.cp * Na * rec[R_W]) * wm; break;
+				case 8: Fa += (kd + prm.rho * rec[R_CP] * Na * rec[R_W]) * wm; break;
 				case 9: Fa -= kd * wm; break;
 				default: break;
 			}
@@ -1064,14 +1120,17 @@ __global__ void k_build_erow(int64_t count, const int32_t* __restrict__ ien, con
 }
 
 // Assembler::assembleDiagonal (Assembler.tpp:142-197) for c_diff*Diffusion + c_mass*Mass
+// + c_tdiff*TangentDiffusion + c_tmass*TangentMass
 template <int NSD, int P>
 __global__ void __launch_bounds__(kAsmThreads) k_asm_diag(const AsmParams prm) {
 	constexpr bool kGrad = true;
 	Needs nd{};
-	nd.state = prm.kExpr.n != 0 || prm.cTDiff != 0.0;
+	nd.state = prm.kExpr.n != 0 || prm.cTDiff != 0.0 || (prm.cpExpr.n != 0 && (prm.cMass != 0.0 || prm.cTMass != 0.0));
+	nd.rate = prm.cTMass != 0.0 && prm.dcpExpr.n != 0;
 	RSD_ELEMENT_LOOP_BEGIN
 	const double Ua = (has && nd.state) ? (row >= 0 ? (prm.U ? prm.U[row] : 0.0) : prm.g[node]) : 0.0;
-	RSD_STAGE_NODE(Ua, 0.0, 0.0)
+	const double Ra = (has && nd.rate && row >= 0 && prm.Udot) ? prm.Udot[row] : 0.0;
+	RSD_STAGE_NODE_R(Ua, 0.0, 0.0, Ra)
 	double Da = 0.0;
 	if (has) {
 		for (int q = 0; q < prm.nq; ++q) {
@@ -1079,14 +1138,11 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_diag(const AsmParams prm) {
 			const double* ta = tab + q * TS + a * 4;
 			double dx[3];
 			node_grad<NSD>(rec, ta, dx);
-			double dd = 0.0;
-#pragma unroll
-			for (int i = 0; i < NSD; ++i) dd += dx[i] * dx[i];
+			const double dd = shape_dot<NSD>(prm, dx, dx);
 			double tg = 0.0;
-			if (prm.cTDiff != 0.0)
-#pragma unroll
-				for (int i = 0; i < NSD; ++i) tg += dx[i] * rec[R_DK] * rec[R_GT + i];
-			Da += (prm.cDiff * rec[R_K] * dd + prm.cMass * prm.rho * prm.cp * ta[0] * ta[0] + prm.cTDiff * tg * ta[0]) * rec[R_WM];
+			if (prm.cTDiff != 0.0) tg = rec[R_DK] * shape_dot<NSD>(prm, dx, rec + R_GT);
+			const double mc = prm.cMass * prm.rho * rec[R_CP] + prm.cTMass * prm.rho * rec[R_DCP] * rec[R_TR];
+			Da += (prm.cDiff * rec[R_K] * dd + mc * ta[0] * ta[0] + prm.cTDiff * tg * ta[0]) * rec[R_WM];
 		}
 	}
 	if (has && row >= 0) atomicAdd(prm.out + row, Da);
@@ -1106,7 +1162,7 @@ __host__ __device__ static inline void lagrange1d(int p, double xi, double* N, d
 // tag carries a flux q(t, x), F_a += sum_q sum_i (q_i(t, x_q) N_a(q)) n_i(q) w_q over the face's nodes,
 // with the point mapped into the element (LagrangeQuad/Hex::mapFaceToElement), n = cof(J) nRef
 // (JacobianTransform::computeBoundaryNormal), w the reference face weight, scattered Free.  One
-// thread per face; faces holds (element, face, tag) triplets.
+// thread per face; faces holds (element, face, flux index) triplets.
 template <int NSD, int P>
 __global__ void __launch_bounds__(128) k_natural(int64_t nfaces, const int32_t* __restrict__ faces,
                                                  const double* __restrict__ xyz, const int32_t* __restrict__ ien,
@@ -1116,7 +1172,7 @@ __global__ void __launch_bounds__(128) k_natural(int64_t nfaces, const int32_t* 
 	const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
 	if (i >= nfaces) return;
 	const int64_t e = faces[3 * i];
-	const int f = faces[3 * i + 1], tag = faces[3 * i + 2];
+	const int f = faces[3 * i + 1], fx = faces[3 * i + 2];   // face, index of its flux expressions
 	const int axis = f / 2;                       // the reference axis normal to the face
 	const double side = (f & 1) ? 1.0 : -1.0;     // its reference coordinate on the face
 	const int32_t* en = ien + e * NPE;
@@ -1173,7 +1229,7 @@ __global__ void __launch_bounds__(128) k_natural(int64_t nfaces, const int32_t* 
 		double val[3];
 #pragma unroll
 		for (int d = 0; d < NSD; ++d)
-			val[d] = eval_expr(flux[tag * 3 + d], time, x[0], x[1], NSD == 3 ? x[2] : 0.0, 0.0);
+			val[d] = eval_expr(flux[fx * 3 + d], time, x[0], x[1], NSD == 3 ? x[2] : 0.0, 0.0);
 		// the face's nodes: the face axis at its end, the other axes in order
 #pragma unroll
 		for (int b = 0; b < NFN; ++b) {
@@ -1252,15 +1308,20 @@ __global__ void __launch_bounds__(128) k_nodal_field(const AsmParams prm, int fi
 		const double k = ke * (prm.kExpr.n ? eval_expr(prm.kExpr, 0.0, 0.0, 0.0, 0.0, T) : prm.kConst);
 		double val[3];
 		if (field == 0) {
+			// HeatFluxField: q = -K grad T with K = k kS
+			double g[3], kg[3];
 #pragma unroll
 			for (int i = 0; i < NSD; ++i) {
 				double gi = 0.0;
 #pragma unroll
 				for (int al = 0; al < NSD; ++al) gi += inv[i * NSD + al] * gxi[al];
-				val[i] = -(k * gi);
+				g[i] = gi;
 			}
+			shape_apply<NSD>(prm, g, kg);
+#pragma unroll
+			for (int i = 0; i < NSD; ++i) val[i] = -(k * kg[i]);
 		} else {
-			val[0] = k;
+			val[0] = prm.aniso ? k * prm.kS[0] : k;   // ConductivityField: K[0]
 		}
 		for (int a = 0; a < NPE; ++a) {
 			const double wa = tq[a * 4] * meas * wq[q];
@@ -1463,6 +1524,10 @@ static int ensure_affine(rsd_ctx* ctx, rsd_heat* h) {
 	return RSD_OK;
 }
 
+// The reference-element integrals hold isotropic gradient products and a constant rho cp: an
+// anisotropic conductivity or cp(T) takes the quadrature path
+static bool model_blocks_affine(const rsd_heat* h) { return h->aniso || h->cpExpr.n != 0; }
+
 static AsmParams params_for(const rsd_heat* h) {
 	AsmParams p{};
 	p.nelem = h->m->nelem;
@@ -1481,6 +1546,10 @@ static AsmParams params_for(const rsd_heat* h) {
 	p.kExpr = h->kExpr;
 	p.dkExpr = h->dkExpr;
 	p.srcExpr = h->srcExpr;
+	p.cpExpr = h->cpExpr;
+	p.dcpExpr = h->dcpExpr;
+	p.aniso = h->aniso ? 1 : 0;
+	for (int i = 0; i < 9; ++i) p.kS[i] = h->kS[i];
 	p.outScale = 1.0;
 	return p;
 }
@@ -1680,7 +1749,9 @@ int assemble_matrix(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, doubl
 	p.cDiff = cDiff; p.cMass = cMass; p.cTDiff = cTDiff; p.cTMass = cTMass;
 	// reference integrals for the affine elements when the coefficients are constant per element
 	RSD_CHECK(ensure_affine(ctx, h));
-	if (h->anyAffine && h->kExpr.n == 0 && h->dkExpr.n == 0 && cTDiff == 0.0) { p.fast = 1; p.affine = h->affine; p.geo = h->geo; p.ktab = h->ktab; if (h->allAffine) p.pts = 0; }
+	if (h->anyAffine && h->kExpr.n == 0 && h->dkExpr.n == 0 && cTDiff == 0.0 && cTMass == 0.0 && !model_blocks_affine(h)) {
+		p.fast = 1; p.affine = h->affine; p.geo = h->geo; p.ktab = h->ktab; if (h->allAffine) p.pts = 0;
+	}
 	p.U = U; p.Udot = Udot;
 	A->sellValid = true;
 	A->csrValid = false;
@@ -1699,9 +1770,6 @@ int assemble_matrix(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, doubl
 	return rc;
 }
 
-int apply_operator(rsd_ctx* ctx, rsd_heat* h, double coef, const double* U, const double* V, double* out,
-                   const int32_t* skip, int which);
-
 // the affine path of the vector kernels: every mode but the adjoint, with no state-dependent
 // conductivity and no load term (both are evaluated per quadrature point)
 static int affine_vector(rsd_ctx* ctx, rsd_heat* h, AsmParams& p) {
@@ -1709,7 +1777,9 @@ static int affine_vector(rsd_ctx* ctx, rsd_heat* h, AsmParams& p) {
 	const int w = p.which;
 	const bool load = w == 0 || w == 7 || w == 9;
 	const bool state = (h->kExpr.n != 0 && (w == 1 || w == 4 || w == 8 || w == 9)) || w == 10;
-	if (h->anyAffine && w != 6 && !state && !(load && h->srcExpr.n != 0)) { p.fast = 1; p.affine = h->affine; p.geo = h->geo; p.ktab = h->ktab; if (h->allAffine) p.pts = 0; }
+	if (h->anyAffine && w != 6 && !state && !(load && h->srcExpr.n != 0) && !model_blocks_affine(h)) {
+		p.fast = 1; p.affine = h->affine; p.geo = h->geo; p.ktab = h->ktab; if (h->allAffine) p.pts = 0;
+	}
 	return RSD_OK;
 }
 
@@ -1718,6 +1788,7 @@ int assemble_vector(rsd_ctx* ctx, rsd_heat* h, int which, double coef, const dou
 	if (which == 4 && !accumulate && outScale == 1.0) return apply_operator(ctx, h, coef, U, operand, out, nullptr, 4);
 	AsmParams p = params_for(h);
 	p.which = which; p.coef = coef; p.U = U; p.Udot = Udot; p.V = operand; p.out = out; p.outScale = outScale;
+	if (which == 10) p.cTDiff = 1.0;   // the Jacobian's product: TangentDiffusion with coefficient 1
 	if (which == 7 && h->gPrevValid) p.gPrev = h->gPrev;
 	RSD_CHECK(affine_vector(ctx, h, p));
 	if (!accumulate) {
@@ -1737,9 +1808,10 @@ int assemble_vector(rsd_ctx* ctx, rsd_heat* h, int which, double coef, const dou
 // most 32 nodes per element, take the sum-factorized kernel (RSD_SUMFAC=0: the table kernels);
 // 4- and 8-node elements keep the one-thread-per-element table kernel, which measured faster for them.
 int apply_operator(rsd_ctx* ctx, rsd_heat* h, double coef, const double* U, const double* V, double* out,
-                   const int32_t* skip, int which) {
+                   const int32_t* skip, int which, double cTDiff, double cTMass, const double* Udot) {
 	AsmParams p = params_for(h);
 	p.which = which; p.coef = coef; p.U = U; p.V = V; p.out = out; p.skip = skip;
+	if (which == 10) { p.cTDiff = cTDiff; p.cTMass = cTMass; p.Udot = Udot; }
 	RSD_CHECK(affine_vector(ctx, h, p));
 	RSD_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * std::max<int64_t>(h->n, 1), ctx->stream));
 	const int pr = prof_begin(ctx, PF_ASM_VECTOR);
@@ -1810,29 +1882,40 @@ int assemble_lift(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, double*
 // the list of boundary faces that carry one
 int set_flux(rsd_ctx* ctx, rsd_heat* h, int tag, const char* const* exprs) {
 	const rsd_mesh* m = h->m;
-	if (tag < 0 || tag >= 2 * m->nsd) return set_error(RSD_EINVAL, "boundary tag out of range");
+	if (tag < 0) return set_error(RSD_EINVAL, "boundary tags are >= 0");
+	size_t slot = h->fluxTags.size();
+	for (size_t i = 0; i < h->fluxTags.size(); ++i) if (h->fluxTags[i] == tag) slot = i;
 	if (exprs) {
 		DevExpr c[3];
 		for (int d = 0; d < m->nsd; ++d) {
 			if (!exprs[d]) return set_error(RSD_EINVAL, "a flux needs one expression per spatial component");
 			RSD_CHECK(compile_expr(exprs[d], &c[d]));
 		}
-		for (int d = 0; d < 3; ++d) h->fluxExpr[tag * 3 + d] = d < m->nsd ? c[d] : DevExpr{};
-		h->hasFlux[tag] = true;
-	} else {
-		h->hasFlux[tag] = false;
+		if (slot == h->fluxTags.size()) { h->fluxTags.push_back(tag); h->fluxExpr.resize(3 * h->fluxTags.size()); }
+		for (int d = 0; d < 3; ++d) h->fluxExpr[slot * 3 + d] = d < m->nsd ? c[d] : DevExpr{};
+	} else if (slot < h->fluxTags.size()) {
+		h->fluxTags.erase(h->fluxTags.begin() + slot);
+		h->fluxExpr.erase(h->fluxExpr.begin() + 3 * slot, h->fluxExpr.begin() + 3 * slot + 3);
 	}
+	std::map<int32_t, int32_t> index;
+	for (size_t i = 0; i < h->fluxTags.size(); ++i) index[h->fluxTags[i]] = (int32_t)i;
 	std::vector<int32_t> fl;
 	for (int64_t e = 0; e < m->nelem; ++e)
 		for (int f = 0; f < m->nfaces; ++f) {
 			const int32_t t = m->h_rng[e * m->nfaces + f];
-			if (t >= 0 && t < 6 && h->hasFlux[t]) { fl.push_back((int32_t)e); fl.push_back(f); fl.push_back(t); }
+			const auto it = t >= 0 ? index.find(t) : index.end();
+			if (it != index.end()) { fl.push_back((int32_t)e); fl.push_back(f); fl.push_back(it->second); }
 		}
+	RSD_CUDA(cudaStreamSynchronize(ctx->stream));   // no launch in flight reads the lists replaced here
 	cudaFree(h->nFaces);
 	h->nFaces = nullptr;
+	cudaFree(h->dFlux);
+	h->dFlux = nullptr;
 	h->nnFaces = (int64_t)fl.size() / 3;
-	if (!h->dFlux) RSD_CUDA(cudaMalloc(&h->dFlux, sizeof(DevExpr) * 18));
-	RSD_CUDA(cudaMemcpyAsync(h->dFlux, h->fluxExpr, sizeof(DevExpr) * 18, cudaMemcpyHostToDevice, ctx->stream));
+	if (!h->fluxExpr.empty()) {
+		RSD_CUDA(cudaMalloc(&h->dFlux, sizeof(DevExpr) * h->fluxExpr.size()));
+		RSD_CUDA(cudaMemcpyAsync(h->dFlux, h->fluxExpr.data(), sizeof(DevExpr) * h->fluxExpr.size(), cudaMemcpyHostToDevice, ctx->stream));
+	}
 	if (h->nnFaces) {
 		RSD_CUDA(cudaMalloc(&h->nFaces, sizeof(int32_t) * fl.size()));
 		RSD_CUDA(cudaMemcpyAsync(h->nFaces, fl.data(), sizeof(int32_t) * fl.size(), cudaMemcpyHostToDevice, ctx->stream));
@@ -1884,9 +1967,10 @@ int nodal_field(rsd_ctx* ctx, rsd_heat* h, int field, const double* U, double* o
 	return RSD_OK;
 }
 
-int assemble_diagonal(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, const double* U, double* d, double cTDiff) {
+int assemble_diagonal(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, const double* U, double* d, double cTDiff,
+                      double cTMass, const double* Udot) {
 	AsmParams p = params_for(h);
-	p.cDiff = cDiff; p.cMass = cMass; p.cTDiff = cTDiff; p.U = U; p.out = d;
+	p.cDiff = cDiff; p.cMass = cMass; p.cTDiff = cTDiff; p.cTMass = cTMass; p.U = U; p.Udot = Udot; p.out = d;
 	RSD_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * std::max<int64_t>(h->n, 1), ctx->stream));
 	return launch_k_asm_diag(ctx, h, p);
 }

@@ -103,11 +103,25 @@ int compile_expr(const char* src, DevExpr* out) {
 		*out = DevExpr();
 		return set_error(RSD_EPARSE, std::string("cannot compile expression '") + src + "'");
 	}
+	// the stack depth the postfix program reaches: operands push one, binary operators pop one
+	int sp = 0, depth = 0;
+	for (int i = 0; i < out->n; ++i) {
+		const int op = out->op[i];
+		if (op == E_CONST || op == E_VAR) ++sp;
+		else if (op == E_ADD || op == E_SUB || op == E_MUL || op == E_DIV || op == E_POW) --sp;
+		depth = std::max(depth, sp);
+	}
+	if (depth > kExprStack) {
+		*out = DevExpr();
+		return set_error(RSD_EPARSE, std::string("expression '") + src + "' needs an evaluation stack of " + std::to_string(depth) +
+		                 " entries; the device machine holds " + std::to_string(kExprStack));
+	}
+	out->depth = depth;
 	return RSD_OK;
 }
 
 double eval_expr_host(const DevExpr& e, double t, double x, double y, double z, double T) {
-	double st[kExprMax];
+	double st[kExprStack];
 	int sp = 0;
 	const double v[5] = {t, x, y, z, T};
 	for (int i = 0; i < e.n; ++i) {
@@ -152,7 +166,7 @@ static void parallel_for(int64_t n, Fn&& fn) {
 // ---------------------------------------------------------------------------------------------
 // TopologicalDOF::buildConstraints, Interleaved ordering (topology/TopologicalDOF.tpp:34-111):
 // nodes on faces whose tag is essential are constrained; the constraint tag is the last face
-// (in element, face order) that marked the node; free nodes are numbered in ascending order.
+// (in element, face order) that marked the node (h_ctag holds that tag's expression index); free nodes are numbered in ascending order.
 // Face-node lists are LagrangeQuad/Hex::getFaceNodes (fem/basis/LagrangeQuad.tpp:136-155,
 // fem/basis/LagrangeHex.tpp:263-304).
 // ---------------------------------------------------------------------------------------------
@@ -183,16 +197,20 @@ int build_dofmap(rsd_heat* h) {
 	const rsd_mesh* m = h->m;
 	h->h_t2a.assign(m->nnodes, 0);
 	h->h_ctag.assign(m->nnodes, -1);
+	std::map<int32_t, int32_t> index;   // essential tag -> its expression
+	for (size_t i = 0; i < h->essTags.size(); ++i) index[h->essTags[i]] = (int32_t)i;
 	int fn[64];
 	for (int64_t e = 0; e < m->nelem; ++e)
 		for (int f = 0; f < m->nfaces; ++f) {
 			const int32_t tag = m->h_rng[e * m->nfaces + f];
-			if (tag < 0 || tag > 5 || !h->essential[tag]) continue;
+			if (tag < 0) continue;
+			const auto it = index.find(tag);
+			if (it == index.end()) continue;
 			const int npf = face_nodes(m->nsd, m->order, f, fn);
 			for (int i = 0; i < npf; ++i) {
 				const int32_t node = m->h_ien[e * m->npe + fn[i]];
 				h->h_t2a[node] = -1;
-				h->h_ctag[node] = tag;
+				h->h_ctag[node] = it->second;
 			}
 		}
 	h->h_a2t.clear();
@@ -235,8 +253,32 @@ int resident_blocks(const void* kernel, int block) {
 }
 
 static void free_csr_arrays(rsd_csr* A) {
-	cudaFree(A->rowPtr); cudaFree(A->col); cudaFree(A->val); cudaFree(A->diag);
-	cudaFree(A->sStart); cudaFree(A->sCol); cudaFree(A->sVal); cudaFree(A->val32); cudaFree(A->sSrc); cudaFree(A->sDiag); cudaFree(A->sCol16); cudaFree(A->sBase); cudaFree(A->sUni); cudaFree(A->sOffs);
+	cudaFree(A->val); cudaFree(A->sVal); cudaFree(A->val32);
+	if (!A->owns_pattern) return;   // the pattern belongs to the matrix it was shared from
+	cudaFree(A->rowPtr); cudaFree(A->col); cudaFree(A->diag);
+	cudaFree(A->sStart); cudaFree(A->sCol); cudaFree(A->sSrc); cudaFree(A->sDiag); cudaFree(A->sCol16); cudaFree(A->sBase); cudaFree(A->sUni); cudaFree(A->sOffs);
+}
+
+// A matrix with src's pattern and layout (shared, not copied) and zero values of its own.
+int share_pattern(rsd_ctx* ctx, const rsd_csr* src, rsd_csr** out) {
+	rsd_csr* A = new rsd_csr(*src);
+	A->owns_pattern = false;
+	A->val = nullptr; A->sVal = nullptr; A->val32 = nullptr;
+	A->fmt32 = -1; A->version = 1; A->version32 = 0;
+	cudaError_t e;
+	if ((e = cudaMalloc(&A->val, sizeof(double) * std::max<int64_t>(A->nnz, 1))) != cudaSuccess ||
+	    (e = cudaMalloc(&A->sVal, sizeof(double) * std::max<int64_t>(A->ssize, 1))) != cudaSuccess ||
+	    (e = cudaMemsetAsync(A->val, 0, sizeof(double) * std::max<int64_t>(A->nnz, 1), ctx->stream)) != cudaSuccess ||
+	    (e = cudaMemsetAsync(A->sVal, 0, sizeof(double) * std::max<int64_t>(A->ssize, 1), ctx->stream)) != cudaSuccess ||
+	    (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) {
+		cudaFree(A->val); cudaFree(A->sVal);
+		delete A;
+		return cuda_error(e, "matrix values");
+	}
+	A->csrValid = true;
+	A->sellValid = true;
+	*out = A;
+	return RSD_OK;
 }
 
 static int upload_csr(rsd_ctx* ctx, int64_t n, const std::vector<int32_t>& rp, const std::vector<int32_t>& col,
@@ -325,6 +367,7 @@ static int upload_csr(rsd_ctx* ctx, int64_t n, const std::vector<int32_t>& rp, c
 				offTable.insert(offTable.end(), pat[s].begin(), pat[s].end());
 			}
 			sUni[s] = it->second;
+			++A->nStencil;
 		}
 		// re-lay the stencil slices by pattern position (the CSR rank order above holds for the rest)
 		parallel_for(ns, [&](int64_t b, int64_t e) {
@@ -597,6 +640,15 @@ int rsd_alloc(rsd_ctx* c, size_t bytes, void** dptr) {
 	return RSD_OK;
 }
 
+int rsd_alloc_managed(rsd_ctx* c, size_t bytes, void** dptr) {
+	if (!c || !dptr) return set_error(RSD_EINVAL, "null argument");
+	RSD_CUDA(cudaSetDevice(c->device));
+	RSD_CUDA(cudaMallocManaged(dptr, std::max<size_t>(bytes, 1), cudaMemAttachGlobal));
+	// resident on the device: kernels read it at full speed; host reads map or migrate pages on demand
+	if (cudaMemAdvise(*dptr, std::max<size_t>(bytes, 1), cudaMemAdviseSetPreferredLocation, c->device) != cudaSuccess) cudaGetLastError();
+	return RSD_OK;
+}
+
 int rsd_free(rsd_ctx* c, void* dptr) {
 	if (!c) return set_error(RSD_EINVAL, "null context");
 	if (dptr) {
@@ -654,6 +706,14 @@ int rsd_csr_info(const rsd_csr* A, int64_t* nrows, int64_t* nnz) {
 	if (!A) return set_error(RSD_EINVAL, "null matrix");
 	if (nrows) *nrows = A->n;
 	if (nnz) *nnz = A->nnz;
+	return RSD_OK;
+}
+
+int rsd_csr_layout(const rsd_csr* A, int64_t* sell_slots, int64_t* slices, int64_t* stencil_slices) {
+	if (!A) return set_error(RSD_EINVAL, "null matrix");
+	if (sell_slots) *sell_slots = A->ssize;
+	if (slices) *slices = A->nslices;
+	if (stencil_slices) *stencil_slices = A->nStencil;
 	return RSD_OK;
 }
 

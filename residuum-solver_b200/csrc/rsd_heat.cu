@@ -17,7 +17,7 @@ static bool uses_time(const DevExpr& e) {
 
 // Dirichlet value per constrained node at time t: the constraint tag's expression at the node's
 // coordinates, as gatherElementVector evaluates it (fem/assembly/backend/cpu/ElementMap.tpp:55-65)
-// g[node] = the Dirichlet expression of the node's constraint tag at (t, x) for every constrained node
+// g[node] = the Dirichlet expression of the node's constraint (tags[i]: its index into bc) at (t, x)
 __global__ void k_bc_values(int64_t nc, const int32_t* __restrict__ nodes, const int32_t* __restrict__ tags,
                             const double* __restrict__ xyz, int nsd, const DevExpr* __restrict__ bc, double t,
                             double* __restrict__ g) {
@@ -38,9 +38,11 @@ static int bc_values_to(rsd_ctx* ctx, rsd_heat* h, double t, double* dst) {
 		for (int64_t i = 0; i < m->nnodes; ++i)
 			if (h->h_t2a[i] < 0) { cn.push_back((int32_t)i); ct.push_back(h->h_ctag[i]); }
 		h->ncNodes = (int64_t)cn.size();
-		RSD_CUDA(cudaMalloc(&h->dBc, sizeof(DevExpr) * 6));
+		const size_t ne = std::max<size_t>(h->bcExpr.size(), 1);
+		RSD_CUDA(cudaMalloc(&h->dBc, sizeof(DevExpr) * ne));
 		RSD_CUDA(cudaMalloc(&h->cNodes, sizeof(int32_t) * 2 * std::max<int64_t>(h->ncNodes, 1)));
-		RSD_CUDA(cudaMemcpyAsync(h->dBc, h->bcExpr, sizeof(DevExpr) * 6, cudaMemcpyHostToDevice, ctx->stream));
+		if (!h->bcExpr.empty())
+			RSD_CUDA(cudaMemcpyAsync(h->dBc, h->bcExpr.data(), sizeof(DevExpr) * h->bcExpr.size(), cudaMemcpyHostToDevice, ctx->stream));
 		if (h->ncNodes) {
 			RSD_CUDA(cudaMemcpyAsync(h->cNodes, cn.data(), sizeof(int32_t) * cn.size(), cudaMemcpyHostToDevice, ctx->stream));
 			RSD_CUDA(cudaMemcpyAsync(h->cNodes + h->ncNodes, ct.data(), sizeof(int32_t) * ct.size(), cudaMemcpyHostToDevice, ctx->stream));
@@ -59,7 +61,7 @@ static int bc_values_to(rsd_ctx* ctx, rsd_heat* h, double t, double* dst) {
 int upload_bc_values(rsd_ctx* ctx, rsd_heat* h) { return bc_values_to(ctx, h, h->time, h->g); }
 
 static bool bc_time_dependent(const rsd_heat* h) {
-	for (int t = 0; t < 6; ++t) if (h->essential[t] && uses_time(h->bcExpr[t])) return true;
+	for (const DevExpr& e : h->bcExpr) if (uses_time(e)) return true;
 	return false;
 }
 
@@ -68,6 +70,17 @@ static int set_time(rsd_ctx* ctx, rsd_heat* h, double t) {
 	h->time = t;
 	if (changed && bc_time_dependent(h)) return upload_bc_values(ctx, h);
 	return RSD_OK;
+}
+
+// U[t2a[v]] = f(t, x_v) for every free node v (HeatProblem::loadNodalField, Expression mode)
+__global__ void k_eval_nodal(int64_t nn, const int32_t* __restrict__ t2a, const double* __restrict__ xyz, int nsd,
+                             const DevExpr f, double t, double* __restrict__ U) {
+	for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nn; v += (int64_t)gridDim.x * blockDim.x) {
+		const int32_t r = t2a[v];
+		if (r < 0) continue;
+		const double* x = xyz + v * nsd;
+		U[r] = eval_expr(f, t, x[0], nsd > 1 ? x[1] : 0.0, nsd > 2 ? x[2] : 0.0, 0.0);
+	}
 }
 
 __global__ void k_be_rate(int64_t n, double inv_dt, const double* __restrict__ U, const double* __restrict__ Up, double* __restrict__ Ud) {
@@ -124,11 +137,37 @@ int rsd_heat_create(rsd_ctx* ctx, const rsd_mesh* m, const rsd_heat_desc* d, rsd
 	h->rho = d->rho;
 	h->cp = d->cp;
 	int rc;
-	if ((rc = compile_expr(d->k_expr, &h->kExpr)) || (rc = compile_expr(d->dk_expr, &h->dkExpr)) || (rc = compile_expr(d->src_expr, &h->srcExpr))) { delete h; return rc; }
-	for (int t = 0; t < 6; ++t) {
-		if (!d->dirichlet_expr[t]) continue;
-		if ((rc = compile_expr(d->dirichlet_expr[t], &h->bcExpr[t]))) { delete h; return rc; }
-		h->essential[t] = true;
+	if ((rc = compile_expr(d->k_expr, &h->kExpr)) || (rc = compile_expr(d->dk_expr, &h->dkExpr)) || (rc = compile_expr(d->src_expr, &h->srcExpr)) ||
+	    (rc = compile_expr(d->cp_expr, &h->cpExpr)) || (rc = compile_expr(d->dcp_expr, &h->dcpExpr))) { delete h; return rc; }
+	if (d->dcp_expr && !d->cp_expr) { delete h; return set_error(RSD_EINVAL, "dcp_expr given without cp_expr"); }
+	if (d->k_tensor) {
+		h->aniso = true;
+		for (int i = 0; i < 9; ++i) h->kS[i] = 0.0;
+		for (int i = 0; i < m->nsd; ++i)
+			for (int j = 0; j < m->nsd; ++j) {
+				const double v = d->k_tensor[i * m->nsd + j];
+				if (!std::isfinite(v)) { delete h; return set_error(RSD_EINVAL, "conductivity tensor entry is not finite"); }
+				h->kS[i * 3 + j] = v;
+			}
+	}
+	// essential tags: dirichlet_expr[0..5], then the tag list (a repeated tag keeps its later expression,
+	// as the reference evaluates every entry registered on a tag in turn)
+	auto add_bc = [&](int32_t tag, const char* src) -> int {
+		if (tag < 0) return set_error(RSD_EINVAL, "boundary tags are >= 0");
+		DevExpr ex;
+		RSD_CHECK(compile_expr(src, &ex));
+		for (size_t i = 0; i < h->essTags.size(); ++i)
+			if (h->essTags[i] == tag) { h->bcExpr[i] = ex; return RSD_OK; }
+		h->essTags.push_back(tag);
+		h->bcExpr.push_back(ex);
+		return RSD_OK;
+	};
+	for (int t = 0; t < 6; ++t)
+		if (d->dirichlet_expr[t] && (rc = add_bc(t, d->dirichlet_expr[t]))) { delete h; return rc; }
+	if (d->num_dirichlet < 0 || (d->num_dirichlet > 0 && (!d->dirichlet_tags || !d->dirichlet_exprs))) { delete h; return set_error(RSD_EINVAL, "bad Dirichlet tag list"); }
+	for (int32_t i = 0; i < d->num_dirichlet; ++i) {
+		if (!d->dirichlet_exprs[i]) { delete h; return set_error(RSD_EINVAL, "Dirichlet tag without an expression"); }
+		if ((rc = add_bc(d->dirichlet_tags[i], d->dirichlet_exprs[i]))) { delete h; return rc; }
 	}
 	build_dofmap(h);
 	cudaError_t e;
@@ -199,6 +238,25 @@ int rsd_heat_matrix(rsd_heat* h, rsd_csr** A) {
 	return RSD_OK;
 }
 
+int rsd_heat_create_matrix(rsd_ctx* ctx, rsd_heat* h, rsd_csr** A) {
+	if (!ctx || !h || !A) return set_error(RSD_EINVAL, "null argument");
+	RSD_CUDA(cudaSetDevice(ctx->device));
+	return share_pattern(ctx, h->K, A);
+}
+
+int rsd_heat_eval_nodal(rsd_ctx* ctx, rsd_heat* h, const char* expr, double t, double* U) {
+	if (!ctx || !h || !expr || (h->n && !U)) return set_error(RSD_EINVAL, "null argument");
+	DevExpr f;
+	RSD_CHECK(compile_expr(expr, &f));
+	const int64_t nn = h->m->nnodes;
+	if (nn) {
+		k_eval_nodal<<<vec_grid(ctx, nn), 256, 0, ctx->stream>>>(nn, h->t2a, h->m->xyz, h->m->nsd, f, t, U);
+		RSD_CUDA(cudaGetLastError());
+	}
+	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+	return RSD_OK;
+}
+
 int rsd_heat_set_time(rsd_ctx* ctx, rsd_heat* h, double t) {
 	if (!ctx || !h) return set_error(RSD_EINVAL, "null argument");
 	h->time = t;
@@ -254,6 +312,17 @@ int rsd_heat_solve_fem(rsd_ctx* ctx, rsd_heat* h, double c_mass, const rsd_solve
                        rsd_report* rep) {
 	if (!ctx || !h || !cfg) return set_error(RSD_EINVAL, "null argument");
 	return solve_fem(ctx, h, c_mass, cfg, b, x, rep);
+}
+
+int rsd_heat_solve_fem_forms(rsd_ctx* ctx, rsd_heat* h, double c_tdiff, double c_mass, double c_tmass, const double* U,
+                             const double* Udot, const rsd_solver_cfg* cfg, const double* b, double* x, rsd_report* rep) {
+	if (!ctx || !h || !cfg) return set_error(RSD_EINVAL, "null argument");
+	if (!std::isfinite(c_tdiff) || !std::isfinite(c_mass) || !std::isfinite(c_tmass)) return set_error(RSD_EINVAL, "form coefficients must be finite");
+	// the state is the iterate itself when none is given or when it is the solution vector (the
+	// stages bind the state to the vector the solver updates)
+	const double* state = (U == nullptr || U == x) ? nullptr : U;
+	if (c_tdiff == 0.0 && c_tmass == 0.0) return solve_fem(ctx, h, c_mass, cfg, b, x, rep, 4, state);
+	return solve_fem(ctx, h, c_mass, cfg, b, x, rep, 10, state, c_tdiff, c_tmass, Udot);
 }
 
 int rsd_apply_dirichlet_lift(rsd_ctx* ctx, rsd_heat* h, double cd, double cm, double* F) {
@@ -420,6 +489,11 @@ int rsd_heat_newton(rsd_ctx* ctx, rsd_heat* h, double abs_tol, double rel_tol, i
 static int adjoint_check(rsd_ctx* ctx, rsd_heat* h, const double* theta, const rsd_solver_cfg* cfg) {
 	if (!ctx || !h || !theta || !cfg) return set_error(RSD_EINVAL, "null argument");
 	if (h->kExpr.n) return set_error(RSD_EINVAL, "the adjoint pair needs a constant conductivity (k_expr unset)");
+	if (h->aniso)
+		for (int i = 0; i < 3; ++i)
+			for (int j = 0; j < i; ++j)
+				if (h->kS[i * 3 + j] != h->kS[j * 3 + i])
+					return set_error(RSD_EINVAL, "the adjoint pair solves K^T with K: the conductivity tensor must be symmetric");
 	if (!h->kElem) RSD_CUDA(cudaMalloc(&h->kElem, sizeof(double) * std::max<int64_t>(h->m->nelem, 1)));
 	const int64_t ne = h->m->nelem;
 	if (ne) {

@@ -113,6 +113,7 @@ struct rsd_csr {
 	// sOffs[sUni[s] + j] = column - row of entry j; the slice's columns are then not read
 	int32_t* sUni = nullptr;       // nslices (or null when no slice qualifies)
 	int32_t* sOffs = nullptr;      // distinct patterns, concatenated
+	int64_t nStencil = 0;          // slices stored as stencil slices
 	bool csrValid = true, sellValid = false;
 	int format = 0;                // SpMV layout: 0 SELL-32 (narrow columns when present), 1 CSR vector with `lanes` lanes per row
 	int lanes = 0;                 // CSR SpMV lanes per row (0: default from nnz/row)
@@ -131,6 +132,7 @@ int csr_sync(rsd_ctx* ctx, rsd_csr* A);      // CSR values current (from SELL if
 int f32_sync(rsd_ctx* ctx, rsd_csr* A);      // FP32 copy current, in the execution layout
 void free_graph_cache(rsd_ctx* ctx);         // release the context's cached solve graphs
 int exec_sync(rsd_ctx* ctx, rsd_csr* A);     // FP64 values current in the execution layout
+int share_pattern(rsd_ctx* ctx, const rsd_csr* src, rsd_csr** out);   // src's pattern, own zero values
 }  // namespace rsd
 
 namespace rsd {
@@ -139,9 +141,11 @@ namespace rsd {
 // expressions: host compiler + device stack machine (bytecode shared by every kernel)
 // ---------------------------------------------------------------------------------------------
 constexpr int kExprMax = 48;
+constexpr int kExprStack = 16;   // evaluation stack of the device machine
 enum ExprOp : int8_t { E_CONST, E_VAR, E_ADD, E_SUB, E_MUL, E_DIV, E_POW, E_NEG, E_SIN, E_COS, E_TAN, E_EXP, E_LOG, E_SQRT, E_ABS };
 struct DevExpr {
 	int32_t n = 0;          // 0: expression absent
+	int32_t depth = 0;      // evaluation stack depth the program needs (at most kExprStack)
 	int8_t op[kExprMax];
 	int8_t arg[kExprMax];   // variable index (t x y z T) for E_VAR, constant slot for E_CONST
 	double c[kExprMax];
@@ -184,9 +188,14 @@ struct rsd_heat {
 	int32_t nq1 = 2;                // Gauss points per direction
 	double k_const = 1.0, rho = 1.0, cp = 1.0;
 	rsd::DevExpr kExpr, dkExpr, srcExpr;
-	rsd::DevExpr bcExpr[6];
-	bool essential[6] = {false, false, false, false, false, false};
-	std::vector<int32_t> h_t2a, h_a2t, h_ctag;
+	rsd::DevExpr cpExpr, dcpExpr;   // cp(T), dcp/dT (SpecificHeatModel, TemperatureDependent)
+	bool aniso = false;             // K = k * kS (ConductivityModel, Anisotropic): kS nsd x nsd row-major
+	double kS[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+	// essential boundary tags (any value >= 0) and their Dirichlet expressions, in registration order
+	std::vector<int32_t> essTags;
+	std::vector<rsd::DevExpr> bcExpr;
+	std::vector<int32_t> h_t2a, h_a2t;
+	std::vector<int32_t> h_ctag;     // per node: index into essTags / bcExpr of its constraint, -1 if free
 	int64_t n = 0;
 	int32_t* t2a = nullptr;         // device, per node (-1: constrained)
 	double* g = nullptr;            // device, Dirichlet value per node at the current time
@@ -211,13 +220,14 @@ struct rsd_heat {
 	int32_t* adjPtr = nullptr;      // device, n + 1
 	int32_t* adj = nullptr;         // device, e * npe + a
 	int32_t* erow = nullptr;        // device, [e][a]: t2a[ien[e][a]] (sum-factorized operator products), or null
-	rsd::DevExpr fluxExpr[18];      // flux boundary conditions: [tag][component]
-	bool hasFlux[6] = {false, false, false, false, false, false};
+	// flux boundary conditions: tag -> one expression per spatial component (three slots per tag)
+	std::vector<int32_t> fluxTags;
+	std::vector<rsd::DevExpr> fluxExpr;
 	rsd::DevExpr* dFlux = nullptr;  // device copy of fluxExpr
-	int32_t* nFaces = nullptr;      // device: (element, face, tag) of the faces whose tag carries a flux
+	int32_t* nFaces = nullptr;      // device: (element, face, flux index) of the faces whose tag carries a flux
 	int64_t nnFaces = 0;
 	rsd::DevExpr* dBc = nullptr;    // device copy of bcExpr
-	int32_t* cNodes = nullptr;      // device: the constrained nodes, then their constraint tags
+	int32_t* cNodes = nullptr;      // device: the constrained nodes, then their bcExpr indices
 	int64_t ncNodes = 0;
 	bool adjTried = false;
 	int32_t maxSlice = 0;           // longest SELL-32 slice of K, in entries per row
@@ -236,17 +246,21 @@ int assemble_matrix(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, doubl
 int assemble_vector(rsd_ctx* ctx, rsd_heat* h, int which, double coef, const double* U, const double* Udot,
                     const double* operand, double* out, double outScale, bool accumulate);
 int assemble_diagonal(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, const double* U, double* d,
-                      double cTDiff = 0.0);
+                      double cTDiff = 0.0, double cTMass = 0.0, const double* Udot = nullptr);
 int assemble_lift(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, double* F);
-// which 4: Diffusion + coef Mass (the stages' operator); 10: Diffusion + TangentDiffusion + coef Mass
-// (Newton's Jacobian), both with the state U read through k(T), dk/dT and grad T
+// which 4: Diffusion + coef Mass (the stages' operator); 10: Diffusion + cTDiff TangentDiffusion + coef Mass
+// + cTMass TangentMass (the Jacobian), both with the state U read through k(T), cp(T), dk/dT and grad T,
+// and the rate Udot read by TangentMass
 int apply_operator(rsd_ctx* ctx, rsd_heat* h, double coef, const double* U, const double* V, double* out,
-                   const int32_t* skip, int which = 4);
+                   const int32_t* skip, int which = 4, double cTDiff = 1.0, double cTMass = 0.0,
+                   const double* Udot = nullptr);
 int set_flux(rsd_ctx* ctx, rsd_heat* h, int tag, const char* const* exprs);
 int apply_natural(rsd_ctx* ctx, rsd_heat* h, double* F);
 int nodal_field(rsd_ctx* ctx, rsd_heat* h, int field, const double* U, double* out, double* scratch);
-// state null: the iterate x is the state (the stages' linear solves); which as for apply_operator
+// state null: the iterate x is the state (the stages' linear solves); which, cTDiff, cTMass and Udot as
+// for apply_operator
 int solve_fem(rsd_ctx* ctx, rsd_heat* h, double coef, const rsd_solver_cfg* cfg, const double* b, double* x,
-              rsd_report* rep, int which = 4, const double* state = nullptr);
+              rsd_report* rep, int which = 4, const double* state = nullptr, double cTDiff = 1.0,
+              double cTMass = 0.0, const double* Udot = nullptr);
 int build_tables(rsd_ctx* ctx, rsd_heat* h);
 }  // namespace rsd

@@ -367,9 +367,9 @@ __host__ __device__ __forceinline__ double next_delta(double delta, double recur
 	return fmin(0.1, fmax(lo, 100.0 * d * delta));
 }
 
-// expression stack machine (bytecode from compile_expr)
+// expression stack machine (bytecode from compile_expr, which rejects programs deeper than kExprStack)
 __device__ __forceinline__ double eval_expr(const DevExpr& e, double t, double x, double y, double z, double T) {
-	double st[16];
+	double st[kExprStack];
 	int sp = 0;
 	for (int i = 0; i < e.n; ++i) {
 		const int op = e.op[i];
@@ -391,7 +391,6 @@ __device__ __forceinline__ double eval_expr(const DevExpr& e, double t, double x
 			case E_SQRT: st[sp - 1] = sqrt(st[sp - 1]); break;
 			default: st[sp - 1] = fabs(st[sp - 1]); break;
 		}
-		if (sp >= 16) return 0.0;
 	}
 	return e.n ? st[0] : 0.0;
 }

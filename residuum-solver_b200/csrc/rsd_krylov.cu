@@ -857,7 +857,7 @@ __global__ void __launch_bounds__(256) k_fem_true_res(int64_t n, const double* _
 // Plain launches in chunks of 8 iterations behind a done-flag poll; after the solve has finished the
 // remaining launches of a chunk return at once (the element pass through its skip flag).
 static int cg_fem(rsd_ctx* ctx, rsd_heat* h, double coef, const rsd_solver_cfg* cfg, const double* b, double* x,
-                  rsd_report* rep, int which, const double* state) {
+                  rsd_report* rep, int which, const double* state, double cTD, double cTM, const double* Udot) {
 	const double* U = state ? state : x;   // the operator's state
 	const int64_t n = h->n;
 	void* wsv;
@@ -878,10 +878,10 @@ static int cg_fem(rsd_ctx* ctx, rsd_heat* h, double coef, const rsd_solver_cfg* 
 	RSD_CUDA(cudaMemsetAsync(S, 0, sizeof(CgScal), st));
 	// Jacobi::update on every solve (cg/Solver.tpp:22); the operator's state is the iterate x
 	if (invD) {
-		RSD_CHECK(assemble_diagonal(ctx, h, 1.0, coef, U, invD, which == 10 ? 1.0 : 0.0));
+		RSD_CHECK(assemble_diagonal(ctx, h, 1.0, coef, U, invD, which == 10 ? cTD : 0.0, which == 10 ? cTM : 0.0, Udot));
 		k_inv_guarded<<<vec_grid(ctx, n), 256, 0, st>>>(n, invD);
 	}
-	RSD_CHECK(apply_operator(ctx, h, coef, U, x, r, nullptr, which));
+	RSD_CHECK(apply_operator(ctx, h, coef, U, x, r, nullptr, which, cTD, cTM, Udot));
 	k_fem_init<<<VG(k_fem_init), 256, 0, st>>>(n, b, r, p, invD, S, partials, tol, rel, maxIt);
 	RSD_CUDA(cudaGetLastError());
 	Poller poll{ctx, S, (int32_t*)ctx->s.hbuf};
@@ -891,7 +891,7 @@ static int cg_fem(rsd_ctx* ctx, rsd_heat* h, double coef, const rsd_solver_cfg* 
 	const GraphCtl off{0, 0, 0, 0};
 	for (int64_t it = 0; it < maxIt + 2 * chunk && !fin; it += chunk) {
 		for (int c = 0; c < chunk; ++c) {
-			RSD_CHECK(apply_operator(ctx, h, coef, U, p, Ap, &S->done, which));
+			RSD_CHECK(apply_operator(ctx, h, coef, U, p, Ap, &S->done, which, cTD, cTM, Udot));
 			k_fem_alpha<<<VG(k_fem_alpha), 256, 0, st>>>(n, p, Ap, S, partials);
 			k_cg_update<<<VGB(k_cg_update, kVT), kVT, 0, st>>>(n, x, r, p, Ap, invD, S, partials, tol, rel, maxIt, xvec);
 			k_cg_pupdate<<<VGB(k_cg_pupdate, kVT), kVT, 0, st>>>(n, p, r, invD, S, off);
@@ -901,7 +901,7 @@ static int cg_fem(rsd_ctx* ctx, rsd_heat* h, double coef, const rsd_solver_cfg* 
 	}
 	RSD_CHECK(finish_report(ctx, S, rep));
 	// FP64 check of the final iterate: ||b - A x||
-	RSD_CHECK(apply_operator(ctx, h, coef, U, x, Ap, nullptr, which));
+	RSD_CHECK(apply_operator(ctx, h, coef, U, x, Ap, nullptr, which, cTD, cTM, Udot));
 	k_fem_true_res<<<VG(k_fem_true_res), 256, 0, st>>>(n, b, Ap, partials, &S1->ticket, &S1->res);
 	RSD_CUDA(cudaGetLastError());
 	double hres = 0.0;
@@ -1069,9 +1069,11 @@ struct GmFemOp {
 	int64_t n;
 	int which;
 	const double* state;   // null: the iterate
+	double cTD, cTM;       // TangentDiffusion / TangentMass coefficients of the Jacobian's product (which 10)
+	const double* Udot;
 	int prepare() { return RSD_OK; }
 	int invdiag(double* invD, const double* x) {
-		RSD_CHECK(assemble_diagonal(ctx, h, 1.0, coef, state ? state : x, invD, which == 10 ? 1.0 : 0.0));
+		RSD_CHECK(assemble_diagonal(ctx, h, 1.0, coef, state ? state : x, invD, which == 10 ? cTD : 0.0, which == 10 ? cTM : 0.0, Udot));
 		k_inv_guarded<<<vec_grid(ctx, n), 256, 0, ctx->stream>>>(n, invD);
 		RSD_CUDA(cudaGetLastError());
 		return RSD_OK;
@@ -1079,9 +1081,9 @@ struct GmFemOp {
 	int prec_apply(const double* q, const double* invD, double* w, double* tmp, const double* x) {
 		k_gm_scale_by<<<vec_grid(ctx, n), 256, 0, ctx->stream>>>(n, q, invD, tmp);
 		RSD_CUDA(cudaGetLastError());
-		return apply_operator(ctx, h, coef, state ? state : x, tmp, w, nullptr, which);
+		return apply_operator(ctx, h, coef, state ? state : x, tmp, w, nullptr, which, cTD, cTM, Udot);
 	}
-	int apply64(const double* x, double* Ax) { return apply_operator(ctx, h, coef, state ? state : x, x, Ax, nullptr, which); }
+	int apply64(const double* x, double* Ax) { return apply_operator(ctx, h, coef, state ? state : x, x, Ax, nullptr, which, cTD, cTM, Udot); }
 };
 
 template <typename T, typename Op>
@@ -1297,7 +1299,7 @@ static int cg_fp64_static(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, c
 }  // namespace
 
 int solve_fem(rsd_ctx* ctx, rsd_heat* h, double coef, const rsd_solver_cfg* cfg, const double* b, double* x,
-              rsd_report* rep, int which, const double* state) {
+              rsd_report* rep, int which, const double* state, double cTD, double cTM, const double* Udot) {
 	if (!ctx || !h || !cfg || (h->n && (!b || !x))) return set_error(RSD_EINVAL, "null argument");
 	if (cfg->max_iters < 0 || !(cfg->tol >= 0)) return set_error(RSD_EINVAL, "bad solver configuration");
 	if (cfg->type != RSD_CG && cfg->type != RSD_GMRES) return set_error(RSD_EINVAL, "unknown solver type");
@@ -1307,10 +1309,10 @@ int solve_fem(rsd_ctx* ctx, rsd_heat* h, double coef, const rsd_solver_cfg* cfg,
 	if (h->n == 0) { if (rep) rep->converged = 1; return RSD_OK; }
 	RSD_CUDA(cudaSetDevice(ctx->device));
 	if (cfg->type == RSD_GMRES) {
-		GmFemOp op{ctx, h, coef, h->n, which, state};
+		GmFemOp op{ctx, h, coef, h->n, which, state, cTD, cTM, Udot};
 		return gmres_core<double>(ctx, op, cfg, b, x, rep);
 	}
-	return cg_fem(ctx, h, coef, cfg, b, x, rep, which, state);
+	return cg_fem(ctx, h, coef, cfg, b, x, rep, which, state, cTD, cTM, Udot);
 }
 
 int solve(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const double* b, double* x, rsd_report* rep) {
