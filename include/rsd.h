@@ -85,6 +85,11 @@ int rsd_ctx_sync(rsd_ctx* ctx);
 void* rsd_ctx_stream(rsd_ctx* ctx);
 const char* rsd_last_error_string(void);
 int rsd_version(int32_t* major, int32_t* minor);
+/* Compile an expression (the subset the heat problem's expression strings take) on the host without a
+ * device: RSD_OK and the evaluation stack depth its program needs, or RSD_EPARSE with the reason,
+ * e.g. a depth above the device machine's 16 entries.  No counterpart in the reference (exprtk
+ * compiles in the reference's ScalarExpression / TemperatureExpression constructors). */
+int rsd_expr_check(const char* expr, int32_t* depth);
 /* Tracing (the reference has only its benchmark Timer, include/benchmark/core/Timer.hpp:10-24):
  * when enabled, every launch of the kernel families "spmv_dot_f64", "spmv_dot_f32", "cg_update",
  * "cg_pupdate", "reliable_update", "assemble_matrix", "assemble_vector", "spmv" is bracketed by

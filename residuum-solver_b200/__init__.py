@@ -69,6 +69,7 @@ SIGNATURES = {
     "rsd_ctx_stream": [_P],
     "rsd_last_error_string": [],
     "rsd_version": [C.POINTER(_I32), C.POINTER(_I32)],
+    "rsd_expr_check": [C.c_char_p, C.POINTER(_I32)],
     "rsd_ctx_profile": [_P, _I32],
     "rsd_ctx_profile_get": [_P, C.c_char_p, C.POINTER(_I64), C.POINTER(_D)],
     "rsd_alloc": [_P, _SZ, C.POINTER(_P)],
@@ -151,6 +152,13 @@ def lib():
         L.rsd_ctx_stream.restype = _P
         _lib = L
     return _lib
+
+
+def expr_check(expr):
+    """Compile an expression on the host: the stack depth its device program needs (RsdError if rejected)."""
+    depth = _I32()
+    check(lib().rsd_expr_check(expr.encode(), C.byref(depth)))
+    return depth.value
 
 
 def check(rc):

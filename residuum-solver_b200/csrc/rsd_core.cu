@@ -576,6 +576,14 @@ int rsd_ctx_profile_get(rsd_ctx* c, const char* family, int64_t* launches, doubl
 
 const char* rsd_last_error_string(void) { return g_last_error.c_str(); }
 
+int rsd_expr_check(const char* expr, int32_t* depth) {
+	if (!expr) return set_error(RSD_EINVAL, "null expression");
+	DevExpr e;
+	RSD_CHECK(compile_expr(expr, &e));
+	if (depth) *depth = e.depth;
+	return RSD_OK;
+}
+
 int rsd_version(int32_t* major, int32_t* minor) {
 	if (major) *major = 0;
 	if (minor) *minor = 1;

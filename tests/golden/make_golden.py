@@ -1,10 +1,11 @@
 """Generate the golden fixtures in this folder from the reference's own templates.
 
-    python tests/golden/make_golden.py [main] [adjoint] [fem]
+    python tests/golden/make_golden.py [main] [adjoint] [fem] [models]
 
 Every array comes from oracle/_ref/libresiduum_ref.so, i.e. the unmodified Residuum templates
 (Assembler<CPU>, BoundaryApplicator<CPU>, TopologicalDOF, cg/gmres::Solver, SteadyStage,
-BackwardEulerStage, NewtonRunner) compiled from the reference tree by oracle/Makefile.  The
+BackwardEulerStage, NewtonRunner, and for the `models` group HeatProblem itself with its
+ConductivityModel and SpecificHeatModel) compiled from the reference tree by oracle/Makefile.  The
 fixtures are small so that the GPU tests can pin the CUDA path to the reference on a machine
 without the reference tree.
 """
@@ -157,7 +158,40 @@ def fem():
     save("fem_steady_q2_hex_kT.npz", U=U, iterations=rep["iterations"], converged=rep["converged"])
 
 
-GROUPS = {"main": main, "adjoint": adjoint, "fem": fem}
+# the conductivity tensor of the model fixtures: not symmetric, so that K = k kS and kS^T cannot be
+# confused
+ANISO_3D = [[2.0, 0.3, 0.0], [0.1, 1.0, 0.2], [0.0, 0.05, 0.5]]
+
+
+def models():
+    """Fixtures from the reference's own HeatProblem (oracle/ref_problem.cpp, its ConductivityModel and
+    SpecificHeatModel): anisotropic k(T), cp(T) with TangentMass, a renumbered Dirichlet tag (block
+    tag 0 -> 9), a flux boundary and an expression source; and a steady Q2 quad with a constant
+    anisotropic tensor and a renumbered tag (3 -> 7)."""
+    r = oracle.RefProblem(3, 1, 2, [4, 3, 3], [0, 0, 0], [1, 1, 1],
+                          conductivity=("k(T) tensor", ANISO_3D, "1 + 0.2*T", "0.2"), rho=2.0,
+                          specific_heat=("cp(T)", "1 + 0.3*T", "0.3"), source="1 + x*y",
+                          bcs=[(9, "value", "0"), (1, "value", "1 + x*y"), (2, "flux", ["1 + y", "0.5", "0"])],
+                          tag_map={0: 9}, solver=dict(type="gmres", tol=1e-12, newton=(1e-10, 1e-10, 30), transient=(0.0, 0.03, 0.01)))
+    rng = np.random.default_rng(11)
+    U = 0.3 * rng.standard_normal(r.n) + 0.5
+    Ud = rng.standard_normal(r.n)
+    rp, col = r.pattern()
+    t = 0.3
+    save("models_aniso_kT_cpT_hex.npz", t2a=r.dofmap(), row_ptr=rp, col=col, U=U, Udot=Ud, t=t, tensor=np.array(ANISO_3D),
+         K=r.assemble_matrix(0, t=t, U=U, Udot=Ud), K_cM=r.assemble_matrix(1, 50.0, t=t, U=U, Udot=Ud),
+         K_KT=r.assemble_matrix(2, t=t, U=U, Udot=Ud), J_BE=r.assemble_matrix(3, 50.0, t=t, U=U, Udot=Ud),
+         F_natural=r.assemble_vector(0, t=t, U=U, Udot=Ud), R_diff=r.assemble_vector(1, t=t, U=U, Udot=Ud),
+         M_Udot=r.assemble_vector(2, t=t, U=U, Udot=Ud))
+    tensor2 = [[1.5, 0.4], [0.4, 0.8]]
+    r = oracle.RefProblem(2, 2, 3, [6, 5], [0, 0], [1, 1], conductivity=("anisotropic", tensor2), source="2 - x",
+                          bcs=[(0, "value", "x*y"), (7, "value", "1")], tag_map={3: 7}, solver=dict(tol=1e-12))
+    Us, ok = r.run()
+    assert ok
+    save("models_aniso_quad_q2.npz", t2a=r.dofmap(), tensor=np.array(tensor2), U=Us)
+
+
+GROUPS = {"main": main, "adjoint": adjoint, "fem": fem, "models": models}
 
 if __name__ == "__main__":
     if not oracle.reference_available():

@@ -48,3 +48,32 @@ def test_no_device_fails_loudly():
         assert e.code in (-1, -3)
     else:
         raise AssertionError("context creation succeeded without a CUDA device")
+
+
+def nested(depth):
+    """1 + (1 + (... (1 + 1))): a right-nested sum whose postfix program needs `depth` stack entries."""
+    e = "1"
+    for _ in range(depth - 1):
+        e = f"1 + ({e})"
+    return e
+
+
+def test_expression_stack_depth_is_bounded_at_compile_time():
+    # the device evaluates expressions on a 16-entry stack: a deeper program is rejected when it is
+    # compiled (RSD_EPARSE), never evaluated to a silent value
+    rsd = load_package()
+    assert rsd.expr_check(nested(16)) == 16
+    try:
+        rsd.expr_check(nested(17))
+    except rsd.RsdError as e:
+        assert e.code == -7 and "stack" in str(e)
+    else:
+        raise AssertionError("a 17-deep expression was accepted")
+    assert rsd.expr_check("1 + 0.5*T") == 3
+    assert rsd.expr_check("sin(pi*x)*sin(pi*y) + t^2") >= 2
+    try:
+        rsd.expr_check("1 + q")
+    except rsd.RsdError as e:
+        assert e.code == -7
+    else:
+        raise AssertionError("an unknown symbol was accepted")

@@ -1,0 +1,97 @@
+"""Device models against fixtures from the reference's own HeatProblem (ConductivityModel with an
+anisotropic k(T) tensor, SpecificHeatModel with cp(T), TangentMassForm, Dirichlet and flux tags outside
+0..5), through the C ABI: DOF map bit-exact, assembled matrices and vectors and a steady solution at
+1e-12 relative."""
+import numpy as np
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+def block(rsd, nsd, nel, order, retag):
+    from importlib import import_module
+    bm = import_module("residuum_solver_b200.blockmesh")
+    xyz, ien, rng = bm.block_mesh(nsd, nel, [0] * nsd, [1] * nsd, order)
+    rng = rng.copy()
+    for a, b in retag.items():
+        rng[rng == a] = b
+    return xyz, ien, rng
+
+
+def rel(a, b):
+    return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / max(np.max(np.abs(b)), 1e-300))
+
+
+def test_anisotropic_kT_cpT_tangent_mass_and_tags(rsd, ctx):
+    g = golden("models_aniso_kT_cpT_hex.npz")
+    xyz, ien, rng = block(rsd, 3, [4, 3, 3], 1, {0: 9})
+    h = rsd.Heat(ctx, rsd.Mesh(ctx, 3, 1, xyz, ien, rng), 2, k_expr="1 + 0.2*T", dk_expr="0.2", k_tensor=g["tensor"],
+                 rho=2.0, cp_expr="1 + 0.3*T", dcp_expr="0.3", src_expr="1 + x*y",
+                 dirichlet={9: "0", 1: "1 + x*y"}, flux={2: ("1 + y", "0.5", "0")})
+    t2a, _ = h.dofmap()
+    assert (t2a == g["t2a"]).all()
+    rp, col = h.K.pattern()
+    assert (rp == g["row_ptr"]).all() and (col == g["col"]).all()
+    t = float(g["t"])
+    h.set_time(t)
+    U, Ud = ctx.to_device(g["U"]), ctx.to_device(g["Udot"])
+    for key, c in (("K", (1.0, 0.0, 0.0, 0.0)), ("K_cM", (1.0, 50.0, 0.0, 0.0)), ("K_KT", (1.0, 0.0, 1.0, 0.0)),
+                   ("J_BE", (1.0, 50.0, 1.0, 1.0))):
+        h.assemble_matrix(*c, U=U, Udot=Ud)
+        assert rel(h.K.values(), g[key]) <= 1e-12, key
+    out = ctx.array(h.n)
+    h.assemble_vector(0, out)
+    h.apply_natural(out)
+    assert rel(out.download(), g["F_natural"]) <= 1e-12
+    h.assemble_vector(1, out, U=U)
+    assert rel(out.download(), g["R_diff"]) <= 1e-12
+    h.assemble_vector(3, out, U=U, Udot=Ud)   # rho cp(T(U)) Mass on Udot
+    assert rel(out.download(), g["M_Udot"]) <= 1e-12
+    # the matrix-free Jacobian product (Diffusion + TangentDiffusion + c Mass + TangentMass) inverts the
+    # assembled Jacobian's SpMV
+    v = ctx.to_device(np.cos(np.arange(h.n) * 0.3))
+    h.assemble_matrix(1.0, 50.0, 1.0, 1.0, U=U, Udot=Ud)
+    y1 = ctx.array(h.n)
+    h.K.spmv(v, y1)
+    b = ctx.to_device(y1.download())
+    x = ctx.array(h.n).zero()
+    rep = h.solve_fem_forms(b, x, c_tdiff=1.0, c_mass=50.0, c_tmass=1.0, U=U, Udot=Ud, type=rsd.GMRES, tol=1e-13,
+                            max_iters=5000, krylov_dim=30)
+    assert rep["converged"]
+    assert rel(x.download(), v.download()) <= 1e-9
+
+
+def test_constant_anisotropic_steady_q2_quad(rsd, ctx):
+    g = golden("models_aniso_quad_q2.npz")
+    xyz, ien, rng = block(rsd, 2, [6, 5], 2, {3: 7})
+    h = rsd.Heat(ctx, rsd.Mesh(ctx, 2, 2, xyz, ien, rng), 3, k_const=1.0, k_tensor=g["tensor"], src_expr="2 - x",
+                 dirichlet={0: "x*y", 7: "1"})
+    t2a, _ = h.dofmap()
+    assert (t2a == g["t2a"]).all()
+    U = ctx.array(h.n).zero()
+    for op in (rsd.OP_CSR, rsd.OP_FEM):
+        U.zero()
+        rep = h.steady(U, tol=1e-12, max_iters=5000, operator_type=op)
+        assert rep["converged"]
+        assert rel(U.download(), g["U"]) <= 1e-10, op
+
+
+def test_adjoint_rejects_a_nonsymmetric_tensor(rsd, ctx):
+    xyz, ien, rng = block(rsd, 3, [2, 2, 2], 1, {})
+    h = rsd.Heat(ctx, rsd.Mesh(ctx, 3, 1, xyz, ien, rng), 2, k_tensor=[[1, 0.5, 0], [0, 1, 0], [0, 0, 1]], src_expr="1",
+                 dirichlet={t: "0" for t in range(6)})
+    theta, T = ctx.array(8).zero(), ctx.array(h.n).zero()
+    with pytest.raises(rsd.RsdError):
+        h.forward(theta, T, tol=1e-10)
+
+
+def test_initial_condition_expression(rsd, ctx):
+    xyz, ien, rng = block(rsd, 3, [3, 2, 2], 1, {})
+    h = rsd.Heat(ctx, rsd.Mesh(ctx, 3, 1, xyz, ien, rng), 2, dirichlet={0: "0"})
+    t2a, a2t = h.dofmap()
+    U = ctx.array(h.n)
+    h.eval_nodal("x*y + 2*z + t", U, t=0.5)
+    X = xyz.reshape(-1, 3)[a2t]
+    assert np.allclose(U.download(), X[:, 0] * X[:, 1] + 2 * X[:, 2] + 0.5, rtol=1e-15, atol=1e-15)
