@@ -328,6 +328,26 @@ int rsd_heat_forward(rsd_ctx* ctx, rsd_heat* h, const double* theta, const rsd_s
 int rsd_heat_backward(rsd_ctx* ctx, rsd_heat* h, const double* theta, const double* T, const double* dJdT,
                       const rsd_solver_cfg* cfg, double* dJdtheta, rsd_report* report);
 
+/* ---- transient adjoint pair, in the shape of an autograd Function (no counterpart in the
+ * reference): the linear Backward-Euler steps of rsd_heat_be_step (BackwardEulerStage.hpp:71-124)
+ * with k_e = k_const * exp(theta_e), constant cp and the assembled operator.
+ * forward:  U = the state after nsteps steps of dt from U0 at time t0 (U0, U device, num_free);
+ *           report: iterations summed over the steps, converged if every step converged.
+ * backward: dJdtheta (device, one per element) = the gradient of a terminal objective J(U_N) whose
+ *           derivative dJdU (device, num_free) is given, by the discrete adjoint of the same steps:
+ *           mu_N = A^-1 dJ/dU_N, mu_k = A^-1 M mu_{k+1} / dt with A = K + M/dt, and
+ *           dJ/dtheta_e = -k_e sum_k int_e grad mu_k . K0 grad U_k.  The forward states are recomputed,
+ *           not kept: every ceil(sqrt(nsteps))-th state is checkpointed and each segment is replayed
+ *           from its checkpoint during the reverse sweep, so about 2 sqrt(nsteps) states are held
+ *           (states_held, may be NULL) for about nsteps extra forward steps.  report: iterations = the
+ *           adjoint solves' total, refinements = the forward solves' total (replays included).
+ * The conductivity tensor, if any, must be symmetric (A^T = A); k_expr and cp_expr must be unset. */
+int rsd_heat_transient_forward(rsd_ctx* ctx, rsd_heat* h, const double* theta, double t0, double dt, int64_t nsteps,
+                               const rsd_solver_cfg* cfg, const double* U0, double* U, rsd_report* report);
+int rsd_heat_transient_backward(rsd_ctx* ctx, rsd_heat* h, const double* theta, double t0, double dt, int64_t nsteps,
+                                const double* U0, const double* dJdU, const rsd_solver_cfg* cfg, double* dJdtheta,
+                                rsd_report* report, int64_t* states_held);
+
 #ifdef __cplusplus
 }
 #endif

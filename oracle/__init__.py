@@ -630,3 +630,34 @@ class RefProblem:
         if L.refp_assemble_vector(self.h, which, t, _ptr(_f64(U)), _ptr(_f64(Udot)), _ptr(out)):
             raise RuntimeError(L.refp_last_error().decode())
         return out
+
+
+def ref_transient_adjoint(nel, theta, U0, dt, nsteps, Uobs, bc_val=None, tol=1e-14):
+    """FP64 CPU discrete adjoint of `nsteps` Backward-Euler steps on the reference's own templates:
+    3D Q1 block mesh, k_e = exp(theta_e), f = 1, Dirichlet constants `bc_val` (default 0) on every face,
+    J = 0.5 ||U_N - Uobs||^2.  Forward steps by the reference's BackwardEulerStage; adjoint solves by its
+    cg::Solver + Jacobi on its assembled K + M/dt; element terms by its DiffusionForm
+    (ref_adjoint_gradient).  Returns (U_N, J, dJ/dtheta, the reference's CG iterations)."""
+    bcs = {t: 0.0 for t in range(6)}
+    bcs.update(bc_val or {})
+    r = Reference(3, 1, 2, nel, [0, 0, 0], [1, 1, 1], list(range(6)), bc_kind=0, bc_val=bcs, src_kind=0, src_c=1.0,
+                  k_elem=np.exp(theta))
+    states = [np.array(U0, dtype=np.float64)]
+    for _ in range(nsteps):
+        U, _, rc = r.backward_euler(dt, 1, states[-1], tol=tol, maxit=100000)
+        if rc:
+            raise RuntimeError("reference step did not converge")
+        states.append(U)
+    rp, col = r.pattern()
+    A = r.assemble_matrix("K+cM", 1.0 / dt)
+    mu_next = np.zeros(r.n)
+    g = np.zeros(len(theta))
+    its = 0
+    for k in range(nsteps, 0, -1):
+        b = states[-1] - Uobs if k == nsteps else r.assemble_vector(3, Udot=mu_next) / dt
+        mu, rep = ref_csr_solve(rp, col, A, b, x0=mu_next, tol=tol, maxit=100000)
+        its += int(rep["iterations"])
+        g += r.adjoint_gradient(states[k], mu)
+        mu_next = mu
+    J = 0.5 * float(np.sum((states[-1] - Uobs) ** 2))
+    return states[-1], J, -np.exp(theta) * g, its

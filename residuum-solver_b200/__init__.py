@@ -134,6 +134,9 @@ SIGNATURES = {
     "rsd_batch_solve": [_P, _P, C.POINTER(SolverConfig), _P, _P, _P],
     "rsd_heat_forward": [_P, _P, _P, C.POINTER(SolverConfig), _P, C.POINTER(Report)],
     "rsd_heat_backward": [_P, _P, _P, _P, _P, C.POINTER(SolverConfig), _P, C.POINTER(Report)],
+    "rsd_heat_transient_forward": [_P, _P, _P, _D, _D, _I64, C.POINTER(SolverConfig), _P, _P, C.POINTER(Report)],
+    "rsd_heat_transient_backward": [_P, _P, _P, _D, _D, _I64, _P, _P, C.POINTER(SolverConfig), _P, C.POINTER(Report),
+                                    C.POINTER(_I64)],
 }
 
 
@@ -575,6 +578,27 @@ class Heat:
         check(lib().rsd_heat_backward(self.ctx.h, self.h, _ptr(theta), _ptr(T), _ptr(dJdT), C.byref(cfg),
                                       _ptr(dJdtheta), C.byref(rep)))
         return rep.as_dict()
+
+    def transient_forward(self, theta, U0, U, t0, dt, nsteps, cfg=None, **kw):
+        """Transient pair, forward: U = the state after nsteps Backward-Euler steps from U0 with
+        k_e = k_const exp(theta_e)."""
+        cfg = cfg or SolverConfig.make(**kw)
+        rep = Report()
+        check(lib().rsd_heat_transient_forward(self.ctx.h, self.h, _ptr(theta), t0, dt, nsteps, C.byref(cfg), _ptr(U0),
+                                               _ptr(U), C.byref(rep)))
+        return rep.as_dict()
+
+    def transient_backward(self, theta, U0, dJdU, dJdtheta, t0, dt, nsteps, cfg=None, **kw):
+        """Transient pair, backward: dJ/dtheta of a terminal objective J(U_N) (dJdU given) by the
+        discrete adjoint, the forward states replayed from checkpoints; returns the report with
+        "states_held", the states kept at once."""
+        cfg = cfg or SolverConfig.make(**kw)
+        rep, held = Report(), _I64()
+        check(lib().rsd_heat_transient_backward(self.ctx.h, self.h, _ptr(theta), t0, dt, nsteps, _ptr(U0), _ptr(dJdU),
+                                                C.byref(cfg), _ptr(dJdtheta), C.byref(rep), C.byref(held)))
+        d = rep.as_dict()
+        d["states_held"] = held.value
+        return d
 
     def newton(self, U, abs_tol=1e-10, rel_tol=1e-10, max_iters=50, cfg=None, **kw):
         cfg = cfg or SolverConfig.make(type=GMRES, **kw)

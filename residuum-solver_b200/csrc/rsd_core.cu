@@ -620,6 +620,7 @@ int rsd_ctx_destroy(rsd_ctx* c) {
 	if (c->stream) cudaStreamSynchronize(c->stream);
 	for (cudaEvent_t e : c->prof.pool) cudaEventDestroy(e);
 	free_graph_cache(c);
+	cudaFree(c->ws);
 	cudaFree(c->s.partials);
 	cudaFree(c->s.scal);
 	cudaFreeHost(c->s.hscal);

@@ -101,6 +101,12 @@ __global__ void k_adjoint_scale(int64_t ne, const double* __restrict__ kElem, do
 		g[e] = -(kElem[e] * k0) * g[e];
 }
 
+// acc[e] += g[e]: the transient gradient's sum over steps
+__global__ void k_accumulate(int64_t ne, const double* __restrict__ g, double* __restrict__ acc) {
+	for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne; e += (int64_t)gridDim.x * blockDim.x)
+		acc[e] += g[e];
+}
+
 __global__ void k_diff_norm(int64_t n, const double* __restrict__ F, const double* __restrict__ R, double* partials,
                             unsigned* ticket, double* out) {
 	double v[1] = {0.0};
@@ -534,6 +540,164 @@ int rsd_heat_backward(rsd_ctx* ctx, rsd_heat* h, const double* theta, const doub
 	}
 	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
 	return RSD_OK;
+}
+
+
+}  // extern "C"
+
+// ---- transient adjoint pair (no counterpart in the reference): N Backward-Euler steps of the linear
+// stage (BackwardEulerStage.hpp:71-124, BackwardEuler.hpp:32-70) with k_e = k_const exp(theta_e), and
+// the gradient of a terminal objective J(U_N) by the discrete adjoint of those steps.  With
+// A = K(theta) + M/dt the steps are A U_k = M U_{k-1} / dt + f_k (f_k: load and Dirichlet lift at t_k),
+// and only K depends on theta, so with mu_N = A^-1 dJ/dU_N and mu_k = A^-1 M mu_{k+1} / dt
+// (A symmetric) dJ/dtheta_e = -k_e sum_k int_e grad(mu_k) . K0 grad(U_k), U_k carrying its Dirichlet
+// values at t_k.  The reverse sweep needs U_k in reverse order: the forward sweep keeps every C-th state
+// (C = ceil(sqrt N)) and each segment's states are recomputed from its checkpoint when the sweep
+// reaches it, so ceil(N / C) + C + 1 states are held instead of N, for about N extra forward steps.
+namespace rsd {
+
+static int transient_check(rsd_ctx* ctx, rsd_heat* h, const double* theta, const rsd_solver_cfg* cfg, double dt, int64_t nsteps) {
+	RSD_CHECK(adjoint_check(ctx, h, theta, cfg));
+	if (h->cpExpr.n) return set_error(RSD_EINVAL, "the transient adjoint pair needs a constant specific heat (cp_expr unset)");
+	if (cfg->operator_type != RSD_OP_CSR) return set_error(RSD_EINVAL, "the transient adjoint pair solves with the assembled matrix (operator_type RSD_OP_CSR)");
+	if (!(dt > 0) || nsteps < 0) return set_error(RSD_EINVAL, "dt must be > 0 and nsteps >= 0");
+	return RSD_OK;
+}
+
+// steps first..last-1 -> first+1..last from the state in U (Uprev its copy), times t0 + k dt
+static int steps(rsd_ctx* ctx, rsd_heat* h, double t0, double dt, int64_t first, int64_t last, const rsd_solver_cfg* cfg,
+                 double* U, double* Uprev, rsd_report* total) {
+	for (int64_t k = first; k < last; ++k) {
+		h->time = t0 + (double)k * dt;   // be_step advances it and re-evaluates the Dirichlet values
+		rsd_report r{};
+		RSD_CHECK(be_step(ctx, h, dt, cfg, U, Uprev, &r, nullptr, nullptr, nullptr));
+		if (total) {
+			total->iterations += r.iterations;
+			if (!r.converged) { total->converged = 0; if (r.status != RSD_OK) total->status = r.status; }
+		}
+	}
+	return RSD_OK;
+}
+
+}  // namespace rsd
+
+extern "C" {
+
+int rsd_heat_transient_forward(rsd_ctx* ctx, rsd_heat* h, const double* theta, double t0, double dt, int64_t nsteps,
+                               const rsd_solver_cfg* cfg, const double* U0, double* U, rsd_report* rep) {
+	if (!U0 || !U) return set_error(RSD_EINVAL, "null argument");
+	RSD_CHECK(transient_check(ctx, h, theta, cfg, dt, nsteps));
+	const int64_t n = h->n;
+	double* Uprev = h->dU;
+	RSD_CUDA(cudaMemcpyAsync(U, U0, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+	RSD_CUDA(cudaMemcpyAsync(Uprev, U0, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+	rsd_report total{};
+	total.converged = 1;
+	RSD_CHECK(steps(ctx, h, t0, dt, 0, nsteps, cfg, U, Uprev, &total));
+	if (rep) *rep = total;
+	RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+	return RSD_OK;
+}
+
+int rsd_heat_transient_backward(rsd_ctx* ctx, rsd_heat* h, const double* theta, double t0, double dt, int64_t nsteps,
+                                const double* U0, const double* dJdU, const rsd_solver_cfg* cfg, double* dJdtheta,
+                                rsd_report* rep, int64_t* states_held) {
+	if (!U0 || !dJdU || !dJdtheta) return set_error(RSD_EINVAL, "null argument");
+	RSD_CHECK(transient_check(ctx, h, theta, cfg, dt, nsteps));
+	const int64_t n = h->n, ne = h->m->nelem, N = nsteps;
+	cudaStream_t st = ctx->stream;
+	RSD_CUDA(cudaMemsetAsync(dJdtheta, 0, sizeof(double) * std::max<int64_t>(ne, 1), st));
+	if (rep) *rep = rsd_report{};
+	if (N == 0 || n == 0) {
+		if (rep) rep->converged = 1;
+		if (states_held) *states_held = 0;
+		RSD_CUDA(cudaStreamSynchronize(st));
+		return RSD_OK;
+	}
+	const int64_t C = (int64_t)std::ceil(std::sqrt((double)N));
+	const int64_t nseg = (N + C - 1) / C;
+	const int64_t ns = (n + 31) & ~int64_t(31);   // 256-byte aligned vectors
+	// checkpoints (nseg), one segment (C + 1), the adjoint pair mu / mu_next, the right-hand side, the
+	// step's previous state; per element the step's gradient term
+	const int64_t nvec = nseg + (C + 1) + 4;
+	double* buf = nullptr;
+	double* gstep = nullptr;
+	RSD_CUDA(cudaMalloc(&buf, sizeof(double) * ns * nvec));
+	if (cudaMalloc(&gstep, sizeof(double) * std::max<int64_t>(ne, 1)) != cudaSuccess) {
+		cudaFree(buf);
+		return set_error(RSD_ENOMEM, "transient adjoint scratch");
+	}
+	auto run = [&]() -> int {
+		double* ck = buf;
+		double* seg = ck + ns * nseg;
+		double* mu = seg + ns * (C + 1);
+		double* muNext = mu + ns;
+		double* rhs = muNext + ns;
+		double* Uprev = rhs + ns;
+		rsd_report fwd{};
+		fwd.converged = 1;
+		// forward sweep: keep the state at the start of every segment
+		double* U = seg;
+		RSD_CUDA(cudaMemcpyAsync(U, U0, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+		RSD_CUDA(cudaMemcpyAsync(Uprev, U0, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+		for (int64_t s = 0; s < nseg; ++s) {
+			RSD_CUDA(cudaMemcpyAsync(ck + ns * s, U, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+			if (s + 1 < nseg) RSD_CHECK(steps(ctx, h, t0, dt, s * C, (s + 1) * C, cfg, U, Uprev, &fwd));
+		}
+		// reverse sweep, segment by segment
+		rsd_report adj{};
+		adj.converged = 1;
+		RSD_CUDA(cudaMemsetAsync(muNext, 0, sizeof(double) * n, st));
+		for (int64_t s = nseg - 1; s >= 0; --s) {
+			const int64_t start = s * C, len = std::min(C, N - start);
+			// seg[j] = U_{start + j}, j = 0..len (recomputed from the checkpoint)
+			RSD_CUDA(cudaMemcpyAsync(seg, ck + ns * s, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+			for (int64_t j = 1; j <= len; ++j) {
+				double* Uj = seg + ns * j;
+				RSD_CUDA(cudaMemcpyAsync(Uj, seg + ns * (j - 1), sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+				RSD_CUDA(cudaMemcpyAsync(Uprev, Uj, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+				RSD_CHECK(steps(ctx, h, t0, dt, start + j - 1, start + j, cfg, Uj, Uprev, &fwd));
+			}
+			// h->K holds A = K + M/dt from the steps just taken (theta is fixed)
+			for (int64_t j = len; j >= 1; --j) {
+				const int64_t k = start + j;
+				const double* b = dJdU;
+				if (k < N) {
+					// M mu_{k+1} / dt: rho cp Mass on a free vector (zero on the Dirichlet nodes)
+					RSD_CHECK(assemble_vector(ctx, h, 3, 0.0, nullptr, muNext, nullptr, rhs, 1.0 / dt, false));
+					b = rhs;
+				}
+				RSD_CUDA(cudaMemcpyAsync(mu, muNext, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));   // warm start
+				rsd_report r{};
+				RSD_CHECK(solve(ctx, h->K, cfg, b, mu, &r));
+				adj.iterations += r.iterations;
+				if (!r.converged) { adj.converged = 0; if (r.status != RSD_OK) adj.status = r.status; }
+				// int_e grad(mu_k) . K0 grad(U_k) with U_k's Dirichlet values at t_k
+				h->time = t0 + (double)k * dt;
+				RSD_CHECK(upload_bc_values(ctx, h));
+				RSD_CHECK(assemble_vector(ctx, h, 6, 0.0, seg + ns * j, nullptr, mu, gstep, 1.0, false));
+				if (ne) k_accumulate<<<vec_grid(ctx, ne), 256, 0, st>>>(ne, gstep, dJdtheta);
+				RSD_CUDA(cudaGetLastError());
+				std::swap(mu, muNext);
+			}
+		}
+		if (ne) k_adjoint_scale<<<vec_grid(ctx, ne), 256, 0, st>>>(ne, h->kElem, h->k_const, dJdtheta);
+		RSD_CUDA(cudaGetLastError());
+		RSD_CUDA(cudaStreamSynchronize(st));
+		if (rep) {
+			rep->converged = adj.converged && fwd.converged;
+			rep->status = adj.status != RSD_OK ? adj.status : fwd.status;
+			rep->iterations = adj.iterations;        // adjoint solves
+			rep->refinements = fwd.iterations;       // forward solves, the recomputed segments included
+		}
+		if (states_held) *states_held = nseg + C + 1;
+		return RSD_OK;
+	};
+	const int rc = run();
+	cudaStreamSynchronize(st);
+	cudaFree(buf);
+	cudaFree(gstep);
+	return rc;
 }
 
 }  // extern "C"

@@ -77,6 +77,8 @@ struct rsd_ctx {
 	rsd::rsd_scratch s;
 	rsd::Profiler prof;
 	void* graphs = nullptr;        // cached CG solve graphs (rsd_krylov.cu)
+	void* ws = nullptr;            // Krylov workspace of this context (grow-only)
+	size_t wsBytes = 0;
 };
 
 namespace rsd {

@@ -392,22 +392,20 @@ __global__ void __launch_bounds__(256) k_true_res(int64_t n, MatView<double> A, 
 }
 
 // ---- workspace -------------------------------------------------------------------------------
-struct Workspace {
-	void* base = nullptr;
-	size_t bytes = 0;
-	int device = -1;
-};
-static Workspace g_ws[16];
-
+// One grow-only buffer per context, used only on that context's stream: contexts on one device (one
+// per host thread, say) never share Krylov vectors, and a grow waits only for this context's own work.
 static int get_ws(rsd_ctx* ctx, size_t bytes, void** out) {
-	Workspace& w = g_ws[ctx->device & 15];
-	if (w.bytes < bytes || w.device != ctx->device) {
-		if (w.base) { cudaStreamSynchronize(ctx->stream); cudaFree(w.base); w.base = nullptr; w.bytes = 0; }
-		RSD_CUDA(cudaMalloc(&w.base, bytes));
-		w.bytes = bytes;
-		w.device = ctx->device;
+	if (ctx->wsBytes < bytes) {
+		if (ctx->ws) {
+			RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+			cudaFree(ctx->ws);
+			ctx->ws = nullptr;
+			ctx->wsBytes = 0;
+		}
+		RSD_CUDA(cudaMalloc(&ctx->ws, bytes));
+		ctx->wsBytes = bytes;
 	}
-	*out = w.base;
+	*out = ctx->ws;
 	return RSD_OK;
 }
 
@@ -927,8 +925,13 @@ namespace {
 // ---- GMRES(m): linalg/solver/iterative/gmres/Solver.tpp:3-170 ---------------------------------
 // Right-preconditioned restarted GMRES.  Device: the preconditioned SpMV (Jacobi folded into the
 // gather, w = A (M^-1 q)), the orthogonalization and the scalings; host: the (m+1) x m Hessenberg,
-// Givens rotations and back substitution, as the reference keeps them (gmres/Workspace.hpp:26-31),
-// with one read-back of the new column per Arnoldi step.
+// Givens rotations and back substitution as the reference computes them (gmres/Solver.tpp:88-126), on
+// the device: one thread applies the previous rotations to the new Hessenberg column, forms the next
+// rotation, updates g and decides whether the cycle ends (convergence on |g_{j+1}|, breakdown, the
+// iteration limit, a non-finite value); every kernel of the following steps reads that decision and
+// returns at once, so the host launches a whole cycle without waiting and reads the outcome once per
+// cycle.  The products and sums use explicit round-to-nearest operations (no fused multiply-add), the
+// same arithmetic as the host loop they replace.
 // Orthogonalization is classical Gram-Schmidt applied twice (CGS2): each pass is one kernel for
 // all j+1 projections Q^T w and one for w -= Q h.  In exact arithmetic it equals the reference's
 // modified Gram-Schmidt; in floating point CGS2 keeps the basis orthogonal to working precision as
@@ -939,7 +942,8 @@ namespace {
 // w = A (M^-1 q) with M^-1 = diag(invD) (identity when invD is null)
 template <int L, typename T>
 __global__ void __launch_bounds__(256, 2 * kRowBlocks) k_gm_spmv(int64_t n, MatView<T> A, const T* __restrict__ q,
-                                                 const T* __restrict__ invD, T* __restrict__ w) {
+                                                 const T* __restrict__ invD, T* __restrict__ w, const int32_t* stop) {
+	if (stop && *(volatile const int32_t*)stop) return;   // uniform over the launch
 	const L2Pol pol = make_l2pol();
 	const RowLoop<L> rl;
 	for (int64_t base = rl.base; base < n; base += rl.step) {
@@ -954,7 +958,8 @@ __global__ void __launch_bounds__(256, 2 * kRowBlocks) k_gm_spmv(int64_t n, MatV
 // h[i] = Q_i . w for i = blockIdx.y (FP64 accumulation; last-block-done reduction per i)
 template <typename T>
 __global__ void k_gm_mdot(int64_t n, const T* __restrict__ Q, int64_t ldq, const T* __restrict__ w, double* partials,
-                          unsigned* tickets, double* h) {
+                          unsigned* tickets, double* h, const int32_t* stop) {
+	if (*(volatile const int32_t*)stop) return;
 	const int i = blockIdx.y;
 	const T* __restrict__ qi = Q + (int64_t)i * ldq;
 	double v[1] = {0.0};
@@ -966,7 +971,8 @@ __global__ void k_gm_mdot(int64_t n, const T* __restrict__ Q, int64_t ldq, const
 // w -= sum_{i<k} h[i] Q_i (basis order)
 template <typename T>
 __global__ void k_gm_mupdate(int64_t n, const T* __restrict__ Q, int64_t ldq, int k, const double* __restrict__ h,
-                             T* __restrict__ w) {
+                             T* __restrict__ w, const int32_t* stop) {
+	if (*(volatile const int32_t*)stop) return;
 	for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
 		double s = (double)w[e];
 		for (int i = 0; i < k; ++i) s -= h[i] * (double)Q[(int64_t)i * ldq + e];
@@ -976,7 +982,9 @@ __global__ void k_gm_mupdate(int64_t n, const T* __restrict__ Q, int64_t ldq, in
 
 // out = ||w||
 template <typename T>
-__global__ void k_gm_nrm2(int64_t n, const T* __restrict__ w, double* partials, unsigned* ticket, double* out) {
+__global__ void k_gm_nrm2(int64_t n, const T* __restrict__ w, double* partials, unsigned* ticket, double* out,
+                          const int32_t* stop) {
+	if (*(volatile const int32_t*)stop) return;
 	double v[1] = {0.0};
 	for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
 		v[0] += (double)w[e] * (double)w[e];
@@ -985,7 +993,9 @@ __global__ void k_gm_nrm2(int64_t n, const T* __restrict__ w, double* partials, 
 
 // q = w / hn unless breakdown (hn <= 1e-14)
 template <typename T>
-__global__ void k_gm_scale(int64_t n, const T* __restrict__ w, const double* __restrict__ hn, T* __restrict__ q) {
+__global__ void k_gm_scale(int64_t n, const T* __restrict__ w, const double* __restrict__ hn, T* __restrict__ q,
+                           const int32_t* stop) {
+	if (*(volatile const int32_t*)stop) return;
 	const double h = *hn;
 	if (h <= 1e-14) return;
 	const double s = 1.0 / h;
@@ -1013,10 +1023,60 @@ __global__ void k_gm_resnorm(int64_t n, const double* __restrict__ b, const doub
 	if (grid_sum<1>(v, partials, ticket)) *out = sqrt(v[0]);
 }
 
-// x += M^-1 (sum_i y_i Q_i), accumulated in basis order in FP64
+// The Hessenberg least-squares state of one GMRES cycle on the device (gmres/Workspace.hpp:26-31)
+struct GmState {
+	int32_t stop, mLocal, status, breakdown;
+	double tol, denom;    // |g_{j+1}| / denom < tol ends the cycle (denom: res0 + 1e-50 when relative, else 1)
+	int64_t budget;       // Arnoldi steps this cycle may take (the iteration limit's remainder)
+};
+
+// Arnoldi step j: the new column (the two CGS passes' coefficients, hNext), the previous rotations, the
+// next rotation, g; ends the cycle on convergence, breakdown (hNext <= 1e-14), the step budget or a
+// non-finite g (gmres/Solver.tpp:88-110).  One thread.
+__global__ void k_gm_givens(GmState* S, int j, int m, const double* __restrict__ h1, const double* __restrict__ h2,
+                            const double* __restrict__ hNextp, double* __restrict__ H, double* __restrict__ cs,
+                            double* __restrict__ sn, double* __restrict__ g) {
+	if (S->stop) return;
+	const int ld = m + 1;   // H column-major: H(i, j) at j * (m + 1) + i
+	double* Hj = H + (int64_t)j * ld;
+	for (int i = 0; i <= j; ++i) Hj[i] = __dadd_rn(h1[i], h2[i]);
+	const double hNext = *hNextp;
+	for (int i = 0; i < j; ++i) {
+		const double a = Hj[i], b = Hj[i + 1];
+		Hj[i] = __dadd_rn(__dmul_rn(cs[i], a), __dmul_rn(sn[i], b));
+		Hj[i + 1] = __dadd_rn(__dmul_rn(-sn[i], a), __dmul_rn(cs[i], b));
+	}
+	const double hjj = Hj[j];
+	const double denom = sqrt(__dadd_rn(__dmul_rn(hjj, hjj), __dmul_rn(hNext, hNext)));
+	if (denom <= 1e-14) { cs[j] = 1.0; sn[j] = 0.0; }
+	else { cs[j] = hjj / denom; sn[j] = hNext / denom; }
+	Hj[j] = __dadd_rn(__dmul_rn(cs[j], hjj), __dmul_rn(sn[j], hNext));
+	const double gj = g[j];
+	g[j] = __dmul_rn(cs[j], gj);
+	g[j + 1] = __dmul_rn(-sn[j], gj);
+	S->mLocal = j + 1;
+	const bool brk = hNext <= 1e-14;
+	S->breakdown = brk;
+	if (!isfinite(g[j + 1])) { S->status = RSD_EBREAKDOWN; S->stop = 1; return; }
+	if (fabs(g[j + 1]) / S->denom < S->tol || brk || j + 1 >= S->budget || j + 1 >= m) S->stop = 1;
+}
+
+// back substitution H(0:m, 0:m) y = g(0:m) for the cycle's m = mLocal steps (one thread)
+__global__ void k_gm_backsub(const GmState* S, int m, const double* __restrict__ H, const double* __restrict__ g,
+                             double* __restrict__ y) {
+	const int ml = S->mLocal, ld = m + 1;
+	for (int i = ml - 1; i >= 0; --i) {
+		double s = g[i];
+		for (int k = i + 1; k < ml; ++k) s = __dsub_rn(s, __dmul_rn(H[(int64_t)k * ld + i], y[k]));
+		y[i] = s / H[(int64_t)i * ld + i];
+	}
+}
+
+// x += M^-1 (sum_i y_i Q_i), accumulated in basis order in FP64, over the cycle's S->mLocal vectors
 template <typename T>
-__global__ void k_gm_update_x(int64_t n, int m, const T* __restrict__ Q, int64_t ldq, const double* __restrict__ yv,
+__global__ void k_gm_update_x(int64_t n, const GmState* S, const T* __restrict__ Q, int64_t ldq, const double* __restrict__ yv,
                               const T* __restrict__ invD, double* __restrict__ x) {
+	const int m = S->mLocal;
 	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
 		double s = 0.0;
 		for (int k = 0; k < m; ++k) s += yv[k] * (double)Q[(int64_t)k * ldq + i];
@@ -1045,11 +1105,11 @@ struct GmCsrOp {
 		RSD_CUDA(cudaGetLastError());
 		return RSD_OK;
 	}
-	// w = A (M^-1 q)
-	int prec_apply(const T* q, const T* invD, T* w, T*, const double*) {
+	// w = A (M^-1 q); the launch returns at once when *stop != 0
+	int prec_apply(const T* q, const T* invD, T* w, T*, const double*, const int32_t* stop) {
 		const int L = exec_lanes(A);
 		const MatView<T> V = exec_view<T>(A);
-		RSD_DISPATCH_L(L, (k_gm_spmv<LL, T><<<wave_blocks(ctx, k_gm_spmv<LL, T>, 256, n * std::max(LL, 1)), 256, 0, ctx->stream>>>(n, V, q, invD, w)));
+		RSD_DISPATCH_L(L, (k_gm_spmv<LL, T><<<wave_blocks(ctx, k_gm_spmv<LL, T>, 256, n * std::max(LL, 1)), 256, 0, ctx->stream>>>(n, V, q, invD, w, stop)));
 		RSD_CUDA(cudaGetLastError());
 		return RSD_OK;
 	}
@@ -1058,7 +1118,9 @@ struct GmCsrOp {
 
 // ... or the matrix-free operator (FEMOperator, FP64): every product an element pass with the
 // iterate as the k(T) state, Jacobi from the element diagonal at the initial iterate
-__global__ void k_gm_scale_by(int64_t n, const double* __restrict__ q, const double* __restrict__ d, double* __restrict__ out) {
+__global__ void k_gm_scale_by(int64_t n, const double* __restrict__ q, const double* __restrict__ d, double* __restrict__ out,
+                              const int32_t* stop) {
+	if (*(volatile const int32_t*)stop) return;
 	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
 		out[i] = d ? q[i] * d[i] : q[i];
 }
@@ -1078,10 +1140,10 @@ struct GmFemOp {
 		RSD_CUDA(cudaGetLastError());
 		return RSD_OK;
 	}
-	int prec_apply(const double* q, const double* invD, double* w, double* tmp, const double* x) {
-		k_gm_scale_by<<<vec_grid(ctx, n), 256, 0, ctx->stream>>>(n, q, invD, tmp);
+	int prec_apply(const double* q, const double* invD, double* w, double* tmp, const double* x, const int32_t* stop) {
+		k_gm_scale_by<<<vec_grid(ctx, n), 256, 0, ctx->stream>>>(n, q, invD, tmp, stop);
 		RSD_CUDA(cudaGetLastError());
-		return apply_operator(ctx, h, coef, state ? state : x, tmp, w, nullptr, which, cTD, cTM, Udot);
+		return apply_operator(ctx, h, coef, state ? state : x, tmp, w, stop, which, cTD, cTM, Udot);
 	}
 	int apply64(const double* x, double* Ax) { return apply_operator(ctx, h, coef, state ? state : x, x, Ax, nullptr, which, cTD, cTM, Udot); }
 };
@@ -1099,7 +1161,9 @@ static int gmres_core(rsd_ctx* ctx, Op& op, const rsd_solver_cfg* cfg, const dou
 	const size_t qBytes = sizeof(T) * (size_t)(m + 4) * ns;
 	const size_t axBytes = sizeof(double) * (size_t)ns;
 	const size_t pBytes = sizeof(double) * (size_t)(m + 1) * kMaxPartials;
-	const size_t hBytes = sizeof(double) * (size_t)(4 * (m + 2) + 8);
+	// the device least-squares state: H ((m + 1) m), cs, sn (m), g (m + 1), y (m), the two CGS passes'
+	// coefficients (m + 2 each), the next norm, and the control block
+	const size_t hBytes = sizeof(double) * (size_t)((m + 1) * m + 2 * m + (m + 1) + m + 2 * (m + 2) + 8) + sizeof(GmState) + 64;
 	const size_t tBytes = sizeof(unsigned) * (size_t)(m + 2);
 	void* wsv;
 	RSD_CHECK(get_ws(ctx, qBytes + axBytes + pBytes + hBytes + tBytes + 1024, &wsv));
@@ -1110,18 +1174,21 @@ static int gmres_core(rsd_ctx* ctx, Op& op, const rsd_solver_cfg* cfg, const dou
 	T* tmp = w + 2 * ns;
 	double* Ax = (double*)(base + qBytes);
 	double* parts = (double*)(base + qBytes + axBytes);
-	double* dH1 = (double*)(base + qBytes + axBytes + pBytes);
+	double* dH = (double*)(base + qBytes + axBytes + pBytes);
+	double* dCs = dH + (m + 1) * m;
+	double* dSn = dCs + m;
+	double* dG = dSn + m;
+	double* dY = dG + (m + 1);
+	double* dH1 = dY + m;
 	double* dH2 = dH1 + (m + 2);
-	double* dY = dH2 + (m + 2);
-	double* dNorm = dY + (m + 2);
+	double* dNorm = dH2 + (m + 2);
+	GmState* dS = (GmState*)(((uintptr_t)(dNorm + 8) + 63) & ~uintptr_t(63));
 	unsigned* tickets = (unsigned*)(base + qBytes + axBytes + pBytes + hBytes);
 	cudaStream_t st = ctx->stream;
 	RSD_CUDA(cudaMemsetAsync(tickets, 0, tBytes, st));
 	const int gv = vec_grid(ctx, n), grd = red_grid(ctx, n);
 	const bool relMode = cfg->tol_type == RSD_TOL_RELATIVE;
-	const double breakdownTol = 1e-14, eps = 1e-50;
-	std::vector<double> H((m + 1) * m, 0.0), cs(m), sn(m), g(m + 1), yv(m), col(2 * (m + 2));
-	auto Hat = [&](int64_t i, int64_t j) -> double& { return H[j * (m + 1) + i]; };
+	const double eps = 1e-50;
 	if (invD) RSD_CHECK(op.invdiag(invD, x));
 	// FP64 residual of the current x; q0 = r / beta
 	auto residual = [&](double* beta) -> int {
@@ -1145,59 +1212,42 @@ static int gmres_core(rsd_ctx* ctx, Op& op, const rsd_solver_cfg* cfg, const dou
 	}
 	int64_t total = 0, cycles = 0;
 	double beta = res0;
+	GmState* hS = reinterpret_cast<GmState*>(ctx->s.hbuf + 16);   // pinned staging
 	while (total < cfg->max_iters) {
+		// a cycle: g = (beta, 0, ...), the control block, q0; then every Arnoldi step launched at once
+		GmState s0{};
+		s0.tol = cfg->tol;
+		s0.denom = relMode ? res0 + eps : 1.0;
+		s0.budget = std::min<int64_t>(m, cfg->max_iters - total);
+		*hS = s0;
+		RSD_CUDA(cudaMemcpyAsync(dS, hS, sizeof(GmState), cudaMemcpyHostToDevice, st));
+		RSD_CUDA(cudaMemsetAsync(dG, 0, sizeof(double) * (m + 1), st));
+		RSD_CUDA(cudaMemcpyAsync(dG, dNorm, sizeof(double), cudaMemcpyDeviceToDevice, st));
 		k_gm_start<T><<<gv, 256, 0, st>>>(n, b, Ax, dNorm, Q);
 		++cycles;
-		g[0] = beta;
-		for (int64_t i = 1; i <= m; ++i) g[i] = 0.0;
-		int64_t mLocal = 0;
-		bool breakdown = false;
-		for (int64_t j = 0; j < m; ++j) {
+		const int32_t* stop = &dS->stop;
+		for (int64_t j = 0; j < s0.budget; ++j) {
 			const T* qj = Q + j * ns;
-			RSD_CHECK(op.prec_apply(qj, invD, w, tmp, x));
+			RSD_CHECK(op.prec_apply(qj, invD, w, tmp, x, stop));
 			const int k = (int)(j + 1);
 			for (double* dh : {dH1, dH2}) {
-				k_gm_mdot<T><<<dim3(grd, k), kReduceThreads, 0, st>>>(n, Q, ns, w, parts, tickets, dh);
-				k_gm_mupdate<T><<<gv, 256, 0, st>>>(n, Q, ns, k, dh, w);
+				k_gm_mdot<T><<<dim3(grd, k), kReduceThreads, 0, st>>>(n, Q, ns, w, parts, tickets, dh, stop);
+				k_gm_mupdate<T><<<gv, 256, 0, st>>>(n, Q, ns, k, dh, w, stop);
 			}
-			k_gm_nrm2<T><<<grd, kReduceThreads, 0, st>>>(n, w, parts, tickets + m + 1, dNorm);
-			k_gm_scale<T><<<gv, 256, 0, st>>>(n, w, dNorm, Q + (j + 1) * ns);
+			k_gm_nrm2<T><<<grd, kReduceThreads, 0, st>>>(n, w, parts, tickets + m + 1, dNorm, stop);
+			k_gm_scale<T><<<gv, 256, 0, st>>>(n, w, dNorm, Q + (j + 1) * ns, stop);
+			k_gm_givens<<<1, 1, 0, st>>>(dS, (int)j, (int)m, dH1, dH2, dNorm, dH, dCs, dSn, dG);
 			RSD_CUDA(cudaGetLastError());
-			RSD_CUDA(cudaMemcpyAsync(col.data(), dH1, sizeof(double) * 2 * (m + 2), cudaMemcpyDeviceToHost, st));
-			double hNext = 0.0;
-			RSD_CUDA(cudaMemcpyAsync(&hNext, dNorm, sizeof(double), cudaMemcpyDeviceToHost, st));
-			RSD_CUDA(cudaStreamSynchronize(st));
-			for (int64_t i = 0; i <= j; ++i) Hat(i, j) = col[i] + col[(m + 2) + i];
-			++total;
-			breakdown = hNext <= breakdownTol;
-			for (int64_t i = 0; i < j; ++i) {
-				const double h1 = Hat(i, j), h2 = Hat(i + 1, j);
-				Hat(i, j) = cs[i] * h1 + sn[i] * h2;
-				Hat(i + 1, j) = -sn[i] * h1 + cs[i] * h2;
-			}
-			const double hjj = Hat(j, j);
-			const double denom = std::sqrt(hjj * hjj + hNext * hNext);
-			if (denom <= breakdownTol) { cs[j] = 1.0; sn[j] = 0.0; }
-			else { cs[j] = hjj / denom; sn[j] = hNext / denom; }
-			Hat(j, j) = cs[j] * hjj + sn[j] * hNext;
-			const double gj = g[j];
-			g[j] = cs[j] * gj;
-			g[j + 1] = -sn[j] * gj;
-			mLocal = j + 1;
-			if (!std::isfinite(g[j + 1])) { R.status = RSD_EBREAKDOWN; break; }
-			if (converged(std::fabs(g[j + 1])) || breakdown || total >= cfg->max_iters) break;
 		}
-		for (int64_t ii = 0; ii < mLocal; ++ii) {
-			const int64_t i = mLocal - 1 - ii;
-			double s = g[i];
-			for (int64_t k = i + 1; k < mLocal; ++k) s -= Hat(i, k) * yv[k];
-			yv[i] = s / Hat(i, i);
-		}
-		RSD_CUDA(cudaMemcpyAsync(dY, yv.data(), sizeof(double) * mLocal, cudaMemcpyHostToDevice, st));
-		k_gm_update_x<T><<<gv, 256, 0, st>>>(n, (int)mLocal, Q, ns, dY, invD, x);
-		RSD_CHECK(residual(&beta));
+		k_gm_backsub<<<1, 1, 0, st>>>(dS, (int)m, dH, dG, dY);
+		k_gm_update_x<T><<<gv, 256, 0, st>>>(n, dS, Q, ns, dY, invD, x);
+		RSD_CUDA(cudaGetLastError());
+		RSD_CUDA(cudaMemcpyAsync(hS, dS, sizeof(GmState), cudaMemcpyDeviceToHost, st));
+		RSD_CHECK(residual(&beta));   // synchronizes: the control block is on the host too
+		total += hS->mLocal;
+		if (hS->status) R.status = hS->status;
 		if (R.status || converged(beta) || total >= cfg->max_iters) break;
-		if (breakdown && !kMixed) break;   // FP64: the Krylov space is exhausted; mixed: restart in FP64
+		if (hS->breakdown && !kMixed) break;   // FP64: the Krylov space is exhausted; mixed: restart in FP64
 	}
 	R.converged = R.status ? 0 : converged(beta);
 	R.finalResidual = beta;

@@ -1,6 +1,6 @@
 """Generate the golden fixtures in this folder from the reference's own templates.
 
-    python tests/golden/make_golden.py [main] [adjoint] [fem] [models]
+    python tests/golden/make_golden.py [main] [adjoint] [fem] [models] [transient_adjoint]
 
 Every array comes from oracle/_ref/libresiduum_ref.so, i.e. the unmodified Residuum templates
 (Assembler<CPU>, BoundaryApplicator<CPU>, TopologicalDOF, cg/gmres::Solver, SteadyStage,
@@ -191,7 +191,31 @@ def models():
     save("models_aniso_quad_q2.npz", t2a=r.dofmap(), tensor=np.array(tensor2), U=Us)
 
 
-GROUPS = {"main": main, "adjoint": adjoint, "fem": fem, "models": models}
+def transient_adjoint():
+    """Transient adjoint fixture: 3D Q1 6x5x4, k_e = exp(theta_e), f = 1, T = 0.5 on x = 1 and 0 on the
+    other faces, 7 Backward-Euler steps of dt = 0.01 from U0, J = 0.5 ||U_7 - U_obs||^2; the FP64 CPU
+    adjoint on the reference's templates (oracle.ref_transient_adjoint), checked here against central
+    differences through the reference's own steps."""
+    rng = np.random.default_rng(77)
+    nel, dt, N = [6, 5, 4], 0.01, 7
+    theta = 0.5 * rng.standard_normal(6 * 5 * 4)
+    r = oracle.Reference(3, 1, 2, nel, [0, 0, 0], [1, 1, 1], list(range(6)), bc_kind=0, bc_val={1: 0.5})
+    n = r.n
+    U0 = 0.3 * np.sin(np.arange(n) * 0.41)
+    Uobs = 0.05 * np.cos(np.arange(n) * 1.3)
+    UN, J, grad, its = oracle.ref_transient_adjoint(nel, theta, U0, dt, N, Uobs, bc_val={1: 0.5})
+    d = rng.standard_normal(theta.size)
+    d /= np.linalg.norm(d)
+    h = 1e-6
+    Jp = oracle.ref_transient_adjoint(nel, theta + h * d, U0, dt, N, Uobs, bc_val={1: 0.5})[1]
+    Jm = oracle.ref_transient_adjoint(nel, theta - h * d, U0, dt, N, Uobs, bc_val={1: 0.5})[1]
+    fd = (Jp - Jm) / (2 * h)
+    assert abs(fd - grad @ d) <= 1e-6 * abs(fd), (fd, grad @ d)
+    save("transient_adjoint_q1_hex_6x5x4.npz", theta=theta, U0=U0, Uobs=Uobs, dt=dt, nsteps=N, UN=UN, J=J, grad=grad,
+         fd_dir=d, fd=fd)
+
+
+GROUPS = {"main": main, "adjoint": adjoint, "fem": fem, "models": models, "transient_adjoint": transient_adjoint}
 
 if __name__ == "__main__":
     if not oracle.reference_available():
