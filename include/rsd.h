@@ -269,6 +269,22 @@ int rsd_apply_natural(rsd_ctx* ctx, rsd_heat* h, double* F);
  * temperature U (device); out: device, nnodes * components (node-major); scratch: device, nnodes. */
 enum { RSD_FIELD_HEAT_FLUX = 0, RSD_FIELD_CONDUCTIVITY = 1 };
 int rsd_heat_nodal_field(rsd_ctx* ctx, rsd_heat* h, int32_t field, const double* U, double* out, double* scratch);
+/* HeatFlux monitors (MonitorConfig::Quantity::HeatFlux, HeatProblem.tpp:410-440) at the problem's current
+ * time, per requested boundary tag:
+ *   RSD_FLUX_STRONG: BoundaryQuadratureMonitorGroup with HeatFluxIntegrand
+ *     (fem/quantity/BoundaryQuadratureMonitorGroup.hpp, equation/heateq/quantity/HeatFluxIntegrand.hpp):
+ *     the sum over the tag's faces and Gauss points of -(K grad T) . n w (n area-scaled);
+ *   RSD_FLUX_WEAK: BoundaryReactionMonitorGroup (fem/quantity/BoundaryReactionMonitorGroup.hpp): the
+ *     element vectors of source - Diffusion(U) [- rho cp Mass(Udot) when `transient`] summed over the
+ *     tag's face nodes (each node once per element and tag, faces in order, as QuantityEvaluator.tpp:92-200).
+ * RSD_REDUCE_AVERAGE divides each value by the tag's measure (sum of |n| w).  U (free DOFs, Dirichlet
+ * values injected) and Udot are device vectors; values and measures (may be NULL) are host arrays of
+ * ntags.  A monitor combination (coefficients times tags, MonitorConfig::terms) is a linear combination
+ * of the per-tag values. */
+enum { RSD_FLUX_WEAK = 0, RSD_FLUX_STRONG = 1 };
+enum { RSD_REDUCE_INTEGRAL = 0, RSD_REDUCE_AVERAGE = 1 };
+int rsd_heat_boundary_flux(rsd_ctx* ctx, rsd_heat* h, int32_t method, int32_t reduction, int32_t transient, int32_t ntags,
+                           const int32_t* tags, const double* U, const double* Udot, double* values, double* measures);
 /* BoundaryApplicator::applyEssentialBCs (fem/boundary/backend/cpu/BoundaryApplicator.tpp:7-64) */
 int rsd_apply_dirichlet_lift(rsd_ctx* ctx, rsd_heat* h, double c_diff, double c_mass, double* F);
 /* Assembler::assembleDiagonal (Assembler.tpp:142-197) */

@@ -333,6 +333,7 @@ def ref_lib():
         L.ref_spmv.argtypes = [_I64, _P, _P, _P, _P, _P]
         L.ref_set_operator.argtypes = [_P, C.c_int]
         L.ref_nodal_field.argtypes = [_P, C.c_int, _P, _P]
+        L.ref_boundary_flux.argtypes = [_P, C.c_int, C.c_int, C.c_int, C.c_int, _P, _P, _P, _P]
         _rlib = L
     return _rlib
 
@@ -457,6 +458,17 @@ class Reference:
         g = np.zeros(self.nelem)
         ref_lib().ref_adjoint_gradient(self.h, _ptr(_f64(T)), _ptr(_f64(lam)), _ptr(g))
         return g
+
+    def boundary_flux(self, tags, U, Udot=None, method="weak", reduction="integral", transient=False):
+        """The reference's HeatFlux monitor groups (BoundaryReactionMonitorGroup for "weak",
+        BoundaryQuadratureMonitorGroup with HeatFluxIntegrand for "strong"), one combination per tag."""
+        tg = np.ascontiguousarray(list(tags), np.int32)
+        out = np.zeros(len(tg))
+        Udot = np.zeros(self.n) if Udot is None else Udot
+        if ref_lib().ref_boundary_flux(self.h, {"weak": 0, "strong": 1}[method], {"integral": 0, "average": 1}[reduction],
+                                       1 if transient else 0, len(tg), _ptr(tg), _ptr(_f64(U)), _ptr(_f64(Udot)), _ptr(out)):
+            raise RuntimeError(ref_lib().ref_last_error().decode())
+        return out
 
 
 def ref_csr_solve(rowPtr, col, val, b, x0=None, solver=0, precond=1, tol=1e-10, maxit=1000, krylov=30):

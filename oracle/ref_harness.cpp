@@ -19,7 +19,10 @@
 //   * RefHeatProblem, a Problem / TransientCapableProblem implementation mirroring
 //     application/heateq/problem/HeatProblem.tpp:217-289 without YAML, IO, loggers or monitors,
 //     so that the reference's own SteadyStage / BackwardEulerStage / NewtonRunner drive it.
-//   * ref_adjoint_gradient: an FP64 element loop over the reference QP evaluator + DiffusionForm.
+//   * ref_adjoint_gradient: an FP64 element loop over the reference QP evaluator + DiffusionForm;
+//   * ref_boundary_flux: the reference's own BoundaryQuadratureMonitorGroup (HeatFluxIntegrand) and
+//     BoundaryReactionMonitorGroup composed as HeatProblem::makeMonitorGroup composes them
+//     (application/heateq/problem/HeatProblem.tpp:368-440), evaluated with a full-precision callback.
 #include <chrono>
 #include <cmath>
 #include <cstdint>
@@ -37,6 +40,13 @@
 #include "linalg/operator/CSROperator.hpp"
 #include "linalg/operator/FEMOperator.hpp"
 #include "fem/quantity/QuantityEvaluator.hpp"
+#include "fem/quantity/BoundaryQuadratureMonitorGroup.hpp"
+#include "fem/quantity/BoundaryReactionMonitorGroup.hpp"
+#include "fem/quantity/QuantityForms.hpp"
+#include "fem/dispatch/DiscretizationDispatch.hpp"
+#include "equation/heateq/quantity/HeatFluxIntegrand.hpp"
+#include "equation/heateq/evaluator/HeatBoundaryStateVector.hpp"
+#include "equation/heateq/evaluator/EvalQuadraturePointBoundary.hpp"
 #include "fem/quantity/recovery/SimpleAverageRecovery.hpp"
 #include "equation/heateq/evaluator/HeatFluxField.hpp"
 #include "equation/heateq/evaluator/ConductivityField.hpp"
@@ -226,6 +236,7 @@ struct Base {
 	virtual int newton(double absTol, double relTol, int64_t maxit, int solverType, int precond, double tol, int64_t linMaxit, int64_t krylov, double* U, ref_report* rep) = 0;
 	virtual int backwardEuler(double dt, int64_t nsteps, int solverType, int precond, double tol, int64_t maxit, int64_t krylov, double* U, double* residualPerStep, double* stepStats) = 0;
 	virtual void adjointGradient(const double* T, const double* lam, double* grad) = 0;
+	virtual void boundaryFlux(int method, int reduction, int transient, int ntags, const int32_t* tags, const double* U, const double* Udot, double* values) = 0;
 	int opType = 0;   // LinearSolverConfig::OperatorType of the stages' linear solves: 0 CSR, 1 FEM
 	virtual void nodalField(int field, const double* U, double* out) = 0;
 };
@@ -571,6 +582,65 @@ struct RefHeatProblem final : Base {
 		else run(equation::heateq::evaluator::ConductivityField{});
 	}
 
+	// HeatFlux monitors, one group per call: method 1 Strong (BoundaryQuadratureMonitorGroup over
+	// ReducedQuantity<HeatFluxIntegrand, mode>), 0 Weak (BoundaryReactionMonitorGroup over the source,
+	// the negated stiffness on the value and, when transient, the negated mass on the rate), each tag one
+	// combination with coefficient 1 (MonitorConfig::terms)
+	void boundaryFlux(int method, int reduction, int transient, int ntags, const int32_t* tags, const double* U, const double* Udot, double* values) override {
+		using Traits = fem::dispatch::ElementTypeTraits<NSD == 2 ? mesh::ElementFamily::Quad : mesh::ElementFamily::Hex>;
+		using QuadBdy = typename Traits::QuadratureBoundaryType;
+		using EvalQPB = equation::heateq::evaluator::EvalQuadraturePointBoundary<EvalEle, typename Fam::Basis, fem::geometry::JacobianTransform<NSD, NSD>>;
+		using BdyState = equation::heateq::evaluator::HeatBoundaryStateVector<1, NSD, NSD, VecT>;
+		using CondBdy = LinearConductivity<EvalQPB>;
+		const QuadBdy quadBdy = [&] { if constexpr (NSD == 2) return QuadBdy(d.nq); else return QuadBdy(d.nq, d.nq); }();
+		loadState(U, Udot);
+		auto collect = [&](fem::quantity::MonitorGroup& group) {
+			for (int t = 0; t < ntags; ++t) {
+				group.registerTag(tags[t]);
+				const Index c = group.addCombination();
+				group.addTerm(c, tags[t], 1.0);
+			}
+			group.evaluate(0.0, [&](Index c, const Real* v) { values[c] = v[0]; });
+		};
+		const auto mode = reduction ? fem::quantity::Reduction::Average : fem::quantity::Reduction::Integral;
+		if (method == 1) {
+			CondBdy condBdy = CondBdy{cond_.ka, cond_.kb};
+			BdyState state;
+			state.valueSource = U_.get();
+			auto run = [&](auto tagMode) {
+				constexpr auto M = decltype(tagMode)::value;
+				using QF = fem::quantity::QuantityForms<fem::quantity::ReducedQuantity<equation::heateq::quantity::HeatFluxIntegrand<EvalQPB>, M>>;
+				fem::quantity::BoundaryQuadratureMonitorGroup<CPU, 1, EvalEle, EvalQPB, CondBdy, QF, QuadBdy, BdyState> group(mesh_, *topo_, ess_, condBdy, QF{}, evalEle_, quadBdy, state);
+				collect(group);
+			};
+			if (reduction) run(std::integral_constant<fem::quantity::Reduction, fem::quantity::Reduction::Average>{});
+			else run(std::integral_constant<fem::quantity::Reduction, fem::quantity::Reduction::Integral>{});
+			return;
+		}
+		StateVectorT state;
+		state.valueSource = U_.get();
+		state.rateSource = Udot_.get();
+		auto selV = [](StateVectorT& s) -> Real* { return s.valueBuffer(); };
+		auto selR = [](StateVectorT& s) -> Real* { return s.rateBuffer(); };
+		using SrcForm = std::decay_t<decltype(sourceForms_.template get<0>())>;
+		using NegStiff = fem::form::ScaledForm<1, StiffnessForms>;
+		using NegMass = fem::form::ScaledForm<1, MassForms>;
+		using SrcPair = fem::assembly::FormsWithOperand<SrcForm, decltype(selV)>;
+		using StiffPair = fem::assembly::FormsWithOperand<NegStiff, decltype(selV)>;
+		using MassPair = fem::assembly::FormsWithOperand<NegMass, decltype(selR)>;
+		const NegStiff negStiff(Real(-1));
+		const NegMass negMass(Real(-1));
+		if (transient) {
+			fem::quantity::BoundaryReactionMonitorGroup<CPU, 1, EvalEle, EvalQP, EvalQPB, OpModelT, typename Fam::Quad, QuadBdy, StateVectorT, SrcPair, StiffPair, MassPair> group(
+				mesh_, *topo_, ess_, opModel_, evalEle_, quad_, quadBdy, state, mode, SrcPair{sourceForms_.template get<0>(), selV}, StiffPair{negStiff, selV}, MassPair{negMass, selR});
+			collect(group);
+		} else {
+			fem::quantity::BoundaryReactionMonitorGroup<CPU, 1, EvalEle, EvalQP, EvalQPB, OpModelT, typename Fam::Quad, QuadBdy, StateVectorT, SrcPair, StiffPair> group(
+				mesh_, *topo_, ess_, opModel_, evalEle_, quad_, quadBdy, state, mode, SrcPair{sourceForms_.template get<0>(), selV}, StiffPair{negStiff, selV});
+			collect(group);
+		}
+	}
+
 	// dJ/dk_e contribution lam_e^T Khat_e T_e for every element, with Khat_e the unit-conductivity
 	// element stiffness built by the reference QP evaluator and DiffusionForm; T and lam are free
 	// vectors (constrained entries contribute their Dirichlet value for T and zero for lam).
@@ -646,6 +716,9 @@ int ref_backward_euler(void* h, double dt, int64_t nsteps, int solverType, int p
 	try { return static_cast<Base*>(h)->backwardEuler(dt, nsteps, solverType, precond, tol, maxit, krylov, U, resPerStep, stepStats); } catch (const std::exception& e) { g_err = e.what(); return -1; }
 }
 void ref_adjoint_gradient(void* h, const double* T, const double* lam, double* grad) { static_cast<Base*>(h)->adjointGradient(T, lam, grad); }
+int ref_boundary_flux(void* h, int method, int reduction, int transient, int ntags, const int32_t* tags, const double* U, const double* Udot, double* values) {
+	try { static_cast<Base*>(h)->boundaryFlux(method, reduction, transient, ntags, tags, U, Udot, values); return 0; } catch (const std::exception& e) { g_err = e.what(); return -1; }
+}
 
 // Generic CSR solve through the reference cg::Solver / gmres::Solver (linalg/solver/iterative/*),
 // Jacobi or Identity preconditioning, NullLogger.  Row pointers and columns are 64-bit like the

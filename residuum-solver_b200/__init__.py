@@ -119,6 +119,7 @@ SIGNATURES = {
     "rsd_assemble_matrix": [_P, _P, _D, _D, _D, _D, _P, _P, _P],
     "rsd_assemble_vector": [_P, _P, _I32, _D, _P, _P, _P, _P],
     "rsd_apply_dirichlet_lift": [_P, _P, _D, _D, _P],
+    "rsd_heat_boundary_flux": [_P, _P, _I32, _I32, _I32, _I32, _P, _P, _P, _P, _P],
     "rsd_assemble_diagonal": [_P, _P, _D, _D, _P, _P],
     "rsd_heat_solve_fem": [_P, _P, _D, C.POINTER(SolverConfig), _P, _P, C.POINTER(Report)],
     "rsd_heat_solve_fem_forms": [_P, _P, _D, _D, _D, _P, _P, C.POINTER(SolverConfig), _P, _P, C.POINTER(Report)],
@@ -518,6 +519,16 @@ class Heat:
         check(lib().rsd_heat_nodal_field(self.ctx.h, self.h, f, _ptr(U), _ptr(out), _ptr(scratch)))
         a = out.download()
         return a.reshape(-1, nc) if nc > 1 else a
+
+    def boundary_flux(self, tags, U, Udot=None, method="weak", reduction="integral", transient=False):
+        """HeatFlux monitors per boundary tag at the current time: (values, measures)."""
+        tg = np.ascontiguousarray(list(tags), np.int32)
+        vals, meas = np.zeros(len(tg)), np.zeros(len(tg))
+        check(lib().rsd_heat_boundary_flux(self.ctx.h, self.h, {"weak": 0, "strong": 1}[method],
+                                           {"integral": 0, "average": 1}[reduction], 1 if transient else 0, len(tg),
+                                           tg.ctypes.data_as(_P), _ptr(U), _ptr(Udot), vals.ctypes.data_as(_P),
+                                           meas.ctypes.data_as(_P)))
+        return vals, meas
 
     def apply_natural(self, F):
         check(lib().rsd_apply_natural(self.ctx.h, self.h, _ptr(F)))

@@ -1332,6 +1332,225 @@ __global__ void __launch_bounds__(128) k_nodal_field(const AsmParams prm, int fi
 	}
 }
 
+// A face point of element e's face f: element coordinates, shape values and reference gradients at
+// the point, the physical point, the Jacobian and the area-scaled outward normal n = cof(J) nRef
+// (LagrangeQuad/Hex::mapFaceToElement, JacobianTransform::computeBoundaryNormal), as k_natural forms them.
+template <int NSD, int P>
+struct FacePoint {
+	static constexpr int N1 = P + 1, NPE = (NSD == 3) ? N1 * N1 * N1 : N1 * N1;
+	double N[NPE], dN[NPE][3], x[3], J[9], n[3];
+	__device__ void eval(const double* __restrict__ xyz, const int32_t* en, int f, double s, double t) {
+		const int axis = f / 2;
+		const double side = (f & 1) ? 1.0 : -1.0;
+		double xi[3] = {0.0, 0.0, 0.0};
+		xi[axis] = side;
+		{
+			int k = 0;
+#pragma unroll
+			for (int d = 0; d < NSD; ++d)
+				if (d != axis) xi[d] = (k++ == 0) ? s : t;
+		}
+		double Nd[3][4], dNd[3][4];
+#pragma unroll
+		for (int d = 0; d < NSD; ++d) lagrange1d(P, xi[d], Nd[d], dNd[d]);
+#pragma unroll
+		for (int i = 0; i < 9; ++i) J[i] = 0.0;
+		x[0] = x[1] = x[2] = 0.0;
+		for (int a = 0; a < NPE; ++a) {
+			const int ix = a % N1, iy = (a / N1) % N1, iz = NSD == 3 ? a / (N1 * N1) : 0;
+			double Na = Nd[0][ix] * Nd[1][iy];
+			dN[a][0] = dNd[0][ix] * Nd[1][iy];
+			dN[a][1] = Nd[0][ix] * dNd[1][iy];
+			if (NSD == 3) { dN[a][0] *= Nd[2][iz]; dN[a][1] *= Nd[2][iz]; dN[a][2] = Nd[0][ix] * Nd[1][iy] * dNd[2][iz]; Na *= Nd[2][iz]; }
+			N[a] = Na;
+			const double* xa = xyz + (int64_t)en[a] * NSD;
+#pragma unroll
+			for (int d = 0; d < NSD; ++d) {
+				x[d] += Na * xa[d];
+#pragma unroll
+				for (int al = 0; al < NSD; ++al) J[d * NSD + al] += dN[a][al] * xa[d];
+			}
+		}
+		if constexpr (NSD == 2) {
+			const double cof[4] = {J[3], -J[2], -J[1], J[0]};
+#pragma unroll
+			for (int d = 0; d < 2; ++d) n[d] = cof[d * 2 + axis] * side;
+			n[2] = 0.0;
+		} else {
+			const double cof[9] = {J[4] * J[8] - J[5] * J[7], -(J[3] * J[8] - J[5] * J[6]), J[3] * J[7] - J[4] * J[6],
+			                       -(J[1] * J[8] - J[2] * J[7]), J[0] * J[8] - J[2] * J[6], -(J[0] * J[7] - J[1] * J[6]),
+			                       J[1] * J[5] - J[2] * J[4], -(J[0] * J[5] - J[2] * J[3]), J[0] * J[4] - J[1] * J[3]};
+#pragma unroll
+			for (int d = 0; d < 3; ++d) n[d] = cof[d * 3 + axis] * side;
+		}
+	}
+};
+
+// HeatFlux monitor, Strong method (BoundaryQuadratureMonitorGroup with HeatFluxIntegrand,
+// equation/heateq/quantity/HeatFluxIntegrand.hpp:24-40, QuantityEvaluator.tpp:14-90): per listed face
+// (element, face, tag slot) the sum over the face's Gauss points of -(K grad T) . n w, T gathered Full,
+// K = k(T) kS times the element factor, and the face's measure sum |n| w; out[2 slot], out[2 slot + 1]
+template <int NSD, int P>
+__global__ void __launch_bounds__(128) k_flux_strong(const AsmParams prm, int64_t nfaces, const int32_t* __restrict__ faces,
+                                                     FaceRule rule, double* __restrict__ out) {
+	using FP = FacePoint<NSD, P>;
+	constexpr int NPE = FP::NPE;
+	const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+	if (i >= nfaces) return;
+	const int64_t e = faces[3 * i];
+	const int f = faces[3 * i + 1], slot = faces[3 * i + 2];
+	const int32_t* en = prm.ien + e * NPE;
+	double Ue[NPE];
+	for (int a = 0; a < NPE; ++a) {
+		const int32_t v = en[a], r = prm.t2a[v];
+		Ue[a] = r >= 0 ? (prm.U ? prm.U[r] : 0.0) : prm.g[v];
+	}
+	const double ke = prm.kElem ? prm.kElem[e] : 1.0;
+	double flux = 0.0, meas = 0.0;
+	const int nqf = (NSD == 3) ? rule.n * rule.n : rule.n;
+	FP fp;
+	for (int q = 0; q < nqf; ++q) {
+		const int qs = q % rule.n, qt = q / rule.n;
+		const double w = NSD == 3 ? rule.w[qs] * rule.w[qt] : rule.w[qs];
+		fp.eval(prm.xyz, en, f, rule.x[qs], NSD == 3 ? rule.x[qt] : 0.0);
+		double inv[9];
+		jac_geom<NSD, true>(fp.J, inv);
+		double T = 0.0, gxi[3] = {0.0, 0.0, 0.0};
+		for (int a = 0; a < NPE; ++a) {
+			T += fp.N[a] * Ue[a];
+#pragma unroll
+			for (int al = 0; al < NSD; ++al) gxi[al] += fp.dN[a][al] * Ue[a];
+		}
+		double g[3], kg[3];
+#pragma unroll
+		for (int d = 0; d < NSD; ++d) {
+			double v = 0.0;
+#pragma unroll
+			for (int al = 0; al < NSD; ++al) v += inv[d * NSD + al] * gxi[al];
+			g[d] = v;
+		}
+		shape_apply<NSD>(prm, g, kg);
+		const double k = ke * (prm.kExpr.n ? eval_expr(prm.kExpr, 0.0, 0.0, 0.0, 0.0, T) : prm.kConst);
+		double fl = 0.0, nn = 0.0;
+#pragma unroll
+		for (int d = 0; d < NSD; ++d) { fl -= (k * kg[d]) * fp.n[d]; nn += fp.n[d] * fp.n[d]; }
+		flux += fl * w;
+		meas += sqrt(nn) * w;
+	}
+	atomicAdd(out + 2 * slot, flux);
+	atomicAdd(out + 2 * slot + 1, meas);
+}
+
+// HeatFlux monitor, Weak method (BoundaryReactionMonitorGroup, QuantityEvaluator.tpp:92-200): per listed
+// element the element vector of the source minus Diffusion on U (Full) minus, when transient, rho cp Mass
+// on Udot (Free), models at the element's T; then, face by face in order, each face on a requested tag adds
+// its Gauss measure to that tag and the entries of its nodes not already claimed by the same tag in this
+// element.  ftag[i * nfaces + f] is the tag slot of face f of element elems[i], or -1.
+template <int NSD, int P>
+__global__ void __launch_bounds__(64) k_flux_weak(const AsmParams prm, int64_t nel, const int32_t* __restrict__ elems,
+                                                  const int32_t* __restrict__ ftag, int nfaces, int G, FaceRule rule,
+                                                  double* __restrict__ out) {
+	using FP = FacePoint<NSD, P>;
+	constexpr int N1 = P + 1, NPE = FP::NPE, NFN = (NSD == 3) ? N1 * N1 : N1;
+	const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+	if (i >= nel) return;
+	const int64_t e = elems[i];
+	const int32_t* en = prm.ien + e * NPE;
+	double Ue[NPE], Ud[NPE], Oe[NPE];
+	for (int a = 0; a < NPE; ++a) {
+		const int32_t v = en[a], r = prm.t2a[v];
+		Ue[a] = r >= 0 ? (prm.U ? prm.U[r] : 0.0) : prm.g[v];
+		Ud[a] = (r >= 0 && prm.Udot) ? prm.Udot[r] : 0.0;
+		Oe[a] = 0.0;
+	}
+	const double ke = prm.kElem ? prm.kElem[e] : 1.0;
+	const double* wq = prm.tables + (size_t)prm.nq * G * 4;
+	for (int q = 0; q < prm.nq; ++q) {
+		const double* tq = prm.tables + (size_t)q * G * 4;
+		double J[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, gxi[3] = {0.0, 0.0, 0.0}, x[3] = {0.0, 0.0, 0.0};
+		double T = 0.0, Tr = 0.0;
+		for (int a = 0; a < NPE; ++a) {
+			const double* ta = tq + a * 4;
+			const double* xa = prm.xyz + (int64_t)en[a] * NSD;
+			T += ta[0] * Ue[a];
+			Tr += ta[0] * Ud[a];
+#pragma unroll
+			for (int d = 0; d < NSD; ++d) {
+				x[d] += ta[0] * xa[d];
+#pragma unroll
+				for (int al = 0; al < NSD; ++al) J[d * NSD + al] += ta[1 + al] * xa[d];
+			}
+#pragma unroll
+			for (int al = 0; al < NSD; ++al) gxi[al] += ta[1 + al] * Ue[a];
+		}
+		double inv[9];
+		const double wm = sqrt(jac_geom<NSD, true>(J, inv)) * wq[q];
+		double g[3], kg[3];
+#pragma unroll
+		for (int d = 0; d < NSD; ++d) {
+			double v = 0.0;
+#pragma unroll
+			for (int al = 0; al < NSD; ++al) v += inv[d * NSD + al] * gxi[al];
+			g[d] = v;
+		}
+		shape_apply<NSD>(prm, g, kg);
+		const double k = ke * (prm.kExpr.n ? eval_expr(prm.kExpr, 0.0, 0.0, 0.0, 0.0, T) : prm.kConst);
+		const double fsrc = prm.srcExpr.n ? eval_expr(prm.srcExpr, prm.time, x[0], x[1], NSD == 3 ? x[2] : 0.0, 0.0) : 0.0;
+		const double cp = prm.cpExpr.n ? eval_expr(prm.cpExpr, 0.0, 0.0, 0.0, 0.0, T) : prm.cp;
+		const double mass = prm.cMass != 0.0 ? prm.rho * cp * Tr : 0.0;   // cMass = 1: the transient term
+		for (int a = 0; a < NPE; ++a) {
+			const double* ta = tq + a * 4;
+			double dN[3];
+#pragma unroll
+			for (int d = 0; d < NSD; ++d) {
+				double v = 0.0;
+#pragma unroll
+				for (int al = 0; al < NSD; ++al) v += inv[d * NSD + al] * ta[1 + al];
+				dN[d] = v;
+			}
+			double dk = 0.0;
+#pragma unroll
+			for (int d = 0; d < NSD; ++d) dk += dN[d] * kg[d];
+			Oe[a] += (fsrc * ta[0]) * wm - (k * dk) * wm - (mass * ta[0]) * wm;
+		}
+	}
+	int claimed[NPE];
+	for (int a = 0; a < NPE; ++a) claimed[a] = -1;
+	const int nqf = (NSD == 3) ? rule.n * rule.n : rule.n;
+	FP fp;
+	for (int f = 0; f < nfaces; ++f) {
+		const int slot = ftag[i * nfaces + f];
+		if (slot < 0) continue;
+		double meas = 0.0;
+		for (int q = 0; q < nqf; ++q) {
+			const int qs = q % rule.n, qt = q / rule.n;
+			const double w = NSD == 3 ? rule.w[qs] * rule.w[qt] : rule.w[qs];
+			fp.eval(prm.xyz, en, f, rule.x[qs], NSD == 3 ? rule.x[qt] : 0.0);
+			double nn = 0.0;
+#pragma unroll
+			for (int d = 0; d < NSD; ++d) nn += fp.n[d] * fp.n[d];
+			meas += sqrt(nn) * w;
+		}
+		atomicAdd(out + 2 * slot + 1, meas);
+		const int axis = f / 2;
+		double r = 0.0;
+		for (int b = 0; b < NFN; ++b) {
+			const int u = b % N1, v = b / N1;
+			int id[3] = {0, 0, 0};
+			id[axis] = (f & 1) ? P : 0;
+			{
+				int k = 0;
+#pragma unroll
+				for (int d = 0; d < NSD; ++d)
+					if (d != axis) id[d] = (k++ == 0) ? u : v;
+			}
+			const int a = id[0] + N1 * id[1] + (NSD == 3 ? N1 * N1 * id[2] : 0);
+			if (claimed[a] != slot) { r += Oe[a]; claimed[a] = slot; }
+		}
+		atomicAdd(out + 2 * slot, r);
+	}
+}
+
 __global__ void k_nodal_finish(int64_t nnodes, int nc, const double* __restrict__ wsum, double* __restrict__ acc) {
 	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nnodes * nc; i += (int64_t)gridDim.x * blockDim.x)
 		acc[i] /= wsum[i / nc];
@@ -1965,6 +2184,85 @@ int nodal_field(rsd_ctx* ctx, rsd_heat* h, int field, const double* U, double* o
 	k_nodal_finish<<<vec_grid(ctx, h->m->nnodes * nc), 256, 0, ctx->stream>>>(h->m->nnodes, nc, scratch, out);
 	RSD_CUDA(cudaGetLastError());
 	return RSD_OK;
+}
+
+// HeatProblem's HeatFlux monitors (HeatProblem.tpp:410-440) at the problem's current time: per requested
+// tag, the Strong (boundary quadrature) or Weak (boundary reaction) flux and the tag's measure, into
+// out[2 t], out[2 t + 1] (device, zeroed here); transient adds the weak method's mass term on Udot
+int boundary_flux(rsd_ctx* ctx, rsd_heat* h, int method, int ntags, const int32_t* tags, const double* U, const double* Udot,
+                  bool transient, double* out) {
+	const rsd_mesh* m = h->m;
+	std::map<int32_t, int32_t> slot;
+	for (int t = 0; t < ntags; ++t) {
+		if (tags[t] < 0) return set_error(RSD_EINVAL, "boundary tags are >= 0");
+		if (slot.count(tags[t])) return set_error(RSD_EINVAL, "a tag is requested twice");
+		slot[tags[t]] = t;
+	}
+	AsmParams p = params_for(h);
+	p.U = U;
+	p.Udot = Udot;
+	p.cMass = transient ? 1.0 : 0.0;
+	FaceRule r{};
+	r.n = h->nq1;
+	gauss_legendre(r.n, r.x, r.w);
+	RSD_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * 2 * std::max(ntags, 1), ctx->stream));
+	const int nsd = m->nsd, ord = m->order, nf = m->nfaces;
+	std::vector<int32_t> list, ftag;
+	for (int64_t e = 0; e < m->nelem; ++e) {
+		bool any = false;
+		for (int f = 0; f < nf; ++f) {
+			const int32_t t = m->h_rng[e * nf + f];
+			const auto it = t >= 0 ? slot.find(t) : slot.end();
+			if (it == slot.end()) continue;
+			if (method == RSD_FLUX_STRONG) { list.push_back((int32_t)e); list.push_back(f); list.push_back(it->second); }
+			any = true;
+		}
+		if (method == RSD_FLUX_WEAK && any) {
+			list.push_back((int32_t)e);
+			for (int f = 0; f < nf; ++f) {
+				const int32_t t = m->h_rng[e * nf + f];
+				const auto it = t >= 0 ? slot.find(t) : slot.end();
+				ftag.push_back(it == slot.end() ? -1 : it->second);
+			}
+		}
+	}
+	if (list.empty()) return RSD_OK;
+	int32_t* dl = nullptr;
+	RSD_CUDA(cudaMalloc(&dl, sizeof(int32_t) * (list.size() + ftag.size())));
+	auto launch = [&]() -> int {
+		RSD_CUDA(cudaMemcpyAsync(dl, list.data(), sizeof(int32_t) * list.size(), cudaMemcpyHostToDevice, ctx->stream));
+		if (!ftag.empty())
+			RSD_CUDA(cudaMemcpyAsync(dl + list.size(), ftag.data(), sizeof(int32_t) * ftag.size(), cudaMemcpyHostToDevice, ctx->stream));
+		if (method == RSD_FLUX_STRONG) {
+			const int64_t cnt = (int64_t)list.size() / 3;
+			const int blocks = (int)((cnt + 127) / 128);
+#define RSD_FS(D, Q) k_flux_strong<D, Q><<<blocks, 128, 0, ctx->stream>>>(p, cnt, dl, r, out)
+			if (nsd == 2 && ord == 1) RSD_FS(2, 1);
+			else if (nsd == 2 && ord == 2) RSD_FS(2, 2);
+			else if (nsd == 2 && ord == 3) RSD_FS(2, 3);
+			else if (nsd == 3 && ord == 1) RSD_FS(3, 1);
+			else if (nsd == 3 && ord == 2) RSD_FS(3, 2);
+			else return set_error(RSD_EINVAL, "unsupported element");
+#undef RSD_FS
+		} else {
+			const int64_t cnt = (int64_t)list.size();
+			const int blocks = (int)((cnt + 63) / 64), G = group_width(m->npe);
+#define RSD_FW(D, Q) k_flux_weak<D, Q><<<blocks, 64, 0, ctx->stream>>>(p, cnt, dl, dl + list.size(), nf, G, r, out)
+			if (nsd == 2 && ord == 1) RSD_FW(2, 1);
+			else if (nsd == 2 && ord == 2) RSD_FW(2, 2);
+			else if (nsd == 2 && ord == 3) RSD_FW(2, 3);
+			else if (nsd == 3 && ord == 1) RSD_FW(3, 1);
+			else if (nsd == 3 && ord == 2) RSD_FW(3, 2);
+			else return set_error(RSD_EINVAL, "unsupported element");
+#undef RSD_FW
+		}
+		RSD_CUDA(cudaGetLastError());
+		RSD_CUDA(cudaStreamSynchronize(ctx->stream));
+		return RSD_OK;
+	};
+	const int rc = launch();
+	cudaFree(dl);
+	return rc;
 }
 
 int assemble_diagonal(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, const double* U, double* d, double cTDiff,

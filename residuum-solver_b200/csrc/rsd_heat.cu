@@ -2,6 +2,7 @@
 // steady linear solve, one Backward-Euler step and the Newton loop.
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "rsd_kernels.cuh"
 
@@ -329,6 +330,30 @@ int rsd_heat_solve_fem_forms(rsd_ctx* ctx, rsd_heat* h, double c_tdiff, double c
 	const double* state = (U == nullptr || U == x) ? nullptr : U;
 	if (c_tdiff == 0.0 && c_tmass == 0.0) return solve_fem(ctx, h, c_mass, cfg, b, x, rep, 4, state);
 	return solve_fem(ctx, h, c_mass, cfg, b, x, rep, 10, state, c_tdiff, c_tmass, Udot);
+}
+
+int rsd_heat_boundary_flux(rsd_ctx* ctx, rsd_heat* h, int32_t method, int32_t reduction, int32_t transient, int32_t ntags,
+                           const int32_t* tags, const double* U, const double* Udot, double* values, double* measures) {
+	if (!ctx || !h || ntags < 0 || (ntags && (!tags || !values)) || (h->n && !U)) return set_error(RSD_EINVAL, "null argument");
+	if (method != RSD_FLUX_WEAK && method != RSD_FLUX_STRONG) return set_error(RSD_EINVAL, "unknown flux evaluation method");
+	if (reduction != RSD_REDUCE_INTEGRAL && reduction != RSD_REDUCE_AVERAGE) return set_error(RSD_EINVAL, "unknown monitor reduction");
+	if (ntags == 0) return RSD_OK;
+	double* d = nullptr;
+	RSD_CUDA(cudaMalloc(&d, sizeof(double) * 2 * ntags));
+	int rc = boundary_flux(ctx, h, method, ntags, tags, U, Udot, transient != 0, d);
+	std::vector<double> hv(2 * ntags, 0.0);
+	if (rc == RSD_OK) {
+		const cudaError_t e = cudaMemcpy(hv.data(), d, sizeof(double) * 2 * ntags, cudaMemcpyDeviceToHost);
+		if (e != cudaSuccess) rc = cuda_error(e, "monitor values");
+	}
+	cudaFree(d);
+	RSD_CHECK(rc);
+	for (int t = 0; t < ntags; ++t) {
+		const double meas = hv[2 * t + 1];
+		values[t] = reduction == RSD_REDUCE_AVERAGE ? hv[2 * t] / meas : hv[2 * t];
+		if (measures) measures[t] = meas;
+	}
+	return RSD_OK;
 }
 
 int rsd_apply_dirichlet_lift(rsd_ctx* ctx, rsd_heat* h, double cd, double cm, double* F) {

@@ -259,6 +259,8 @@ int apply_operator(rsd_ctx* ctx, rsd_heat* h, double coef, const double* U, cons
 int set_flux(rsd_ctx* ctx, rsd_heat* h, int tag, const char* const* exprs);
 int apply_natural(rsd_ctx* ctx, rsd_heat* h, double* F);
 int nodal_field(rsd_ctx* ctx, rsd_heat* h, int field, const double* U, double* out, double* scratch);
+int boundary_flux(rsd_ctx* ctx, rsd_heat* h, int method, int ntags, const int32_t* tags, const double* U, const double* Udot,
+                  bool transient, double* out);
 // state null: the iterate x is the state (the stages' linear solves); which, cTDiff, cTMass and Udot as
 // for apply_operator
 int solve_fem(rsd_ctx* ctx, rsd_heat* h, double coef, const rsd_solver_cfg* cfg, const double* b, double* x,

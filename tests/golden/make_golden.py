@@ -1,6 +1,6 @@
 """Generate the golden fixtures in this folder from the reference's own templates.
 
-    python tests/golden/make_golden.py [main] [adjoint] [fem] [models] [transient_adjoint]
+    python tests/golden/make_golden.py [main] [adjoint] [fem] [models] [transient_adjoint] [monitors]
 
 Every array comes from oracle/_ref/libresiduum_ref.so, i.e. the unmodified Residuum templates
 (Assembler<CPU>, BoundaryApplicator<CPU>, TopologicalDOF, cg/gmres::Solver, SteadyStage,
@@ -215,7 +215,34 @@ def transient_adjoint():
          fd_dir=d, fd=fd)
 
 
-GROUPS = {"main": main, "adjoint": adjoint, "fem": fem, "models": models, "transient_adjoint": transient_adjoint}
+def monitors():
+    """HeatFlux monitors through the reference's own monitor groups (oracle/ref_harness.cpp builds them
+    as HeatProblem::makeMonitorGroup does): the weak (boundary reaction, steady and transient) and
+    strong (boundary quadrature of HeatFluxIntegrand) methods, Integral and Average, on a Q2 hex box
+    [0,2]x[0,1]x[0,0.5] with k(T) = 1 + 0.5 T and a 2D Q1 quad [0,1.5]x[0,0.75] with g = (1-x)(1-y)."""
+    cases = {
+        "monitors_q2_hex_kT.npz": dict(args=(3, 2, 3, [3, 3, 2], [0, 0, 0], [2.0, 1.0, 0.5], [0, 1]),
+                                       kw=dict(bc_kind=0, bc_val={0: 0.0, 1: 1.0}, src_kind=0, src_c=10.0, k_a=1.0, k_b=0.5),
+                                       tags=[0, 1, 2, 4]),
+        "monitors_q1_quad.npz": dict(args=(2, 1, 2, [6, 5], [0, 0], [1.5, 0.75], [0, 1, 2, 3]),
+                                     kw=dict(bc_kind=2, src_kind=1, src_c=2.0, rho=1.5, cp=0.8), tags=[0, 1, 2, 3]),
+    }
+    for name, c in cases.items():
+        r = oracle.Reference(*c["args"], **c["kw"])
+        rng = np.random.default_rng(5)
+        U = 0.4 * rng.standard_normal(r.n) + 0.3
+        Ud = rng.standard_normal(r.n)
+        arrays = dict(tags=np.array(c["tags"], np.int32), U=U, Udot=Ud)
+        for method in ("weak", "strong"):
+            for red in ("integral", "average"):
+                arrays[f"{method}_{red}"] = r.boundary_flux(c["tags"], U, Ud, method, red, False)
+        for red in ("integral", "average"):
+            arrays[f"weak_transient_{red}"] = r.boundary_flux(c["tags"], U, Ud, "weak", red, True)
+        save(name, **arrays)
+
+
+GROUPS = {"main": main, "adjoint": adjoint, "fem": fem, "models": models, "transient_adjoint": transient_adjoint,
+          "monitors": monitors}
 
 if __name__ == "__main__":
     if not oracle.reference_available():

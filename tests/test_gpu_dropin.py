@@ -42,10 +42,10 @@ def test_reference_stages_on_the_b200_heat_problem():
     out = subprocess.run([STAGES], capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stdout + out.stderr
     d = json.loads(out.stdout)
-    assert len(d) == 9, d
+    assert len(d) == 8, d
     for name, r in d.items():
         assert r["cpu_ok"] and r["b200_ok"], (name, r)
         assert r["n"] == r["n_b200"], (name, r)
         assert r["max_abs"] > 0.0, (name, r)
-        # FP64 on both sides; the Newton and Krylov tolerances are 1e-10 .. 1e-12
-        assert r["rel_diff"] <= 1e-10, (name, r)
+        # FP64 on both sides, the same iterations: the states agree to rounding
+        assert r["rel_diff"] <= 1e-12, (name, r)

@@ -95,3 +95,28 @@ def test_initial_condition_expression(rsd, ctx):
     h.eval_nodal("x*y + 2*z + t", U, t=0.5)
     X = xyz.reshape(-1, 3)[a2t]
     assert np.allclose(U.download(), X[:, 0] * X[:, 1] + 2 * X[:, 2] + 0.5, rtol=1e-15, atol=1e-15)
+
+
+@pytest.mark.parametrize("name,nsd,order,nq,nel,hi,kw", [
+    ("monitors_q2_hex_kT.npz", 3, 2, 3, [3, 3, 2], [2.0, 1.0, 0.5],
+     dict(k_expr="1 + 0.5*T", dk_expr="0.5", src_expr="10", dirichlet={0: "0", 1: "1"})),
+    ("monitors_q1_quad.npz", 2, 1, 2, [6, 5], [1.5, 0.75],
+     dict(rho=1.5, cp=0.8, src_expr="2*x*y", dirichlet={t: "(1-x)*(1-y)" for t in range(4)})),
+])
+def test_heat_flux_monitors(rsd, ctx, name, nsd, order, nq, nel, hi, kw):
+    """HeatFlux monitors (weak reaction and strong boundary quadrature, Integral and Average, steady
+    and transient) against the reference's own monitor groups."""
+    from importlib import import_module
+    bm = import_module("residuum_solver_b200.blockmesh")
+    g = golden(name)
+    xyz, ien, rng = bm.block_mesh(nsd, nel, [0] * nsd, hi, order)
+    h = rsd.Heat(ctx, rsd.Mesh(ctx, nsd, order, xyz, ien, rng), nq, **kw)
+    U, Ud = ctx.to_device(g["U"]), ctx.to_device(g["Udot"])
+    for method in ("weak", "strong"):
+        for red in ("integral", "average"):
+            v, m = h.boundary_flux(g["tags"], U, Ud, method=method, reduction=red)
+            assert rel(v, g[f"{method}_{red}"]) <= 1e-12, (method, red)
+            assert np.all(m > 0)
+    for red in ("integral", "average"):
+        v, _ = h.boundary_flux(g["tags"], U, Ud, method="weak", reduction=red, transient=True)
+        assert rel(v, g[f"weak_transient_{red}"]) <= 1e-12, red

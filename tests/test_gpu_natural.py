@@ -109,7 +109,12 @@ def test_stages_with_flux_match_restatement(rsd, ctx):
 def test_flux_arguments(rsd, ctx):
     h = make_heat(rsd, ctx, 2, 1, 2, [3, 3], [0, 0], [1, 1], dirichlet={0: "0"})
     with pytest.raises(rsd.RsdError, match="RSD_EINVAL"):
-        h.set_flux(4, ("1", "0"))          # a quad has tags 0-3
+        h.set_flux(-1, ("1", "0"))         # boundary tags are >= 0
+    h.set_flux(9, ("1", "0"))              # any tag may carry a flux; no face has tag 9 here
+    F9 = ctx.array(h.n).zero()
+    h.apply_natural(F9)
+    assert not np.any(F9.download())
+    h.set_flux(9, None)
     with pytest.raises(rsd.RsdError, match="RSD_EPARSE"):
         h.set_flux(1, ("1 +", "0"))
     h.set_flux(1, ("1", "0"))
