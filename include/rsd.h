@@ -179,6 +179,23 @@ int rsd_cg_solve_static(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, con
 int rsd_mesh_create(rsd_ctx* ctx, int32_t nsd, int32_t order, int64_t num_nodes, int64_t num_elements,
                     const double* xyz, const int64_t* ien, const int32_t* rng, rsd_mesh** out);
 int rsd_mesh_destroy(rsd_mesh* m);
+/* PMSH, the reference's binary mesh file (MeshIO::readBinary, src/io/MeshIO.cpp:84-151; layout as
+ * MeshIO::writeBinary writes it, include/io/MeshIO.hpp:16-35).  rsd_pmsh_read runs on the host without a
+ * device: the header into info and, when the arrays are given (each may be NULL), xyz (num_nodes *
+ * spatial_dim), ien (num_elements * nodes_per_element, 64-bit) and rng (num_elements * faces_per_element).
+ * rsd_mesh_read_pmsh reads a Lagrange quadrilateral or hexahedral mesh of equal order in every direction
+ * into a device mesh.  Malformed files give RSD_EINVAL with the reason. */
+typedef struct rsd_pmsh_info {
+	int32_t parametric_dim, spatial_dim;
+	int32_t family;              /* mesh::ElementFamily: 0 Quad, 1 Tri, 2 Hex, 3 Tet, 4 Wedge */
+	int32_t basis;               /* mesh::BasisType: 0 Lagrange, 1 Spline */
+	int64_t num_nodes, num_elements;
+	int32_t nodes_per_element, faces_per_element;
+	int32_t num_orders, order[3];
+	int32_t iga;                 /* extraction operators present */
+} rsd_pmsh_info;
+int rsd_pmsh_read(const char* path, rsd_pmsh_info* info, double* xyz, int64_t* ien, int32_t* rng);
+int rsd_mesh_read_pmsh(rsd_ctx* ctx, const char* path, rsd_mesh** out);
 
 /* ---- heat problem: HeatProblem<CUDA, HeatEquation<NSD,NSD,Family>>
  *      (application/heateq/problem/HeatProblem.hpp:34-206).  Expression strings use the

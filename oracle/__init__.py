@@ -515,6 +515,7 @@ def _refp_lib():
         L.refp_pattern.argtypes = [_P, _P, _P]
         L.refp_assemble_matrix.argtypes = [_P, C.c_int, _D, _D, _P, _P, _P]
         L.refp_assemble_vector.argtypes = [_P, C.c_int, _D, _P, _P, _P]
+        L.refp_write_pmsh.argtypes = [C.POINTER(_RefpDesc), C.c_char_p]
         _refp_bound = True
     return L
 
@@ -673,3 +674,20 @@ def ref_transient_adjoint(nel, theta, U0, dt, nsteps, Uobs, bc_val=None, tol=1e-
         mu_next = mu
     J = 0.5 * float(np.sum((states[-1] - Uobs) ** 2))
     return states[-1], J, -np.exp(theta) * g, its
+
+
+def ref_write_pmsh(path, nsd, order, nel, lo, hi, tag_map=None):
+    """The reference's BlockMesh2D/3D mesh (boundary tags renumbered by tag_map) written by its own
+    MeshIO::writeBinary to `path`; returns the mesh arrays (xyz, ien, rng) the reference built."""
+    L = _refp_lib()
+    d = _RefpDesc()
+    d.nsd, d.order = nsd, order
+    nel = list(nel) + [1] * (3 - len(nel))
+    for i in range(3):
+        d.nel[i] = nel[i]
+    for i in range(nsd):
+        d.lo[i], d.hi[i] = lo[i], hi[i]
+    for t in range(6):
+        d.tag_map[t] = (tag_map or {}).get(t, -1)
+    if L.refp_write_pmsh(C.byref(d), path.encode()):
+        raise RuntimeError(L.refp_last_error().decode())

@@ -25,6 +25,7 @@
 #include "equation/heateq/HeatEquation.hpp"
 #include "mesh/generator/BlockMesh2D.hpp"
 #include "mesh/generator/BlockMesh3D.hpp"
+#include "io/MeshIO.hpp"
 #include "solver/driver/Steady.hpp"
 #include "solver/driver/Transient.hpp"
 #include "solver/stage/SteadyStage.hpp"
@@ -336,6 +337,10 @@ int64_t refp_nnz(void* h) { return static_cast<Base*>(h)->nnz(); }
 void refp_pattern(void* h, int64_t* rp, int64_t* col) { static_cast<Base*>(h)->pattern(rp, col); }
 int refp_assemble_matrix(void* h, int formset, double c, double t, const double* U, const double* Udot, double* val) {
 	try { static_cast<Base*>(h)->assembleMatrix(formset, c, t, U, Udot, val); return 0; } catch (const std::exception& e) { g_err = e.what(); return -1; }
+}
+// the reference's block mesh (tags renumbered by the description) written by MeshIO::writeBinary
+int refp_write_pmsh(const refp_desc* d, const char* path) {
+	try { io::MeshIO::writeBinary(make_mesh(*d), path); return 0; } catch (const std::exception& e) { g_err = e.what(); return -1; }
 }
 int refp_assemble_vector(void* h, int which, double t, const double* U, const double* Udot, double* out) {
 	try { static_cast<Base*>(h)->assembleVector(which, t, U, Udot, out); return 0; } catch (const std::exception& e) { g_err = e.what(); return -1; }

@@ -59,6 +59,12 @@ class HeatDesc(C.Structure):
                 ("dirichlet_tags", _P), ("dirichlet_exprs", _P)]
 
 
+class PmshInfo(C.Structure):
+    _fields_ = [("parametric_dim", _I32), ("spatial_dim", _I32), ("family", _I32), ("basis", _I32), ("num_nodes", _I64),
+                ("num_elements", _I64), ("nodes_per_element", _I32), ("faces_per_element", _I32), ("num_orders", _I32),
+                ("order", _I32 * 3), ("iga", _I32)]
+
+
 _lib = None
 
 # (name, argtypes) for every entry point of include/rsd.h
@@ -107,6 +113,8 @@ SIGNATURES = {
     "rsd_cg_solve_static": [_P, _P, C.POINTER(SolverConfig), _P, _P, C.POINTER(Report)],
     "rsd_mesh_create": [_P, _I32, _I32, _I64, _I64, _P, _P, _P, C.POINTER(_P)],
     "rsd_mesh_destroy": [_P],
+    "rsd_pmsh_read": [C.c_char_p, C.POINTER(PmshInfo), _P, _P, _P],
+    "rsd_mesh_read_pmsh": [_P, C.c_char_p, C.POINTER(_P)],
     "rsd_heat_create": [_P, _P, C.POINTER(HeatDesc), C.POINTER(_P)],
     "rsd_heat_destroy": [_P],
     "rsd_heat_info": [_P, C.POINTER(_I64), C.POINTER(_I64)],
@@ -404,6 +412,32 @@ class Mesh:
                 lib().rsd_mesh_destroy(self.h)
         except Exception:
             pass
+
+
+def read_pmsh(path):
+    """A PMSH mesh file on the host: (info dict, xyz, ien, rng), as MeshIO::readBinary reads it."""
+    info = PmshInfo()
+    check(lib().rsd_pmsh_read(path.encode(), C.byref(info), None, None, None))
+    xyz = np.zeros(info.num_nodes * info.spatial_dim)
+    ien = np.zeros(info.num_elements * info.nodes_per_element, np.int64)
+    rng = np.zeros(info.num_elements * info.faces_per_element, np.int32)
+    check(lib().rsd_pmsh_read(path.encode(), C.byref(info), xyz.ctypes.data_as(_P), ien.ctypes.data_as(_P), rng.ctypes.data_as(_P)))
+    d = {k: getattr(info, k) for k, _ in PmshInfo._fields_ if k != "order"}
+    d["order"] = list(info.order)[: info.num_orders]
+    return d, xyz, ien, rng
+
+
+class PmshMesh(Mesh):
+    """A device mesh read from a PMSH file (rsd_mesh_read_pmsh)."""
+
+    def __init__(self, ctx, path):
+        info, _, _, _ = read_pmsh(path)
+        self.ctx = ctx
+        self.nsd, self.order = info["spatial_dim"], info["order"][0]
+        self.npe = info["nodes_per_element"]
+        self.nnodes, self.nelem = info["num_nodes"], info["num_elements"]
+        self.h = _P()
+        check(lib().rsd_mesh_read_pmsh(ctx.h, path.encode(), C.byref(self.h)))
 
 
 class Heat:

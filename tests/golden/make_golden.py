@@ -1,6 +1,6 @@
 """Generate the golden fixtures in this folder from the reference's own templates.
 
-    python tests/golden/make_golden.py [main] [adjoint] [fem] [models] [transient_adjoint] [monitors]
+    python tests/golden/make_golden.py [main] [adjoint] [fem] [models] [transient_adjoint] [monitors] [pmsh]
 
 Every array comes from oracle/_ref/libresiduum_ref.so, i.e. the unmodified Residuum templates
 (Assembler<CPU>, BoundaryApplicator<CPU>, TopologicalDOF, cg/gmres::Solver, SteadyStage,
@@ -241,8 +241,24 @@ def monitors():
         save(name, **arrays)
 
 
+def pmsh():
+    """PMSH mesh files written by the reference's own MeshIO::writeBinary from its block meshes (a Q2 hex
+    box with tag 0 renumbered to 9, a Q1 quad), with the reference's arrays beside them."""
+    for name, args, tags in (("block_q2_hex_3x2x2", (3, 2, [3, 2, 2], [0, 0, 0], [1.0, 0.5, 0.5]), {0: 9}),
+                             ("block_q1_quad_5x4", (2, 1, [5, 4], [0, 0], [1.0, 1.0]), None)):
+        path = os.path.join(HERE, name + ".pmsh")
+        oracle.ref_write_pmsh(path, *args, tag_map=tags)
+        print(path, os.path.getsize(path))
+        nsd, order, nel, lo, hi = args
+        m = oracle.BlockMesh(nsd, nel, lo, hi, order)
+        rng = m.rng.copy()
+        for a, b in (tags or {}).items():
+            rng[rng == a] = b
+        save(name + ".npz", xyz=m.xyz, ien=m.ien, rng=rng)
+
+
 GROUPS = {"main": main, "adjoint": adjoint, "fem": fem, "models": models, "transient_adjoint": transient_adjoint,
-          "monitors": monitors}
+          "monitors": monitors, "pmsh": pmsh}
 
 if __name__ == "__main__":
     if not oracle.reference_available():

@@ -120,3 +120,20 @@ def test_heat_flux_monitors(rsd, ctx, name, nsd, order, nq, nel, hi, kw):
     for red in ("integral", "average"):
         v, _ = h.boundary_flux(g["tags"], U, Ud, method="weak", reduction=red, transient=True)
         assert rel(v, g[f"weak_transient_{red}"]) <= 1e-12, red
+
+
+def test_pmsh_mesh_solves_like_the_block_mesh(rsd, ctx):
+    """A PMSH file written by the reference's MeshIO (block tag 0 renumbered to 9) read into a device
+    mesh gives the DOF map and steady solution of the same mesh built in memory."""
+    import os
+    from conftest import GOLDEN
+    path = os.path.join(GOLDEN, "block_q2_hex_3x2x2.pmsh")
+    g = golden("block_q2_hex_3x2x2.npz")
+    bc = {9: "x*y", 1: "1"}
+    hp = rsd.Heat(ctx, rsd.PmshMesh(ctx, path), 3, src_expr="1", dirichlet=bc)
+    hb = rsd.Heat(ctx, rsd.Mesh(ctx, 3, 2, g["xyz"], g["ien"], g["rng"]), 3, src_expr="1", dirichlet=bc)
+    assert (hp.dofmap()[0] == hb.dofmap()[0]).all()
+    Up, Ub = ctx.array(hp.n).zero(), ctx.array(hb.n).zero()
+    hp.steady(Up, tol=1e-12)
+    hb.steady(Ub, tol=1e-12)
+    assert np.array_equal(Up.download(), Ub.download())
