@@ -170,7 +170,7 @@ static void parallel_for(int64_t n, Fn&& fn) {
 // Face-node lists are LagrangeQuad/Hex::getFaceNodes (fem/basis/LagrangeQuad.tpp:136-155,
 // fem/basis/LagrangeHex.tpp:263-304).
 // ---------------------------------------------------------------------------------------------
-static int face_nodes(int nsd, int p, int f, int* out) {
+int face_nodes(int nsd, int p, int f, int* out) {
 	const int q = p + 1;
 	int k = 0;
 	if (nsd == 2) {
@@ -191,6 +191,12 @@ static int face_nodes(int nsd, int p, int f, int* out) {
 			out[k++] = v;
 		}
 	return k;
+}
+
+// the device builds the DOF map and the pattern unless RSD_HOST_SETUP=1 selects the host loops
+bool device_setup() {
+	const char* env = getenv("RSD_HOST_SETUP");
+	return !(env && env[0] == '1');
 }
 
 int build_dofmap(rsd_heat* h) {
@@ -458,6 +464,12 @@ static int upload_csr(rsd_ctx* ctx, int64_t n, const std::vector<int32_t>& rp, c
 // sorted, unique free columns of every element touching free DOF i.  Built per row from a
 // node->element incidence list, in parallel on the host (one-time setup).
 int build_pattern(rsd_ctx* ctx, const rsd_heat* h, rsd_csr** out) {
+	if (device_setup()) {
+		std::vector<int32_t> rp, col;
+		bool fallback = false;
+		RSD_CHECK(device_pattern(ctx, h, rp, col, &fallback));
+		if (!fallback) return upload_csr(ctx, h->n, rp, col, nullptr, out);
+	}
 	const rsd_mesh* m = h->m;
 	const int64_t n = h->n, nn = m->nnodes, ne = m->nelem;
 	const int npe = m->npe;

@@ -176,17 +176,24 @@ int rsd_heat_create(rsd_ctx* ctx, const rsd_mesh* m, const rsd_heat_desc* d, rsd
 		if (!d->dirichlet_exprs[i]) { delete h; return set_error(RSD_EINVAL, "Dirichlet tag without an expression"); }
 		if ((rc = add_bc(d->dirichlet_tags[i], d->dirichlet_exprs[i]))) { delete h; return rc; }
 	}
-	build_dofmap(h);
 	cudaError_t e;
-	const int64_t nn = m->nnodes, n = std::max<int64_t>(h->n, 1);
-	if ((e = cudaMalloc(&h->t2a, sizeof(int32_t) * nn)) != cudaSuccess || (e = cudaMalloc(&h->g, sizeof(double) * nn)) != cudaSuccess ||
+	const int64_t nn = m->nnodes;
+	if ((e = cudaMalloc(&h->t2a, sizeof(int32_t) * nn)) != cudaSuccess) { free_heat(h); return cuda_error(e, "dof map allocation"); }
+	const bool onDevice = device_setup();
+	if (onDevice) {
+		if ((rc = device_dofmap(ctx, h))) { free_heat(h); return rc; }
+	} else {
+		build_dofmap(h);
+	}
+	const int64_t n = std::max<int64_t>(h->n, 1);
+	if ((e = cudaMalloc(&h->g, sizeof(double) * nn)) != cudaSuccess ||
 	    (e = cudaMalloc(&h->F, sizeof(double) * n)) != cudaSuccess || (e = cudaMalloc(&h->R, sizeof(double) * n)) != cudaSuccess ||
 	    (e = cudaMalloc(&h->Udot, sizeof(double) * n)) != cudaSuccess || (e = cudaMalloc(&h->ms, sizeof(double) * n)) != cudaSuccess ||
 	    (e = cudaMalloc(&h->dU, sizeof(double) * n)) != cudaSuccess) {
 		free_heat(h);
 		return cuda_error(e, "heat problem allocation");
 	}
-	if ((e = cudaMemcpyAsync(h->t2a, h->h_t2a.data(), sizeof(int32_t) * nn, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) { free_heat(h); return cuda_error(e, "dof map upload"); }
+	if (!onDevice && (e = cudaMemcpyAsync(h->t2a, h->h_t2a.data(), sizeof(int32_t) * nn, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) { free_heat(h); return cuda_error(e, "dof map upload"); }
 	if (d->k_elem) {
 		if ((e = cudaMalloc(&h->kElem, sizeof(double) * m->nelem)) != cudaSuccess ||
 		    (e = cudaMemcpyAsync(h->kElem, d->k_elem, sizeof(double) * m->nelem, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) {

@@ -241,6 +241,10 @@ struct rsd_heat {
 
 namespace rsd {
 int build_dofmap(rsd_heat* h);
+int face_nodes(int nsd, int p, int f, int* out);      // element-local nodes of face f (getFaceNodes order)
+bool device_setup();                                  // DOF map and pattern on the device (RSD_HOST_SETUP=1: host)
+int device_dofmap(rsd_ctx* ctx, rsd_heat* h);         // needs h->t2a allocated
+int device_pattern(rsd_ctx* ctx, const rsd_heat* h, std::vector<int32_t>& rp, std::vector<int32_t>& col, bool* fallback);
 int build_pattern(rsd_ctx* ctx, const rsd_heat* h, rsd_csr** out);
 int upload_bc_values(rsd_ctx* ctx, rsd_heat* h);
 int assemble_matrix(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, double cTDiff, double cTMass,

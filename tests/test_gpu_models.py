@@ -137,3 +137,37 @@ def test_pmsh_mesh_solves_like_the_block_mesh(rsd, ctx):
     hp.steady(Up, tol=1e-12)
     hb.steady(Ub, tol=1e-12)
     assert np.array_equal(Up.download(), Ub.download())
+
+
+@pytest.mark.parametrize("nsd,order,nel,dirichlet,perm", [
+    (3, 1, [7, 6, 5], {0: "0", 3: "x", 5: "1"}, False),
+    (3, 2, [4, 3, 3], {9: "0", 1: "1"}, True),
+    (2, 3, [6, 4], {0: "0", 2: "y", 3: "1"}, True),
+    (2, 1, [9, 8], {}, False),
+])
+def test_device_setup_matches_host_setup(rsd, ctx, monkeypatch, nsd, order, nel, dirichlet, perm):
+    """The DOF map and CSR pattern built on the device (the default) equal the host build
+    (RSD_HOST_SETUP=1) bit for bit, on block meshes and on block meshes with shuffled node numbers."""
+    from importlib import import_module
+    bm = import_module("residuum_solver_b200.blockmesh")
+    xyz, ien, rng = bm.block_mesh(nsd, nel, [0] * nsd, [1] * nsd, order)
+    rng = rng.copy()
+    if 9 in dirichlet:
+        rng[rng == 0] = 9
+    if perm:
+        nn = xyz.size // nsd
+        p = np.random.default_rng(1).permutation(nn)      # new id of old node v is p[v]
+        x2 = np.empty_like(xyz.reshape(nn, nsd))
+        x2[p] = xyz.reshape(nn, nsd)
+        xyz, ien = x2.reshape(-1), p[ien]
+    out = []
+    for host in ("1", "0"):
+        monkeypatch.setenv("RSD_HOST_SETUP", host)
+        h = rsd.Heat(ctx, rsd.Mesh(ctx, nsd, order, xyz, ien, rng), order + 1, src_expr="1", dirichlet=dirichlet)
+        t2a, a2t = h.dofmap()
+        rp, col = h.K.pattern()
+        U = ctx.array(h.n).zero()
+        h.steady(U, tol=1e-12, max_iters=5000)
+        out.append((t2a, a2t, rp, col, U.download()))
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
