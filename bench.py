@@ -710,6 +710,70 @@ def run_adjoint(rsd, ctx, stream, S, ndir):
             "tangent_linear_max_rel_error": max(terrs), "tangent_linear_median_rel_error": float(np.median(terrs))}
 
 
+def run_transient_adjoint(rsd, ctx, stream, S, nsteps, ndir, cpu):
+    """Transient adjoint on S^3 Q1 hexes: k_e = exp(theta_e) (16 seeded Fourier modes, seed 5), f = 1,
+    T = 0 on the boundary, nsteps Backward-Euler steps of dt = 1e-3 from the sine-mode T0 (seed 2),
+    J = 0.5 ||U_N - U_obs||^2 with U_obs = T0 / 2; CG + Jacobi to 1e-14.  The adjoint gradient against
+    central differences (h = 1e-6) along `ndir` directions through the device steps, and against the FP64
+    CPU adjoint on the reference's templates (oracle.ref_transient_adjoint) when `cpu`."""
+    import torch
+    from importlib import import_module
+    bm = import_module("residuum_solver_b200.blockmesh")
+    xyz, ien, rg = bm.block_mesh(3, [S] * 3, [0, 0, 0], [1, 1, 1], 1)
+    h = rsd.Heat(ctx, rsd.Mesh(ctx, 3, 1, xyz, ien, rg), 2, src_expr="1", dirichlet={t: "0" for t in range(6)})
+    ne, n, dt = S ** 3, h.n, 1e-3
+    th = fourier_theta(xyz, ien, 8, 5)
+    t2a, a2t = h.dofmap()
+    u0 = initial_condition(xyz, a2t)
+    uobs = 0.5 * u0
+    cfg = rsd.SolverConfig.make(tol=1e-14, max_iters=100000)
+    theta, U0, U, grad, dJdU = ctx.to_device(th), ctx.to_device(u0), ctx.array(n), ctx.array(ne), ctx.array(n)
+    times = []
+    for _ in range(3):
+        e0, e1, e2, e3 = (torch.cuda.Event(enable_timing=True) for _ in range(4))
+        e0.record(stream)
+        rf = h.transient_forward(theta, U0, U, 0.0, dt, nsteps, cfg)
+        e1.record(stream)
+        dJdU.upload(U.download() - uobs)
+        e2.record(stream)
+        rb = h.transient_backward(theta, U0, dJdU, grad, 0.0, dt, nsteps, cfg)
+        e3.record(stream)
+        e3.synchronize()
+        times.append((e0.elapsed_time(e1), e2.elapsed_time(e3)))
+    g = grad.download()
+    u = uniforms(mt19937_64_stream(555, 2 * ne * ndir)).reshape(ndir, ne, 2)
+    dirs = np.sqrt(-2.0 * np.log1p(-u[..., 0])) * np.cos(2.0 * np.pi * u[..., 1])
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    hstep = 1e-6
+    Ut = ctx.array(n)
+
+    def J(t):
+        h.transient_forward(ctx.to_device(t), U0, Ut, 0.0, dt, nsteps, cfg)
+        return 0.5 * float(np.sum((Ut.download() - uobs) ** 2))
+    errs = []
+    for d in dirs:
+        fd = (J(th + hstep * d) - J(th - hstep * d)) / (2 * hstep)
+        errs.append(abs(fd - g @ d) / abs(fd))
+    fwd, bwd = (float(np.median([t[i] for t in times])) for i in (0, 1))
+    out = {"workload": f"{S}^3 Q1 hexes, k_e = exp(theta_e), {nsteps} Backward-Euler steps dt = {dt}, J = 0.5||U_N - U_obs||^2, "
+                       f"CG + Jacobi 1e-14",
+           "n_free": n, "elements": ne, "forward_ms": fwd, "backward_ms": bwd, "states_held": rb["states_held"],
+           "forward_iterations": rf["iterations"], "adjoint_iterations": rb["iterations"],
+           "forward_iterations_in_backward": rb["refinements"], "fd_directions": ndir, "fd_max_rel_error": max(errs),
+           "fd_median_rel_error": float(np.median(errs))}
+    if cpu:
+        import oracle
+        if oracle.reference_available():
+            t0 = time.perf_counter()
+            uN, Jr, gr, its = oracle.ref_transient_adjoint([S] * 3, th, u0, dt, nsteps, uobs, tol=1e-14)
+            out["cpu_adjoint"] = {"ms": 1e3 * (time.perf_counter() - t0), "cores": 1, "kind": "reference",
+                                  "max_rel_diff_gradient": float(np.max(np.abs(g - gr)) / np.max(np.abs(gr))),
+                                  "max_rel_diff_state": float(np.max(np.abs(U.download() - uN)) / np.max(np.abs(uN))),
+                                  "how": "forward steps by the reference's BackwardEulerStage, adjoint solves by its cg::Solver + "
+                                         "Jacobi on its K + M/dt, element terms by its DiffusionForm (oracle/_ref), 1 core"}
+    return out
+
+
 METRIC = "time to a 1e-8 FP64-checked relative residual per Backward-Euler step, mixed FP32/FP64 CG+Jacobi (FP64 CG alongside)"
 WORKLOAD = ("3D transient heat, unit cube, {S}^3 Q1 hexes, k = rho*cp = 1, Backward Euler dt = 1e-3, "
             "T0 = 8 seeded sine modes (amplitude 0.1, seed 2), Dirichlet T = 0 on all faces")
@@ -730,6 +794,8 @@ def main():
     ap.add_argument("--adjoint", type=int, default=96, help="mesh size of the adjoint workload (0: skip it)")
     ap.add_argument("--fem", type=int, default=48, help="Q2 mesh size of the matrix-free operator workload (0: skip it)")
     ap.add_argument("--fd-directions", type=int, default=20)
+    ap.add_argument("--transient-adjoint", type=int, default=48, help="mesh size of the transient adjoint workload (0: skip it)")
+    ap.add_argument("--transient-steps", type=int, default=10)
     ap.add_argument("--only", choices=["mixed", "fp64", "fem-product"], default=None,
                     help="run one solver path only (no e2e, no CPU leg), or 4 matrix-free products on the "
                          "--fem Q2 mesh: for profiler captures")
@@ -882,6 +948,11 @@ def main():
             adjoint["cpu_baseline"] = adjoint_cpu_baseline(rsd, ctx, stream, 48)
         except Exception as e:  # noqa: BLE001
             adjoint["cpu_baseline"] = {"value": None, "sample": f"failed: {e}"}
+
+    tadj = None
+    if args.transient_adjoint > 0:
+        tadj = run_transient_adjoint(rsd, ctx, stream, args.transient_adjoint, args.transient_steps, args.fd_directions,
+                                     cpu=rank == 0 and world == 1 and not args.no_cpu)
 
     fem_op = None
     if args.fem > 0:
@@ -1063,6 +1134,7 @@ def main():
         "newton": newton,
         "fem_operator": fem_op,
         "adjoint": adjoint,
+        "transient_adjoint": tadj,
         "cpu_baseline": cpu,
         "parity_at_size": parity,
         "e2e": {"value": ms_e2e, "unit": "ms", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
