@@ -502,6 +502,65 @@ def fem_steady(rsd, ctx, stream, S, op, reps=3):
     return h, U.download(), rep, float(np.median(ts))
 
 
+def permuted_problem(rsd, bm, ctx, S, seed=7):
+    """The S^3 Q1 Backward-Euler problem of the metric with its node numbers shuffled (seeded), so that
+    the DOF numbering, which follows node order, scatters every row's columns: an unstructured-mesh
+    matrix with no stencil slices.  K + M/dt assembled (dt = 1e-3)."""
+    xyz, ien, rng = bm.block_mesh(3, [S] * 3, [0, 0, 0], [1, 1, 1], 1)
+    nn = xyz.size // 3
+    p = np.random.default_rng(seed).permutation(nn)          # new id of old node v is p[v]
+    x2 = np.empty((nn, 3))
+    x2[p] = xyz.reshape(nn, 3)
+    h = rsd.Heat(ctx, rsd.Mesh(ctx, 3, 1, x2.reshape(-1), p[ien].astype(np.int64), rng), 2,
+                 dirichlet={t: "0" for t in range(6)})
+    h.assemble_matrix(1.0, 1.0 / 1e-3)
+    return h
+
+
+def time_spmv(ctx, stream, A, n, launches=20):
+    """Average CUDA-event time (ms) of one FP64 and one FP32 SpMV over `launches` back-to-back launches
+    (operands of n entries; the matrix is larger than L2, so it streams from HBM every launch)."""
+    import torch
+    x, y = ctx.to_device(np.cos(np.arange(n) * 0.37)), ctx.array(n)
+    x32, y32 = ctx.to_device(np.cos(np.arange(n) * 0.37), np.float32), ctx.array(n, np.float32)
+    A.sync_f32()
+    out = {}
+    for key, f in (("fp64", lambda: A.spmv(x, y)), ("fp32", lambda: A.spmv_f32(x32, y32))):
+        for _ in range(3):
+            f()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(launches):
+            f()
+        e1.record(stream)
+        e1.synchronize()
+        out[key] = e0.elapsed_time(e1) / launches
+    return out
+
+
+def run_unstructured_spmv(rsd, bm, ctx, stream, heat, S, peak):
+    """SpMV on the metric's matrix (stencil slices) and on the same matrix with shuffled node numbers
+    (16/32-bit column indices, gathered x): event-timed, with the CSR byte model (value + 4-byte column
+    per entry, x read and y written once) and its fraction of the HBM peak."""
+    hp = permuted_problem(rsd, bm, ctx, S)
+    out = {"workload": f"{S}^3 Q1 K + M/dt, FP64 and FP32 SpMV, 20 launches each, structured vs node numbers shuffled (seed 7)"}
+    for name, h in (("structured", heat), ("shuffled", hp)):
+        t = time_spmv(ctx, stream, h.K, h.n)
+        lay = h.K.layout()
+        rec = {"n": h.n, "nnz": h.nnz, "stencil_slices": lay["stencil_slices"], "slices": lay["slices"],
+               "sell_slots": lay["sell_slots"]}
+        for key, ms in t.items():
+            vb = 8 if key == "fp64" else 4
+            model = h.nnz * (vb + 4) + 2 * h.n * vb
+            rec[key] = {"us": 1e3 * ms, "csr_model_bytes": model, "csr_model_gbs": model / (ms * 1e-3) / 1e9,
+                        "csr_model_frac": model / (ms * 1e-3) / 1e9 / peak}
+        out[name] = rec
+    out["note"] = ("csr_model counts 4-byte columns; the structured matrix's stencil slices read none, so its "
+                   "model fraction overstates DRAM traffic (the DRAM-traffic figure is in the ncu summary)")
+    del hp
+    return out
+
+
 def run_fem_operator(rsd, ctx, stream, S):
     """The matrix-free operator (operator type fem) against the assembled matrix on S^3 Q2 hexes: the
     whole steady stage both ways, and one operator product (sum-factorized element pass against the
@@ -541,19 +600,21 @@ def run_fem_operator(rsd, ctx, stream, S):
     fp64_rate = rate.value   # TFLOP/s, measured on this GPU
     E = S ** 3
     # bytes: per element the 27 free rows (4 B) and the geometry record (64 B), the operand read and
-    # the result written once; flops: 210 multiply-adds per lane of the kernel, 9 lanes per element
+    # the result written once; flops: about 693 multiply-adds per lane of the kernel (x contraction
+    # 54, nine points of y/z contraction, flux and z back-projection 56 each, y/x back 135), 3 lanes
+    # per element, counted as 2 flops each
     fem_bytes = E * (27 * 4 + 64) + 16 * h.n
-    fem_flops = E * 9 * 210 * 2
+    fem_flops = E * 3 * 693 * 2
     t_hbm = fem_bytes / (measured_peak_hbm()[0] * 1e3)
     t_fp64 = fem_flops / (fp64_rate * 1e6) if fp64_rate else None
     bound = max(t_hbm, t_fp64 or 0.0)
     out["product_us"] = {"csr_spmv_fp64": spmv_us, "fem_sum_factorized": fem_us, "speedup": spmv_us / fem_us}
-    out["product_roofline"] = {"kernel": "k_apply_hex27_lines", "bytes": fem_bytes, "flops": fem_flops,
+    out["product_roofline"] = {"kernel": "k_apply_hex27_planes", "bytes": fem_bytes, "flops": fem_flops,
                                "hbm_us": t_hbm, "fp64_us": t_fp64, "bound": "fp64" if (t_fp64 or 0) > t_hbm else "hbm",
                                "roofline_us": bound, "achieved_us": fem_us, "frac": bound / fem_us,
                                "fp64_tflops": fp64_rate, "hbm_peak_gbs": measured_peak_hbm()[0],
                                "csr_bytes": h.nnz * 12 + 4 * (h.n + 1) + 16 * h.n,
-                               "note": "shared-memory line exchanges bound the kernel (ncu: L1/shared pipe ~90% busy)"}
+                               "note": "three lanes per element, z contraction by shuffles; FP64 pipe is the bound"}
     return out
 
 
@@ -796,9 +857,11 @@ def main():
     ap.add_argument("--fd-directions", type=int, default=20)
     ap.add_argument("--transient-adjoint", type=int, default=48, help="mesh size of the transient adjoint workload (0: skip it)")
     ap.add_argument("--transient-steps", type=int, default=10)
-    ap.add_argument("--only", choices=["mixed", "fp64", "fem-product"], default=None,
-                    help="run one solver path only (no e2e, no CPU leg), or 4 matrix-free products on the "
-                         "--fem Q2 mesh: for profiler captures")
+    ap.add_argument("--only", choices=["mixed", "fp64", "fem-product", "spmv-shuffled"], default=None,
+                    help="run one solver path only (no e2e, no CPU leg), 4 matrix-free products on the "
+                         "--fem Q2 mesh, or 4 FP64 + 4 FP32 SpMV on the --size matrix with shuffled node "
+                         "numbers: for profiler captures")
+    ap.add_argument("--unstructured", type=int, default=1, help="time SpMV on the shuffled-node matrix too (0: skip it)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -837,6 +900,17 @@ def main():
         if rank == 0:
             print(json.dumps({"only": args.only, "n_free": hq.n, "elements": F ** 3}))
         del hq
+        ctx.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    if args.only == "spmv-shuffled":
+        hp = permuted_problem(rsd, bm, ctx, args.size)
+        time_spmv(ctx, stream, hp.K, hp.n, launches=1)
+        if rank == 0:
+            print(json.dumps({"only": args.only, "n_free": hp.n, "nnz": hp.nnz, **hp.K.layout()}))
+        del hp
         ctx.close()
         if dist is not None:
             dist.destroy_process_group()
@@ -931,6 +1005,10 @@ def main():
         solve_t[key] = float(np.median(ts))
         solve_it[key] = r["iterations"]
         solve_tr[key] = r["trueResidualRel"]
+
+    unstructured = None
+    if args.unstructured:
+        unstructured = run_unstructured_spmv(rsd, bm, ctx, stream, heat, S, measured_peak_hbm()[0])
 
     batch = None
     if args.batch > 0:
@@ -1135,6 +1213,7 @@ def main():
         "fem_operator": fem_op,
         "adjoint": adjoint,
         "transient_adjoint": tadj,
+        "spmv_unstructured": unstructured,
         "cpu_baseline": cpu,
         "parity_at_size": parity,
         "e2e": {"value": ms_e2e, "unit": "ms", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},

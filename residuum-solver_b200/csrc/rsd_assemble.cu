@@ -966,49 +966,53 @@ __global__ void __launch_bounds__(256) k_apply_sumfac(const AsmParams prm, const
 	}
 }
 
-// The same product for 27-node hexahedra with one lane per grid line of the element: a warp holds 3
-// elements, lane (p, r) of an element owns the line of 3 values along the axis of the current stage,
-// so each 1D contraction is local to the lane (its 3x3 factors are compile-time indices into the
-// kernel's parameters) and values cross lanes only between stages, through shared memory: 6 line
-// exchanges per element instead of a shuffle per value and factor.
-__global__ void __launch_bounds__(256) k_apply_hex27_lines(const AsmParams prm, const Tab1D t) {
-	// shared-memory layout of one element's arrays: point (x, y, z) at x + 4y + 11z, 33 entries per
-	// array, 3 arrays per element; within an element the 9 lanes of every exchange (a fixed x, y or z)
-	// then fall in distinct banks, and the third element of a warp is shifted by 11 entries to reduce
-	// the conflicts with the second one in the same half-warp
-	constexpr int EPW = 3, NPE = 27, WPB = 8, ARR = 33, SLOT = 3 * ARR, WARPBUF = EPW * SLOT + 11;
+// The same product for 27-node hexahedra with three lanes per element: lane k of an element owns its
+// nodes, and quadrature points, in the plane z = k.  The x and y contractions stay in the lane's
+// registers; only the z contraction crosses lanes, by shuffles among the element's three lanes
+// (forward: this plane's partial sums of the other two planes; backward: the other two points'
+// contributions to this plane's nodes).  The quadrature points are visited one x-point at a time, so
+// a lane keeps the x-contracted lines of its plane, one x-point's temporaries and its nine node sums
+// live.  Ten elements per warp; lanes 30 and 31 compute on nothing and write nothing.
+__global__ void __launch_bounds__(128, 3) k_apply_hex27_planes(const AsmParams prm, const Tab1D t) {
+	constexpr int EPW = 10, NPE = 27;
 	if (prm.skip && *(volatile const int32_t*)prm.skip) return;   // uniform over the launch
-	__shared__ double sbuf[WPB * WARPBUF];
-	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	// lanes 27-31 compute along but write nothing; they read the addresses of lanes 18-22 (the same
-	// half-warp: broadcasts, no extra bank wavefronts)
-	const bool act = lane < EPW * 9;
-	const int slot = act ? lane / 9 : 2, l = act ? lane % 9 : lane - 27, p = l % 3, r = l / 3;
-	double* buf = sbuf + warp * WARPBUF + slot * SLOT + (slot == 2 ? 11 : 0);
-	// buffer entry of array k (0..2) at point (x, y, z)
-	auto at = [&](int k, int x, int y, int z) -> double& { return buf[k * ARR + x + 4 * y + 11 * z]; };
+	const int lane = threadIdx.x & 31, grp = lane / 3, k = lane - 3 * grp;
+	const bool act = grp < EPW;
+	// planes k+1 and k+2 (mod 3) and their lanes; lanes 30/31 (no element) wrap into the warp harmlessly
+	const int k1 = k == 2 ? 0 : k + 1, k2 = k == 0 ? 2 : k - 1;
+	const int src1 = (3 * grp + k1) & 31, src2 = (3 * grp + k2) & 31;
+	auto sel = [](int i, double a, double b, double c) { return i == 0 ? a : (i == 1 ? b : c); };
+	// row k of the 1D tables (point z = k) at nodes k, k+1, k+2, and the point's weight
+	const double cB0 = sel(k, t.B[0][0], t.B[1][1], t.B[2][2]);
+	const double cB1 = sel(k, t.B[0][1], t.B[1][2], t.B[2][0]);
+	const double cB2 = sel(k, t.B[0][2], t.B[1][0], t.B[2][1]);
+	const double cD0 = sel(k, t.D[0][0], t.D[1][1], t.D[2][2]);
+	const double cD1 = sel(k, t.D[0][1], t.D[1][2], t.D[2][0]);
+	const double cD2 = sel(k, t.D[0][2], t.D[1][0], t.D[2][1]);
+	const double wk = sel(k, t.w[0], t.w[1], t.w[2]);
 	const double k0 = prm.kExpr.n ? eval_expr(prm.kExpr, 0.0, 0.0, 0.0, 0.0, 0.0) : prm.kConst;
 	const double massc = prm.coef * prm.rho * prm.cp;
 	const int64_t warpId = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const int64_t step = (((int64_t)gridDim.x * blockDim.x) >> 5) * EPW;
-	// the rows and operand values of this lane's x-line (nodes (i, p, r)) of element ee
-	auto load = [&](int64_t ee, int32_t (&rw)[3], double (&uv)[3]) {
+	// the rows and operand values of this lane's plane (nodes (i, j, k), index i + 3 j) of element ee
+	auto load = [&](int64_t ee, int32_t (&rw)[9], double (&uv)[9]) {
+		const bool ok = act && ee < prm.nelem;
 #pragma unroll
-		for (int i = 0; i < 3; ++i) rw[i] = (act && ee < prm.nelem) ? prm.erow[ee * NPE + i + 3 * p + 9 * r] : -1;
+		for (int a = 0; a < 9; ++a) rw[a] = ok ? prm.erow[ee * NPE + 9 * k + a] : -1;
 #pragma unroll
-		for (int i = 0; i < 3; ++i) uv[i] = (rw[i] >= 0 && prm.V) ? prm.V[rw[i]] : 0.0;
+		for (int a = 0; a < 9; ++a) uv[a] = (rw[a] >= 0 && prm.V) ? prm.V[rw[a]] : 0.0;
 	};
-	int32_t rowN[3];
-	double uN[3];
-	load(warpId * EPW + slot, rowN, uN);
-	for (int64_t eb = warpId * EPW; eb < prm.nelem; eb += step) {
-		const int64_t e = eb + slot;
+	int32_t rowN[9];
+	double uN[9];
+	load(warpId * EPW + grp, rowN, uN);
+	for (int64_t eb = warpId * EPW; eb < prm.nelem; eb += step) {   // warp-uniform trip count
+		const int64_t e = eb + grp;
 		const bool in = act && e < prm.nelem;
-		int32_t row[3];
-		double u[3];
+		int32_t row[9];
+		double u[9];
 #pragma unroll
-		for (int i = 0; i < 3; ++i) { row[i] = rowN[i]; u[i] = uN[i]; }
-		load(e + step, rowN, uN);   // the next element's line, in flight during this one
+		for (int a = 0; a < 9; ++a) { row[a] = rowN[a]; u[a] = uN[a]; }
+		load(e + step, rowN, uN);   // the next element's plane, in flight during this one
 		double c[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, detJ = 0.0, ke = 1.0;
 		if (in) {
 			const double2* gp2 = reinterpret_cast<const double2*>(prm.geo + e * 8);
@@ -1016,99 +1020,62 @@ __global__ void __launch_bounds__(256) k_apply_hex27_lines(const AsmParams prm, 
 			c[0] = g0.x; c[1] = g0.y; c[2] = g1.x; c[3] = g1.y; c[4] = g2.x; c[5] = g2.y; detJ = g3.x;
 			if (prm.kElem) ke = prm.kElem[e];
 		}
-		// x: lane (p, r) = line (y, z); B and D of u along x
-		{
-			double xb[3], xd[3];
+		const double sK = ke * k0 * detJ * wk, sM = massc * detJ * wk;
+		// x: xb[q][j] = sum_i B[q][i] u(i, j), xd with D
+		double xb[3][3], xd[3][3];
 #pragma unroll
-			for (int q = 0; q < 3; ++q) {
-				xb[q] = t.B[q][0] * u[0] + t.B[q][1] * u[1] + t.B[q][2] * u[2];
-				xd[q] = t.D[q][0] * u[0] + t.D[q][1] * u[1] + t.D[q][2] * u[2];
+		for (int q = 0; q < 3; ++q)
+#pragma unroll
+			for (int j = 0; j < 3; ++j) {
+				xb[q][j] = t.B[q][0] * u[3 * j] + t.B[q][1] * u[3 * j + 1] + t.B[q][2] * u[3 * j + 2];
+				xd[q][j] = t.D[q][0] * u[3 * j] + t.D[q][1] * u[3 * j + 1] + t.D[q][2] * u[3 * j + 2];
 			}
-			__syncwarp();
+		double F[9];
 #pragma unroll
-			for (int q = 0; q < 3; ++q) if (act) { at(0, q, p, r) = xb[q]; at(1, q, p, r) = xd[q]; }
-			__syncwarp();
-		}
-		// y: lane (p, r) = line (x, z)
-		{
-			double vb[3], vd[3];
+		for (int a = 0; a < 9; ++a) F[a] = 0.0;
 #pragma unroll
-			for (int j = 0; j < 3; ++j) { vb[j] = at(0, p, j, r); vd[j] = at(1, p, j, r); }
-			double bb[3], db[3], bd[3];
-#pragma unroll
-			for (int q = 0; q < 3; ++q) {
-				bb[q] = t.B[q][0] * vb[0] + t.B[q][1] * vb[1] + t.B[q][2] * vb[2];
-				db[q] = t.D[q][0] * vb[0] + t.D[q][1] * vb[1] + t.D[q][2] * vb[2];
-				bd[q] = t.B[q][0] * vd[0] + t.B[q][1] * vd[1] + t.B[q][2] * vd[2];
-			}
-			__syncwarp();
-#pragma unroll
-			for (int q = 0; q < 3; ++q) if (act) { at(0, p, q, r) = bb[q]; at(1, p, q, r) = db[q]; at(2, p, q, r) = bd[q]; }
-			__syncwarp();
-		}
-		// z: lane (p, r) = line (x, y); values and reference gradients at the points (p, r, q), the
-		// flux and mass term there, and back along z
-		{
-			double vbb[3], vdb[3], vbd[3];
-#pragma unroll
-			for (int j = 0; j < 3; ++j) { vbb[j] = at(0, p, r, j); vdb[j] = at(1, p, r, j); vbd[j] = at(2, p, r, j); }
-			double fx[3], fy[3], fz[3], m[3];
-			const double s0 = ke * k0 * detJ * t.w[p] * t.w[r];
-			const double m0 = massc * detJ * t.w[p] * t.w[r];
-#pragma unroll
-			for (int q = 0; q < 3; ++q) {
-				const double val = t.B[q][0] * vbb[0] + t.B[q][1] * vbb[1] + t.B[q][2] * vbb[2];
-				const double gz = t.D[q][0] * vbb[0] + t.D[q][1] * vbb[1] + t.D[q][2] * vbb[2];
-				const double gy = t.B[q][0] * vdb[0] + t.B[q][1] * vdb[1] + t.B[q][2] * vdb[2];
-				const double gx = t.B[q][0] * vbd[0] + t.B[q][1] * vbd[1] + t.B[q][2] * vbd[2];
-				const double s = s0 * t.w[q];
-				fx[q] = s * (c[0] * gx + c[3] * gy + c[4] * gz);
-				fy[q] = s * (c[3] * gx + c[1] * gy + c[5] * gz);
-				fz[q] = s * (c[4] * gx + c[5] * gy + c[2] * gz);
-				m[q] = m0 * t.w[q] * val;
-			}
+		for (int q1 = 0; q1 < 3; ++q1) {
 			double A1[3], A2[3], A3[3];
 #pragma unroll
-			for (int k = 0; k < 3; ++k) {
-				A1[k] = t.B[0][k] * fx[0] + t.B[1][k] * fx[1] + t.B[2][k] * fx[2];
-				A2[k] = t.B[0][k] * fy[0] + t.B[1][k] * fy[1] + t.B[2][k] * fy[2];
-				A3[k] = t.D[0][k] * fz[0] + t.D[1][k] * fz[1] + t.D[2][k] * fz[2]
-				      + t.B[0][k] * m[0] + t.B[1][k] * m[1] + t.B[2][k] * m[2];
+			for (int q2 = 0; q2 < 3; ++q2) {
+				// y: this plane's node values contracted to the point (q1, q2)
+				const double bb = t.B[q2][0] * xb[q1][0] + t.B[q2][1] * xb[q1][1] + t.B[q2][2] * xb[q1][2];
+				const double db = t.D[q2][0] * xb[q1][0] + t.D[q2][1] * xb[q1][1] + t.D[q2][2] * xb[q1][2];
+				const double bd = t.B[q2][0] * xd[q1][0] + t.B[q2][1] * xd[q1][1] + t.B[q2][2] * xd[q1][2];
+				// z: the other planes' sums, then value and reference gradient at the point (q1, q2, k)
+				const double bb1 = __shfl_sync(0xffffffffu, bb, src1), bb2 = __shfl_sync(0xffffffffu, bb, src2);
+				const double db1 = __shfl_sync(0xffffffffu, db, src1), db2 = __shfl_sync(0xffffffffu, db, src2);
+				const double bd1 = __shfl_sync(0xffffffffu, bd, src1), bd2 = __shfl_sync(0xffffffffu, bd, src2);
+				const double val = cB0 * bb + cB1 * bb1 + cB2 * bb2;
+				const double gz = cD0 * bb + cD1 * bb1 + cD2 * bb2;
+				const double gy = cB0 * db + cB1 * db1 + cB2 * db2;
+				const double gx = cB0 * bd + cB1 * bd1 + cB2 * bd2;
+				// the point's flux and mass term (c: C00, C11, C22, C01, C02, C12)
+				const double s = sK * t.w[q1] * t.w[q2];
+				const double fx = s * (c[0] * gx + c[3] * gy + c[4] * gz);
+				const double fy = s * (c[3] * gx + c[1] * gy + c[5] * gz);
+				const double fz = s * (c[4] * gx + c[5] * gy + c[2] * gz);
+				const double m = sM * t.w[q1] * t.w[q2] * val;
+				// back along z: this point's share of its own plane's nodes plus the shares the points
+				// of planes k+2 and k+1 computed for this plane (their "+1" and "+2" targets)
+				const double o3a = cD1 * fz + cB1 * m, o3b = cD2 * fz + cB2 * m;
+				A1[q2] = cB0 * fx + __shfl_sync(0xffffffffu, cB1 * fx, src2) + __shfl_sync(0xffffffffu, cB2 * fx, src1);
+				A2[q2] = cB0 * fy + __shfl_sync(0xffffffffu, cB1 * fy, src2) + __shfl_sync(0xffffffffu, cB2 * fy, src1);
+				A3[q2] = cD0 * fz + cB0 * m + __shfl_sync(0xffffffffu, o3a, src2) + __shfl_sync(0xffffffffu, o3b, src1);
 			}
-			__syncwarp();
+			// back along y to the nodes j of this x-point, then along x into the node sums
 #pragma unroll
-			for (int k = 0; k < 3; ++k) if (act) { at(0, p, r, k) = A1[k]; at(1, p, r, k) = A2[k]; at(2, p, r, k) = A3[k]; }
-			__syncwarp();
-		}
-		// y back: lane (p, r) = line (x, z)
-		{
-			double v1[3], v2[3], v3[3];
+			for (int j = 0; j < 3; ++j) {
+				const double C1 = t.B[0][j] * A1[0] + t.B[1][j] * A1[1] + t.B[2][j] * A1[2];
+				const double C2 = t.D[0][j] * A2[0] + t.D[1][j] * A2[1] + t.D[2][j] * A2[2]
+				                + t.B[0][j] * A3[0] + t.B[1][j] * A3[1] + t.B[2][j] * A3[2];
 #pragma unroll
-			for (int q = 0; q < 3; ++q) { v1[q] = at(0, p, q, r); v2[q] = at(1, p, q, r); v3[q] = at(2, p, q, r); }
-			double C1[3], C2[3];
-#pragma unroll
-			for (int k = 0; k < 3; ++k) {
-				C1[k] = t.B[0][k] * v1[0] + t.B[1][k] * v1[1] + t.B[2][k] * v1[2];
-				C2[k] = t.D[0][k] * v2[0] + t.D[1][k] * v2[1] + t.D[2][k] * v2[2]
-				      + t.B[0][k] * v3[0] + t.B[1][k] * v3[1] + t.B[2][k] * v3[2];
-			}
-			__syncwarp();
-#pragma unroll
-			for (int k = 0; k < 3; ++k) if (act) { at(0, p, k, r) = C1[k]; at(1, p, k, r) = C2[k]; }
-			__syncwarp();
-		}
-		// x back: lane (p, r) = line (y, z), the nodes of its x-line
-		{
-			double v1[3], v2[3];
-#pragma unroll
-			for (int q = 0; q < 3; ++q) { v1[q] = at(0, q, p, r); v2[q] = at(1, q, p, r); }
-#pragma unroll
-			for (int k = 0; k < 3; ++k) {
-				const double F = t.D[0][k] * v1[0] + t.D[1][k] * v1[1] + t.D[2][k] * v1[2]
-				               + t.B[0][k] * v2[0] + t.B[1][k] * v2[1] + t.B[2][k] * v2[2];
-				if (row[k] >= 0) atomicAdd(prm.out + row[k], prm.outScale * F);
+				for (int i = 0; i < 3; ++i) F[3 * j + i] += t.D[q1][i] * C1 + t.B[q1][i] * C2;
 			}
 		}
+#pragma unroll
+		for (int a = 0; a < 9; ++a)
+			if (row[a] >= 0) atomicAdd(prm.out + row[a], prm.outScale * F[a]);
 	}
 }
 
@@ -2065,14 +2032,14 @@ int apply_operator(rsd_ctx* ctx, rsd_heat* h, double coef, const double* U, cons
 			RSD_CUDA(cudaGetLastError());
 			return RSD_OK;
 		};
-		const char* lines = getenv("RSD_SUMFAC_LINES");
+		const char* planes = getenv("RSD_SUMFAC_PLANES");
 		if (nsd == 2 && ord == 2) rc = go(k_apply_sumfac<2, 2>);
 		else if (nsd == 2 && ord == 3) rc = go(k_apply_sumfac<2, 3>);
-		else if (lines && lines[0] == '0') rc = go(k_apply_sumfac<3, 2>);
+		else if (planes && planes[0] == '0') rc = go(k_apply_sumfac<3, 2>);
 		else {
-			const int64_t wn = (p.nelem + 2) / 3;
-			const int b = (int)std::max<int64_t>(1, std::min<int64_t>((wn + 7) / 8, (int64_t)ctx->num_sms * 8));
-			k_apply_hex27_lines<<<b, 256, 0, ctx->stream>>>(p, t);
+			const int64_t wn = (p.nelem + 9) / 10;
+			const int b = (int)std::max<int64_t>(1, std::min<int64_t>((wn + 3) / 4, (int64_t)ctx->num_sms * 3));   // resident: 3 per SM
+			k_apply_hex27_planes<<<b, 128, 0, ctx->stream>>>(p, t);
 			RSD_CUDA(cudaGetLastError());
 			rc = RSD_OK;
 		}

@@ -367,32 +367,61 @@ __host__ __device__ __forceinline__ double next_delta(double delta, double recur
 	return fmin(0.1, fmax(lo, 100.0 * d * delta));
 }
 
-// expression stack machine (bytecode from compile_expr, which rejects programs deeper than kExprStack)
-__device__ __forceinline__ double eval_expr(const DevExpr& e, double t, double x, double y, double z, double T) {
-	double st[kExprStack];
-	int sp = 0;
+// expression stack machine (bytecode from compile_expr, which rejects programs deeper than kExprStack
+// and records each program's depth).  The stack lives in registers: D slots indexed only by
+// compile-time constants (s[0] the top), a push shifting the slots up and a binary operator folding
+// the top two and shifting down.  A stack array indexed by a running stack pointer lives in local
+// memory instead, and inlined into the boundary-reaction monitor kernel (an element loop that keeps
+// per-node local arrays live across its quadrature points) it was given the storage of the element's
+// rate array (nvcc 12.9, sm_100a): the source value overwrote a nodal rate from the second point on
+// (test_heat_flux_monitors pins the monitor against the reference).
+template <int D>
+__device__ __forceinline__ double eval_expr_d(const DevExpr& e, double t, double x, double y, double z, double T) {
+	double s[D];
+#pragma unroll
+	for (int k = 0; k < D; ++k) s[k] = 0.0;
 	for (int i = 0; i < e.n; ++i) {
 		const int op = e.op[i];
 		const int a = e.arg[i];
-		switch (op) {
-			case E_CONST: st[sp++] = e.c[a]; break;
-			case E_VAR: st[sp++] = a == 0 ? t : a == 1 ? x : a == 2 ? y : a == 3 ? z : T; break;
-			case E_ADD: --sp; st[sp - 1] = st[sp - 1] + st[sp]; break;
-			case E_SUB: --sp; st[sp - 1] = st[sp - 1] - st[sp]; break;
-			case E_MUL: --sp; st[sp - 1] = st[sp - 1] * st[sp]; break;
-			case E_DIV: --sp; st[sp - 1] = st[sp - 1] / st[sp]; break;
-			case E_POW: --sp; st[sp - 1] = pow(st[sp - 1], st[sp]); break;
-			case E_NEG: st[sp - 1] = -st[sp - 1]; break;
-			case E_SIN: st[sp - 1] = sin(st[sp - 1]); break;
-			case E_COS: st[sp - 1] = cos(st[sp - 1]); break;
-			case E_TAN: st[sp - 1] = tan(st[sp - 1]); break;
-			case E_EXP: st[sp - 1] = exp(st[sp - 1]); break;
-			case E_LOG: st[sp - 1] = log(st[sp - 1]); break;
-			case E_SQRT: st[sp - 1] = sqrt(st[sp - 1]); break;
-			default: st[sp - 1] = fabs(st[sp - 1]); break;
+		if (op == E_CONST || op == E_VAR) {
+			const double v = op == E_CONST ? e.c[a] : (a == 0 ? t : a == 1 ? x : a == 2 ? y : a == 3 ? z : T);
+#pragma unroll
+			for (int k = D - 1; k > 0; --k) s[k] = s[k - 1];
+			s[0] = v;
+		} else if (op <= E_POW) {
+			const double l = s[1], r = s[0];
+			double v;
+			switch (op) {
+				case E_ADD: v = l + r; break;
+				case E_SUB: v = l - r; break;
+				case E_MUL: v = l * r; break;
+				case E_DIV: v = l / r; break;
+				default: v = pow(l, r); break;
+			}
+			s[0] = v;
+#pragma unroll
+			for (int k = 1; k < D - 1; ++k) s[k] = s[k + 1];
+		} else {
+			double v = s[0];
+			switch (op) {
+				case E_NEG: v = -v; break;
+				case E_SIN: v = sin(v); break;
+				case E_COS: v = cos(v); break;
+				case E_TAN: v = tan(v); break;
+				case E_EXP: v = exp(v); break;
+				case E_LOG: v = log(v); break;
+				case E_SQRT: v = sqrt(v); break;
+				default: v = fabs(v); break;
+			}
+			s[0] = v;
 		}
 	}
-	return e.n ? st[0] : 0.0;
+	return e.n ? s[0] : 0.0;
+}
+__device__ __forceinline__ double eval_expr(const DevExpr& e, double t, double x, double y, double z, double T) {
+	if (e.depth <= 4) return eval_expr_d<4>(e, t, x, y, z, T);
+	if (e.depth <= 8) return eval_expr_d<8>(e, t, x, y, z, T);
+	return eval_expr_d<kExprStack>(e, t, x, y, z, T);
 }
 
 // lanes per row of the execution layout: -1 for SELL-32 with narrow columns, 0 for SELL-32, else

@@ -130,10 +130,10 @@ def test_sum_factorized_product_matches_tables_and_matrix(rsd, ctx, monkeypatch,
     if nsd == 3 and order == 2:
         # the 27-node kernel by lanes per node (shuffles) instead of lanes per grid line
         monkeypatch.setenv("RSD_SUMFAC", "1")
-        monkeypatch.setenv("RSD_SUMFAC_LINES", "0")
+        monkeypatch.setenv("RSD_SUMFAC_PLANES", "0")
         h.assemble_vector(4, y3, coef=c, operand=v)
         assert relerr(y3.download(), y1.download()) <= REL
-        monkeypatch.delenv("RSD_SUMFAC_LINES")
+        monkeypatch.delenv("RSD_SUMFAC_PLANES")
     # the diffusion operator alone (coef 0)
     monkeypatch.delenv("RSD_SUMFAC")
     h.assemble_matrix(1.0, 0.0)

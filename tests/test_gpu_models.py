@@ -136,7 +136,8 @@ def test_pmsh_mesh_solves_like_the_block_mesh(rsd, ctx):
     Up, Ub = ctx.array(hp.n).zero(), ctx.array(hb.n).zero()
     hp.steady(Up, tol=1e-12)
     hb.steady(Ub, tol=1e-12)
-    assert np.array_equal(Up.download(), Ub.download())
+    # the element vectors sum by atomics, so the two solves agree to rounding, not bit for bit
+    assert rel(Up.download(), Ub.download()) <= 1e-10
 
 
 @pytest.mark.parametrize("nsd,order,nel,dirichlet,perm", [
@@ -147,7 +148,8 @@ def test_pmsh_mesh_solves_like_the_block_mesh(rsd, ctx):
 ])
 def test_device_setup_matches_host_setup(rsd, ctx, monkeypatch, nsd, order, nel, dirichlet, perm):
     """The DOF map and CSR pattern built on the device (the default) equal the host build
-    (RSD_HOST_SETUP=1) bit for bit, on block meshes and on block meshes with shuffled node numbers."""
+    (RSD_HOST_SETUP=1) bit for bit, on block meshes and on block meshes with shuffled node numbers; the
+    steady solutions on either agree to rounding (element vectors sum by atomics)."""
     from importlib import import_module
     bm = import_module("residuum_solver_b200.blockmesh")
     xyz, ien, rng = bm.block_mesh(nsd, nel, [0] * nsd, [1] * nsd, order)
@@ -167,7 +169,10 @@ def test_device_setup_matches_host_setup(rsd, ctx, monkeypatch, nsd, order, nel,
         t2a, a2t = h.dofmap()
         rp, col = h.K.pattern()
         U = ctx.array(h.n).zero()
-        h.steady(U, tol=1e-12, max_iters=5000)
+        if dirichlet:     # without an essential tag the steady problem is singular
+            h.steady(U, tol=1e-12, max_iters=5000)
         out.append((t2a, a2t, rp, col, U.download()))
-    for a, b in zip(out[0], out[1]):
+    for a, b in zip(out[0][:4], out[1][:4]):
         assert np.array_equal(a, b)
+    if dirichlet:
+        assert rel(out[0][4], out[1][4]) <= 1e-10
