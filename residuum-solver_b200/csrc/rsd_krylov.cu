@@ -980,6 +980,139 @@ __global__ void k_gm_mupdate(int64_t n, const T* __restrict__ Q, int64_t ldq, in
 	}
 }
 
+// The fused classical Gram-Schmidt passes for k <= KMAX basis vectors (k uniform over the launch):
+// each thread keeps k running sums over its elements, a block sums them in a fixed tree (warp
+// shuffles, then the warps in order), one partial per (sum, block), and the last block to arrive adds
+// each sum's partials in block order (a warp per sum: lanes over strided partials, then a shuffle
+// tree) into out[i].  Deterministic for a given grid.  256-thread blocks.
+constexpr int kGmFusedThreads = 256, kGmFusedMax = 32;
+template <int KMAX>
+__device__ __forceinline__ void gm_multi_sum(double (&acc)[KMAX], int k, double* partials, unsigned* ticket, double* out) {
+	__shared__ double sm[KMAX][kGmFusedThreads / 32];
+	__shared__ bool last;
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+	for (int i = 0; i < KMAX; ++i)
+		if (i < k) {
+			const double v = group_sum<32>(acc[i]);
+			if (lane == 0) sm[i][warp] = v;
+		}
+	__syncthreads();
+	if (threadIdx.x < k) {
+		double s = 0.0;
+		for (int wi = 0; wi < nw; ++wi) s += sm[threadIdx.x][wi];
+		partials[(size_t)threadIdx.x * kMaxPartials + blockIdx.x] = s;
+		__threadfence();
+	}
+	__syncthreads();
+	if (threadIdx.x == 0) last = atomicInc(ticket, gridDim.x - 1) == gridDim.x - 1;
+	__syncthreads();
+	if (!last) return;
+	__threadfence();
+	for (int i = warp; i < k; i += nw) {
+		double s = 0.0;
+		for (int b = lane; b < (int)gridDim.x; b += 32) s += __ldcg(&partials[(size_t)i * kMaxPartials + b]);
+		s = group_sum<32>(s);
+		if (lane == 0) out[i] = s;
+	}
+}
+
+// CGS pass 1: h[i] = Q_i . w for i < k, w read once per element
+template <typename T, int KMAX>
+__global__ void __launch_bounds__(kGmFusedThreads, 1) k_gm_mdot_k(int64_t n, const T* __restrict__ Q, int64_t ldq, int k,
+                                                             const T* __restrict__ w, double* partials, unsigned* ticket,
+                                                             double* h, const int32_t* stop) {
+	if (*(volatile const int32_t*)stop) return;
+	double acc[KMAX];
+#pragma unroll
+	for (int i = 0; i < KMAX; ++i) acc[i] = 0.0;
+	for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+		const double we = (double)w[e];
+		// every load unconditional (sums past k read vector k - 1 again and are never reduced), so the
+		// compiler issues them all before the first multiply-add
+#pragma unroll
+		for (int i = 0; i < KMAX; ++i) acc[i] += (double)__ldg(Q + (int64_t)min(i, k - 1) * ldq + e) * we;
+	}
+	gm_multi_sum<KMAX>(acc, k, partials, ticket, h);
+}
+
+// CGS pass 1's update fused with pass 2's dots: w -= sum_{i<k} h1[i] Q_i (basis order, FP64 per
+// element, stored in T, as k_gm_mupdate), then h2[i] = Q_i . w with the stored w
+template <typename T, int KMAX>
+__global__ void __launch_bounds__(kGmFusedThreads, 1) k_gm_update_mdot(int64_t n, const T* __restrict__ Q, int64_t ldq, int k,
+                                                                  const double* __restrict__ h1, T* __restrict__ w,
+                                                                  double* partials, unsigned* ticket, double* h2,
+                                                                  const int32_t* stop) {
+	if (*(volatile const int32_t*)stop) return;
+	__shared__ double hs[KMAX];
+	if (threadIdx.x < KMAX) hs[threadIdx.x] = threadIdx.x < k ? h1[threadIdx.x] : 0.0;
+	__syncthreads();
+	double acc[KMAX];
+#pragma unroll
+	for (int i = 0; i < KMAX; ++i) acc[i] = 0.0;
+	for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+		double s = (double)w[e];
+		// unconditional loads (past k: vector k - 1 again, times a zero coefficient, which leaves s
+		// unchanged), so that they all issue before the first multiply-add
+#pragma unroll
+		for (int i = 0; i < KMAX; ++i) s -= hs[i] * (double)__ldg(Q + (int64_t)min(i, k - 1) * ldq + e);
+		const T wn = (T)s;
+		w[e] = wn;
+		const double wd = (double)wn;
+#pragma unroll
+		for (int i = 0; i < KMAX; ++i) acc[i] += (double)__ldg(Q + (int64_t)min(i, k - 1) * ldq + e) * wd;
+	}
+	gm_multi_sum<KMAX>(acc, k, partials, ticket, h2);
+}
+
+// CGS pass 2's update fused with the norm: w -= sum_{i<k} h2[i] Q_i, then out = ||w|| of the stored w
+template <typename T, int KMAX>
+__global__ void __launch_bounds__(kGmFusedThreads, 1) k_gm_update_nrm(int64_t n, const T* __restrict__ Q, int64_t ldq, int k,
+                                                                 const double* __restrict__ h2, T* __restrict__ w,
+                                                                 double* partials, unsigned* ticket, double* out,
+                                                                 const int32_t* stop) {
+	if (*(volatile const int32_t*)stop) return;
+	__shared__ double hs[KMAX];
+	if (threadIdx.x < KMAX) hs[threadIdx.x] = threadIdx.x < k ? h2[threadIdx.x] : 0.0;
+	__syncthreads();
+	double v[1] = {0.0};
+	for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+		double s = (double)w[e];
+		// unconditional loads (past k: vector k - 1 again, times a zero coefficient, which leaves s
+		// unchanged), so that they all issue before the first multiply-add
+#pragma unroll
+		for (int i = 0; i < KMAX; ++i) s -= hs[i] * (double)__ldg(Q + (int64_t)min(i, k - 1) * ldq + e);
+		const T wn = (T)s;
+		w[e] = wn;
+		v[0] += (double)wn * (double)wn;
+	}
+	if (grid_sum<1>(v, partials, ticket)) *out = sqrt(v[0]);
+}
+
+template <typename T, int KMAX>
+static int gm_fused_k(rsd_ctx* ctx, int64_t n, const T* Q, int64_t ldq, int k, T* w, double* parts, unsigned* tk,
+                      unsigned* tn, double* h1, double* h2, double* nrm, const int32_t* stop) {
+	cudaStream_t st = ctx->stream;
+	const int g1 = wave_blocks(ctx, k_gm_mdot_k<T, KMAX>, kGmFusedThreads, n);
+	const int g2 = wave_blocks(ctx, k_gm_update_mdot<T, KMAX>, kGmFusedThreads, n);
+	const int g3 = wave_blocks(ctx, k_gm_update_nrm<T, KMAX>, kGmFusedThreads, n);
+	k_gm_mdot_k<T, KMAX><<<g1, kGmFusedThreads, 0, st>>>(n, Q, ldq, k, w, parts, tk, h1, stop);
+	k_gm_update_mdot<T, KMAX><<<g2, kGmFusedThreads, 0, st>>>(n, Q, ldq, k, h1, w, parts, tk, h2, stop);
+	k_gm_update_nrm<T, KMAX><<<g3, kGmFusedThreads, 0, st>>>(n, Q, ldq, k, h2, w, parts, tn, nrm, stop);
+	RSD_CUDA(cudaGetLastError());
+	return RSD_OK;
+}
+template <typename T>
+static int gm_fused(rsd_ctx* ctx, int64_t n, const T* Q, int64_t ldq, int k, T* w, double* parts, unsigned* tk,
+                    unsigned* tn, double* h1, double* h2, double* nrm, const int32_t* stop) {
+	if (k <= 4) return gm_fused_k<T, 4>(ctx, n, Q, ldq, k, w, parts, tk, tn, h1, h2, nrm, stop);
+	if (k <= 8) return gm_fused_k<T, 8>(ctx, n, Q, ldq, k, w, parts, tk, tn, h1, h2, nrm, stop);
+	if (k <= 12) return gm_fused_k<T, 12>(ctx, n, Q, ldq, k, w, parts, tk, tn, h1, h2, nrm, stop);
+	if (k <= 16) return gm_fused_k<T, 16>(ctx, n, Q, ldq, k, w, parts, tk, tn, h1, h2, nrm, stop);
+	if (k <= 24) return gm_fused_k<T, 24>(ctx, n, Q, ldq, k, w, parts, tk, tn, h1, h2, nrm, stop);
+	return gm_fused_k<T, kGmFusedMax>(ctx, n, Q, ldq, k, w, parts, tk, tn, h1, h2, nrm, stop);
+}
+
 // out = ||w||
 template <typename T>
 __global__ void k_gm_nrm2(int64_t n, const T* __restrict__ w, double* partials, unsigned* ticket, double* out,
@@ -1032,33 +1165,49 @@ struct GmState {
 
 // Arnoldi step j: the new column (the two CGS passes' coefficients, hNext), the previous rotations, the
 // next rotation, g; ends the cycle on convergence, breakdown (hNext <= 1e-14), the step budget or a
-// non-finite g (gmres/Solver.tpp:88-110).  One thread.
-__global__ void k_gm_givens(GmState* S, int j, int m, const double* __restrict__ h1, const double* __restrict__ h2,
-                            const double* __restrict__ hNextp, double* __restrict__ H, double* __restrict__ cs,
-                            double* __restrict__ sn, double* __restrict__ g) {
-	if (S->stop) return;
+// non-finite g (gmres/Solver.tpp:88-110).  One warp: the lanes stage the column and the rotations in
+// shared memory, lane 0 runs the rotations in order (the column entry it carries in a register), the
+// lanes write the column back.
+constexpr int kGmMaxDim = 256;
+__global__ void __launch_bounds__(32) k_gm_givens(GmState* S, int j, int m, const double* __restrict__ h1,
+                                                  const double* __restrict__ h2, const double* __restrict__ hNextp,
+                                                  double* __restrict__ H, double* __restrict__ cs, double* __restrict__ sn,
+                                                  double* __restrict__ g) {
+	if (*(volatile const int32_t*)&S->stop) return;   // uniform over the warp
+	__shared__ double hj[kGmMaxDim], c[kGmMaxDim], sv[kGmMaxDim];
+	const int lane = threadIdx.x;
 	const int ld = m + 1;   // H column-major: H(i, j) at j * (m + 1) + i
 	double* Hj = H + (int64_t)j * ld;
-	for (int i = 0; i <= j; ++i) Hj[i] = __dadd_rn(h1[i], h2[i]);
-	const double hNext = *hNextp;
-	for (int i = 0; i < j; ++i) {
-		const double a = Hj[i], b = Hj[i + 1];
-		Hj[i] = __dadd_rn(__dmul_rn(cs[i], a), __dmul_rn(sn[i], b));
-		Hj[i + 1] = __dadd_rn(__dmul_rn(-sn[i], a), __dmul_rn(cs[i], b));
+	for (int i = lane; i <= j; i += 32) hj[i] = __dadd_rn(h1[i], h2[i]);
+	for (int i = lane; i < j; i += 32) { c[i] = cs[i]; sv[i] = sn[i]; }
+	__syncwarp();
+	if (lane == 0) {
+		const double hNext = *hNextp;
+		double a = hj[0];
+		for (int i = 0; i < j; ++i) {
+			const double b = hj[i + 1];
+			hj[i] = __dadd_rn(__dmul_rn(c[i], a), __dmul_rn(sv[i], b));
+			a = __dadd_rn(__dmul_rn(-sv[i], a), __dmul_rn(c[i], b));
+		}
+		const double hjj = a;
+		const double denom = sqrt(__dadd_rn(__dmul_rn(hjj, hjj), __dmul_rn(hNext, hNext)));
+		double cj, sj;
+		if (denom <= 1e-14) { cj = 1.0; sj = 0.0; }
+		else { cj = hjj / denom; sj = hNext / denom; }
+		cs[j] = cj; sn[j] = sj;
+		hj[j] = __dadd_rn(__dmul_rn(cj, hjj), __dmul_rn(sj, hNext));
+		const double gj = g[j];
+		g[j] = __dmul_rn(cj, gj);
+		const double gn = __dmul_rn(-sj, gj);
+		g[j + 1] = gn;
+		S->mLocal = j + 1;
+		const bool brk = hNext <= 1e-14;
+		S->breakdown = brk;
+		if (!isfinite(gn)) { S->status = RSD_EBREAKDOWN; S->stop = 1; }
+		else if (fabs(gn) / S->denom < S->tol || brk || j + 1 >= S->budget || j + 1 >= m) S->stop = 1;
 	}
-	const double hjj = Hj[j];
-	const double denom = sqrt(__dadd_rn(__dmul_rn(hjj, hjj), __dmul_rn(hNext, hNext)));
-	if (denom <= 1e-14) { cs[j] = 1.0; sn[j] = 0.0; }
-	else { cs[j] = hjj / denom; sn[j] = hNext / denom; }
-	Hj[j] = __dadd_rn(__dmul_rn(cs[j], hjj), __dmul_rn(sn[j], hNext));
-	const double gj = g[j];
-	g[j] = __dmul_rn(cs[j], gj);
-	g[j + 1] = __dmul_rn(-sn[j], gj);
-	S->mLocal = j + 1;
-	const bool brk = hNext <= 1e-14;
-	S->breakdown = brk;
-	if (!isfinite(g[j + 1])) { S->status = RSD_EBREAKDOWN; S->stop = 1; return; }
-	if (fabs(g[j + 1]) / S->denom < S->tol || brk || j + 1 >= S->budget || j + 1 >= m) S->stop = 1;
+	__syncwarp();
+	for (int i = lane; i <= j; i += 32) Hj[i] = hj[i];
 }
 
 // back substitution H(0:m, 0:m) y = g(0:m) for the cycle's m = mLocal steps (one thread)
@@ -1153,7 +1302,7 @@ static int gmres_core(rsd_ctx* ctx, Op& op, const rsd_solver_cfg* cfg, const dou
 	constexpr bool kMixed = sizeof(T) == 4;
 	const int64_t n = op.n;
 	const int64_t m = std::max<int64_t>(1, cfg->krylov_dim);
-	if (m + 1 > 255) return set_error(RSD_EINVAL, "GMRES krylov_dim above 254");
+	if (m + 1 > kGmMaxDim - 1) return set_error(RSD_EINVAL, "GMRES krylov_dim above 254");
 	RSD_CHECK(op.prepare());
 	const int64_t ns = pad_len(n);
 	// workspace: Q (m+1 vectors), w, invD and a scratch vector in T; Ax in FP64; partials for m+1
@@ -1230,13 +1379,18 @@ static int gmres_core(rsd_ctx* ctx, Op& op, const rsd_solver_cfg* cfg, const dou
 			const T* qj = Q + j * ns;
 			RSD_CHECK(op.prec_apply(qj, invD, w, tmp, x, stop));
 			const int k = (int)(j + 1);
-			for (double* dh : {dH1, dH2}) {
-				k_gm_mdot<T><<<dim3(grd, k), kReduceThreads, 0, st>>>(n, Q, ns, w, parts, tickets, dh, stop);
-				k_gm_mupdate<T><<<gv, 256, 0, st>>>(n, Q, ns, k, dh, w, stop);
+			if (k <= kGmFusedMax) {
+				// the two CGS passes in three streaming kernels: dots; update + dots; update + norm
+				RSD_CHECK(gm_fused(ctx, n, Q, ns, k, w, parts, tickets + m, tickets + m + 1, dH1, dH2, dNorm, stop));
+			} else {
+				for (double* dh : {dH1, dH2}) {
+					k_gm_mdot<T><<<dim3(grd, k), kReduceThreads, 0, st>>>(n, Q, ns, w, parts, tickets, dh, stop);
+					k_gm_mupdate<T><<<gv, 256, 0, st>>>(n, Q, ns, k, dh, w, stop);
+				}
+				k_gm_nrm2<T><<<grd, kReduceThreads, 0, st>>>(n, w, parts, tickets + m + 1, dNorm, stop);
 			}
-			k_gm_nrm2<T><<<grd, kReduceThreads, 0, st>>>(n, w, parts, tickets + m + 1, dNorm, stop);
 			k_gm_scale<T><<<gv, 256, 0, st>>>(n, w, dNorm, Q + (j + 1) * ns, stop);
-			k_gm_givens<<<1, 1, 0, st>>>(dS, (int)j, (int)m, dH1, dH2, dNorm, dH, dCs, dSn, dG);
+			k_gm_givens<<<1, 32, 0, st>>>(dS, (int)j, (int)m, dH1, dH2, dNorm, dH, dCs, dSn, dG);
 			RSD_CUDA(cudaGetLastError());
 		}
 		k_gm_backsub<<<1, 1, 0, st>>>(dS, (int)m, dH, dG, dY);
