@@ -361,6 +361,204 @@ __global__ void __launch_bounds__(kST, kRowBlocks) k_mx_reliable(int64_t n, MatV
 	}
 }
 
+// ---- the mixed solve as one persistent cooperative kernel ---------------------------------------
+// The iteration of the kernels above (k_mx_spmv_dot, k_mx_step, and the replacement k_mx_fold +
+// k_mx_reliable when due) run by one cooperative launch whose blocks stay resident for the whole
+// solve: a grid barrier separates the phases, and every block sums the phase's per-block partials
+// itself (the same partials in the same order, so every block holds the same scalars and takes the
+// same decisions).  What it saves over one launch per phase is each kernel's ramp, its dependent
+// scalar loads at the start and its last-block reduction tail.  Each barrier waits a bounded time;
+// a barrier that gives up ends the solve with RSD_ETIMEOUT.
+constexpr int kPersistSlots = 5;                        // partial slots: SpMV 0; step 1, 2; replacement 3, 4
+constexpr unsigned long long kBarrierPolls = 1ull << 22;  // 256 ns apart: about a second
+
+__device__ __forceinline__ bool grid_barrier(unsigned long long* count, unsigned long long target) {
+	__shared__ int ok;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		__threadfence();
+		atomicAdd(count, 1ull);
+		unsigned long long polls = 0;
+		int good = 1;
+		while (*(volatile unsigned long long*)count < target) {
+			if (++polls > kBarrierPolls) { good = 0; break; }
+			__nanosleep(256);
+		}
+		__threadfence();
+		ok = good;
+	}
+	__syncthreads();
+	return ok != 0;
+}
+
+// every block's NCH sums, then (after the barrier) their totals in every block: the partials of
+// slot c + blockIdx.x, summed strided and by block_sum as grid_sum's last block does
+template <int NCH>
+__device__ __forceinline__ bool grid_allreduce(double (&v)[NCH], double* partials, int slot0, unsigned long long* count,
+                                               unsigned long long& gen) {
+	__shared__ double tot[NCH];
+	block_sum<NCH>(v);
+	if (threadIdx.x == 0)
+#pragma unroll
+		for (int c = 0; c < NCH; ++c) partials[(size_t)(slot0 + c) * kMaxPartials + blockIdx.x] = v[c];
+	gen += gridDim.x;
+	if (!grid_barrier(count, gen)) return false;
+	double acc[NCH];
+#pragma unroll
+	for (int c = 0; c < NCH; ++c) {
+		acc[c] = 0.0;
+		for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) acc[c] += __ldcg(&partials[(size_t)(slot0 + c) * kMaxPartials + b]);
+	}
+	block_sum<NCH>(acc);
+	if (threadIdx.x == 0)
+#pragma unroll
+		for (int c = 0; c < NCH; ++c) tot[c] = acc[c];
+	__syncthreads();
+#pragma unroll
+	for (int c = 0; c < NCH; ++c) v[c] = tot[c];
+	return true;
+}
+
+struct MxPersistArgs {
+	int64_t n;
+	MatView<float> A32;
+	MatView<double> A64;
+	const double* b;
+	double* x;
+	float *z, *p, *s, *w, *y;
+	const float* invD;
+	CgScal* S;
+	double* partials;            // kPersistSlots slots of kMaxPartials
+	unsigned long long* count;   // barrier arrivals (zeroed before the launch)
+	double tol;
+	int relMode, adaptive;
+	int64_t maxIters;
+};
+
+template <int L>
+__global__ void __launch_bounds__(kST, kRowBlocks) k_mx_persist(const MxPersistArgs a) {
+	const L2Pol pol = make_l2pol();
+	const int64_t n = a.n;
+	CgScal* S = a.S;
+	// the state k_mx_init left, read once; from here on every block carries the same copy
+	double rho = S->rz, rhoPrev = S->rhoPrev, alphaPrev = S->alpha, betaPrev = S->beta;
+	const double res0 = S->res0;
+	double res = S->res, rmax = S->rmax, dcur = S->dcur, res64 = S->res64, trueRel = S->trueRel;
+	int64_t iter = S->iter;
+	int refinements = S->refinements, done = S->done, converged = S->converged, status = S->status;
+	unsigned long long gen = 0;
+	const uint64_t h = pol.last;
+	for (int64_t guard = 0; !done && guard <= a.maxIters + 2; ++guard) {
+		// w = A32 z, mu = z.w
+		double vA[1] = {0.0};
+		{
+			const RowLoop<L> rl;
+			for (int64_t base = rl.base; base < n; base += rl.step) {
+				const int64_t row = base + rl.sub;
+				// z was written by this launch: coherent loads (the .nc path holds no such guarantee)
+				const float sr = row_sum<L, float, float>(a.A32, row, n, rl.lane, pol, [&](int c) { return ldh_rw(a.z + c, pol.last); });
+				if (rl.lane == 0 && row < n) { sth(a.w + row, sr, pol.last); vA[0] += (double)ldh_rw(a.z + row, pol.last) * (double)sr; }
+			}
+		}
+		if (!grid_allreduce<1>(vA, a.partials, 0, a.count, gen)) { status = RSD_ETIMEOUT; done = 1; break; }
+		const double mu = vA[0];
+		// the single-reduction vector pass (k_mx_step)
+		const bool first = !(rhoPrev != 0.0);
+		const double beta = first ? 0.0 : rho / rhoPrev;
+		const double alpha = first ? rho / mu : rho / (mu - beta * rho / alphaPrev);
+		const float fa = (float)alpha, fb = (float)beta;
+		double vB[2] = {0.0, 0.0};
+		packet_loop<float>(n, true, [&](int64_t i, int wd) {
+			if (wd > 1) {
+				Pk<float> Z = ldp_rw(a.z + i, h), W = ldp_rw(a.w + i, h), Y = ldp_rw(a.y + i, h), P, Q, D;
+				if (first) { P = Z; Q = W; }
+				else {
+					P = ldp_rw(a.p + i, h); Q = ldp_rw(a.s + i, h);
+#pragma unroll
+					for (int k = 0; k < Pk<float>::W; ++k) { P.v[k] = Z.v[k] + fb * P.v[k]; Q.v[k] = W.v[k] + fb * Q.v[k]; }
+				}
+				if (a.invD) D = ldp(a.invD + i, h);
+#pragma unroll
+				for (int k = 0; k < Pk<float>::W; ++k) {
+					Y.v[k] = Y.v[k] + fa * P.v[k];
+					const float zi = a.invD ? Z.v[k] - fa * (Q.v[k] * D.v[k]) : Z.v[k] - fa * Q.v[k];
+					const float ri = a.invD ? zi / D.v[k] : zi;
+					Z.v[k] = zi;
+					vB[0] += (double)ri * (double)ri;
+					vB[1] += (double)ri * (double)zi;
+				}
+				stp(a.p + i, P, h); stp(a.s + i, Q, h); stp(a.y + i, Y, h); stp(a.z + i, Z, h);
+			} else {
+				const float zo = ldh_rw(a.z + i, h), wo = ldh_rw(a.w + i, h);
+				const float pi = first ? zo : zo + fb * ldh_rw(a.p + i, h);
+				const float si = first ? wo : wo + fb * ldh_rw(a.s + i, h);
+				sth(a.p + i, pi, h); sth(a.s + i, si, h);
+				sth(a.y + i, ldh_rw(a.y + i, h) + fa * pi, h);
+				const float di = a.invD ? ldh(a.invD + i, h) : 1.0f;
+				const float zi = a.invD ? zo - fa * (si * di) : zo - fa * si;
+				const float ri = a.invD ? zi / di : zi;
+				sth(a.z + i, zi, h);
+				vB[0] += (double)ri * (double)ri;
+				vB[1] += (double)ri * (double)zi;
+			}
+		});
+		if (!grid_allreduce<2>(vB, a.partials, 1, a.count, gen)) { status = RSD_ETIMEOUT; done = 1; break; }
+		const int64_t k = iter + 1;
+		res = sqrt(vB[0]);
+		iter = k;
+		bool reliable = false;
+		if (!isfinite(alpha)) { done = 1; converged = 0; status = RSD_EBREAKDOWN; }
+		else if (!isfinite(res)) { done = 1; converged = 0; status = RSD_ENAN; }
+		else {
+			alphaPrev = alpha; betaPrev = beta; rhoPrev = rho; rho = vB[1];
+			const double crit = a.relMode ? res / (res0 + 1e-50) : res;
+			reliable = crit < a.tol || res < dcur * rmax || k + 1 >= a.maxIters;
+		}
+		if (done || !reliable) continue;
+		// replacement: x += y, y = 0; then r64 = b - A64 x, z = M r (k_mx_fold, k_mx_reliable)
+		for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+			sth(a.x + i, ldh_rw(a.x + i, h) + (double)ldh_rw(a.y + i, h), h);
+			sth(a.y + i, 0.0f, h);
+		}
+		gen += gridDim.x;
+		if (!grid_barrier(a.count, gen)) { status = RSD_ETIMEOUT; done = 1; break; }
+		double vR[2] = {0.0, 0.0};
+		{
+			const RowLoop<L> rl;
+			for (int64_t base = rl.base; base < n; base += rl.step) {
+				const int64_t row = base + rl.sub;
+				const double ax = row_sum<L, double, double>(a.A64, row, n, rl.lane, pol, [&](int c) { return ldh_rw(a.x + c, pol.last); });
+				if (rl.lane == 0 && row < n) {
+					const double r64 = ldh(a.b + row, pol.first) - ax;
+					const float ri = (float)r64;
+					const float zi = a.invD ? ri * ldh(a.invD + row, pol.last) : ri;
+					sth(a.z + row, zi, pol.last);
+					vR[0] += r64 * r64;
+					vR[1] += (double)ri * (double)zi;
+				}
+			}
+		}
+		if (!grid_allreduce<2>(vR, a.partials, 3, a.count, gen)) { status = RSD_ETIMEOUT; done = 1; break; }
+		const double rt = sqrt(vR[0]);
+		const double rel = rt / (res0 + 1e-50);
+		if (a.adaptive) dcur = next_delta(dcur, res, rt, kDeltaFloorCg);
+		res64 = rt; trueRel = rel; rmax = rt; res = rt;
+		refinements += 1;
+		const double crit = a.relMode ? rel : rt;
+		if (!isfinite(rt)) { done = 1; converged = 0; status = RSD_ENAN; }
+		else if (crit < a.tol) { done = 1; converged = 1; }
+		else if (iter + 1 >= a.maxIters) { done = 1; converged = 0; iter = a.maxIters; }
+		else rho = vR[1];
+	}
+	if (!done) { done = 1; converged = 0; }   // the guard ran out (cannot happen with a finite maxIters)
+	if (blockIdx.x == 0 && threadIdx.x == 0) {
+		S->rz = rho; S->rhoPrev = rhoPrev; S->alpha = alphaPrev; S->beta = betaPrev;
+		S->res = res; S->rmax = rmax; S->dcur = dcur; S->res64 = res64; S->trueRel = trueRel;
+		S->iter = iter; S->refinements = refinements; S->done = done; S->converged = converged; S->status = status;
+		S->reliable = 0;
+	}
+}
+
 __global__ void k_invdiag32(int64_t n, const int32_t* __restrict__ dpos, const double* __restrict__ val, float* __restrict__ d) {
 	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
 		const int32_t q = dpos[i];
@@ -505,6 +703,16 @@ static bool graph_mode(const rsd_ctx* ctx) {
 	if (ctx->prof.on) return false;              // per-kernel timing needs the plain launches
 	const char* e = getenv("RSD_CG_GRAPH");
 	return !(e && e[0] == '0');
+}
+
+// the persistent mixed solve (k_mx_persist) needs cooperative launches; RSD_CG_PERSIST=0 keeps the
+// graph of per-phase kernels
+static bool persist_mode(const rsd_ctx* ctx) {
+	const char* e = getenv("RSD_CG_PERSIST");
+	if (e && e[0] == '0') return false;
+	int coop = 0;
+	cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device);
+	return coop != 0;
 }
 
 static GraphCache* graph_cache(rsd_ctx* ctx) {
@@ -700,7 +908,11 @@ static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const d
 	const MatView<float> V32 = view32(A);
 	void* wsv;
 	const int64_t ns = pad_len(n);
-	RSD_CHECK(get_ws(ctx, sizeof(float) * 6 * ns, &wsv));
+	// six FP32 vectors, then the persistent kernel's partial slots and barrier count
+	const size_t vecBytes = sizeof(float) * 6 * ns;
+	RSD_CHECK(get_ws(ctx, vecBytes + sizeof(double) * kPersistSlots * kMaxPartials + 256, &wsv));
+	double* pslots = (double*)((char*)wsv + vecBytes);
+	unsigned long long* pcount = (unsigned long long*)(pslots + kPersistSlots * kMaxPartials);
 	// the residual is carried as z = M r alone (r = D z for the reductions)
 	float* z = (float*)wsv;  // M r, the vector the SpMV multiplies
 	float* p = z + ns;
@@ -729,7 +941,9 @@ static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const d
 		RSD_DISPATCH_L(L, (k_mx_spmv_dot<LL><<<RGB(k_mx_spmv_dot<LL>, kST), kST, 0, st>>>(n, V32, z, w, S, partials)));
 	};
 	auto step = [&](GraphCtl gc) {
-		k_mx_step<<<VGB(k_mx_step, kVT), kVT, 0, st>>>(n, y, z, p, sv, w, invD, S, partials, tol, rel, maxIt, gc);
+		// 512-thread blocks on the SpMV's grid: the partition k_mx_persist uses, so that both paths
+		// give the same sums, bit for bit
+		k_mx_step<<<VGB(k_mx_step, kST), kST, 0, st>>>(n, y, z, p, sv, w, invD, S, partials, tol, rel, maxIt, gc);
 	};
 	auto body_a = [&](GraphCtl gc) -> int {
 		spmv();
@@ -744,7 +958,22 @@ static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const d
 		return RSD_OK;
 	};
 	auto body_b = [&](GraphCtl) -> int { return RSD_OK; };   // the step kernel sets the loop condition
-	if (graph_mode(ctx)) {
+	if (graph_mode(ctx) && L <= 0 && persist_mode(ctx)) {
+		// the whole iteration in one cooperative launch (SELL-32 layouts)
+		RSD_CHECK(prologue());
+		RSD_CUDA(cudaMemsetAsync(pcount, 0, sizeof(unsigned long long), st));
+		MxPersistArgs args{n, V32, V, b, x, z, p, sv, w, y, invD, S, pslots, pcount, tol, rel, adaptive, maxIt};
+		void* params[] = {&args};
+		auto go = [&](const void* kern) -> int {
+			int per = 0;
+			RSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kST, 0));
+			const int grid = std::min(std::max(per, 1) * ctx->num_sms, kMaxPartials);
+			RSD_CUDA(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kST), params, 0, st));
+			return RSD_OK;
+		};
+		RSD_CHECK(L == -1 ? go((const void*)k_mx_persist<-1>) : go((const void*)k_mx_persist<0>));
+		RSD_CHECK(finish_report(ctx, S, rep));
+	} else if (graph_mode(ctx)) {
 		CgGraph& G = graph_cache(ctx)->cg[1];
 		CgKey key{};
 		const void* ptrs[] = {A, V.ptr, V.col, V.val, V32.val, exec_diag(A), b, x, z, invD, S, partials};
