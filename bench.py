@@ -959,7 +959,8 @@ def main():
         ms = e0.elapsed_time(e1) / steps
         prof = {}
         if profile:
-            for fam in ("spmv_dot_f32", "spmv_dot_f64", "cg_update", "cg_pupdate", "reliable_update", "assemble_matrix", "assemble_vector"):
+            for fam in ("cg_persist", "spmv_dot_f32", "spmv_dot_f64", "cg_update", "cg_pupdate", "reliable_update",
+                        "assemble_matrix", "assemble_vector"):
                 prof[fam] = ctx.profile_get(fam)
             ctx.profile(False)
         return ms, reps, prof, clk
@@ -975,11 +976,16 @@ def main():
         if dist is not None:
             dist.destroy_process_group()
         return
-    # timed: the solves run as cached CUDA graphs; then the same steps once more with per-kernel
-    # event timing (plain launches) for the breakdown and the roofline
+    # timed: the mixed solves run as one persistent kernel each (the FP64 ones as cached CUDA graphs);
+    # then the same steps once more with event timing around each kernel family (the persistent
+    # kernel, the assembly), and once with the mixed iteration as one kernel per phase (plain
+    # launches) for the phase breakdown
     ms_mx, reps_mx, _, clk = run(cfgs["mixed"], args.steps, args.warmup, clocks=clocks)
     ms_64, reps_64, _, clk64 = run(cfgs["fp64"], args.steps, args.warmup, clocks=ClockSampler(local))
-    _, _, prof_mx, _ = run(cfgs["mixed"], args.steps, args.warmup, profile=True)
+    _, reps_pr, prof_mx, _ = run(cfgs["mixed"], args.steps, args.warmup, profile=True)
+    os.environ["RSD_CG_PERSIST"] = "0"
+    _, _, prof_ph, _ = run(cfgs["mixed"], args.steps, args.warmup, profile=True)
+    del os.environ["RSD_CG_PERSIST"]
     _, _, prof_64, _ = run(cfgs["fp64"], args.steps, args.warmup, profile=True)
 
     # time to the FP64-checked 1e-8 residual of the first step's system alone: K + M/dt, b = M U0 / dt,
@@ -1082,8 +1088,8 @@ def main():
     ms_mx, ms_64, ms_e2e = reduce_max(ms_mx), reduce_max(ms_64), reduce_max(ms_e2e)
     solve_t = {k: reduce_max(v) for k, v in solve_t.items()}
 
-    # dominant kernel of the mixed step: the FP32 SpMV (+ p.Ap) of every CG iteration
-    launches, tot = prof_mx["spmv_dot_f32"]
+    # the mixed iteration's phases run one kernel each: the FP32 SpMV (+ z.w) dominates them
+    launches, tot = prof_ph["spmv_dot_f32"]
     avg_ms = tot / max(launches, 1)
     bytes_spmv32 = nnz * (4 + 4) + 4 * (n + 1) + 2 * n * 4
     peak, peak_kind = measured_peak_hbm()
@@ -1095,13 +1101,12 @@ def main():
 
     it_mx = [r["iterations"] for r in reps_mx]
     it_64 = [r["iterations"] for r in reps_64]
-    solve_mx = sum(prof_mx[f][1] for f in ("spmv_dot_f32", "cg_update", "cg_pupdate", "reliable_update")) / args.steps
+    solve_mx = prof_mx["cg_persist"][1] / args.steps
     solve_64 = sum(prof_64[f][1] for f in ("spmv_dot_f64", "cg_update", "cg_pupdate")) / args.steps
-    # kernels run in the timed mixed steps: per step 8 outside the solve (Udot, K + M/dt with its FP32
-    # copy, right-hand side, lift, inverse diagonal, initial residual, stage residual, its norm); in the
-    # solve 2 per loop body (SpMV + z.Az, vector pass) and 2 per replacement node (fold, FP64
-    # residual), with one idle body and replacement node after the converged one
-    gpu_launches = int(sum(8 + 2 * (r["iterations"] + 1) + 2 * (r["refinements"] + 1) for r in reps_mx))
+    # kernels run in the timed mixed steps: per step 8 outside the solve loop (Udot, K + M/dt with its
+    # FP32 copy, right-hand side, lift, inverse diagonal, initial residual, stage residual, its norm)
+    # and the persistent solve kernel
+    gpu_launches = int(9 * len(reps_mx))
 
     # the reference's own first step of the same workload (one core), timed on the host, and parity
     # at the configured size: the device's first step from T0 in FP64 and mixed precision against it
@@ -1171,14 +1176,32 @@ def main():
         achieved_dram = traffic / (avg_ms * 1e6)
     else:
         achieved_dram = None
-    roofline = {"kernel": "k_mx_spmv_dot (FP32 SELL-32 SpMV + z.w)", "bound": "hbm",
-                "achieved": achieved_dram, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                "frac": achieved_dram / peak if achieved_dram else None,
-                "frac_nominal_8tbs": achieved_dram / 8000.0 if achieved_dram else None,
-                "traffic": traffic, "avg_launch_us": avg_ms * 1e3, "launches": launches,
-                "algorithmic_bytes": bytes_spmv32, "algorithmic_equiv_gbs": achieved,
-                "algorithmic_equiv_frac": achieved / peak if achieved else None,
-                "note": "achieved = ncu DRAM bytes per launch / CUDA-event average launch time on the solve stream",
+    # the timed region's dominant kernel: k_mx_persist, one launch per mixed solve.  Its DRAM traffic
+    # per CG iteration (replacements included) from the ncu capture of this workload, times the
+    # iterations of the profiled solves, over their event-timed launches
+    persist = ncu_traffic("k_mx_persist") or {}
+    pl, pt = prof_mx["cg_persist"]
+    it_pr = float(np.mean([r["iterations"] for r in reps_pr])) if reps_pr else None
+    per_iter = persist.get("bytes_per_launch", 0) / persist["iterations"] if persist.get("iterations") else None
+    p_avg_ms = pt / max(pl, 1)
+    p_traffic = per_iter * it_pr if per_iter and it_pr else None
+    p_achieved = p_traffic / (p_avg_ms * 1e6) if p_traffic and pl else None
+    alg_iter = bytes_spmv32 + 10 * n * 4   # the SpMV's algorithmic bytes + the vector pass's ten FP32 vectors
+    roofline = {"kernel": "k_mx_persist (mixed CG: FP32 SELL-32 SpMV + z.w, vector pass, FP64 replacements)", "bound": "hbm",
+                "achieved": p_achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                "frac": p_achieved / peak if p_achieved else None,
+                "frac_nominal_8tbs": p_achieved / 8000.0 if p_achieved else None,
+                "traffic": p_traffic, "avg_launch_us": p_avg_ms * 1e3, "launches": pl, "iterations_per_launch": it_pr,
+                "traffic_per_iteration": per_iter, "traffic_source": persist.get("source"),
+                "algorithmic_bytes": alg_iter * it_pr if it_pr else None,
+                "algorithmic_equiv_gbs": alg_iter * it_pr / (p_avg_ms * 1e6) if it_pr and pl else None,
+                "note": "achieved = ncu DRAM bytes per CG iteration x iterations of the profiled solves / "
+                        "CUDA-event average launch time on the solve stream",
+                "spmv_phase": {"kernel": "k_mx_spmv_dot (the SpMV phase as its own kernel)", "traffic": traffic,
+                               "avg_launch_us": avg_ms * 1e3, "launches": launches,
+                               "achieved": achieved_dram, "frac": achieved_dram / peak if achieved_dram else None,
+                               "algorithmic_bytes": bytes_spmv32, "algorithmic_equiv_gbs": achieved,
+                               "algorithmic_equiv_frac": achieved / peak if achieved else None},
                 "fp64_spmv": {"kernel": "k_cg_spmv_dot", "traffic": ncu_traffic("k_cg_spmv_dot"),
                               "avg_launch_us": 1e3 * t64 / max(l64, 1),
                               "achieved": (ncu_traffic("k_cg_spmv_dot") / (t64 / max(l64, 1) * 1e6)) if ncu_traffic("k_cg_spmv_dot") and l64 else None,
@@ -1205,6 +1228,7 @@ def main():
         "roofline": roofline,
         "assembly_roofline": asm_roof,
         "kernel_ms_per_step": {k: v[1] / args.steps for k, v in prof_mx.items()},
+        "phase_kernel_ms_per_step": {k: v[1] / args.steps for k, v in prof_ph.items()},
         "kernel_ms_per_step_fp64": {k: v[1] / args.steps for k, v in prof_64.items()},
         "clocks_fp64": clk64,
         "full_run_50_steps": full_run,

@@ -92,8 +92,9 @@ int rsd_version(int32_t* major, int32_t* minor);
 int rsd_expr_check(const char* expr, int32_t* depth);
 /* Tracing (the reference has only its benchmark Timer, include/benchmark/core/Timer.hpp:10-24):
  * when enabled, every launch of the kernel families "spmv_dot_f64", "spmv_dot_f32", "cg_update",
- * "cg_pupdate", "reliable_update", "assemble_matrix", "assemble_vector", "spmv" is bracketed by
- * CUDA events on the context stream; rsd_ctx_profile_get returns launches and summed device time.
+ * "cg_pupdate", "reliable_update", "assemble_matrix", "assemble_vector", "spmv", "cg_persist" (the
+ * mixed solve's persistent kernel, one launch per solve) is bracketed by CUDA events on the context
+ * stream; rsd_ctx_profile_get returns launches and summed device time.
  * Enabling (or disabling) resets the totals. */
 int rsd_ctx_profile(rsd_ctx* ctx, int32_t enable);
 int rsd_ctx_profile_get(rsd_ctx* ctx, const char* family, int64_t* launches, double* total_ms);

@@ -515,7 +515,7 @@ int build_pattern(rsd_ctx* ctx, const rsd_heat* h, rsd_csr** out) {
 // per-kernel-family event timing
 // ---------------------------------------------------------------------------------------------
 static const char* kFamilyNames[PF_COUNT] = {"spmv_dot_f64", "spmv_dot_f32", "cg_update", "cg_pupdate", "reliable_update",
-                                             "assemble_matrix", "assemble_vector", "spmv"};
+                                             "assemble_matrix", "assemble_vector", "spmv", "cg_persist"};
 
 int prof_begin(rsd_ctx* ctx, int family) {
 	Profiler& p = ctx->prof;

@@ -57,7 +57,7 @@ struct rsd_scratch {
 namespace rsd {
 // per-kernel-family launch timing with CUDA events on the context stream (off by default)
 enum ProfFamily { PF_SPMV_DOT_F64, PF_SPMV_DOT_F32, PF_CG_UPDATE, PF_CG_PUPDATE, PF_RELIABLE, PF_ASM_MATRIX,
-                  PF_ASM_VECTOR, PF_SPMV, PF_COUNT };
+                  PF_ASM_VECTOR, PF_SPMV, PF_CG_PERSIST, PF_COUNT };
 struct Profiler {
 	bool on = false;
 	std::vector<cudaEvent_t> pool;

@@ -370,7 +370,7 @@ __global__ void __launch_bounds__(kST, kRowBlocks) k_mx_reliable(int64_t n, MatV
 // scalar loads at the start and its last-block reduction tail.  Each barrier waits a bounded time;
 // a barrier that gives up ends the solve with RSD_ETIMEOUT.
 constexpr int kPersistSlots = 5;                        // partial slots: SpMV 0; step 1, 2; replacement 3, 4
-constexpr unsigned long long kBarrierPolls = 1ull << 22;  // 256 ns apart: about a second
+constexpr unsigned long long kBarrierPolls = 1ull << 24;  // the first 4096 back to back, then 64 ns apart: about a second
 
 __device__ __forceinline__ bool grid_barrier(unsigned long long* count, unsigned long long target) {
 	__shared__ int ok;
@@ -382,7 +382,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned long long* count, unsigned
 		int good = 1;
 		while (*(volatile unsigned long long*)count < target) {
 			if (++polls > kBarrierPolls) { good = 0; break; }
-			__nanosleep(256);
+			if (polls > 4096) __nanosleep(64);
 		}
 		__threadfence();
 		ok = good;
@@ -706,10 +706,13 @@ static bool graph_mode(const rsd_ctx* ctx) {
 }
 
 // the persistent mixed solve (k_mx_persist) needs cooperative launches; RSD_CG_PERSIST=0 keeps the
-// graph of per-phase kernels
+// per-phase kernels (as a graph, or as plain launches under RSD_CG_GRAPH=0 or profiling, which then
+// times each phase)
 static bool persist_mode(const rsd_ctx* ctx) {
 	const char* e = getenv("RSD_CG_PERSIST");
 	if (e && e[0] == '0') return false;
+	const char* g = getenv("RSD_CG_GRAPH");
+	if (g && g[0] == '0') return false;
 	int coop = 0;
 	cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device);
 	return coop != 0;
@@ -958,7 +961,7 @@ static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const d
 		return RSD_OK;
 	};
 	auto body_b = [&](GraphCtl) -> int { return RSD_OK; };   // the step kernel sets the loop condition
-	if (graph_mode(ctx) && L <= 0 && persist_mode(ctx)) {
+	if (L <= 0 && persist_mode(ctx)) {
 		// the whole iteration in one cooperative launch (SELL-32 layouts)
 		RSD_CHECK(prologue());
 		RSD_CUDA(cudaMemsetAsync(pcount, 0, sizeof(unsigned long long), st));
@@ -971,7 +974,9 @@ static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const d
 			RSD_CUDA(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kST), params, 0, st));
 			return RSD_OK;
 		};
+		const int pf = prof_begin(ctx, PF_CG_PERSIST);
 		RSD_CHECK(L == -1 ? go((const void*)k_mx_persist<-1>) : go((const void*)k_mx_persist<0>));
+		prof_end(ctx, pf);
 		RSD_CHECK(finish_report(ctx, S, rep));
 	} else if (graph_mode(ctx)) {
 		CgGraph& G = graph_cache(ctx)->cg[1];
