@@ -171,8 +171,11 @@ int rsd_solve(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const double*
  * limits A to at most 262,144 rows; larger matrices are rejected with RSD_EINVAL and a message.
  * The scalars and reduction tickets that must start at zero are cleared on the stream by each call.
  * The array is shared by every call on a device: calls that overlap on one device (two host threads,
- * or two streams in flight) race on it and must be serialized by the caller.  The first call on a
- * device looks up the array's device address (setup), so make it before any stream capture. */
+ * or two streams in flight) race on it and must be serialized by the caller.  The call synchronizes
+ * the stream and reads its report into pageable host memory, so it cannot be used inside a stream
+ * capture.  The first call on a device looks up the array's device address and keeps it for the
+ * life of the process: a primary context torn down and recreated (cudaDeviceReset) leaves that
+ * address stale, so do not reset the device between calls. */
 int rsd_cg_solve_static(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const double* b, double* x,
                         rsd_report* report);
 
@@ -330,7 +333,9 @@ int rsd_heat_be_step_host(rsd_ctx* ctx, rsd_heat* h, double dt, const rsd_solver
  * solver/stage/SteadyStage.hpp:89-116): R = F - K(T)T, J = K + K_T, J dU = R, U += dU.
  * linear->operator_type RSD_OP_FEM: J is not assembled; each product of the linear solve is an element
  * pass of Diffusion + TangentDiffusion at the Newton state (the reference's FEMOperator over the
- * Jacobian forms), Jacobi from that operator's element diagonal. */
+ * Jacobian forms), Jacobi from that operator's element diagonal.  With a nonzero dk/dT the Jacobian
+ * K + K_T is not symmetric: solve it with GMRES (linear->type RSD_GMRES); CG has no convergence
+ * guarantee there and may stop at max_iters unconverged, reported as such. */
 int rsd_heat_newton(rsd_ctx* ctx, rsd_heat* h, double abs_tol, double rel_tol, int64_t max_iters,
                     const rsd_solver_cfg* linear, double* U, rsd_report* report);
 

@@ -604,6 +604,110 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_asm_matrix_rows(const AsmPar
 	}
 }
 
+// The same row gather for 4- and 8-node elements with the reference integrals formed in registers
+// from their 1D factors: on the tensor-product rule the reference-element integral of
+// dN_a/dxi_s dN_b/dxi_t (symmetrised for s != t) and of N_a N_b is a product over the directions of
+// the 1D integrals K = int N_i' N_j', M = int N_i N_j and G = int N_i' N_j with i, j the nodes' 1D
+// indices (bit d of the local node number).  The table kernel above reads 7 shared-memory entries
+// per (row, element, column) and was bound by the shared-memory pipe; these products cost about 20
+// FP64 operations and no memory.  Same integrals, same summation order per entry.
+struct Q1Fac {
+	double K[2][2], M[2][2], G[2][2];
+};
+template <int NSD>
+__global__ void __launch_bounds__(32 * kRowWarps) k_asm_matrix_rows_q1(const AsmParams prm, const Q1Fac f,
+                                                                        const int32_t* __restrict__ adjPtr,
+                                                                        const int32_t* __restrict__ adj, int64_t n, int32_t maxLen) {
+	constexpr int NPE = NSD == 3 ? 8 : 4, RB = 8;
+	extern __shared__ double sm[];
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	double* acc = sm + (size_t)warp * maxLen * 32 + lane;   // this lane's column of the slice image
+	const int64_t ns = (n + 31) >> 5;
+	for (int64_t s = (int64_t)blockIdx.x * kRowWarps + warp; s < ns; s += (int64_t)gridDim.x * kRowWarps) {
+		const int32_t s0 = prm.sStart[s];
+		const int len = (prm.sStart[s + 1] - s0) >> 5;
+		for (int j = 0; j < len; ++j) acc[j * 32] = 0.0;
+		const int64_t row = 32 * s + lane;
+		if (row < n) {
+			constexpr int ABATCH = 2;
+			const int32_t q1 = adjPtr[row + 1];
+			for (int32_t q0 = adjPtr[row]; q0 < q1; q0 += ABATCH) {
+				int32_t ea[ABATCH];
+				double gk[ABATCH][8];
+				unsigned long long w[ABATCH];
+#pragma unroll
+				for (int k = 0; k < ABATCH; ++k) ea[k] = q0 + k < q1 ? adj[q0 + k] : -1;
+#pragma unroll
+				for (int k = 0; k < ABATCH; ++k) {
+					if (ea[k] < 0) continue;
+					const int32_t e = ea[k] / NPE;
+					const double2* gp = reinterpret_cast<const double2*>(prm.geo + (int64_t)e * 8);
+#pragma unroll
+					for (int i = 0; i < 4; ++i) { const double2 v = gp[i]; gk[k][2 * i] = v.x; gk[k][2 * i + 1] = v.y; }
+					gk[k][7] = prm.kElem ? prm.kElem[e] : 1.0;
+					w[k] = __ldcs(reinterpret_cast<const unsigned long long*>(prm.ranks + (int64_t)ea[k] * RB));
+				}
+#pragma unroll
+				for (int k = 0; k < ABATCH; ++k) {
+					if (ea[k] < 0) continue;
+					const int a = ea[k] - (ea[k] / NPE) * NPE;
+					const double cd = prm.cDiff * gk[k][7] * prm.kConst * gk[k][6];
+					const double cm = prm.cMass * prm.rho * prm.cp * gk[k][6];
+					// the 1D factors of this row's node, per direction d and 1D column index c
+					double Km[3][2], Mm[3][2], Gr[3][2], Gc[3][2];
+#pragma unroll
+					for (int d = 0; d < NSD; ++d) {
+						const int ia = (a >> d) & 1;
+#pragma unroll
+						for (int c = 0; c < 2; ++c) {
+							Km[d][c] = ia ? f.K[1][c] : f.K[0][c];
+							Mm[d][c] = ia ? f.M[1][c] : f.M[0][c];
+							Gr[d][c] = ia ? f.G[1][c] : f.G[0][c];   // int N_a' N_b
+							Gc[d][c] = ia ? f.G[c][1] : f.G[c][0];   // int N_a N_b'
+						}
+					}
+#pragma unroll
+					for (int b = 0; b < NPE; ++b) {
+						const int j = (int)((w[k] >> (8 * b)) & 0xFF);
+						if (j == 0xFF) continue;
+						const int b0 = b & 1, b1 = (b >> 1) & 1, b2 = (b >> 2) & 1;
+						double g, mass;
+						if constexpr (NSD == 3) {
+							const double m12 = Mm[1][b1] * Mm[2][b2], m02 = Mm[0][b0] * Mm[2][b2], m01 = Mm[0][b0] * Mm[1][b1];
+							const double s00 = Km[0][b0] * m12, s11 = Km[1][b1] * m02, s22 = Km[2][b2] * m01;
+							const double s01 = (Gr[0][b0] * Gc[1][b1] + Gc[0][b0] * Gr[1][b1]) * Mm[2][b2];
+							const double s02 = (Gr[0][b0] * Gc[2][b2] + Gc[0][b0] * Gr[2][b2]) * Mm[1][b1];
+							const double s12 = (Gr[1][b1] * Gc[2][b2] + Gc[1][b1] * Gr[2][b2]) * Mm[0][b0];
+							g = gk[k][0] * s00;
+							g += gk[k][1] * s11;
+							g += gk[k][2] * s22;
+							g += gk[k][3] * s01;
+							g += gk[k][4] * s02;
+							g += gk[k][5] * s12;
+							mass = Mm[0][b0] * m12;
+						} else {
+							const double s00 = Km[0][b0] * Mm[1][b1], s11 = Mm[0][b0] * Km[1][b1];
+							const double s01 = Gr[0][b0] * Gc[1][b1] + Gc[0][b0] * Gr[1][b1];
+							g = gk[k][0] * s00;
+							g += gk[k][1] * s11;
+							g += gk[k][2] * s01;
+							mass = Mm[0][b0] * Mm[1][b1];
+						}
+						acc[j * 32] += cd * g + cm * mass;
+					}
+				}
+			}
+		}
+		double2* out = reinterpret_cast<double2*>(prm.val + s0) + lane;
+		for (int jp = 0; jp < (len >> 1); ++jp) out[32 * jp] = make_double2(acc[(2 * jp) * 32], acc[(2 * jp + 1) * 32]);
+		if (prm.val32) {
+			float2* out32 = reinterpret_cast<float2*>(prm.val32 + s0) + lane;
+			for (int jp = 0; jp < (len >> 1); ++jp)
+				out32[32 * jp] = make_float2((float)acc[(2 * jp) * 32], (float)acc[(2 * jp + 1) * 32]);
+		}
+	}
+}
+
 template <int NSD, int P>
 __global__ void k_build_slots(int64_t nelem, const int32_t* __restrict__ ien, const int32_t* __restrict__ t2a,
                               const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
@@ -1916,6 +2020,36 @@ static int launch_matrix_rows(rsd_ctx* ctx, rsd_heat* h, const AsmParams& p, boo
 		*done = true;
 		return RSD_OK;
 	};
+	if (ord == 1) {
+		// the 1D factors on the problem's rule (the 3D tables are their products)
+		Q1Fac f{};
+		double xq[5], wq[5], N[4], dN[4], Nq[5][2], dNq[5][2];
+		gauss_legendre(h->nq1, xq, wq);
+		for (int q = 0; q < h->nq1; ++q) {
+			lagrange1d(1, xq[q], N, dN);
+			for (int i = 0; i < 2; ++i) { Nq[q][i] = N[i]; dNq[q][i] = dN[i]; }
+		}
+		for (int i = 0; i < 2; ++i)
+			for (int j = 0; j < 2; ++j) {
+				double k = 0.0, m = 0.0, g = 0.0;
+				for (int q = 0; q < h->nq1; ++q) {
+					k += wq[q] * dNq[q][i] * dNq[q][j];
+					m += wq[q] * Nq[q][i] * Nq[q][j];
+					g += wq[q] * dNq[q][i] * Nq[q][j];
+				}
+				f.K[i][j] = k; f.M[i][j] = m; f.G[i][j] = g;
+			}
+		const size_t smem1 = sizeof(double) * (size_t)kRowWarps * h->maxSlice * 32;
+		auto go1 = [&](auto kern) -> int {
+			if (smem1 > 48 * 1024) RSD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1));
+			kern<<<blocks, 32 * kRowWarps, smem1, ctx->stream>>>(p, f, h->adjPtr, h->adj, h->n, h->maxSlice);
+			RSD_CUDA(cudaGetLastError());
+			*done = true;
+			return RSD_OK;
+		};
+		const char* tabEnv = getenv("RSD_ROW_ASM_TABLES");
+		if (!(tabEnv && tabEnv[0] == '1')) return nsd == 3 ? go1(k_asm_matrix_rows_q1<3>) : go1(k_asm_matrix_rows_q1<2>);
+	}
 	if (nsd == 2 && ord == 1) return go(k_asm_matrix_rows<2, 1>);
 	if (nsd == 2 && ord == 2) return go(k_asm_matrix_rows<2, 2>);
 	if (nsd == 2 && ord == 3) return go(k_asm_matrix_rows<2, 3>);

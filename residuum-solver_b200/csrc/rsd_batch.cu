@@ -87,6 +87,10 @@ template <typename TI, int L>
 __device__ void solve_one(const BatchProb<TI>& P, BatchOut* out, double tol, int relMode, int64_t maxIt, double delta,
                           int adaptive, double (*sm)[kBW]) {
 	constexpr bool kMixed = sizeof(TI) == 4;
+	constexpr int PW = 16 / sizeof(TI);   // entries per 16-byte packet
+	struct Vec { TI v[PW]; };
+	auto ldv = [](const TI* a) { Vec o; *reinterpret_cast<uint4*>(&o) = *reinterpret_cast<const uint4*>(a); return o; };
+	auto stv = [](TI* a, const Vec& o) { *reinterpret_cast<uint4*>(a) = *reinterpret_cast<const uint4*>(&o); };
 	const int64_t n = P.n;
 	const L2Pol pol = make_l2pol();
 	TI* __restrict__ r = P.r;
@@ -142,15 +146,25 @@ __device__ void solve_one(const BatchProb<TI>& P, BatchOut* out, double tol, int
 		if (!isfinite(alpha)) { status = RSD_EBREAKDOWN; break; }
 		const TI a = (TI)alpha;
 		double u[2] = {0.0, 0.0};
-		for (int64_t i = tid; i < n; i += kBT) {
-			if (kMixed) y[i] = y[i] + a * p[i];
-			else x[i] = x[i] + alpha * (double)p[i];    // FP64: x += alpha p as cg/Solver.tpp:74-76
-			const TI ri = r[i] - a * Ap[i];
-			r[i] = ri;
-			const TI zi = zr(i, ri);
+		auto upd = [&](int64_t i, TI pi, TI api, TI ri0, TI di) {
+			if (kMixed) y[i] = y[i] + a * pi;
+			else x[i] = x[i] + alpha * (double)pi;    // FP64: x += alpha p as cg/Solver.tpp:74-76
+			const TI ri = ri0 - a * api;
+			const TI zi = invD ? ri * di : ri;
 			u[0] += (double)ri * (double)ri;
 			u[1] += (double)ri * (double)zi;
+			return ri;
+		};
+		// 16-byte packets (the workspace vectors start 256-byte aligned), then the scalar tail
+		for (int64_t iv = tid; iv < n / PW; iv += kBT) {
+			const int64_t i0 = iv * PW;
+			Vec P = ldv(p + i0), AP = ldv(Ap + i0), R = ldv(r + i0), D{};
+			if (invD) D = ldv(invD + i0);
+#pragma unroll
+			for (int k = 0; k < PW; ++k) R.v[k] = upd(i0 + k, P.v[k], AP.v[k], R.v[k], D.v[k]);
+			stv(r + i0, R);
 		}
+		for (int64_t i = (n / PW) * PW + tid; i < n; i += kBT) r[i] = upd(i, p[i], Ap[i], r[i], invD ? invD[i] : (TI)1);
 		bsum<2>(u, sm);
 		++it;
 		res = sqrt(u[0]);
@@ -177,7 +191,15 @@ __device__ void solve_one(const BatchProb<TI>& P, BatchOut* out, double tol, int
 		const TI beta = (TI)(rzNew / rz);
 		rz = rzNew;
 		__syncthreads();
-		for (int64_t i = tid; i < n; i += kBT) p[i] = p[i] * beta + zr(i, r[i]);
+		for (int64_t iv = tid; iv < n / PW; iv += kBT) {
+			const int64_t i0 = iv * PW;
+			Vec P = ldv(p + i0), R = ldv(r + i0), D{};
+			if (invD) D = ldv(invD + i0);
+#pragma unroll
+			for (int k = 0; k < PW; ++k) P.v[k] = P.v[k] * beta + (invD ? R.v[k] * D.v[k] : R.v[k]);
+			stv(p + i0, P);
+		}
+		for (int64_t i = (n / PW) * PW + tid; i < n; i += kBT) p[i] = p[i] * beta + zr(i, r[i]);
 		__syncthreads();
 	}
 	if (kMixed && !converged) {

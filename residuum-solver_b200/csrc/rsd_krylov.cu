@@ -1672,6 +1672,8 @@ namespace {
 
 constexpr int kStaticMaxDevices = 64;
 static std::mutex g_static_mu;
+// the static scratch's device address per device, looked up on the first call and kept for the life
+// of the process: it assumes the primary context outlives every call (no cudaDeviceReset between them)
 static void* g_static_ptr[kStaticMaxDevices];
 
 // device address of this device's scratch, looked up once per device
