@@ -28,10 +28,11 @@ namespace rsd {
 
 // Position j of CSR entry q (column c) of row `row` in its SELL-32 slice: the rank within the row,
 // or in a stencil slice the index of the offset c - row in the slice's sorted pattern (whose padding
-// repeats the last offset, so the first match is the entry)
+// repeats the last offset, so the first match is the entry).  iperm: the row's slot row in a layout
+// whose slices hold the rows in another order, or null
 __device__ __forceinline__ int32_t sell_rank(const int32_t* sStart, const int32_t* sUni, const int32_t* sOffs,
-                                             const int32_t* rp, int32_t row, int32_t q, int32_t c) {
-	const int32_t sl = row >> 5;
+                                             const int32_t* iperm, const int32_t* rp, int32_t row, int32_t q, int32_t c) {
+	const int32_t sl = (iperm ? iperm[row] : row) >> 5;
 	const int32_t u = sUni ? sUni[sl] : -1;
 	if (u < 0) return q - rp[row];
 	const int32_t* pat = sOffs + u;
@@ -46,9 +47,10 @@ __device__ __forceinline__ int32_t sell_rank(const int32_t* sStart, const int32_
 
 // SELL-32 slot of CSR entry q (column c) of row `row`
 __device__ __forceinline__ int32_t sell_slot(const int32_t* sStart, const int32_t* sUni, const int32_t* sOffs,
-                                             const int32_t* rp, int32_t row, int32_t q, int32_t c) {
-	const int32_t j = sell_rank(sStart, sUni, sOffs, rp, row, q, c);
-	return sStart[row >> 5] + 64 * (j >> 1) + 2 * (row & 31) + (j & 1);
+                                             const int32_t* iperm, const int32_t* rp, int32_t row, int32_t q, int32_t c) {
+	const int32_t j = sell_rank(sStart, sUni, sOffs, iperm, rp, row, q, c);
+	const int32_t sr = iperm ? iperm[row] : row;
+	return sStart[sr >> 5] + 64 * (j >> 1) + 2 * (sr & 31) + (j & 1);
 }
 
 struct AsmParams {
@@ -78,6 +80,8 @@ struct AsmParams {
 	const int32_t* __restrict__ sStart;
 	const int32_t* __restrict__ sUni;   // stencil slices (pattern start per slice, -1 for none), or null
 	const int32_t* __restrict__ sOffs;
+	const int32_t* __restrict__ sPerm;  // slot row -> matrix row of the layout, or null (identity)
+	const int32_t* __restrict__ sIperm; // matrix row -> slot row, or null
 	double* __restrict__ val;
 	float* __restrict__ val32;          // row-gather assembly: the FP32 copy written alongside, or null
 	// element -> column-rank map [e][a][b]: the SELL-32 position j (sell_rank) of column t2a[node_b] in
@@ -499,7 +503,8 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_matrix(const AsmParams prm)
 			unsigned long long w[RB / 8];
 #pragma unroll
 			for (int k = 0; k < RB / 8; ++k) w[k] = __ldcs(rk + k);
-			double* rowBase = prm.val + prm.sStart[row >> 5] + 2 * (row & 31);
+			const int32_t sr = prm.sIperm ? prm.sIperm[row] : row;
+			double* rowBase = prm.val + prm.sStart[sr >> 5] + 2 * (sr & 31);
 #pragma unroll
 			for (int b = 0; b < NPE; ++b) {
 				const int j = (int)((w[b >> 3] >> (8 * (b & 7))) & 0xFF);
@@ -519,7 +524,7 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_matrix(const AsmParams prm)
 					if (prm.col[mid] < cb) lo = mid + 1; else hi = mid;
 				}
 				if (lo < end && prm.col[lo] == cb)
-					atomicAdd(prm.val + sell_slot(prm.sStart, prm.sUni, prm.sOffs, prm.rp, row, lo, cb), Ke[b]);
+					atomicAdd(prm.val + sell_slot(prm.sStart, prm.sUni, prm.sOffs, prm.sIperm, prm.rp, row, lo, cb), Ke[b]);
 			}
 		}
 	}
@@ -551,8 +556,9 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_asm_matrix_rows(const AsmPar
 		const int32_t s0 = prm.sStart[s];
 		const int len = (prm.sStart[s + 1] - s0) >> 5;
 		for (int j = 0; j < len; ++j) acc[j * 32] = 0.0;
-		const int64_t row = 32 * s + lane;
-		if (row < n) {
+		const int64_t srow = 32 * s + lane;
+		if (srow < n) {
+			const int64_t row = prm.sPerm ? prm.sPerm[srow] : srow;   // the matrix row this lane holds
 			// elements in batches of ABATCH: all their loads first, then the sums (in element order)
 			constexpr int ABATCH = 4;
 			const int32_t q1 = adjPtr[row + 1];
@@ -627,8 +633,9 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_asm_matrix_rows_q1(const Asm
 		const int32_t s0 = prm.sStart[s];
 		const int len = (prm.sStart[s + 1] - s0) >> 5;
 		for (int j = 0; j < len; ++j) acc[j * 32] = 0.0;
-		const int64_t row = 32 * s + lane;
-		if (row < n) {
+		const int64_t srow = 32 * s + lane;
+		if (srow < n) {
+			const int64_t row = prm.sPerm ? prm.sPerm[srow] : srow;   // the matrix row this lane holds
 			constexpr int ABATCH = 2;
 			const int32_t q1 = adjPtr[row + 1];
 			for (int32_t q0 = adjPtr[row]; q0 < q1; q0 += ABATCH) {
@@ -712,7 +719,8 @@ template <int NSD, int P>
 __global__ void k_build_slots(int64_t nelem, const int32_t* __restrict__ ien, const int32_t* __restrict__ t2a,
                               const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
                               const int32_t* __restrict__ sStart, const int32_t* __restrict__ sUni,
-                              const int32_t* __restrict__ sOffs, uint8_t* __restrict__ ranks, int32_t stride) {
+                              const int32_t* __restrict__ sOffs, const int32_t* __restrict__ iperm,
+                              uint8_t* __restrict__ ranks, int32_t stride) {
 	using E = Elem<NSD, P>;
 	constexpr int NPE = E::NPE;
 	const int64_t total = nelem * NPE;
@@ -731,7 +739,7 @@ __global__ void k_build_slots(int64_t nelem, const int32_t* __restrict__ ien, co
 					const int mid = (lo + hi) >> 1;
 					if (col[mid] < cb) lo = mid + 1; else hi = mid;
 				}
-				if (lo < end && col[lo] == cb) s = sell_rank(sStart, sUni, sOffs, rp, row, lo, cb);
+				if (lo < end && col[lo] == cb) s = sell_rank(sStart, sUni, sOffs, iperm, rp, row, lo, cb);
 			}
 			out[b] = (uint8_t)s;
 		}
@@ -1959,7 +1967,7 @@ static int ensure_slots(rsd_ctx* ctx, rsd_heat* h) {
 	const int64_t total = h->m->nelem * npe;
 	const int blocks = (int)std::min<int64_t>((total + 255) / 256, (int64_t)ctx->num_sms * 8);
 	const int nsd = h->m->nsd, ord = h->m->order;
-#define RSD_SLOTS(D, Q) k_build_slots<D, Q><<<std::max(blocks, 1), 256, 0, ctx->stream>>>(h->m->nelem, h->m->ien, h->t2a, K->rowPtr, K->col, K->sStart, K->sUni, K->sOffs, h->ranks, stride)
+#define RSD_SLOTS(D, Q) k_build_slots<D, Q><<<std::max(blocks, 1), 256, 0, ctx->stream>>>(h->m->nelem, h->m->ien, h->t2a, K->rowPtr, K->col, K->sStart, K->sUni, K->sOffs, K->sIperm, h->ranks, stride)
 	if (nsd == 2 && ord == 1) RSD_SLOTS(2, 1);
 	else if (nsd == 2 && ord == 2) RSD_SLOTS(2, 2);
 	else if (nsd == 2 && ord == 3) RSD_SLOTS(2, 3);
@@ -2064,6 +2072,7 @@ int assemble_matrix(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, doubl
 	RSD_CHECK(ensure_slots(ctx, h));
 	AsmParams p = params_for(h);
 	p.rp = A->rowPtr; p.col = A->col; p.sStart = A->sStart; p.sUni = A->sUni; p.sOffs = A->sOffs; p.val = A->sVal;
+	p.sPerm = A->sPerm; p.sIperm = A->sIperm;
 	// the slot map indexes h's pattern; another matrix of equal size may differ, so it searches
 	if (A == h->K || A->rowPtr == h->K->rowPtr) p.ranks = h->ranks;
 	p.cDiff = cDiff; p.cMass = cMass; p.cTDiff = cTDiff; p.cTMass = cTMass;

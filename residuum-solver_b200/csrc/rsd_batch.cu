@@ -79,7 +79,7 @@ __device__ __forceinline__ void slice_rows(const MatView<T>& A, int64_t n, int64
 	for (int64_t sl = warp; sl < nslices; sl += kBW) {
 		const int64_t row = sl * 32 + lane;
 		const double s = (double)row_sum<L, T, T>(A, row, n, 0, pol, xf);
-		if (row < n) f(row, s);
+		if (row < n) f(mat_row(A, row), s);
 	}
 }
 
@@ -313,8 +313,8 @@ int rsd_batch_solve(rsd_ctx* ctx, rsd_batch* B, const rsd_solver_cfg* cfg, const
 			BatchProb<TI>& P = d[i];
 			P.n = A->n;
 			P.nslices = A->nslices;
-			P.A = MatView<TI>{A->sStart, A->sCol, mixed ? (const TI*)A->val32 : (const TI*)A->sVal, A->sCol16, A->sBase, A->sUni, A->sOffs};
-			P.A64 = MatView<double>{A->sStart, A->sCol, A->sVal, A->sCol16, A->sBase, A->sUni, A->sOffs};
+			P.A = MatView<TI>{A->sStart, A->sCol, mixed ? (const TI*)A->val32 : (const TI*)A->sVal, A->sCol16, A->sBase, A->sUni, A->sOffs, A->sPerm};
+			P.A64 = MatView<double>{A->sStart, A->sCol, A->sVal, A->sCol16, A->sBase, A->sUni, A->sOffs, A->sPerm};
 			P.sDiag = A->sDiag;
 			P.b = b[i];
 			P.x = x[i];

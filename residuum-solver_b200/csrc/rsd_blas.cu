@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(512, kRowBlocks) k_spmv(int64_t n, MatView<T> 
 	for (int64_t base = rl.base; base < n; base += rl.step) {
 		const int64_t row = base + rl.sub;
 		const T s = row_dot<L, T, T>(A, x, row, n, rl.lane, pol);
-		if (rl.lane == 0 && row < n) sth(y + row, s, pol.first);
+		if (rl.lane == 0 && row < n) sth(y + mat_row(A, row), s, pol.first);
 	}
 }
 
@@ -165,7 +165,7 @@ __global__ void k_diag(int64_t n, const int32_t* __restrict__ dpos, const double
 __global__ void k_lump(int64_t n, MatView<double> A, double* __restrict__ d) {
 	const L2Pol pol = make_l2pol();
 	for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n; row += (int64_t)gridDim.x * blockDim.x)
-		d[row] = row_sum<0, double, double>(A, row, n, 0, pol, [](int) { return 1.0; });
+		d[mat_row(A, row)] = row_sum<0, double, double>(A, row, n, 0, pol, [](int) { return 1.0; });
 }
 
 }  // namespace rsd
@@ -288,7 +288,7 @@ int rsd_csr_lump(rsd_ctx* c, const rsd_csr* Ac, double* d) {
 	if (!c || !A || (A->n && !d)) return set_error(RSD_EINVAL, "null argument");
 	if (!A->n) return RSD_OK;
 	RSD_CHECK(sell_sync(c, A));
-	k_lump<<<vec_grid(c, A->n), 256, 0, c->stream>>>(A->n, MatView<double>{A->sStart, A->sCol, A->sVal}, d);
+	k_lump<<<vec_grid(c, A->n), 256, 0, c->stream>>>(A->n, MatView<double>{A->sStart, A->sCol, A->sVal, nullptr, nullptr, nullptr, nullptr, A->sPerm}, d);
 	RSD_CUDA(cudaGetLastError());
 	RSD_CUDA(cudaStreamSynchronize(c->stream));
 	return RSD_OK;

@@ -263,6 +263,58 @@ static void free_csr_arrays(rsd_csr* A) {
 	if (!A->owns_pattern) return;   // the pattern belongs to the matrix it was shared from
 	cudaFree(A->rowPtr); cudaFree(A->col); cudaFree(A->diag);
 	cudaFree(A->sStart); cudaFree(A->sCol); cudaFree(A->sSrc); cudaFree(A->sDiag); cudaFree(A->sCol16); cudaFree(A->sBase); cudaFree(A->sUni); cudaFree(A->sOffs);
+	cudaFree(A->sPerm); cudaFree(A->sIperm);
+}
+
+// The row order of the SELL-32 slices (SELL-C-sigma): within windows of kSellWindow rows, rows sorted
+// by length (longest first) and then by their column-offset pattern, stably, so that a slice holds
+// rows of one kind (on a Q2 mesh: vertex, edge, face or interior nodes, whose rows have 125, 75, 45
+// or 27 entries and one offset pattern each) instead of alternating kinds padded to the longest.
+// Opt-in (RSD_SELL_SORT=1), and then used when it shrinks the padded layout by a tenth or more.  On
+// the 48^3 Q2 Jacobian it cut the padding from 1.59 to 1.06 slots per entry but made GMRES's Arnoldi
+// step slower (241 against 223 us FP64): a slice's rows are then every other row of a grid line, so
+// the gathers touch twice the sectors, and fewer slices share one stencil pattern.  The rows past the
+// last whole window keep their order.
+constexpr int64_t kSellWindow = 32 * 16;
+static bool sell_row_order(int64_t n, const std::vector<int32_t>& rp, const std::vector<int32_t>& col,
+                           std::vector<int32_t>* perm) {
+	const char* env = getenv("RSD_SELL_SORT");
+	if (!(env && env[0] == '1') || n < kSellWindow) return false;
+	auto padded = [&](const int32_t* order) {
+		int64_t total = 0;
+		for (int64_t s0 = 0; s0 < n; s0 += 32) {
+			int32_t len = 0;
+			for (int64_t i = s0; i < std::min<int64_t>(n, s0 + 32); ++i) {
+				const int32_t r = order ? order[i] : (int32_t)i;
+				len = std::max(len, rp[r + 1] - rp[r]);
+			}
+			total += 32 * (int64_t)((len + 1) & ~1);
+		}
+		return total;
+	};
+	std::vector<uint64_t> key(n);
+	parallel_for(n, [&](int64_t b, int64_t e) {
+		for (int64_t i = b; i < e; ++i) {
+			uint64_t hsh = 1469598103934665603ull;   // FNV-1a over the offsets col - row
+			for (int32_t q = rp[i]; q < rp[i + 1]; ++q) {
+				hsh ^= (uint64_t)(uint32_t)(col[q] - (int32_t)i);
+				hsh *= 1099511628211ull;
+			}
+			const uint64_t len = (uint64_t)(rp[i + 1] - rp[i]);
+			key[i] = ((0xFFFFull - std::min<uint64_t>(len, 0xFFFF)) << 48) | (hsh >> 16);
+		}
+	});
+	std::vector<int32_t> order(n);
+	for (int64_t i = 0; i < n; ++i) order[i] = (int32_t)i;
+	const int64_t windows = n / kSellWindow;
+	parallel_for(windows, [&](int64_t b, int64_t e) {
+		for (int64_t w = b; w < e; ++w)
+			std::stable_sort(order.begin() + w * kSellWindow, order.begin() + (w + 1) * kSellWindow,
+			                 [&](int32_t x, int32_t y) { return key[x] < key[y]; });
+	});
+	if (padded(order.data()) * 10 > padded(nullptr) * 9) return false;
+	*perm = std::move(order);
+	return true;
 }
 
 // A matrix with src's pattern and layout (shared, not copied) and zero values of its own.
@@ -295,14 +347,18 @@ static int upload_csr(rsd_ctx* ctx, int64_t n, const std::vector<int32_t>& rp, c
 	A->nnz = nnz;
 	std::vector<int32_t> d(n);
 	diag_index(n, rp.data(), col.data(), d.data());
-	// SELL-32 layout: slice s holds rows 32s..32s+31, padded to its longest row rounded up to even;
+	// SELL-32 layout: slice s holds slot rows 32s..32s+31 (matrix rows prow(slot row): the identity
+	// unless sell_row_order groups rows of one kind), padded to its longest row rounded up to even;
 	// entries are stored in pairs, entry j of lane l at start[s] + 64 (j / 2) + 2 l + (j % 2), so that a
 	// lane reads two consecutive entries of its row with one 8- or 16-byte load
+	std::vector<int32_t> perm;
+	const bool permuted = sell_row_order(n, rp, col, &perm);
+	auto prow = [&](int64_t r) -> int64_t { return permuted ? (int64_t)perm[r] : r; };
 	const int64_t ns = (n + 31) / 32;
 	std::vector<int64_t> start(ns + 1, 0);
 	for (int64_t s = 0; s < ns; ++s) {
 		int32_t len = 0;
-		for (int64_t i = 32 * s; i < std::min<int64_t>(n, 32 * s + 32); ++i) len = std::max(len, rp[i + 1] - rp[i]);
+		for (int64_t i = 32 * s; i < std::min<int64_t>(n, 32 * s + 32); ++i) len = std::max(len, rp[prow(i) + 1] - rp[prow(i)]);
 		start[s + 1] = start[s] + 32 * (int64_t)((len + 1) & ~1);
 	}
 	auto pos = [&](int64_t s, int64_t l, int64_t j) { return start[s] + 64 * (j >> 1) + 2 * l + (j & 1); };
@@ -314,21 +370,22 @@ static int upload_csr(rsd_ctx* ctx, int64_t n, const std::vector<int32_t>& rp, c
 	parallel_for(ns, [&](int64_t b, int64_t e) {
 		for (int64_t s = b; s < e; ++s) {
 			const int64_t len = (start[s + 1] - start[s]) / 32;
-			const int64_t r0 = 32 * s;
+			const int64_t r0 = prow(32 * s);
 			// padding repeats a column the row already holds (value 0), so that it reads nothing new
 			const int32_t pad0 = rp[r0] < rp[r0 + 1] ? col[rp[r0]] : (int32_t)r0;
 			int32_t lo = INT32_MAX, hi = INT32_MIN;
 			for (int64_t l = 0; l < 32; ++l) {
-				const int64_t i = r0 + l;
-				const int32_t pad = i < n ? (rp[i] < rp[i + 1] ? col[rp[i + 1] - 1] : (int32_t)i) : pad0;
+				const bool in = 32 * s + l < n;
+				const int64_t i = in ? prow(32 * s + l) : -1;   // the matrix row of the slot row
+				const int32_t pad = in ? (rp[i] < rp[i + 1] ? col[rp[i + 1] - 1] : (int32_t)i) : pad0;
 				for (int64_t j = 0; j < len; ++j) {
 					const int64_t slot = pos(s, l, j);
-					if (i < n && rp[i] + j < rp[i + 1]) { sCol[slot] = col[rp[i] + j]; sSrc[slot] = (int32_t)(rp[i] + j); }
+					if (in && rp[i] + j < rp[i + 1]) { sCol[slot] = col[rp[i] + j]; sSrc[slot] = (int32_t)(rp[i] + j); }
 					else sCol[slot] = pad;
 					lo = std::min(lo, sCol[slot]);
 					hi = std::max(hi, sCol[slot]);
 				}
-				if (i < n && d[i] >= 0) sDiag[i] = (int32_t)pos(s, l, d[i] - rp[i]);
+				if (in && d[i] >= 0) sDiag[i] = (int32_t)pos(s, l, d[i] - rp[i]);
 			}
 			sMin[s] = len ? lo : 0;
 			sMax[s] = len ? hi : 0;
@@ -350,16 +407,21 @@ static int upload_csr(rsd_ctx* ctx, int64_t n, const std::vector<int32_t>& rp, c
 				if (r0 + 32 > n || len2 == 0) continue;
 				u.clear();
 				bool sorted = true;   // rows in increasing column order (the re-lay below matches in order)
-				for (int64_t i = r0; i < r0 + 32; ++i)
+				int64_t rmin = INT64_MAX, rmax = -1;
+				for (int64_t l = 0; l < 32; ++l) {
+					const int64_t i = prow(r0 + l);
+					rmin = std::min(rmin, i);
+					rmax = std::max(rmax, i);
 					for (int32_t q = rp[i]; q < rp[i + 1]; ++q) {
 						u.push_back(col[q] - (int32_t)i);
 						sorted = sorted && (q == rp[i] || col[q - 1] < col[q]);
 					}
+				}
 				if (!sorted) continue;
 				std::sort(u.begin(), u.end());
 				u.erase(std::unique(u.begin(), u.end()), u.end());
 				if (u.empty() || (int64_t)u.size() > len2) continue;
-				if (r0 + u.front() < 0 || r0 + 31 + (int64_t)u.back() >= n) continue;
+				if (rmin + u.front() < 0 || rmax + (int64_t)u.back() >= n) continue;
 				pat[s] = u;
 				pat[s].resize(len2, u.back());
 			}
@@ -383,7 +445,7 @@ static int upload_csr(rsd_ctx* ctx, int64_t n, const std::vector<int32_t>& rp, c
 				const int64_t len = (start[s + 1] - start[s]) / 32;
 				int32_t lo = INT32_MAX, hi = INT32_MIN;
 				for (int64_t l = 0; l < 32; ++l) {
-					const int64_t i = 32 * s + l;
+					const int64_t i = prow(32 * s + l);
 					int32_t q = rp[i];
 					sDiag[i] = -1;
 					for (int64_t j = 0; j < len; ++j) {
@@ -443,6 +505,16 @@ static int upload_csr(rsd_ctx* ctx, int64_t n, const std::vector<int32_t>& rp, c
 		if ((e = cudaMalloc(&A->sOffs, sizeof(int32_t) * offTable.size())) != cudaSuccess) return fail(e, "cudaMalloc sOffs");
 		if ((e = cudaMemcpyAsync(A->sUni, sUni.data(), sizeof(int32_t) * ns, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload sUni");
 		if ((e = cudaMemcpyAsync(A->sOffs, offTable.data(), sizeof(int32_t) * offTable.size(), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload sOffs");
+	}
+	if (permuted) {
+		std::vector<int32_t> iperm(n);
+		for (int64_t r = 0; r < n; ++r) iperm[perm[r]] = (int32_t)r;
+		if ((e = cudaMalloc(&A->sPerm, sizeof(int32_t) * n)) != cudaSuccess) return fail(e, "cudaMalloc sPerm");
+		if ((e = cudaMalloc(&A->sIperm, sizeof(int32_t) * n)) != cudaSuccess) return fail(e, "cudaMalloc sIperm");
+		if ((e = cudaMemcpyAsync(A->sPerm, perm.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload sPerm");
+		if ((e = cudaMemcpyAsync(A->sIperm, iperm.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload sIperm");
+		// the host copy must outlive the asynchronous copies: synchronize before it goes out of scope
+		if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return fail(e, "upload sIperm");
 	}
 	if (narrow) {
 		if ((e = cudaMalloc(&A->sCol16, sizeof(uint16_t) * ssize)) != cudaSuccess) return fail(e, "cudaMalloc sCol16");

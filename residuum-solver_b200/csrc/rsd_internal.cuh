@@ -116,6 +116,11 @@ struct rsd_csr {
 	int32_t* sUni = nullptr;       // nslices (or null when no slice qualifies)
 	int32_t* sOffs = nullptr;      // distinct patterns, concatenated
 	int64_t nStencil = 0;          // slices stored as stencil slices
+	// row order of the slices: slot row r of the layout holds matrix row sPerm[r] (rows of one column
+	// pattern grouped within windows, so that slices pad less and share stencil patterns), sIperm
+	// the inverse; both null when slot row r is row r
+	int32_t* sPerm = nullptr;      // n
+	int32_t* sIperm = nullptr;     // n
 	bool csrValid = true, sellValid = false;
 	int format = 0;                // SpMV layout: 0 SELL-32 (narrow columns when present), 1 CSR vector with `lanes` lanes per row
 	int lanes = 0;                 // CSR SpMV lanes per row (0: default from nnz/row)

@@ -203,7 +203,12 @@ struct MatView {
 	const int32_t* __restrict__ base = nullptr;
 	const int32_t* __restrict__ uni = nullptr;      // SELL-32 stencil slices (L <= 0), or null
 	const int32_t* __restrict__ offs = nullptr;
+	const int32_t* __restrict__ perm = nullptr;     // SELL-32: matrix row of each slot row, or null (identity)
 };
+
+// the matrix row a kernel's slot row `row` (< n) stands for
+template <typename T>
+__device__ __forceinline__ int64_t mat_row(const MatView<T>& A, int64_t row) { return A.perm ? (int64_t)A.perm[row] : row; }
 
 // Resident blocks of 512 threads per SM the SELL-32 row-sum kernels are compiled for: 2 leaves 64
 // registers per thread, enough for the 64 bytes of values in flight per lane of row_sum (eight FP32
@@ -290,7 +295,7 @@ __device__ __forceinline__ AccT row_sum(const MatView<T>& A, int64_t row, int64_
 			const int u = A.uni ? A.uni[sl] : -1;
 			if (u >= 0) {
 				const int32_t* __restrict__ op = A.offs + u;
-				const int r = (int)row;
+				const int r = (int)mat_row(A, row);   // the stencil's offsets are relative to the matrix row
 				auto by_load = [&]() {
 					run([&](int jp) {
 						const int2 o = ldh2(op + 2 * jp, pol.last);
@@ -428,11 +433,11 @@ __device__ __forceinline__ double eval_expr(const DevExpr& e, double t, double x
 // the CSR group size
 inline int exec_lanes(const rsd_csr* A) { return A->format == 0 ? (A->sCol16 ? -1 : 0) : default_lanes(A); }
 inline MatView<double> view64(const rsd_csr* A) {
-	return A->format == 0 ? MatView<double>{A->sStart, A->sCol, A->sVal, A->sCol16, A->sBase, A->sUni, A->sOffs}
+	return A->format == 0 ? MatView<double>{A->sStart, A->sCol, A->sVal, A->sCol16, A->sBase, A->sUni, A->sOffs, A->sPerm}
 	                      : MatView<double>{A->rowPtr, A->col, A->val};
 }
 inline MatView<float> view32(const rsd_csr* A) {
-	return A->format == 0 ? MatView<float>{A->sStart, A->sCol, A->val32, A->sCol16, A->sBase, A->sUni, A->sOffs}
+	return A->format == 0 ? MatView<float>{A->sStart, A->sCol, A->val32, A->sCol16, A->sBase, A->sUni, A->sOffs, A->sPerm}
 	                      : MatView<float>{A->rowPtr, A->col, A->val32};
 }
 template <typename T>

@@ -75,10 +75,11 @@ __global__ void __launch_bounds__(256) k_cg_init(int64_t n, MatView<double> A, c
 		const int64_t row = base + rl.sub;
 		const double ax = row_dot<L, double, double>(A, x, row, n, rl.lane, pol);
 		if (rl.lane == 0 && row < n) {
-			const double ri = ldh(b + row, pol.first) + (-1.0) * ax;
-			const double zi = invD ? ri * ldh(invD + row, pol.last) : ri;
-			sth(r + row, ri, pol.last);
-			sth(p + row, zi, pol.last);
+			const int64_t i = mat_row(A, row);
+			const double ri = ldh(b + i, pol.first) + (-1.0) * ax;
+			const double zi = invD ? ri * ldh(invD + i, pol.last) : ri;
+			sth(r + i, ri, pol.last);
+			sth(p + i, zi, pol.last);
 			v[0] += ri * ri;
 			v[1] += ri * zi;
 		}
@@ -105,7 +106,7 @@ __global__ void __launch_bounds__(kST, kRowBlocks) k_cg_spmv_dot(int64_t n, MatV
 	for (int64_t base = rl.base; base < n; base += rl.step) {
 		const int64_t row = base + rl.sub;
 		const double s = row_dot<L, double, double>(A, p, row, n, rl.lane, pol);
-		if (rl.lane == 0 && row < n) { sth(Ap + row, s, pol.last); v[0] += ldh(p + row, pol.last) * s; }
+		if (rl.lane == 0 && row < n) { const int64_t i = mat_row(A, row); sth(Ap + i, s, pol.last); v[0] += ldh(p + i, pol.last) * s; }
 	}
 	if (grid_sum<1>(v, partials, &S->ticket)) {
 		S->pAp = v[0];
@@ -203,10 +204,11 @@ __global__ void __launch_bounds__(256) k_mx_init(int64_t n, MatView<double> A, c
 		const int64_t row = base + rl.sub;
 		const double ax = row_dot<L, double, double>(A, x, row, n, rl.lane, pol);
 		if (rl.lane == 0 && row < n) {
-			const double r64 = ldh(b + row, pol.first) - ax;
+			const int64_t i = mat_row(A, row);
+			const double r64 = ldh(b + i, pol.first) - ax;
 			const float ri = (float)r64;
-			const float zi = invD ? ri * ldh(invD + row, pol.last) : ri;
-			sth(z + row, zi, pol.last); sth(y + row, 0.0f, pol.last);
+			const float zi = invD ? ri * ldh(invD + i, pol.last) : ri;
+			sth(z + i, zi, pol.last); sth(y + i, 0.0f, pol.last);
 			v[0] += r64 * r64;
 			v[1] += (double)ri * (double)zi;
 		}
@@ -235,7 +237,7 @@ __global__ void __launch_bounds__(kST, kRowBlocks) k_mx_spmv_dot(int64_t n, MatV
 	for (int64_t base = rl.base; base < n; base += rl.step) {
 		const int64_t row = base + rl.sub;
 		const float s = row_dot<L, float, float>(A, z, row, n, rl.lane, pol);
-		if (rl.lane == 0 && row < n) { sth(w + row, s, pol.last); v[0] += (double)ldh(z + row, pol.last) * (double)s; }
+		if (rl.lane == 0 && row < n) { const int64_t i = mat_row(A, row); sth(w + i, s, pol.last); v[0] += (double)ldh(z + i, pol.last) * (double)s; }
 	}
 	if (grid_sum<1>(v, partials, &S->ticket)) S->pAp = v[0];
 }
@@ -339,10 +341,11 @@ __global__ void __launch_bounds__(kST, kRowBlocks) k_mx_reliable(int64_t n, MatV
 		const int64_t row = base + rl.sub;
 		const double ax = row_dot<L, double, double>(A, x, row, n, rl.lane, pol);
 		if (rl.lane == 0 && row < n) {
-			const double r64 = ldh(b + row, pol.first) - ax;
+			const int64_t i = mat_row(A, row);
+			const double r64 = ldh(b + i, pol.first) - ax;
 			const float ri = (float)r64;
-			const float zi = invD ? ri * ldh(invD + row, pol.last) : ri;
-			sth(z + row, zi, pol.last);
+			const float zi = invD ? ri * ldh(invD + i, pol.last) : ri;
+			sth(z + i, zi, pol.last);
 			v[0] += r64 * r64;
 			v[1] += (double)ri * (double)zi;
 		}
@@ -457,7 +460,11 @@ __global__ void __launch_bounds__(kST, kRowBlocks) k_mx_persist(const MxPersistA
 				const int64_t row = base + rl.sub;
 				// z was written by this launch: coherent loads (the .nc path holds no such guarantee)
 				const float sr = row_sum<L, float, float>(a.A32, row, n, rl.lane, pol, [&](int c) { return ldh_rw(a.z + c, pol.last); });
-				if (rl.lane == 0 && row < n) { sth(a.w + row, sr, pol.last); vA[0] += (double)ldh_rw(a.z + row, pol.last) * (double)sr; }
+				if (rl.lane == 0 && row < n) {
+					const int64_t i = mat_row(a.A32, row);
+					sth(a.w + i, sr, pol.last);
+					vA[0] += (double)ldh_rw(a.z + i, pol.last) * (double)sr;
+				}
 			}
 		}
 		if (!grid_allreduce<1>(vA, a.partials, 0, a.count, gen)) { status = RSD_ETIMEOUT; done = 1; break; }
@@ -529,10 +536,11 @@ __global__ void __launch_bounds__(kST, kRowBlocks) k_mx_persist(const MxPersistA
 				const int64_t row = base + rl.sub;
 				const double ax = row_sum<L, double, double>(a.A64, row, n, rl.lane, pol, [&](int c) { return ldh_rw(a.x + c, pol.last); });
 				if (rl.lane == 0 && row < n) {
-					const double r64 = ldh(a.b + row, pol.first) - ax;
+					const int64_t i = mat_row(a.A64, row);
+					const double r64 = ldh(a.b + i, pol.first) - ax;
 					const float ri = (float)r64;
-					const float zi = a.invD ? ri * ldh(a.invD + row, pol.last) : ri;
-					sth(a.z + row, zi, pol.last);
+					const float zi = a.invD ? ri * ldh(a.invD + i, pol.last) : ri;
+					sth(a.z + i, zi, pol.last);
 					vR[0] += r64 * r64;
 					vR[1] += (double)ri * (double)zi;
 				}
@@ -584,7 +592,7 @@ __global__ void __launch_bounds__(256) k_true_res(int64_t n, MatView<double> A, 
 	for (int64_t base = rl.base; base < n; base += rl.step) {
 		const int64_t row = base + rl.sub;
 		const double ax = row_dot<L, double, double>(A, x, row, n, rl.lane, pol);
-		if (rl.lane == 0 && row < n) { const double ri = ldh(b + row, pol.first) - ax; v[0] += ri * ri; }
+		if (rl.lane == 0 && row < n) { const double ri = ldh(b + mat_row(A, row), pol.first) - ax; v[0] += ri * ri; }
 	}
 	if (grid_sum<1>(v, partials, ticket)) *out = sqrt(v[0]);
 }
@@ -1185,7 +1193,7 @@ __global__ void __launch_bounds__(256, 2 * kRowBlocks) k_gm_spmv(int64_t n, MatV
 		const T s = row_sum<L, T, T>(A, row, n, rl.lane, pol, [&](int c) {
 			return invD ? ldh(invD + c, pol.last) * ldh(q + c, pol.last) : ldh(q + c, pol.last);
 		});
-		if (rl.lane == 0 && row < n) sth(w + row, s, pol.last);
+		if (rl.lane == 0 && row < n) sth(w + mat_row(A, row), s, pol.last);
 	}
 }
 
