@@ -539,6 +539,12 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_matrix(const AsmParams prm)
 // in element order, into its column of a shared-memory image of the slice [entry][lane], which the
 // warp then writes out in the pair layout.  Every value is written once: no zero fill, no atomics,
 // and the sums are deterministic.
+// the 1D factors of the reference integrals of 4- and 8-node elements on the problem's Gauss rule:
+// K = int N_i' N_j', M = int N_i N_j, G = int N_i' N_j (the 2D and 3D tables are their products)
+struct Q1Fac {
+	double K[2][2], M[2][2], G[2][2];
+};
+
 constexpr int kRowWarps = 4;
 template <int NSD, int P>
 __global__ void __launch_bounds__(32 * kRowWarps) k_asm_matrix_rows(const AsmParams prm, const int32_t* __restrict__ adjPtr,
@@ -617,9 +623,6 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_asm_matrix_rows(const AsmPar
 // indices (bit d of the local node number).  The table kernel above reads 7 shared-memory entries
 // per (row, element, column) and was bound by the shared-memory pipe; these products cost about 20
 // FP64 operations and no memory.  Same integrals, same summation order per entry.
-struct Q1Fac {
-	double K[2][2], M[2][2], G[2][2];
-};
 template <int NSD>
 __global__ void __launch_bounds__(32 * kRowWarps) k_asm_matrix_rows_q1(const AsmParams prm, const Q1Fac f,
                                                                         const int32_t* __restrict__ adjPtr,
@@ -861,16 +864,45 @@ __global__ void __launch_bounds__(kAsmThreads) k_asm_vector(const AsmParams prm)
 // element (4- and 8-node elements): a warp keeps 32 elements' gathers in flight instead of 32 / G,
 // and the reference integrals (staged in shared memory, rows of npe) are read by all lanes at once.
 // Each element's rows are formed as in the group kernel's affine branch, in the same order.
+// Applying a reference integral of an 8-node element to the element vector as a Kronecker product
+// of 1D factors, one direction at a time: out[a] = sum_b A[a_d][b_d] in[b] over the node pairs
+// that differ only in bit d (16 multiply-adds instead of 64)
+template <int AX>
+__device__ __forceinline__ void kron_stage(const double (&A)[2][2], const double (&in)[8], double (&out)[8]) {
+	constexpr int S = 1 << AX;
+#pragma unroll
+	for (int a = 0; a < 8; ++a) {
+		const int i = (a >> AX) & 1, b0 = a & ~S;
+		out[a] = A[i][0] * in[b0] + A[i][1] * in[b0 | S];
+	}
+}
+// (Ax (x) Ay) applied in x and y to a vector already contracted in z
+__device__ __forceinline__ void kron_xy(const double (&Ax)[2][2], const double (&Ay)[2][2], const double (&in)[8],
+                                        double (&out)[8]) {
+	double t[8];
+	kron_stage<1>(Ay, in, t);
+	kron_stage<0>(Ax, t, out);
+}
+
 template <int NSD, int P, int W>
-__global__ void __launch_bounds__(256) k_asm_vector_elem(const AsmParams prm) {
+__global__ void __launch_bounds__(256) k_asm_vector_elem(const AsmParams prm, const Q1Fac fac) {
 	using E = Elem<NSD, P>;
 	constexpr int NPE = E::NPE, NT = NSD == 3 ? 6 : 3;
 	constexpr bool kGrad = W == 1 || W == 4 || W == 5 || W == 8 || W == 9;
 	static_assert(NPE == 4 || NPE == 8, "one thread per element for 4- and 8-node elements");
 	if (prm.skip && *(volatile const int32_t*)prm.skip) return;   // uniform over the launch
+	// 8-node elements apply the reference integrals as Kronecker products of the 1D factors (no table
+	// reads: the table products were bound by the shared-memory pipe); 4-node ones read the tables
 	extern __shared__ double kt[];
-	for (int i = threadIdx.x; i < (NT + 1) * NPE * NPE; i += blockDim.x) kt[i] = prm.ktab[i];
-	__syncthreads();
+	if constexpr (NSD == 2) {
+		for (int i = threadIdx.x; i < (NT + 1) * NPE * NPE; i += blockDim.x) kt[i] = prm.ktab[i];
+		__syncthreads();
+	}
+	double GT[2][2];
+#pragma unroll
+	for (int i = 0; i < 2; ++i)
+#pragma unroll
+		for (int j = 0; j < 2; ++j) GT[i][j] = fac.G[j][i];
 	const double k0 = kGrad ? (prm.kExpr.n ? eval_expr(prm.kExpr, 0.0, 0.0, 0.0, 0.0, 0.0) : prm.kConst) : 0.0;
 	for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < prm.nelem; idx += (int64_t)gridDim.x * blockDim.x) {
 		const int64_t e = prm.elist ? (int64_t)prm.elist[idx] : idx;
@@ -899,6 +931,67 @@ __global__ void __launch_bounds__(256) k_asm_vector_elem(const AsmParams prm) {
 			Wv[a] = (W == 8 && row >= 0 && prm.Udot) ? prm.Udot[row] : 0.0;
 		}
 		const double detJ = gk[6];
+		if constexpr (NSD == 3) {
+			// the element vector's diffusion and mass products, all rows at once
+			double kd[8], mv[8], mw[8];
+			{
+				double zM[8];
+				kron_stage<2>(fac.M, V, zM);
+				kron_xy(fac.M, fac.M, zM, mv);
+				if constexpr (W == 8) {
+					double wz[8];
+					kron_stage<2>(fac.M, Wv, wz);
+					kron_xy(fac.M, fac.M, wz, mw);
+				}
+				if constexpr (kGrad) {
+					double zK[8], zG[8], zGT[8], t[8], u[8];
+					kron_stage<2>(fac.K, V, zK);
+					kron_stage<2>(fac.G, V, zG);
+					kron_stage<2>(GT, V, zGT);
+					const double c = ke * k0 * detJ;
+					// g = C00 S00 V + C11 S11 V + C22 S22 V + C01 S01 V + C02 S02 V + C12 S12 V
+					kron_xy(fac.K, fac.M, zM, t);
+#pragma unroll
+					for (int a = 0; a < 8; ++a) kd[a] = gk[0] * t[a];
+					kron_xy(fac.M, fac.K, zM, t);
+#pragma unroll
+					for (int a = 0; a < 8; ++a) kd[a] += gk[1] * t[a];
+					kron_xy(fac.M, fac.M, zK, t);
+#pragma unroll
+					for (int a = 0; a < 8; ++a) kd[a] += gk[2] * t[a];
+					kron_xy(fac.G, GT, zM, t);
+					kron_xy(GT, fac.G, zM, u);
+#pragma unroll
+					for (int a = 0; a < 8; ++a) kd[a] += gk[3] * (t[a] + u[a]);
+					kron_xy(fac.G, fac.M, zGT, t);
+					kron_xy(GT, fac.M, zG, u);
+#pragma unroll
+					for (int a = 0; a < 8; ++a) kd[a] += gk[4] * (t[a] + u[a]);
+					kron_xy(fac.M, fac.G, zGT, t);
+					kron_xy(fac.M, GT, zG, u);
+#pragma unroll
+					for (int a = 0; a < 8; ++a) kd[a] = c * (kd[a] + gk[5] * (t[a] + u[a]));
+				}
+			}
+#pragma unroll
+			for (int a = 0; a < NPE; ++a) {
+				const double kdV = kGrad ? kd[a] : 0.0;
+				const double massV = prm.rho * prm.cp * detJ * mv[a];
+				double Fa = 0.0;
+				switch (W) {
+					case 1: Fa = kdV; break;
+					case 2: case 3: Fa = massV; break;
+					case 4: Fa = kdV + prm.coef * massV; break;
+					case 5: Fa = prm.cDiff * kdV + prm.cMass * massV; break;
+					case 7: Fa = prm.coef * massV; break;
+					case 8: Fa = kdV + prm.rho * prm.cp * detJ * mw[a]; break;
+					case 9: Fa = -kdV; break;
+					default: break;
+				}
+				if (rows[a] >= 0) atomicAdd(prm.out + rows[a], prm.outScale * Fa);
+			}
+			continue;
+		}
 #pragma unroll
 		for (int a = 0; a < NPE; ++a) {
 			double kdV = 0.0;
@@ -1900,13 +1993,15 @@ static int launch_vector_mode(rsd_ctx* ctx, dim3 gr, size_t smem, const AsmParam
 
 // one thread per element for all-affine problems of 4- and 8-node elements (RSD_ELEM_VEC=0: the
 // group kernel)
+static Q1Fac q1_factors(const rsd_heat* h);
 template <int NSD, int P>
-static int launch_vector_elem(rsd_ctx* ctx, const AsmParams& p) {
+static int launch_vector_elem(rsd_ctx* ctx, const rsd_heat* h, const AsmParams& p) {
 	constexpr int NPE = Elem<NSD, P>::NPE, NT = NSD == 3 ? 6 : 3;
-	const size_t smem = sizeof(double) * (NT + 1) * NPE * NPE;
+	const size_t smem = NSD == 3 ? 0 : sizeof(double) * (NT + 1) * NPE * NPE;
 	const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((p.nelem + 255) / 256, (int64_t)ctx->num_sms * 16));
+	const Q1Fac fac = q1_factors(h);
 	auto go = [&](auto kern) -> int {
-		kern<<<blocks, 256, smem, ctx->stream>>>(p);
+		kern<<<blocks, 256, smem, ctx->stream>>>(p, fac);
 		RSD_CUDA(cudaGetLastError());
 		return RSD_OK;
 	};
@@ -1927,7 +2022,7 @@ static int launch_k_asm_vector(rsd_ctx* ctx, const rsd_heat* h, const AsmParams&
 	const int nsd = h->m->nsd, ord = h->m->order, G = group_width(h->m->npe);
 	if (p.fast && p.pts == 0 && ord == 1 && p.which != 0 && p.which != 6 && p.nelem > 0) {
 		const char* env = getenv("RSD_ELEM_VEC");
-		if (!(env && env[0] == '0')) return nsd == 3 ? launch_vector_elem<3, 1>(ctx, p) : launch_vector_elem<2, 1>(ctx, p);
+		if (!(env && env[0] == '0')) return nsd == 3 ? launch_vector_elem<3, 1>(ctx, h, p) : launch_vector_elem<2, 1>(ctx, h, p);
 	}
 	const size_t smem = asm_smem_bytes(h->m->npe, h->nq, nsd, p.fast != 0, p.pts);
 	const int epb = kAsmWarps * (32 / G);
@@ -2010,6 +2105,28 @@ static int ensure_adjacency(rsd_ctx* ctx, rsd_heat* h) {
 	return RSD_OK;
 }
 
+// the 1D factors of the 4- and 8-node reference integrals on the problem's rule
+static Q1Fac q1_factors(const rsd_heat* h) {
+	Q1Fac f{};
+	double xq[5], wq[5], N[4], dN[4], Nq[5][2], dNq[5][2];
+	gauss_legendre(h->nq1, xq, wq);
+	for (int q = 0; q < h->nq1; ++q) {
+		lagrange1d(1, xq[q], N, dN);
+		for (int i = 0; i < 2; ++i) { Nq[q][i] = N[i]; dNq[q][i] = dN[i]; }
+	}
+	for (int i = 0; i < 2; ++i)
+		for (int j = 0; j < 2; ++j) {
+			double k = 0.0, m = 0.0, g = 0.0;
+			for (int q = 0; q < h->nq1; ++q) {
+				k += wq[q] * dNq[q][i] * dNq[q][j];
+				m += wq[q] * Nq[q][i] * Nq[q][j];
+				g += wq[q] * dNq[q][i] * Nq[q][j];
+			}
+			f.K[i][j] = k; f.M[i][j] = m; f.G[i][j] = g;
+		}
+	return f;
+}
+
 // the row-gather kernel for an all-affine launch with the slot map (RSD_ROW_ASM=0: the scatter)
 static int launch_matrix_rows(rsd_ctx* ctx, rsd_heat* h, const AsmParams& p, bool* done) {
 	*done = false;
@@ -2029,24 +2146,7 @@ static int launch_matrix_rows(rsd_ctx* ctx, rsd_heat* h, const AsmParams& p, boo
 		return RSD_OK;
 	};
 	if (ord == 1) {
-		// the 1D factors on the problem's rule (the 3D tables are their products)
-		Q1Fac f{};
-		double xq[5], wq[5], N[4], dN[4], Nq[5][2], dNq[5][2];
-		gauss_legendre(h->nq1, xq, wq);
-		for (int q = 0; q < h->nq1; ++q) {
-			lagrange1d(1, xq[q], N, dN);
-			for (int i = 0; i < 2; ++i) { Nq[q][i] = N[i]; dNq[q][i] = dN[i]; }
-		}
-		for (int i = 0; i < 2; ++i)
-			for (int j = 0; j < 2; ++j) {
-				double k = 0.0, m = 0.0, g = 0.0;
-				for (int q = 0; q < h->nq1; ++q) {
-					k += wq[q] * dNq[q][i] * dNq[q][j];
-					m += wq[q] * Nq[q][i] * Nq[q][j];
-					g += wq[q] * dNq[q][i] * Nq[q][j];
-				}
-				f.K[i][j] = k; f.M[i][j] = m; f.G[i][j] = g;
-			}
+		const Q1Fac f = q1_factors(h);
 		const size_t smem1 = sizeof(double) * (size_t)kRowWarps * h->maxSlice * 32;
 		auto go1 = [&](auto kern) -> int {
 			if (smem1 > 48 * 1024) RSD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1));
