@@ -134,6 +134,11 @@ int rsd_csr_info(const rsd_csr* A, int64_t* nrows, int64_t* nnz);
  * slots (entries including padding), slices of 32 rows, and the slices stored as stencil slices
  * (no column indices); any output may be NULL. */
 int rsd_csr_layout(const rsd_csr* A, int64_t* sell_slots, int64_t* slices, int64_t* stencil_slices);
+/* Mirrored stencil slices of the layout (no counterpart in the reference): slices whose entries at
+ * negative column offsets the mixed CG's FP32 SpMV reads from the mirror rows' own entries while the
+ * values are known symmetric to the last bit (as the row-gather assembly of 4- and 8-node elements
+ * writes them); `active` is 1 when the current values qualify.  Either output may be NULL. */
+int rsd_csr_mirrored(const rsd_csr* A, int64_t* mirrored_slices, int32_t* active);
 /* device pointer to the CSR-order values (writes through it are allowed until the next call on A) */
 int rsd_csr_values(rsd_ctx* ctx, rsd_csr* A, double** dvalues);
 int rsd_csr_set_values(rsd_ctx* ctx, rsd_csr* A, const double* host_values);

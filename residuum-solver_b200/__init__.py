@@ -96,6 +96,7 @@ SIGNATURES = {
     "rsd_csr_destroy": [_P],
     "rsd_csr_info": [_P, C.POINTER(_I64), C.POINTER(_I64)],
     "rsd_csr_layout": [_P, C.POINTER(_I64), C.POINTER(_I64), C.POINTER(_I64)],
+    "rsd_csr_mirrored": [_P, C.POINTER(_I64), C.POINTER(_I32)],
     "rsd_csr_values": [_P, _P, C.POINTER(_P)],
     "rsd_csr_set_values": [_P, _P, _P],
     "rsd_csr_get_values": [_P, _P, _P],
@@ -313,7 +314,10 @@ class CSR:
         """SELL-32 slots (padding included), slices and stencil slices of the execution layout."""
         a, b, c = _I64(), _I64(), _I64()
         check(lib().rsd_csr_layout(self.h, C.byref(a), C.byref(b), C.byref(c)))
-        return {"sell_slots": a.value, "slices": b.value, "stencil_slices": c.value}
+        d, e = _I64(), _I32()
+        check(lib().rsd_csr_mirrored(self.h, C.byref(d), C.byref(e)))
+        return {"sell_slots": a.value, "slices": b.value, "stencil_slices": c.value, "mirrored_slices": d.value,
+                "mirrored_active": bool(e.value)}
 
     def pattern(self):
         rp = np.empty(self.n + 1, np.int64)

@@ -2114,12 +2114,14 @@ static Q1Fac q1_factors(const rsd_heat* h) {
 		lagrange1d(1, xq[q], N, dN);
 		for (int i = 0; i < 2; ++i) { Nq[q][i] = N[i]; dNq[q][i] = dN[i]; }
 	}
+	// K and M symmetric to the last bit (one evaluation per pair, mirrored), so that the row-gather
+	// kernel's element entries (a, b) and (b, a) come out equal and so does the assembled matrix
 	for (int i = 0; i < 2; ++i)
 		for (int j = 0; j < 2; ++j) {
 			double k = 0.0, m = 0.0, g = 0.0;
 			for (int q = 0; q < h->nq1; ++q) {
-				k += wq[q] * dNq[q][i] * dNq[q][j];
-				m += wq[q] * Nq[q][i] * Nq[q][j];
+				k += wq[q] * dNq[q][std::min(i, j)] * dNq[q][std::max(i, j)];
+				m += wq[q] * Nq[q][std::min(i, j)] * Nq[q][std::max(i, j)];
 				g += wq[q] * dNq[q][i] * Nq[q][j];
 			}
 			f.K[i][j] = k; f.M[i][j] = m; f.G[i][j] = g;
@@ -2128,8 +2130,9 @@ static Q1Fac q1_factors(const rsd_heat* h) {
 }
 
 // the row-gather kernel for an all-affine launch with the slot map (RSD_ROW_ASM=0: the scatter)
-static int launch_matrix_rows(rsd_ctx* ctx, rsd_heat* h, const AsmParams& p, bool* done) {
+static int launch_matrix_rows(rsd_ctx* ctx, rsd_heat* h, const AsmParams& p, bool* done, bool* symmetric) {
 	*done = false;
+	*symmetric = false;
 	const char* env = getenv("RSD_ROW_ASM");
 	if ((env && env[0] == '0') || !p.fast || p.pts != 0 || !p.ranks || h->maxSlice > 64) return RSD_OK;
 	RSD_CHECK(ensure_adjacency(ctx, h));
@@ -2156,7 +2159,12 @@ static int launch_matrix_rows(rsd_ctx* ctx, rsd_heat* h, const AsmParams& p, boo
 			return RSD_OK;
 		};
 		const char* tabEnv = getenv("RSD_ROW_ASM_TABLES");
-		if (!(tabEnv && tabEnv[0] == '1')) return nsd == 3 ? go1(k_asm_matrix_rows_q1<3>) : go1(k_asm_matrix_rows_q1<2>);
+		if (!(tabEnv && tabEnv[0] == '1')) {
+			// entries (a, b) and (b, a) of an element come out equal and every row sums its elements in
+			// element order: the assembled values are symmetric to the last bit
+			*symmetric = true;
+			return nsd == 3 ? go1(k_asm_matrix_rows_q1<3>) : go1(k_asm_matrix_rows_q1<2>);
+		}
 	}
 	if (nsd == 2 && ord == 1) return go(k_asm_matrix_rows<2, 1>);
 	if (nsd == 2 && ord == 2) return go(k_asm_matrix_rows<2, 2>);
@@ -2186,11 +2194,12 @@ int assemble_matrix(rsd_ctx* ctx, rsd_heat* h, double cDiff, double cMass, doubl
 	A->csrValid = false;
 	A->version++;
 	const int pr = prof_begin(ctx, PF_ASM_MATRIX);
-	bool rows = false;
+	bool rows = false, symmetric = false;
 	// a matrix that already has an FP32 copy in the SELL layout gets it written by the row gather too
 	if (A->val32 && A->format == 0) p.val32 = A->val32;
-	int rc = launch_matrix_rows(ctx, h, p, &rows);
+	int rc = launch_matrix_rows(ctx, h, p, &rows, &symmetric);
 	if (rc == RSD_OK && rows && p.val32) { A->version32 = A->version; A->fmt32 = 0; }
+	if (rc == RSD_OK && rows && symmetric) A->symVersion = A->version;
 	if (rc == RSD_OK && !rows) {
 		RSD_CUDA(cudaMemsetAsync(A->sVal, 0, sizeof(double) * std::max<int64_t>(A->ssize, 1), ctx->stream));
 		rc = launch_k_asm_matrix(ctx, h, p);

@@ -263,7 +263,7 @@ static void free_csr_arrays(rsd_csr* A) {
 	if (!A->owns_pattern) return;   // the pattern belongs to the matrix it was shared from
 	cudaFree(A->rowPtr); cudaFree(A->col); cudaFree(A->diag);
 	cudaFree(A->sStart); cudaFree(A->sCol); cudaFree(A->sSrc); cudaFree(A->sDiag); cudaFree(A->sCol16); cudaFree(A->sBase); cudaFree(A->sUni); cudaFree(A->sOffs);
-	cudaFree(A->sPerm); cudaFree(A->sIperm);
+	cudaFree(A->sPerm); cudaFree(A->sIperm); cudaFree(A->sNeg); cudaFree(A->sMir); cudaFree(A->sMk);
 }
 
 // The row order of the SELL-32 slices (SELL-C-sigma): within windows of kSellWindow rows, rows sorted
@@ -322,7 +322,7 @@ int share_pattern(rsd_ctx* ctx, const rsd_csr* src, rsd_csr** out) {
 	rsd_csr* A = new rsd_csr(*src);
 	A->owns_pattern = false;
 	A->val = nullptr; A->sVal = nullptr; A->val32 = nullptr;
-	A->fmt32 = -1; A->version = 1; A->version32 = 0;
+	A->fmt32 = -1; A->version = 1; A->version32 = 0; A->symVersion = 0;
 	cudaError_t e;
 	if ((e = cudaMalloc(&A->val, sizeof(double) * std::max<int64_t>(A->nnz, 1))) != cudaSuccess ||
 	    (e = cudaMalloc(&A->sVal, sizeof(double) * std::max<int64_t>(A->ssize, 1))) != cudaSuccess ||
@@ -468,6 +468,46 @@ static int upload_csr(rsd_ctx* ctx, int64_t n, const std::vector<int32_t>& rp, c
 		});
 	}
 	const bool stencil = !offTable.empty();
+	// mirrored stencil slices: for a symmetric matrix, entry (i, i + o) with o < 0 equals entry
+	// (i + o, i), which the mirror row stores at offset -o; a slice qualifies when for each of its
+	// negative offsets the mirror rows (one or two slices) are stencil slices holding -o at one common
+	// position.  The SpMV then reads only its own entries from offset 0 on; the mirrored ones come from
+	// rows a few slices back, still in L2.
+	std::vector<int32_t> sNeg, sMir;
+	std::vector<uint8_t> sMk;
+	if (stencil && !permuted) {
+		sNeg.assign(ns, 0);
+		sMir.assign(ns, 0);
+		auto find_off = [&](int64_t t, int32_t off) -> int {
+			if (t < 0 || t >= ns || sUni[t] < 0) return -1;
+			const int32_t* pt = offTable.data() + sUni[t];
+			const int64_t lt = (start[t + 1] - start[t]) / 32;
+			for (int64_t j = 0; j < lt; ++j)
+				if (pt[j] == off) return (int)j;
+			return -1;
+		};
+		for (int64_t sl = 0; sl < ns; ++sl) {
+			if (sUni[sl] < 0) continue;
+			const int32_t* pt = offTable.data() + sUni[sl];
+			const int64_t len = (start[sl + 1] - start[sl]) / 32;
+			int nneg = 0;
+			while (nneg < len && pt[nneg] < 0) ++nneg;
+			if (nneg == 0 || nneg > 32) continue;
+			std::vector<uint8_t> mk(nneg);
+			bool ok = true;
+			for (int j = 0; j < nneg && ok; ++j) {
+				const int64_t m0 = 32 * sl + pt[j], m1 = m0 + 31;   // the mirror rows of the slice's lanes
+				const int a = find_off(m0 >> 5, -pt[j]), b = find_off(m1 >> 5, -pt[j]);
+				ok = a >= 0 && a < 255 && a == b;
+				if (ok) mk[j] = (uint8_t)a;
+			}
+			if (!ok) continue;
+			sNeg[sl] = nneg;
+			sMir[sl] = (int32_t)sMk.size();
+			sMk.insert(sMk.end(), mk.begin(), mk.end());
+			++A->nMirrored;
+		}
+	}
 	// 16-bit columns: every slice's columns within 65,535 of the slice's smallest one
 	bool narrow = ssize > 0;
 	for (int64_t s = 0; s < ns && narrow; ++s) narrow = (int64_t)sMax[s] - sMin[s] <= 65535;
@@ -505,6 +545,14 @@ static int upload_csr(rsd_ctx* ctx, int64_t n, const std::vector<int32_t>& rp, c
 		if ((e = cudaMalloc(&A->sOffs, sizeof(int32_t) * offTable.size())) != cudaSuccess) return fail(e, "cudaMalloc sOffs");
 		if ((e = cudaMemcpyAsync(A->sUni, sUni.data(), sizeof(int32_t) * ns, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload sUni");
 		if ((e = cudaMemcpyAsync(A->sOffs, offTable.data(), sizeof(int32_t) * offTable.size(), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload sOffs");
+	}
+	if (A->nMirrored) {
+		if ((e = cudaMalloc(&A->sNeg, sizeof(int32_t) * ns)) != cudaSuccess) return fail(e, "cudaMalloc sNeg");
+		if ((e = cudaMalloc(&A->sMir, sizeof(int32_t) * ns)) != cudaSuccess) return fail(e, "cudaMalloc sMir");
+		if ((e = cudaMalloc(&A->sMk, sMk.size())) != cudaSuccess) return fail(e, "cudaMalloc sMk");
+		if ((e = cudaMemcpyAsync(A->sNeg, sNeg.data(), sizeof(int32_t) * ns, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload sNeg");
+		if ((e = cudaMemcpyAsync(A->sMir, sMir.data(), sizeof(int32_t) * ns, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload sMir");
+		if ((e = cudaMemcpyAsync(A->sMk, sMk.data(), sMk.size(), cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess) return fail(e, "upload sMk");
 	}
 	if (permuted) {
 		std::vector<int32_t> iperm(n);
@@ -807,6 +855,13 @@ int rsd_csr_layout(const rsd_csr* A, int64_t* sell_slots, int64_t* slices, int64
 	if (sell_slots) *sell_slots = A->ssize;
 	if (slices) *slices = A->nslices;
 	if (stencil_slices) *stencil_slices = A->nStencil;
+	return RSD_OK;
+}
+
+int rsd_csr_mirrored(const rsd_csr* A, int64_t* mirrored_slices, int32_t* active) {
+	if (!A) return set_error(RSD_EINVAL, "null matrix");
+	if (mirrored_slices) *mirrored_slices = A->nMirrored;
+	if (active) *active = (A->format == 0 && A->nMirrored && A->symVersion == A->version && !A->sPerm) ? 1 : 0;
 	return RSD_OK;
 }
 

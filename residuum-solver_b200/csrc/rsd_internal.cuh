@@ -121,6 +121,14 @@ struct rsd_csr {
 	// the inverse; both null when slot row r is row r
 	int32_t* sPerm = nullptr;      // n
 	int32_t* sIperm = nullptr;     // n
+	// mirrored stencil slices (symmetric matrices): slice s reads its first sNeg[s] entries (the
+	// negative offsets o) from the mirror rows r + o, entry sMk[sMir[s] + j] of their slice; 0 reads the
+	// slice whole.  Used while symVersion == version (values assembled symmetric to the last bit).
+	int32_t* sNeg = nullptr;       // nslices (or null)
+	int32_t* sMir = nullptr;       // nslices
+	uint8_t* sMk = nullptr;        // mirrored entries, concatenated
+	int64_t nMirrored = 0;         // slices that read mirrored entries
+	uint64_t symVersion = 0;       // value version known symmetric (0: none)
 	bool csrValid = true, sellValid = false;
 	int format = 0;                // SpMV layout: 0 SELL-32 (narrow columns when present), 1 CSR vector with `lanes` lanes per row
 	int lanes = 0;                 // CSR SpMV lanes per row (0: default from nnz/row)

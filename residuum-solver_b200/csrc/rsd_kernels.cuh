@@ -25,12 +25,13 @@ __device__ __forceinline__ T ld_ro(const T* p) { return __ldg(p); }
 // SpMV after three vector writes).  So: matrix streams and single-use vector traffic are loaded and
 // stored evict-first, the gathered vector evict-last.
 struct L2Pol {
-	uint64_t first, last;
+	uint64_t first, last, normal;
 };
 __device__ __forceinline__ L2Pol make_l2pol() {
 	L2Pol p;
 	asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p.first));
 	asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p.last));
+	asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p.normal));
 	return p;
 }
 __device__ __forceinline__ double ldh(const double* a, uint64_t pol) {
@@ -204,6 +205,11 @@ struct MatView {
 	const int32_t* __restrict__ uni = nullptr;      // SELL-32 stencil slices (L <= 0), or null
 	const int32_t* __restrict__ offs = nullptr;
 	const int32_t* __restrict__ perm = nullptr;     // SELL-32: matrix row of each slot row, or null (identity)
+	// mirrored stencil slices of a symmetric matrix (FP32 row sums only), or null: slice s takes its
+	// first neg[s] entries from the mirror rows, entry mk[mir[s] + j] of their slices
+	const int32_t* __restrict__ neg = nullptr;
+	const int32_t* __restrict__ mir = nullptr;
+	const uint8_t* __restrict__ mk = nullptr;
 };
 
 // the matrix row a kernel's slot row `row` (< n) stands for
@@ -234,8 +240,8 @@ __device__ __forceinline__ AccT row_sum(const MatView<T>& A, int64_t row, int64_
 			const int npair = (A.ptr[sl + 1] - s0) >> 6;
 			const int q0 = s0 + 2 * (int)(row & 31);
 			const T* __restrict__ vp = A.val + q0;
-			auto run = [&](auto colpair) {
-				int jp = 0;
+			uint64_t vpol = pol.first;   // the value stream: read once, unless mirrored reads follow
+			auto run = [&](auto colpair, int jp) {
 				// 64 bytes of values per step (eight FP32 pairs or four FP64 pairs: their value loads,
 				// pattern offsets and gathers issued together), then two pairs, then one; the SpMV
 				// kernels get the registers for it (kRowBlocks)
@@ -244,7 +250,7 @@ __device__ __forceinline__ AccT row_sum(const MatView<T>& A, int64_t row, int64_
 						decltype(ldh2(vp, pol.first)) vv[8];
 						AccT xv[16];
 #pragma unroll
-						for (int k = 0; k < 8; ++k) vv[k] = ldh2(vp + 64 * (jp + k), pol.first);
+						for (int k = 0; k < 8; ++k) vv[k] = ldh2(vp + 64 * (jp + k), vpol);
 #pragma unroll
 						for (int k = 0; k < 8; ++k) {
 							const int2 c = colpair(jp + k);
@@ -259,8 +265,8 @@ __device__ __forceinline__ AccT row_sum(const MatView<T>& A, int64_t row, int64_
 					}
 				}
 				for (; jp + 4 <= npair; jp += 4) {
-					const auto va = ldh2(vp + 64 * jp, pol.first), vb = ldh2(vp + 64 * (jp + 1), pol.first);
-					const auto vc = ldh2(vp + 64 * (jp + 2), pol.first), vd = ldh2(vp + 64 * (jp + 3), pol.first);
+					const auto va = ldh2(vp + 64 * jp, vpol), vb = ldh2(vp + 64 * (jp + 1), vpol);
+					const auto vc = ldh2(vp + 64 * (jp + 2), vpol), vd = ldh2(vp + 64 * (jp + 3), vpol);
 					const int2 ca = colpair(jp), cb = colpair(jp + 1), cc = colpair(jp + 2), cd = colpair(jp + 3);
 					const AccT x0 = xf(ca.x), x1 = xf(ca.y), x2 = xf(cb.x), x3 = xf(cb.y);
 					const AccT x4 = xf(cc.x), x5 = xf(cc.y), x6 = xf(cd.x), x7 = xf(cd.y);
@@ -274,7 +280,7 @@ __device__ __forceinline__ AccT row_sum(const MatView<T>& A, int64_t row, int64_
 					s += (AccT)vd.y * x7;
 				}
 				for (; jp + 2 <= npair; jp += 2) {
-					const auto va = ldh2(vp + 64 * jp, pol.first), vb = ldh2(vp + 64 * (jp + 1), pol.first);
+					const auto va = ldh2(vp + 64 * jp, vpol), vb = ldh2(vp + 64 * (jp + 1), vpol);
 					const int2 ca = colpair(jp), cb = colpair(jp + 1);
 					const AccT x0 = xf(ca.x), x1 = xf(ca.y), x2 = xf(cb.x), x3 = xf(cb.y);
 					s += (AccT)va.x * x0;
@@ -283,7 +289,7 @@ __device__ __forceinline__ AccT row_sum(const MatView<T>& A, int64_t row, int64_
 					s += (AccT)vb.y * x3;
 				}
 				for (; jp < npair; ++jp) {
-					const auto va = ldh2(vp + 64 * jp, pol.first);
+					const auto va = ldh2(vp + 64 * jp, vpol);
 					const int2 ca = colpair(jp);
 					const AccT x0 = xf(ca.x), x1 = xf(ca.y);
 					s += (AccT)va.x * x0;
@@ -300,7 +306,7 @@ __device__ __forceinline__ AccT row_sum(const MatView<T>& A, int64_t row, int64_
 					run([&](int jp) {
 						const int2 o = ldh2(op + 2 * jp, pol.last);
 						return make_int2(r + o.x, r + o.y);
-					});
+					}, 0);
 				};
 				if constexpr (sizeof(T) == 4) {
 					// FP32 values: a stencil slice fills the warp, so lane k holds pattern entry k (read once
@@ -308,9 +314,42 @@ __device__ __forceinline__ AccT row_sum(const MatView<T>& A, int64_t row, int64_
 					// the extra register spills under the 32-register budget, so those keep the loads)
 					if (npair <= 16) {
 						const int mine = __ldg(op + min((int)(row & 31), 2 * npair - 1));
-						run([&](int jp) {
+						auto colpair = [&](int jp) {
 							return make_int2(r + __shfl_sync(0xffffffffu, mine, 2 * jp), r + __shfl_sync(0xffffffffu, mine, 2 * jp + 1));
-						});
+						};
+						const int nn = A.neg ? A.neg[sl] : 0;
+						if (nn > 0) {
+							// a mirrored slice of a symmetric matrix: entries 0..nn-1 (negative offsets o)
+							// from the mirror rows r + o, whose own reads of them went by a few slices ago
+							// (still in L2), then this row's entries from nn on; the sum keeps the pattern
+							// order, so it equals the whole row's to the last bit
+							vpol = pol.normal;
+							const uint8_t* __restrict__ mk = A.mk + A.mir[sl];
+							for (int j = 0; j < nn; j += 8) {
+								T mv[8];
+								AccT mx[8];
+#pragma unroll
+								for (int k = 0; k < 8; ++k) {
+									const int jj = min(j + k, nn - 1);   // clamped: every load issues
+									const int m = r + __shfl_sync(0xffffffffu, mine, jj);
+									const int e = mk[jj];
+									mv[k] = A.val[A.ptr[m >> 5] + 64 * (e >> 1) + 2 * (m & 31) + (e & 1)];
+									mx[k] = xf(m);
+								}
+#pragma unroll
+								for (int k = 0; k < 8; ++k)
+									if (j + k < nn) s += (AccT)mv[k] * mx[k];
+							}
+							int jp = nn >> 1;
+							if (nn & 1) {   // entry nn is the second of pair nn / 2
+								const auto va = ldh2(vp + 64 * jp, vpol);
+								s += (AccT)va.y * xf(r + __shfl_sync(0xffffffffu, mine, nn));
+								++jp;
+							}
+							run(colpair, jp);
+						} else {
+							run(colpair, 0);
+						}
 					} else {
 						by_load();
 					}
@@ -323,10 +362,10 @@ __device__ __forceinline__ AccT row_sum(const MatView<T>& A, int64_t row, int64_
 				run([&](int jp) {
 					const uint32_t w = ldh(reinterpret_cast<const uint32_t*>(cp16 + 64 * jp), pol.first);
 					return make_int2(cb + (int)(w & 0xFFFFu), cb + (int)(w >> 16));
-				});
+				}, 0);
 			} else {
 				const int32_t* __restrict__ cp32 = A.col + q0;
-				run([&](int jp) { return ldh2(cp32 + 64 * jp, pol.first); });
+				run([&](int jp) { return ldh2(cp32 + 64 * jp, pol.first); }, 0);
 			}
 		} else {
 			const int e = A.ptr[row + 1];
@@ -439,6 +478,14 @@ inline MatView<double> view64(const rsd_csr* A) {
 inline MatView<float> view32(const rsd_csr* A) {
 	return A->format == 0 ? MatView<float>{A->sStart, A->sCol, A->val32, A->sCol16, A->sBase, A->sUni, A->sOffs, A->sPerm}
 	                      : MatView<float>{A->rowPtr, A->col, A->val32};
+}
+// the FP32 view with the mirrored slices when the values are known symmetric (the mixed CG's SpMV)
+inline MatView<float> view32_sym(const rsd_csr* A) {
+	MatView<float> V = view32(A);
+	if (A->format == 0 && A->nMirrored && A->symVersion == A->version && !A->sPerm) {
+		V.neg = A->sNeg; V.mir = A->sMir; V.mk = A->sMk;
+	}
+	return V;
 }
 template <typename T>
 inline MatView<T> exec_view(const rsd_csr* A) {

@@ -916,7 +916,11 @@ static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const d
 	RSD_CHECK(f32_sync(ctx, A));
 	const int L = exec_lanes(A);
 	const MatView<double> V = view64(A);
-	const MatView<float> V32 = view32(A);
+	// the mirrored reads of a symmetric matrix are opt-in (RSD_SYM_SPMV=1): on the 128^3 BE system they
+	// cut the value stream to 57 % but the dependent mirror loads (slice start, then value) made the
+	// step slower (7.17 against 4.53 ms)
+	const char* symEnv = getenv("RSD_SYM_SPMV");
+	const MatView<float> V32 = (symEnv && symEnv[0] == '1') ? view32_sym(A) : view32(A);
 	void* wsv;
 	const int64_t ns = pad_len(n);
 	// six FP32 vectors, then the persistent kernel's partial slots and barrier count
@@ -989,7 +993,7 @@ static int cg_mixed(rsd_ctx* ctx, rsd_csr* A, const rsd_solver_cfg* cfg, const d
 	} else if (graph_mode(ctx)) {
 		CgGraph& G = graph_cache(ctx)->cg[1];
 		CgKey key{};
-		const void* ptrs[] = {A, V.ptr, V.col, V.val, V32.val, exec_diag(A), b, x, z, invD, S, partials};
+		const void* ptrs[] = {A, V.ptr, V.col, V.val, V32.val, exec_diag(A), b, x, z, invD, S, partials, V32.neg};
 		std::copy(std::begin(ptrs), std::end(ptrs), key.p);
 		const int64_t ints[] = {n, L, maxIt, rel};
 		std::copy(std::begin(ints), std::end(ints), key.i);

@@ -577,3 +577,35 @@ def test_sorted_slice_layout_matches_natural_layout(rsd, ctx, monkeypatch):
     for key in s0:
         assert abs(s1[key][0] - s0[key][0]) <= 2, key
         assert relerr(s1[key][1], s0[key][1]) <= 1e-9, key
+
+
+def test_mirrored_slices_give_the_same_mixed_solve(rsd, ctx, monkeypatch):
+    """The row-gather assembly of 8-node elements writes K + M/dt symmetric to the last bit; the mixed
+    CG's FP32 SpMV then reads the negative-offset entries of mirrored stencil slices from the mirror
+    rows.  Same row sums in the same order: the solve equals the whole-row one bit for bit.  A write
+    that is not known symmetric turns the mirrored reads off."""
+    h = make_heat(rsd, ctx, 3, 1, 2, [20, 18, 16], [0, 0, 0], [1, 1, 1], src_expr="1 + x*y",
+                  k_elem=np.exp(np.sin(np.arange(20 * 18 * 16))), dirichlet={t: "0" for t in range(6)})
+    h.assemble_matrix(1.0, 1.0 / 1e-3)
+    lay = h.K.layout()
+    assert lay["mirrored_slices"] > 0.5 * lay["slices"] and lay["mirrored_active"]
+    F = ctx.array(h.n)
+    h.assemble_vector(0, F)
+    outs = []
+    for sym in ("1", "0"):
+        monkeypatch.setenv("RSD_SYM_SPMV", sym)
+        for persist in ("1", "0"):
+            monkeypatch.setenv("RSD_CG_PERSIST", persist)
+            x = ctx.array(h.n).zero()
+            rep = rsd.solve(ctx, h.K, F, x, type=rsd.CG, precision=rsd.MIXED, tol=1e-10, max_iters=5000)
+            assert rep["converged"]
+            outs.append((rep["iterations"], x.download()))
+    for it, xv in outs[1:]:
+        assert it == outs[0][0] and np.array_equal(xv, outs[0][1])
+    # values written through the CSR view are not known symmetric: the whole rows are read again
+    h.K.set_values(h.K.values())
+    assert not h.K.layout()["mirrored_active"]
+    monkeypatch.setenv("RSD_SYM_SPMV", "1")
+    x = ctx.array(h.n).zero()
+    rep = rsd.solve(ctx, h.K, F, x, type=rsd.CG, precision=rsd.MIXED, tol=1e-10, max_iters=5000)
+    assert rep["converged"] and rep["iterations"] == outs[0][0] and np.array_equal(x.download(), outs[0][1])
