@@ -16,6 +16,8 @@
 #include <numeric>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "rsd_kernels.cuh"
 
 struct rsd_batch {
@@ -32,6 +34,8 @@ struct rsd_batch {
 
 namespace rsd {
 namespace {
+
+namespace cg = cooperative_groups;
 
 constexpr int kBT = 1024;              // threads per CTA: 32 warps keep enough gathers in flight
 constexpr int kBW = kBT / 32;
@@ -220,6 +224,201 @@ __device__ void solve_one(const BatchProb<TI>& P, BatchOut* out, double tol, int
 	__syncthreads();
 }
 
+// ---- teams: one problem over the kTeam CTAs of a thread-block cluster -----------------------------
+// The work per problem grows about as rows^1.5 (its CG iterations grow with the grid size), so with
+// one CTA per problem the largest problems outlast the rest of the batch by far.  A cluster of kTeam
+// CTAs solves each problem instead: the rows (slices) and vector entries are dealt across the CTAs,
+// the reductions add the CTAs' block sums through distributed shared memory in rank order (the same
+// totals in every CTA, deterministic), and a cluster barrier orders each phase's global writes before
+// the next phase reads them.  Same formulas as solve_one.
+constexpr int kTeam = 4;
+
+template <int NCH>
+__device__ __forceinline__ void team_sum(double (&v)[NCH], double (*sm)[kBW], double (*xch)[4], int& parity) {
+	cg::cluster_group cl = cg::this_cluster();
+	bsum<NCH>(v, sm);
+	if (threadIdx.x == 0)
+#pragma unroll
+		for (int c = 0; c < NCH; ++c) xch[parity][c] = v[c];
+	cl.sync();
+	double t[NCH];
+#pragma unroll
+	for (int c = 0; c < NCH; ++c) t[c] = 0.0;
+	for (int r = 0; r < kTeam; ++r) {
+		const double* rem = cl.map_shared_rank(&xch[parity][0], r);
+#pragma unroll
+		for (int c = 0; c < NCH; ++c) t[c] += rem[c];
+	}
+#pragma unroll
+	for (int c = 0; c < NCH; ++c) v[c] = t[c];
+	parity ^= 1;   // the next sum writes the other slot: a CTA still reading this one has not passed it
+}
+
+// the team's share of one problem's slices; f(row, rowSum) for the rows < n
+template <int L, typename T, typename XF, typename F>
+__device__ __forceinline__ void team_rows(const MatView<T>& A, int64_t n, int64_t nslices, int rank, const L2Pol& pol, XF xf, F f) {
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	for (int64_t sl = (int64_t)rank * kBW + warp; sl < nslices; sl += kBW * kTeam) {
+		const int64_t row = sl * 32 + lane;
+		const double s = (double)row_sum<L, T, T>(A, row, n, 0, pol, xf);
+		if (row < n) f(mat_row(A, row), s);
+	}
+}
+
+template <typename TI, int L>
+__device__ void solve_team(const BatchProb<TI>& P, BatchOut* out, double tol, int relMode, int64_t maxIt, double delta,
+                           int adaptive, double (*sm)[kBW], double (*xch)[4]) {
+	constexpr bool kMixed = sizeof(TI) == 4;
+	constexpr int PW = 16 / sizeof(TI);
+	struct Vec { TI v[PW]; };
+	auto ldv = [](const TI* a) { Vec o; *reinterpret_cast<uint4*>(&o) = *reinterpret_cast<const uint4*>(a); return o; };
+	auto stv = [](TI* a, const Vec& o) { *reinterpret_cast<uint4*>(a) = *reinterpret_cast<const uint4*>(&o); };
+	cg::cluster_group cl = cg::this_cluster();
+	const int rank = (int)cl.block_rank();
+	const int64_t n = P.n;
+	const L2Pol pol = make_l2pol();
+	TI* __restrict__ r = P.r;
+	TI* __restrict__ p = P.p;
+	TI* __restrict__ Ap = P.Ap;
+	TI* __restrict__ y = P.y;
+	TI* __restrict__ invD = P.invD;
+	double* __restrict__ x = P.x;
+	const int64_t gt = (int64_t)rank * kBT + threadIdx.x, gs = (int64_t)kBT * kTeam;   // entry deal
+	int parity = 0;
+	for (int64_t i = gt; i < n; i += gs) {
+		if (invD) {
+			const int32_t q = P.sDiag[i];
+			const double d = q >= 0 ? P.A64.val[q] : 0.0;
+			invD[i] = (TI)(fabs(d) > 1e-300 ? 1.0 / d : 1.0);
+		}
+		y[i] = (TI)0;
+	}
+	cl.sync();
+	auto zr = [&](int64_t i, TI ri) -> TI { return invD ? ri * invD[i] : ri; };
+	auto residual64 = [&](double (&v)[2]) {
+		v[0] = v[1] = 0.0;
+		team_rows<L, double>(P.A64, n, P.nslices, rank, pol, [&](int c) { return x[c] + (double)y[c]; }, [&](int64_t i, double ax) {
+			const double r64 = P.b[i] - ax;
+			const TI ri = (TI)r64;
+			const TI zi = zr(i, ri);
+			r[i] = ri;
+			v[0] += r64 * r64;
+			v[1] += (double)ri * (double)zi;
+		});
+	};
+	double v[2];
+	residual64(v);
+	team_sum<2>(v, sm, xch, parity);
+	for (int64_t i = gt; i < n; i += gs) p[i] = zr(i, r[i]);
+	cl.sync();
+	const double res0 = sqrt(v[0]);
+	double rz = v[1], res = res0, rmax = res0, trueRel = 1.0;
+	int64_t it = 0, refinements = 0;
+	int32_t converged = 0, status = 0;
+	auto crit = [&](double rr) { return relMode ? rr / (res0 + 1e-50) : rr; };
+	if (crit(res0) < tol || n == 0) converged = 1;
+	while (!converged && !status && it < maxIt - 1) {
+		double w[1] = {0.0};
+		team_rows<L, TI>(P.A, n, P.nslices, rank, pol, [&](int c) { return (TI)p[c]; }, [&](int64_t i, double s) {
+			Ap[i] = (TI)s;
+			w[0] += (double)p[i] * (double)(TI)s;
+		});
+		team_sum<1>(w, sm, xch, parity);
+		const double alpha = rz / w[0];
+		if (!isfinite(alpha)) { status = RSD_EBREAKDOWN; break; }
+		const TI a = (TI)alpha;
+		double u[2] = {0.0, 0.0};
+		auto upd = [&](int64_t i, TI pi, TI api, TI ri0, TI di) {
+			if (kMixed) y[i] = y[i] + a * pi;
+			else x[i] = x[i] + alpha * (double)pi;
+			const TI ri = ri0 - a * api;
+			const TI zi = invD ? ri * di : ri;
+			u[0] += (double)ri * (double)ri;
+			u[1] += (double)ri * (double)zi;
+			return ri;
+		};
+		for (int64_t iv = gt; iv < n / PW; iv += gs) {
+			const int64_t i0 = iv * PW;
+			Vec Pv = ldv(p + i0), AP = ldv(Ap + i0), R = ldv(r + i0), D{};
+			if (invD) D = ldv(invD + i0);
+#pragma unroll
+			for (int k = 0; k < PW; ++k) R.v[k] = upd(i0 + k, Pv.v[k], AP.v[k], R.v[k], D.v[k]);
+			stv(r + i0, R);
+		}
+		for (int64_t i = (n / PW) * PW + gt; i < n; i += gs) r[i] = upd(i, p[i], Ap[i], r[i], invD ? invD[i] : (TI)1);
+		team_sum<2>(u, sm, xch, parity);
+		++it;
+		res = sqrt(u[0]);
+		if (!isfinite(res)) { status = RSD_ENAN; break; }
+		double rzNew = u[1];
+		const bool replace = kMixed && (crit(res) < tol || res < delta * rmax || it + 1 >= maxIt);
+		if (replace) {
+			residual64(v);
+			team_sum<2>(v, sm, xch, parity);
+			for (int64_t i = gt; i < n; i += gs) { x[i] += (double)y[i]; y[i] = (TI)0; }
+			const double recurrence = res;
+			res = sqrt(v[0]);
+			if (adaptive) delta = next_delta(delta, recurrence, res, kDeltaFloorBatch);
+			rmax = res;
+			trueRel = res / (res0 + 1e-50);
+			rzNew = v[1];
+			++refinements;
+			if (crit(res) < tol) { converged = 1; break; }
+		} else if (!kMixed && crit(res) < tol) {
+			converged = 1;
+			break;
+		}
+		const TI beta = (TI)(rzNew / rz);
+		rz = rzNew;
+		for (int64_t iv = gt; iv < n / PW; iv += gs) {
+			const int64_t i0 = iv * PW;
+			Vec Pv = ldv(p + i0), R = ldv(r + i0), D{};
+			if (invD) D = ldv(invD + i0);
+#pragma unroll
+			for (int k = 0; k < PW; ++k) Pv.v[k] = Pv.v[k] * beta + (invD ? R.v[k] * D.v[k] : R.v[k]);
+			stv(p + i0, Pv);
+		}
+		for (int64_t i = (n / PW) * PW + gt; i < n; i += gs) p[i] = p[i] * beta + zr(i, r[i]);
+		cl.sync();   // the next product gathers p from every CTA's share
+	}
+	if (kMixed && !converged) {
+		cl.sync();
+		for (int64_t i = gt; i < n; i += gs) { x[i] += (double)y[i]; y[i] = (TI)0; }
+	}
+	if (!kMixed) trueRel = res / (res0 + 1e-50);
+	if (rank == 0 && threadIdx.x == 0) {
+		out->iterations = converged ? it : (status ? it : maxIt);
+		out->refinements = refinements;
+		out->res0 = res0;
+		out->res = res;
+		out->trueRel = trueRel;
+		out->converged = converged;
+		out->status = status;
+	}
+	cl.sync();   // the workspace vectors of this problem are not reused, but the exchange slots are
+}
+
+template <typename TI>
+__global__ void __launch_bounds__(kBT) k_batch_cg_team(const BatchProb<TI>* probs, const int32_t* order, int32_t count,
+                                                       int32_t* next, BatchOut* outs, double tol, int relMode,
+                                                       int64_t maxIt, double delta, int adaptive) {
+	__shared__ double sm[2][kBW];
+	__shared__ double xch[2][4];
+	__shared__ int32_t job;
+	cg::cluster_group cl = cg::this_cluster();
+	for (;;) {
+		if (cl.block_rank() == 0 && threadIdx.x == 0) job = atomicAdd(next, 1);
+		cl.sync();
+		const int32_t j = *cl.map_shared_rank(&job, 0);
+		cl.sync();   // every CTA has read the job before rank 0 takes the next
+		if (j >= count) return;
+		const int32_t pi = order[j];
+		const BatchProb<TI> P = probs[pi];
+		if (P.A.col16) solve_team<TI, -1>(P, outs + pi, tol, relMode, maxIt, delta, adaptive, sm, xch);
+		else solve_team<TI, 0>(P, outs + pi, tol, relMode, maxIt, delta, adaptive, sm, xch);
+	}
+}
+
 template <typename TI>
 __global__ void __launch_bounds__(kBT) k_batch_cg(const BatchProb<TI>* probs, const int32_t* order, int32_t count,
                                                   int32_t* next, BatchOut* outs, double tol, int relMode,
@@ -327,6 +526,34 @@ int rsd_batch_solve(rsd_ctx* ctx, rsd_batch* B, const rsd_solver_cfg* cfg, const
 	};
 	RSD_CHECK(mixed ? fill(float()) : fill(double()));
 	RSD_CUDA(cudaMemsetAsync(B->next, 0, sizeof(int32_t), ctx->stream));
+	// teams of kTeam CTAs (thread-block clusters) per problem when the device launches clusters
+	// (RSD_BATCH_TEAM=0: one CTA per problem)
+	const char* teamEnv = getenv("RSD_BATCH_TEAM");
+	int clusterOk = 0;
+	cudaDeviceGetAttribute(&clusterOk, cudaDevAttrClusterLaunch, ctx->device);
+	if (clusterOk && !(teamEnv && teamEnv[0] == '0')) {
+		const void* tk = mixed ? (const void*)k_batch_cg_team<float> : (const void*)k_batch_cg_team<double>;
+		cudaLaunchConfig_t lc{};
+		cudaLaunchAttribute at[1];
+		at[0].id = cudaLaunchAttributeClusterDimension;
+		at[0].val.clusterDim.x = kTeam; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+		lc.blockDim = dim3(kBT);
+		lc.dynamicSmemBytes = 0;
+		lc.stream = ctx->stream;
+		lc.attrs = at;
+		lc.numAttrs = 1;
+		lc.gridDim = dim3(kTeam * ctx->num_sms);
+		int clusters = 0;
+		RSD_CUDA(cudaOccupancyMaxActiveClusters(&clusters, tk, &lc));
+		clusters = std::max(1, std::min(count, clusters));
+		lc.gridDim = dim3(kTeam * clusters);
+		if (mixed)
+			RSD_CUDA(cudaLaunchKernelEx(&lc, k_batch_cg_team<float>, (const BatchProb<float>*)B->desc, (const int32_t*)B->dorder, count,
+			                            B->next, (BatchOut*)B->out, cfg->tol, rel, cfg->max_iters, delta, adaptive));
+		else
+			RSD_CUDA(cudaLaunchKernelEx(&lc, k_batch_cg_team<double>, (const BatchProb<double>*)B->desc, (const int32_t*)B->dorder, count,
+			                            B->next, (BatchOut*)B->out, cfg->tol, rel, cfg->max_iters, delta, adaptive));
+	} else {
 	int occ = 0;
 	const void* kern = mixed ? (const void*)k_batch_cg<float> : (const void*)k_batch_cg<double>;
 	RSD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kBT, 0));
@@ -337,6 +564,7 @@ int rsd_batch_solve(rsd_ctx* ctx, rsd_batch* B, const rsd_solver_cfg* cfg, const
 	else
 		k_batch_cg<double><<<grid, kBT, 0, ctx->stream>>>((const BatchProb<double>*)B->desc, B->dorder, count, B->next,
 		                                                 (BatchOut*)B->out, cfg->tol, rel, cfg->max_iters, delta, adaptive);
+	}
 	RSD_CUDA(cudaGetLastError());
 	std::vector<BatchOut> h(count);
 	RSD_CUDA(cudaMemcpyAsync(h.data(), B->out, sizeof(BatchOut) * count, cudaMemcpyDeviceToHost, ctx->stream));

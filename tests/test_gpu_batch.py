@@ -101,3 +101,27 @@ def test_batch_edge_cases(rsd, ctx):
     assert not reps[2]["converged"] and reps[2]["iterations"] == 3
     with pytest.raises(rsd.RsdError):
         B.solve([None, b1, F], xs)
+
+
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
+def test_team_and_single_cta_paths_agree(rsd, ctx, prec, monkeypatch):
+    # a cluster of four CTAs per problem (the default) and one CTA per problem (RSD_BATCH_TEAM=0) run
+    # the same PCG with a different reduction order: same convergence, solutions within the tolerance
+    probs = make_problems(rsd, ctx, 12, seed=21)
+    precision = rsd.MIXED if prec == "mixed" else rsd.FP64
+    cfg = rsd.SolverConfig.make(precision=precision, tol=1e-9, max_iters=20000)
+    B = rsd.Batch(ctx, [h.K for h, *_ in probs])
+    runs = []
+    for env in (None, "0"):
+        if env is None:
+            monkeypatch.delenv("RSD_BATCH_TEAM", raising=False)
+        else:
+            monkeypatch.setenv("RSD_BATCH_TEAM", env)
+        xs = [ctx.array(h.n).zero() for h, *_ in probs]
+        reps = B.solve([F for _, F, *_ in probs], xs, cfg)
+        runs.append(([x.download() for x in xs], reps))
+    for (h, F, *_), xa, xb, ra, rb in zip(probs, runs[0][0], runs[1][0], runs[0][1], runs[1][1]):
+        assert ra["converged"] and rb["converged"]
+        assert true_rel(h, F, xa) < 1.0000001e-9 and true_rel(h, F, xb) < 1.0000001e-9
+        assert abs(ra["iterations"] - rb["iterations"]) <= max(2, 0.02 * rb["iterations"])
+        assert relerr(xa, xb) < 1e-6
