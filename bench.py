@@ -864,10 +864,11 @@ def main():
     ap.add_argument("--fd-directions", type=int, default=20)
     ap.add_argument("--transient-adjoint", type=int, default=48, help="mesh size of the transient adjoint workload (0: skip it)")
     ap.add_argument("--transient-steps", type=int, default=10)
-    ap.add_argument("--only", choices=["mixed", "fp64", "fem-product", "spmv-shuffled"], default=None,
+    ap.add_argument("--only", choices=["mixed", "fp64", "fem-product", "spmv-shuffled", "batch"], default=None,
                     help="run one solver path only (no e2e, no CPU leg), 4 matrix-free products on the "
-                         "--fem Q2 mesh, or 4 FP64 + 4 FP32 SpMV on the --size matrix with shuffled node "
-                         "numbers: for profiler captures")
+                         "--fem Q2 mesh, 4 FP64 + 4 FP32 SpMV on the --size matrix with shuffled node "
+                         "numbers, or the batched workload of --batch problems (2 mixed and 2 FP64 batch "
+                         "solves): for profiler captures")
     ap.add_argument("--unstructured", type=int, default=1, help="time SpMV on the shuffled-node matrix too (0: skip it)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -907,6 +908,16 @@ def main():
         if rank == 0:
             print(json.dumps({"only": args.only, "n_free": hq.n, "elements": F ** 3}))
         del hq
+        ctx.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    if args.only == "batch":
+        out = run_batch(rsd, ctx, stream, args.batch, 1, measured_peak_hbm()[0])
+        if rank == 0:
+            print(json.dumps({"only": args.only, **{k: out[k] for k in ("problems", "rows", "nnz")},
+                              **{k: {kk: out[k][kk] for kk in ("ms", "iterations_max", "all_converged")} for k in ("mixed", "fp64")}}))
         ctx.close()
         if dist is not None:
             dist.destroy_process_group()

@@ -57,8 +57,18 @@ struct BatchOut {
 	int32_t converged, status;
 };
 
+// The problem descriptor (two matrix views and the vector pointers, about 60 registers' worth) is
+// copied into shared memory once per problem and read from there: held in registers it pushed the
+// solver loop into local-memory spills.
+template <typename TI>
+__device__ __forceinline__ void load_prob(uint64_t* pbuf, const BatchProb<TI>* src) {
+	static_assert(sizeof(BatchProb<TI>) % 8 == 0, "descriptor of whole 8-byte words");
+	const uint64_t* w = reinterpret_cast<const uint64_t*>(src);
+	for (int k = threadIdx.x; k < (int)(sizeof(BatchProb<TI>) / 8); k += blockDim.x) pbuf[k] = w[k];
+}
+
 // block-wide sums of NCH doubles; every thread receives the totals (fixed order: deterministic)
-template <int NCH>
+template <int NCH, int NW = kBW>
 __device__ __forceinline__ void bsum(double (&v)[NCH], double (*sm)[kBW]) {
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -70,7 +80,7 @@ __device__ __forceinline__ void bsum(double (&v)[NCH], double (*sm)[kBW]) {
 #pragma unroll
 	for (int c = 0; c < NCH; ++c) {
 		double t = 0.0;
-		for (int w = 0; w < kBW; ++w) t += sm[c][w];
+		for (int w = 0; w < NW; ++w) t += sm[c][w];
 		v[c] = t;
 	}
 	__syncthreads();
@@ -82,7 +92,7 @@ __device__ __forceinline__ void slice_rows(const MatView<T>& A, int64_t n, int64
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	for (int64_t sl = warp; sl < nslices; sl += kBW) {
 		const int64_t row = sl * 32 + lane;
-		const double s = (double)row_sum<L, T, T>(A, row, n, 0, pol, xf);
+		const double s = (double)row_sum<L, T, T, false>(A, row, n, 0, pol, xf);
 		if (row < n) f(mat_row(A, row), s);
 	}
 }
@@ -231,12 +241,16 @@ __device__ void solve_one(const BatchProb<TI>& P, BatchOut* out, double tol, int
 // the reductions add the CTAs' block sums through distributed shared memory in rank order (the same
 // totals in every CTA, deterministic), and a cluster barrier orders each phase's global writes before
 // the next phase reads them.  Same formulas as solve_one.
+// Team shape: kTeam CTAs of kBT threads (4 SMs' worth of warps on each problem).  Measured on the
+// 256-problem batch (mixed / FP64 ms): 4 x 1024 threads 133.6 / 134.2; 8 x 512 (128 registers, no
+// spills) 194 / 196; 4 x 512 150 / 153; one CTA of 1024 per problem 159 / 177.  The functions
+// below take the shape as TT threads per CTA and TM CTAs per team.
 constexpr int kTeam = 4;
 
-template <int NCH>
+template <int NCH, int TT, int TM>
 __device__ __forceinline__ void team_sum(double (&v)[NCH], double (*sm)[kBW], double (*xch)[4], int& parity) {
 	cg::cluster_group cl = cg::this_cluster();
-	bsum<NCH>(v, sm);
+	bsum<NCH, TT / 32>(v, sm);
 	if (threadIdx.x == 0)
 #pragma unroll
 		for (int c = 0; c < NCH; ++c) xch[parity][c] = v[c];
@@ -244,7 +258,7 @@ __device__ __forceinline__ void team_sum(double (&v)[NCH], double (*sm)[kBW], do
 	double t[NCH];
 #pragma unroll
 	for (int c = 0; c < NCH; ++c) t[c] = 0.0;
-	for (int r = 0; r < kTeam; ++r) {
+	for (int r = 0; r < TM; ++r) {
 		const double* rem = cl.map_shared_rank(&xch[parity][0], r);
 #pragma unroll
 		for (int c = 0; c < NCH; ++c) t[c] += rem[c];
@@ -255,17 +269,17 @@ __device__ __forceinline__ void team_sum(double (&v)[NCH], double (*sm)[kBW], do
 }
 
 // the team's share of one problem's slices; f(row, rowSum) for the rows < n
-template <int L, typename T, typename XF, typename F>
+template <int L, typename T, int TT, int TM, typename XF, typename F>
 __device__ __forceinline__ void team_rows(const MatView<T>& A, int64_t n, int64_t nslices, int rank, const L2Pol& pol, XF xf, F f) {
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	for (int64_t sl = (int64_t)rank * kBW + warp; sl < nslices; sl += kBW * kTeam) {
+	for (int64_t sl = (int64_t)rank * (TT / 32) + warp; sl < nslices; sl += (TT / 32) * TM) {
 		const int64_t row = sl * 32 + lane;
-		const double s = (double)row_sum<L, T, T>(A, row, n, 0, pol, xf);
+		const double s = (double)row_sum<L, T, T, false>(A, row, n, 0, pol, xf);
 		if (row < n) f(mat_row(A, row), s);
 	}
 }
 
-template <typename TI, int L>
+template <typename TI, int L, int TT, int TM>
 __device__ void solve_team(const BatchProb<TI>& P, BatchOut* out, double tol, int relMode, int64_t maxIt, double delta,
                            int adaptive, double (*sm)[kBW], double (*xch)[4]) {
 	constexpr bool kMixed = sizeof(TI) == 4;
@@ -283,7 +297,7 @@ __device__ void solve_team(const BatchProb<TI>& P, BatchOut* out, double tol, in
 	TI* __restrict__ y = P.y;
 	TI* __restrict__ invD = P.invD;
 	double* __restrict__ x = P.x;
-	const int64_t gt = (int64_t)rank * kBT + threadIdx.x, gs = (int64_t)kBT * kTeam;   // entry deal
+	const int64_t gt = (int64_t)rank * TT + threadIdx.x, gs = (int64_t)TT * TM;   // entry deal
 	int parity = 0;
 	for (int64_t i = gt; i < n; i += gs) {
 		if (invD) {
@@ -297,7 +311,7 @@ __device__ void solve_team(const BatchProb<TI>& P, BatchOut* out, double tol, in
 	auto zr = [&](int64_t i, TI ri) -> TI { return invD ? ri * invD[i] : ri; };
 	auto residual64 = [&](double (&v)[2]) {
 		v[0] = v[1] = 0.0;
-		team_rows<L, double>(P.A64, n, P.nslices, rank, pol, [&](int c) { return x[c] + (double)y[c]; }, [&](int64_t i, double ax) {
+		team_rows<L, double, TT, TM>(P.A64, n, P.nslices, rank, pol, [&](int c) { return x[c] + (double)y[c]; }, [&](int64_t i, double ax) {
 			const double r64 = P.b[i] - ax;
 			const TI ri = (TI)r64;
 			const TI zi = zr(i, ri);
@@ -308,7 +322,7 @@ __device__ void solve_team(const BatchProb<TI>& P, BatchOut* out, double tol, in
 	};
 	double v[2];
 	residual64(v);
-	team_sum<2>(v, sm, xch, parity);
+	team_sum<2, TT, TM>(v, sm, xch, parity);
 	for (int64_t i = gt; i < n; i += gs) p[i] = zr(i, r[i]);
 	cl.sync();
 	const double res0 = sqrt(v[0]);
@@ -319,11 +333,11 @@ __device__ void solve_team(const BatchProb<TI>& P, BatchOut* out, double tol, in
 	if (crit(res0) < tol || n == 0) converged = 1;
 	while (!converged && !status && it < maxIt - 1) {
 		double w[1] = {0.0};
-		team_rows<L, TI>(P.A, n, P.nslices, rank, pol, [&](int c) { return (TI)p[c]; }, [&](int64_t i, double s) {
+		team_rows<L, TI, TT, TM>(P.A, n, P.nslices, rank, pol, [&](int c) { return (TI)p[c]; }, [&](int64_t i, double s) {
 			Ap[i] = (TI)s;
 			w[0] += (double)p[i] * (double)(TI)s;
 		});
-		team_sum<1>(w, sm, xch, parity);
+		team_sum<1, TT, TM>(w, sm, xch, parity);
 		const double alpha = rz / w[0];
 		if (!isfinite(alpha)) { status = RSD_EBREAKDOWN; break; }
 		const TI a = (TI)alpha;
@@ -346,7 +360,7 @@ __device__ void solve_team(const BatchProb<TI>& P, BatchOut* out, double tol, in
 			stv(r + i0, R);
 		}
 		for (int64_t i = (n / PW) * PW + gt; i < n; i += gs) r[i] = upd(i, p[i], Ap[i], r[i], invD ? invD[i] : (TI)1);
-		team_sum<2>(u, sm, xch, parity);
+		team_sum<2, TT, TM>(u, sm, xch, parity);
 		++it;
 		res = sqrt(u[0]);
 		if (!isfinite(res)) { status = RSD_ENAN; break; }
@@ -354,7 +368,7 @@ __device__ void solve_team(const BatchProb<TI>& P, BatchOut* out, double tol, in
 		const bool replace = kMixed && (crit(res) < tol || res < delta * rmax || it + 1 >= maxIt);
 		if (replace) {
 			residual64(v);
-			team_sum<2>(v, sm, xch, parity);
+			team_sum<2, TT, TM>(v, sm, xch, parity);
 			for (int64_t i = gt; i < n; i += gs) { x[i] += (double)y[i]; y[i] = (TI)0; }
 			const double recurrence = res;
 			res = sqrt(v[0]);
@@ -398,24 +412,26 @@ __device__ void solve_team(const BatchProb<TI>& P, BatchOut* out, double tol, in
 	cl.sync();   // the workspace vectors of this problem are not reused, but the exchange slots are
 }
 
-template <typename TI>
-__global__ void __launch_bounds__(kBT) k_batch_cg_team(const BatchProb<TI>* probs, const int32_t* order, int32_t count,
+template <typename TI, int TT, int TM>
+__global__ void __launch_bounds__(TT, 1) k_batch_cg_team(const BatchProb<TI>* probs, const int32_t* order, int32_t count,
                                                        int32_t* next, BatchOut* outs, double tol, int relMode,
                                                        int64_t maxIt, double delta, int adaptive) {
 	__shared__ double sm[2][kBW];
 	__shared__ double xch[2][4];
 	__shared__ int32_t job;
+	__shared__ alignas(16) uint64_t pbuf[sizeof(BatchProb<TI>) / 8];
+	const BatchProb<TI>& P = *reinterpret_cast<const BatchProb<TI>*>(pbuf);
 	cg::cluster_group cl = cg::this_cluster();
 	for (;;) {
 		if (cl.block_rank() == 0 && threadIdx.x == 0) job = atomicAdd(next, 1);
 		cl.sync();
 		const int32_t j = *cl.map_shared_rank(&job, 0);
-		cl.sync();   // every CTA has read the job before rank 0 takes the next
+		if (j < count) load_prob(pbuf, probs + order[j]);
+		cl.sync();   // every CTA has read the job (and its descriptor) before rank 0 takes the next
 		if (j >= count) return;
 		const int32_t pi = order[j];
-		const BatchProb<TI> P = probs[pi];
-		if (P.A.col16) solve_team<TI, -1>(P, outs + pi, tol, relMode, maxIt, delta, adaptive, sm, xch);
-		else solve_team<TI, 0>(P, outs + pi, tol, relMode, maxIt, delta, adaptive, sm, xch);
+		if (P.A.col16) solve_team<TI, -1, TT, TM>(P, outs + pi, tol, relMode, maxIt, delta, adaptive, sm, xch);
+		else solve_team<TI, 0, TT, TM>(P, outs + pi, tol, relMode, maxIt, delta, adaptive, sm, xch);
 	}
 }
 
@@ -425,20 +441,45 @@ __global__ void __launch_bounds__(kBT) k_batch_cg(const BatchProb<TI>* probs, co
                                                   int64_t maxIt, double delta, int adaptive) {
 	__shared__ double sm[2][kBW];
 	__shared__ int32_t job;
+	__shared__ alignas(16) uint64_t pbuf[sizeof(BatchProb<TI>) / 8];
+	const BatchProb<TI>& P = *reinterpret_cast<const BatchProb<TI>*>(pbuf);
 	for (;;) {
 		if (threadIdx.x == 0) job = atomicAdd(next, 1);
 		__syncthreads();
 		const int32_t j = job;
+		if (j < count) load_prob(pbuf, probs + order[j]);
 		__syncthreads();
 		if (j >= count) return;
 		const int32_t pi = order[j];
-		const BatchProb<TI> P = probs[pi];
 		if (P.A.col16) solve_one<TI, -1>(P, outs + pi, tol, relMode, maxIt, delta, adaptive, sm);
 		else solve_one<TI, 0>(P, outs + pi, tol, relMode, maxIt, delta, adaptive, sm);
 	}
 }
 
 int64_t pad_len(int64_t n) { return (n + 63) & ~int64_t(63); }
+
+// one launch of the team kernel: clusters of TM CTAs of TT threads, as many as fit at once (at most
+// one per problem), taking problems from the queue
+template <typename TI, int TT, int TM>
+int launch_team(rsd_ctx* ctx, rsd_batch* B, int32_t count, const rsd_solver_cfg* cfg, int rel, double delta, int adaptive) {
+	cudaLaunchConfig_t lc{};
+	cudaLaunchAttribute at[1];
+	at[0].id = cudaLaunchAttributeClusterDimension;
+	at[0].val.clusterDim.x = TM; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+	lc.blockDim = dim3(TT);
+	lc.dynamicSmemBytes = 0;
+	lc.stream = ctx->stream;
+	lc.attrs = at;
+	lc.numAttrs = 1;
+	lc.gridDim = dim3(TM * ctx->num_sms);
+	int clusters = 0;
+	RSD_CUDA(cudaOccupancyMaxActiveClusters(&clusters, (const void*)k_batch_cg_team<TI, TT, TM>, &lc));
+	clusters = std::max(1, std::min(count, clusters));
+	lc.gridDim = dim3(TM * clusters);
+	RSD_CUDA(cudaLaunchKernelEx(&lc, k_batch_cg_team<TI, TT, TM>, (const BatchProb<TI>*)B->desc, (const int32_t*)B->dorder, count,
+	                            B->next, (BatchOut*)B->out, cfg->tol, rel, cfg->max_iters, delta, adaptive));
+	return RSD_OK;
+}
 
 }  // namespace
 }  // namespace rsd
@@ -526,33 +567,15 @@ int rsd_batch_solve(rsd_ctx* ctx, rsd_batch* B, const rsd_solver_cfg* cfg, const
 	};
 	RSD_CHECK(mixed ? fill(float()) : fill(double()));
 	RSD_CUDA(cudaMemsetAsync(B->next, 0, sizeof(int32_t), ctx->stream));
-	// teams of kTeam CTAs (thread-block clusters) per problem when the device launches clusters
-	// (RSD_BATCH_TEAM=0: one CTA per problem)
+	// teams of kTeam CTAs of kBT threads (thread-block clusters) per problem when the device launches
+	// clusters (RSD_BATCH_TEAM=0: one CTA per problem)
 	const char* teamEnv = getenv("RSD_BATCH_TEAM");
 	int clusterOk = 0;
 	cudaDeviceGetAttribute(&clusterOk, cudaDevAttrClusterLaunch, ctx->device);
 	if (clusterOk && !(teamEnv && teamEnv[0] == '0')) {
-		const void* tk = mixed ? (const void*)k_batch_cg_team<float> : (const void*)k_batch_cg_team<double>;
-		cudaLaunchConfig_t lc{};
-		cudaLaunchAttribute at[1];
-		at[0].id = cudaLaunchAttributeClusterDimension;
-		at[0].val.clusterDim.x = kTeam; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
-		lc.blockDim = dim3(kBT);
-		lc.dynamicSmemBytes = 0;
-		lc.stream = ctx->stream;
-		lc.attrs = at;
-		lc.numAttrs = 1;
-		lc.gridDim = dim3(kTeam * ctx->num_sms);
-		int clusters = 0;
-		RSD_CUDA(cudaOccupancyMaxActiveClusters(&clusters, tk, &lc));
-		clusters = std::max(1, std::min(count, clusters));
-		lc.gridDim = dim3(kTeam * clusters);
-		if (mixed)
-			RSD_CUDA(cudaLaunchKernelEx(&lc, k_batch_cg_team<float>, (const BatchProb<float>*)B->desc, (const int32_t*)B->dorder, count,
-			                            B->next, (BatchOut*)B->out, cfg->tol, rel, cfg->max_iters, delta, adaptive));
-		else
-			RSD_CUDA(cudaLaunchKernelEx(&lc, k_batch_cg_team<double>, (const BatchProb<double>*)B->desc, (const int32_t*)B->dorder, count,
-			                            B->next, (BatchOut*)B->out, cfg->tol, rel, cfg->max_iters, delta, adaptive));
+		const int rc = mixed ? launch_team<float, kBT, kTeam>(ctx, B, count, cfg, rel, delta, adaptive)
+		                     : launch_team<double, kBT, kTeam>(ctx, B, count, cfg, rel, delta, adaptive);
+		RSD_CHECK(rc);
 	} else {
 	int occ = 0;
 	const void* kern = mixed ? (const void*)k_batch_cg<float> : (const void*)k_batch_cg<double>;

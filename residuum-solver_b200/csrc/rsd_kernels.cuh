@@ -227,7 +227,9 @@ constexpr int kRowBlocks = 2;
 // offsets from the slice base; L > 0: CSR with a group of L lanes per row, every lane of the group
 // receiving the total.  Values and columns stream evict-first; xf reads the gathered vector with
 // evict-last.
-template <int L, typename T, typename AccT, typename XF>
+// RND8: FP32 values in rounds of eight pairs (the SpMV kernels, compiled for the registers it needs);
+// false keeps the rounds at four pairs, for callers that hold much other state in registers.
+template <int L, typename T, typename AccT, bool RND8 = true, typename XF>
 __device__ __forceinline__ AccT row_sum(const MatView<T>& A, int64_t row, int64_t n, int lane, const L2Pol& pol, XF xf) {
 	AccT s = AccT(0);
 	if (row < n) {
@@ -245,7 +247,7 @@ __device__ __forceinline__ AccT row_sum(const MatView<T>& A, int64_t row, int64_
 				// 64 bytes of values per step (eight FP32 pairs or four FP64 pairs: their value loads,
 				// pattern offsets and gathers issued together), then two pairs, then one; the SpMV
 				// kernels get the registers for it (kRowBlocks)
-				if constexpr (sizeof(T) == 4) {
+				if constexpr (sizeof(T) == 4 && RND8) {
 					for (; jp + 8 <= npair; jp += 8) {
 						decltype(ldh2(vp, pol.first)) vv[8];
 						AccT xv[16];
