@@ -241,11 +241,13 @@ __device__ void solve_one(const BatchProb<TI>& P, BatchOut* out, double tol, int
 // the reductions add the CTAs' block sums through distributed shared memory in rank order (the same
 // totals in every CTA, deterministic), and a cluster barrier orders each phase's global writes before
 // the next phase reads them.  Same formulas as solve_one.
-// Team shape: kTeam CTAs of kBT threads (4 SMs' worth of warps on each problem).  Measured on the
-// 256-problem batch (mixed / FP64 ms): 4 x 1024 threads 133.6 / 134.2; 8 x 512 (128 registers, no
-// spills) 194 / 196; 4 x 512 150 / 153; one CTA of 1024 per problem 159 / 177.  The functions
-// below take the shape as TT threads per CTA and TM CTAs per team.
-constexpr int kTeam = 4;
+// Team shape: kTeam CTAs of kBT threads.  Measured on the 256-problem batch (mixed / FP64 ms), teams
+// of 1024-thread CTAs: one CTA per problem 159 / 177, 2 CTAs 99.0 / 112.0, 3 CTAs 117.4 / 124.9,
+// 4 CTAs 133.7 / 135.6, 8 CTAs 215 / 199; 512-thread CTAs (128 registers, no spills): 4 x 512 150 /
+// 153, 8 x 512 194 / 196.  Two SMs per problem already shorten the largest problems' iterations,
+// while more problems run at once and each reduction and cluster barrier spans fewer SMs.  The
+// functions below take the shape as TT threads per CTA and TM CTAs per team.
+constexpr int kTeam = 2;
 
 template <int NCH, int TT, int TM>
 __device__ __forceinline__ void team_sum(double (&v)[NCH], double (*sm)[kBW], double (*xch)[4], int& parity) {

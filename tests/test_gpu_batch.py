@@ -105,7 +105,7 @@ def test_batch_edge_cases(rsd, ctx):
 
 @pytest.mark.parametrize("prec", ["mixed", "fp64"])
 def test_team_and_single_cta_paths_agree(rsd, ctx, prec, monkeypatch):
-    # a cluster of four CTAs per problem (the default) and one CTA per problem (RSD_BATCH_TEAM=0) run
+    # a cluster of two CTAs per problem (the default) and one CTA per problem (RSD_BATCH_TEAM=0) run
     # the same PCG with a different reduction order: same convergence, solutions within the tolerance
     probs = make_problems(rsd, ctx, 12, seed=21)
     precision = rsd.MIXED if prec == "mixed" else rsd.FP64
