@@ -234,20 +234,17 @@ __device__ void solve_one(const BatchProb<TI>& P, BatchOut* out, double tol, int
 	__syncthreads();
 }
 
-// ---- teams: one problem over the kTeam CTAs of a thread-block cluster -----------------------------
+// ---- teams: one problem over the CTAs of a thread-block cluster -----------------------------------
 // The work per problem grows about as rows^1.5 (its CG iterations grow with the grid size), so with
-// one CTA per problem the largest problems outlast the rest of the batch by far.  A cluster of kTeam
+// one CTA per problem the largest problems outlast the rest of the batch by far.  A cluster of
 // CTAs solves each problem instead: the rows (slices) and vector entries are dealt across the CTAs,
 // the reductions add the CTAs' block sums through distributed shared memory in rank order (the same
 // totals in every CTA, deterministic), and a cluster barrier orders each phase's global writes before
 // the next phase reads them.  Same formulas as solve_one.
-// Team shape: kTeam CTAs of kBT threads.  Measured on the 256-problem batch (mixed / FP64 ms), teams
-// of 1024-thread CTAs: one CTA per problem 159 / 177, 2 CTAs 99.0 / 112.0, 3 CTAs 117.4 / 124.9,
-// 4 CTAs 133.7 / 135.6, 8 CTAs 215 / 199; 512-thread CTAs (128 registers, no spills): 4 x 512 150 /
-// 153, 8 x 512 194 / 196.  Two SMs per problem already shorten the largest problems' iterations,
-// while more problems run at once and each reduction and cluster barrier spans fewer SMs.  The
-// functions below take the shape as TT threads per CTA and TM CTAs per team.
-constexpr int kTeam = 2;
+// Team shape: TM CTAs of TT threads (kBT; the size is chosen per batch, launch_teams).  Measured on
+// the 256-problem batch (mixed / FP64 ms), teams of 1024-thread CTAs: one CTA per problem 159 / 177,
+// 2 CTAs 99.0 / 112.0, 3 CTAs 117.4 / 124.9, 4 CTAs 133.7 / 135.6, 8 CTAs 215 / 199; 512-thread CTAs
+// (128 registers, no spills): 4 x 512 150 / 153, 8 x 512 194 / 196.
 
 template <int NCH, int TT, int TM>
 __device__ __forceinline__ void team_sum(double (&v)[NCH], double (*sm)[kBW], double (*xch)[4], int& parity) {
@@ -460,12 +457,11 @@ __global__ void __launch_bounds__(kBT) k_batch_cg(const BatchProb<TI>* probs, co
 
 int64_t pad_len(int64_t n) { return (n + 63) & ~int64_t(63); }
 
-// one launch of the team kernel: clusters of TM CTAs of TT threads, as many as fit at once (at most
-// one per problem), taking problems from the queue
+// launch configuration of the team kernel: clusters of TM CTAs of TT threads; *clusters = how many
+// are resident at once
 template <typename TI, int TT, int TM>
-int launch_team(rsd_ctx* ctx, rsd_batch* B, int32_t count, const rsd_solver_cfg* cfg, int rel, double delta, int adaptive) {
-	cudaLaunchConfig_t lc{};
-	cudaLaunchAttribute at[1];
+int team_config(rsd_ctx* ctx, cudaLaunchConfig_t& lc, cudaLaunchAttribute* at, int* clusters) {
+	lc = cudaLaunchConfig_t{};
 	at[0].id = cudaLaunchAttributeClusterDimension;
 	at[0].val.clusterDim.x = TM; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
 	lc.blockDim = dim3(TT);
@@ -474,13 +470,47 @@ int launch_team(rsd_ctx* ctx, rsd_batch* B, int32_t count, const rsd_solver_cfg*
 	lc.attrs = at;
 	lc.numAttrs = 1;
 	lc.gridDim = dim3(TM * ctx->num_sms);
+	*clusters = 0;
+	RSD_CUDA(cudaOccupancyMaxActiveClusters(clusters, (const void*)k_batch_cg_team<TI, TT, TM>, &lc));
+	return RSD_OK;
+}
+
+// one launch of the team kernel with as many clusters as are resident (at most one per problem),
+// taking problems from the queue
+template <typename TI, int TT, int TM>
+int launch_team(rsd_ctx* ctx, rsd_batch* B, int32_t count, const rsd_solver_cfg* cfg, int rel, double delta, int adaptive) {
+	cudaLaunchConfig_t lc;
+	cudaLaunchAttribute at[1];
 	int clusters = 0;
-	RSD_CUDA(cudaOccupancyMaxActiveClusters(&clusters, (const void*)k_batch_cg_team<TI, TT, TM>, &lc));
+	RSD_CHECK((team_config<TI, TT, TM>(ctx, lc, at, &clusters)));
 	clusters = std::max(1, std::min(count, clusters));
 	lc.gridDim = dim3(TM * clusters);
 	RSD_CUDA(cudaLaunchKernelEx(&lc, k_batch_cg_team<TI, TT, TM>, (const BatchProb<TI>*)B->desc, (const int32_t*)B->dorder, count,
 	                            B->next, (BatchOut*)B->out, cfg->tol, rel, cfg->max_iters, delta, adaptive));
 	return RSD_OK;
+}
+
+// The team size for a batch of `count` problems (forced: 2, 4 or 8 CTAs, 0 to choose).  A batch
+// solve ends when its largest problem does, and that problem's iterations shorten with more SMs on
+// it, while smaller teams run more problems at once and span fewer SMs per reduction.  Measured
+// (1024-thread CTAs, mixed ms): 256 problems 99.0 with teams of 2, 133.7 with 4, 215 with 8; 64
+// problems 78.1 with 2, 44.4 with 4.  Rule: the smallest team whose resident clusters number at most
+// two thirds of the problems (every cluster then solves 1.5 problems or more), else 8.
+template <typename TI>
+int launch_teams(rsd_ctx* ctx, rsd_batch* B, int32_t count, const rsd_solver_cfg* cfg, int rel, double delta, int adaptive,
+                 int forced) {
+	int tm = forced;
+	if (tm != 2 && tm != 4 && tm != 8) {
+		cudaLaunchConfig_t lc;
+		cudaLaunchAttribute at[1];
+		int c2 = 0, c4 = 0;
+		RSD_CHECK((team_config<TI, kBT, 2>(ctx, lc, at, &c2)));
+		RSD_CHECK((team_config<TI, kBT, 4>(ctx, lc, at, &c4)));
+		tm = 3 * c2 <= 2 * count ? 2 : (3 * c4 <= 2 * count ? 4 : 8);
+	}
+	if (tm == 2) return launch_team<TI, kBT, 2>(ctx, B, count, cfg, rel, delta, adaptive);
+	if (tm == 4) return launch_team<TI, kBT, 4>(ctx, B, count, cfg, rel, delta, adaptive);
+	return launch_team<TI, kBT, 8>(ctx, B, count, cfg, rel, delta, adaptive);
 }
 
 }  // namespace
@@ -569,14 +599,15 @@ int rsd_batch_solve(rsd_ctx* ctx, rsd_batch* B, const rsd_solver_cfg* cfg, const
 	};
 	RSD_CHECK(mixed ? fill(float()) : fill(double()));
 	RSD_CUDA(cudaMemsetAsync(B->next, 0, sizeof(int32_t), ctx->stream));
-	// teams of kTeam CTAs of kBT threads (thread-block clusters) per problem when the device launches
-	// clusters (RSD_BATCH_TEAM=0: one CTA per problem)
+	// teams of CTAs of kBT threads (thread-block clusters) per problem when the device launches
+	// clusters (RSD_BATCH_TEAM=0: one CTA per problem; 2, 4 or 8: that team size)
 	const char* teamEnv = getenv("RSD_BATCH_TEAM");
 	int clusterOk = 0;
 	cudaDeviceGetAttribute(&clusterOk, cudaDevAttrClusterLaunch, ctx->device);
 	if (clusterOk && !(teamEnv && teamEnv[0] == '0')) {
-		const int rc = mixed ? launch_team<float, kBT, kTeam>(ctx, B, count, cfg, rel, delta, adaptive)
-		                     : launch_team<double, kBT, kTeam>(ctx, B, count, cfg, rel, delta, adaptive);
+		const int forced = teamEnv ? atoi(teamEnv) : 0;
+		const int rc = mixed ? launch_teams<float>(ctx, B, count, cfg, rel, delta, adaptive, forced)
+		                     : launch_teams<double>(ctx, B, count, cfg, rel, delta, adaptive, forced);
 		RSD_CHECK(rc);
 	} else {
 	int occ = 0;

@@ -103,16 +103,17 @@ def test_batch_edge_cases(rsd, ctx):
         B.solve([None, b1, F], xs)
 
 
-@pytest.mark.parametrize("prec", ["mixed", "fp64"])
-def test_team_and_single_cta_paths_agree(rsd, ctx, prec, monkeypatch):
-    # a cluster of two CTAs per problem (the default) and one CTA per problem (RSD_BATCH_TEAM=0) run
-    # the same PCG with a different reduction order: same convergence, solutions within the tolerance
+@pytest.mark.parametrize("prec,team", [("mixed", None), ("fp64", None), ("mixed", "2"), ("mixed", "4"), ("fp64", "8")])
+def test_team_and_single_cta_paths_agree(rsd, ctx, prec, team, monkeypatch):
+    # teams of CTAs per problem (the size chosen for the batch, or forced by RSD_BATCH_TEAM) and one
+    # CTA per problem (RSD_BATCH_TEAM=0) run the same PCG with a different reduction order: same
+    # convergence, solutions within the tolerance
     probs = make_problems(rsd, ctx, 12, seed=21)
     precision = rsd.MIXED if prec == "mixed" else rsd.FP64
     cfg = rsd.SolverConfig.make(precision=precision, tol=1e-9, max_iters=20000)
     B = rsd.Batch(ctx, [h.K for h, *_ in probs])
     runs = []
-    for env in (None, "0"):
+    for env in (team, "0"):
         if env is None:
             monkeypatch.delenv("RSD_BATCH_TEAM", raising=False)
         else:
