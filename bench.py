@@ -864,11 +864,11 @@ def main():
     ap.add_argument("--fd-directions", type=int, default=20)
     ap.add_argument("--transient-adjoint", type=int, default=48, help="mesh size of the transient adjoint workload (0: skip it)")
     ap.add_argument("--transient-steps", type=int, default=10)
-    ap.add_argument("--only", choices=["mixed", "fp64", "fem-product", "spmv-shuffled", "batch"], default=None,
+    ap.add_argument("--only", choices=["mixed", "fp64", "fem-product", "spmv-shuffled", "batch", "newton"], default=None,
                     help="run one solver path only (no e2e, no CPU leg), 4 matrix-free products on the "
                          "--fem Q2 mesh, 4 FP64 + 4 FP32 SpMV on the --size matrix with shuffled node "
-                         "numbers, or the batched workload of --batch problems (2 mixed and 2 FP64 batch "
-                         "solves): for profiler captures")
+                         "numbers, the batched workload of --batch problems (2 mixed and 2 FP64 batch "
+                         "solves), or one mixed Newton solve of the --newton workload: for profiler captures")
     ap.add_argument("--unstructured", type=int, default=1, help="time SpMV on the shuffled-node matrix too (0: skip it)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -907,6 +907,24 @@ def main():
         ctx.sync()
         if rank == 0:
             print(json.dumps({"only": args.only, "n_free": hq.n, "elements": F ** 3}))
+        del hq
+        ctx.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    if args.only == "newton":
+        S = args.newton
+        xq, iq, rq = bm.block_mesh(3, [S] * 3, [0, 0, 0], [1, 1, 1], 2)
+        hq = rsd.Heat(ctx, rsd.Mesh(ctx, 3, 2, xq, iq, rq), 3, k_expr="1 + 0.5*T", dk_expr="0.5", src_expr="10",
+                      dirichlet={0: "0", 1: "1"})
+        U = ctx.array(hq.n).zero()
+        cfg = rsd.SolverConfig.make(type=rsd.GMRES, krylov_dim=30, tol=1e-12, max_iters=100000, precision=rsd.MIXED)
+        rep = hq.newton(U, 1e-10, 1e-10, 50, cfg)
+        ctx.sync()
+        if rank == 0:
+            print(json.dumps({"only": args.only, "n_free": hq.n, "newton_iterations": rep["iterations"],
+                              "gmres_iterations_total": rep["refinements"], "converged": bool(rep["converged"])}))
         del hq
         ctx.close()
         if dist is not None:

@@ -1311,12 +1311,78 @@ __global__ void __launch_bounds__(kGmFusedThreads, 1) k_gm_update_mdot(int64_t n
 	gm_multi_sum<KMAX>(acc, k, partials, ticket, h2);
 }
 
-// CGS pass 2's update fused with the norm: w -= sum_{i<k} h2[i] Q_i, then out = ||w|| of the stored w
+// The Hessenberg least-squares state of one GMRES cycle on the device (gmres/Workspace.hpp:26-31)
+struct GmState {
+	int32_t stop, mLocal, status, breakdown;
+	double tol, denom;    // |g_{j+1}| / denom < tol ends the cycle (denom: res0 + 1e-50 when relative, else 1)
+	int64_t budget;       // Arnoldi steps this cycle may take (the iteration limit's remainder)
+};
+
+// Arnoldi step j: the new column (the two CGS passes' coefficients, hNext), the previous rotations, the
+// next rotation, g; ends the cycle on convergence, breakdown (hNext <= 1e-14), the step budget or a
+// non-finite g (gmres/Solver.tpp:88-110).  One warp: the lanes stage the column and the rotations in
+// shared memory, lane 0 runs the rotations in order (the column entry it carries in a register), the
+// lanes write the column back.
+constexpr int kGmMaxDim = 256;
+struct GmGivensArgs {
+	GmState* S;
+	int j, m;
+	const double* h1;
+	const double* h2;
+	double *H, *cs, *sn, *g;
+};
+// run by one warp (lanes 0..31) with hNext, the new column's last entry, in *hNextp
+__device__ __forceinline__ void gm_givens_warp(const GmGivensArgs& a, const double* __restrict__ hNextp) {
+	__shared__ double hj[kGmMaxDim], c[kGmMaxDim], sv[kGmMaxDim];
+	const int lane = threadIdx.x & 31, j = a.j;
+	const int ld = a.m + 1;   // H column-major: H(i, j) at j * (m + 1) + i
+	double* Hj = a.H + (int64_t)j * ld;
+	for (int i = lane; i <= j; i += 32) hj[i] = __dadd_rn(a.h1[i], a.h2[i]);
+	for (int i = lane; i < j; i += 32) { c[i] = a.cs[i]; sv[i] = a.sn[i]; }
+	__syncwarp();
+	if (lane == 0) {
+		GmState* S = a.S;
+		const double hNext = *hNextp;
+		double x = hj[0];
+		for (int i = 0; i < j; ++i) {
+			const double b = hj[i + 1];
+			hj[i] = __dadd_rn(__dmul_rn(c[i], x), __dmul_rn(sv[i], b));
+			x = __dadd_rn(__dmul_rn(-sv[i], x), __dmul_rn(c[i], b));
+		}
+		const double hjj = x;
+		const double denom = sqrt(__dadd_rn(__dmul_rn(hjj, hjj), __dmul_rn(hNext, hNext)));
+		double cj, sj;
+		if (denom <= 1e-14) { cj = 1.0; sj = 0.0; }
+		else { cj = hjj / denom; sj = hNext / denom; }
+		a.cs[j] = cj; a.sn[j] = sj;
+		hj[j] = __dadd_rn(__dmul_rn(cj, hjj), __dmul_rn(sj, hNext));
+		const double gj = a.g[j];
+		a.g[j] = __dmul_rn(cj, gj);
+		const double gn = __dmul_rn(-sj, gj);
+		a.g[j + 1] = gn;
+		S->mLocal = j + 1;
+		const bool brk = hNext <= 1e-14;
+		S->breakdown = brk;
+		if (!isfinite(gn)) { S->status = RSD_EBREAKDOWN; S->stop = 1; }
+		else if (fabs(gn) / S->denom < S->tol || brk || j + 1 >= S->budget || j + 1 >= a.m) S->stop = 1;
+	}
+	__syncwarp();
+	for (int i = lane; i <= j; i += 32) Hj[i] = hj[i];
+}
+
+__global__ void __launch_bounds__(32) k_gm_givens(const GmGivensArgs a, const double* __restrict__ hNextp) {
+	if (*(volatile const int32_t*)&a.S->stop) return;   // uniform over the warp
+	gm_givens_warp(a, hNextp);
+}
+
+// CGS pass 2's update fused with the norm: w -= sum_{i<k} h2[i] Q_i, then out = ||w|| of the stored w;
+// the last block to finish (it holds the norm) then runs the step's Givens update in its first warp
+// when ga.S is set, which saves the step a launch of its own
 template <typename T, int KMAX>
 __global__ void __launch_bounds__(kGmFusedThreads, 1) k_gm_update_nrm(int64_t n, const T* __restrict__ Q, int64_t ldq, int k,
                                                                  const double* __restrict__ h2, T* __restrict__ w,
                                                                  double* partials, unsigned* ticket, double* out,
-                                                                 const int32_t* stop) {
+                                                                 const int32_t* stop, const GmGivensArgs ga) {
 	if (*(volatile const int32_t*)stop) return;
 	__shared__ double hs[KMAX];
 	if (threadIdx.x < KMAX) hs[threadIdx.x] = threadIdx.x < k ? h2[threadIdx.x] : 0.0;
@@ -1332,31 +1398,38 @@ __global__ void __launch_bounds__(kGmFusedThreads, 1) k_gm_update_nrm(int64_t n,
 		w[e] = wn;
 		v[0] += (double)wn * (double)wn;
 	}
-	if (grid_sum<1>(v, partials, ticket)) *out = sqrt(v[0]);
+	__shared__ int lastBlock;
+	const bool last = grid_sum<1>(v, partials, ticket);   // thread 0 of the last block
+	if (last) *out = sqrt(v[0]);
+	if (ga.S) {
+		if (threadIdx.x == 0) lastBlock = last;
+		__syncthreads();
+		if (lastBlock && threadIdx.x < 32) gm_givens_warp(ga, out);
+	}
 }
 
 template <typename T, int KMAX>
 static int gm_fused_k(rsd_ctx* ctx, int64_t n, const T* Q, int64_t ldq, int k, T* w, double* parts, unsigned* tk,
-                      unsigned* tn, double* h1, double* h2, double* nrm, const int32_t* stop) {
+                      unsigned* tn, double* h1, double* h2, double* nrm, const int32_t* stop, const GmGivensArgs& ga) {
 	cudaStream_t st = ctx->stream;
 	const int g1 = wave_blocks(ctx, k_gm_mdot_k<T, KMAX>, kGmFusedThreads, n);
 	const int g2 = wave_blocks(ctx, k_gm_update_mdot<T, KMAX>, kGmFusedThreads, n);
 	const int g3 = wave_blocks(ctx, k_gm_update_nrm<T, KMAX>, kGmFusedThreads, n);
 	k_gm_mdot_k<T, KMAX><<<g1, kGmFusedThreads, 0, st>>>(n, Q, ldq, k, w, parts, tk, h1, stop);
 	k_gm_update_mdot<T, KMAX><<<g2, kGmFusedThreads, 0, st>>>(n, Q, ldq, k, h1, w, parts, tk, h2, stop);
-	k_gm_update_nrm<T, KMAX><<<g3, kGmFusedThreads, 0, st>>>(n, Q, ldq, k, h2, w, parts, tn, nrm, stop);
+	k_gm_update_nrm<T, KMAX><<<g3, kGmFusedThreads, 0, st>>>(n, Q, ldq, k, h2, w, parts, tn, nrm, stop, ga);
 	RSD_CUDA(cudaGetLastError());
 	return RSD_OK;
 }
 template <typename T>
 static int gm_fused(rsd_ctx* ctx, int64_t n, const T* Q, int64_t ldq, int k, T* w, double* parts, unsigned* tk,
-                    unsigned* tn, double* h1, double* h2, double* nrm, const int32_t* stop) {
-	if (k <= 4) return gm_fused_k<T, 4>(ctx, n, Q, ldq, k, w, parts, tk, tn, h1, h2, nrm, stop);
-	if (k <= 8) return gm_fused_k<T, 8>(ctx, n, Q, ldq, k, w, parts, tk, tn, h1, h2, nrm, stop);
-	if (k <= 12) return gm_fused_k<T, 12>(ctx, n, Q, ldq, k, w, parts, tk, tn, h1, h2, nrm, stop);
-	if (k <= 16) return gm_fused_k<T, 16>(ctx, n, Q, ldq, k, w, parts, tk, tn, h1, h2, nrm, stop);
-	if (k <= 24) return gm_fused_k<T, 24>(ctx, n, Q, ldq, k, w, parts, tk, tn, h1, h2, nrm, stop);
-	return gm_fused_k<T, kGmFusedMax>(ctx, n, Q, ldq, k, w, parts, tk, tn, h1, h2, nrm, stop);
+                    unsigned* tn, double* h1, double* h2, double* nrm, const int32_t* stop, const GmGivensArgs& ga) {
+	if (k <= 4) return gm_fused_k<T, 4>(ctx, n, Q, ldq, k, w, parts, tk, tn, h1, h2, nrm, stop, ga);
+	if (k <= 8) return gm_fused_k<T, 8>(ctx, n, Q, ldq, k, w, parts, tk, tn, h1, h2, nrm, stop, ga);
+	if (k <= 12) return gm_fused_k<T, 12>(ctx, n, Q, ldq, k, w, parts, tk, tn, h1, h2, nrm, stop, ga);
+	if (k <= 16) return gm_fused_k<T, 16>(ctx, n, Q, ldq, k, w, parts, tk, tn, h1, h2, nrm, stop, ga);
+	if (k <= 24) return gm_fused_k<T, 24>(ctx, n, Q, ldq, k, w, parts, tk, tn, h1, h2, nrm, stop, ga);
+	return gm_fused_k<T, kGmFusedMax>(ctx, n, Q, ldq, k, w, parts, tk, tn, h1, h2, nrm, stop, ga);
 }
 
 // out = ||w||
@@ -1400,60 +1473,6 @@ __global__ void k_gm_resnorm(int64_t n, const double* __restrict__ b, const doub
 		v[0] += r * r;
 	}
 	if (grid_sum<1>(v, partials, ticket)) *out = sqrt(v[0]);
-}
-
-// The Hessenberg least-squares state of one GMRES cycle on the device (gmres/Workspace.hpp:26-31)
-struct GmState {
-	int32_t stop, mLocal, status, breakdown;
-	double tol, denom;    // |g_{j+1}| / denom < tol ends the cycle (denom: res0 + 1e-50 when relative, else 1)
-	int64_t budget;       // Arnoldi steps this cycle may take (the iteration limit's remainder)
-};
-
-// Arnoldi step j: the new column (the two CGS passes' coefficients, hNext), the previous rotations, the
-// next rotation, g; ends the cycle on convergence, breakdown (hNext <= 1e-14), the step budget or a
-// non-finite g (gmres/Solver.tpp:88-110).  One warp: the lanes stage the column and the rotations in
-// shared memory, lane 0 runs the rotations in order (the column entry it carries in a register), the
-// lanes write the column back.
-constexpr int kGmMaxDim = 256;
-__global__ void __launch_bounds__(32) k_gm_givens(GmState* S, int j, int m, const double* __restrict__ h1,
-                                                  const double* __restrict__ h2, const double* __restrict__ hNextp,
-                                                  double* __restrict__ H, double* __restrict__ cs, double* __restrict__ sn,
-                                                  double* __restrict__ g) {
-	if (*(volatile const int32_t*)&S->stop) return;   // uniform over the warp
-	__shared__ double hj[kGmMaxDim], c[kGmMaxDim], sv[kGmMaxDim];
-	const int lane = threadIdx.x;
-	const int ld = m + 1;   // H column-major: H(i, j) at j * (m + 1) + i
-	double* Hj = H + (int64_t)j * ld;
-	for (int i = lane; i <= j; i += 32) hj[i] = __dadd_rn(h1[i], h2[i]);
-	for (int i = lane; i < j; i += 32) { c[i] = cs[i]; sv[i] = sn[i]; }
-	__syncwarp();
-	if (lane == 0) {
-		const double hNext = *hNextp;
-		double a = hj[0];
-		for (int i = 0; i < j; ++i) {
-			const double b = hj[i + 1];
-			hj[i] = __dadd_rn(__dmul_rn(c[i], a), __dmul_rn(sv[i], b));
-			a = __dadd_rn(__dmul_rn(-sv[i], a), __dmul_rn(c[i], b));
-		}
-		const double hjj = a;
-		const double denom = sqrt(__dadd_rn(__dmul_rn(hjj, hjj), __dmul_rn(hNext, hNext)));
-		double cj, sj;
-		if (denom <= 1e-14) { cj = 1.0; sj = 0.0; }
-		else { cj = hjj / denom; sj = hNext / denom; }
-		cs[j] = cj; sn[j] = sj;
-		hj[j] = __dadd_rn(__dmul_rn(cj, hjj), __dmul_rn(sj, hNext));
-		const double gj = g[j];
-		g[j] = __dmul_rn(cj, gj);
-		const double gn = __dmul_rn(-sj, gj);
-		g[j + 1] = gn;
-		S->mLocal = j + 1;
-		const bool brk = hNext <= 1e-14;
-		S->breakdown = brk;
-		if (!isfinite(gn)) { S->status = RSD_EBREAKDOWN; S->stop = 1; }
-		else if (fabs(gn) / S->denom < S->tol || brk || j + 1 >= S->budget || j + 1 >= m) S->stop = 1;
-	}
-	__syncwarp();
-	for (int i = lane; i <= j; i += 32) Hj[i] = hj[i];
 }
 
 // back substitution H(0:m, 0:m) y = g(0:m) for the cycle's m = mLocal steps (one thread)
@@ -1627,7 +1646,9 @@ static int gmres_core(rsd_ctx* ctx, Op& op, const rsd_solver_cfg* cfg, const dou
 			const int k = (int)(j + 1);
 			if (k <= kGmFusedMax) {
 				// the two CGS passes in three streaming kernels: dots; update + dots; update + norm
-				RSD_CHECK(gm_fused(ctx, n, Q, ns, k, w, parts, tickets + m, tickets + m + 1, dH1, dH2, dNorm, stop));
+				// the Givens update runs in the last block of the third kernel
+				const GmGivensArgs ga{dS, (int)j, (int)m, dH1, dH2, dH, dCs, dSn, dG};
+				RSD_CHECK(gm_fused(ctx, n, Q, ns, k, w, parts, tickets + m, tickets + m + 1, dH1, dH2, dNorm, stop, ga));
 			} else {
 				for (double* dh : {dH1, dH2}) {
 					k_gm_mdot<T><<<dim3(grd, k), kReduceThreads, 0, st>>>(n, Q, ns, w, parts, tickets, dh, stop);
@@ -1635,8 +1656,10 @@ static int gmres_core(rsd_ctx* ctx, Op& op, const rsd_solver_cfg* cfg, const dou
 				}
 				k_gm_nrm2<T><<<grd, kReduceThreads, 0, st>>>(n, w, parts, tickets + m + 1, dNorm, stop);
 			}
+			if (k > kGmFusedMax) k_gm_givens<<<1, 32, 0, st>>>(GmGivensArgs{dS, (int)j, (int)m, dH1, dH2, dH, dCs, dSn, dG}, dNorm);
+			// after the Givens update: a step that ended the cycle (stop) leaves q_{j+1}, which no one
+			// reads, unwritten
 			k_gm_scale<T><<<gv, 256, 0, st>>>(n, w, dNorm, Q + (j + 1) * ns, stop);
-			k_gm_givens<<<1, 32, 0, st>>>(dS, (int)j, (int)m, dH1, dH2, dNorm, dH, dCs, dSn, dG);
 			RSD_CUDA(cudaGetLastError());
 		}
 		k_gm_backsub<<<1, 1, 0, st>>>(dS, (int)m, dH, dG, dY);
