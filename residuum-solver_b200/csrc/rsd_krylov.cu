@@ -1475,15 +1475,34 @@ __global__ void k_gm_resnorm(int64_t n, const double* __restrict__ b, const doub
 	if (grid_sum<1>(v, partials, ticket)) *out = sqrt(v[0]);
 }
 
-// back substitution H(0:m, 0:m) y = g(0:m) for the cycle's m = mLocal steps (one thread)
-__global__ void k_gm_backsub(const GmState* S, int m, const double* __restrict__ H, const double* __restrict__ g,
-                             double* __restrict__ y) {
-	const int ml = S->mLocal, ld = m + 1;
-	for (int i = ml - 1; i >= 0; --i) {
-		double s = g[i];
-		for (int k = i + 1; k < ml; ++k) s = __dsub_rn(s, __dmul_rn(H[(int64_t)k * ld + i], y[k]));
-		y[i] = s / H[(int64_t)i * ld + i];
+// back substitution H(0:m, 0:m) y = g(0:m) for the cycle's m = mLocal steps: one warp stages the
+// triangle and g in shared memory, lane 0 solves in the serial order (cycles whose triangle does not
+// fit solve from global memory)
+constexpr int kGmBacksubDim = 64;
+__global__ void __launch_bounds__(32) k_gm_backsub(const GmState* S, int m, const double* __restrict__ H,
+                                                   const double* __restrict__ g, double* __restrict__ y) {
+	__shared__ double Hs[kGmBacksubDim * (kGmBacksubDim + 1)], gs[kGmBacksubDim], ys[kGmBacksubDim];
+	const int ml = S->mLocal, ld = m + 1, lane = threadIdx.x;
+	// the triangle's columns 0..ml-1 span ml * ld entries (ld = m + 1): staged when they fit
+	const bool staged = ml <= kGmBacksubDim && (int64_t)ml * ld <= (int64_t)kGmBacksubDim * (kGmBacksubDim + 1);
+	if (staged) {
+		for (int q = lane; q < ml * ld; q += 32) Hs[q] = H[q];   // columns 0..ml-1
+		for (int i = lane; i < ml; i += 32) gs[i] = g[i];
 	}
+	__syncwarp();
+	if (lane == 0) {
+		const double* Hp = staged ? Hs : H;
+		const double* gp = staged ? gs : g;
+		double* yp = staged ? ys : y;
+		for (int i = ml - 1; i >= 0; --i) {
+			double s = gp[i];
+			for (int k = i + 1; k < ml; ++k) s = __dsub_rn(s, __dmul_rn(Hp[(int64_t)k * ld + i], yp[k]));
+			yp[i] = s / Hp[(int64_t)i * ld + i];
+		}
+	}
+	__syncwarp();
+	if (staged)
+		for (int i = lane; i < ml; i += 32) y[i] = ys[i];
 }
 
 // x += M^-1 (sum_i y_i Q_i), accumulated in basis order in FP64, over the cycle's S->mLocal vectors
@@ -1662,7 +1681,7 @@ static int gmres_core(rsd_ctx* ctx, Op& op, const rsd_solver_cfg* cfg, const dou
 			k_gm_scale<T><<<gv, 256, 0, st>>>(n, w, dNorm, Q + (j + 1) * ns, stop);
 			RSD_CUDA(cudaGetLastError());
 		}
-		k_gm_backsub<<<1, 1, 0, st>>>(dS, (int)m, dH, dG, dY);
+		k_gm_backsub<<<1, 32, 0, st>>>(dS, (int)m, dH, dG, dY);
 		k_gm_update_x<T><<<gv, 256, 0, st>>>(n, dS, Q, ns, dY, invD, x);
 		RSD_CUDA(cudaGetLastError());
 		RSD_CUDA(cudaMemcpyAsync(hS, dS, sizeof(GmState), cudaMemcpyDeviceToHost, st));

@@ -267,6 +267,30 @@ def test_mixed_gmres_and_newton(rsd, ctx):
     assert rep["refinements"] >= 1
 
 
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_gmres_long_cycles(rsd, ctx, prec):
+    # Krylov dimensions past the fused orthogonalization (per-vector CGS passes and a Givens launch of
+    # its own beyond 32) and past the shared-memory back substitution (beyond 64 columns): the same
+    # solution as GMRES(30), to the FP64-checked tolerance
+    h = make_heat(rsd, ctx, 3, 2, 3, [6, 5, 4], [0, 0, 0], [1, 1, 1], src_expr="10", k_expr="1 + 0.5*T", dk_expr="0.5",
+                  dirichlet={0: "0", 1: "1"})
+    U = ctx.array(h.n)
+    U.upload(np.linspace(0.0, 1.0, h.n))
+    h.assemble_matrix(1.0, 0.0, 1.0, 0.0, U=U)   # the nonsymmetric Jacobian
+    F = ctx.to_device(np.random.default_rng(5).standard_normal(h.n))
+    rp, col = h.K.pattern()
+    vals = h.K.values()
+    precision = rsd.MIXED if prec == "mixed" else rsd.FP64
+    sols = {}
+    for m in (30, 40, 100):
+        x = ctx.array(h.n).zero()
+        rep = rsd.solve(ctx, h.K, F, x, type=rsd.GMRES, precision=precision, tol=1e-11, max_iters=5000, krylov_dim=m)
+        r = F.download() - oracle.spmv(rp, col, vals, x.download())
+        assert rep["converged"] and np.linalg.norm(r) / np.linalg.norm(F.download()) < 1e-11, (m, rep)
+        sols[m] = x.download()
+    assert relerr(sols[40], sols[30]) < 1e-8 and relerr(sols[100], sols[30]) < 1e-8
+
+
 def random_csr(n, per_row, seed):
     rng = np.random.default_rng(seed)
     rows = []
