@@ -621,10 +621,12 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_asm_matrix_rows(const AsmPar
 // dN_a/dxi_s dN_b/dxi_t (symmetrised for s != t) and of N_a N_b is a product over the directions of
 // the 1D integrals K = int N_i' N_j', M = int N_i N_j and G = int N_i' N_j with i, j the nodes' 1D
 // indices (bit d of the local node number).  The table kernel above reads 7 shared-memory entries
-// per (row, element, column) and was bound by the shared-memory pipe; these products cost about 20
-// FP64 operations and no memory.  Same integrals, same summation order per entry.
+// per (row, element, column) and was bound by the shared-memory pipe; here the element's row is formed
+// with the last direction factored out (about 14 FP64 operations per entry, no memory), and every row
+// sums its elements in element order.  Compiled for 4 resident 128-thread blocks (128 registers):
+// 0.408 ms per 128^3 assembly against 0.420 ms for the unfactored products at the compiler's choice.
 template <int NSD>
-__global__ void __launch_bounds__(32 * kRowWarps) k_asm_matrix_rows_q1(const AsmParams prm, const Q1Fac f,
+__global__ void __launch_bounds__(32 * kRowWarps, 4) k_asm_matrix_rows_q1(const AsmParams prm, const Q1Fac f,
                                                                         const int32_t* __restrict__ adjPtr,
                                                                         const int32_t* __restrict__ adj, int64_t n, int32_t maxLen) {
 	constexpr int NPE = NSD == 3 ? 8 : 4, RB = 8;
@@ -676,34 +678,55 @@ __global__ void __launch_bounds__(32 * kRowWarps) k_asm_matrix_rows_q1(const Asm
 							Gc[d][c] = ia ? f.G[c][1] : f.G[c][0];   // int N_a N_b'
 						}
 					}
+					// entry (a, b) = cd sum_t C_t S_t(a, b) + cm M(a, b) with S_t and M products of the
+					// 1D factors; the last direction is factored out, entry = M_z A + K_z B + (G_z C + G'_z D)
+					// with A..D per column pair of the other directions.  The two sums of mirrored products
+					// (the cross terms, and G_z C + G'_z D, whose C and D trade places when a and b do) are
+					// rounded without contraction, so that entries (a, b) and (b, a) come out equal
+					double c[6];
 #pragma unroll
-					for (int b = 0; b < NPE; ++b) {
-						const int j = (int)((w[k] >> (8 * b)) & 0xFF);
-						if (j == 0xFF) continue;
-						const int b0 = b & 1, b1 = (b >> 1) & 1, b2 = (b >> 2) & 1;
-						double g, mass;
+					for (int t = 0; t < 6; ++t) c[t] = cd * gk[k][t];
+					constexpr int NB = NSD == 3 ? 4 : 2;   // column pairs / columns of the other directions
+#pragma unroll
+					for (int bl = 0; bl < NB; ++bl) {
+						const int b0 = bl & 1, b1 = (bl >> 1) & 1;
+						double A, B = 0.0, Cz = 0.0, Dz = 0.0;
 						if constexpr (NSD == 3) {
-							const double m12 = Mm[1][b1] * Mm[2][b2], m02 = Mm[0][b0] * Mm[2][b2], m01 = Mm[0][b0] * Mm[1][b1];
-							const double s00 = Km[0][b0] * m12, s11 = Km[1][b1] * m02, s22 = Km[2][b2] * m01;
-							const double s01 = (Gr[0][b0] * Gc[1][b1] + Gc[0][b0] * Gr[1][b1]) * Mm[2][b2];
-							const double s02 = (Gr[0][b0] * Gc[2][b2] + Gc[0][b0] * Gr[2][b2]) * Mm[1][b1];
-							const double s12 = (Gr[1][b1] * Gc[2][b2] + Gc[1][b1] * Gr[2][b2]) * Mm[0][b0];
-							g = gk[k][0] * s00;
-							g += gk[k][1] * s11;
-							g += gk[k][2] * s22;
-							g += gk[k][3] * s01;
-							g += gk[k][4] * s02;
-							g += gk[k][5] * s12;
-							mass = Mm[0][b0] * m12;
+							const double m01 = Mm[0][b0] * Mm[1][b1];
+							const double x01 = __dadd_rn(__dmul_rn(Gr[0][b0], Gc[1][b1]), __dmul_rn(Gc[0][b0], Gr[1][b1]));
+							A = c[0] * (Km[0][b0] * Mm[1][b1]);
+							A += c[1] * (Mm[0][b0] * Km[1][b1]);
+							A += c[3] * x01;
+							A += cm * m01;
+							B = c[2] * m01;
+							const double p4 = c[4] * Mm[1][b1], p5 = c[5] * Mm[0][b0];
+							Cz = __dadd_rn(__dmul_rn(p4, Gc[0][b0]), __dmul_rn(p5, Gc[1][b1]));   // coefficient of G_z (row)
+							Dz = __dadd_rn(__dmul_rn(p4, Gr[0][b0]), __dmul_rn(p5, Gr[1][b1]));   // coefficient of G'_z
 						} else {
-							const double s00 = Km[0][b0] * Mm[1][b1], s11 = Mm[0][b0] * Km[1][b1];
-							const double s01 = Gr[0][b0] * Gc[1][b1] + Gc[0][b0] * Gr[1][b1];
-							g = gk[k][0] * s00;
-							g += gk[k][1] * s11;
-							g += gk[k][2] * s01;
-							mass = Mm[0][b0] * Mm[1][b1];
+							A = 0.0;
 						}
-						acc[j * 32] += cd * g + cm * mass;
+#pragma unroll
+						for (int bz = 0; bz < 2; ++bz) {
+							const int b = NSD == 3 ? bl | (bz << 2) : (bl | (bz << 1));
+							const int j = (int)((w[k] >> (8 * b)) & 0xFF);
+							if (j == 0xFF) continue;
+							double v;
+							if constexpr (NSD == 3) {
+								v = Mm[2][bz] * A;
+								v += Km[2][bz] * B;
+								v += __dadd_rn(__dmul_rn(Gr[2][bz], Cz), __dmul_rn(Gc[2][bz], Dz));
+							} else {
+								// 2D: entry = cd (C0 K_x M_y + C1 M_x K_y + C2 (G_x G'_y + G'_x G_y)) + cm M_x M_y
+								const int bx = bl;
+								const double mm = Mm[0][bx] * Mm[1][bz];
+								const double x01 = __dadd_rn(__dmul_rn(Gr[0][bx], Gc[1][bz]), __dmul_rn(Gc[0][bx], Gr[1][bz]));
+								v = c[0] * (Km[0][bx] * Mm[1][bz]);
+								v += c[1] * (Mm[0][bx] * Km[1][bz]);
+								v += c[2] * x01;
+								v += cm * mm;
+							}
+							acc[j * 32] += v;
+						}
 					}
 				}
 			}
