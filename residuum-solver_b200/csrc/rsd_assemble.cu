@@ -653,9 +653,10 @@ __global__ void __launch_bounds__(32 * kRowWarps, 4) k_asm_matrix_rows_q1(const 
 				for (int k = 0; k < ABATCH; ++k) {
 					if (ea[k] < 0) continue;
 					const int32_t e = ea[k] / NPE;
-					const double2* gp = reinterpret_cast<const double2*>(prm.geo + (int64_t)e * 8);
-#pragma unroll
-					for (int i = 0; i < 4; ++i) { const double2 v = gp[i]; gk[k][2 * i] = v.x; gk[k][2 * i + 1] = v.y; }
+					// the 64-byte geometry record (64-byte aligned) in two 32-byte loads
+					const double* gp = prm.geo + (int64_t)e * 8;
+					ld_nc_v4(gp, gk[k][0], gk[k][1], gk[k][2], gk[k][3]);
+					ld_nc_v4(gp + 4, gk[k][4], gk[k][5], gk[k][6], gk[k][7]);
 					gk[k][7] = prm.kElem ? prm.kElem[e] : 1.0;
 					w[k] = __ldcs(reinterpret_cast<const unsigned long long*>(prm.ranks + (int64_t)ea[k] * RB));
 				}
@@ -930,9 +931,8 @@ __global__ void __launch_bounds__(256) k_asm_vector_elem(const AsmParams prm, co
 	for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < prm.nelem; idx += (int64_t)gridDim.x * blockDim.x) {
 		const int64_t e = prm.elist ? (int64_t)prm.elist[idx] : idx;
 		double gk[8];
-		const double2* gp2 = reinterpret_cast<const double2*>(prm.geo + e * 8);
-#pragma unroll
-		for (int i = 0; i < 4; ++i) { const double2 v = gp2[i]; gk[2 * i] = v.x; gk[2 * i + 1] = v.y; }
+		ld_nc_v4(prm.geo + e * 8, gk[0], gk[1], gk[2], gk[3]);   // the 64-byte record in two 32-byte loads
+		ld_nc_v4(prm.geo + e * 8 + 4, gk[4], gk[5], gk[6], gk[7]);
 		const double ke = prm.kElem ? prm.kElem[e] : 1.0;
 		int32_t rows[NPE];
 		double V[NPE], Wv[NPE];

@@ -93,6 +93,11 @@ __device__ __forceinline__ void sth(float* a, float v, uint64_t pol) {
 	asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(a), "f"(v), "l"(pol) : "memory");
 }
 
+// 32 bytes per lane in one load (sm_100's 256-bit vector loads), read-only path; p 32-byte aligned
+__device__ __forceinline__ void ld_nc_v4(const double* p, double& a, double& b, double& c, double& d) {
+	asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];" : "=d"(a), "=d"(b), "=d"(c), "=d"(d) : "l"(p));
+}
+
 // 16-byte packets for the element-wise Krylov kernels (4 floats or 2 doubles per load/store)
 template <typename T> struct Pk;
 template <> struct Pk<float> { static constexpr int W = 4; float v[4]; };
