@@ -1195,13 +1195,15 @@ def main():
     t_hbm = asm_bytes / (peak * 1e9) * 1e3
     t_fp64 = asm_flops / (fp64.value * 1e12) * 1e3
     asm_ms = prof_mx["assemble_matrix"][1] / max(prof_mx["assemble_matrix"][0], 1) if "assemble_matrix" in prof_mx else None
-    asm_roof = {"kernel": "k_asm_matrix_rows (K + M/dt with its FP32 copy, one launch per step)", "bound": "hbm",
+    asm_roof = {"kernel": "k_asm_matrix_rows_q1 (K + M/dt with its FP32 copy, one launch per step)", "bound": "hbm",
                 "bytes": asm_bytes, "flops": asm_flops, "hbm_ms": t_hbm, "fp64_ms": t_fp64,
                 "achieved_ms": asm_ms, "achieved_gbs": asm_bytes / (asm_ms * 1e6) if asm_ms else None,
                 "frac": t_hbm / asm_ms if asm_ms else None, "peak_gbs": peak, "peak_kind": peak_kind,
                 "path_bytes": path_bytes, "fp64_tflops": fp64.value, "layout": lay,
                 "note": "frac = kernel bytes / measured HBM copy peak / event-timed duration; the executed flops "
-                        "(reference-element integrals) need 3% of the duration at the measured FP64 rate"}
+                        "(reference-element integrals) need %s of the duration at the measured FP64 rate; ncu: the "
+                        "L1/tex pipe on the element-record loads bounds it (k_asm_matrix_rows_q1_96.md)"
+                        % (f"{100 * t_fp64 / asm_ms:.0f}%" if asm_ms else "a fraction")}
 
     # the dominant kernel's roofline on the bytes it moves: DRAM traffic per launch from the ncu
     # capture of this workload (dram__bytes_read.sum + dram__bytes_write.sum) over the event-timed
