@@ -89,8 +89,6 @@ __global__ void k_be_rate(int64_t n, double inv_dt, const double* __restrict__ U
 	for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
 		Ud[i] = inv_dt * U[i] + (-inv_dt) * Up[i];
 }
-// |F - R| with the deterministic grid reduction: axpby(1, -1, F, R) then norm(R)
-// (BackwardEulerStage.hpp:120-122), without storing F - R
 // k_e = exp(theta_e): the per-element conductivity multiplier of the adjoint pair
 __global__ void k_exp_theta(int64_t ne, const double* __restrict__ theta, double* __restrict__ kElem) {
 	for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne; e += (int64_t)gridDim.x * blockDim.x)
@@ -108,6 +106,8 @@ __global__ void k_accumulate(int64_t ne, const double* __restrict__ g, double* _
 		acc[e] += g[e];
 }
 
+// |F - R| with the deterministic grid reduction: axpby(1, -1, F, R) then norm(R)
+// (BackwardEulerStage.hpp:120-122), without storing F - R
 __global__ void k_diff_norm(int64_t n, const double* __restrict__ F, const double* __restrict__ R, double* partials,
                             unsigned* ticket, double* out) {
 	double v[1] = {0.0};
